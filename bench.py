@@ -1,0 +1,405 @@
+#!/usr/bin/env python
+"""Benchmark of the gooseberry sparse hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload NAME]
+
+Default workload (N=1): plain FP64 conjugate gradient on the 2D 5-point
+Laplacian of a 1024x1024 grid (n = 1,048,576, nnz = 5,238,784), b uniform in
+[-1, 1] (seed 2), x0 = 0, stop at ||r|| <= 1e-8 ||b|| or 5000 iterations --
+the reference's cgd contract (src/cgd.c:40-129).  One step = one full solve
+with the matrix and b already in HBM; L2 is flushed (256 MB write) between
+steps, outside the timed events.  `value` = solves/s over all ranks.
+
+Other workloads (--workload): spmv_uniform (100k x 100k, 10 nnz/row, FP64),
+spmv_powerlaw (8M rows, 128M nnz, power-law rows, FP64 and FP32).
+
+--impl reference times the reference's own OpenMP CPU code (oracle/_ref,
+else the oracle restatement) on this host's cores for the same workload and
+metric, on a bounded sample of iterations per step.
+
+Multi-GPU: the path runs on one GPU; with --gpus N (under torchrun) every rank
+runs an independent replica (no data-path collective), timing is the max over
+ranks and `value` sums all ranks' solves ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+PROFILES = os.path.join(ROOT, "profiles")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_PATH) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs, copy burst)"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
+
+
+def ncu_traffic(kernel_key: str):
+    """Per-launch DRAM bytes of a kernel from a committed ncu summary
+    (profiles/*.txt lines `traffic_bytes_per_launch <key> <bytes> <scale>`)."""
+    if not os.path.isdir(PROFILES):
+        return None
+    for fn in sorted(os.listdir(PROFILES)):
+        if not fn.endswith(".txt"):
+            continue
+        with open(os.path.join(PROFILES, fn)) as f:
+            for ln in f:
+                parts = ln.split()
+                if len(parts) >= 3 and parts[0] == "traffic_bytes_per_launch" \
+                        and parts[1] == kernel_key:
+                    return float(parts[2])
+    return None
+
+
+# ---- distributed plumbing -------------------------------------------------------
+
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---- clocks -----------------------------------------------------------------------
+
+class Clocks:
+    """nvidia-smi sampled every 200 ms while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+        self.err = None
+
+    def start(self):
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(self.dev)
+            sel = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+        except Exception:
+            sel = str(self.dev)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", sel, f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception as e:  # no nvidia-smi
+            self.err = str(e)
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        rows = [[c.strip() for c in ln.split(",")] for ln in self.lines if ln.count(",") >= 8]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [],
+                    "note": self.err or "no samples"}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4)
+                          if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ---- workloads --------------------------------------------------------------------
+
+def cg_laplace_setup():
+    from gooseberry_b200 import workloads as W
+    L = W.laplacian_2d(1024)
+    b = W.rhs(L.nrows, 2)
+    return L, b
+
+
+REF_CG_ITERS_FALLBACK = None
+
+
+def reference_cg_iterations():
+    """The reference's iteration count on the full system (committed golden,
+    generated by tests/golden/make_golden.py from the reference itself)."""
+    p = os.path.join(ROOT, "tests", "golden", "full_sizes.json")
+    try:
+        with open(p) as f:
+            return int(json.load(f)["cg_laplace_1024"]["iterations"])
+    except Exception:
+        return None
+
+
+def cpu_cg_sample(L, b, rtol, iters_full, budget_s=10.0, threads=None):
+    """Time the reference cgd (oracle/_ref, else the restatement) for a bounded
+    number of iterations on this host; returns (solves/s, info)."""
+    import oracle
+    threads = threads or os.cpu_count() or 1
+    err = rtol * float(np.linalg.norm(b))
+    kind = "reference" if oracle.ref_available("f64") else "port"
+    if kind == "reference":
+        oracle.ref_set_threads(threads)
+
+        def run(k):
+            return oracle.ref_cgd(L.rowptr, L.rowind, L.rowval, b, err, k)
+    else:
+        def run(k):
+            return oracle.cgd(L.rowptr, L.rowind, L.rowval, b, err, k, threads=threads)
+    t0 = time.perf_counter()
+    run(10)
+    t_iter = (time.perf_counter() - t0) / 10
+    k = int(max(20, min(iters_full, budget_s / max(t_iter, 1e-9))))
+    t0 = time.perf_counter()
+    _, done, _ = run(k)
+    dt = time.perf_counter() - t0
+    t_iter = dt / max(done, 1)
+    solves = 1.0 / (t_iter * iters_full)
+    return solves, {"kind": kind, "cores": threads, "iterations_timed": done,
+                    "seconds": dt, "s_per_iteration": t_iter}
+
+
+def run_cg_laplace(args, dist: Dist):
+    import torch
+
+    import gooseberry_b200 as gb
+
+    dev = dist.local if torch.cuda.device_count() > dist.local else 0
+    torch.cuda.set_device(dev)
+    L, b = cg_laplace_setup()
+    n, nnz = L.nrows, L.nnz
+    rtol, niter = 1e-8, 5000
+    A = gb.CsrMatrix.from_host(L)
+    A.autotune()
+    S = gb.CgSolver(A)
+    bd = torch.from_numpy(b).cuda()
+    xd = torch.empty_like(bd)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    # live per-kernel timing (first iterations of a real solve)
+    ms_a, ms_b = S.profile(bd, iterations=40)
+    bytes_a = 4 * (n + 1) + 12 * nnz + 32 * n   # rowptr, ind+val, r & p gathered, p & Ap written
+    bytes_b = 48 * n                             # x, p, r, Ap read; x, r written
+    bytes_textbook = 4 * (n + 1) + 12 * nnz + 14 * 8 * n
+
+    for _ in range(args.warmup):
+        S.solve(bd, xd, tol=rtol, relative=True, niter=niter)
+    torch.cuda.synchronize()
+
+    clocks = Clocks(dev)
+    clocks.start()
+    dist.barrier()
+    torch.cuda.synchronize()
+    evs = []
+    results = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _, r = S.solve(bd, xd, tol=rtol, relative=True, niter=niter)
+        e1.record()
+        evs.append((e0, e1))
+        results.append(r)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    t_local = sum(a.elapsed_time(b_) for a, b_ in evs) / 1e3
+    t_max = dist.max(t_local)
+    solves_total = dist.sum(float(args.steps))
+    iters = results[-1].iterations
+    assert all(r.status == "converged" for r in results), [r.status for r in results]
+
+    # end to end through the drop-in C ABI, host (pinned) buffers, copies timed
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
+        t.numpy()[...] = a
+        return t.numpy()
+    h_rp, h_ri, h_rv, h_b = pinned(L.rowptr.view(np.int32)).view(np.uint32), \
+        pinned(L.rowind.view(np.int32)).view(np.uint32), pinned(L.rowval), pinned(b)
+    err_abs = rtol * float(np.linalg.norm(b))
+    gb.cgd(h_rp, h_ri, h_rv, h_b, err_abs, niter)  # warm
+    e2e_steps = max(1, min(args.steps, 3))
+    dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        xh, it_e2e, _ = gb.cgd(h_rp, h_ri, h_rv, h_b, err_abs, niter)
+    t_e2e = dist.max(time.perf_counter() - t0)
+    h2d = 4 * (n + 1) + 4 * nnz + 8 * nnz + 8 * n
+    d2h = 8 * n
+
+    peak, peak_src = hbm_peak()
+    ach_a = bytes_a / (ms_a * 1e-3) / 1e9
+    out = {
+        "metric": "CG solves/s (FP64, 2D 5-point Laplacian 1024x1024, rel-res 1e-8)",
+        "value": solves_total / t_max,
+        "unit": "solves/s",
+        "n_gpus": dist.world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": t_max / args.steps * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic: seeded b ~ U[-1,1] (seed 2), exact 5-point Laplacian",
+        "config": {
+            "workload": "cg_laplace2d_1024 (plain FP64 CG, x0=0, rel-res 1e-8, max 5000 it)",
+            "n": n, "nnz": nnz, "rtol": rtol, "niter": niter, "iterations": iters,
+            "reference_iterations": reference_cg_iterations(),
+            "schedule": gb.SCHED_NAMES[A.info().schedule],
+            "tile_items": A.info().tile_items,
+            "l2": "flushed between steps (256 MB write, outside the timed events)",
+            "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "single GPU",
+        },
+        "roofline": {
+            "bound": "hbm", "kernel": "cg_a_kernel (SpMV + p update + p.Ap)",
+            "achieved": ach_a, "peak": peak, "unit": "GB/s", "frac": ach_a / peak,
+            "traffic": ncu_traffic("cg_a_laplace1024"),
+            "bytes_per_launch": bytes_a, "launch_ms": ms_a, "peak_source": peak_src,
+        },
+        "kernels": {
+            "cg_a_ms": ms_a, "cg_b_ms": ms_b,
+            "cg_b_gbs": bytes_b / (ms_b * 1e-3) / 1e9,
+            "iteration_ms": (t_local / args.steps) / iters * 1e3,
+            "iteration_textbook_gbs": bytes_textbook * iters * args.steps / t_local / 1e9,
+            "bytes_per_iteration_fused": bytes_a + bytes_b,
+            "bytes_per_iteration_textbook": bytes_textbook,
+        },
+        "e2e": {"value": e2e_steps * dist.world / t_e2e, "unit": "solves/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "api": "gooseberry_cgd_f64 (host pinned buffers)", "iterations": it_e2e},
+        "gpu_launches": int(sum(r.kernel_launches for r in results)),
+        "clocks": clk,
+    }
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        ref_it = reference_cg_iterations() or iters
+        v, info = cpu_cg_sample(L, b, rtol, ref_it)
+        out["cpu_baseline"] = {
+            "value": v, "unit": "solves/s", "cores": info["cores"], "kind": info["kind"],
+            "sample": (f"{info['iterations_timed']} of the {ref_it} iterations of one solve "
+                       f"({info['seconds']:.1f} s, {info['s_per_iteration'] * 1e3:.2f} ms/it), "
+                       "scaled to a full solve"),
+        }
+    return out
+
+
+def run_reference_cg(args):
+    L, b = cg_laplace_setup()
+    ref_it = reference_cg_iterations() or 2966
+    cores = os.cpu_count() or 1
+    vals = []
+    info = None
+    for k in range(args.warmup + args.steps):
+        v, info = cpu_cg_sample(L, b, 1e-8, ref_it, budget_s=max(2.0, 60.0 / max(
+            args.steps + args.warmup, 1)), threads=cores)
+        if k >= args.warmup:
+            vals.append(v)
+    v = float(np.median(vals))
+    return {
+        "impl": "reference",
+        "metric": "CG solves/s (FP64, 2D 5-point Laplacian 1024x1024, rel-res 1e-8)",
+        "value": v, "unit": "solves/s", "n_gpus": 0, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: seeded b ~ U[-1,1] (seed 2), exact 5-point Laplacian",
+        "config": {"workload": "cg_laplace2d_1024 (plain FP64 CG, x0=0, rel-res 1e-8, max 5000 it)",
+                   "n": L.nrows, "nnz": L.nnz, "reference_iterations": ref_it},
+        "cpu_baseline": {"value": v, "unit": "solves/s", "cores": info["cores"],
+                         "kind": info["kind"],
+                         "sample": (f"per step {info['iterations_timed']} of {ref_it} "
+                                    "iterations of the reference cgd, scaled to a full solve")},
+        "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="cg_laplace2d")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+
+    if args.impl == "reference":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return 0
+        out = run_reference_cg(args)
+        print(json.dumps(out), flush=True)
+        return 0
+
+    dist = Dist()
+    try:
+        if args.workload == "cg_laplace2d":
+            out = run_cg_laplace(args, dist)
+        else:
+            raise SystemExit(f"unknown workload {args.workload}")
+        if dist.rank == 0:
+            print(json.dumps(out), flush=True)
+    finally:
+        dist.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

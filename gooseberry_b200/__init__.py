@@ -1,0 +1,412 @@
+"""gooseberry_b200 -- B200 (sm_100a) implementation of gooseberry's sparse hot
+path: CSR SpMV (reference ``src/blas.c:552-606``) and the conjugate-gradient
+solver built on it (``src/cgd.c:40-129``).
+
+Everything here is a thin ctypes layer over ``libgooseberry_b200.so``, whose
+C ABI is declared in ``include/gooseberry.h`` (the reference's drop-in entry
+points, host pointers) and ``include/gooseberry_b200.h`` (device-resident
+matrices, SpMV, BLAS-1 and CG solvers).  There is no CPU fallback: if the
+library is missing every call raises.
+
+Host-pointer API (mirrors the reference's public functions)::
+
+    spmult(rowptr, rowind, rowval, B, ...)   # gooseberry_spmult
+    scale(v, s), add_scalar(v, s)            # gooseberry_scale / _add_scalar
+    cgd(rowptr, rowind, rowval, b, error, niter)   # cgd
+
+Device API (torch CUDA tensors as device memory)::
+
+    A = CsrMatrix.from_host(csr)            # or CsrMatrix.from_device(...)
+    A.spmv(x, y)                             # y = A x
+    CgSolver(A).solve(b, x, tol=1e-8, relative=True, niter=5000)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+__all__ = [
+    "GooseberryError", "lib", "spmult", "scale", "add_scalar", "cgd",
+    "CsrMatrix", "CgSolver", "CgResult", "dot", "SUCCESS",
+    "SCHED_AUTO", "SCHED_THREAD", "SCHED_GROUP4", "SCHED_GROUP8", "SCHED_WARP",
+    "SCHED_MERGE", "CG_F64", "CG_MIXED", "plan_tiles",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgooseberry_b200.so")
+
+SUCCESS = 1
+ERROR_NAMES = {
+    1: "SUCCESS", 2: "UNIMPLEMENTED", 3: "INVALIDINPUT", 4: "READ", 5: "WRITE",
+    6: "FILENOTFOUND", 7: "PERMISSIONDENIED", 8: "UNKNOWN",
+}
+VALUES_F64, VALUES_F32, DEVICE_POINTERS = 0x1, 0x2, 0x4
+SCHED_AUTO, SCHED_THREAD, SCHED_GROUP4, SCHED_GROUP8, SCHED_WARP, SCHED_MERGE = range(6)
+SCHED_NAMES = {0: "auto", 1: "thread", 2: "group4", 3: "group8", 4: "warp", 5: "merge"}
+CG_F64, CG_MIXED = 0, 1
+CG_STATUS = {0: "converged", 1: "maxiter", 2: "breakdown", 3: "nonfinite"}
+
+
+class GooseberryError(RuntimeError):
+    def __init__(self, code: int, where: str, msg: str):
+        super().__init__(f"{where}: {ERROR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class CsrInfo(C.Structure):
+    _fields_ = [("nrows", C.c_uint32), ("ncols", C.c_uint32), ("nnz", C.c_uint32),
+                ("ntiles", C.c_uint32), ("nlong", C.c_uint32), ("max_row", C.c_uint32),
+                ("mean_row", C.c_double), ("row_p50", C.c_uint32), ("row_p90", C.c_uint32),
+                ("row_p99", C.c_uint32), ("schedule", C.c_int), ("schedule_f32", C.c_int),
+                ("tile_items", C.c_uint32)]
+
+
+class _CgResult(C.Structure):
+    _fields_ = [("iterations", C.c_size_t), ("refinements", C.c_size_t),
+                ("rnorm", C.c_double), ("bnorm", C.c_double), ("status", C.c_int),
+                ("kernel_launches", C.c_size_t)]
+
+
+_LIB = None
+
+_vp, _u32, _sz, _d, _f, _i = C.c_void_p, C.c_uint32, C.c_size_t, C.c_double, C.c_float, C.c_int
+
+# name -> (restype, argtypes); every symbol the headers declare
+SIGNATURES = {
+    "gb_last_error": (C.c_char_p, []),
+    "gooseberry_scale": (_i, [_u32, _vp, _f]),
+    "gooseberry_scale_f64": (_i, [_u32, _vp, _d]),
+    "gooseberry_add_scalar": (_i, [_u32, _vp, _f]),
+    "gooseberry_add_scalar_f64": (_i, [_u32, _vp, _d]),
+    "gooseberry_spmult": (_i, [_u32, _u32, _u32, _vp, _vp, _vp, _vp, _vp, _vp, _u32]),
+    "gooseberry_spmult_f64": (_i, [_u32, _u32, _u32, _vp, _vp, _vp, _vp, _vp, _vp, _u32]),
+    "gooseberry_cgd": (_i, [_u32, _vp, _vp, _vp, _vp, _vp, _f, _sz, _vp, _vp, _vp, _sz]),
+    "gooseberry_cgd_f64": (_i, [_u32, _vp, _vp, _vp, _vp, _vp, _d, _sz, _vp, _vp, _vp, _sz]),
+    "gb_csr_create": (_i, [_u32, _u32, _u32, _vp, _vp, _vp, _vp, C.c_uint, _vp, _vp]),
+    "gb_csr_destroy": (_i, [_vp]),
+    "gb_csr_get_info": (_i, [_vp, _vp]),
+    "gb_csr_set_schedule": (_i, [_vp, C.c_uint, _i, _u32]),
+    "gb_csr_autotune": (_i, [_vp, C.c_uint, _vp]),
+    "gb_plan_tiles_host": (_i, [_u32, _vp, _u32, _u32, _vp, _sz, _vp, _vp, _vp]),
+    "gb_spmv_f64": (_i, [_vp, _vp, _vp, _vp]),
+    "gb_spmv_f32": (_i, [_vp, _vp, _vp, _vp]),
+    "gb_spmm_f64": (_i, [_vp, _u32, _vp, _vp, _vp]),
+    "gb_dot_f64": (_i, [_sz, _vp, _vp, _vp, _vp]),
+    "gb_dot_f32": (_i, [_sz, _vp, _vp, _vp, _vp]),
+    "gb_scale_f64": (_i, [_sz, _vp, _d, _vp]),
+    "gb_add_scalar_f64": (_i, [_sz, _vp, _d, _vp]),
+    "gb_add_f64": (_i, [_sz, _vp, _vp, _vp, _vp]),
+    "gb_sub_f64": (_i, [_sz, _vp, _vp, _vp, _vp]),
+    "gb_scale_f32": (_i, [_sz, _vp, _f, _vp]),
+    "gb_add_scalar_f32": (_i, [_sz, _vp, _f, _vp]),
+    "gb_cg_create": (_i, [_vp, _i, _vp]),
+    "gb_cg_destroy": (_i, [_vp]),
+    "gb_cg_solve": (_i, [_vp, _vp, _vp, _d, _i, _sz, _vp, _sz, _vp, _vp]),
+    "gb_cg_profile": (_i, [_vp, _vp, _sz, _vp, _sz, _vp, _vp]),
+}
+
+
+def lib():
+    """The loaded C library (raises if it was not built)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m gooseberry_b200.build` "
+                "(there is no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def last_error() -> str:
+    return (lib().gb_last_error() or b"").decode(errors="replace")
+
+
+def _check(rc: int, where: str) -> None:
+    if rc != SUCCESS:
+        raise GooseberryError(rc, where, last_error())
+
+
+def _ptr(a) -> int | None:
+    """Data pointer of a numpy array or torch tensor (None for None)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()
+
+
+def _stream_ptr(stream) -> int | None:
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+# ---- host-pointer API (the reference's entry points) ----------------------------
+
+def _real(dtype) -> str:
+    dt = np.dtype(dtype)
+    if dt == np.float64:
+        return "f64"
+    if dt == np.float32:
+        return "f32"
+    raise TypeError(f"values must be float32 or float64, got {dt}")
+
+
+def spmult(rowptr, rowind, rowval, B, ncols: int | None = None, bncols: int = 1,
+           blocks=None, out=None):
+    """C = A B through ``gooseberry_spmult`` (reference ``include/gooseberry.h:174-184``).
+
+    ``B`` is column-major (``B[j*ncols + l]``), the result row-major
+    (``C[i*bncols + j]``).  float64 values use ``gooseberry_spmult_f64``,
+    float32 the float ABI.  With ``blocks`` only those row ranges are written
+    (``out`` keeps its other rows)."""
+    rowval = np.ascontiguousarray(rowval)
+    real = _real(rowval.dtype)
+    dt = rowval.dtype
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+    rowind = np.ascontiguousarray(rowind, dtype=np.uint32)
+    B = np.ascontiguousarray(B, dtype=dt).reshape(-1)
+    n = len(rowptr) - 1
+    ncols = n if ncols is None else int(ncols)
+    if out is None:
+        out = np.zeros(n * bncols, dtype=dt)
+    assert out.dtype == dt and out.flags.c_contiguous and out.size >= n * bncols
+    bl = None if blocks is None else np.ascontiguousarray(blocks, dtype=np.uint32)
+    nb = 0 if bl is None else len(bl) - 1
+    fn = lib().gooseberry_spmult_f64 if real == "f64" else lib().gooseberry_spmult
+    _check(fn(n, ncols, bncols, _ptr(rowptr), _ptr(rowind), _ptr(rowval), _ptr(B),
+              _ptr(out), _ptr(bl), nb), "gooseberry_spmult")
+    return out
+
+
+def scale(v: np.ndarray, s: float) -> np.ndarray:
+    """v *= s in place through ``gooseberry_scale`` (``include/gooseberry.h:134-137``)."""
+    real = _real(v.dtype)
+    assert v.flags.c_contiguous
+    fn = lib().gooseberry_scale_f64 if real == "f64" else lib().gooseberry_scale
+    _check(fn(v.size, _ptr(v), s), "gooseberry_scale")
+    return v
+
+
+def add_scalar(v: np.ndarray, s: float) -> np.ndarray:
+    """v += s in place through ``gooseberry_add_scalar`` (``include/gooseberry.h:150-153``)."""
+    real = _real(v.dtype)
+    assert v.flags.c_contiguous
+    fn = lib().gooseberry_add_scalar_f64 if real == "f64" else lib().gooseberry_add_scalar
+    _check(fn(v.size, _ptr(v), s), "gooseberry_add_scalar")
+    return v
+
+
+def cgd(rowptr, rowind, rowval, b, error: float, niter: int, history: bool = False):
+    """Conjugate gradient with the reference's contract (``src/cgd.c:40-129``):
+    x0 = 0, stop when ||r||_2 <= error (absolute) or after niter iterations.
+
+    Returns ``(x, iterations, rnorm)`` (plus the ||r|| history if asked)."""
+    rowval = np.ascontiguousarray(rowval)
+    real = _real(rowval.dtype)
+    dt = rowval.dtype
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+    rowind = np.ascontiguousarray(rowind, dtype=np.uint32)
+    b = np.ascontiguousarray(b, dtype=dt)
+    n = len(b)
+    x = np.zeros(n, dtype=dt)
+    it = C.c_size_t(0)
+    rn = C.c_double(0)
+    hist = np.zeros(max(int(niter), 1), dtype=np.float64) if history else None
+    fn = lib().gooseberry_cgd_f64 if real == "f64" else lib().gooseberry_cgd
+    _check(fn(n, _ptr(rowptr), _ptr(rowind), _ptr(rowval), _ptr(b), _ptr(x), error,
+              int(niter), C.addressof(it), C.addressof(rn), _ptr(hist),
+              0 if hist is None else len(hist)), "gooseberry_cgd")
+    if history:
+        return x, int(it.value), rn.value, hist[: it.value]
+    return x, int(it.value), rn.value
+
+
+def plan_tiles(rowptr, tile_items: int = 2048):
+    """Run the SpMV tile planner on a host rowptr (no GPU).  Returns
+    ``(tiles[ntiles, 4], nlong, info)``; see ``gb_plan_tiles_host``."""
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+    n = len(rowptr) - 1
+    nt, nl = C.c_uint32(0), C.c_uint32(0)
+    info = CsrInfo()
+    _check(lib().gb_plan_tiles_host(n, _ptr(rowptr), int(rowptr[-1]), tile_items, None, 0,
+                                    C.addressof(nt), C.addressof(nl), C.addressof(info)),
+           "gb_plan_tiles_host")
+    tiles = np.zeros((max(nt.value, 1), 4), dtype=np.uint32)
+    _check(lib().gb_plan_tiles_host(n, _ptr(rowptr), int(rowptr[-1]), tile_items,
+                                    _ptr(tiles), nt.value, None, None, None),
+           "gb_plan_tiles_host")
+    return tiles[: nt.value], nl.value, info
+
+
+# ---- device API ----------------------------------------------------------------------
+
+def _torch():
+    import torch
+    return torch
+
+
+def dot(a, b, stream=None) -> float:
+    """sum a*b of two CUDA tensors (float64 accumulation, fixed order)."""
+    torch = _torch()
+    out = torch.empty(1, dtype=torch.float64, device=a.device)
+    fn = lib().gb_dot_f64 if a.dtype == torch.float64 else lib().gb_dot_f32
+    _check(fn(a.numel(), a.data_ptr(), b.data_ptr(), out.data_ptr(), _stream_ptr(stream)),
+           "gb_dot")
+    return float(out.item())
+
+
+class CsrMatrix:
+    """A device-resident CSR matrix (``gb_csr_t``)."""
+
+    def __init__(self, handle: int, nrows: int, ncols: int, nnz: int, keep=()):
+        self._h = C.c_void_p(handle)
+        self.nrows, self.ncols, self.nnz = nrows, ncols, nnz
+        self._keep = keep  # borrowed device tensors must outlive the handle
+
+    @classmethod
+    def from_host(cls, csr=None, *, rowptr=None, rowind=None, rowval=None, ncols=None,
+                  f64: bool = True, f32: bool = False, stream=None) -> "CsrMatrix":
+        """Upload a host CSR (numpy arrays or a ``workloads.Csr``)."""
+        if csr is not None:
+            rowptr, rowind, rowval, ncols = csr.rowptr, csr.rowind, csr.rowval, csr.ncols
+        rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+        rowind = np.ascontiguousarray(rowind, dtype=np.uint32)
+        v64 = np.ascontiguousarray(rowval, dtype=np.float64)
+        n = len(rowptr) - 1
+        ncols = n if ncols is None else int(ncols)
+        flags = (VALUES_F64 if f64 else 0) | (VALUES_F32 if f32 else 0)
+        h = C.c_void_p()
+        _check(lib().gb_csr_create(n, ncols, int(rowptr[-1]), _ptr(rowptr), _ptr(rowind),
+                                   _ptr(v64), None, flags,
+                                   _stream_ptr(stream) if stream is not None else None,
+                                   C.addressof(h)), "gb_csr_create")
+        return cls(h.value, n, ncols, int(rowptr[-1]))
+
+    @classmethod
+    def from_device(cls, rowptr, rowind, val64=None, val32=None, ncols=None,
+                    stream=None) -> "CsrMatrix":
+        """Borrow CSR arrays that are already CUDA tensors (uint32/int32 indices)."""
+        n = rowptr.numel() - 1
+        ncols = n if ncols is None else int(ncols)
+        flags = DEVICE_POINTERS | (VALUES_F64 if val64 is not None else 0) | (
+            VALUES_F32 if val32 is not None else 0)
+        h = C.c_void_p()
+        _check(lib().gb_csr_create(n, ncols, rowind.numel(), rowptr.data_ptr(),
+                                   rowind.data_ptr(), _ptr(val64), _ptr(val32), flags,
+                                   _stream_ptr(stream), C.addressof(h)), "gb_csr_create")
+        return cls(h.value, n, ncols, rowind.numel(), keep=(rowptr, rowind, val64, val32))
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().gb_csr_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    def info(self) -> CsrInfo:
+        i = CsrInfo()
+        _check(lib().gb_csr_get_info(self._h, C.addressof(i)), "gb_csr_get_info")
+        return i
+
+    def set_schedule(self, schedule: int, tile_items: int = 0, f32: bool = False):
+        _check(lib().gb_csr_set_schedule(self._h, VALUES_F32 if f32 else VALUES_F64,
+                                         schedule, tile_items), "gb_csr_set_schedule")
+
+    def autotune(self, f32: bool = False, stream=None):
+        _check(lib().gb_csr_autotune(self._h, VALUES_F32 if f32 else VALUES_F64,
+                                     _stream_ptr(stream)), "gb_csr_autotune")
+
+    def spmv(self, x, y=None, stream=None):
+        """y = A x for CUDA tensors (float64 or float32)."""
+        torch = _torch()
+        if y is None:
+            y = torch.empty(self.nrows, dtype=x.dtype, device=x.device)
+        assert x.is_contiguous() and y.is_contiguous() and x.dtype == y.dtype
+        fn = lib().gb_spmv_f64 if x.dtype == torch.float64 else lib().gb_spmv_f32
+        _check(fn(self._h, x.data_ptr(), y.data_ptr(), _stream_ptr(stream)), "gb_spmv")
+        return y
+
+    def spmm(self, B, bncols: int, out=None, stream=None):
+        torch = _torch()
+        if out is None:
+            out = torch.empty(self.nrows * bncols, dtype=torch.float64, device=B.device)
+        _check(lib().gb_spmm_f64(self._h, bncols, B.data_ptr(), out.data_ptr(),
+                                 _stream_ptr(stream)), "gb_spmm_f64")
+        return out
+
+
+@dataclass
+class CgResult:
+    iterations: int
+    refinements: int
+    rnorm: float
+    bnorm: float
+    status: str
+    kernel_launches: int
+
+
+class CgSolver:
+    """CG workspace bound to one matrix (``gb_cg_t``)."""
+
+    def __init__(self, A: CsrMatrix, mode: int = CG_F64):
+        self.A = A
+        h = C.c_void_p()
+        _check(lib().gb_cg_create(A._h, mode, C.addressof(h)), "gb_cg_create")
+        self._h = h
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().gb_cg_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve(self, b, x=None, tol: float = 1e-8, relative: bool = True, niter: int = 0,
+              history: bool = False, stream=None):
+        torch = _torch()
+        if x is None:
+            x = torch.empty_like(b)
+        res = _CgResult()
+        hist = np.zeros(max(int(niter), 1), dtype=np.float64) if history else None
+        _check(lib().gb_cg_solve(self._h, b.data_ptr(), x.data_ptr(), tol, int(relative),
+                                 int(niter), _ptr(hist), 0 if hist is None else len(hist),
+                                 C.addressof(res), _stream_ptr(stream)), "gb_cg_solve")
+        out = CgResult(res.iterations, res.refinements, res.rnorm, res.bnorm,
+                       CG_STATUS.get(res.status, str(res.status)), res.kernel_launches)
+        if history:
+            return x, out, hist[: res.iterations]
+        return x, out
+
+    def profile(self, b, iterations: int = 20, stream=None):
+        """Mean device time (ms) of each kernel of one iteration, timed launch
+        by launch with CUDA events over the first `iterations` iterations."""
+        ms = np.zeros(4, dtype=np.float64)
+        nk = C.c_size_t(0)
+        _check(lib().gb_cg_profile(self._h, b.data_ptr(), int(iterations), _ptr(ms), 4,
+                                   C.addressof(nk), _stream_ptr(stream)), "gb_cg_profile")
+        return ms[: nk.value].tolist()

@@ -1,0 +1,183 @@
+// blas1.cu -- dense vector BLAS-1 on device vectors: dot, scale, add_scalar,
+// add, sub (reference src/blas.c:244-336, 397-430).
+//
+// All are HBM-streaming grid-stride kernels with grids a multiple of the SM
+// count.  The CG solver does not call them: it fuses the same vector work into
+// its own kernels (cg.cu).  The dot product reduces per-CTA partials in a fixed
+// order, so it is bitwise reproducible for a given n on a given GPU (the
+// reference's OpenMP reduction order varies with the thread count,
+// src/blas.c:423-427).
+#include <algorithm>
+
+#include "gb_internal.h"
+#include "spmv_tiles.cuh"
+
+namespace gb {
+
+namespace {
+
+constexpr int kBlock = 256;
+
+// [begin, end) of CTA `b` out of `g` over n elements, split in 2-element units
+__device__ __forceinline__ void chunk_of(size_t n, unsigned b, unsigned g, size_t & s,
+    size_t & e) {
+  const size_t units = (n + 1) / 2;
+  const size_t q = units / g, r = units % g;
+  const size_t us = b * q + min(static_cast<size_t>(b), r);
+  const size_t ue = us + q + (b < r ? 1 : 0);
+  s = min(us * 2, n);
+  e = min(ue * 2, n);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBlock) dot_partial_kernel(size_t n,
+    const T * __restrict__ a, const T * __restrict__ b, double * __restrict__ partial) {
+  __shared__ double red[32];
+  size_t s, e;
+  chunk_of(n, blockIdx.x, gridDim.x, s, e);
+  double acc = 0.0;
+  for (size_t i = s + threadIdx.x; i < e; i += kBlock)
+    acc += static_cast<double>(a[i]) * static_cast<double>(b[i]);
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) partial[blockIdx.x] = acc;
+}
+
+__global__ void __launch_bounds__(kBlock) dot_final_kernel(unsigned g,
+    const double * __restrict__ partial, double * __restrict__ out) {
+  __shared__ double red[32];
+  double acc = 0.0;
+  for (unsigned i = threadIdx.x; i < g; i += kBlock) acc += partial[i];
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) *out = acc;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBlock) scale_kernel(size_t n, T * __restrict__ v, T s) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(kBlock) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * kBlock)
+    v[i] *= s;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBlock) add_scalar_kernel(size_t n, T * __restrict__ v, T s) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(kBlock) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * kBlock)
+    v[i] += s;
+}
+
+// c = a + sign*b; c may alias a or b (each element read before written)
+template <typename T>
+__global__ void __launch_bounds__(kBlock) axpby_kernel(size_t n, const T * a, const T * b,
+    T * c, int subtract) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(kBlock) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * kBlock) {
+    const T av = a[i], bv = b[i];
+    c[i] = subtract ? av - bv : av + bv;
+  }
+}
+
+unsigned grid_for(size_t n, int per_sm) {
+  int sms = 148;
+  sm_count_of_current_device(&sms);
+  const size_t want = (n + kBlock * 4 - 1) / (kBlock * 4);
+  return static_cast<unsigned>(std::max<size_t>(1, std::min<size_t>(want,
+      static_cast<size_t>(sms) * per_sm)));
+}
+
+template <typename T>
+int dot_impl(size_t n, const T * a, const T * b, double * result, cudaStream_t s) {
+  GB_CHECK_INPUT(result != nullptr, "result is NULL");
+  GB_CHECK_INPUT(n == 0 || (a && b), "NULL vector");
+  const unsigned g = grid_for(n, 4);
+  double * partial = nullptr;
+  GB_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&partial), g * sizeof(double), s));
+  dot_partial_kernel<T><<<g, kBlock, 0, s>>>(n, a, b, partial);
+  dot_final_kernel<<<1, kBlock, 0, s>>>(g, partial, result);
+  cudaError_t e = cudaGetLastError();
+  cudaFreeAsync(partial, s);
+  GB_CUDA_TRY(e);
+  return GOOSEBERRY_SUCCESS;
+}
+
+}  // namespace
+
+int launch_scale_f64(size_t n, double * v, double s, cudaStream_t st) {
+  if (n == 0) return GOOSEBERRY_SUCCESS;
+  scale_kernel<double><<<grid_for(n, 8), kBlock, 0, st>>>(n, v, s);
+  GB_CUDA_TRY(cudaGetLastError());
+  return GOOSEBERRY_SUCCESS;
+}
+int launch_scale_f32(size_t n, float * v, float s, cudaStream_t st) {
+  if (n == 0) return GOOSEBERRY_SUCCESS;
+  scale_kernel<float><<<grid_for(n, 8), kBlock, 0, st>>>(n, v, s);
+  GB_CUDA_TRY(cudaGetLastError());
+  return GOOSEBERRY_SUCCESS;
+}
+int launch_add_scalar_f64(size_t n, double * v, double s, cudaStream_t st) {
+  if (n == 0) return GOOSEBERRY_SUCCESS;
+  add_scalar_kernel<double><<<grid_for(n, 8), kBlock, 0, st>>>(n, v, s);
+  GB_CUDA_TRY(cudaGetLastError());
+  return GOOSEBERRY_SUCCESS;
+}
+int launch_add_scalar_f32(size_t n, float * v, float s, cudaStream_t st) {
+  if (n == 0) return GOOSEBERRY_SUCCESS;
+  add_scalar_kernel<float><<<grid_for(n, 8), kBlock, 0, st>>>(n, v, s);
+  GB_CUDA_TRY(cudaGetLastError());
+  return GOOSEBERRY_SUCCESS;
+}
+
+}  // namespace gb
+
+extern "C" {
+
+int gb_dot_f64(size_t n, const double * a, const double * b, double * result,
+    gb_stream_t stream) {
+  return gb::dot_impl<double>(n, a, b, result, static_cast<cudaStream_t>(stream));
+}
+
+int gb_dot_f32(size_t n, const float * a, const float * b, double * result,
+    gb_stream_t stream) {
+  return gb::dot_impl<float>(n, a, b, result, static_cast<cudaStream_t>(stream));
+}
+
+int gb_scale_f64(size_t n, double * v, double s, gb_stream_t stream) {
+  GB_CHECK_INPUT(n == 0 || v, "NULL vector");
+  return gb::launch_scale_f64(n, v, s, static_cast<cudaStream_t>(stream));
+}
+
+int gb_scale_f32(size_t n, float * v, float s, gb_stream_t stream) {
+  GB_CHECK_INPUT(n == 0 || v, "NULL vector");
+  return gb::launch_scale_f32(n, v, s, static_cast<cudaStream_t>(stream));
+}
+
+int gb_add_scalar_f64(size_t n, double * v, double s, gb_stream_t stream) {
+  GB_CHECK_INPUT(n == 0 || v, "NULL vector");
+  return gb::launch_add_scalar_f64(n, v, s, static_cast<cudaStream_t>(stream));
+}
+
+int gb_add_scalar_f32(size_t n, float * v, float s, gb_stream_t stream) {
+  GB_CHECK_INPUT(n == 0 || v, "NULL vector");
+  return gb::launch_add_scalar_f32(n, v, s, static_cast<cudaStream_t>(stream));
+}
+
+int gb_add_f64(size_t n, const double * a, const double * b, double * c,
+    gb_stream_t stream) {
+  GB_CHECK_INPUT(n == 0 || (a && b && c), "NULL vector");
+  if (n == 0) return GOOSEBERRY_SUCCESS;
+  gb::axpby_kernel<double><<<gb::grid_for(n, 8), gb::kBlock, 0,
+      static_cast<cudaStream_t>(stream)>>>(n, a, b, c, 0);
+  GB_CUDA_TRY(cudaGetLastError());
+  return GOOSEBERRY_SUCCESS;
+}
+
+int gb_sub_f64(size_t n, const double * a, const double * b, double * c,
+    gb_stream_t stream) {
+  GB_CHECK_INPUT(n == 0 || (a && b && c), "NULL vector");
+  if (n == 0) return GOOSEBERRY_SUCCESS;
+  gb::axpby_kernel<double><<<gb::grid_for(n, 8), gb::kBlock, 0,
+      static_cast<cudaStream_t>(stream)>>>(n, a, b, c, 1);
+  GB_CUDA_TRY(cudaGetLastError());
+  return GOOSEBERRY_SUCCESS;
+}
+
+}  // extern "C"

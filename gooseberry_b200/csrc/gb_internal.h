@@ -1,0 +1,158 @@
+// gb_internal.h -- shared internals of libgooseberry_b200 (not installed).
+//
+// Layout of a device-resident CSR matrix and of its SpMV tile plan, error
+// plumbing and launch helpers used by the .cu/.cpp translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include "gooseberry_b200.h"
+
+namespace gb {
+
+// ---- errors -----------------------------------------------------------------
+
+// Record a printf-style message as this thread's last error.
+void set_error(const char * fmt, ...);
+void clear_error();
+
+#define GB_CUDA_TRY(expr)                                                      \
+  do {                                                                         \
+    cudaError_t gb_e_ = (expr);                                                \
+    if (gb_e_ != cudaSuccess) {                                                \
+      ::gb::set_error("%s failed: %s (%s:%d)", #expr,                          \
+          cudaGetErrorString(gb_e_), __FILE__, __LINE__);                      \
+      return GOOSEBERRY_ERROR_UNKNOWN;                                         \
+    }                                                                          \
+  } while (0)
+
+#define GB_TRY(expr)                                                           \
+  do {                                                                         \
+    int gb_rc_ = (expr);                                                       \
+    if (gb_rc_ != GOOSEBERRY_SUCCESS) return gb_rc_;                           \
+  } while (0)
+
+#define GB_CHECK_INPUT(cond, ...)                                              \
+  do {                                                                         \
+    if (!(cond)) {                                                             \
+      ::gb::set_error(__VA_ARGS__);                                            \
+      return GOOSEBERRY_ERROR_INVALIDINPUT;                                    \
+    }                                                                          \
+  } while (0)
+
+// ---- SpMV tile plan ---------------------------------------------------------
+//
+// The rows are cut, in order, into tiles.  A normal tile is a run of whole
+// rows holding at most `tile_items` rows + nonzeros; its products are staged
+// in shared memory and reduced there, so no row crosses a normal tile.  A row
+// too long for one tile (nnz >= tile_items) is a "long row": it is cut into
+// consecutive chunk tiles of at most `chunk_nnz` nonzeros each; every chunk
+// writes a partial sum into the plan's scratch and the last chunk to finish
+// adds them up in chunk order (deterministic).
+
+struct TileDesc {
+  uint32_t row_begin;  // normal: first row; chunk: index into the long-row table
+  uint32_t row_count;  // normal: rows in the tile (>= 1); chunk: 0
+  uint32_t nnz_begin;  // first nonzero of the tile (absolute index)
+  uint32_t nnz_count;  // nonzeros in the tile
+};
+
+struct LongRowDesc {
+  uint32_t row;         // the row
+  uint32_t first_tile;  // its chunks are tiles [first_tile, first_tile+nchunks)
+  uint32_t nchunks;
+  uint32_t pad;
+};
+
+// Device view of a plan, passed by value to kernels.
+struct PlanView {
+  const TileDesc * tiles;
+  const LongRowDesc * longrows;
+  double * chunk_partial;     // [ntiles] partial sums of chunk tiles
+  unsigned int * long_count;  // [nlong] chunk-arrival counters (kept at 0)
+  uint32_t ntiles;
+  uint32_t nlong;
+  uint32_t tile_items;
+  uint32_t ncols;
+};
+
+struct Plan {
+  uint32_t tile_items = 0;
+  uint32_t chunk_nnz = 0;
+  std::vector<TileDesc> tiles;
+  std::vector<LongRowDesc> longrows;
+  // row-length summary
+  uint32_t max_row = 0, p50 = 0, p90 = 0, p99 = 0;
+  double mean_row = 0.0;
+  // device copies
+  TileDesc * d_tiles = nullptr;
+  LongRowDesc * d_longrows = nullptr;
+  double * d_chunk_partial = nullptr;
+  unsigned int * d_long_count = nullptr;
+};
+
+// Build the tile plan from a HOST copy of rowptr.  Returns INVALIDINPUT if
+// rowptr decreases or does not span nnz.
+int build_plan(uint32_t nrows, const uint32_t * rowptr, uint32_t nnz,
+    uint32_t tile_items, Plan & plan);
+int upload_plan(Plan & plan, cudaStream_t stream);
+void free_plan(Plan & plan);
+
+}  // namespace gb
+
+// ---- the opaque handles -----------------------------------------------------
+
+struct gb_csr {
+  uint32_t nrows = 0, ncols = 0, nnz = 0;
+  int device = 0;
+  const uint32_t * rowptr = nullptr;  // device
+  const uint32_t * rowind = nullptr;  // device
+  const double * val64 = nullptr;     // device (may be null)
+  const float * val32 = nullptr;      // device (may be null)
+  // owned allocations (freed by gb_csr_destroy)
+  void * own_rowptr = nullptr;
+  void * own_rowind = nullptr;
+  void * own_val64 = nullptr;
+  void * own_val32 = nullptr;
+  gb::Plan plan;
+  int sched64 = GB_SCHED_AUTO;  // resolved schedule (never AUTO after create)
+  int sched32 = GB_SCHED_AUTO;
+  int sm_count = 0;
+};
+
+namespace gb {
+
+inline PlanView plan_view(const gb_csr & a) {
+  PlanView v;
+  v.tiles = a.plan.d_tiles;
+  v.longrows = a.plan.d_longrows;
+  v.chunk_partial = a.plan.d_chunk_partial;
+  v.long_count = a.plan.d_long_count;
+  v.ntiles = static_cast<uint32_t>(a.plan.tiles.size());
+  v.nlong = static_cast<uint32_t>(a.plan.longrows.size());
+  v.tile_items = a.plan.tile_items;
+  v.ncols = a.ncols;
+  return v;
+}
+
+// Heuristic schedule from the row-length summary (used until autotuned).
+int default_schedule(const Plan & plan);
+
+// SpMV launchers (spmv.cu).  `stride` is the output element stride (1 for
+// SpMV; bncols for the columns of a row-major SpMM result).
+int launch_spmv_f64(const gb_csr & a, int sched, const double * x, double * y,
+    uint32_t stride, cudaStream_t stream);
+int launch_spmv_f32(const gb_csr & a, int sched, const float * x, float * y,
+    uint32_t stride, cudaStream_t stream);
+// max(rowind) over nnz into *d_out (device), for validation.
+int launch_max_index(const uint32_t * rowind, uint32_t nnz, unsigned int * d_out,
+    cudaStream_t stream);
+int launch_round_f32(const double * in, float * out, size_t n, cudaStream_t stream);
+
+int sm_count_of_current_device(int * out);
+
+}  // namespace gb

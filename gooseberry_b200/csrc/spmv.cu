@@ -1,0 +1,650 @@
+// spmv.cu -- device-resident CSR matrices, the SpMV tile plan, the SpMV /
+// SpMM launchers and the schedule autotuner.
+//
+// Reference path: blas_spmult (src/blas.c:552-606) splits rows evenly over
+// OpenMP threads and runs __sparse_mult_dense_block (src/blas.c:67-92), a
+// sequential per-row sum.  Here the rows are cut into row-aligned tiles of
+// equal rows+nonzeros (balanced whatever the row-length distribution) and
+// each tile is reduced on chip by a schedule picked per matrix.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "gb_internal.h"
+#include "spmv_tiles.cuh"
+
+namespace gb {
+
+// ---- plan -------------------------------------------------------------------
+
+namespace {
+constexpr uint32_t kDefaultTileItems = 2048;
+constexpr uint32_t kChunkTiles = 4;  // a long-row chunk is 4 tiles of nonzeros
+}  // namespace
+
+int build_plan(uint32_t nrows, const uint32_t * rowptr, uint32_t nnz,
+    uint32_t tile_items, Plan & plan) {
+  if (tile_items < 64 || tile_items > 16384)
+    GB_CHECK_INPUT(false, "tile_items %u outside [64, 16384]", tile_items);
+  GB_CHECK_INPUT(rowptr[nrows] == nnz,
+      "rowptr[nrows] = %u but the matrix has %u stored entries", rowptr[nrows], nnz);
+  plan.tile_items = tile_items;
+  plan.chunk_nnz = tile_items * kChunkTiles;
+  plan.tiles.clear();
+  plan.longrows.clear();
+
+  // exact counts of lengths < 1024, log2 buckets above, for quantiles
+  std::vector<uint64_t> small(1024, 0), big(33, 0);
+  uint32_t maxlen = 0;
+  uint32_t r = 0;
+  while (r < nrows) {
+    const uint32_t b = rowptr[r], e = rowptr[r + 1];
+    GB_CHECK_INPUT(e >= b, "rowptr decreases at row %u (%u > %u)", r, b, e);
+    const uint32_t len = e - b;
+    if (static_cast<uint64_t>(len) + 1 > tile_items) {
+      // long row -> chunk tiles
+      LongRowDesc L;
+      L.row = r;
+      L.first_tile = static_cast<uint32_t>(plan.tiles.size());
+      L.nchunks = (len + plan.chunk_nnz - 1) / plan.chunk_nnz;
+      L.pad = 0;
+      const uint32_t lid = static_cast<uint32_t>(plan.longrows.size());
+      for (uint32_t q = 0; q < L.nchunks; ++q) {
+        TileDesc t;
+        t.row_begin = lid;
+        t.row_count = 0;
+        t.nnz_begin = b + q * plan.chunk_nnz;
+        t.nnz_count = std::min(plan.chunk_nnz, len - q * plan.chunk_nnz);
+        plan.tiles.push_back(t);
+      }
+      plan.longrows.push_back(L);
+      maxlen = std::max(maxlen, len);
+      if (len < 1024) ++small[len]; else ++big[32 - __builtin_clz(len)];
+      ++r;
+      continue;
+    }
+    TileDesc t;
+    t.row_begin = r;
+    t.nnz_begin = b;
+    uint32_t items = 0;
+    while (r < nrows) {
+      const uint32_t bb = rowptr[r], ee = rowptr[r + 1];
+      GB_CHECK_INPUT(ee >= bb, "rowptr decreases at row %u (%u > %u)", r, bb, ee);
+      const uint32_t l = ee - bb;
+      if (static_cast<uint64_t>(l) + 1 > tile_items) break;
+      if (items + l + 1 > tile_items) break;
+      items += l + 1;
+      maxlen = std::max(maxlen, l);
+      if (l < 1024) ++small[l]; else ++big[32 - __builtin_clz(l)];
+      ++r;
+    }
+    t.row_count = r - t.row_begin;
+    t.nnz_count = rowptr[r] - b;
+    plan.tiles.push_back(t);
+  }
+  // quantiles (exact below 1024, bucket upper bound above)
+  auto quant = [&](double q) -> uint32_t {
+    const uint64_t want = static_cast<uint64_t>(std::ceil(q * nrows));
+    uint64_t acc = 0;
+    for (uint32_t l = 0; l < 1024; ++l) {
+      acc += small[l];
+      if (acc >= want && want > 0) return l;
+    }
+    for (uint32_t k = 0; k < 33; ++k) {
+      acc += big[k];
+      if (acc >= want) return k >= 32 ? 0xffffffffu : ((1u << k) - 1);
+    }
+    return maxlen;
+  };
+  plan.max_row = maxlen;
+  plan.mean_row = nrows ? static_cast<double>(nnz) / nrows : 0.0;
+  plan.p50 = quant(0.50);
+  plan.p90 = quant(0.90);
+  plan.p99 = quant(0.99);
+  return GOOSEBERRY_SUCCESS;
+}
+
+void free_plan(Plan & plan) {
+  if (plan.d_tiles) cudaFree(plan.d_tiles);
+  if (plan.d_longrows) cudaFree(plan.d_longrows);
+  if (plan.d_chunk_partial) cudaFree(plan.d_chunk_partial);
+  if (plan.d_long_count) cudaFree(plan.d_long_count);
+  plan.d_tiles = nullptr;
+  plan.d_longrows = nullptr;
+  plan.d_chunk_partial = nullptr;
+  plan.d_long_count = nullptr;
+}
+
+int upload_plan(Plan & plan, cudaStream_t stream) {
+  free_plan(plan);
+  const size_t nt = std::max<size_t>(plan.tiles.size(), 1);
+  const size_t nl = std::max<size_t>(plan.longrows.size(), 1);
+  GB_CUDA_TRY(cudaMalloc(&plan.d_tiles, nt * sizeof(TileDesc)));
+  GB_CUDA_TRY(cudaMalloc(&plan.d_longrows, nl * sizeof(LongRowDesc)));
+  GB_CUDA_TRY(cudaMalloc(&plan.d_chunk_partial, nt * sizeof(double)));
+  GB_CUDA_TRY(cudaMalloc(&plan.d_long_count, nl * sizeof(unsigned int)));
+  if (!plan.tiles.empty())
+    GB_CUDA_TRY(cudaMemcpyAsync(plan.d_tiles, plan.tiles.data(),
+        plan.tiles.size() * sizeof(TileDesc), cudaMemcpyHostToDevice, stream));
+  if (!plan.longrows.empty())
+    GB_CUDA_TRY(cudaMemcpyAsync(plan.d_longrows, plan.longrows.data(),
+        plan.longrows.size() * sizeof(LongRowDesc), cudaMemcpyHostToDevice, stream));
+  GB_CUDA_TRY(cudaMemsetAsync(plan.d_long_count, 0, nl * sizeof(unsigned int), stream));
+  GB_CUDA_TRY(cudaStreamSynchronize(stream));  // host vectors may change later
+  return GOOSEBERRY_SUCCESS;
+}
+
+int default_schedule(const Plan & plan) {
+  if (plan.max_row <= 12 && plan.mean_row <= 12.0) return GB_SCHED_THREAD;
+  if (plan.p99 <= 2 * plan.p50 + 8 && plan.mean_row <= 40.0) return GB_SCHED_GROUP4;
+  if (plan.p99 <= 2 * plan.p50 + 8 && plan.mean_row <= 160.0) return GB_SCHED_GROUP8;
+  return GB_SCHED_MERGE;
+}
+
+// ---- kernels ----------------------------------------------------------------
+
+template <typename Acc, typename Y>
+struct OutStore {
+  Y * y;
+  uint32_t stride;
+  __device__ __forceinline__ void row(uint32_t r, Acc v) {
+    y[static_cast<size_t>(r) * stride] = static_cast<Y>(v);
+  }
+  __device__ __forceinline__ void long_row(uint32_t, uint32_t r, Acc v) { row(r, v); }
+  __device__ __forceinline__ void finish() {}
+};
+
+template <typename V, typename Acc, int SCHED, class Gather, class Out>
+__global__ void __launch_bounds__(kSpmvBlock) spmv_tiles_kernel(const PlanView plan,
+    const uint32_t * __restrict__ rowptr, const uint32_t * __restrict__ rowind,
+    const V * __restrict__ val, const Gather gather, Out out) {
+  spmv_tiles_body<V, Acc, SCHED, kSpmvBlock>(plan, rowptr, rowind, val, gather, out);
+}
+
+__global__ void max_index_kernel(const uint32_t * __restrict__ ind, uint32_t n,
+    unsigned int * out) {
+  uint32_t m = 0;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x)
+    m = max(m, ind[i]);
+  m = max(m, __reduce_max_sync(0xffffffffu, m));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+__global__ void round_f32_kernel(const double * __restrict__ in, float * __restrict__ out,
+    size_t n) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x)
+    out[i] = static_cast<float>(in[i]);
+}
+
+// ---- launch helpers ---------------------------------------------------------
+
+// Resident CTAs per SM of a kernel at a dynamic shared-memory size (cached).
+int occupancy(const void * func, size_t smem, int * out) {
+  static std::mutex mu;
+  static std::map<std::pair<const void *, size_t>, int> cache;
+  std::lock_guard<std::mutex> lock(mu);
+  auto key = std::make_pair(func, smem);
+  auto it = cache.find(key);
+  if (it != cache.end()) {
+    *out = it->second;
+    return GOOSEBERRY_SUCCESS;
+  }
+  if (smem > 48 * 1024)
+    GB_CUDA_TRY(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        static_cast<int>(smem)));
+  int n = 0;
+  GB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, func, kSpmvBlock, smem));
+  if (n < 1) {
+    set_error("SpMV kernel cannot be resident with %zu bytes of shared memory", smem);
+    return GOOSEBERRY_ERROR_UNKNOWN;
+  }
+  cache[key] = n;
+  *out = n;
+  return GOOSEBERRY_SUCCESS;
+}
+
+template <typename V, typename Acc, int SCHED, class Gather, class Out>
+int launch_tiles(const gb_csr & a, const V * val, const Gather & g, const Out & o,
+    cudaStream_t stream) {
+  if (a.plan.tiles.empty()) return GOOSEBERRY_SUCCESS;
+  auto kern = spmv_tiles_kernel<V, Acc, SCHED, Gather, Out>;
+  const size_t smem = TileSmem<Acc>::bytes(a.plan.tile_items);
+  int occ = 0;
+  GB_TRY(occupancy(reinterpret_cast<const void *>(kern), smem, &occ));
+  const uint32_t ntiles = static_cast<uint32_t>(a.plan.tiles.size());
+  const uint32_t grid = std::min<uint32_t>(ntiles, static_cast<uint32_t>(a.sm_count * occ));
+  kern<<<grid, kSpmvBlock, smem, stream>>>(plan_view(a), a.rowptr, a.rowind, val, g, o);
+  GB_CUDA_TRY(cudaGetLastError());
+  return GOOSEBERRY_SUCCESS;
+}
+
+template <typename V, typename Acc, class Gather, class Out>
+int launch_sched(const gb_csr & a, int sched, const V * val, const Gather & g,
+    const Out & o, cudaStream_t stream) {
+  switch (sched) {
+    case GB_SCHED_THREAD: return launch_tiles<V, Acc, SCHED_THREAD>(a, val, g, o, stream);
+    case GB_SCHED_GROUP4: return launch_tiles<V, Acc, SCHED_GROUP4>(a, val, g, o, stream);
+    case GB_SCHED_GROUP8: return launch_tiles<V, Acc, SCHED_GROUP8>(a, val, g, o, stream);
+    case GB_SCHED_WARP: return launch_tiles<V, Acc, SCHED_WARP>(a, val, g, o, stream);
+    case GB_SCHED_MERGE: return launch_tiles<V, Acc, SCHED_MERGE>(a, val, g, o, stream);
+    default:
+      set_error("unknown SpMV schedule %d", sched);
+      return GOOSEBERRY_ERROR_INVALIDINPUT;
+  }
+}
+
+int launch_spmv_f64(const gb_csr & a, int sched, const double * x, double * y,
+    uint32_t stride, cudaStream_t stream) {
+  GB_CHECK_INPUT(a.val64 != nullptr, "matrix holds no double values");
+  GatherPlain<double> g{x};
+  OutStore<double, double> o{y, stride};
+  return launch_sched<double, double>(a, sched, a.val64, g, o, stream);
+}
+
+int launch_spmv_f32(const gb_csr & a, int sched, const float * x, float * y,
+    uint32_t stride, cudaStream_t stream) {
+  GB_CHECK_INPUT(a.val32 != nullptr, "matrix holds no float values");
+  GatherPlain<float> g{x};
+  OutStore<float, float> o{y, stride};
+  return launch_sched<float, float>(a, sched, a.val32, g, o, stream);
+}
+
+int launch_max_index(const uint32_t * rowind, uint32_t nnz, unsigned int * d_out,
+    cudaStream_t stream) {
+  GB_CUDA_TRY(cudaMemsetAsync(d_out, 0, sizeof(unsigned int), stream));
+  if (nnz == 0) return GOOSEBERRY_SUCCESS;
+  int sms = 0;
+  GB_TRY(sm_count_of_current_device(&sms));
+  const uint32_t grid = std::min<uint32_t>((nnz + 255) / 256, static_cast<uint32_t>(sms) * 8);
+  max_index_kernel<<<grid, 256, 0, stream>>>(rowind, nnz, d_out);
+  GB_CUDA_TRY(cudaGetLastError());
+  return GOOSEBERRY_SUCCESS;
+}
+
+int launch_round_f32(const double * in, float * out, size_t n, cudaStream_t stream) {
+  if (n == 0) return GOOSEBERRY_SUCCESS;
+  int sms = 0;
+  GB_TRY(sm_count_of_current_device(&sms));
+  const size_t grid = std::min<size_t>((n + 255) / 256, static_cast<size_t>(sms) * 8);
+  round_f32_kernel<<<static_cast<unsigned>(grid), 256, 0, stream>>>(in, out, n);
+  GB_CUDA_TRY(cudaGetLastError());
+  return GOOSEBERRY_SUCCESS;
+}
+
+// ---- autotuner --------------------------------------------------------------
+
+namespace {
+
+struct TuneKey {
+  uint32_t p50, p90, p99, maxlog2, nrows_log2, nnz_log2;
+  unsigned width;
+  bool operator<(const TuneKey & o) const {
+    return std::tie(p50, p90, p99, maxlog2, nrows_log2, nnz_log2, width) <
+           std::tie(o.p50, o.p90, o.p99, o.maxlog2, o.nrows_log2, o.nnz_log2, o.width);
+  }
+};
+struct TuneChoice {
+  int sched;
+  uint32_t tile_items;
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneChoice> g_tune_cache;
+
+uint32_t ilog2(uint64_t v) { return v ? 63u - static_cast<uint32_t>(__builtin_clzll(v)) : 0u; }
+
+TuneKey make_key(const gb_csr & a, unsigned width) {
+  TuneKey k;
+  k.p50 = a.plan.p50;
+  k.p90 = a.plan.p90;
+  k.p99 = a.plan.p99;
+  k.maxlog2 = ilog2(a.plan.max_row);
+  k.nrows_log2 = ilog2(a.nrows);
+  k.nnz_log2 = ilog2(a.nnz);
+  k.width = width;
+  return k;
+}
+
+}  // namespace
+
+int rebuild_plan(gb_csr & a, uint32_t tile_items, cudaStream_t stream) {
+  if (tile_items == a.plan.tile_items && a.plan.d_tiles) return GOOSEBERRY_SUCCESS;
+  std::vector<uint32_t> hrp(static_cast<size_t>(a.nrows) + 1);
+  GB_CUDA_TRY(cudaMemcpyAsync(hrp.data(), a.rowptr, hrp.size() * sizeof(uint32_t),
+      cudaMemcpyDeviceToHost, stream));
+  GB_CUDA_TRY(cudaStreamSynchronize(stream));
+  Plan p;
+  GB_TRY(build_plan(a.nrows, hrp.data(), a.nnz, tile_items, p));
+  GB_TRY(upload_plan(p, stream));
+  free_plan(a.plan);
+  a.plan = std::move(p);
+  return GOOSEBERRY_SUCCESS;
+}
+
+int autotune(gb_csr & a, unsigned width, cudaStream_t stream) {
+  const TuneKey key = make_key(a, width);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      GB_TRY(rebuild_plan(a, it->second.tile_items, stream));
+      (width == GB_CSR_VALUES_F32 ? a.sched32 : a.sched64) = it->second.sched;
+      return GOOSEBERRY_SUCCESS;
+    }
+  }
+  const size_t xb = static_cast<size_t>(a.ncols) * (width == GB_CSR_VALUES_F32 ? 4 : 8);
+  const size_t yb = static_cast<size_t>(a.nrows) * (width == GB_CSR_VALUES_F32 ? 4 : 8);
+  void * x = nullptr;
+  void * y = nullptr;
+  GB_CUDA_TRY(cudaMalloc(&x, std::max<size_t>(xb, 8)));
+  GB_CUDA_TRY(cudaMalloc(&y, std::max<size_t>(yb, 8)));
+  GB_CUDA_TRY(cudaMemsetAsync(x, 0, std::max<size_t>(xb, 8), stream));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const uint32_t tiles_opts[] = {1024, 2048, 4096};
+  const int sched_opts[] = {GB_SCHED_THREAD, GB_SCHED_GROUP4, GB_SCHED_GROUP8,
+                            GB_SCHED_WARP, GB_SCHED_MERGE};
+  float best = 1e30f;
+  TuneChoice choice{default_schedule(a.plan), a.plan.tile_items};
+  int rc = GOOSEBERRY_SUCCESS;
+  for (uint32_t ti : tiles_opts) {
+    rc = rebuild_plan(a, ti, stream);
+    if (rc != GOOSEBERRY_SUCCESS) break;
+    for (int s : sched_opts) {
+      // skip schedules that cannot suit this matrix
+      if (s == GB_SCHED_THREAD && a.plan.p90 > 64) continue;
+      if (s == GB_SCHED_WARP && a.plan.p50 < 8) continue;
+      auto run = [&]() {
+        return width == GB_CSR_VALUES_F32
+                   ? launch_spmv_f32(a, s, static_cast<const float *>(x),
+                         static_cast<float *>(y), 1, stream)
+                   : launch_spmv_f64(a, s, static_cast<const double *>(x),
+                         static_cast<double *>(y), 1, stream);
+      };
+      rc = run();  // warm-up
+      if (rc != GOOSEBERRY_SUCCESS) break;
+      const int reps = 5;
+      cudaEventRecord(e0, stream);
+      for (int q = 0; q < reps && rc == GOOSEBERRY_SUCCESS; ++q) rc = run();
+      cudaEventRecord(e1, stream);
+      if (rc != GOOSEBERRY_SUCCESS) break;
+      if (cudaEventSynchronize(e1) != cudaSuccess) {
+        set_error("autotune timing failed: %s", cudaGetErrorString(cudaGetLastError()));
+        rc = GOOSEBERRY_ERROR_UNKNOWN;
+        break;
+      }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best) {
+        best = ms;
+        choice = TuneChoice{s, ti};
+      }
+    }
+    if (rc != GOOSEBERRY_SUCCESS) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(x);
+  cudaFree(y);
+  GB_TRY(rc);
+  GB_TRY(rebuild_plan(a, choice.tile_items, stream));
+  (width == GB_CSR_VALUES_F32 ? a.sched32 : a.sched64) = choice.sched;
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  g_tune_cache[key] = choice;
+  return GOOSEBERRY_SUCCESS;
+}
+
+}  // namespace gb
+
+// ---- C ABI ------------------------------------------------------------------
+
+using gb::set_error;
+
+namespace {
+
+template <typename T>
+int alloc_copy(void ** dst, const T * src, size_t n, bool device_src, cudaStream_t s) {
+  GB_CUDA_TRY(cudaMalloc(dst, std::max<size_t>(n, 1) * sizeof(T)));
+  if (n)
+    GB_CUDA_TRY(cudaMemcpyAsync(*dst, src, n * sizeof(T),
+        device_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+  return GOOSEBERRY_SUCCESS;
+}
+
+void release(gb_csr * a) {
+  if (!a) return;
+  gb::free_plan(a->plan);
+  if (a->own_rowptr) cudaFree(a->own_rowptr);
+  if (a->own_rowind) cudaFree(a->own_rowind);
+  if (a->own_val64) cudaFree(a->own_val64);
+  if (a->own_val32) cudaFree(a->own_val32);
+  delete a;
+}
+
+int create_impl(dim_t nrows, dim_t ncols, ind_t nnz, const ind_t * rowptr,
+    const dim_t * rowind, const double * rowval64, const float * rowval32,
+    unsigned flags, cudaStream_t stream, gb_csr * a) {
+  const bool dev = (flags & GB_CSR_DEVICE_POINTERS) != 0;
+  const bool want64 = (flags & GB_CSR_VALUES_F64) != 0;
+  const bool want32 = (flags & GB_CSR_VALUES_F32) != 0;
+  GB_CHECK_INPUT(want64 || want32, "flags select no value width");
+  GB_CHECK_INPUT(rowptr != nullptr, "rowptr is NULL");
+  GB_CHECK_INPUT(nnz == 0 || rowind != nullptr, "rowind is NULL");
+  GB_CHECK_INPUT(!want64 || nnz == 0 || rowval64 != nullptr, "double values requested but rowval64 is NULL");
+  GB_CHECK_INPUT(!want32 || nnz == 0 || rowval32 != nullptr || rowval64 != nullptr,
+      "float values requested but no values given");
+  GB_CHECK_INPUT(nrows == 0 || ncols > 0, "matrix with rows but no columns");
+
+  a->nrows = nrows;
+  a->ncols = ncols;
+  a->nnz = nnz;
+  GB_CUDA_TRY(cudaGetDevice(&a->device));
+  GB_TRY(gb::sm_count_of_current_device(&a->sm_count));
+
+  // host copy of rowptr for the plan
+  std::vector<uint32_t> hrp;
+  const uint32_t * rp_host = rowptr;
+  if (dev) {
+    hrp.resize(static_cast<size_t>(nrows) + 1);
+    GB_CUDA_TRY(cudaMemcpyAsync(hrp.data(), rowptr, hrp.size() * sizeof(uint32_t),
+        cudaMemcpyDeviceToHost, stream));
+    GB_CUDA_TRY(cudaStreamSynchronize(stream));
+    rp_host = hrp.data();
+  }
+  GB_TRY(gb::build_plan(nrows, rp_host, nnz, gb::kDefaultTileItems, a->plan));
+
+  if (dev) {
+    a->rowptr = rowptr;
+    a->rowind = rowind;
+    a->val64 = want64 ? rowval64 : nullptr;
+    a->val32 = (want32 && rowval32) ? rowval32 : nullptr;
+  } else {
+    GB_TRY(alloc_copy(&a->own_rowptr, rowptr, static_cast<size_t>(nrows) + 1, false, stream));
+    GB_TRY(alloc_copy(&a->own_rowind, rowind, nnz, false, stream));
+    a->rowptr = static_cast<const uint32_t *>(a->own_rowptr);
+    a->rowind = static_cast<const uint32_t *>(a->own_rowind);
+    if (want64) {
+      GB_TRY(alloc_copy(&a->own_val64, rowval64, nnz, false, stream));
+      a->val64 = static_cast<const double *>(a->own_val64);
+    }
+    if (want32 && rowval32) {
+      GB_TRY(alloc_copy(&a->own_val32, rowval32, nnz, false, stream));
+      a->val32 = static_cast<const float *>(a->own_val32);
+    }
+  }
+  if (want32 && !a->val32) {
+    // round from the double values (already on the device, or upload them)
+    const double * src = a->val64;
+    void * tmp = nullptr;
+    if (!src) {
+      GB_TRY(alloc_copy(&tmp, rowval64, nnz, dev, stream));
+      src = static_cast<const double *>(tmp);
+    }
+    GB_CUDA_TRY(cudaMalloc(&a->own_val32, std::max<size_t>(nnz, 1) * sizeof(float)));
+    int rc = gb::launch_round_f32(src, static_cast<float *>(a->own_val32), nnz, stream);
+    if (tmp) {
+      cudaStreamSynchronize(stream);
+      cudaFree(tmp);
+    }
+    GB_TRY(rc);
+    a->val32 = static_cast<const float *>(a->own_val32);
+  }
+
+  // validate column indices on the device
+  if (nnz > 0) {
+    unsigned int * d_max = nullptr;
+    GB_CUDA_TRY(cudaMalloc(&d_max, sizeof(unsigned int)));
+    unsigned int hmax = 0;
+    int rc = gb::launch_max_index(a->rowind, nnz, d_max, stream);
+    if (rc == GOOSEBERRY_SUCCESS) {
+      cudaError_t e = cudaMemcpyAsync(&hmax, d_max, sizeof(hmax), cudaMemcpyDeviceToHost, stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+      if (e != cudaSuccess) {
+        set_error("index validation failed: %s", cudaGetErrorString(e));
+        rc = GOOSEBERRY_ERROR_UNKNOWN;
+      }
+    }
+    cudaFree(d_max);
+    GB_TRY(rc);
+    GB_CHECK_INPUT(hmax < ncols, "column index %u out of range for %u columns", hmax, ncols);
+  }
+  GB_TRY(gb::upload_plan(a->plan, stream));
+  a->sched64 = gb::default_schedule(a->plan);
+  a->sched32 = a->sched64;
+  return GOOSEBERRY_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gb_csr_create(dim_t nrows, dim_t ncols, ind_t nnz, const ind_t * rowptr,
+    const dim_t * rowind, const double * rowval64, const float * rowval32,
+    unsigned flags, gb_stream_t stream, gb_csr_t ** out) {
+  GB_CHECK_INPUT(out != nullptr, "out is NULL");
+  *out = nullptr;
+  gb_csr * a = new gb_csr();
+  int rc = create_impl(nrows, ncols, nnz, rowptr, rowind, rowval64, rowval32, flags,
+      static_cast<cudaStream_t>(stream), a);
+  if (rc != GOOSEBERRY_SUCCESS) {
+    release(a);
+    return rc;
+  }
+  *out = a;
+  return GOOSEBERRY_SUCCESS;
+}
+
+int gb_csr_destroy(gb_csr_t * a) {
+  release(a);
+  return GOOSEBERRY_SUCCESS;
+}
+
+int gb_csr_get_info(const gb_csr_t * a, gb_csr_info_t * info) {
+  GB_CHECK_INPUT(a && info, "NULL argument");
+  info->nrows = a->nrows;
+  info->ncols = a->ncols;
+  info->nnz = a->nnz;
+  info->ntiles = static_cast<uint32_t>(a->plan.tiles.size());
+  info->nlong = static_cast<uint32_t>(a->plan.longrows.size());
+  info->max_row = a->plan.max_row;
+  info->mean_row = a->plan.mean_row;
+  info->row_p50 = a->plan.p50;
+  info->row_p90 = a->plan.p90;
+  info->row_p99 = a->plan.p99;
+  info->schedule = a->sched64;
+  info->schedule_f32 = a->sched32;
+  info->tile_items = a->plan.tile_items;
+  return GOOSEBERRY_SUCCESS;
+}
+
+int gb_csr_set_schedule(gb_csr_t * a, unsigned value_width, int schedule,
+    uint32_t tile_items) {
+  GB_CHECK_INPUT(a != nullptr, "matrix is NULL");
+  GB_CHECK_INPUT(schedule >= GB_SCHED_AUTO && schedule <= GB_SCHED_MERGE,
+      "unknown schedule %d", schedule);
+  GB_CHECK_INPUT(value_width == GB_CSR_VALUES_F64 || value_width == GB_CSR_VALUES_F32,
+      "value_width must be GB_CSR_VALUES_F64 or GB_CSR_VALUES_F32");
+  if (tile_items) GB_TRY(gb::rebuild_plan(*a, tile_items, nullptr));
+  const int s = schedule == GB_SCHED_AUTO ? gb::default_schedule(a->plan) : schedule;
+  (value_width == GB_CSR_VALUES_F32 ? a->sched32 : a->sched64) = s;
+  return GOOSEBERRY_SUCCESS;
+}
+
+int gb_csr_autotune(gb_csr_t * a, unsigned value_width, gb_stream_t stream) {
+  GB_CHECK_INPUT(a != nullptr, "matrix is NULL");
+  GB_CHECK_INPUT(value_width == GB_CSR_VALUES_F64 || value_width == GB_CSR_VALUES_F32,
+      "value_width must be GB_CSR_VALUES_F64 or GB_CSR_VALUES_F32");
+  GB_CHECK_INPUT(value_width == GB_CSR_VALUES_F64 ? a->val64 != nullptr : a->val32 != nullptr,
+      "matrix holds no values of that width");
+  return gb::autotune(*a, value_width, static_cast<cudaStream_t>(stream));
+}
+
+int gb_plan_tiles_host(dim_t nrows, const ind_t * rowptr, ind_t nnz, uint32_t tile_items,
+    uint32_t * tiles, size_t max_tiles, uint32_t * ntiles, uint32_t * nlong,
+    gb_csr_info_t * info) {
+  GB_CHECK_INPUT(rowptr != nullptr, "rowptr is NULL");
+  gb::Plan p;
+  GB_TRY(gb::build_plan(nrows, rowptr, nnz, tile_items ? tile_items : 2048u, p));
+  if (ntiles) *ntiles = static_cast<uint32_t>(p.tiles.size());
+  if (nlong) *nlong = static_cast<uint32_t>(p.longrows.size());
+  if (tiles) {
+    GB_CHECK_INPUT(max_tiles >= p.tiles.size(), "room for %zu tiles, plan has %zu",
+        max_tiles, p.tiles.size());
+    for (size_t t = 0; t < p.tiles.size(); ++t) {
+      tiles[4 * t + 0] = p.tiles[t].row_begin;
+      tiles[4 * t + 1] = p.tiles[t].row_count;
+      tiles[4 * t + 2] = p.tiles[t].nnz_begin;
+      tiles[4 * t + 3] = p.tiles[t].nnz_count;
+    }
+  }
+  if (info) {
+    std::memset(info, 0, sizeof(*info));
+    info->nrows = nrows;
+    info->ncols = 0;
+    info->nnz = nnz;
+    info->ntiles = static_cast<uint32_t>(p.tiles.size());
+    info->nlong = static_cast<uint32_t>(p.longrows.size());
+    info->max_row = p.max_row;
+    info->mean_row = p.mean_row;
+    info->row_p50 = p.p50;
+    info->row_p90 = p.p90;
+    info->row_p99 = p.p99;
+    info->schedule = gb::default_schedule(p);
+    info->schedule_f32 = info->schedule;
+    info->tile_items = p.tile_items;
+  }
+  return GOOSEBERRY_SUCCESS;
+}
+
+int gb_spmv_f64(const gb_csr_t * a, const double * x, double * y, gb_stream_t stream) {
+  GB_CHECK_INPUT(a != nullptr, "matrix is NULL");
+  GB_CHECK_INPUT(a->nrows == 0 || y != nullptr, "y is NULL");
+  GB_CHECK_INPUT(a->nnz == 0 || x != nullptr, "x is NULL");
+  return gb::launch_spmv_f64(*a, a->sched64, x, y, 1, static_cast<cudaStream_t>(stream));
+}
+
+int gb_spmv_f32(const gb_csr_t * a, const float * x, float * y, gb_stream_t stream) {
+  GB_CHECK_INPUT(a != nullptr, "matrix is NULL");
+  GB_CHECK_INPUT(a->nrows == 0 || y != nullptr, "y is NULL");
+  GB_CHECK_INPUT(a->nnz == 0 || x != nullptr, "x is NULL");
+  return gb::launch_spmv_f32(*a, a->sched32, x, y, 1, static_cast<cudaStream_t>(stream));
+}
+
+int gb_spmm_f64(const gb_csr_t * a, dim_t bncols, const double * b, double * c,
+    gb_stream_t stream) {
+  GB_CHECK_INPUT(a != nullptr, "matrix is NULL");
+  GB_CHECK_INPUT(a->nrows == 0 || bncols == 0 || c != nullptr, "c is NULL");
+  GB_CHECK_INPUT(a->nnz == 0 || bncols == 0 || b != nullptr, "b is NULL");
+  for (dim_t j = 0; j < bncols; ++j)
+    GB_TRY(gb::launch_spmv_f64(*a, a->sched64, b + static_cast<size_t>(j) * a->ncols, c + j,
+        bncols, static_cast<cudaStream_t>(stream)));
+  return GOOSEBERRY_SUCCESS;
+}
+
+}  // extern "C"

@@ -1,0 +1,211 @@
+/*
+ * gooseberry_b200.h -- device-resident extension API of libgooseberry_b200.so.
+ *
+ * The reference keeps everything in host memory and re-reads the matrix on
+ * every call (src/blas.c:552-606, src/cgd.c:40-129).  On a GPU the matrix and
+ * the Krylov vectors should stay in HBM across calls, so this header adds
+ * opaque device-resident handles beside the drop-in API of gooseberry.h:
+ *
+ *   gb_csr_t  a CSR matrix in HBM (owned copy or borrowed device arrays) plus
+ *             its SpMV tile plan and schedule;
+ *   gb_cg_t   a CG solver workspace bound to one gb_csr_t.
+ *
+ * Conventions
+ *   - Return GOOSEBERRY_SUCCESS (1) or a gooseberry_error_t code; on failure
+ *     gb_last_error() returns a message (thread-local).
+ *   - `stream` is a cudaStream_t passed as void*; NULL is the legacy default
+ *     stream.  Calls taking device pointers are asynchronous on `stream`
+ *     unless stated otherwise.
+ *   - Index layout is gooseberry's CSR: uint32 rowptr[nrows+1] (row i holds
+ *     rowptr[i]..rowptr[i+1]-1), uint32 rowind[nnz] column indices, values
+ *     rowval[nnz] (src/matrix.h:37-45).
+ *   - The current CUDA device of the calling thread is used.
+ */
+#ifndef GOOSEBERRY_B200_H
+#define GOOSEBERRY_B200_H
+
+#include "gooseberry.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct gb_csr gb_csr_t;
+typedef struct gb_cg gb_cg_t;
+typedef void * gb_stream_t;
+
+/* ---- errors -------------------------------------------------------------- */
+
+/* Message describing the last failed call on this thread ("" if none).
+ * No reference counterpart (the reference prints with eprintf). */
+GOOSEBERRY_API const char * gb_last_error(void);
+
+/* ---- matrices ------------------------------------------------------------ */
+
+/* gb_csr_create flags */
+#define GB_CSR_VALUES_F64 0x1u      /* keep double values on the device      */
+#define GB_CSR_VALUES_F32 0x2u      /* keep float values (rounded from f64)   */
+#define GB_CSR_DEVICE_POINTERS 0x4u /* arrays are device memory; borrow them  */
+
+/* Row-length summary and chosen SpMV schedule of a matrix. */
+typedef struct gb_csr_info {
+  dim_t nrows, ncols;
+  ind_t nnz;
+  uint32_t ntiles;       /* row-aligned tiles of the SpMV plan               */
+  uint32_t nlong;        /* rows split across several tiles                  */
+  uint32_t max_row;      /* longest row                                      */
+  double mean_row;       /* nnz / nrows                                      */
+  uint32_t row_p50, row_p90, row_p99; /* row-length quantiles               */
+  int schedule;          /* gb_schedule_t of the f64 SpMV                    */
+  int schedule_f32;      /* gb_schedule_t of the f32 SpMV                    */
+  uint32_t tile_items;   /* rows + nnz per tile                              */
+} gb_csr_info_t;
+
+/* How the SpMV kernel reduces the products of one tile (a run of whole rows
+ * holding at most tile_items rows + nonzeros, staged in shared memory) into
+ * row sums. */
+typedef enum gb_schedule {
+  GB_SCHED_AUTO = 0,     /* autotuner decides (default)                      */
+  GB_SCHED_THREAD = 1,   /* one thread per row                               */
+  GB_SCHED_GROUP4 = 2,   /* 4 lanes per row                                  */
+  GB_SCHED_GROUP8 = 3,   /* 8 lanes per row                                  */
+  GB_SCHED_WARP = 4,     /* 32 lanes per row                                 */
+  GB_SCHED_MERGE = 5     /* merge-path split of rows+nnz over threads        */
+} gb_schedule_t;
+
+/*
+ * Create a device-resident CSR matrix.  Without GB_CSR_DEVICE_POINTERS the
+ * host arrays are uploaded into library-owned device memory; with it the
+ * device arrays are borrowed (they must outlive the handle and stay
+ * unchanged).  rowval64 is required for GB_CSR_VALUES_F64; rowval32 may be
+ * NULL, in which case float values are rounded from rowval64 on the device.
+ * Validates rowptr (non-decreasing, rowptr[nrows]-rowptr[0] == nnz) and every
+ * column index (< ncols); builds the tile plan.  Synchronous.
+ * Counterpart of matrix_init(MATRIX_TYPE_SPARSE_MATRIX, ...) followed by the
+ * caller filling rowptr/rowind/rowval (reference src/matrix.c:44-143).
+ */
+GOOSEBERRY_API int gb_csr_create(dim_t nrows, dim_t ncols, ind_t nnz, const ind_t * rowptr,
+    const dim_t * rowind, const double * rowval64, const float * rowval32,
+    unsigned flags, gb_stream_t stream, gb_csr_t ** out);
+
+/* Release a matrix (matrix_free, reference src/matrix.c:483-535). */
+GOOSEBERRY_API int gb_csr_destroy(gb_csr_t * a);
+
+GOOSEBERRY_API int gb_csr_get_info(const gb_csr_t * a, gb_csr_info_t * info);
+
+/* Fix the SpMV schedule of one value width (GB_CSR_VALUES_F64 or _F32).
+ * tile_items == 0 keeps the current tile size. */
+GOOSEBERRY_API int gb_csr_set_schedule(gb_csr_t * a, unsigned value_width, int schedule,
+    uint32_t tile_items);
+
+/* Time every candidate schedule on this matrix and keep the fastest; the
+ * choice is cached per process under a key of (row-length quantiles, nrows,
+ * nnz, value width) so equal-shaped matrices skip the timing.  Synchronous. */
+GOOSEBERRY_API int gb_csr_autotune(gb_csr_t * a, unsigned value_width, gb_stream_t stream);
+
+/* Run the SpMV tile planner on a HOST rowptr (no GPU involved).  Writes the
+ * tile and long-row counts; when tiles != NULL (room for max_tiles) also the
+ * tiles, 4 uint32 each: {first row | long-row id, row count (0 marks a chunk
+ * of a long row), first nonzero, nonzero count}.  Row-length quantiles go to
+ * info (optional).  Used for inspection and host-side tests; no reference
+ * counterpart (the reference splits rows evenly per thread,
+ * src/blas.c:597-601). */
+GOOSEBERRY_API int gb_plan_tiles_host(dim_t nrows, const ind_t * rowptr, ind_t nnz,
+    uint32_t tile_items, uint32_t * tiles, size_t max_tiles, uint32_t * ntiles,
+    uint32_t * nlong, gb_csr_info_t * info);
+
+/* ---- SpMV / SpMM on device vectors ---------------------------------------- */
+
+/* y = A x.  Device-resident counterpart of blas_spmult with bncols == 1
+ * (reference src/blas.c:552-606, inner loop src/blas.c:82-91).  f64: double
+ * values, x, y and accumulation.  f32: float values, x, y and accumulation. */
+GOOSEBERRY_API int gb_spmv_f64(const gb_csr_t * a, const double * x, double * y,
+    gb_stream_t stream);
+GOOSEBERRY_API int gb_spmv_f32(const gb_csr_t * a, const float * x, float * y,
+    gb_stream_t stream);
+
+/* C = A B, B column-major ncols x bncols, C row-major nrows x bncols
+ * (reference src/blas.c:82-91 with bncols > 1). */
+GOOSEBERRY_API int gb_spmm_f64(const gb_csr_t * a, dim_t bncols, const double * b, double * c,
+    gb_stream_t stream);
+
+/* ---- BLAS-1 on device vectors --------------------------------------------- */
+
+/* *result = sum a[i]*b[i], accumulated in double, deterministic (fixed
+ * reduction order).  result is a DEVICE pointer.  blas_dot, reference
+ * src/blas.c:413-430. */
+GOOSEBERRY_API int gb_dot_f64(size_t n, const double * a, const double * b, double * result,
+    gb_stream_t stream);
+GOOSEBERRY_API int gb_dot_f32(size_t n, const float * a, const float * b, double * result,
+    gb_stream_t stream);
+/* v *= s (blas_scale, src/blas.c:244-257); v += s (blas_add_scalar,
+ * src/blas.c:397-410); c = a + b (blas_add, src/blas.c:275-290);
+ * c = a - b (blas_sub, src/blas.c:321-336).  c may alias a or b. */
+GOOSEBERRY_API int gb_scale_f64(size_t n, double * v, double s, gb_stream_t stream);
+GOOSEBERRY_API int gb_add_scalar_f64(size_t n, double * v, double s, gb_stream_t stream);
+GOOSEBERRY_API int gb_add_f64(size_t n, const double * a, const double * b, double * c,
+    gb_stream_t stream);
+GOOSEBERRY_API int gb_sub_f64(size_t n, const double * a, const double * b, double * c,
+    gb_stream_t stream);
+GOOSEBERRY_API int gb_scale_f32(size_t n, float * v, float s, gb_stream_t stream);
+GOOSEBERRY_API int gb_add_scalar_f32(size_t n, float * v, float s, gb_stream_t stream);
+
+/* ---- conjugate gradient --------------------------------------------------- */
+
+typedef enum gb_cg_mode {
+  GB_CG_F64 = 0,   /* plain FP64 CG, the reference's algorithm             */
+  GB_CG_MIXED = 1  /* FP32 values/vectors inside, FP64 residual refinement  */
+} gb_cg_mode_t;
+
+typedef enum gb_cg_status {
+  GB_CG_CONVERGED = 0,  /* ||r|| <= tolerance                                 */
+  GB_CG_MAXITER = 1,    /* iteration limit reached first                      */
+  GB_CG_BREAKDOWN = 2,  /* p.Ap <= 0: matrix not SPD                          */
+  GB_CG_NONFINITE = 3   /* NaN or Inf appeared                                */
+} gb_cg_status_t;
+
+typedef struct gb_cg_result {
+  size_t iterations;    /* CG iterations run (inner iterations for MIXED)     */
+  size_t refinements;   /* FP64 residual recomputations (MIXED)               */
+  double rnorm;         /* final ||b - A x||_2 as tracked by the solver       */
+  double bnorm;         /* ||b||_2                                            */
+  int status;           /* gb_cg_status_t                                     */
+  size_t kernel_launches; /* GPU kernels this solve launched                  */
+} gb_cg_result_t;
+
+/* Allocate the workspace of a CG solver for matrix a (the matrix must hold
+ * the value widths the mode needs: F64 for GB_CG_F64, F64 and F32 for
+ * GB_CG_MIXED).  Reference: the five work vectors cgd allocates per call
+ * (src/cgd.c:67-77). */
+GOOSEBERRY_API int gb_cg_create(const gb_csr_t * a, int mode, gb_cg_t ** out);
+GOOSEBERRY_API int gb_cg_destroy(gb_cg_t * s);
+
+/*
+ * Solve A x = b from x0 = 0 with device vectors b, x.  Stops when
+ * ||r||_2 <= tol (tol_relative == 0: absolute, the reference's rule,
+ * src/cgd.c:115-119) or ||r||_2 <= tol * ||b||_2 (tol_relative != 0), or
+ * after niter iterations (0: no limit).  history (optional, HOST pointer)
+ * receives ||r||_2 after each iteration, up to history_len entries.
+ * Synchronous on `stream` (returns after the solve finished).
+ */
+GOOSEBERRY_API int gb_cg_solve(gb_cg_t * s, const double * b, double * x, double tol,
+    int tol_relative, size_t niter, double * history, size_t history_len,
+    gb_cg_result_t * result, gb_stream_t stream);
+
+/*
+ * Measurement hook: start a solve of A x = b and run its first `iterations`
+ * iterations launch by launch, timing every launch with CUDA events on
+ * `stream`.  ms[k] receives the mean duration in milliseconds of kernel k of
+ * an iteration (k < nkernels; F64: 0 = SpMV+direction+p.Ap, 1 = x/r update +
+ * r.r).  Returns the number of kernels per iteration in *nkernels.  Leaves
+ * the solver ready for the next gb_cg_solve.  No reference counterpart (the
+ * reference only has wall-clock phase timers, src/gooseberry_bin.c:2078-2113).
+ */
+GOOSEBERRY_API int gb_cg_profile(gb_cg_t * s, const double * b, size_t iterations,
+    double * ms, size_t ms_len, size_t * nkernels, gb_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GOOSEBERRY_B200_H */

@@ -1,0 +1,226 @@
+"""CPU oracle for the SpMV / CG hot path -- TEST INFRASTRUCTURE ONLY.
+
+Two checkers, both loaded with ctypes:
+
+* ``liboracle.so`` -- our C restatement (``oracle/gb_oracle.c``) of
+  ``src/blas.c:82-91`` (per-row sequential SpMV), ``src/blas.c:413-430``
+  (dot) and ``src/cgd.c:81-119`` (CG update order).
+* ``_ref/libgbref_{f64,f32}.so`` -- the reference's OWN ``src/blas.c``,
+  ``src/cgd.c`` and ``src/matrix.c`` compiled unmodified against a
+  project-written domlib shim (``oracle/Makefile``), reached through
+  ``oracle/ref_driver.c``.  Present only where it was built (it needs the
+  reference sources at build time; the built files travel with the repo).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline /
+reference legs may import this package.  The product (``gooseberry_b200``)
+never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+_REF = {}
+
+_u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+
+
+def build(ref_root: str | None = "/root/reference", quiet: bool = True) -> None:
+    """Compile the restatement, and the reference build when its sources exist."""
+    targets = ["oracle"]
+    if ref_root and os.path.isdir(os.path.join(ref_root, "src")):
+        targets.append("ref")
+    cmd = ["make", "-C", _HERE, f"REF={ref_root or ''}"] + targets
+    subprocess.run(cmd, check=True, capture_output=quiet)
+
+
+def _lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build(quiet=True)
+        lib = C.CDLL(path)
+        for real, p in (("f64", _f64p), ("f32", _f32p)):
+            ctype = C.c_double if real == "f64" else C.c_float
+            f = getattr(lib, f"oracle_spmm_{real}")
+            f.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, _u32p, _u32p, p, p, p,
+                          C.c_void_p, C.c_uint32, C.c_int]
+            f.restype = None
+            f = getattr(lib, f"oracle_dot_{real}")
+            f.argtypes = [C.c_size_t, p, p]
+            f.restype = ctype
+            for nm in ("scale", "add_scalar"):
+                f = getattr(lib, f"oracle_{nm}_{real}")
+                f.argtypes = [C.c_size_t, p, ctype]
+                f.restype = None
+            f = getattr(lib, f"oracle_cgd_{real}")
+            f.argtypes = [C.c_uint32, _u32p, _u32p, p, p, p, ctype, C.c_size_t,
+                          C.c_void_p, C.c_size_t, C.POINTER(C.c_double), C.c_int]
+            f.restype = C.c_size_t
+        _LIB = lib
+    return _LIB
+
+
+def ref_available(real: str = "f64") -> bool:
+    return os.path.exists(os.path.join(_HERE, "_ref", f"libgbref_{real}.so"))
+
+
+def _ref(real: str = "f64"):
+    if real not in _REF:
+        path = os.path.join(_HERE, "_ref", f"libgbref_{real}.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"reference oracle not built: {path}")
+        lib = C.CDLL(path)
+        p = _f64p if real == "f64" else _f32p
+        lib.gbref_real_size.restype = C.c_int
+        lib.gbref_set_threads.argtypes = [C.c_int]
+        lib.gbref_set_threads.restype = None
+        lib.gbref_spmult.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, _u32p, _u32p,
+                                     p, p, p, C.c_void_p, C.c_uint32]
+        lib.gbref_spmult.restype = C.c_int
+        lib.gbref_dot.argtypes = [C.c_uint32, p, p]
+        lib.gbref_dot.restype = C.c_double
+        lib.gbref_cgd.argtypes = [C.c_uint32, _u32p, _u32p, p, p, p, C.c_double,
+                                  C.c_size_t, C.POINTER(C.c_size_t),
+                                  C.POINTER(C.c_double), C.c_void_p, C.c_size_t]
+        lib.gbref_cgd.restype = C.c_int
+        want = 8 if real == "f64" else 4
+        if lib.gbref_real_size() != want:
+            raise RuntimeError(f"{path}: real_t has {lib.gbref_real_size()} bytes")
+        _REF[real] = lib
+    return _REF[real]
+
+
+def ref_set_threads(n: int) -> None:
+    """OpenMP threads used by the reference build (both widths)."""
+    for real in ("f64", "f32"):
+        if ref_available(real):
+            _ref(real).gbref_set_threads(int(n))
+
+
+def _dt(real):
+    return np.float64 if real == "f64" else np.float32
+
+
+def _blocks_arg(blocks):
+    if blocks is None:
+        return None, 0, None
+    b = np.ascontiguousarray(blocks, dtype=np.uint32)
+    return b.ctypes.data_as(C.c_void_p), len(b) - 1, b
+
+
+def spmm(rowptr, rowind, rowval, B, ncols=None, bncols=1, blocks=None, out=None,
+         threads=1, real="f64"):
+    """C = A*B via the restatement (src/blas.c:82-91).  B is column-major."""
+    dt = _dt(real)
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+    rowind = np.ascontiguousarray(rowind, dtype=np.uint32)
+    rowval = np.ascontiguousarray(rowval, dtype=dt)
+    B = np.ascontiguousarray(B, dtype=dt).reshape(-1)
+    n = len(rowptr) - 1
+    ncols = n if ncols is None else ncols
+    C_ = np.zeros(n * bncols, dtype=dt) if out is None else out
+    bp, nb, keep = _blocks_arg(blocks)
+    getattr(_lib(), f"oracle_spmm_{real}")(n, ncols, bncols, rowptr, rowind, rowval, B,
+                                           C_, bp, nb, int(threads))
+    del keep
+    return C_
+
+
+def spmv(rowptr, rowind, rowval, x, threads=1, real="f64"):
+    return spmm(rowptr, rowind, rowval, x, ncols=len(x), threads=threads, real=real)
+
+
+def dot(a, b, real="f64"):
+    dt = _dt(real)
+    a = np.ascontiguousarray(a, dtype=dt)
+    b = np.ascontiguousarray(b, dtype=dt)
+    return float(getattr(_lib(), f"oracle_dot_{real}")(len(a), a, b))
+
+
+def scale(v, s, real="f64"):
+    v = np.array(v, dtype=_dt(real), copy=True)
+    getattr(_lib(), f"oracle_scale_{real}")(len(v), v, s)
+    return v
+
+
+def add_scalar(v, s, real="f64"):
+    v = np.array(v, dtype=_dt(real), copy=True)
+    getattr(_lib(), f"oracle_add_scalar_{real}")(len(v), v, s)
+    return v
+
+
+def cgd(rowptr, rowind, rowval, b, error, niter, threads=1, real="f64", history=False):
+    """Restated cgd (src/cgd.c:40-129).  Returns (x, iterations, last_norm[, hist])."""
+    dt = _dt(real)
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+    rowind = np.ascontiguousarray(rowind, dtype=np.uint32)
+    rowval = np.ascontiguousarray(rowval, dtype=dt)
+    b = np.ascontiguousarray(b, dtype=dt)
+    n = len(b)
+    x = np.zeros(n, dtype=dt)
+    last = C.c_double(0)
+    hist = np.zeros(niter if niter else 0, dtype=np.float64)
+    hp = hist.ctypes.data_as(C.c_void_p) if history and niter else None
+    it = getattr(_lib(), f"oracle_cgd_{real}")(n, rowptr, rowind, rowval, b, x, error,
+                                               niter, hp, len(hist), C.byref(last),
+                                               int(threads))
+    if history:
+        return x, int(it), last.value, hist[:it]
+    return x, int(it), last.value
+
+
+def ref_spmm(rowptr, rowind, rowval, B, ncols=None, bncols=1, blocks=None, out=None,
+             real="f64"):
+    """C = A*B through the reference's own blas_spmult (src/blas.c:552-606)."""
+    dt = _dt(real)
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+    rowind = np.ascontiguousarray(rowind, dtype=np.uint32)
+    rowval = np.ascontiguousarray(rowval, dtype=dt)
+    B = np.ascontiguousarray(B, dtype=dt).reshape(-1)
+    n = len(rowptr) - 1
+    ncols = n if ncols is None else ncols
+    C_ = np.zeros(n * bncols, dtype=dt) if out is None else out
+    bp, nb, keep = _blocks_arg(blocks)
+    rc = _ref(real).gbref_spmult(n, ncols, bncols, rowptr, rowind, rowval, B, C_, bp, nb)
+    del keep
+    if rc != 1:
+        raise RuntimeError(f"blas_spmult returned {rc}")
+    return C_
+
+
+def ref_dot(a, b, real="f64"):
+    dt = _dt(real)
+    a = np.ascontiguousarray(a, dtype=dt)
+    b = np.ascontiguousarray(b, dtype=dt)
+    return float(_ref(real).gbref_dot(len(a), a, b))
+
+
+def ref_cgd(rowptr, rowind, rowval, b, error, niter, real="f64", history=False):
+    """The reference's own cgd (src/cgd.c:40-129); iterations parsed from its ITER lines."""
+    dt = _dt(real)
+    rowptr = np.array(rowptr, dtype=np.uint32)
+    rowind = np.array(rowind, dtype=np.uint32)
+    rowval = np.array(rowval, dtype=dt)
+    b = np.array(b, dtype=dt)
+    n = len(b)
+    x = np.zeros(n, dtype=dt)
+    it = C.c_size_t(0)
+    last = C.c_double(0)
+    hist = np.zeros(niter if niter else 0, dtype=np.float64)
+    hp = hist.ctypes.data_as(C.c_void_p) if history and niter else None
+    rc = _ref(real).gbref_cgd(n, rowptr, rowind, rowval, b, x, float(error), niter,
+                              C.byref(it), C.byref(last), hp, len(hist))
+    if rc != 1:
+        raise RuntimeError(f"cgd returned {rc}")
+    if history:
+        return x, int(it.value), last.value, hist[: it.value]
+    return x, int(it.value), last.value

@@ -1,0 +1,200 @@
+/*
+ * gb_oracle.c -- CPU restatement of gooseberry's SpMV / BLAS-1 / CG hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker for the CUDA path and the "port" CPU
+ * baseline.  The product never links, loads or calls it.  Compiled with
+ * -ffp-contract=off so no multiply-add is fused, like the reference's x86-64
+ * build (no FMA in the baseline ISA).
+ *
+ * Each function states the reference lines it follows.  With one thread the
+ * results are bit-identical to the reference built from its own sources
+ * (oracle/_ref), which the CPU tests check.
+ */
+#include <math.h>
+#include <stddef.h>
+#include <stdint.h>
+#include <string.h>
+#include <stdlib.h>
+
+typedef uint32_t dim_t;
+typedef uint32_t ind_t;
+
+/*
+ * C = A*B for CSR A and column-major dense B (bcolval[j*ancols + l]), output
+ * row-major (crowval[i*bncols + j]).  Per row and column: the sum starts at 0
+ * and adds val[k]*B[ind[k]] for k ascending -- src/blas.c:82-91
+ * (__sparse_mult_dense_block).  `blocks` (nblocks+1 row boundaries) restricts
+ * the computed rows to the union of [blocks[c], blocks[c+1]) exactly as the
+ * blocks branch of blas_spmult (src/blas.c:576-595); rows outside stay
+ * untouched.  `nthreads` > 1 splits rows over OpenMP threads (src/blas.c:565,
+ * 597-601); the split never changes a row's result.
+ */
+#define GB_ORACLE_SPMM(NAME, REAL)                                             \
+  void NAME(dim_t anrows, dim_t ancols, dim_t bncols, const ind_t * rowptr,   \
+      const dim_t * rowind, const REAL * rowval, const REAL * bcolval,         \
+      REAL * crowval, const dim_t * blocks, dim_t nblocks, int nthreads);      \
+  static void NAME##_block(dim_t start, dim_t end, dim_t ancols,              \
+      dim_t bncols, const ind_t * rowptr, const dim_t * rowind,                \
+      const REAL * rowval, const REAL * bcolval, REAL * crowval)               \
+  {                                                                            \
+    dim_t i, j;                                                                \
+    ind_t k;                                                                   \
+    for (i = start; i < end; ++i) {                                            \
+      for (j = 0; j < bncols; ++j) {                                           \
+        REAL acc = 0;                                                          \
+        for (k = rowptr[i]; k < rowptr[i + 1]; ++k) {                          \
+          acc += rowval[k] *                                                   \
+              bcolval[(size_t)j * (size_t)ancols + (size_t)rowind[k]];         \
+        }                                                                      \
+        crowval[(size_t)i * (size_t)bncols + (size_t)j] = acc;                 \
+      }                                                                        \
+    }                                                                          \
+  }                                                                            \
+  void NAME(dim_t anrows, dim_t ancols, dim_t bncols, const ind_t * rowptr,   \
+      const dim_t * rowind, const REAL * rowval, const REAL * bcolval,         \
+      REAL * crowval, const dim_t * blocks, dim_t nblocks, int nthreads)       \
+  {                                                                            \
+    if (nthreads < 1) {                                                        \
+      nthreads = 1;                                                            \
+    }                                                                          \
+    if (blocks) {                                                              \
+      long c;                                                                  \
+      _Pragma("omp parallel for num_threads(nthreads) schedule(static,1)")     \
+      for (c = 0; c < (long)nblocks; ++c) {                                    \
+        NAME##_block(blocks[c], blocks[c + 1], ancols, bncols, rowptr, rowind, \
+            rowval, bcolval, crowval);                                         \
+      }                                                                        \
+    } else {                                                                   \
+      long c;                                                                  \
+      long const nchunk = (long)nthreads * 8;                                  \
+      _Pragma("omp parallel for num_threads(nthreads) schedule(static,1)")     \
+      for (c = 0; c < nchunk; ++c) {                                           \
+        size_t const q = anrows / (size_t)nchunk, r = anrows % (size_t)nchunk; \
+        size_t const s = (size_t)c * q + ((size_t)c < r ? (size_t)c : r);      \
+        size_t const e = s + q + ((size_t)c < r ? 1 : 0);                      \
+        NAME##_block((dim_t)s, (dim_t)e, ancols, bncols, rowptr, rowind,       \
+            rowval, bcolval, crowval);                                         \
+      }                                                                        \
+    }                                                                          \
+  }
+
+GB_ORACLE_SPMM(oracle_spmm_f64, double)
+GB_ORACLE_SPMM(oracle_spmm_f32, float)
+
+/* sum_i a[i]*b[i], i ascending, accumulated in REAL -- src/blas.c:413-430
+ * (blas_dot) as it runs on one OpenMP thread. */
+#define GB_ORACLE_DOT(NAME, REAL)                                              \
+  REAL NAME(size_t n, const REAL * a, const REAL * b);                         \
+  REAL NAME(size_t n, const REAL * a, const REAL * b)                          \
+  {                                                                            \
+    size_t i;                                                                  \
+    REAL x = 0;                                                                \
+    for (i = 0; i < n; ++i) {                                                  \
+      x += a[i] * b[i];                                                        \
+    }                                                                          \
+    return x;                                                                  \
+  }
+GB_ORACLE_DOT(oracle_dot_f64, double)
+GB_ORACLE_DOT(oracle_dot_f32, float)
+
+/* v[i] *= s -- src/blas.c:244-257 (blas_scale); v[i] += s --
+ * src/blas.c:397-410 (blas_add_scalar). */
+void oracle_scale_f64(size_t n, double * v, double s);
+void oracle_scale_f64(size_t n, double * v, double s)
+{
+  size_t i;
+  for (i = 0; i < n; ++i) v[i] *= s;
+}
+void oracle_add_scalar_f64(size_t n, double * v, double s);
+void oracle_add_scalar_f64(size_t n, double * v, double s)
+{
+  size_t i;
+  for (i = 0; i < n; ++i) v[i] += s;
+}
+void oracle_scale_f32(size_t n, float * v, float s);
+void oracle_scale_f32(size_t n, float * v, float s)
+{
+  size_t i;
+  for (i = 0; i < n; ++i) v[i] *= s;
+}
+void oracle_add_scalar_f32(size_t n, float * v, float s);
+void oracle_add_scalar_f32(size_t n, float * v, float s)
+{
+  size_t i;
+  for (i = 0; i < n; ++i) v[i] += s;
+}
+
+/*
+ * Unpreconditioned CG with exactly the update order of cgd (src/cgd.c:81-119):
+ *   x = 0; r = b; p = r; dr = r.r
+ *   loop iter = 0.. while iter < niter or niter == 0:
+ *     ap = A p; alpha = dr / (p.ap)
+ *     p *= alpha; nx = x + p                      (cgd.c:92-93)
+ *     ap *= alpha; nr = r - ap                    (cgd.c:96-97)
+ *     dnr = nr.nr; beta = dnr / dr                (cgd.c:100-101)
+ *     p *= beta/alpha; p = nr + p                 (cgd.c:104-105)
+ *     x = nx; r = nr; dr = dnr                    (cgd.c:108-112)
+ *     rmse = sqrt(dr); record; stop if rmse <= error   (cgd.c:115-119)
+ * `error` is the reference's ABSOLUTE bound on ||r||_2.  Returns the number of
+ * iterations run (the reference's ITER line count); history[k] (if given)
+ * receives rmse after iteration k.  Dots are sequential (one-thread blas_dot);
+ * the SpMV uses `nthreads` threads (row split only, results unchanged).
+ * niter == 0 is unbounded, as in the reference; the tests never pass it.
+ */
+#define GB_ORACLE_CGD(NAME, REAL, SPMM, DOT)                                   \
+  size_t NAME(dim_t n, const ind_t * rowptr, const dim_t * rowind,             \
+      const REAL * rowval, const REAL * b, REAL * x, REAL error, size_t niter, \
+      double * history, size_t history_len, double * last_norm,                \
+      int nthreads);                                                           \
+  size_t NAME(dim_t n, const ind_t * rowptr, const dim_t * rowind,             \
+      const REAL * rowval, const REAL * b, REAL * x, REAL error, size_t niter, \
+      double * history, size_t history_len, double * last_norm, int nthreads)  \
+  {                                                                            \
+    size_t iter, i, count = 0;                                                 \
+    REAL alpha, beta, rmse, dr, dnr;                                           \
+    REAL * r = (REAL *)malloc(sizeof(REAL) * (n ? n : 1));                     \
+    REAL * p = (REAL *)malloc(sizeof(REAL) * (n ? n : 1));                     \
+    REAL * nr = (REAL *)malloc(sizeof(REAL) * (n ? n : 1));                    \
+    REAL * nx = (REAL *)malloc(sizeof(REAL) * (n ? n : 1));                    \
+    REAL * ap = (REAL *)malloc(sizeof(REAL) * (n ? n : 1));                    \
+    *last_norm = -1.0;                                                         \
+    for (i = 0; i < n; ++i) {                                                  \
+      x[i] = 0;                                                                \
+      r[i] = b[i];                                                             \
+      p[i] = r[i];                                                             \
+    }                                                                          \
+    dr = DOT(n, r, r);                                                         \
+    for (iter = 0; iter < niter || niter == 0; ++iter) {                       \
+      SPMM(n, n, 1, rowptr, rowind, rowval, p, ap, NULL, 0, nthreads);         \
+      alpha = dr / DOT(n, p, ap);                                              \
+      for (i = 0; i < n; ++i) p[i] *= alpha;                                   \
+      for (i = 0; i < n; ++i) nx[i] = x[i] + p[i];                             \
+      for (i = 0; i < n; ++i) ap[i] *= alpha;                                  \
+      for (i = 0; i < n; ++i) nr[i] = r[i] - ap[i];                            \
+      dnr = DOT(n, nr, nr);                                                    \
+      beta = dnr / dr;                                                         \
+      {                                                                        \
+        REAL const s = beta / alpha;                                           \
+        for (i = 0; i < n; ++i) p[i] *= s;                                     \
+      }                                                                        \
+      for (i = 0; i < n; ++i) p[i] = nr[i] + p[i];                             \
+      memcpy(x, nx, sizeof(REAL) * n);                                         \
+      memcpy(r, nr, sizeof(REAL) * n);                                         \
+      dr = dnr;                                                                \
+      rmse = (REAL)sqrt((double)dr);                                           \
+      if (history && count < history_len) history[count] = (double)rmse;      \
+      ++count;                                                                 \
+      *last_norm = (double)rmse;                                               \
+      if (rmse <= error) {                                                     \
+        break;                                                                 \
+      }                                                                        \
+    }                                                                          \
+    free(r);                                                                   \
+    free(p);                                                                   \
+    free(nr);                                                                  \
+    free(nx);                                                                  \
+    free(ap);                                                                  \
+    return count;                                                              \
+  }
+GB_ORACLE_CGD(oracle_cgd_f64, double, oracle_spmm_f64, oracle_dot_f64)
+GB_ORACLE_CGD(oracle_cgd_f32, float, oracle_spmm_f32, oracle_dot_f32)

@@ -1,0 +1,150 @@
+#define _POSIX_C_SOURCE 200809L
+/*
+ * ref_driver.c -- flat C entry points into the REFERENCE's own hot path,
+ * compiled together with the unmodified reference sources src/blas.c,
+ * src/cgd.c and src/matrix.c into oracle/_ref/libgbref_{f64,f32}.so.
+ *
+ * TEST INFRASTRUCTURE ONLY (the checker and the CPU baseline).  Nothing in the
+ * product links it.  `real_t` is double when built with
+ * -DGOOSEBERRY_DOUBLE_REALS=1 and float otherwise, exactly as in the reference
+ * (include/gooseberry.h:73-79).
+ *
+ * - gbref_spmult: forwards to blas_spmult (src/blas.c:552-606), the body of
+ *   gooseberry_spmult (src/gooseberry.c:53-67).
+ * - gbref_dot:    forwards to blas_dot (src/blas.c:413-430).
+ * - gbref_cgd:    wraps cgd (src/cgd.c:40-129) for raw CSR arrays.  cgd prints
+ *   one "ITER: k RMSE: v" line per iteration (src/cgd.c:116) and returns no
+ *   iteration count, so stdout is redirected to a temporary file for the call
+ *   and the ITER lines are parsed back into (iterations, last norm, history).
+ * - permute_* stubs: src/matrix.c:256-373 references them for permutations,
+ *   which nothing on the SpMV/CG path calls.
+ */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <unistd.h>
+
+#include "matrix.h"
+#include "blas.h"
+#include "cgd.h"
+#include "permute.h"
+#include <omp.h>
+
+int permute_sparse(dim_t nrows, dim_t ncols, ind_t * rowptr, dim_t * rowind,
+    real_t * rowval, const dim_t * rowperm, const dim_t * colperm)
+{
+  (void)nrows; (void)ncols; (void)rowptr; (void)rowind; (void)rowval;
+  (void)rowperm; (void)colperm;
+  return GOOSEBERRY_ERROR_UNIMPLEMENTED;
+}
+
+int permute_dense(dim_t nrows, dim_t ncols, real_t * rowval,
+    const dim_t * rowperm, const dim_t * colperm)
+{
+  (void)nrows; (void)ncols; (void)rowval; (void)rowperm; (void)colperm;
+  return GOOSEBERRY_ERROR_UNIMPLEMENTED;
+}
+
+int permute_dense_rev(dim_t nrows, dim_t ncols, real_t * rowval,
+    const dim_t * rowperm, const dim_t * colperm)
+{
+  (void)nrows; (void)ncols; (void)rowval; (void)rowperm; (void)colperm;
+  return GOOSEBERRY_ERROR_UNIMPLEMENTED;
+}
+
+int gbref_real_size(void);
+void gbref_set_threads(int n);
+int gbref_spmult(dim_t anrows, dim_t ancols, dim_t bncols,
+    const ind_t * arowptr, const dim_t * arowind, const real_t * arowval,
+    const real_t * bcolval, real_t * crowval, const dim_t * blocks,
+    dim_t nblocks);
+double gbref_dot(dim_t n, const real_t * a, const real_t * b);
+int gbref_cgd(dim_t n, ind_t * rowptr, dim_t * rowind, real_t * rowval,
+    real_t * b, real_t * x, double error, size_t niter, size_t * iters,
+    double * last_norm, double * history, size_t history_len);
+
+/* OpenMP thread count of the reference's parallel regions.  With 1 thread
+ * blas_dot sums in index order, which makes cgd bit-reproducible. */
+void gbref_set_threads(int n)
+{
+  omp_set_num_threads(n > 0 ? n : 1);
+}
+
+int gbref_real_size(void)
+{
+  return (int)sizeof(real_t);
+}
+
+int gbref_spmult(dim_t anrows, dim_t ancols, dim_t bncols,
+    const ind_t * arowptr, const dim_t * arowind, const real_t * arowval,
+    const real_t * bcolval, real_t * crowval, const dim_t * blocks,
+    dim_t nblocks)
+{
+  return blas_spmult(anrows, ancols, bncols, arowptr, arowind, arowval,
+      bcolval, crowval, blocks, nblocks);
+}
+
+double gbref_dot(dim_t n, const real_t * a, const real_t * b)
+{
+  return (double)blas_dot(n, a, b);
+}
+
+int gbref_cgd(dim_t n, ind_t * rowptr, dim_t * rowind, real_t * rowval,
+    real_t * b, real_t * x, double error, size_t niter, size_t * iters,
+    double * last_norm, double * history, size_t history_len)
+{
+  matrix_t a, bv, xv;
+  FILE * tmp;
+  int saved, rv;
+  char line[256];
+  size_t count = 0, k;
+  double v, last = -1.0;
+
+  memset(&a, 0, sizeof(a));
+  memset(&bv, 0, sizeof(bv));
+  memset(&xv, 0, sizeof(xv));
+  a.type = MATRIX_TYPE_SPARSE_MATRIX;
+  a.nrows = n;
+  a.ncols = n;
+  a.rowptr = rowptr;
+  a.rowind = rowind;
+  a.rowval = rowval;
+  bv.type = MATRIX_TYPE_DENSE_VECTOR;
+  bv.nrows = n;
+  bv.ncols = 1;
+  bv.rowval = bv.colval = b;
+  xv.type = MATRIX_TYPE_DENSE_VECTOR;
+  xv.nrows = n;
+  xv.ncols = 1;
+  xv.rowval = xv.colval = x;
+
+  tmp = tmpfile();
+  if (!tmp) {
+    return -1;
+  }
+  fflush(stdout);
+  saved = dup(STDOUT_FILENO);
+  if (saved < 0 || dup2(fileno(tmp), STDOUT_FILENO) < 0) {
+    fclose(tmp);
+    return -1;
+  }
+  rv = cgd(&a, &bv, &xv, (real_t)error, niter);
+  fflush(stdout);
+  dup2(saved, STDOUT_FILENO);
+  close(saved);
+
+  rewind(tmp);
+  while (fgets(line, sizeof(line), tmp)) {
+    if (sscanf(line, "ITER: %zu RMSE: %lf", &k, &v) == 2) {
+      if (history && count < history_len) {
+        history[count] = v;
+      }
+      ++count;
+      last = v;
+    }
+  }
+  fclose(tmp);
+  *iters = count;
+  *last_norm = last;
+  return rv;
+}

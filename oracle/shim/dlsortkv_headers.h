@@ -1,0 +1,2 @@
+/* Oracle shim (test infrastructure): dlsortkv_headers.h is instantiated by the
+ * reference headers but nothing on the SpMV/CG path uses it. */

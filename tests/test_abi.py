@@ -1,0 +1,89 @@
+"""The C-ABI library without a GPU: it loads, exports every entry point the
+headers declare, and its host-side planner behaves."""
+from __future__ import annotations
+
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import gooseberry_b200 as gb
+from gooseberry_b200 import workloads as W
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for h in ("gooseberry.h", "gooseberry_b200.h"):
+        src = open(os.path.join(ROOT, "include", h)).read()
+        names |= set(re.findall(r"GOOSEBERRY_API\s+[\w\s\*]+?\b(\w+)\s*\(", src))
+    return names
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    L = gb.lib()
+    decl = declared_symbols()
+    assert len(decl) >= 25
+    missing = [n for n in decl if not hasattr(L, n)]
+    assert not missing, missing
+    # and the Python layer binds exactly what the headers declare
+    assert decl == set(gb.SIGNATURES), decl ^ set(gb.SIGNATURES)
+    out = subprocess.run(["nm", "-D", "--defined-only", gb.LIB_PATH], capture_output=True,
+                         text=True, check=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines() if " T " in ln}
+    assert decl <= exported
+
+
+def test_missing_library_fails_loudly(monkeypatch):
+    monkeypatch.setattr(gb, "_LIB", None)
+    monkeypatch.setattr(gb, "LIB_PATH", "/nonexistent/libgooseberry_b200.so")
+    with pytest.raises(ImportError):
+        gb.lib()
+
+
+def _check_plan(rowptr, tiles, nlong, T):
+    n = len(rowptr) - 1
+    covered = np.zeros(n, np.int64)
+    long_rows = []
+    for rb, rc, nb, nc in tiles.astype(np.int64):
+        if rc == 0:
+            long_rows.append(nb)
+            continue
+        assert rowptr[rb] == nb and rowptr[rb + rc] - nb == nc
+        assert nc + rc <= T
+        covered[rb:rb + rc] += 1
+    lengths = np.diff(rowptr.astype(np.int64))
+    is_long = lengths + 1 > T
+    assert np.all(covered[~is_long] == 1) and np.all(covered[is_long] == 0)
+    assert nlong == int(is_long.sum())
+    # chunks of a long row cover it exactly, in order
+    chunks = tiles[tiles[:, 1] == 0].astype(np.int64)
+    assert chunks[:, 3].sum() == lengths[is_long].sum()
+
+
+def test_planner_uniform_and_powerlaw():
+    for A in (W.uniform_rows(5000, 10, seed=1), W.powerlaw_rows(20000, 320000, seed=2,
+                                                                  cap=20000)):
+        for T in (256, 2048):
+            tiles, nlong, info = gb.plan_tiles(A.rowptr, T)
+            _check_plan(A.rowptr, tiles, nlong, T)
+            L = A.row_lengths()
+            assert info.max_row == L.max()
+            assert info.row_p50 == int(np.quantile(L, 0.5, method="inverted_cdf"))
+
+
+def test_planner_empty_rows_and_empty_matrix():
+    rp = np.array([0, 0, 0, 3, 3, 3, 10], np.uint32)
+    tiles, nlong, _ = gb.plan_tiles(rp, 64)
+    _check_plan(rp, tiles, nlong, 64)
+    tiles, nlong, info = gb.plan_tiles(np.zeros(1, np.uint32), 64)
+    assert len(tiles) == 0 and nlong == 0
+
+
+def test_planner_rejects_bad_rowptr():
+    with pytest.raises(gb.GooseberryError) as e:
+        gb.plan_tiles(np.array([0, 5, 3, 8], np.uint32), 64)
+    assert e.value.code == 3 and "decreases" in str(e.value)

@@ -1,0 +1,86 @@
+"""CG parity on the GPU: same stopping rule and iteration count as the
+reference's cgd (within +-2 iterations) and a true residual at the requested
+level, on the golden cases and on the full 1024x1024 Laplacian."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import gooseberry_b200 as gb
+from gooseberry_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    assert t.cuda.is_available()
+    return t
+
+
+def _true_res(c, x):
+    import scipy.sparse as sp
+    n = len(c["b"])
+    A = sp.csr_matrix((c["rowval"], c["rowind"].astype(np.int64),
+                       c["rowptr"].astype(np.int64)), shape=(n, n))
+    return float(np.linalg.norm(c["b"] - A @ x))
+
+
+def test_dropin_cgd_matches_reference_iterations(cg_golden):
+    for name, c in cg_golden.items():
+        err, niter = float(c["error"]), int(c["niter"])
+        x, it, rn, hist = gb.cgd(c["rowptr"], c["rowind"], c["rowval"], c["b"], err, niter,
+                                 history=True)
+        ref_it = int(c["iterations"])
+        assert abs(it - ref_it) <= 2, (name, it, ref_it)
+        assert len(hist) == it and hist[-1] == pytest.approx(rn)
+        if name == "maxiter":
+            assert it == niter
+        else:
+            assert rn <= err and hist[-2] > err
+            assert _true_res(c, x) <= 1.5 * err, name
+        # the solution agrees with the reference's to the accuracy CG reached
+        xr = c["x"]
+        assert np.linalg.norm(x - xr) <= 1e-4 * np.linalg.norm(xr) + 1e-12, name
+
+
+def test_device_solver_relative_tolerance(torch, cg_golden):
+    c = cg_golden["laplace64"]
+    A = gb.CsrMatrix.from_host(rowptr=c["rowptr"], rowind=c["rowind"], rowval=c["rowval"])
+    S = gb.CgSolver(A)
+    b = torch.from_numpy(c["b"]).cuda()
+    bn = float(np.linalg.norm(c["b"]))
+    x1, r1 = S.solve(b, tol=float(c["error"]) / bn, relative=True, niter=5000)
+    x2, r2 = S.solve(b, tol=float(c["error"]), relative=False, niter=5000)
+    assert r1.status == "converged" and r1.iterations == r2.iterations
+    assert torch.equal(x1, x2)  # bitwise reproducible
+    assert abs(r1.iterations - int(c["iterations"])) <= 2
+    assert r1.bnorm == pytest.approx(bn, rel=1e-14)
+
+
+def test_zero_rhs_and_breakdown(torch):
+    L = W.laplacian_2d(8)
+    A = gb.CsrMatrix.from_host(L)
+    S = gb.CgSolver(A)
+    x, r = S.solve(torch.zeros(64, dtype=torch.float64, device="cuda"), niter=10)
+    assert r.status == "converged" and r.iterations == 0
+    assert torch.count_nonzero(x).item() == 0
+    neg = W.Csr(L.nrows, L.ncols, L.rowptr, L.rowind, -L.rowval)  # negative definite
+    S2 = gb.CgSolver(gb.CsrMatrix.from_host(neg))
+    _, r2 = S2.solve(torch.ones(64, dtype=torch.float64, device="cuda"), niter=10)
+    assert r2.status == "breakdown"
+
+
+def test_full_laplacian_1024_matches_reference(torch, full_golden):
+    g = full_golden["cg_laplace_1024"]
+    L = W.laplacian_2d(g["side"])
+    b = W.rhs(L.nrows, g["seed"])
+    A = gb.CsrMatrix.from_host(L)
+    S = gb.CgSolver(A)
+    x, r = S.solve(torch.from_numpy(b).cuda(), tol=g["rtol"], relative=True, niter=g["niter"])
+    assert r.status == "converged"
+    assert abs(r.iterations - g["iterations"]) <= 2, (r.iterations, g["iterations"])
+    xs = x.cpu().numpy()
+    res = np.linalg.norm(b - L.to_scipy() @ xs) / np.linalg.norm(b)
+    assert res <= 1.5 * g["rtol"]

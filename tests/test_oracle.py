@@ -1,0 +1,93 @@
+"""The CPU oracle: the restatement (oracle/gb_oracle.c) against the reference's
+own outputs (golden fixtures generated by tests/golden/make_golden.py from
+oracle/_ref), and against the reference build itself where it is present."""
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+import pytest
+
+import oracle
+from gooseberry_b200 import workloads as W
+
+
+def test_known_answer_tridiagonal():
+    # tridiag(-1, 2, -1) * [1..5] = [0, 0, 0, 0, 6]
+    rp = np.array([0, 2, 5, 8, 11, 13], np.uint32)
+    ri = np.array([0, 1, 0, 1, 2, 1, 2, 3, 2, 3, 4, 3, 4], np.uint32)
+    rv = np.array([2, -1, -1, 2, -1, -1, 2, -1, -1, 2, -1, -1, 2], float)
+    x = np.arange(1, 6, dtype=float)
+    y = oracle.spmv(rp, ri, rv, x)
+    assert y.tolist() == [0, 0, 0, 0, 6]
+    xs, it, _ = oracle.cgd(rp, ri, rv, y, 1e-12, 100)
+    assert it == 5
+    np.testing.assert_allclose(xs, x, rtol=0, atol=1e-12)
+
+
+def test_spmv_restatement_bitwise_equals_reference(spmv_golden):
+    for name, c in spmv_golden.items():
+        if "rowptr" not in c:
+            continue
+        y64 = oracle.spmv(c["rowptr"], c["rowind"], c["rowval"], c["x"])
+        assert np.array_equal(y64, c["y64"]), name
+        y32 = oracle.spmv(c["rowptr"], c["rowind"], c["rowval"].astype(np.float32),
+                          c["x"].astype(np.float32), real="f32")
+        assert np.array_equal(y32, c["y32"]), name
+        # the row split over threads never changes a row's sum
+        y64t = oracle.spmv(c["rowptr"], c["rowind"], c["rowval"], c["x"], threads=4)
+        assert np.array_equal(y64t, c["y64"]), name
+
+
+def test_spmm_and_blocks_restatement(spmv_golden):
+    u = spmv_golden["uniform300"]
+    C = oracle.spmm(u["rowptr"], u["rowind"], u["rowval"], spmv_golden["spmm3"]["B"],
+                    bncols=3)
+    assert np.array_equal(C, spmv_golden["spmm3"]["C"])
+    bl = spmv_golden["blocks"]
+    out = bl["init"].copy()
+    oracle.spmm(u["rowptr"], u["rowind"], u["rowval"], u["x"],
+                blocks=bl["blocks_partial"], out=out)
+    assert np.array_equal(out, bl["C"])
+    # rows outside the blocks keep their previous contents
+    assert np.all(out[120:] == 7.0)
+
+
+def test_cg_restatement_bitwise_equals_reference(cg_golden):
+    for name, c in cg_golden.items():
+        x, it, _ = oracle.cgd(c["rowptr"], c["rowind"], c["rowval"], c["b"],
+                              float(c["error"]), int(c["niter"]))
+        assert it == int(c["iterations"]), name
+        assert np.array_equal(x, c["x"]), name
+
+
+def test_full_uniform_spmv_checksum(full_golden):
+    g = full_golden["spmv_uniform_100k"]
+    A = W.uniform_rows(g["n"], g["k"], seed=g["seed"])
+    x = W.dense_x(g["n"], g["seed"])
+    y = oracle.spmv(A.rowptr, A.rowind, A.rowval, x, threads=4)
+    assert hashlib.sha256(y.tobytes()).hexdigest() == g["y_sha256"]
+
+
+@pytest.mark.skipif(not oracle.ref_available("f64"), reason="reference build absent")
+def test_reference_build_matches_restatement_random():
+    A = W.powerlaw_rows(3000, 40000, seed=99, cap=3000)
+    x = W.dense_x(3000, 99)
+    assert np.array_equal(oracle.ref_spmm(A.rowptr, A.rowind, A.rowval, x),
+                          oracle.spmv(A.rowptr, A.rowind, A.rowval, x))
+    b = W.rhs(400, 98)
+    L = W.laplacian_2d(20)
+    oracle.ref_set_threads(1)
+    xr, itr, _ = oracle.ref_cgd(L.rowptr, L.rowind, L.rowval, b, 1e-9, 500)
+    xo, ito, _ = oracle.cgd(L.rowptr, L.rowind, L.rowval, b, 1e-9, 500)
+    assert itr == ito and np.array_equal(xr, xo)
+
+
+def test_dot_scale_add_scalar():
+    a = W.dense_x(1001, 5)
+    b = W.rhs(1001, 6)
+    assert oracle.dot(a, b) == float(np.sum(a * b)) or abs(oracle.dot(a, b) - a @ b) < 1e-12
+    s = oracle.scale(a, 3.0)
+    assert np.array_equal(s, a * 3.0)
+    t = oracle.add_scalar(a, -0.5)
+    assert np.array_equal(t, a - 0.5)

@@ -1,0 +1,188 @@
+"""SpMV parity on the GPU against the reference (golden fixtures) and the
+oracle restatement.  FP64 bar: |y - y_ref| <= 1e-13 * sum_k |a_ik x_k| per row
+(the 1e-13 relative-per-row target, scaled by the row's condition so rows that
+cancel to ~0 are judged fairly).  FP32 (float values, float accumulation as in
+the reference's float build): the same form at 64 * 2^-24."""
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+import pytest
+
+import gooseberry_b200 as gb
+import oracle
+from gooseberry_b200 import workloads as W
+from conftest import cond_scaled_err
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-13
+TOL32 = 64 * 2.0 ** -24
+SCHEDS = [gb.SCHED_THREAD, gb.SCHED_GROUP4, gb.SCHED_GROUP8, gb.SCHED_WARP, gb.SCHED_MERGE]
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    assert t.cuda.is_available()
+    return t
+
+
+def _dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def test_golden_cases_all_schedules_f64(torch, spmv_golden):
+    for name, c in spmv_golden.items():
+        if "rowptr" not in c:
+            continue
+        A = gb.CsrMatrix.from_host(rowptr=c["rowptr"], rowind=c["rowind"], rowval=c["rowval"],
+                                   f64=True, f32=True)
+        x = _dev(torch, c["x"])
+        for tile in (256, 2048):
+            for s in SCHEDS:
+                A.set_schedule(s, tile_items=tile)
+                y = A.spmv(x).cpu().numpy()
+                err = cond_scaled_err(y, c["y64"], c["rowptr"], c["rowind"], c["rowval"], c["x"])
+                assert err <= TOL64, (name, s, tile, err)
+                # deterministic: a second run is bitwise identical
+                assert np.array_equal(y, A.spmv(x).cpu().numpy()), (name, s, tile)
+        A.close()
+
+
+def test_golden_cases_f32(torch, spmv_golden):
+    for name, c in spmv_golden.items():
+        if "rowptr" not in c:
+            continue
+        A = gb.CsrMatrix.from_host(rowptr=c["rowptr"], rowind=c["rowind"], rowval=c["rowval"],
+                                   f64=False, f32=True)
+        x = _dev(torch, c["x"].astype(np.float32))
+        for s in SCHEDS:
+            A.set_schedule(s, f32=True)
+            y = A.spmv(x).cpu().numpy()
+            err = cond_scaled_err(y, c["y32"], c["rowptr"], c["rowind"],
+                                  c["rowval"].astype(np.float32), c["x"].astype(np.float32))
+            assert err <= TOL32, (name, s, err)
+
+
+def test_dropin_spmult_f64_and_f32(spmv_golden):
+    for name, c in spmv_golden.items():
+        if "rowptr" not in c:
+            continue
+        y = gb.spmult(c["rowptr"], c["rowind"], c["rowval"], c["x"])
+        assert cond_scaled_err(y, c["y64"], c["rowptr"], c["rowind"], c["rowval"],
+                               c["x"]) <= TOL64, name
+        y32 = gb.spmult(c["rowptr"], c["rowind"], c["rowval"].astype(np.float32),
+                        c["x"].astype(np.float32))
+        assert y32.dtype == np.float32
+        assert cond_scaled_err(y32, c["y32"], c["rowptr"], c["rowind"],
+                               c["rowval"].astype(np.float32),
+                               c["x"].astype(np.float32)) <= TOL32, name
+
+
+def test_dropin_spmm_and_blocks(spmv_golden):
+    u = spmv_golden["uniform300"]
+    C = gb.spmult(u["rowptr"], u["rowind"], u["rowval"], spmv_golden["spmm3"]["B"], bncols=3)
+    np.testing.assert_allclose(C, spmv_golden["spmm3"]["C"], rtol=1e-13, atol=1e-13)
+    bl = spmv_golden["blocks"]
+    out = bl["init"].copy()
+    gb.spmult(u["rowptr"], u["rowind"], u["rowval"], u["x"], blocks=bl["blocks_partial"],
+              out=out)
+    np.testing.assert_allclose(out, bl["C"], rtol=1e-13, atol=1e-13)
+    assert np.all(out[120:] == 7.0)
+    # nblocks == 0 computes nothing (the reference's cgd -R case)
+    out2 = bl["init"].copy()
+    gb.spmult(u["rowptr"], u["rowind"], u["rowval"], u["x"], blocks=np.zeros(1, np.uint32),
+              out=out2)
+    assert np.all(out2 == 7.0)
+
+
+def test_full_uniform_100k(torch, full_golden):
+    g = full_golden["spmv_uniform_100k"]
+    A = W.uniform_rows(g["n"], g["k"], seed=g["seed"])
+    x = W.dense_x(g["n"], g["seed"])
+    y_ref = oracle.spmv(A.rowptr, A.rowind, A.rowval, x, threads=8)
+    assert hashlib.sha256(y_ref.tobytes()).hexdigest() == g["y_sha256"]
+    M = gb.CsrMatrix.from_host(A)
+    xd = _dev(torch, x)
+    for s in SCHEDS:
+        M.set_schedule(s)
+        y = M.spmv(xd).cpu().numpy()
+        assert cond_scaled_err(y, y_ref, A.rowptr, A.rowind, A.rowval, x) <= TOL64, s
+    M.autotune()
+    y = M.spmv(xd).cpu().numpy()
+    assert cond_scaled_err(y, y_ref, A.rowptr, A.rowind, A.rowval, x) <= TOL64
+    y2 = gb.spmult(A.rowptr, A.rowind, A.rowval, x)
+    assert cond_scaled_err(y2, y_ref, A.rowptr, A.rowind, A.rowval, x) <= TOL64
+
+
+def test_powerlaw_long_rows(torch):
+    # rows up to 200k nonzeros: many chunked long rows
+    A = W.powerlaw_rows(400_000, 6_400_000, seed=31, cap=200_000)
+    x = W.dense_x(A.ncols, 31)
+    y_ref = oracle.spmv(A.rowptr, A.rowind, A.rowval, x, threads=8)
+    M = gb.CsrMatrix.from_host(A, f64=True, f32=True)
+    assert M.info().nlong > 0
+    xd = _dev(torch, x)
+    for s in (gb.SCHED_MERGE, gb.SCHED_GROUP8, gb.SCHED_THREAD):
+        M.set_schedule(s)
+        y = M.spmv(xd).cpu().numpy()
+        assert cond_scaled_err(y, y_ref, A.rowptr, A.rowind, A.rowval, x) <= TOL64, s
+        assert np.array_equal(y, M.spmv(xd).cpu().numpy())
+    y32_ref = oracle.spmv(A.rowptr, A.rowind, A.rowval.astype(np.float32),
+                          x.astype(np.float32), threads=8, real="f32")
+    y32 = M.spmv(_dev(torch, x.astype(np.float32))).cpu().numpy()
+    assert cond_scaled_err(y32, y32_ref, A.rowptr, A.rowind, A.rowval.astype(np.float32),
+                           x.astype(np.float32)) <= TOL32
+
+
+def test_device_pointer_matrix(torch):
+    A = W.uniform_rows(3000, 7, seed=41)
+    x = W.dense_x(3000, 41)
+    rp = _dev(torch, A.rowptr.view(np.int32))
+    ri = _dev(torch, A.rowind.view(np.int32))
+    v = _dev(torch, A.rowval)
+    M = gb.CsrMatrix.from_device(rp, ri, val64=v)
+    y = M.spmv(_dev(torch, x)).cpu().numpy()
+    y_ref = oracle.spmv(A.rowptr, A.rowind, A.rowval, x)
+    assert cond_scaled_err(y, y_ref, A.rowptr, A.rowind, A.rowval, x) <= TOL64
+
+
+def test_empty_and_degenerate(torch):
+    # all rows empty: y = 0
+    rp = np.zeros(101, np.uint32)
+    M = gb.CsrMatrix.from_host(rowptr=rp, rowind=np.zeros(0, np.uint32),
+                               rowval=np.zeros(0), ncols=100)
+    y = M.spmv(torch.ones(100, dtype=torch.float64, device="cuda"))
+    assert torch.count_nonzero(y).item() == 0
+    # zero rows: nothing to do
+    y = gb.spmult(np.zeros(1, np.uint32), np.zeros(0, np.uint32), np.zeros(0), np.zeros(4),
+                  ncols=4)
+    assert y.size == 0
+
+
+def test_invalid_input_is_rejected_before_any_kernel():
+    rp = np.array([0, 2, 3], np.uint32)
+    ri = np.array([0, 5, 1], np.uint32)  # column 5 of a 2-column matrix
+    with pytest.raises(gb.GooseberryError) as e:
+        gb.spmult(rp, ri, np.ones(3), np.ones(2), ncols=2)
+    assert e.value.code == 3 and "out of range" in str(e.value)
+    with pytest.raises(gb.GooseberryError):
+        gb.spmult(np.array([0, 2, 1], np.uint32), ri, np.ones(3), np.ones(2), ncols=2)
+
+
+def test_blas1_device(torch):
+    a = _dev(torch, W.dense_x(100_003, 1))
+    b = _dev(torch, W.rhs(100_003, 2))
+    ref = float(np.dot(a.cpu().numpy(), b.cpu().numpy()))
+    assert abs(gb.dot(a, b) - ref) <= 1e-12 * float(torch.sum(torch.abs(a * b)))
+    assert gb.dot(a, b) == gb.dot(a, b)
+    v = np.arange(10, dtype=np.float64)
+    gb.scale(v, 2.5)
+    assert np.array_equal(v, np.arange(10) * 2.5)
+    gb.add_scalar(v, 1.0)
+    assert np.array_equal(v, np.arange(10) * 2.5 + 1.0)
+    w = np.arange(10, dtype=np.float32)
+    gb.scale(w, 0.5)
+    assert np.array_equal(w, np.arange(10, dtype=np.float32) * np.float32(0.5))
