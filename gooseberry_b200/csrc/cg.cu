@@ -69,10 +69,35 @@ struct CgStatus {
 
 constexpr int kVecBlock = 256;
 
+// Programmatic dependent launch: a kernel lets the next one in the stream be
+// scheduled as soon as its own CTAs start retiring, and waits for the
+// previous kernel's completion (and memory) before touching any data.
+__device__ __forceinline__ void pdl_wait_and_release() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_k(void (*k)(KArgs...), unsigned grid, unsigned block, size_t smem,
+    cudaStream_t s, bool pdl, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...);
+}
+
 // Returns true in thread 0 of the last CTA to arrive (ticket pattern).
 __device__ __forceinline__ bool arrive_last(unsigned int * ticket, bool * flag) {
-  __threadfence();
+  __syncthreads();  // every thread's writes of this CTA precede thread 0's fence
   if (threadIdx.x == 0) {
+    __threadfence();
     const unsigned prev = atomicAdd(ticket, 1u);
     *flag = (prev == gridDim.x - 1);
   }
@@ -126,6 +151,16 @@ struct OutCgA {
     pnew[i] = pn;
     longdot[lid] = pn * v;
   }
+  struct Pre {
+    double r, pold;
+  };
+  __device__ __forceinline__ Pre pre(uint32_t i) const { return Pre{r[i], pold[i]}; }
+  __device__ __forceinline__ void row_pre(uint32_t i, double v, const Pre & q) {
+    ap[i] = v;
+    const double pn = fma(beta, q.pold, q.r);
+    pnew[i] = pn;
+    local += pn * v;
+  }
   __device__ __forceinline__ void finish() {
     __shared__ double red[32];
     __shared__ bool last;
@@ -151,24 +186,28 @@ struct OutCgA {
 };
 
 template <int SCHED>
-__global__ void __launch_bounds__(kSpmvBlock) cg_a_kernel(const PlanView plan,
+__global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_a_kernel(const PlanView plan,
     const uint32_t * __restrict__ rowptr, const uint32_t * __restrict__ rowind,
     const double * __restrict__ val, const double * __restrict__ r,
     const double * __restrict__ pold, double * __restrict__ pnew,
     double * __restrict__ ap, double * __restrict__ longdot,
     double * __restrict__ partial, CgState * st) {
+  pdl_wait_and_release();
   if (*reinterpret_cast<volatile int *>(&st->done)) return;
   const double beta = st->beta;
   GatherP g{r, pold, beta};
-  OutCgA o{ap, pnew, r, pold, longdot, partial, st, beta, plan.nlong, 0.0};
+  // the row schedule finishes long rows through row() like any other row
+  OutCgA o{ap, pnew, r, pold, longdot, partial, st, beta,
+           SCHED == SCHED_ROW ? 0u : plan.nlong, 0.0};
   spmv_tiles_body<double, double, SCHED, kSpmvBlock>(plan, rowptr, rowind, val, g, o);
 }
 
 // ---- B: x / r update and r.r ----------------------------------------------------
 
-__global__ void __launch_bounds__(kVecBlock) cg_b_kernel(size_t n,
+__global__ void __launch_bounds__(kVecBlock, kSpmvMinBlocks) cg_b_kernel(size_t n,
     double * __restrict__ x, double * __restrict__ r, const double * __restrict__ p,
     const double * __restrict__ ap, double * __restrict__ partial, CgState * st) {
+  pdl_wait_and_release();
   if (*reinterpret_cast<volatile int *>(&st->done)) return;
   __shared__ double red[32];
   __shared__ bool last;
@@ -181,27 +220,43 @@ __global__ void __launch_bounds__(kVecBlock) cg_b_kernel(size_t n,
   const size_t ue = us + q + (b < rem ? 1 : 0);
   double acc = 0.0;
   const size_t full = n / 2;  // complete pairs
-  for (size_t u = us + threadIdx.x; u < ue; u += kVecBlock) {
-    if (u < full) {
-      const double2 pv = reinterpret_cast<const double2 *>(p)[u];
-      const double2 av = reinterpret_cast<const double2 *>(ap)[u];
-      double2 xv = reinterpret_cast<double2 *>(x)[u];
-      double2 rv = reinterpret_cast<double2 *>(r)[u];
-      xv.x = fma(alpha, pv.x, xv.x);
-      xv.y = fma(alpha, pv.y, xv.y);
-      rv.x = fma(-alpha, av.x, rv.x);
-      rv.y = fma(-alpha, av.y, rv.y);
-      reinterpret_cast<double2 *>(x)[u] = xv;
-      reinterpret_cast<double2 *>(r)[u] = rv;
-      acc += rv.x * rv.x;
-      acc += rv.y * rv.y;
-    } else {
-      const size_t i = 2 * u;  // odd tail element
-      x[i] = fma(alpha, p[i], x[i]);
-      const double rn = fma(-alpha, ap[i], r[i]);
-      r[i] = rn;
-      acc += rn * rn;
+  const size_t ve = min(ue, full);
+  // all loads of a batch are issued before any arithmetic (memory-level
+  // parallelism: one round trip per batch)
+  constexpr int U = 2;
+  for (size_t base = us; base < ve; base += U * kVecBlock) {
+    double2 pv[U], av[U], xv[U], rv[U];
+#pragma unroll
+    for (int j = 0; j < U; ++j) {
+      const size_t u = base + threadIdx.x + j * kVecBlock;
+      if (u < ve) {
+        pv[j] = reinterpret_cast<const double2 *>(p)[u];
+        av[j] = reinterpret_cast<const double2 *>(ap)[u];
+        xv[j] = reinterpret_cast<const double2 *>(x)[u];
+        rv[j] = reinterpret_cast<const double2 *>(r)[u];
+      }
     }
+#pragma unroll
+    for (int j = 0; j < U; ++j) {
+      const size_t u = base + threadIdx.x + j * kVecBlock;
+      if (u < ve) {
+        xv[j].x = fma(alpha, pv[j].x, xv[j].x);
+        xv[j].y = fma(alpha, pv[j].y, xv[j].y);
+        rv[j].x = fma(-alpha, av[j].x, rv[j].x);
+        rv[j].y = fma(-alpha, av[j].y, rv[j].y);
+        reinterpret_cast<double2 *>(x)[u] = xv[j];
+        reinterpret_cast<double2 *>(r)[u] = rv[j];
+        acc += rv[j].x * rv[j].x;
+        acc += rv[j].y * rv[j].y;
+      }
+    }
+  }
+  if (ue > full && threadIdx.x == 0) {  // odd n: the last element
+    const size_t i = 2 * full;
+    x[i] = fma(alpha, p[i], x[i]);
+    const double rn = fma(-alpha, ap[i], r[i]);
+    r[i] = rn;
+    acc += rn * rn;
   }
   const double s = block_sum(acc, red);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
@@ -278,35 +333,47 @@ __global__ void __launch_bounds__(kVecBlock) cg_init_kernel(size_t n,
   }
 }
 
+// dynamic shared memory of the SpMV phase (the row schedule stages nothing)
+size_t spmv_smem(int sched, uint32_t tile_items) {
+  return sched == GB_SCHED_ROW ? 0 : TileSmem<double, double>::bytes(tile_items);
+}
+
 template <int SCHED>
 int launch_cg_a_t(const gb_csr & a, const double * r, const double * pold, double * pnew,
     double * ap, double * longdot, double * partial, CgState * st, unsigned grid,
-    cudaStream_t s) {
-  const size_t smem = TileSmem<double>::bytes(a.plan.tile_items);
+    cudaStream_t s, bool pdl) {
+  const size_t smem = spmv_smem(SCHED, a.plan.tile_items);
   auto kern = cg_a_kernel<SCHED>;
   if (smem > 48 * 1024)
     GB_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void *>(kern),
         cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-  kern<<<grid, kSpmvBlock, smem, s>>>(plan_view(a), a.rowptr, a.rowind, a.val64, r, pold,
-      pnew, ap, longdot, partial, st);
-  GB_CUDA_TRY(cudaGetLastError());
+  GB_CUDA_TRY(launch_k(kern, grid, kSpmvBlock, smem, s, pdl, plan_view(a), a.rowptr,
+      a.rowind, a.val64, r, pold, pnew, ap, longdot, partial, st));
   return GOOSEBERRY_SUCCESS;
 }
 
 int launch_cg_a(const gb_csr & a, int sched, const double * r, const double * pold,
     double * pnew, double * ap, double * longdot, double * partial, CgState * st,
-    unsigned grid, cudaStream_t s) {
+    unsigned grid, cudaStream_t s, bool pdl) {
   switch (sched) {
     case GB_SCHED_THREAD:
-      return launch_cg_a_t<SCHED_THREAD>(a, r, pold, pnew, ap, longdot, partial, st, grid, s);
+      return launch_cg_a_t<SCHED_THREAD>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
+          pdl);
     case GB_SCHED_GROUP4:
-      return launch_cg_a_t<SCHED_GROUP4>(a, r, pold, pnew, ap, longdot, partial, st, grid, s);
+      return launch_cg_a_t<SCHED_GROUP4>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
+          pdl);
     case GB_SCHED_GROUP8:
-      return launch_cg_a_t<SCHED_GROUP8>(a, r, pold, pnew, ap, longdot, partial, st, grid, s);
+      return launch_cg_a_t<SCHED_GROUP8>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
+          pdl);
     case GB_SCHED_WARP:
-      return launch_cg_a_t<SCHED_WARP>(a, r, pold, pnew, ap, longdot, partial, st, grid, s);
+      return launch_cg_a_t<SCHED_WARP>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
+          pdl);
+    case GB_SCHED_ROW:
+      return launch_cg_a_t<SCHED_ROW>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
+          pdl);
     default:
-      return launch_cg_a_t<SCHED_MERGE>(a, r, pold, pnew, ap, longdot, partial, st, grid, s);
+      return launch_cg_a_t<SCHED_MERGE>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
+          pdl);
   }
 }
 
@@ -326,7 +393,284 @@ int occupancy_cg_a_sched(int sched, size_t smem, int * out) {
     case GB_SCHED_GROUP4: return occupancy_cg_a<SCHED_GROUP4>(smem, out);
     case GB_SCHED_GROUP8: return occupancy_cg_a<SCHED_GROUP8>(smem, out);
     case GB_SCHED_WARP: return occupancy_cg_a<SCHED_WARP>(smem, out);
+    case GB_SCHED_ROW: return occupancy_cg_a<SCHED_ROW>(smem, out);
     default: return occupancy_cg_a<SCHED_MERGE>(smem, out);
+  }
+}
+
+// ---- persistent solve: the whole CG in one cooperative launch -------------------
+//
+// Every CTA owns a contiguous run of tiles (and so a contiguous run of rows)
+// for the whole solve.  Per iteration:
+//   phase A  SpMV of its tiles with the fused direction update, p.Ap partial
+//   barrier  every CTA then sums the G partials itself, in CTA order, so all
+//            CTAs hold the same alpha without a serial last-CTA step
+//   phase B  x += alpha p, r -= alpha Ap on its own rows, r.r partial
+//   barrier  every CTA sums r.r, forms beta and takes the same stop decision
+// Vectors that other CTAs write during the launch (r, p) are read through L2
+// (ld.global.cg), never the read-only path.  Barriers wait on a global
+// counter with a 2 s limit; on time-out the CTA raises `abort`, every waiting
+// CTA leaves, and the solve reports GB_CG_NONFINITE with rnorm = NaN.
+
+constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned * p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ double ld_cg(const double * p, uint64_t pol) {
+  double v;
+  asm volatile("ld.global.cg.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+  return v;
+}
+
+// Grid barrier number `epoch` (1, 2, ...): returns false if it was abandoned.
+__device__ __forceinline__ bool grid_barrier(unsigned * counter, int * abort_flag,
+    unsigned epoch, int * ok_smem) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(counter, 1u);
+    const unsigned target = epoch * gridDim.x;
+    const unsigned long long t0 = global_ns();
+    int ok = 1;
+    unsigned polls = 0;
+    while (ld_acquire_u32(counter) < target) {
+      if (*reinterpret_cast<volatile int *>(abort_flag)) { ok = 0; break; }
+      if (++polls > 64) {
+        __nanosleep(64);
+        if (global_ns() - t0 > kBarrierTimeoutNs) {
+          atomicExch(abort_flag, 1);
+          ok = 0;
+          break;
+        }
+      }
+    }
+    __threadfence();
+    *ok_smem = ok;
+  }
+  __syncthreads();
+  return *ok_smem != 0;
+}
+
+// Sum of partial[0..n) in index order, identical in every CTA; all threads
+// receive the result.
+__device__ __forceinline__ double ordered_allsum(const double * partial, unsigned n,
+    double * red, double * bcast) {
+  const unsigned per = (n + blockDim.x - 1) / blockDim.x;
+  const unsigned s = min(n, threadIdx.x * per), e = min(n, s + per);
+  double acc = 0.0;
+  for (unsigned i = s; i < e; ++i) acc += __ldcg(partial + i);
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) *bcast = acc;
+  __syncthreads();
+  return *bcast;
+}
+
+struct GatherPcg {
+  const double * r;
+  const double * pold;
+  double beta;
+  __device__ __forceinline__ double operator()(uint32_t c, uint64_t pol) const {
+    return fma(beta, ld_cg(pold + c, pol), ld_cg(r + c, pol));
+  }
+};
+
+struct OutPersistA {
+  double * ap;
+  double * pnew;
+  const double * r;
+  const double * pold;
+  double beta;
+  double local;
+  __device__ __forceinline__ void row(uint32_t i, double v) {
+    ap[i] = v;
+    const double pn = fma(beta, __ldcg(pold + i), __ldcg(r + i));
+    pnew[i] = pn;
+    local += pn * v;
+  }
+  __device__ __forceinline__ void long_row(uint32_t, uint32_t i, double v) { row(i, v); }
+  __device__ __forceinline__ void finish() {}
+  struct Pre {
+    double r, pold;
+  };
+  __device__ __forceinline__ Pre pre(uint32_t i) const {
+    return Pre{__ldcg(r + i), __ldcg(pold + i)};
+  }
+  __device__ __forceinline__ void row_pre(uint32_t i, double v, const Pre & q) {
+    ap[i] = v;
+    const double pn = fma(beta, q.pold, q.r);
+    pnew[i] = pn;
+    local += pn * v;
+  }
+};
+
+struct PersistArgs {
+  PlanView plan;
+  const uint32_t * rowptr;
+  const uint32_t * rowind;
+  const double * val;
+  const double * b;
+  double * x;
+  double * r;
+  double * p0;
+  double * p1;
+  double * ap;
+  double * partial_a;
+  double * partial_b;
+  const uint32_t * cta_tiles;  // [G + 1]
+  unsigned * sync;
+  int * abort_flag;
+  CgState * st;
+  int tol_relative;
+  int keep_matrix_in_l2;
+};
+
+template <int SCHED>
+__global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_persistent_kernel(const PersistArgs a) {
+  __shared__ double red[32];
+  __shared__ double bcast;
+  __shared__ int ok_smem;
+  const unsigned G = gridDim.x, cta = blockIdx.x;
+  const int tid = threadIdx.x;
+  const uint32_t t0 = a.cta_tiles[cta], t1 = a.cta_tiles[cta + 1];
+  uint32_t lo = 0, hi = 0;
+  if (t0 < t1) {
+    lo = a.plan.tiles[t0].row_begin;
+    const TileDesc last = a.plan.tiles[t1 - 1];
+    hi = last.row_begin + last.row_count;
+  }
+  const uint64_t pol_x = policy_evict_last();
+  const uint64_t pol_m = a.keep_matrix_in_l2 ? policy_evict_last() : policy_evict_first();
+  const double tol_in = a.st->tol;
+  const unsigned long long niter = a.st->niter;
+  double * const hist = a.st->hist;
+  const unsigned long long hist_len = a.st->hist_len;
+
+  // phase 0: x = 0, r = b, p = 0, rr = b.b
+  double acc = 0.0;
+  for (uint32_t i = lo + tid; i < hi; i += kSpmvBlock) {
+    const double bv = a.b[i];
+    a.x[i] = 0.0;
+    a.r[i] = bv;
+    a.p0[i] = 0.0;
+    acc += bv * bv;
+  }
+  acc = block_sum(acc, red);
+  if (tid == 0) a.partial_b[cta] = acc;
+  unsigned epoch = 0;
+  int status = GB_CG_MAXITER;
+  unsigned long long it = 0;
+  double rr = 0.0, bnorm = 0.0, tol = tol_in, beta = 0.0;
+  bool aborted = false;
+  if (!grid_barrier(a.sync, a.abort_flag, ++epoch, &ok_smem)) {
+    aborted = true;
+  } else {
+    rr = ordered_allsum(a.partial_b, G, red, &bcast);
+    bnorm = sqrt(rr);
+    if (a.tol_relative) tol = tol_in * bnorm;
+    if (rr == 0.0) status = GB_CG_CONVERGED;
+    else if (!(rr == rr) || isinf(rr)) status = GB_CG_NONFINITE;
+    bool running = (rr != 0.0) && (rr == rr) && !isinf(rr);
+    while (running) {
+      double * pold = (it & 1) ? a.p1 : a.p0;
+      double * pnew = (it & 1) ? a.p0 : a.p1;
+      // phase A
+      GatherPcg g{a.r, pold, beta};
+      OutPersistA o{a.ap, pnew, a.r, pold, beta, 0.0};
+      if (SCHED == SCHED_ROW)
+        spmv_row_loop<double, double>(lo + tid, hi, kSpmvBlock, a.plan.ncols, a.rowptr,
+            a.rowind, a.val, g, o, pol_m, pol_x);
+      else
+        spmv_tile_loop<double, double, SCHED, kSpmvBlock>(a.plan, t0, t1, 1, a.rowptr,
+            a.rowind, a.val, g, o, pol_m, pol_x);
+      double s = block_sum(o.local, red);
+      if (tid == 0) a.partial_a[cta] = s;
+      if (!grid_barrier(a.sync, a.abort_flag, ++epoch, &ok_smem)) { aborted = true; break; }
+      const double pap = ordered_allsum(a.partial_a, G, red, &bcast);
+      if (!(pap > 0.0)) {
+        status = (pap == pap && rr == rr) ? GB_CG_BREAKDOWN : GB_CG_NONFINITE;
+        break;
+      }
+      const double alpha = rr / pap;
+      // phase B
+      acc = 0.0;
+      constexpr int U = 4;
+      for (uint32_t base = lo; base < hi; base += U * kSpmvBlock) {
+        double pv[U], av[U], xv[U], rv[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+          const uint32_t i = base + tid + j * kSpmvBlock;
+          if (i < hi) {
+            pv[j] = __ldcg(pnew + i);
+            av[j] = __ldcg(a.ap + i);
+            xv[j] = __ldcg(a.x + i);
+            rv[j] = __ldcg(a.r + i);
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+          const uint32_t i = base + tid + j * kSpmvBlock;
+          if (i < hi) {
+            a.x[i] = fma(alpha, pv[j], xv[j]);
+            const double rn = fma(-alpha, av[j], rv[j]);
+            a.r[i] = rn;
+            acc += rn * rn;
+          }
+        }
+      }
+      s = block_sum(acc, red);
+      if (tid == 0) a.partial_b[cta] = s;
+      if (!grid_barrier(a.sync, a.abort_flag, ++epoch, &ok_smem)) { aborted = true; break; }
+      const double rr_new = ordered_allsum(a.partial_b, G, red, &bcast);
+      beta = rr_new / rr;
+      rr = rr_new;
+      ++it;
+      const double rnorm = sqrt(rr);
+      if (cta == 0 && tid == 0 && hist && it <= hist_len) hist[it - 1] = rnorm;
+      if (!(rnorm == rnorm) || isinf(rnorm)) { status = GB_CG_NONFINITE; running = false; }
+      else if (rnorm <= tol) { status = GB_CG_CONVERGED; running = false; }
+      else if (niter && it >= niter) { status = GB_CG_MAXITER; running = false; }
+    }
+  }
+  if (cta == 0 && tid == 0) {
+    CgState * st = a.st;
+    st->iter = it;
+    st->rr = aborted ? __longlong_as_double(0x7ff8000000000000ll) : rr;
+    st->bnorm = bnorm;
+    st->tol = tol;
+    st->status = aborted ? GB_CG_NONFINITE : status;
+    st->done = 1;
+  }
+}
+
+template <int SCHED>
+int persistent_setup_t(size_t smem, int * occ, const void ** fn) {
+  auto kern = cg_persistent_kernel<SCHED>;
+  *fn = reinterpret_cast<const void *>(kern);
+  if (smem > 48 * 1024)
+    GB_CUDA_TRY(cudaFuncSetAttribute(*fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        static_cast<int>(smem)));
+  GB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, kSpmvBlock, smem));
+  return GOOSEBERRY_SUCCESS;
+}
+
+int persistent_setup(int sched, size_t smem, int * occ, const void ** fn) {
+  switch (sched) {
+    case GB_SCHED_THREAD: return persistent_setup_t<SCHED_THREAD>(smem, occ, fn);
+    case GB_SCHED_GROUP4: return persistent_setup_t<SCHED_GROUP4>(smem, occ, fn);
+    case GB_SCHED_GROUP8: return persistent_setup_t<SCHED_GROUP8>(smem, occ, fn);
+    case GB_SCHED_WARP: return persistent_setup_t<SCHED_WARP>(smem, occ, fn);
+    case GB_SCHED_ROW: return persistent_setup_t<SCHED_ROW>(smem, occ, fn);
+    default: return persistent_setup_t<SCHED_MERGE>(smem, occ, fn);
   }
 }
 
@@ -356,6 +700,14 @@ struct gb_cg {
   int chunk = 32;  // iterations per graph (even)
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // status into slot 0 / slot 1
+  // persistent (one cooperative launch per solve) mode
+  bool persistent = false;
+  unsigned grid_p = 0;
+  size_t smem_p = 0;
+  const void * fn_p = nullptr;
+  uint32_t * cta_tiles = nullptr;
+  unsigned * sync = nullptr;  // [0] barrier counter, [1] abort flag
+  int keep_l2 = 0;
 };
 
 namespace gb {
@@ -376,6 +728,8 @@ void destroy_cg(gb_cg * s) {
   cudaFree(s->partial_i);
   cudaFree(s->longdot);
   cudaFree(s->st);
+  cudaFree(s->cta_tiles);
+  cudaFree(s->sync);
   if (s->host_status) cudaFreeHost(s->host_status);
   delete s;
 }
@@ -388,11 +742,12 @@ int capture_chunk(gb_cg * s, int slot) {
     const double * pold = s->p[k & 1];
     double * pnew = s->p[(k + 1) & 1];
     rc = launch_cg_a(*s->a, s->sched, s->r, pold, pnew, s->ap, s->longdot, s->partial_a,
-        s->st, s->grid_a, cs);
+        s->st, s->grid_a, cs, k > 0);
     if (rc != GOOSEBERRY_SUCCESS) break;
-    cg_b_kernel<<<s->grid_b, kVecBlock, 0, cs>>>(s->n, s->x, s->r, pnew, s->ap,
-        s->partial_b, s->st);
-    if (cudaGetLastError() != cudaSuccess) rc = GOOSEBERRY_ERROR_UNKNOWN;
+    if (launch_k(cg_b_kernel, s->grid_b, kVecBlock, 0, cs, true, s->n, s->x, s->r,
+            static_cast<const double *>(pnew), static_cast<const double *>(s->ap),
+            s->partial_b, s->st) != cudaSuccess)
+      rc = GOOSEBERRY_ERROR_UNKNOWN;
   }
   if (rc == GOOSEBERRY_SUCCESS) {
     // status mirror: done, status, iter, rr, bnorm
@@ -421,9 +776,82 @@ int capture_chunk(gb_cg * s, int slot) {
   return GOOSEBERRY_SUCCESS;
 }
 
+// One cooperative launch per solve when every row fits a tile (no long rows)
+// and all CTAs of the grid can be resident at once.  Tiles are dealt to CTAs
+// in contiguous runs of nearly equal rows + nonzeros.
+int setup_persistent(const gb_csr * a, gb_cg * s) {
+  int dev = 0, coop = 0;
+  GB_CUDA_TRY(cudaGetDevice(&dev));
+  GB_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+  const size_t ntiles = a->plan.tiles.size();
+  if (!coop || !a->plan.longrows.empty() || ntiles == 0) return GOOSEBERRY_SUCCESS;
+  s->smem_p = spmv_smem(s->sched, a->plan.tile_items);
+  int occ = 0;
+  GB_TRY(persistent_setup(s->sched, s->smem_p, &occ, &s->fn_p));
+  if (occ < 1) return GOOSEBERRY_SUCCESS;
+  const unsigned G = static_cast<unsigned>(std::min<size_t>(ntiles,
+      static_cast<size_t>(a->sm_count) * occ));
+  std::vector<uint64_t> cum(ntiles + 1, 0);
+  for (size_t t = 0; t < ntiles; ++t)
+    cum[t + 1] = cum[t] + a->plan.tiles[t].row_count + a->plan.tiles[t].nnz_count;
+  std::vector<uint32_t> bounds(G + 1, 0);
+  size_t t = 0;
+  for (unsigned g = 1; g < G; ++g) {
+    const uint64_t want = cum[ntiles] * g / G;
+    while (t < ntiles && cum[t] < want) ++t;
+    bounds[g] = static_cast<uint32_t>(std::max<size_t>(t, bounds[g - 1]));
+  }
+  bounds[G] = static_cast<uint32_t>(ntiles);
+  GB_CUDA_TRY(cudaMalloc(&s->cta_tiles, (G + 1) * sizeof(uint32_t)));
+  GB_CUDA_TRY(cudaMemcpy(s->cta_tiles, bounds.data(), (G + 1) * sizeof(uint32_t),
+      cudaMemcpyHostToDevice));
+  GB_CUDA_TRY(cudaMalloc(&s->sync, 2 * sizeof(unsigned)));
+  // the matrix stays L2-resident across iterations when the working set of
+  // one iteration fits in about 3/4 of L2
+  int l2 = 0;
+  GB_CUDA_TRY(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev));
+  const double ws = 4.0 * (a->nrows + 1) + 12.0 * a->nnz + 40.0 * a->nrows;
+#ifndef GB_L2_KEEP_FRACTION
+#define GB_L2_KEEP_FRACTION 0.75
+#endif
+  s->keep_l2 = ws <= GB_L2_KEEP_FRACTION * l2 ? 1 : 0;
+  s->grid_p = G;
+  s->persistent = true;
+  return GOOSEBERRY_SUCCESS;
+}
+
+int launch_persistent(gb_cg * s, const double * b, int tol_relative, cudaStream_t stream) {
+  GB_CUDA_TRY(cudaMemsetAsync(s->sync, 0, 2 * sizeof(unsigned), stream));
+  PersistArgs args;
+  args.plan = plan_view(*s->a);
+  args.rowptr = s->a->rowptr;
+  args.rowind = s->a->rowind;
+  args.val = s->a->val64;
+  args.b = b;
+  args.x = s->x;
+  args.r = s->r;
+  args.p0 = s->p[0];
+  args.p1 = s->p[1];
+  args.ap = s->ap;
+  args.partial_a = s->partial_a;
+  args.partial_b = s->partial_b;
+  args.cta_tiles = s->cta_tiles;
+  args.sync = s->sync;
+  args.abort_flag = reinterpret_cast<int *>(s->sync + 1);
+  args.st = s->st;
+  args.tol_relative = tol_relative;
+  args.keep_matrix_in_l2 = s->keep_l2;
+  void * kargs[] = {&args};
+  GB_CUDA_TRY(cudaLaunchCooperativeKernel(s->fn_p, dim3(s->grid_p), dim3(kSpmvBlock), kargs,
+      s->smem_p, stream));
+  return GOOSEBERRY_SUCCESS;
+}
+
 int create_cg(const gb_csr * a, int mode, gb_cg * s) {
   GB_CHECK_INPUT(a->nrows == a->ncols, "CG needs a square matrix, got %ux%u", a->nrows,
       a->ncols);
+  const bool want_persistent = (mode & GB_CG_PERSISTENT) != 0;
+  mode &= ~GB_CG_PERSISTENT;
   GB_CHECK_INPUT(mode == GB_CG_F64, "CG mode %d is not available", mode);
   GB_CHECK_INPUT(a->val64 != nullptr, "CG (FP64) needs double values on the matrix");
   s->a = a;
@@ -437,16 +865,25 @@ int create_cg(const gb_csr * a, int mode, gb_cg * s) {
   GB_CUDA_TRY(cudaMalloc(&s->ap, n * sizeof(double)));
   s->sched = a->sched64;
   s->tile_items = a->plan.tile_items;
-  const size_t smem = TileSmem<double>::bytes(a->plan.tile_items);
+  const size_t smem = spmv_smem(s->sched, a->plan.tile_items);
   int occ = 0;
   GB_TRY(occupancy_cg_a_sched(s->sched, smem, &occ));
   GB_CHECK_INPUT(occ > 0, "CG kernel cannot be resident");
   const unsigned ntiles = static_cast<unsigned>(std::max<size_t>(a->plan.tiles.size(), 1));
-  s->grid_a = std::min<unsigned>(ntiles, static_cast<unsigned>(a->sm_count * occ));
+  const unsigned work_a = s->sched == GB_SCHED_ROW
+      ? static_cast<unsigned>((s->n + kSpmvBlock - 1) / kSpmvBlock) : ntiles;
+  s->grid_a = std::min<unsigned>(std::max(work_a, 1u),
+      static_cast<unsigned>(a->sm_count * occ));
   const size_t units = (s->n + 1) / 2;
+  // vector kernels: one resident wave, each CTA streaming a contiguous chunk
+  int occ_b = 0;
+  GB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, cg_b_kernel, kVecBlock, 0));
   s->grid_b = static_cast<unsigned>(std::max<size_t>(1, std::min<size_t>(
-      (units + kVecBlock * 2 - 1) / (kVecBlock * 2), static_cast<size_t>(a->sm_count) * 8)));
-  const unsigned gmax = std::max(s->grid_a, s->grid_b);
+      (units + kVecBlock - 1) / kVecBlock,
+      static_cast<size_t>(a->sm_count) * std::max(occ_b, 1))));
+  const unsigned gmax = std::max<unsigned>(std::max(s->grid_a, s->grid_b),
+      static_cast<unsigned>(std::min<size_t>(a->plan.tiles.size() + 1,
+          static_cast<size_t>(a->sm_count) * 32)));
   GB_CUDA_TRY(cudaMalloc(&s->partial_a, gmax * sizeof(double)));
   GB_CUDA_TRY(cudaMalloc(&s->partial_b, gmax * sizeof(double)));
   GB_CUDA_TRY(cudaMalloc(&s->partial_i, gmax * sizeof(double)));
@@ -455,9 +892,12 @@ int create_cg(const gb_csr * a, int mode, gb_cg * s) {
   GB_CUDA_TRY(cudaMalloc(&s->st, sizeof(CgState)));
   GB_CUDA_TRY(cudaMemset(s->st, 0, sizeof(CgState)));
   GB_CUDA_TRY(cudaMallocHost(&s->host_status, 2 * sizeof(CgStatus)));
-  GB_CUDA_TRY(cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking));
-  GB_TRY(capture_chunk(s, 0));
-  GB_TRY(capture_chunk(s, 1));
+  if (want_persistent) GB_TRY(setup_persistent(a, s));
+  if (!s->persistent) {
+    GB_CUDA_TRY(cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking));
+    GB_TRY(capture_chunk(s, 0));
+    GB_TRY(capture_chunk(s, 1));
+  }
   return GOOSEBERRY_SUCCESS;
 }
 
@@ -473,6 +913,7 @@ int start_solve(gb_cg * s, const double * b, double tol, int tol_relative, size_
   init.hist = dhist;
   init.hist_len = hl;
   GB_CUDA_TRY(cudaMemcpyAsync(s->st, &init, sizeof(CgState), cudaMemcpyHostToDevice, stream));
+  if (s->persistent) return launch_persistent(s, b, tol_relative, stream);
   cg_init_kernel<<<s->grid_b, kVecBlock, 0, stream>>>(s->n, b, s->x, s->r, s->p[0],
       s->partial_i, s->st, tol_relative);
   GB_CUDA_TRY(cudaGetLastError());
@@ -512,10 +953,12 @@ int solve_cg(gb_cg * s, const double * b, double * x, double tol, int tol_relati
     }
     return GOOSEBERRY_SUCCESS;
   };
-  rc = launch(0);
-  if (rc == GOOSEBERRY_SUCCESS) rc = launch(1);
+  if (!s->persistent) {
+    rc = launch(0);
+    if (rc == GOOSEBERRY_SUCCESS) rc = launch(1);
+  }
   int slot = 0;
-  while (rc == GOOSEBERRY_SUCCESS) {
+  while (rc == GOOSEBERRY_SUCCESS && !s->persistent) {
     cudaError_t e = cudaEventSynchronize(ev[slot]);
     if (e != cudaSuccess) {
       set_error("CG solve failed: %s", cudaGetErrorString(e));
@@ -542,8 +985,14 @@ int solve_cg(gb_cg * s, const double * b, double * x, double tol, int tol_relati
       e = cudaMemcpyAsync(history, dhist, std::min<size_t>(hl, fin.iter) * sizeof(double),
           cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    unsigned flags[2] = {0, 0};
+    if (e == cudaSuccess && s->persistent)
+      e = cudaMemcpy(flags, s->sync, sizeof(flags), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) {
       set_error("CG result copy failed: %s", cudaGetErrorString(e));
+      rc = GOOSEBERRY_ERROR_UNKNOWN;
+    } else if (flags[1]) {
+      set_error("CG solve abandoned: a grid barrier timed out");
       rc = GOOSEBERRY_ERROR_UNKNOWN;
     } else if (res) {
       res->iterations = fin.iter;
@@ -562,6 +1011,25 @@ int profile_cg(gb_cg * s, const double * b, size_t iterations, double * ms, size
     size_t * nkernels, cudaStream_t stream) {
   GB_CHECK_INPUT(s->n > 0 && b != nullptr, "profile needs a non-empty system and b");
   GB_CHECK_INPUT(iterations > 0, "iterations must be positive");
+  if (s->persistent) {
+    // one launch runs every iteration: time it and report ms per iteration
+    if (nkernels) *nkernels = 1;
+    cudaEvent_t e0, e1;
+    GB_CUDA_TRY(cudaEventCreate(&e0));
+    GB_CUDA_TRY(cudaEventCreate(&e1));
+    GB_CUDA_TRY(cudaEventRecord(e0, stream));
+    int rc = start_solve(s, b, 0.0, 0, iterations, nullptr, 0, stream);
+    cudaEventRecord(e1, stream);
+    cudaError_t e = cudaEventSynchronize(e1);
+    float t = 0.f;
+    if (rc == GOOSEBERRY_SUCCESS && e == cudaSuccess) cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    GB_TRY(rc);
+    GB_CUDA_TRY(e);
+    if (ms && ms_len > 0) ms[0] = static_cast<double>(t) / iterations;
+    return GOOSEBERRY_SUCCESS;
+  }
   if (nkernels) *nkernels = 2;
   GB_TRY(start_solve(s, b, 0.0, 0, 0, nullptr, 0, stream));
   std::vector<cudaEvent_t> ev(3 * iterations);
@@ -572,7 +1040,7 @@ int profile_cg(gb_cg * s, const double * b, size_t iterations, double * ms, size
     double * pnew = s->p[(k + 1) & 1];
     cudaEventRecord(ev[3 * k], stream);
     rc = launch_cg_a(*s->a, s->sched, s->r, pold, pnew, s->ap, s->longdot, s->partial_a,
-        s->st, s->grid_a, stream);
+        s->st, s->grid_a, stream, false);
     cudaEventRecord(ev[3 * k + 1], stream);
     cg_b_kernel<<<s->grid_b, kVecBlock, 0, stream>>>(s->n, s->x, s->r, pnew, s->ap,
         s->partial_b, s->st);

@@ -78,6 +78,7 @@ struct PlanView {
   uint32_t nlong;
   uint32_t tile_items;
   uint32_t ncols;
+  uint32_t nrows;
 };
 
 struct Plan {
@@ -136,6 +137,7 @@ inline PlanView plan_view(const gb_csr & a) {
   v.nlong = static_cast<uint32_t>(a.plan.longrows.size());
   v.tile_items = a.plan.tile_items;
   v.ncols = a.ncols;
+  v.nrows = a.nrows;
   return v;
 }
 

@@ -139,7 +139,8 @@ int upload_plan(Plan & plan, cudaStream_t stream) {
 }
 
 int default_schedule(const Plan & plan) {
-  if (plan.max_row <= 12 && plan.mean_row <= 12.0) return GB_SCHED_THREAD;
+  if (plan.max_row <= 16 && plan.mean_row <= 12.0) return GB_SCHED_ROW;
+  if (plan.max_row <= 32 && plan.mean_row <= 16.0) return GB_SCHED_THREAD;
   if (plan.p99 <= 2 * plan.p50 + 8 && plan.mean_row <= 40.0) return GB_SCHED_GROUP4;
   if (plan.p99 <= 2 * plan.p50 + 8 && plan.mean_row <= 160.0) return GB_SCHED_GROUP8;
   return GB_SCHED_MERGE;
@@ -156,10 +157,14 @@ struct OutStore {
   }
   __device__ __forceinline__ void long_row(uint32_t, uint32_t r, Acc v) { row(r, v); }
   __device__ __forceinline__ void finish() {}
+  // per-row operands prefetched by the row schedule (none for a plain store)
+  struct Pre {};
+  __device__ __forceinline__ Pre pre(uint32_t) const { return Pre{}; }
+  __device__ __forceinline__ void row_pre(uint32_t r, Acc v, const Pre &) { row(r, v); }
 };
 
 template <typename V, typename Acc, int SCHED, class Gather, class Out>
-__global__ void __launch_bounds__(kSpmvBlock) spmv_tiles_kernel(const PlanView plan,
+__global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) spmv_tiles_kernel(const PlanView plan,
     const uint32_t * __restrict__ rowptr, const uint32_t * __restrict__ rowind,
     const V * __restrict__ val, const Gather gather, Out out) {
   spmv_tiles_body<V, Acc, SCHED, kSpmvBlock>(plan, rowptr, rowind, val, gather, out);
@@ -214,11 +219,13 @@ int launch_tiles(const gb_csr & a, const V * val, const Gather & g, const Out & 
     cudaStream_t stream) {
   if (a.plan.tiles.empty()) return GOOSEBERRY_SUCCESS;
   auto kern = spmv_tiles_kernel<V, Acc, SCHED, Gather, Out>;
-  const size_t smem = TileSmem<Acc>::bytes(a.plan.tile_items);
+  const size_t smem = SCHED == SCHED_ROW ? 0 : TileSmem<V, Acc>::bytes(a.plan.tile_items);
   int occ = 0;
   GB_TRY(occupancy(reinterpret_cast<const void *>(kern), smem, &occ));
-  const uint32_t ntiles = static_cast<uint32_t>(a.plan.tiles.size());
-  const uint32_t grid = std::min<uint32_t>(ntiles, static_cast<uint32_t>(a.sm_count * occ));
+  const uint32_t units = SCHED == SCHED_ROW
+      ? (a.nrows + kSpmvBlock - 1) / kSpmvBlock
+      : static_cast<uint32_t>(a.plan.tiles.size());
+  const uint32_t grid = std::min<uint32_t>(units, static_cast<uint32_t>(a.sm_count * occ));
   kern<<<grid, kSpmvBlock, smem, stream>>>(plan_view(a), a.rowptr, a.rowind, val, g, o);
   GB_CUDA_TRY(cudaGetLastError());
   return GOOSEBERRY_SUCCESS;
@@ -233,6 +240,7 @@ int launch_sched(const gb_csr & a, int sched, const V * val, const Gather & g,
     case GB_SCHED_GROUP8: return launch_tiles<V, Acc, SCHED_GROUP8>(a, val, g, o, stream);
     case GB_SCHED_WARP: return launch_tiles<V, Acc, SCHED_WARP>(a, val, g, o, stream);
     case GB_SCHED_MERGE: return launch_tiles<V, Acc, SCHED_MERGE>(a, val, g, o, stream);
+    case GB_SCHED_ROW: return launch_tiles<V, Acc, SCHED_ROW>(a, val, g, o, stream);
     default:
       set_error("unknown SpMV schedule %d", sched);
       return GOOSEBERRY_ERROR_INVALIDINPUT;
@@ -348,7 +356,7 @@ int autotune(gb_csr & a, unsigned width, cudaStream_t stream) {
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   const uint32_t tiles_opts[] = {1024, 2048, 4096};
-  const int sched_opts[] = {GB_SCHED_THREAD, GB_SCHED_GROUP4, GB_SCHED_GROUP8,
+  const int sched_opts[] = {GB_SCHED_ROW, GB_SCHED_THREAD, GB_SCHED_GROUP4, GB_SCHED_GROUP8,
                             GB_SCHED_WARP, GB_SCHED_MERGE};
   float best = 1e30f;
   TuneChoice choice{default_schedule(a.plan), a.plan.tile_items};
@@ -357,7 +365,10 @@ int autotune(gb_csr & a, unsigned width, cudaStream_t stream) {
     rc = rebuild_plan(a, ti, stream);
     if (rc != GOOSEBERRY_SUCCESS) break;
     for (int s : sched_opts) {
-      // skip schedules that cannot suit this matrix
+      // skip schedules that cannot suit this matrix (the row schedule does
+      // not use tiles: time it once)
+      if (s == GB_SCHED_ROW && (ti != tiles_opts[0] || a.plan.p99 > 64 ||
+                                a.plan.max_row > 4096)) continue;
       if (s == GB_SCHED_THREAD && a.plan.p90 > 64) continue;
       if (s == GB_SCHED_WARP && a.plan.p50 < 8) continue;
       auto run = [&]() {
@@ -566,7 +577,7 @@ int gb_csr_get_info(const gb_csr_t * a, gb_csr_info_t * info) {
 int gb_csr_set_schedule(gb_csr_t * a, unsigned value_width, int schedule,
     uint32_t tile_items) {
   GB_CHECK_INPUT(a != nullptr, "matrix is NULL");
-  GB_CHECK_INPUT(schedule >= GB_SCHED_AUTO && schedule <= GB_SCHED_MERGE,
+  GB_CHECK_INPUT(schedule >= GB_SCHED_AUTO && schedule <= GB_SCHED_ROW,
       "unknown schedule %d", schedule);
   GB_CHECK_INPUT(value_width == GB_CSR_VALUES_F64 || value_width == GB_CSR_VALUES_F32,
       "value_width must be GB_CSR_VALUES_F64 or GB_CSR_VALUES_F32");

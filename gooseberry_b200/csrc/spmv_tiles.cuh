@@ -38,10 +38,21 @@ enum : int {
   SCHED_GROUP4 = GB_SCHED_GROUP4,
   SCHED_GROUP8 = GB_SCHED_GROUP8,
   SCHED_WARP = GB_SCHED_WARP,
-  SCHED_MERGE = GB_SCHED_MERGE
+  SCHED_MERGE = GB_SCHED_MERGE,
+  SCHED_ROW = GB_SCHED_ROW
 };
 
 constexpr int kSpmvBlock = 256;
+// Elements per thread whose loads are issued together, and the resident CTAs
+// per SM the register budget is sized for (both tunable at build time).
+#ifndef GB_SPMV_STAGE
+#define GB_SPMV_STAGE 8
+#endif
+#ifndef GB_SPMV_MIN_BLOCKS
+#define GB_SPMV_MIN_BLOCKS 3
+#endif
+constexpr int kStage = GB_SPMV_STAGE;
+constexpr int kSpmvMinBlocks = GB_SPMV_MIN_BLOCKS;
 
 // ---- cache-policy loads -------------------------------------------------------
 
@@ -87,6 +98,13 @@ __device__ __forceinline__ float ld_keep(const float * p, uint64_t pol) {
   return v;
 }
 
+// Round-to-nearest multiply and add that the compiler may not contract into
+// a fused multiply-add (the reference's x86-64 build never fuses).
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+
 // ---- shuffle helpers -----------------------------------------------------------
 
 template <int G, typename T>
@@ -124,13 +142,46 @@ struct GatherPlain {
 
 // ---- the tile kernel ----------------------------------------------------------
 
-template <typename Acc>
+// Shared-memory layout of the tile pipeline: two stages, each holding one
+// tile's rowptr slice (tile_items + 1 entries), column indices and values
+// (tile_items entries each), plus one product buffer.
+template <typename V, typename Acc>
 struct TileSmem {
-  // products (tile_items entries) followed by row offsets (tile_items + 1)
-  static __host__ __device__ size_t bytes(uint32_t tile_items) {
-    return sizeof(Acc) * tile_items + sizeof(uint32_t) * (tile_items + 1) + 16;
+  static __host__ __device__ size_t stage_bytes(uint32_t t) {
+    const size_t offs = (sizeof(uint32_t) * (t + 1) + 15) & ~size_t(15);
+    const size_t ind = (sizeof(uint32_t) * t + 15) & ~size_t(15);
+    const size_t val = (sizeof(V) * t + 15) & ~size_t(15);
+    return offs + ind + val;
+  }
+  static __host__ __device__ size_t bytes(uint32_t t) {
+    return 2 * stage_bytes(t) + ((sizeof(Acc) * t + 15) & ~size_t(15));
   }
 };
+
+// cp.async (global -> shared, bypassing registers) with an L2 cache policy.
+__device__ __forceinline__ void cp_async4(void * smem, const void * gmem, uint64_t pol) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 4, %2;"
+               :: "r"(s), "l"(gmem), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void * smem, const void * gmem, uint64_t pol) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 8, %2;"
+               :: "r"(s), "l"(gmem), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void cp_async_v(void * smem, const double * g, uint64_t pol) {
+  cp_async8(smem, g, pol);
+}
+__device__ __forceinline__ void cp_async_v(void * smem, const float * g, uint64_t pol) {
+  cp_async4(smem, g, pol);
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory");
+}
 
 // Reduction of one staged tile.  `prod` holds the tile's products, `offs` the
 // R+1 row offsets into prod.  Calls out.row(row, sum) once per row.
@@ -215,47 +266,98 @@ __device__ __forceinline__ void reduce_tile(const Acc * prod, const uint32_t * o
   }
 }
 
-// The persistent tile kernel.  V: stored value type; Acc: product/accumulator
-// type; Gather: x-access functor; Out: per-row epilogue with
+// Runs the tiles t_begin, t_begin + t_step, ... (< t_end) of a plan.
+//
+// Pipeline: while tile t is gathered and reduced, cp.async is already copying
+// tile t + t_step's rowptr slice, indices and values into the other shared
+// memory stage, so the matrix stream never waits behind the reduction.  Only
+// the x gathers of the current tile are exposed latency; every thread issues
+// kStage of them before consuming any.
+//
+// V: stored value type; Acc: product/accumulator type; Gather: x-access
+// functor; Out: per-row epilogue with
 //   row(row, Acc)                -- one finished row
-//   long_row(lid, row, Acc)      -- a finished long row (single thread)
-//   finish()                     -- once per thread after the last tile
+//   long_row(lid, row, Acc)      -- a finished long row (called by one thread)
+// `pol_matrix` is the L2 policy of the matrix stream (evict-first when the
+// matrix cannot stay in L2, evict-normal/last when it can).
 template <typename V, typename Acc, int SCHED, int BLOCK, class Gather, class Out>
-__device__ __forceinline__ void spmv_tiles_body(const PlanView plan,
-    const uint32_t * __restrict__ rowptr, const uint32_t * __restrict__ rowind,
-    const V * __restrict__ val, const Gather gather, Out & out) {
+__device__ __forceinline__ void spmv_tile_loop(const PlanView & plan, uint32_t t_begin,
+    uint32_t t_end, uint32_t t_step, const uint32_t * __restrict__ rowptr,
+    const uint32_t * __restrict__ rowind, const V * __restrict__ val,
+    const Gather & gather, Out & out, uint64_t pol_matrix, uint64_t pol_x) {
   extern __shared__ __align__(16) unsigned char gb_smem[];
   __shared__ Acc scan_v[BLOCK / 32];
   __shared__ uint32_t scan_k[BLOCK / 32];
   __shared__ Acc red[32];
-  __shared__ bool last_chunk;
 
-  Acc * prod = reinterpret_cast<Acc *>(gb_smem);
-  uint32_t * offs = reinterpret_cast<uint32_t *>(prod + plan.tile_items);
-  const uint64_t pol_stream = policy_evict_first();
-  const uint64_t pol_keep = policy_evict_last();
+  const uint32_t T = plan.tile_items;
+  const size_t sb = TileSmem<V, Acc>::stage_bytes(T);
+  const size_t offs_b = (sizeof(uint32_t) * (T + 1) + 15) & ~size_t(15);
+  const size_t ind_b = (sizeof(uint32_t) * T + 15) & ~size_t(15);
+  Acc * prod = reinterpret_cast<Acc *>(gb_smem + 2 * sb);
   const uint32_t cmax = plan.ncols - 1;
   const int tid = threadIdx.x;
 
-  for (uint32_t t = blockIdx.x; t < plan.ntiles; t += gridDim.x) {
+  auto stage_offs = [&](int s) { return reinterpret_cast<uint32_t *>(gb_smem + s * sb); };
+  auto stage_ind = [&](int s) {
+    return reinterpret_cast<uint32_t *>(gb_smem + s * sb + offs_b);
+  };
+  auto stage_val = [&](int s) { return reinterpret_cast<V *>(gb_smem + s * sb + offs_b + ind_b); };
+
+  // queue the copies of tile t into stage s (chunk tiles stream from global)
+  auto issue = [&](uint32_t t, int s) {
+    const TileDesc d = plan.tiles[t];
+    if (d.row_count != 0) {
+      uint32_t * so = stage_offs(s);
+      uint32_t * si = stage_ind(s);
+      V * sv = stage_val(s);
+      for (uint32_t r = tid; r <= d.row_count; r += BLOCK)
+        cp_async4(so + r, rowptr + d.row_begin + r, pol_matrix);
+      for (uint32_t k = tid; k < d.nnz_count; k += BLOCK) {
+        cp_async4(si + k, rowind + d.nnz_begin + k, pol_matrix);
+        cp_async_v(sv + k, val + d.nnz_begin + k, pol_matrix);
+      }
+    }
+    cp_async_commit();
+  };
+
+  if (t_begin < t_end) issue(t_begin, 0);
+  int s = 0;
+  for (uint32_t t = t_begin; t < t_end; t += t_step) {
+    const uint32_t tn = t + t_step;
+    if (tn < t_end) issue(tn, s ^ 1); else cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
     const TileDesc d = plan.tiles[t];
     const uint32_t nb = d.nnz_begin;
     const int N = static_cast<int>(d.nnz_count);
     if (d.row_count == 0) {
       // ---- chunk of a long row: block tree sum, then last-arrival combine
-      Acc s = Acc(0);
-      for (int k = tid; k < N; k += BLOCK) {
-        const uint32_t c = min(ld_stream(rowind + nb + k, pol_stream), cmax);
-        s += static_cast<Acc>(ld_stream(val + nb + k, pol_stream)) * gather(c, pol_keep);
+      Acc sum = Acc(0);
+      for (int base = 0; base < N; base += kStage * BLOCK) {
+        uint32_t c[kStage];
+        V v[kStage];
+#pragma unroll
+        for (int j = 0; j < kStage; ++j) {
+          const int k = base + tid + j * BLOCK;
+          if (k < N) {
+            c[j] = ld_stream(rowind + nb + k, pol_matrix);
+            v[j] = ld_stream(val + nb + k, pol_matrix);
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < kStage; ++j) {
+          const int k = base + tid + j * BLOCK;
+          if (k < N) sum += static_cast<Acc>(v[j]) * gather(min(c[j], cmax), pol_x);
+        }
       }
-      s = block_sum(s, red);
+      sum = block_sum(sum, red);
       if (tid == 0) {
-        plan.chunk_partial[t] = static_cast<double>(s);
+        plan.chunk_partial[t] = static_cast<double>(sum);
         __threadfence();
         const LongRowDesc L = plan.longrows[d.row_begin];
         const unsigned prev = atomicAdd(plan.long_count + d.row_begin, 1u);
-        last_chunk = (prev == L.nchunks - 1);
-        if (last_chunk) {
+        if (prev == L.nchunks - 1) {
           __threadfence();
           Acc tot = Acc(0);
           for (uint32_t q = 0; q < L.nchunks; ++q)
@@ -264,40 +366,145 @@ __device__ __forceinline__ void spmv_tiles_body(const PlanView plan,
           out.long_row(d.row_begin, L.row, tot);
         }
       }
+    } else {
+      const int R = static_cast<int>(d.row_count);
+      uint32_t * offs = stage_offs(s);
+      const uint32_t * si = stage_ind(s);
+      const V * sv = stage_val(s);
+      for (int r = tid; r <= R; r += BLOCK) offs[r] -= nb;
+      // products: kStage gathers in flight per thread
+      for (int base = 0; base < N; base += kStage * BLOCK) {
+        Acc xv[kStage];
+#pragma unroll
+        for (int j = 0; j < kStage; ++j) {
+          const int k = base + tid + j * BLOCK;
+          if (k < N) xv[j] = gather(min(si[k], cmax), pol_x);
+        }
+#pragma unroll
+        for (int j = 0; j < kStage; ++j) {
+          const int k = base + tid + j * BLOCK;
+          if (k < N) prod[k] = static_cast<Acc>(sv[k]) * xv[j];
+        }
+      }
       __syncthreads();
-      continue;
+      reduce_tile<SCHED, BLOCK, Acc>(prod, offs, d.row_begin, R, N, out, scan_v, scan_k);
     }
-    const int R = static_cast<int>(d.row_count);
-    // ---- stage row offsets and products
-    for (int r = tid; r <= R; r += BLOCK) offs[r] = rowptr[d.row_begin + r] - nb;
-    const uint32_t * ip = rowind + nb;
-    const V * vp = val + nb;
-    int k = tid;
-    for (; k + 3 * BLOCK < N; k += 4 * BLOCK) {
-      const uint32_t c0 = min(ld_stream(ip + k, pol_stream), cmax);
-      const uint32_t c1 = min(ld_stream(ip + k + BLOCK, pol_stream), cmax);
-      const uint32_t c2 = min(ld_stream(ip + k + 2 * BLOCK, pol_stream), cmax);
-      const uint32_t c3 = min(ld_stream(ip + k + 3 * BLOCK, pol_stream), cmax);
-      const V v0 = ld_stream(vp + k, pol_stream);
-      const V v1 = ld_stream(vp + k + BLOCK, pol_stream);
-      const V v2 = ld_stream(vp + k + 2 * BLOCK, pol_stream);
-      const V v3 = ld_stream(vp + k + 3 * BLOCK, pol_stream);
-      const Acc x0 = gather(c0, pol_keep);
-      const Acc x1 = gather(c1, pol_keep);
-      const Acc x2 = gather(c2, pol_keep);
-      const Acc x3 = gather(c3, pol_keep);
-      prod[k] = static_cast<Acc>(v0) * x0;
-      prod[k + BLOCK] = static_cast<Acc>(v1) * x1;
-      prod[k + 2 * BLOCK] = static_cast<Acc>(v2) * x2;
-      prod[k + 3 * BLOCK] = static_cast<Acc>(v3) * x3;
+    __syncthreads();  // stage s and prod are free again
+    s ^= 1;
+  }
+  cp_async_wait<0>();
+}
+
+// Row-parallel schedule: rows first, first + step, ... (< end), one thread per
+// row, read straight from global memory (the L1 keeps the lines that
+// neighbouring threads' rows share).  Each row is summed exactly like the
+// reference's inner loop (src/blas.c:85-88): from 0, k ascending, the product
+// rounded before the add (no fused multiply-add), so y is bit-identical to
+// blas_spmult's.
+//
+// The loop is a three-stage register pipeline over a thread's rows: while the
+// x values of row i are gathered, the indices/values (and the epilogue's
+// per-row operands, Out::pre) of row i + step and the rowptr pair of row
+// i + 2 step are already in flight, so a row costs about one memory round
+// trip instead of three.  The first kRowStage entries of a row ride in the
+// pipeline; longer rows finish their tail inline.
+#ifndef GB_ROW_STAGE
+#define GB_ROW_STAGE 6
+#endif
+#ifndef GB_ROW_MIN_BLOCKS
+#define GB_ROW_MIN_BLOCKS 2
+#endif
+constexpr int kRowStage = GB_ROW_STAGE;
+// resident CTAs per SM the register budget of a kernel is sized for
+template <int SCHED>
+struct MinBlocks {
+  static constexpr int value = SCHED == SCHED_ROW ? GB_ROW_MIN_BLOCKS : kSpmvMinBlocks;
+};
+
+template <typename V>
+struct RowStage {
+  uint32_t b = 0, e = 0;
+  uint32_t c[kRowStage];
+  V v[kRowStage];
+};
+
+template <typename V>
+__device__ __forceinline__ void row_stage_load(RowStage<V> & s, const uint32_t * rowind,
+    const V * val, uint64_t pol) {
+#pragma unroll
+  for (int j = 0; j < kRowStage; ++j) {
+    if (s.b + j < s.e) {
+      s.c[j] = ld_stream(rowind + s.b + j, pol);
+      s.v[j] = ld_stream(val + s.b + j, pol);
     }
-    for (; k < N; k += BLOCK) {
-      const uint32_t c = min(ld_stream(ip + k, pol_stream), cmax);
-      prod[k] = static_cast<Acc>(ld_stream(vp + k, pol_stream)) * gather(c, pol_keep);
+  }
+}
+
+template <typename V, typename Acc, class Gather, class Out>
+__device__ __forceinline__ void spmv_row_loop(uint32_t first, uint32_t end, uint32_t step,
+    uint32_t ncols, const uint32_t * __restrict__ rowptr,
+    const uint32_t * __restrict__ rowind, const V * __restrict__ val, const Gather & gather,
+    Out & out, uint64_t pol_matrix, uint64_t pol_x) {
+  const uint32_t cmax = ncols - 1;
+  if (first >= end) return;
+  // stage L: row `first`; stage P: rowptr pair of row first + step
+  RowStage<V> cur;
+  cur.b = __ldg(rowptr + first);
+  cur.e = __ldg(rowptr + first + 1);
+  typename Out::Pre cur_pre = out.pre(first);
+  row_stage_load(cur, rowind, val, pol_matrix);
+  uint32_t nb = 0, ne = 0;
+  if (first + step < end) {
+    nb = __ldg(rowptr + first + step);
+    ne = __ldg(rowptr + first + step + 1);
+  }
+  for (uint32_t i = first; i < end; i += step) {
+    // issue the next row's indices/values/operands and the rowptr two ahead
+    RowStage<V> nxt;
+    typename Out::Pre nxt_pre{};
+    const uint32_t i1 = i + step, i2 = i + 2 * step;
+    if (i1 < end) {
+      nxt.b = nb;
+      nxt.e = ne;
+      nxt_pre = out.pre(i1);
+      row_stage_load(nxt, rowind, val, pol_matrix);
     }
-    __syncthreads();
-    reduce_tile<SCHED, BLOCK, Acc>(prod, offs, d.row_begin, R, N, out, scan_v, scan_k);
-    __syncthreads();
+    if (i2 < end) {
+      nb = __ldg(rowptr + i2);
+      ne = __ldg(rowptr + i2 + 1);
+    }
+    // gather and sum the current row (reference order)
+    Acc xv[kRowStage];
+#pragma unroll
+    for (int j = 0; j < kRowStage; ++j)
+      if (cur.b + j < cur.e) xv[j] = gather(min(cur.c[j], cmax), pol_x);
+    Acc sum = Acc(0);
+#pragma unroll
+    for (int j = 0; j < kRowStage; ++j)
+      if (cur.b + j < cur.e) sum = add_rn(sum, mul_rn(static_cast<Acc>(cur.v[j]), xv[j]));
+    for (uint32_t k = cur.b + kRowStage; k < cur.e; ++k)  // long-row tail
+      sum = add_rn(sum, mul_rn(static_cast<Acc>(ld_stream(val + k, pol_matrix)),
+                               gather(min(ld_stream(rowind + k, pol_matrix), cmax), pol_x)));
+    out.row_pre(i, sum, cur_pre);
+    cur = nxt;
+    cur_pre = nxt_pre;
+  }
+}
+
+// Round-robin driver: CTA b runs tiles b, b + gridDim.x, ... (or, for the
+// row schedule, rows in a grid-stride loop); then out.finish() once per
+// thread.
+template <typename V, typename Acc, int SCHED, int BLOCK, class Gather, class Out>
+__device__ __forceinline__ void spmv_tiles_body(const PlanView plan,
+    const uint32_t * __restrict__ rowptr, const uint32_t * __restrict__ rowind,
+    const V * __restrict__ val, const Gather gather, Out & out) {
+  if (SCHED == SCHED_ROW) {
+    spmv_row_loop<V, Acc>(blockIdx.x * BLOCK + threadIdx.x, plan.nrows, gridDim.x * BLOCK,
+        plan.ncols, rowptr, rowind, val, gather, out, policy_evict_first(),
+        policy_evict_last());
+  } else {
+    spmv_tile_loop<V, Acc, SCHED, BLOCK>(plan, blockIdx.x, plan.ntiles, gridDim.x, rowptr,
+        rowind, val, gather, out, policy_evict_first(), policy_evict_last());
   }
   out.finish();
 }

@@ -70,7 +70,11 @@ typedef enum gb_schedule {
   GB_SCHED_GROUP4 = 2,   /* 4 lanes per row                                  */
   GB_SCHED_GROUP8 = 3,   /* 8 lanes per row                                  */
   GB_SCHED_WARP = 4,     /* 32 lanes per row                                 */
-  GB_SCHED_MERGE = 5     /* merge-path split of rows+nnz over threads        */
+  GB_SCHED_MERGE = 5,    /* merge-path split of rows+nnz over threads        */
+  GB_SCHED_ROW = 6       /* one thread per row straight from global memory,
+                            no tile staging; sums each row in the reference's
+                            order (k ascending, unfused multiply and add), so
+                            its SpMV is bit-identical to the reference       */
 } gb_schedule_t;
 
 /*
@@ -156,6 +160,13 @@ typedef enum gb_cg_mode {
   GB_CG_F64 = 0,   /* plain FP64 CG, the reference's algorithm             */
   GB_CG_MIXED = 1  /* FP32 values/vectors inside, FP64 residual refinement  */
 } gb_cg_mode_t;
+
+/* OR-ed into the mode of gb_cg_create: run the whole solve as ONE persistent
+ * cooperative launch (CTAs own fixed rows; two grid barriers per iteration)
+ * instead of the default two graph-replayed kernels per iteration.  Taken
+ * only when every row fits a tile and the grid can be co-resident; it holds
+ * every SM until the solve ends. */
+#define GB_CG_PERSISTENT 0x100
 
 typedef enum gb_cg_status {
   GB_CG_CONVERGED = 0,  /* ||r|| <= tolerance                                 */

@@ -84,3 +84,28 @@ def test_full_laplacian_1024_matches_reference(torch, full_golden):
     xs = x.cpu().numpy()
     res = np.linalg.norm(b - L.to_scipy() @ xs) / np.linalg.norm(b)
     assert res <= 1.5 * g["rtol"]
+
+
+def test_persistent_and_graph_paths_agree(torch, cg_golden):
+    """The one-launch cooperative solve and the graph-replayed two-kernel
+    solve run the same algorithm: same iteration count (+-2 of the
+    reference), both converged, solutions equal to CG accuracy."""
+    for name in ("laplace64", "diffusion3d12"):
+        c = cg_golden[name]
+        b = torch.from_numpy(c["b"]).cuda()
+        out = {}
+        for pers in (False, True):
+            for sched in (gb.SCHED_ROW, gb.SCHED_THREAD, gb.SCHED_MERGE):
+                A = gb.CsrMatrix.from_host(rowptr=c["rowptr"], rowind=c["rowind"],
+                                           rowval=c["rowval"])
+                A.set_schedule(sched, tile_items=256)
+                S = gb.CgSolver(A, persistent=pers)
+                x, r = S.solve(b, tol=float(c["error"]), relative=False, niter=int(c["niter"]))
+                assert r.status == "converged", (name, pers, sched, r)
+                assert abs(r.iterations - int(c["iterations"])) <= 2, (name, pers, sched, r)
+                if pers:
+                    assert r.kernel_launches == 1
+                out[(pers, sched)] = x.cpu().numpy()
+        ref = c["x"]
+        for k, x in out.items():
+            assert np.linalg.norm(x - ref) <= 1e-4 * np.linalg.norm(ref), (name, k)

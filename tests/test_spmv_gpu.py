@@ -19,7 +19,8 @@ pytestmark = pytest.mark.gpu
 
 TOL64 = 1e-13
 TOL32 = 64 * 2.0 ** -24
-SCHEDS = [gb.SCHED_THREAD, gb.SCHED_GROUP4, gb.SCHED_GROUP8, gb.SCHED_WARP, gb.SCHED_MERGE]
+SCHEDS = [gb.SCHED_THREAD, gb.SCHED_GROUP4, gb.SCHED_GROUP8, gb.SCHED_WARP, gb.SCHED_MERGE,
+          gb.SCHED_ROW]
 
 
 @pytest.fixture(scope="module")
@@ -49,6 +50,22 @@ def test_golden_cases_all_schedules_f64(torch, spmv_golden):
                 # deterministic: a second run is bitwise identical
                 assert np.array_equal(y, A.spmv(x).cpu().numpy()), (name, s, tile)
         A.close()
+
+
+def test_row_schedule_is_bit_identical_to_reference(torch, spmv_golden):
+    """The row schedule sums each row in the reference's order without fused
+    multiply-adds, so its y equals blas_spmult's bit for bit (f64 and f32)."""
+    for name, c in spmv_golden.items():
+        if "rowptr" not in c:
+            continue
+        A = gb.CsrMatrix.from_host(rowptr=c["rowptr"], rowind=c["rowind"], rowval=c["rowval"],
+                                   f64=True, f32=True)
+        A.set_schedule(gb.SCHED_ROW)
+        A.set_schedule(gb.SCHED_ROW, f32=True)
+        y = A.spmv(_dev(torch, c["x"])).cpu().numpy()
+        assert np.array_equal(y, c["y64"]), name
+        y32 = A.spmv(_dev(torch, c["x"].astype(np.float32))).cpu().numpy()
+        assert np.array_equal(y32, c["y32"]), name
 
 
 def test_golden_cases_f32(torch, spmv_golden):
