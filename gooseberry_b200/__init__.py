@@ -98,6 +98,7 @@ SIGNATURES = {
     "gb_spmm_f64": (_i, [_vp, _u32, _vp, _vp, _vp]),
     "gb_dot_f64": (_i, [_sz, _vp, _vp, _vp, _vp]),
     "gb_dot_f32": (_i, [_sz, _vp, _vp, _vp, _vp]),
+    "gb_dot_f64_noalloc": (_i, [_sz, _vp, _vp, _vp, _vp]),
     "gb_scale_f64": (_i, [_sz, _vp, _d, _vp]),
     "gb_add_scalar_f64": (_i, [_sz, _vp, _d, _vp]),
     "gb_add_f64": (_i, [_sz, _vp, _vp, _vp, _vp]),

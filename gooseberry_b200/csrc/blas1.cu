@@ -8,6 +8,8 @@
 // reference's OpenMP reduction order varies with the thread count,
 // src/blas.c:423-427).
 #include <algorithm>
+#include <mutex>
+#include <vector>
 
 #include "gb_internal.h"
 #include "spmv_tiles.cuh"
@@ -126,9 +128,85 @@ int launch_add_scalar_f32(size_t n, float * v, float s, cudaStream_t st) {
   return GOOSEBERRY_SUCCESS;
 }
 
+// ---- allocation-free dot product --------------------------------------------
+//
+// Same two-kernel reduction as dot_impl, but each CTA owns a fixed chunk of
+// kNoAllocChunk elements and writes its partial sum into a file-scope device
+// array instead of memory obtained from the allocator.  Host code must not
+// pass `g_dot_scratch` itself to a kernel: in host code that name is only a
+// host-side stand-in for the symbol, so the device address is looked up with
+// cudaGetSymbolAddress once per device and cached.
+
+namespace {
+
+constexpr size_t kNoAllocChunk = 16384;       // elements per CTA
+constexpr unsigned kNoAllocMaxChunks = 8192;  // partial sums the array holds
+static_assert(GB_DOT_NOALLOC_MAX_N == kNoAllocChunk * kNoAllocMaxChunks,
+    "header limit and array size disagree");
+
+static __device__ __align__(256) double g_dot_scratch[kNoAllocMaxChunks];
+
+std::mutex g_dot_scratch_mu;
+std::vector<double *> g_dot_scratch_ptr;  // device address of the array, per device
+
+__global__ void __launch_bounds__(kBlock) dot_chunk_kernel(size_t n,
+    const double * __restrict__ a, const double * __restrict__ b,
+    double * __restrict__ partial) {
+  __shared__ double red[32];
+  const size_t s = static_cast<size_t>(blockIdx.x) * kNoAllocChunk;
+  const size_t e = min(n, s + kNoAllocChunk);
+  double acc = 0.0;
+  for (size_t i = s + threadIdx.x; i < e; i += kBlock) acc += a[i] * b[i];
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) partial[blockIdx.x] = acc;
+}
+
+// Device address of g_dot_scratch on the current device (looked up once).
+int dot_scratch_address(double ** out) {
+  int dev = 0;
+  GB_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_dot_scratch_mu);
+  if (g_dot_scratch_ptr.size() <= static_cast<size_t>(dev))
+    g_dot_scratch_ptr.resize(dev + 1, nullptr);
+  if (!g_dot_scratch_ptr[dev]) {
+    void * p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_dot_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+      set_error("cudaGetSymbolAddress of the dot scratch array failed on device %d: %s", dev,
+          cudaGetErrorString(e));
+      return GOOSEBERRY_ERROR_UNKNOWN;
+    }
+    g_dot_scratch_ptr[dev] = static_cast<double *>(p);
+  }
+  *out = g_dot_scratch_ptr[dev];
+  return GOOSEBERRY_SUCCESS;
+}
+
+}  // namespace
+
 }  // namespace gb
 
 extern "C" {
+
+int gb_dot_f64_noalloc(size_t n, const double * a, const double * b, double * result,
+    gb_stream_t stream) {
+  GB_CHECK_INPUT(result != nullptr, "result is NULL");
+  GB_CHECK_INPUT(n == 0 || (a && b), "NULL vector");
+  GB_CHECK_INPUT(n <= GB_DOT_NOALLOC_MAX_N,
+      "n = %zu exceeds the %zu elements the allocation-free dot product can reduce "
+      "(its fixed scratch holds %u partial sums of %zu elements each)",
+      n, static_cast<size_t>(GB_DOT_NOALLOC_MAX_N), gb::kNoAllocMaxChunks,
+      gb::kNoAllocChunk);
+  double * scratch = nullptr;
+  GB_TRY(gb::dot_scratch_address(&scratch));
+  const unsigned chunks = static_cast<unsigned>(
+      std::max<size_t>(1, (n + gb::kNoAllocChunk - 1) / gb::kNoAllocChunk));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  gb::dot_chunk_kernel<<<chunks, gb::kBlock, 0, s>>>(n, a, b, scratch);
+  gb::dot_final_kernel<<<1, gb::kBlock, 0, s>>>(chunks, scratch, result);
+  GB_CUDA_TRY(cudaGetLastError());
+  return GOOSEBERRY_SUCCESS;
+}
 
 int gb_dot_f64(size_t n, const double * a, const double * b, double * result,
     gb_stream_t stream) {

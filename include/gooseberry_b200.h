@@ -142,6 +142,32 @@ GOOSEBERRY_API int gb_dot_f64(size_t n, const double * a, const double * b, doub
     gb_stream_t stream);
 GOOSEBERRY_API int gb_dot_f32(size_t n, const float * a, const float * b, double * result,
     gb_stream_t stream);
+
+/*
+ * Allocation-free form of gb_dot_f64, for callers that must not allocate
+ * device memory during a call: code whose device memory is entirely owned by
+ * another allocator (a framework's caching pool holding all of HBM, where
+ * cudaMalloc fails or forces that pool to release memory), and
+ * latency-critical loops where cudaMalloc/cudaFree would synchronise the
+ * device.  It computes the same sum as gb_dot_f64 (double accumulation,
+ * fixed order; the grouping differs, so the last bits can too), but it keeps
+ * its per-CTA partial sums in one fixed 64 KiB array in device memory,
+ * declared in the library, instead of asking for memory.
+ *   - n may be at most GB_DOT_NOALLOC_MAX_N; larger n is rejected with
+ *     GOOSEBERRY_ERROR_INVALIDINPUT before anything runs.
+ *   - The first call on each device looks up that array's device address
+ *     (with that device current) and remembers it: make that first call
+ *     before any stream capture.
+ *   - Every call on a device shares the one array, and it keeps the previous
+ *     call's partial sums (each call writes every entry it reads first), so
+ *     calls whose kernels overlap on the GPU (different streams, or threads
+ *     racing) corrupt each other's result: serialise them.
+ * The array stays allocated on every GPU that loaded the library until the
+ * process exits.  No counterpart in the reference.
+ */
+#define GB_DOT_NOALLOC_MAX_N ((size_t)16384 * 8192)
+GOOSEBERRY_API int gb_dot_f64_noalloc(size_t n, const double * a, const double * b,
+    double * result, gb_stream_t stream);
 /* v *= s (blas_scale, src/blas.c:244-257); v += s (blas_add_scalar,
  * src/blas.c:397-410); c = a + b (blas_add, src/blas.c:275-290);
  * c = a - b (blas_sub, src/blas.c:321-336).  c may alias a or b. */
