@@ -34,6 +34,7 @@
 
 #include "gb_internal.h"
 #include "spmv_tiles.cuh"
+#include "cg_common.cuh"
 
 namespace gb {
 
@@ -66,56 +67,6 @@ struct CgStatus {
   double rr;
   double bnorm;
 };
-
-constexpr int kVecBlock = 256;
-
-// Programmatic dependent launch: a kernel lets the next one in the stream be
-// scheduled as soon as its own CTAs start retiring, and waits for the
-// previous kernel's completion (and memory) before touching any data.
-__device__ __forceinline__ void pdl_wait_and_release() {
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-
-template <typename... KArgs, typename... Args>
-cudaError_t launch_k(void (*k)(KArgs...), unsigned grid, unsigned block, size_t smem,
-    cudaStream_t s, bool pdl, Args... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(grid);
-  cfg.blockDim = dim3(block);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = s;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = pdl ? 1 : 0;
-  return cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...);
-}
-
-// Returns true in thread 0 of the last CTA to arrive (ticket pattern).
-__device__ __forceinline__ bool arrive_last(unsigned int * ticket, bool * flag) {
-  __syncthreads();  // every thread's writes of this CTA precede thread 0's fence
-  if (threadIdx.x == 0) {
-    __threadfence();
-    const unsigned prev = atomicAdd(ticket, 1u);
-    *flag = (prev == gridDim.x - 1);
-  }
-  __syncthreads();
-  return *flag;
-}
-
-// Sum of partial[0..n) in index order, by one CTA; result valid in thread 0.
-__device__ __forceinline__ double ordered_sum(const double * partial, unsigned n,
-    double * red) {
-  // each thread sums a contiguous run, then runs are summed in thread order
-  const unsigned per = (n + blockDim.x - 1) / blockDim.x;
-  const unsigned s = min(n, threadIdx.x * per), e = min(n, s + per);
-  double acc = 0.0;
-  for (unsigned i = s; i < e; ++i) acc += __ldcg(partial + i);
-  // ordered combine: warp tree is order-fixed as well
-  return block_sum(acc, red);
-}
 
 // ---- A: SpMV with fused direction update and p.Ap -----------------------------
 
@@ -335,7 +286,7 @@ __global__ void __launch_bounds__(kVecBlock) cg_init_kernel(size_t n,
 
 // dynamic shared memory of the SpMV phase (the row schedule stages nothing)
 size_t spmv_smem(int sched, uint32_t tile_items) {
-  return sched == GB_SCHED_ROW ? 0 : TileSmem<double, double>::bytes(tile_items);
+  return spmv_smem_bytes<double, double>(sched, tile_items, kSpmvBlock);
 }
 
 template <int SCHED>
@@ -371,6 +322,9 @@ int launch_cg_a(const gb_csr & a, int sched, const double * r, const double * po
     case GB_SCHED_ROW:
       return launch_cg_a_t<SCHED_ROW>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
           pdl);
+    case GB_SCHED_WTILE:
+      return launch_cg_a_t<SCHED_WTILE>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
+          pdl);
     default:
       return launch_cg_a_t<SCHED_MERGE>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
           pdl);
@@ -394,6 +348,7 @@ int occupancy_cg_a_sched(int sched, size_t smem, int * out) {
     case GB_SCHED_GROUP8: return occupancy_cg_a<SCHED_GROUP8>(smem, out);
     case GB_SCHED_WARP: return occupancy_cg_a<SCHED_WARP>(smem, out);
     case GB_SCHED_ROW: return occupancy_cg_a<SCHED_ROW>(smem, out);
+    case GB_SCHED_WTILE: return occupancy_cg_a<SCHED_WTILE>(smem, out);
     default: return occupancy_cg_a<SCHED_MERGE>(smem, out);
   }
 }
@@ -589,6 +544,9 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_persis
       if (SCHED == SCHED_ROW)
         spmv_row_loop<double, double>(lo + tid, hi, kSpmvBlock, a.plan.ncols, a.rowptr,
             a.rowind, a.val, g, o, pol_m, pol_x);
+      else if (SCHED == SCHED_WTILE)
+        spmv_warp_loop<double, double>(a.plan, t0 + (tid >> 5), t1, kSpmvBlock / 32,
+            a.rowptr, a.rowind, a.val, g, o, pol_m, pol_x);
       else
         spmv_tile_loop<double, double, SCHED, kSpmvBlock>(a.plan, t0, t1, 1, a.rowptr,
             a.rowind, a.val, g, o, pol_m, pol_x);
@@ -670,6 +628,7 @@ int persistent_setup(int sched, size_t smem, int * occ, const void ** fn) {
     case GB_SCHED_GROUP8: return persistent_setup_t<SCHED_GROUP8>(smem, occ, fn);
     case GB_SCHED_WARP: return persistent_setup_t<SCHED_WARP>(smem, occ, fn);
     case GB_SCHED_ROW: return persistent_setup_t<SCHED_ROW>(smem, occ, fn);
+    case GB_SCHED_WTILE: return persistent_setup_t<SCHED_WTILE>(smem, occ, fn);
     default: return persistent_setup_t<SCHED_MERGE>(smem, occ, fn);
   }
 }
@@ -708,6 +667,7 @@ struct gb_cg {
   uint32_t * cta_tiles = nullptr;
   unsigned * sync = nullptr;  // [0] barrier counter, [1] abort flag
   int keep_l2 = 0;
+  gb::MixedCg * mixed = nullptr;  // GB_CG_MIXED solver (owns its workspace)
 };
 
 namespace gb {
@@ -715,6 +675,7 @@ namespace {
 
 void destroy_cg(gb_cg * s) {
   if (!s) return;
+  mixed_destroy(s->mixed);
   for (auto & g : s->graph)
     if (g) cudaGraphExecDestroy(g);
   if (s->cap_stream) cudaStreamDestroy(s->cap_stream);
@@ -852,7 +813,13 @@ int create_cg(const gb_csr * a, int mode, gb_cg * s) {
       a->ncols);
   const bool want_persistent = (mode & GB_CG_PERSISTENT) != 0;
   mode &= ~GB_CG_PERSISTENT;
-  GB_CHECK_INPUT(mode == GB_CG_F64, "CG mode %d is not available", mode);
+  GB_CHECK_INPUT(mode == GB_CG_F64 || mode == GB_CG_MIXED, "unknown CG mode %d", mode);
+  if (mode == GB_CG_MIXED) {
+    s->a = a;
+    s->mode = mode;
+    s->n = a->nrows;
+    return mixed_create(a, &s->mixed);
+  }
   GB_CHECK_INPUT(a->val64 != nullptr, "CG (FP64) needs double values on the matrix");
   s->a = a;
   s->mode = mode;
@@ -870,8 +837,8 @@ int create_cg(const gb_csr * a, int mode, gb_cg * s) {
   GB_TRY(occupancy_cg_a_sched(s->sched, smem, &occ));
   GB_CHECK_INPUT(occ > 0, "CG kernel cannot be resident");
   const unsigned ntiles = static_cast<unsigned>(std::max<size_t>(a->plan.tiles.size(), 1));
-  const unsigned work_a = s->sched == GB_SCHED_ROW
-      ? static_cast<unsigned>((s->n + kSpmvBlock - 1) / kSpmvBlock) : ntiles;
+  const unsigned work_a = spmv_work_units(s->sched, static_cast<uint32_t>(s->n), ntiles,
+      kSpmvBlock);
   s->grid_a = std::min<unsigned>(std::max(work_a, 1u),
       static_cast<unsigned>(a->sm_count * occ));
   const size_t units = (s->n + 1) / 2;
@@ -923,6 +890,9 @@ int start_solve(gb_cg * s, const double * b, double tol, int tol_relative, size_
 int solve_cg(gb_cg * s, const double * b, double * x, double tol, int tol_relative,
     size_t niter, double * history, size_t history_len, gb_cg_result_t * res,
     cudaStream_t stream) {
+  if (s->mixed)
+    return mixed_solve(s->mixed, b, x, tol, tol_relative, niter, history, history_len, res,
+        stream);
   GB_CHECK_INPUT(s->n == 0 || (b && x), "NULL vector");
   GB_CHECK_INPUT(s->a->sched64 == s->sched && s->a->plan.tile_items == s->tile_items,
       "matrix schedule changed after the solver was created");
@@ -1011,6 +981,7 @@ int profile_cg(gb_cg * s, const double * b, size_t iterations, double * ms, size
     size_t * nkernels, cudaStream_t stream) {
   GB_CHECK_INPUT(s->n > 0 && b != nullptr, "profile needs a non-empty system and b");
   GB_CHECK_INPUT(iterations > 0, "iterations must be positive");
+  if (s->mixed) return mixed_profile(s->mixed, b, iterations, ms, ms_len, nkernels, stream);
   if (s->persistent) {
     // one launch runs every iteration: time it and report ms per iteration
     if (nkernels) *nkernels = 1;

@@ -1,0 +1,784 @@
+// cg_mixed.cu -- mixed-precision CG: FP32 inner iterations, FP64 refinement.
+//
+// Same iteration as the reference's cgd (src/cgd.c:87-120), but the matrix
+// values and the Krylov vectors of the inner loop are FP32 (half the bytes of
+// an FP64 iteration), while everything that decides accuracy stays FP64:
+//
+//   * the dots p.Ap and r.r are accumulated in FP64 (alpha, beta, ||r||);
+//   * the solution is x (FP64) + y (FP32 correction since the last update);
+//   * a "reliable update" (Sleijpen & van der Vorst, 1996) replaces the
+//     iterated FP32 residual by the true one whenever ||r|| has dropped by
+//     kDelta below its largest value since the last update, or looks
+//     converged:  x <- x + y,  r = b - A x  computed with the FP64 values and
+//     FP64 accumulation, then rounded to FP32.  The search direction is kept,
+//     so the Krylov process continues instead of restarting, and convergence
+//     is only ever declared on the true FP64 residual.
+//
+// Per iteration three kernels, graph-captured 32 iterations at a time with
+// programmatic dependent launch:
+//   A32  SpMV (FP32) with the fused direction update, p.Ap in FP64
+//   B32  y += alpha p, r -= alpha Ap, r.r in FP64, update decision
+//   R    only when an update is pending (returns at once otherwise): FP64
+//        SpMV of b - A (x + y) fused with x <- x + y (into the other x
+//        buffer, so no CTA reads an x another CTA already changed) and the
+//        FP32 rounding of r; true ||r||, convergence test.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "gb_internal.h"
+#include "spmv_tiles.cuh"
+#include "cg_common.cuh"
+
+namespace gb {
+
+namespace {
+
+constexpr double kDelta = 0.1;  // reliable update when ||r|| < kDelta * max ||r||
+
+struct MixState {
+  double rr_hat;      // ||r||^2 of the FP32 residual the directions are built on
+  double rr_hat_old;  // its value one iteration earlier
+  double alpha;
+  double beta;
+  double tol;         // absolute bound on the true ||b - A x||
+  double bnorm;
+  double rmax;        // largest ||r|| since the last reliable update
+  double rr_true;     // ||b - A x||^2 at the last reliable update
+  unsigned long long iter;
+  unsigned long long niter;
+  unsigned long long refinements;
+  int done;
+  int status;
+  int update;         // a reliable update is pending
+  int y_reset;        // y was folded into x: the next B starts y afresh
+  int xpar;           // index of the current x buffer
+  int force;          // run R even without a pending update (final fold)
+  unsigned ticket_a, ticket_b, ticket_r, ticket_i;
+  double * hist;
+  unsigned long long hist_len;
+};
+
+struct MixStatus {
+  int done;
+  int status;
+  unsigned long long iter;
+};
+
+// ---- A32 ----------------------------------------------------------------------
+
+struct GatherP32 {
+  const float * r;
+  const float * pold;
+  float beta;
+  __device__ __forceinline__ float operator()(uint32_t c, uint64_t pol) const {
+    return fmaf(beta, ld_keep(pold + c, pol), ld_keep(r + c, pol));
+  }
+};
+
+struct OutA32 {
+  float * ap;
+  float * pnew;
+  const float * r;
+  const float * pold;
+  double * longdot;
+  double * partial;
+  MixState * st;
+  float beta;
+  unsigned nlong;
+  double local;
+  __device__ __forceinline__ void row(uint32_t i, float v) {
+    ap[i] = v;
+    const float pn = fmaf(beta, pold[i], r[i]);
+    pnew[i] = pn;
+    local += static_cast<double>(pn) * static_cast<double>(v);
+  }
+  __device__ __forceinline__ void long_row(uint32_t lid, uint32_t i, float v) {
+    ap[i] = v;
+    const float pn = fmaf(beta, pold[i], r[i]);
+    pnew[i] = pn;
+    longdot[lid] = static_cast<double>(pn) * static_cast<double>(v);
+  }
+  struct Pre {
+    float r, pold;
+  };
+  __device__ __forceinline__ Pre pre(uint32_t i) const { return Pre{r[i], pold[i]}; }
+  __device__ __forceinline__ void row_pre(uint32_t i, float v, const Pre & q) {
+    ap[i] = v;
+    const float pn = fmaf(beta, q.pold, q.r);
+    pnew[i] = pn;
+    local += static_cast<double>(pn) * static_cast<double>(v);
+  }
+  __device__ __forceinline__ void finish() {
+    __shared__ double red[32];
+    __shared__ bool last;
+    const double s = block_sum(local, red);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+    if (!arrive_last(&st->ticket_a, &last)) return;
+    __threadfence();
+    double tot = ordered_sum(partial, gridDim.x, red);
+    if (threadIdx.x == 0) {
+      for (unsigned q = 0; q < nlong; ++q) tot += __ldcg(longdot + q);
+      st->ticket_a = 0;
+      const double rr = st->rr_hat;
+      if (!(tot > 0.0)) {
+        st->done = 1;
+        st->status = (tot == tot && rr == rr) ? GB_CG_BREAKDOWN : GB_CG_NONFINITE;
+        st->alpha = 0.0;
+      } else {
+        st->alpha = rr / tot;
+      }
+    }
+  }
+};
+
+template <int SCHED>
+__global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_a32_kernel(
+    const PlanView plan, const uint32_t * __restrict__ rowptr,
+    const uint32_t * __restrict__ rowind, const float * __restrict__ val,
+    const float * __restrict__ r, const float * __restrict__ pold, float * __restrict__ pnew,
+    float * __restrict__ ap, double * __restrict__ longdot, double * __restrict__ partial,
+    MixState * st) {
+  pdl_wait_and_release();
+  if (*reinterpret_cast<volatile int *>(&st->done)) return;
+  const float beta = static_cast<float>(st->beta);
+  GatherP32 g{r, pold, beta};
+  OutA32 o{ap, pnew, r, pold, longdot, partial, st, beta,
+           SCHED == SCHED_ROW ? 0u : plan.nlong, 0.0};
+  spmv_tiles_body<float, float, SCHED, kSpmvBlock>(plan, rowptr, rowind, val, g, o);
+}
+
+// ---- B32 ----------------------------------------------------------------------
+
+__global__ void __launch_bounds__(kVecBlock, kSpmvMinBlocks) cg_b32_kernel(size_t n,
+    float * __restrict__ y, float * __restrict__ r, const float * __restrict__ p,
+    const float * __restrict__ ap, double * __restrict__ partial, MixState * st) {
+  pdl_wait_and_release();
+  if (*reinterpret_cast<volatile int *>(&st->done)) return;
+  __shared__ double red[32];
+  __shared__ bool last;
+  const float alpha = static_cast<float>(st->alpha);
+  const bool fresh = st->y_reset != 0;
+  const size_t q = n / gridDim.x, rem = n % gridDim.x;
+  const size_t b = blockIdx.x;
+  const size_t s = b * q + min(b, rem);
+  const size_t e = s + q + (b < rem ? 1 : 0);
+  double acc = 0.0;
+  constexpr int U = 4;
+  for (size_t base = s; base < e; base += U * kVecBlock) {
+    float pv[U], av[U], yv[U], rv[U];
+#pragma unroll
+    for (int j = 0; j < U; ++j) {
+      const size_t i = base + threadIdx.x + j * kVecBlock;
+      if (i < e) {
+        pv[j] = p[i];
+        av[j] = ap[i];
+        yv[j] = fresh ? 0.0f : y[i];
+        rv[j] = r[i];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < U; ++j) {
+      const size_t i = base + threadIdx.x + j * kVecBlock;
+      if (i < e) {
+        y[i] = fmaf(alpha, pv[j], yv[j]);
+        const float rn = fmaf(-alpha, av[j], rv[j]);
+        r[i] = rn;
+        acc += static_cast<double>(rn) * static_cast<double>(rn);
+      }
+    }
+  }
+  const double bs = block_sum(acc, red);
+  if (threadIdx.x == 0) partial[blockIdx.x] = bs;
+  if (!arrive_last(&st->ticket_b, &last)) return;
+  __threadfence();
+  const double rr = ordered_sum(partial, gridDim.x, red);
+  if (threadIdx.x == 0) {
+    st->ticket_b = 0;
+    st->y_reset = 0;
+    st->rr_hat_old = st->rr_hat;
+    st->beta = rr / st->rr_hat;
+    st->rr_hat = rr;
+    const unsigned long long it = st->iter + 1;
+    st->iter = it;
+    const double rnorm = sqrt(rr);
+    if (st->hist && it <= st->hist_len) st->hist[it - 1] = rnorm;
+    st->rmax = fmax(st->rmax, rnorm);
+    if (!(rnorm == rnorm) || isinf(rnorm)) {
+      st->done = 1;
+      st->status = GB_CG_NONFINITE;
+    } else if (rnorm <= st->tol || rnorm < kDelta * st->rmax) {
+      st->update = 1;  // R folds y into x and checks the true residual
+    } else if (st->niter && it >= st->niter) {
+      st->done = 1;
+      st->status = GB_CG_MAXITER;
+    }
+  }
+}
+
+// ---- R: reliable update -------------------------------------------------------
+
+struct GatherXY {
+  const double * x;
+  const float * y;
+  bool use_y;
+  __device__ __forceinline__ double operator()(uint32_t c, uint64_t pol) const {
+    const double xv = ld_keep(x + c, pol);
+    return use_y ? xv + static_cast<double>(ld_keep(y + c, pol)) : xv;
+  }
+};
+
+struct OutR {
+  const double * b;
+  const double * xold;
+  double * xnew;
+  const float * y;
+  float * r32;
+  double * longdot;
+  double * partial;
+  MixState * st;
+  bool use_y;
+  unsigned nlong;
+  double local;
+  __device__ __forceinline__ double fold(uint32_t i, double ax) {
+    xnew[i] = use_y ? xold[i] + static_cast<double>(y[i]) : xold[i];
+    const double rt = b[i] - ax;
+    r32[i] = static_cast<float>(rt);
+    return rt * rt;
+  }
+  __device__ __forceinline__ void row(uint32_t i, double v) { local += fold(i, v); }
+  __device__ __forceinline__ void long_row(uint32_t lid, uint32_t i, double v) {
+    longdot[lid] = fold(i, v);
+  }
+  struct Pre {};
+  __device__ __forceinline__ Pre pre(uint32_t) const { return Pre{}; }
+  __device__ __forceinline__ void row_pre(uint32_t i, double v, const Pre &) { row(i, v); }
+  __device__ __forceinline__ void finish() {
+    __shared__ double red[32];
+    __shared__ bool last;
+    const double s = block_sum(local, red);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+    if (!arrive_last(&st->ticket_r, &last)) return;
+    __threadfence();
+    double tot = ordered_sum(partial, gridDim.x, red);
+    if (threadIdx.x == 0) {
+      for (unsigned q = 0; q < nlong; ++q) tot += __ldcg(longdot + q);
+      st->ticket_r = 0;
+      st->rr_true = tot;
+      st->refinements += 1;
+      st->xpar ^= 1;
+      st->y_reset = 1;
+      st->update = 0;
+      const bool forced = st->force != 0;
+      st->force = 0;
+      const double rnorm = sqrt(tot);
+      const unsigned long long it = st->iter;
+      if (st->hist && it >= 1 && it <= st->hist_len) st->hist[it - 1] = rnorm;
+      if (!(rnorm == rnorm) || isinf(rnorm)) {
+        st->done = 1;
+        st->status = GB_CG_NONFINITE;
+      } else if (rnorm <= st->tol) {
+        st->done = 1;
+        st->status = GB_CG_CONVERGED;
+      } else if (!forced) {
+        // continue from the true residual, keeping the search direction
+        st->beta = tot / st->rr_hat_old;
+        st->rr_hat = tot;
+        st->rmax = rnorm;
+        if (st->niter && it >= st->niter) {
+          st->done = 1;
+          st->status = GB_CG_MAXITER;
+        }
+      }
+    }
+  }
+};
+
+template <int SCHED>
+__global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_r_kernel(
+    const PlanView plan, const uint32_t * __restrict__ rowptr,
+    const uint32_t * __restrict__ rowind, const double * __restrict__ val,
+    const double * __restrict__ b, const double * __restrict__ x0, double * __restrict__ x1,
+    const float * __restrict__ y, float * __restrict__ r32, double * __restrict__ longdot,
+    double * __restrict__ partial, MixState * st) {
+  pdl_wait_and_release();
+  const int force = *reinterpret_cast<volatile int *>(&st->force);
+  if (!force) {
+    if (*reinterpret_cast<volatile int *>(&st->done)) return;
+    if (!*reinterpret_cast<volatile int *>(&st->update)) return;
+  }
+  const int xpar = st->xpar;
+  const bool use_y = st->y_reset == 0;
+  const double * xold = xpar ? x1 : x0;
+  double * xnew = xpar ? const_cast<double *>(x0) : x1;
+  GatherXY g{xold, y, use_y};
+  OutR o{b, xold, xnew, y, r32, longdot, partial, st, use_y,
+         SCHED == SCHED_ROW ? 0u : plan.nlong, 0.0};
+  spmv_tiles_body<double, double, SCHED, kSpmvBlock>(plan, rowptr, rowind, val, g, o);
+}
+
+// ---- init -----------------------------------------------------------------------
+
+__global__ void __launch_bounds__(kVecBlock) cg_mixed_init_kernel(size_t n,
+    const double * __restrict__ b, double * __restrict__ x0, float * __restrict__ r32,
+    float * __restrict__ p0, double * __restrict__ partial, MixState * st,
+    int tol_relative) {
+  __shared__ double red[32];
+  __shared__ double red2[32];
+  __shared__ bool last;
+  double acc = 0.0, acc32 = 0.0;
+  for (size_t i = blockIdx.x * static_cast<size_t>(kVecBlock) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * kVecBlock) {
+    const double bv = b[i];
+    const float rv = static_cast<float>(bv);
+    x0[i] = 0.0;
+    r32[i] = rv;
+    p0[i] = 0.0f;
+    acc += bv * bv;
+    acc32 += static_cast<double>(rv) * static_cast<double>(rv);
+  }
+  const double s = block_sum(acc, red);
+  const double s32 = block_sum(acc32, red2);
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = s;
+    partial[2 * blockIdx.x + 1] = s32;
+  }
+  if (!arrive_last(&st->ticket_i, &last)) return;
+  __threadfence();
+  // ordered sums of the even (b.b) and odd (r32.r32) entries
+  double bb = 0.0, rr = 0.0;
+  if (threadIdx.x == 0) {
+    for (unsigned i = 0; i < gridDim.x; ++i) {
+      bb += __ldcg(partial + 2 * i);
+      rr += __ldcg(partial + 2 * i + 1);
+    }
+    st->ticket_i = 0;
+    st->bnorm = sqrt(bb);
+    st->rr_true = bb;
+    st->rr_hat = rr;
+    st->rr_hat_old = rr;
+    st->rmax = sqrt(rr);
+    st->beta = 0.0;
+    st->alpha = 0.0;
+    st->iter = 0;
+    st->refinements = 0;
+    st->xpar = 0;
+    st->y_reset = 1;
+    st->update = 0;
+    st->force = 0;
+    if (tol_relative) st->tol = st->tol * st->bnorm;
+    st->done = 0;
+    st->status = GB_CG_MAXITER;
+    if (bb == 0.0) {
+      st->done = 1;
+      st->status = GB_CG_CONVERGED;
+    } else if (!(bb == bb) || isinf(bb)) {
+      st->done = 1;
+      st->status = GB_CG_NONFINITE;
+    }
+  }
+}
+
+// ---- launch helpers ----------------------------------------------------------------
+
+size_t smem_of(int sched, uint32_t tile_items, size_t value_bytes) {
+  return value_bytes == 4 ? spmv_smem_bytes<float, float>(sched, tile_items, kSpmvBlock)
+                          : spmv_smem_bytes<double, double>(sched, tile_items, kSpmvBlock);
+}
+
+template <typename K>
+int prep_kernel(K kern, size_t smem, int * occ) {
+  if (smem > 48 * 1024)
+    GB_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void *>(kern),
+        cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  if (occ)
+    GB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, kSpmvBlock, smem));
+  return GOOSEBERRY_SUCCESS;
+}
+
+template <int SCHED>
+int launch_a32_t(const gb_csr & a, unsigned grid, cudaStream_t s, bool pdl,
+    const float * r, const float * pold, float * pnew, float * ap, double * longdot,
+    double * partial, MixState * st) {
+  const size_t smem = smem_of(SCHED, a.plan.tile_items, 4);
+  auto kern = cg_a32_kernel<SCHED>;
+  GB_TRY(prep_kernel(kern, smem, nullptr));
+  GB_CUDA_TRY(launch_k(kern, grid, kSpmvBlock, smem, s, pdl, plan_view(a), a.rowptr,
+      a.rowind, a.val32, r, pold, pnew, ap, longdot, partial, st));
+  return GOOSEBERRY_SUCCESS;
+}
+
+template <int SCHED>
+int launch_r_t(const gb_csr & a, unsigned grid, cudaStream_t s, bool pdl, const double * b,
+    const double * x0, double * x1, const float * y, float * r32, double * longdot,
+    double * partial, MixState * st) {
+  const size_t smem = smem_of(SCHED, a.plan.tile_items, 8);
+  auto kern = cg_r_kernel<SCHED>;
+  GB_TRY(prep_kernel(kern, smem, nullptr));
+  GB_CUDA_TRY(launch_k(kern, grid, kSpmvBlock, smem, s, pdl, plan_view(a), a.rowptr,
+      a.rowind, a.val64, b, x0, x1, y, r32, longdot, partial, st));
+  return GOOSEBERRY_SUCCESS;
+}
+
+#define GB_SCHED_SWITCH(sched, CALL)                                            \
+  switch (sched) {                                                              \
+    case GB_SCHED_THREAD: return CALL(SCHED_THREAD);                            \
+    case GB_SCHED_GROUP4: return CALL(SCHED_GROUP4);                            \
+    case GB_SCHED_GROUP8: return CALL(SCHED_GROUP8);                            \
+    case GB_SCHED_WARP: return CALL(SCHED_WARP);                                \
+    case GB_SCHED_ROW: return CALL(SCHED_ROW);                                  \
+    case GB_SCHED_WTILE: return CALL(SCHED_WTILE);                              \
+    default: return CALL(SCHED_MERGE);                                          \
+  }
+
+template <int SCHED>
+int occ_a32_t(size_t smem, int * occ) { return prep_kernel(cg_a32_kernel<SCHED>, smem, occ); }
+template <int SCHED>
+int occ_r_t(size_t smem, int * occ) { return prep_kernel(cg_r_kernel<SCHED>, smem, occ); }
+
+}  // namespace
+
+// ---- the solver ------------------------------------------------------------------
+
+struct MixedCg {
+  const gb_csr * a = nullptr;
+  size_t n = 0;
+  int sched32 = GB_SCHED_MERGE, sched64 = GB_SCHED_MERGE;
+  uint32_t tile_items = 0;
+  double * x[2] = {nullptr, nullptr};
+  double * b = nullptr;
+  float * y = nullptr;
+  float * r = nullptr;
+  float * p[2] = {nullptr, nullptr};
+  float * ap = nullptr;
+  double * partial_a = nullptr;
+  double * partial_b = nullptr;
+  double * partial_r = nullptr;
+  double * partial_i = nullptr;
+  double * longdot = nullptr;
+  MixState * st = nullptr;
+  MixStatus * host_status = nullptr;
+  unsigned grid_a = 0, grid_b = 0, grid_r = 0;
+  int chunk = 32;
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+};
+
+namespace {
+
+int launch_a32(MixedCg * m, cudaStream_t s, bool pdl, int k) {
+  const float * pold = m->p[k & 1];
+  float * pnew = m->p[(k + 1) & 1];
+#define GB_CALL(S) launch_a32_t<S>(*m->a, m->grid_a, s, pdl, m->r, pold, pnew, m->ap, \
+                                   m->longdot, m->partial_a, m->st)
+  GB_SCHED_SWITCH(m->sched32, GB_CALL)
+#undef GB_CALL
+}
+
+int launch_r(MixedCg * m, cudaStream_t s, bool pdl) {
+#define GB_CALL(S) launch_r_t<S>(*m->a, m->grid_r, s, pdl, m->b, m->x[0], m->x[1], m->y, \
+                                 m->r, m->longdot, m->partial_r, m->st)
+  GB_SCHED_SWITCH(m->sched64, GB_CALL)
+#undef GB_CALL
+}
+
+int launch_b32(MixedCg * m, cudaStream_t s, bool pdl, int k) {
+  float * pnew = m->p[(k + 1) & 1];
+  GB_CUDA_TRY(launch_k(cg_b32_kernel, m->grid_b, kVecBlock, 0, s, pdl, m->n, m->y, m->r,
+      static_cast<const float *>(pnew), static_cast<const float *>(m->ap), m->partial_b,
+      m->st));
+  return GOOSEBERRY_SUCCESS;
+}
+
+int iteration(MixedCg * m, cudaStream_t s, bool pdl_first, int k) {
+  GB_TRY(launch_a32(m, s, pdl_first, k));
+  GB_TRY(launch_b32(m, s, true, k));
+  GB_TRY(launch_r(m, s, true));
+  return GOOSEBERRY_SUCCESS;
+}
+
+int capture(MixedCg * m, int slot) {
+  cudaStream_t cs = m->cap_stream;
+  GB_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+  int rc = GOOSEBERRY_SUCCESS;
+  for (int k = 0; k < m->chunk && rc == GOOSEBERRY_SUCCESS; ++k) rc = iteration(m, cs, k > 0, k);
+  if (rc == GOOSEBERRY_SUCCESS) {
+    cudaMemcpyAsync(&m->host_status[slot].done, &m->st->done, sizeof(int),
+        cudaMemcpyDeviceToHost, cs);
+    cudaMemcpyAsync(&m->host_status[slot].iter, &m->st->iter, sizeof(unsigned long long),
+        cudaMemcpyDeviceToHost, cs);
+  }
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(cs, &g);
+  if (rc != GOOSEBERRY_SUCCESS) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  GB_CUDA_TRY(e);
+  e = cudaGraphInstantiate(&m->graph[slot], g, 0);
+  cudaGraphDestroy(g);
+  GB_CUDA_TRY(e);
+  return GOOSEBERRY_SUCCESS;
+}
+
+int grid_of(const gb_csr * a, int sched, size_t smem, bool f32, unsigned * grid) {
+  int occ = 0;
+  if (f32) {
+#define GB_CALL(S) occ_a32_t<S>(smem, &occ)
+    int rc;
+    switch (sched) {
+      case GB_SCHED_THREAD: rc = GB_CALL(SCHED_THREAD); break;
+      case GB_SCHED_GROUP4: rc = GB_CALL(SCHED_GROUP4); break;
+      case GB_SCHED_GROUP8: rc = GB_CALL(SCHED_GROUP8); break;
+      case GB_SCHED_WARP: rc = GB_CALL(SCHED_WARP); break;
+      case GB_SCHED_ROW: rc = GB_CALL(SCHED_ROW); break;
+      case GB_SCHED_WTILE: rc = GB_CALL(SCHED_WTILE); break;
+      default: rc = GB_CALL(SCHED_MERGE); break;
+    }
+#undef GB_CALL
+    GB_TRY(rc);
+  } else {
+#define GB_CALL(S) occ_r_t<S>(smem, &occ)
+    int rc;
+    switch (sched) {
+      case GB_SCHED_THREAD: rc = GB_CALL(SCHED_THREAD); break;
+      case GB_SCHED_GROUP4: rc = GB_CALL(SCHED_GROUP4); break;
+      case GB_SCHED_GROUP8: rc = GB_CALL(SCHED_GROUP8); break;
+      case GB_SCHED_WARP: rc = GB_CALL(SCHED_WARP); break;
+      case GB_SCHED_ROW: rc = GB_CALL(SCHED_ROW); break;
+      case GB_SCHED_WTILE: rc = GB_CALL(SCHED_WTILE); break;
+      default: rc = GB_CALL(SCHED_MERGE); break;
+    }
+#undef GB_CALL
+    GB_TRY(rc);
+  }
+  GB_CHECK_INPUT(occ > 0, "mixed CG kernel cannot be resident");
+  const unsigned ntiles = static_cast<unsigned>(std::max<size_t>(a->plan.tiles.size(), 1));
+  const unsigned work = spmv_work_units(sched, a->nrows, ntiles, kSpmvBlock);
+  *grid = std::min<unsigned>(std::max(work, 1u), static_cast<unsigned>(a->sm_count * occ));
+  return GOOSEBERRY_SUCCESS;
+}
+
+}  // namespace
+
+void mixed_destroy(MixedCg * m) {
+  if (!m) return;
+  for (auto & g : m->graph)
+    if (g) cudaGraphExecDestroy(g);
+  if (m->cap_stream) cudaStreamDestroy(m->cap_stream);
+  cudaFree(m->x[0]);
+  cudaFree(m->x[1]);
+  cudaFree(m->b);
+  cudaFree(m->y);
+  cudaFree(m->r);
+  cudaFree(m->p[0]);
+  cudaFree(m->p[1]);
+  cudaFree(m->ap);
+  cudaFree(m->partial_a);
+  cudaFree(m->partial_b);
+  cudaFree(m->partial_r);
+  cudaFree(m->partial_i);
+  cudaFree(m->longdot);
+  cudaFree(m->st);
+  if (m->host_status) cudaFreeHost(m->host_status);
+  delete m;
+}
+
+int mixed_create(const gb_csr * a, MixedCg ** out) {
+  GB_CHECK_INPUT(a->val64 && a->val32,
+      "mixed-precision CG needs both double and float values on the matrix "
+      "(GB_CSR_VALUES_F64 | GB_CSR_VALUES_F32)");
+  MixedCg * m = new MixedCg();
+  *out = m;
+  m->a = a;
+  m->n = a->nrows;
+  m->sched32 = a->sched32;
+  m->sched64 = a->sched64;
+  m->tile_items = a->plan.tile_items;
+  const size_t n = std::max<size_t>(m->n, 2);
+  GB_CUDA_TRY(cudaMalloc(&m->x[0], n * sizeof(double)));
+  GB_CUDA_TRY(cudaMalloc(&m->x[1], n * sizeof(double)));
+  GB_CUDA_TRY(cudaMalloc(&m->b, n * sizeof(double)));
+  GB_CUDA_TRY(cudaMalloc(&m->y, n * sizeof(float)));
+  GB_CUDA_TRY(cudaMalloc(&m->r, n * sizeof(float)));
+  GB_CUDA_TRY(cudaMalloc(&m->p[0], n * sizeof(float)));
+  GB_CUDA_TRY(cudaMalloc(&m->p[1], n * sizeof(float)));
+  GB_CUDA_TRY(cudaMalloc(&m->ap, n * sizeof(float)));
+  GB_TRY(grid_of(a, m->sched32, smem_of(m->sched32, m->tile_items, 4), true, &m->grid_a));
+  GB_TRY(grid_of(a, m->sched64, smem_of(m->sched64, m->tile_items, 8), false, &m->grid_r));
+  int occ_b = 0;
+  GB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, cg_b32_kernel, kVecBlock, 0));
+  m->grid_b = static_cast<unsigned>(std::max<size_t>(1, std::min<size_t>(
+      (m->n + kVecBlock - 1) / kVecBlock, static_cast<size_t>(a->sm_count) * std::max(occ_b, 1))));
+  const unsigned gmax = std::max({m->grid_a, m->grid_b, m->grid_r, 1u});
+  GB_CUDA_TRY(cudaMalloc(&m->partial_a, gmax * sizeof(double)));
+  GB_CUDA_TRY(cudaMalloc(&m->partial_b, gmax * sizeof(double)));
+  GB_CUDA_TRY(cudaMalloc(&m->partial_r, gmax * sizeof(double)));
+  GB_CUDA_TRY(cudaMalloc(&m->partial_i, 2 * gmax * sizeof(double)));
+  GB_CUDA_TRY(cudaMalloc(&m->longdot,
+      std::max<size_t>(a->plan.longrows.size(), 1) * sizeof(double)));
+  GB_CUDA_TRY(cudaMalloc(&m->st, sizeof(MixState)));
+  GB_CUDA_TRY(cudaMemset(m->st, 0, sizeof(MixState)));
+  GB_CUDA_TRY(cudaMallocHost(&m->host_status, 2 * sizeof(MixStatus)));
+  GB_CUDA_TRY(cudaStreamCreateWithFlags(&m->cap_stream, cudaStreamNonBlocking));
+  GB_TRY(capture(m, 0));
+  GB_TRY(capture(m, 1));
+  return GOOSEBERRY_SUCCESS;
+}
+
+namespace {
+
+int mixed_start(MixedCg * m, const double * b, double tol, int tol_relative, size_t niter,
+    double * dhist, size_t hl, cudaStream_t stream) {
+  const size_t cap = std::max<size_t>(1000, 100 * m->n);
+  MixState init{};
+  init.tol = tol;
+  init.niter = niter ? niter : cap;
+  init.hist = dhist;
+  init.hist_len = hl;
+  GB_CUDA_TRY(cudaMemcpyAsync(m->st, &init, sizeof(MixState), cudaMemcpyHostToDevice, stream));
+  GB_CUDA_TRY(cudaMemcpyAsync(m->b, b, m->n * sizeof(double), cudaMemcpyDeviceToDevice,
+      stream));
+  cg_mixed_init_kernel<<<m->grid_b, kVecBlock, 0, stream>>>(m->n, m->b, m->x[0], m->r,
+      m->p[0], m->partial_i, m->st, tol_relative);
+  GB_CUDA_TRY(cudaGetLastError());
+  return GOOSEBERRY_SUCCESS;
+}
+
+}  // namespace
+
+int mixed_solve(MixedCg * m, const double * b, double * x, double tol, int tol_relative,
+    size_t niter, double * history, size_t history_len, gb_cg_result_t * res,
+    cudaStream_t stream) {
+  GB_CHECK_INPUT(m->n == 0 || (b && x), "NULL vector");
+  GB_CHECK_INPUT(m->a->sched32 == m->sched32 && m->a->sched64 == m->sched64 &&
+                 m->a->plan.tile_items == m->tile_items,
+      "matrix schedule changed after the solver was created");
+  if (m->n == 0) {
+    if (res) *res = gb_cg_result_t{0, 0, 0.0, 0.0, GB_CG_CONVERGED, 0};
+    return GOOSEBERRY_SUCCESS;
+  }
+  double * dhist = nullptr;
+  const size_t hl = history ? std::min(history_len, niter ? niter : history_len) : 0;
+  if (hl) GB_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&dhist), hl * sizeof(double),
+      stream));
+  GB_TRY(mixed_start(m, b, tol, tol_relative, niter, dhist, hl, stream));
+  size_t launches = 1;
+  cudaEvent_t ev[2];
+  GB_CUDA_TRY(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+  GB_CUDA_TRY(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+  m->host_status[0].done = m->host_status[1].done = 0;
+  int rc = GOOSEBERRY_SUCCESS;
+  auto launch = [&](int slot) -> int {
+    cudaError_t e = cudaGraphLaunch(m->graph[slot], stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[slot], stream);
+    launches += 3 * static_cast<size_t>(m->chunk);
+    if (e != cudaSuccess) {
+      set_error("mixed CG graph launch failed: %s", cudaGetErrorString(e));
+      return GOOSEBERRY_ERROR_UNKNOWN;
+    }
+    return GOOSEBERRY_SUCCESS;
+  };
+  rc = launch(0);
+  if (rc == GOOSEBERRY_SUCCESS) rc = launch(1);
+  int slot = 0;
+  while (rc == GOOSEBERRY_SUCCESS) {
+    cudaError_t e = cudaEventSynchronize(ev[slot]);
+    if (e != cudaSuccess) {
+      set_error("mixed CG solve failed: %s", cudaGetErrorString(e));
+      rc = GOOSEBERRY_ERROR_UNKNOWN;
+      break;
+    }
+    if (m->host_status[slot].done) break;
+    rc = launch(slot);
+    slot ^= 1;
+  }
+  cudaError_t e = cudaStreamSynchronize(stream);
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  if (rc == GOOSEBERRY_SUCCESS && e != cudaSuccess) {
+    set_error("mixed CG solve failed: %s", cudaGetErrorString(e));
+    rc = GOOSEBERRY_ERROR_UNKNOWN;
+  }
+  MixState fin{};
+  if (rc == GOOSEBERRY_SUCCESS) {
+    e = cudaMemcpy(&fin, m->st, sizeof(MixState), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && fin.status != GB_CG_CONVERGED && fin.status != GB_CG_NONFINITE &&
+        fin.y_reset == 0) {
+      // stopped on the iteration limit (or breakdown) with a pending FP32
+      // correction: fold it into x once more and measure the true residual
+      const int one = 1;
+      e = cudaMemcpyAsync(&m->st->force, &one, sizeof(int), cudaMemcpyHostToDevice, stream);
+      if (e == cudaSuccess) {
+        rc = launch_r(m, stream, false);
+        launches += 1;
+      }
+      if (e == cudaSuccess && rc == GOOSEBERRY_SUCCESS) e = cudaStreamSynchronize(stream);
+      if (e == cudaSuccess && rc == GOOSEBERRY_SUCCESS)
+        e = cudaMemcpy(&fin, m->st, sizeof(MixState), cudaMemcpyDeviceToHost);
+    }
+    if (e == cudaSuccess && rc == GOOSEBERRY_SUCCESS)
+      e = cudaMemcpyAsync(x, m->x[fin.xpar], m->n * sizeof(double), cudaMemcpyDeviceToDevice,
+          stream);
+    if (e == cudaSuccess && rc == GOOSEBERRY_SUCCESS && hl && fin.iter)
+      e = cudaMemcpyAsync(history, dhist, std::min<size_t>(hl, fin.iter) * sizeof(double),
+          cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess && rc == GOOSEBERRY_SUCCESS) e = cudaStreamSynchronize(stream);
+    if (rc == GOOSEBERRY_SUCCESS && e != cudaSuccess) {
+      set_error("mixed CG result copy failed: %s", cudaGetErrorString(e));
+      rc = GOOSEBERRY_ERROR_UNKNOWN;
+    }
+  }
+  if (rc == GOOSEBERRY_SUCCESS && res) {
+    res->iterations = fin.iter;
+    res->refinements = fin.refinements;
+    res->rnorm = std::sqrt(fin.rr_true);
+    res->bnorm = fin.bnorm;
+    res->status = fin.status;
+    res->kernel_launches = launches;
+  }
+  if (dhist) cudaFreeAsync(dhist, stream);
+  return rc;
+}
+
+int mixed_profile(MixedCg * m, const double * b, size_t iterations, double * ms,
+    size_t ms_len, size_t * nkernels, cudaStream_t stream) {
+  GB_CHECK_INPUT(m->n > 0 && b != nullptr, "profile needs a non-empty system and b");
+  GB_CHECK_INPUT(iterations > 0, "iterations must be positive");
+  if (nkernels) *nkernels = 3;
+  GB_TRY(mixed_start(m, b, 0.0, 0, 0, nullptr, 0, stream));
+  std::vector<cudaEvent_t> ev(4 * iterations);
+  for (auto & e : ev) GB_CUDA_TRY(cudaEventCreate(&e));
+  int rc = GOOSEBERRY_SUCCESS;
+  const int one = 1;
+  for (size_t k = 0; k < iterations && rc == GOOSEBERRY_SUCCESS; ++k) {
+    // the FP64 refinement kernel is forced to run so every iteration times it
+    cudaMemcpyAsync(&m->st->force, &one, sizeof(int), cudaMemcpyHostToDevice, stream);
+    cudaEventRecord(ev[4 * k], stream);
+    rc = launch_a32(m, stream, false, static_cast<int>(k));
+    cudaEventRecord(ev[4 * k + 1], stream);
+    if (rc == GOOSEBERRY_SUCCESS) rc = launch_b32(m, stream, false, static_cast<int>(k));
+    cudaEventRecord(ev[4 * k + 2], stream);
+    if (rc == GOOSEBERRY_SUCCESS) rc = launch_r(m, stream, false);
+    cudaEventRecord(ev[4 * k + 3], stream);
+  }
+  cudaError_t e = cudaStreamSynchronize(stream);
+  if (rc == GOOSEBERRY_SUCCESS && e != cudaSuccess) {
+    set_error("mixed CG profile failed: %s", cudaGetErrorString(e));
+    rc = GOOSEBERRY_ERROR_UNKNOWN;
+  }
+  if (rc == GOOSEBERRY_SUCCESS) {
+    double t[3] = {0, 0, 0};
+    for (size_t k = 0; k < iterations; ++k)
+      for (int j = 0; j < 3; ++j) {
+        float v = 0.f;
+        cudaEventElapsedTime(&v, ev[4 * k + j], ev[4 * k + j + 1]);
+        t[j] += v;
+      }
+    for (size_t j = 0; j < 3 && j < ms_len; ++j) ms[j] = t[j] / iterations;
+  }
+  for (auto & ee : ev) cudaEventDestroy(ee);
+  return rc;
+}
+
+}  // namespace gb

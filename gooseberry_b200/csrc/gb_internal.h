@@ -157,4 +157,14 @@ int launch_round_f32(const double * in, float * out, size_t n, cudaStream_t stre
 
 int sm_count_of_current_device(int * out);
 
+// Mixed-precision CG (cg_mixed.cu), owned by a gb_cg created with GB_CG_MIXED.
+struct MixedCg;
+int mixed_create(const gb_csr * a, MixedCg ** out);
+void mixed_destroy(MixedCg * m);
+int mixed_solve(MixedCg * m, const double * b, double * x, double tol, int tol_relative,
+    size_t niter, double * history, size_t history_len, gb_cg_result_t * res,
+    cudaStream_t stream);
+int mixed_profile(MixedCg * m, const double * b, size_t iterations, double * ms,
+    size_t ms_len, size_t * nkernels, cudaStream_t stream);
+
 }  // namespace gb

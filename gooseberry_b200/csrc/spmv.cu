@@ -200,6 +200,12 @@ int occupancy(const void * func, size_t smem, int * out) {
     *out = it->second;
     return GOOSEBERRY_SUCCESS;
   }
+  int dev = 0, max_smem = 0;
+  GB_CUDA_TRY(cudaGetDevice(&dev));
+  GB_CUDA_TRY(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  GB_CHECK_INPUT(smem <= static_cast<size_t>(max_smem),
+      "this schedule needs %zu bytes of shared memory per CTA at this tile size; the "
+      "device allows %d (choose smaller tile_items)", smem, max_smem);
   if (smem > 48 * 1024)
     GB_CUDA_TRY(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize,
         static_cast<int>(smem)));
@@ -219,12 +225,11 @@ int launch_tiles(const gb_csr & a, const V * val, const Gather & g, const Out & 
     cudaStream_t stream) {
   if (a.plan.tiles.empty()) return GOOSEBERRY_SUCCESS;
   auto kern = spmv_tiles_kernel<V, Acc, SCHED, Gather, Out>;
-  const size_t smem = SCHED == SCHED_ROW ? 0 : TileSmem<V, Acc>::bytes(a.plan.tile_items);
+  const size_t smem = spmv_smem_bytes<V, Acc>(SCHED, a.plan.tile_items, kSpmvBlock);
   int occ = 0;
   GB_TRY(occupancy(reinterpret_cast<const void *>(kern), smem, &occ));
-  const uint32_t units = SCHED == SCHED_ROW
-      ? (a.nrows + kSpmvBlock - 1) / kSpmvBlock
-      : static_cast<uint32_t>(a.plan.tiles.size());
+  const uint32_t units = spmv_work_units(SCHED, a.nrows,
+      static_cast<uint32_t>(a.plan.tiles.size()), kSpmvBlock);
   const uint32_t grid = std::min<uint32_t>(units, static_cast<uint32_t>(a.sm_count * occ));
   kern<<<grid, kSpmvBlock, smem, stream>>>(plan_view(a), a.rowptr, a.rowind, val, g, o);
   GB_CUDA_TRY(cudaGetLastError());
@@ -241,6 +246,7 @@ int launch_sched(const gb_csr & a, int sched, const V * val, const Gather & g,
     case GB_SCHED_WARP: return launch_tiles<V, Acc, SCHED_WARP>(a, val, g, o, stream);
     case GB_SCHED_MERGE: return launch_tiles<V, Acc, SCHED_MERGE>(a, val, g, o, stream);
     case GB_SCHED_ROW: return launch_tiles<V, Acc, SCHED_ROW>(a, val, g, o, stream);
+    case GB_SCHED_WTILE: return launch_tiles<V, Acc, SCHED_WTILE>(a, val, g, o, stream);
     default:
       set_error("unknown SpMV schedule %d", sched);
       return GOOSEBERRY_ERROR_INVALIDINPUT;
@@ -355,22 +361,32 @@ int autotune(gb_csr & a, unsigned width, cudaStream_t stream) {
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  const uint32_t tiles_opts[] = {1024, 2048, 4096};
-  const int sched_opts[] = {GB_SCHED_ROW, GB_SCHED_THREAD, GB_SCHED_GROUP4, GB_SCHED_GROUP8,
-                            GB_SCHED_WARP, GB_SCHED_MERGE};
+  // (tile_items, schedule) candidates: CTA tiles are large, per-warp tiles
+  // small, the row schedule ignores tiles
+  struct Cand {
+    uint32_t tile;
+    int sched;
+  };
+  std::vector<Cand> cands;
+  const bool short_rows = a.plan.p99 <= 64 && a.plan.max_row <= 4096;
+  if (short_rows) cands.push_back({1024, GB_SCHED_ROW});
+  for (uint32_t t : {128u, 256u, 512u}) cands.push_back({t, GB_SCHED_WTILE});
+  for (uint32_t t : {1024u, 2048u, 4096u}) {
+    if (a.plan.p90 <= 64) cands.push_back({t, GB_SCHED_THREAD});
+    cands.push_back({t, GB_SCHED_GROUP4});
+    cands.push_back({t, GB_SCHED_GROUP8});
+    if (a.plan.p50 >= 8) cands.push_back({t, GB_SCHED_WARP});
+    cands.push_back({t, GB_SCHED_MERGE});
+  }
   float best = 1e30f;
   TuneChoice choice{default_schedule(a.plan), a.plan.tile_items};
   int rc = GOOSEBERRY_SUCCESS;
-  for (uint32_t ti : tiles_opts) {
-    rc = rebuild_plan(a, ti, stream);
+  for (const Cand & cd : cands) {
+    rc = rebuild_plan(a, cd.tile, stream);
     if (rc != GOOSEBERRY_SUCCESS) break;
-    for (int s : sched_opts) {
-      // skip schedules that cannot suit this matrix (the row schedule does
-      // not use tiles: time it once)
-      if (s == GB_SCHED_ROW && (ti != tiles_opts[0] || a.plan.p99 > 64 ||
-                                a.plan.max_row > 4096)) continue;
-      if (s == GB_SCHED_THREAD && a.plan.p90 > 64) continue;
-      if (s == GB_SCHED_WARP && a.plan.p50 < 8) continue;
+    {
+      const int s = cd.sched;
+      const uint32_t ti = cd.tile;
       auto run = [&]() {
         return width == GB_CSR_VALUES_F32
                    ? launch_spmv_f32(a, s, static_cast<const float *>(x),
@@ -577,10 +593,16 @@ int gb_csr_get_info(const gb_csr_t * a, gb_csr_info_t * info) {
 int gb_csr_set_schedule(gb_csr_t * a, unsigned value_width, int schedule,
     uint32_t tile_items) {
   GB_CHECK_INPUT(a != nullptr, "matrix is NULL");
-  GB_CHECK_INPUT(schedule >= GB_SCHED_AUTO && schedule <= GB_SCHED_ROW,
+  GB_CHECK_INPUT(schedule >= GB_SCHED_AUTO && schedule <= GB_SCHED_WTILE,
       "unknown schedule %d", schedule);
   GB_CHECK_INPUT(value_width == GB_CSR_VALUES_F64 || value_width == GB_CSR_VALUES_F32,
       "value_width must be GB_CSR_VALUES_F64 or GB_CSR_VALUES_F32");
+  // per-warp tiles keep two stages per warp in shared memory: they need small
+  // tiles, so a plan built for CTA tiles is rebuilt at 256 items
+  if (schedule == GB_SCHED_WTILE && tile_items == 0 && a->plan.tile_items > 512)
+    tile_items = 256;
+  GB_CHECK_INPUT(schedule != GB_SCHED_WTILE || (tile_items ? tile_items : a->plan.tile_items) <= 512,
+      "per-warp tiles need tile_items <= 512");
   if (tile_items) GB_TRY(gb::rebuild_plan(*a, tile_items, nullptr));
   const int s = schedule == GB_SCHED_AUTO ? gb::default_schedule(a->plan) : schedule;
   (value_width == GB_CSR_VALUES_F32 ? a->sched32 : a->sched64) = s;

@@ -39,7 +39,8 @@ enum : int {
   SCHED_GROUP8 = GB_SCHED_GROUP8,
   SCHED_WARP = GB_SCHED_WARP,
   SCHED_MERGE = GB_SCHED_MERGE,
-  SCHED_ROW = GB_SCHED_ROW
+  SCHED_ROW = GB_SCHED_ROW,
+  SCHED_WTILE = GB_SCHED_WTILE
 };
 
 constexpr int kSpmvBlock = 256;
@@ -491,9 +492,152 @@ __device__ __forceinline__ void spmv_row_loop(uint32_t first, uint32_t end, uint
   }
 }
 
-// Round-robin driver: CTA b runs tiles b, b + gridDim.x, ... (or, for the
-// row schedule, rows in a grid-stride loop); then out.finish() once per
-// thread.
+// ---- per-warp tiles -----------------------------------------------------------
+//
+// Each warp is an independent pipeline over its own small row-aligned tiles:
+// while its lanes sum tile t, cp.async already streams tile t + step (rowptr
+// slice, indices, values) into the warp's other shared-memory stage.  Only
+// warp-level synchronisation is needed, so every warp of the SM keeps its own
+// tile in flight (the CTA-wide tile loop above has one per CTA).  A lane sums
+// whole rows, k ascending with unfused multiply and add, exactly like the
+// reference (src/blas.c:85-88): the result is bit-identical to blas_spmult.
+// kStage x values are gathered per lane before any is consumed.
+
+template <typename V>
+struct WarpSmem {
+  static __host__ __device__ size_t stage_bytes(uint32_t t) {
+    return ((sizeof(uint32_t) * (t + 1) + 15) & ~size_t(15)) +
+           ((sizeof(uint32_t) * t + 15) & ~size_t(15)) + ((sizeof(V) * t + 15) & ~size_t(15));
+  }
+  static __host__ __device__ size_t bytes(uint32_t t, int warps) {
+    return static_cast<size_t>(warps) * 2 * stage_bytes(t);
+  }
+};
+
+template <typename V, typename Acc, class Gather, class Out>
+__device__ __forceinline__ void spmv_warp_loop(const PlanView & plan, uint32_t t_first,
+    uint32_t t_end, uint32_t t_step, const uint32_t * __restrict__ rowptr,
+    const uint32_t * __restrict__ rowind, const V * __restrict__ val, const Gather & gather,
+    Out & out, uint64_t pol_matrix, uint64_t pol_x) {
+  extern __shared__ __align__(16) unsigned char gb_smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t T = plan.tile_items;
+  const size_t sb = WarpSmem<V>::stage_bytes(T);
+  const size_t offs_b = (sizeof(uint32_t) * (T + 1) + 15) & ~size_t(15);
+  const size_t ind_b = (sizeof(uint32_t) * T + 15) & ~size_t(15);
+  unsigned char * mine = gb_smem + static_cast<size_t>(warp) * 2 * sb;
+  const uint32_t cmax = plan.ncols - 1;
+
+  auto offs_of = [&](int s) { return reinterpret_cast<uint32_t *>(mine + s * sb); };
+  auto ind_of = [&](int s) { return reinterpret_cast<uint32_t *>(mine + s * sb + offs_b); };
+  auto val_of = [&](int s) { return reinterpret_cast<V *>(mine + s * sb + offs_b + ind_b); };
+
+  auto issue = [&](uint32_t t, int s) {
+    const TileDesc d = plan.tiles[t];
+    if (d.row_count != 0) {
+      uint32_t * so = offs_of(s);
+      uint32_t * si = ind_of(s);
+      V * sv = val_of(s);
+      for (uint32_t r = lane; r <= d.row_count; r += 32)
+        cp_async4(so + r, rowptr + d.row_begin + r, pol_matrix);
+      for (uint32_t k = lane; k < d.nnz_count; k += 32) {
+        cp_async4(si + k, rowind + d.nnz_begin + k, pol_matrix);
+        cp_async_v(sv + k, val + d.nnz_begin + k, pol_matrix);
+      }
+    }
+    cp_async_commit();
+  };
+
+  if (t_first < t_end) issue(t_first, 0);
+  int s = 0;
+  for (uint32_t t = t_first; t < t_end; t += t_step) {
+    const uint32_t tn = t + t_step;
+    if (tn < t_end) issue(tn, s ^ 1); else cp_async_commit();
+    cp_async_wait<1>();
+    __syncwarp();
+    const TileDesc d = plan.tiles[t];
+    const uint32_t nb = d.nnz_begin;
+    if (d.row_count == 0) {
+      // chunk of a long row: the warp sums it, then last-arrival combine
+      const int N = static_cast<int>(d.nnz_count);
+      Acc sum = Acc(0);
+      for (int base = 0; base < N; base += kStage * 32) {
+        uint32_t c[kStage];
+        V v[kStage];
+#pragma unroll
+        for (int j = 0; j < kStage; ++j) {
+          const int k = base + lane + j * 32;
+          if (k < N) {
+            c[j] = ld_stream(rowind + nb + k, pol_matrix);
+            v[j] = ld_stream(val + nb + k, pol_matrix);
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < kStage; ++j) {
+          const int k = base + lane + j * 32;
+          if (k < N) sum += static_cast<Acc>(v[j]) * gather(min(c[j], cmax), pol_x);
+        }
+      }
+      sum = group_sum<32>(sum);
+      if (lane == 0) {
+        plan.chunk_partial[t] = static_cast<double>(sum);
+        __threadfence();
+        const LongRowDesc L = plan.longrows[d.row_begin];
+        const unsigned prev = atomicAdd(plan.long_count + d.row_begin, 1u);
+        if (prev == L.nchunks - 1) {
+          __threadfence();
+          Acc tot = Acc(0);
+          for (uint32_t q = 0; q < L.nchunks; ++q)
+            tot += static_cast<Acc>(__ldcg(plan.chunk_partial + L.first_tile + q));
+          plan.long_count[d.row_begin] = 0u;  // ready for the next launch
+          out.long_row(d.row_begin, L.row, tot);
+        }
+      }
+    } else {
+      const uint32_t * so = offs_of(s);
+      const uint32_t * si = ind_of(s);
+      const V * sv = val_of(s);
+      for (uint32_t r = lane; r < d.row_count; r += 32) {
+        const uint32_t i = d.row_begin + r;
+        const typename Out::Pre pre = out.pre(i);
+        const uint32_t b = so[r] - nb, e = so[r + 1] - nb;
+        Acc sum = Acc(0);
+        for (uint32_t base = b; base < e; base += kStage) {
+          Acc xv[kStage];
+#pragma unroll
+          for (int j = 0; j < kStage; ++j)
+            if (base + j < e) xv[j] = gather(min(si[base + j], cmax), pol_x);
+#pragma unroll
+          for (int j = 0; j < kStage; ++j)
+            if (base + j < e) sum = add_rn(sum, mul_rn(static_cast<Acc>(sv[base + j]), xv[j]));
+        }
+        out.row_pre(i, sum, pre);
+      }
+    }
+    __syncwarp();  // stage s is free again
+    s ^= 1;
+  }
+  cp_async_wait<0>();
+}
+
+// Dynamic shared memory a schedule needs per CTA.
+template <typename V, typename Acc>
+__host__ __device__ inline size_t spmv_smem_bytes(int sched, uint32_t tile_items, int block) {
+  if (sched == SCHED_ROW) return 0;
+  if (sched == SCHED_WTILE) return WarpSmem<V>::bytes(tile_items, block / 32);
+  return TileSmem<V, Acc>::bytes(tile_items);
+}
+
+// Work units a schedule distributes over CTAs (for the grid size).
+inline uint32_t spmv_work_units(int sched, uint32_t nrows, uint32_t ntiles, int block) {
+  if (sched == SCHED_ROW) return (nrows + block - 1) / block;
+  if (sched == SCHED_WTILE) return (ntiles + block / 32 - 1) / (block / 32);
+  return ntiles;
+}
+
+// Round-robin driver: CTA b runs tiles b, b + gridDim.x, ... (for the row
+// schedule rows in a grid-stride loop, for per-warp tiles warp w of CTA b
+// runs tiles b * warps + w, ...); then out.finish() once per thread.
 template <typename V, typename Acc, int SCHED, int BLOCK, class Gather, class Out>
 __device__ __forceinline__ void spmv_tiles_body(const PlanView plan,
     const uint32_t * __restrict__ rowptr, const uint32_t * __restrict__ rowind,
@@ -501,6 +645,11 @@ __device__ __forceinline__ void spmv_tiles_body(const PlanView plan,
   if (SCHED == SCHED_ROW) {
     spmv_row_loop<V, Acc>(blockIdx.x * BLOCK + threadIdx.x, plan.nrows, gridDim.x * BLOCK,
         plan.ncols, rowptr, rowind, val, gather, out, policy_evict_first(),
+        policy_evict_last());
+  } else if (SCHED == SCHED_WTILE) {
+    constexpr int W = BLOCK / 32;
+    spmv_warp_loop<V, Acc>(plan, blockIdx.x * W + (threadIdx.x >> 5), plan.ntiles,
+        gridDim.x * W, rowptr, rowind, val, gather, out, policy_evict_first(),
         policy_evict_last());
   } else {
     spmv_tile_loop<V, Acc, SCHED, BLOCK>(plan, blockIdx.x, plan.ntiles, gridDim.x, rowptr,

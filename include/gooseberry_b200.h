@@ -71,10 +71,15 @@ typedef enum gb_schedule {
   GB_SCHED_GROUP8 = 3,   /* 8 lanes per row                                  */
   GB_SCHED_WARP = 4,     /* 32 lanes per row                                 */
   GB_SCHED_MERGE = 5,    /* merge-path split of rows+nnz over threads        */
-  GB_SCHED_ROW = 6       /* one thread per row straight from global memory,
+  GB_SCHED_ROW = 6,      /* one thread per row straight from global memory,
                             no tile staging; sums each row in the reference's
                             order (k ascending, unfused multiply and add), so
                             its SpMV is bit-identical to the reference       */
+  GB_SCHED_WTILE = 7     /* per-WARP tiles (small tile_items, ~256): each
+                            warp streams its next tile into its own shared
+                            memory stage with cp.async while its lanes sum
+                            the current tile's rows, one row per lane, in
+                            the reference's order (bit-identical, like ROW) */
 } gb_schedule_t;
 
 /*

@@ -95,7 +95,7 @@ def test_persistent_and_graph_paths_agree(torch, cg_golden):
         b = torch.from_numpy(c["b"]).cuda()
         out = {}
         for pers in (False, True):
-            for sched in (gb.SCHED_ROW, gb.SCHED_THREAD, gb.SCHED_MERGE):
+            for sched in (gb.SCHED_ROW, gb.SCHED_THREAD, gb.SCHED_MERGE, gb.SCHED_WTILE):
                 A = gb.CsrMatrix.from_host(rowptr=c["rowptr"], rowind=c["rowind"],
                                            rowval=c["rowval"])
                 A.set_schedule(sched, tile_items=256)

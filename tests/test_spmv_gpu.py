@@ -20,7 +20,7 @@ pytestmark = pytest.mark.gpu
 TOL64 = 1e-13
 TOL32 = 64 * 2.0 ** -24
 SCHEDS = [gb.SCHED_THREAD, gb.SCHED_GROUP4, gb.SCHED_GROUP8, gb.SCHED_WARP, gb.SCHED_MERGE,
-          gb.SCHED_ROW]
+          gb.SCHED_ROW, gb.SCHED_WTILE]
 
 
 @pytest.fixture(scope="module")
@@ -43,7 +43,7 @@ def test_golden_cases_all_schedules_f64(torch, spmv_golden):
         x = _dev(torch, c["x"])
         for tile in (256, 2048):
             for s in SCHEDS:
-                A.set_schedule(s, tile_items=tile)
+                A.set_schedule(s, tile_items=tile if s != gb.SCHED_WTILE else max(64, tile // 8))
                 y = A.spmv(x).cpu().numpy()
                 err = cond_scaled_err(y, c["y64"], c["rowptr"], c["rowind"], c["rowval"], c["x"])
                 assert err <= TOL64, (name, s, tile, err)
@@ -52,19 +52,27 @@ def test_golden_cases_all_schedules_f64(torch, spmv_golden):
         A.close()
 
 
-def test_row_schedule_is_bit_identical_to_reference(torch, spmv_golden):
-    """The row schedule sums each row in the reference's order without fused
-    multiply-adds, so its y equals blas_spmult's bit for bit (f64 and f32)."""
+@pytest.mark.parametrize("sched,tile", [(gb.SCHED_ROW, 2048), (gb.SCHED_WTILE, 128),
+                                        (gb.SCHED_WTILE, 256), (gb.SCHED_WTILE, 512)])
+def test_reference_order_schedules_are_bit_identical(torch, spmv_golden, sched, tile):
+    """The row and per-warp-tile schedules sum each row in the reference's
+    order without fused multiply-adds, so their y equals blas_spmult's bit for
+    bit (f64 and f32 builds); rows too long for a tile are chunked instead and
+    checked to the usual bound."""
     for name, c in spmv_golden.items():
         if "rowptr" not in c:
             continue
         A = gb.CsrMatrix.from_host(rowptr=c["rowptr"], rowind=c["rowind"], rowval=c["rowval"],
                                    f64=True, f32=True)
-        A.set_schedule(gb.SCHED_ROW)
-        A.set_schedule(gb.SCHED_ROW, f32=True)
+        A.set_schedule(sched, tile_items=tile)
+        A.set_schedule(sched, f32=True)
         y = A.spmv(_dev(torch, c["x"])).cpu().numpy()
-        assert np.array_equal(y, c["y64"]), name
         y32 = A.spmv(_dev(torch, c["x"].astype(np.float32))).cpu().numpy()
+        if sched == gb.SCHED_WTILE and A.info().nlong > 0:
+            assert cond_scaled_err(y, c["y64"], c["rowptr"], c["rowind"], c["rowval"],
+                                   c["x"]) <= TOL64, name
+            continue
+        assert np.array_equal(y, c["y64"]), name
         assert np.array_equal(y32, c["y32"]), name
 
 
@@ -142,8 +150,9 @@ def test_powerlaw_long_rows(torch):
     M = gb.CsrMatrix.from_host(A, f64=True, f32=True)
     assert M.info().nlong > 0
     xd = _dev(torch, x)
-    for s in (gb.SCHED_MERGE, gb.SCHED_GROUP8, gb.SCHED_THREAD):
-        M.set_schedule(s)
+    for s, t in ((gb.SCHED_MERGE, 2048), (gb.SCHED_GROUP8, 2048), (gb.SCHED_THREAD, 2048),
+                 (gb.SCHED_WTILE, 256)):
+        M.set_schedule(s, tile_items=t)
         y = M.spmv(xd).cpu().numpy()
         assert cond_scaled_err(y, y_ref, A.rowptr, A.rowind, A.rowval, x) <= TOL64, s
         assert np.array_equal(y, M.spmv(xd).cpu().numpy())
