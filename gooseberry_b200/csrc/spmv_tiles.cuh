@@ -86,6 +86,23 @@ __device__ __forceinline__ float ld_stream(const float * p, uint64_t pol) {
                : "=f"(v) : "l"(p), "l"(pol));
   return v;
 }
+// Read-only loads that DO allocate in L1 (for access patterns where several
+// instructions of a warp touch the same sector, e.g. one row per lane).
+__device__ __forceinline__ uint32_t ld_l1(const uint32_t * p, uint64_t pol) {
+  uint32_t v;
+  asm volatile("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ double ld_l1(const double * p, uint64_t pol) {
+  double v;
+  asm volatile("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ float ld_l1(const float * p, uint64_t pol) {
+  float v;
+  asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+  return v;
+}
 __device__ __forceinline__ double ld_keep(const double * p, uint64_t pol) {
   double v;
   asm volatile("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;"
@@ -435,8 +452,8 @@ __device__ __forceinline__ void row_stage_load(RowStage<V> & s, const uint32_t *
 #pragma unroll
   for (int j = 0; j < kRowStage; ++j) {
     if (s.b + j < s.e) {
-      s.c[j] = ld_stream(rowind + s.b + j, pol);
-      s.v[j] = ld_stream(val + s.b + j, pol);
+      s.c[j] = ld_l1(rowind + s.b + j, pol);
+      s.v[j] = ld_l1(val + s.b + j, pol);
     }
   }
 }
@@ -484,8 +501,8 @@ __device__ __forceinline__ void spmv_row_loop(uint32_t first, uint32_t end, uint
     for (int j = 0; j < kRowStage; ++j)
       if (cur.b + j < cur.e) sum = add_rn(sum, mul_rn(static_cast<Acc>(cur.v[j]), xv[j]));
     for (uint32_t k = cur.b + kRowStage; k < cur.e; ++k)  // long-row tail
-      sum = add_rn(sum, mul_rn(static_cast<Acc>(ld_stream(val + k, pol_matrix)),
-                               gather(min(ld_stream(rowind + k, pol_matrix), cmax), pol_x)));
+      sum = add_rn(sum, mul_rn(static_cast<Acc>(ld_l1(val + k, pol_matrix)),
+                               gather(min(ld_l1(rowind + k, pol_matrix), cmax), pol_x)));
     out.row_pre(i, sum, cur_pre);
     cur = nxt;
     cur_pre = nxt_pre;
