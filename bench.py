@@ -341,6 +341,257 @@ def run_cg_laplace(args, dist: Dist):
     return out
 
 
+def _spmv_bytes(n, nnz, s_v, s_x):
+    # 4(n+1) rowptr + nnz (index + value) + x once + y once
+    return 4 * (n + 1) + nnz * (4 + s_v) + n * s_x + n * s_x
+
+
+def _cond_err(y, y_ref, A, x):
+    import scipy.sparse as sp
+    S = sp.csr_matrix((np.abs(A.rowval), A.rowind.astype(np.int64),
+                       A.rowptr.astype(np.int64)), shape=(A.nrows, A.ncols))
+    scale = S @ np.abs(x.astype(np.float64))
+    return float(np.max(np.abs(y.astype(np.float64) - y_ref) / np.maximum(scale, 1e-300)))
+
+
+def measure_spmv(A, x, reps=20, f32=False, flush=None, schedule=None):
+    """Device time of one SpMV (CUDA events, L2 flushed before each rep).
+    Returns (ms, y, info)."""
+    import torch
+
+    import gooseberry_b200 as gb
+    M = gb.CsrMatrix.from_host(A, f64=not f32, f32=f32)
+    if schedule is None:
+        M.autotune(f32=f32)
+    else:
+        M.set_schedule(schedule, f32=f32)
+    xd = torch.from_numpy(x.astype(np.float32 if f32 else np.float64)).cuda()
+    y = M.spmv(xd)
+    for _ in range(3):
+        M.spmv(xd, y)
+    times = []
+    for _ in range(reps):
+        if flush is not None:
+            flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        M.spmv(xd, y)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    info = M.info()
+    sched = gb.SCHED_NAMES[info.schedule_f32 if f32 else info.schedule]
+    return float(np.median(times)), y.cpu().numpy(), {"schedule": sched,
+                                                      "tile_items": info.tile_items,
+                                                      "nlong": info.nlong}
+
+
+def spmv_extra(name, A, x, peak, flush, rows_check=200_000):
+    """SpMV GB/s for one matrix, FP64 and FP32, with parity on the first
+    `rows_check` rows against the oracle (FP64 oracle for both widths)."""
+    import oracle
+    out = {"n": A.nrows, "nnz": A.nnz}
+    k = min(rows_check, A.nrows)
+    nnz_k = int(A.rowptr[k])
+    rp, ri, rv = A.rowptr[: k + 1], A.rowind[:nnz_k], A.rowval[:nnz_k]
+    y_ref = oracle.spmv(rp, ri, rv, x, threads=os.cpu_count() or 1)
+    sub = type(A)(k, A.ncols, rp, ri, rv)
+    for f32 in (False, True):
+        ms, y, info = measure_spmv(A, x, f32=f32, flush=flush)
+        b = _spmv_bytes(A.nrows, A.nnz, 4 if f32 else 8, 4 if f32 else 8)
+        gbs = b / (ms * 1e-3) / 1e9
+        out["f32" if f32 else "f64"] = {
+            "ms": ms, "GB/s": gbs, "frac_of_peak": gbs / peak, "bytes": b, **info,
+            "max_cond_err_vs_fp64_oracle_first_rows": _cond_err(y[:k], y_ref, sub, x),
+        }
+    return out
+
+
+def run_spmv(args, dist: Dist, which: str):
+    """--workload spmv_uniform | spmv_powerlaw: SpMV GB/s (FP64 headline)."""
+    import torch
+
+    import gooseberry_b200 as gb
+    import oracle
+    from gooseberry_b200 import workloads as W
+    dev = dist.local if torch.cuda.device_count() > dist.local else 0
+    torch.cuda.set_device(dev)
+    if which == "spmv_uniform":
+        A = W.uniform_rows(100_000, 10, seed=1)
+        x = W.dense_x(A.ncols, 1)
+        label = "uniform 100k x 100k, 10 nnz/row"
+    else:
+        A = W.powerlaw_rows(8_000_000, 128_000_000, seed=3, cap=200_000)
+        x = W.dense_x(A.ncols, 3)
+        label = "power-law rows 8M x 8M, 128M nnz, exponent 2.1, cap 200k"
+    n, nnz = A.nrows, A.nnz
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    peak, peak_src = hbm_peak()
+    M = gb.CsrMatrix.from_host(A)
+    M.autotune()
+    xd = torch.from_numpy(x).cuda()
+    y = M.spmv(xd)
+    for _ in range(args.warmup):
+        M.spmv(xd, y)
+    clocks = Clocks(dev)
+    clocks.start()
+    dist.barrier()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        M.spmv(xd, y)
+        e1.record()
+        times.append((e0, e1))
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    t_local = sum(a.elapsed_time(b) for a, b in times) / 1e3
+    t_max = dist.max(t_local)
+    b = _spmv_bytes(n, nnz, 8, 8)
+    ms = t_local / args.steps * 1e3
+    # parity on the first rows against the oracle
+    k = min(200_000, n)
+    nnz_k = int(A.rowptr[k])
+    y_ref = oracle.spmv(A.rowptr[: k + 1], A.rowind[:nnz_k], A.rowval[:nnz_k], x,
+                        threads=os.cpu_count() or 1)
+    sub = type(A)(k, A.ncols, A.rowptr[: k + 1], A.rowind[:nnz_k], A.rowval[:nnz_k])
+    err = _cond_err(y.cpu().numpy()[:k], y_ref, sub, x)
+    # end to end: gooseberry_spmult_f64 with pinned host buffers
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
+        t.numpy()[...] = a
+        return t.numpy()
+    h_rp = pinned(A.rowptr.view(np.int32)).view(np.uint32)
+    h_ri = pinned(A.rowind.view(np.int32)).view(np.uint32)
+    h_rv, h_x = pinned(A.rowval), pinned(x)
+    h_y = pinned(np.zeros(n))
+    gb.spmult(h_rp, h_ri, h_rv, h_x, out=h_y)
+    e2e_steps = max(1, min(args.steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        gb.spmult(h_rp, h_ri, h_rv, h_x, out=h_y)
+    t_e2e = dist.max(time.perf_counter() - t0)
+    info = M.info()
+    out = {
+        "metric": f"SpMV GB/s (FP64, {label})",
+        "value": dist.world * args.steps * b / t_max / 1e9,
+        "unit": "GB/s", "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic, seeded (gooseberry_b200.workloads)",
+        "config": {"workload": which, "n": n, "nnz": nnz, "bytes_per_spmv": b,
+                   "schedule": gb.SCHED_NAMES[info.schedule], "tile_items": info.tile_items,
+                   "long_rows": info.nlong, "max_row": info.max_row,
+                   "l2": "flushed before every SpMV (256 MB write, outside the events)",
+                   "parity_max_cond_err_first_200k_rows": err},
+        "roofline": {"bound": "hbm", "kernel": "spmv_tiles_kernel",
+                     "achieved": b / (ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": b / (ms * 1e-3) / 1e9 / peak, "traffic": ncu_traffic(which),
+                     "peak_source": peak_src},
+        "e2e": {"value": e2e_steps * b / t_e2e / 1e9, "unit": "GB/s",
+                "h2d_bytes_per_step": 4 * (n + 1) + 12 * nnz + 8 * n,
+                "d2h_bytes_per_step": 8 * n, "api": "gooseberry_spmult_f64 (pinned host)"},
+        "gpu_launches": args.steps, "clocks": clk,
+    }
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        v, cinfo = cpu_spmv_sample(A, x, b)
+        out["cpu_baseline"] = {"value": v, "unit": "GB/s", "cores": cinfo["cores"],
+                               "kind": cinfo["kind"], "sample": cinfo["sample"]}
+    return out
+
+
+def cpu_spmv_sample(A, x, nbytes, budget_s=10.0):
+    """The reference's blas_spmult (oracle/_ref, else the restatement) on all
+    host threads; GB/s over repeated full SpMVs within the time budget."""
+    import oracle
+    threads = os.cpu_count() or 1
+    kind = "reference" if oracle.ref_available("f64") else "port"
+    if kind == "reference":
+        oracle.ref_set_threads(threads)
+        run = lambda: oracle.ref_spmm(A.rowptr, A.rowind, A.rowval, x, ncols=A.ncols)  # noqa: E731
+    else:
+        run = lambda: oracle.spmv(A.rowptr, A.rowind, A.rowval, x, threads=threads)  # noqa: E731
+    run()
+    t0 = time.perf_counter()
+    reps = 0
+    while time.perf_counter() - t0 < budget_s or reps == 0:
+        run()
+        reps += 1
+        if reps >= 1000:
+            break
+    dt = time.perf_counter() - t0
+    return reps * nbytes / dt / 1e9, {"kind": kind, "cores": threads,
+                                      "sample": f"{reps} full SpMVs in {dt:.1f} s"}
+
+
+def mixed_extra(side=160, rtol=1e-10, reps=2):
+    """Mixed-precision CG (FP32 inner, FP64 refinement) against plain FP64 CG
+    on the 3D 7-point variable-coefficient operator (160^3, coefficients
+    log-uniform in [1e-2, 1e2]); errors are true FP64 residuals on the host."""
+    import torch
+
+    import gooseberry_b200 as gb
+    from gooseberry_b200 import workloads as W
+    A = W.diffusion_3d(side, seed=4)
+    b = W.rhs(A.nrows, 4)
+    M = gb.CsrMatrix.from_host(A, f64=True, f32=True)
+    bd = torch.from_numpy(b).cuda()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    S_ = A.to_scipy()
+    out = {"n": A.nrows, "nnz": A.nnz, "rtol": rtol}
+    for name, mode in (("f64", gb.CG_F64), ("mixed", gb.CG_MIXED)):
+        S = gb.CgSolver(M, mode=mode)
+        x, r = S.solve(bd, tol=rtol, niter=50000)
+        ts = []
+        for _ in range(reps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            x, r = S.solve(bd, tol=rtol, niter=50000)
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        rel = float(np.linalg.norm(b - S_ @ x.cpu().numpy()) / np.linalg.norm(b))
+        out[name] = {"ms": min(ts), "solves_per_s": 1e3 / min(ts), "iterations": r.iterations,
+                     "refinements": r.refinements, "status": r.status,
+                     "true_rel_residual": rel, "schedule": gb.SCHED_NAMES[
+                         M.info().schedule_f32 if mode == gb.CG_MIXED else M.info().schedule]}
+        if mode == gb.CG_F64:
+            out["f64"]["x"] = None
+            x64 = x.cpu().numpy()
+        else:
+            out["mixed"]["rel_diff_to_fp64_solution"] = float(
+                np.linalg.norm(x.cpu().numpy() - x64) / np.linalg.norm(x64))
+        S.close()
+    out["f64"].pop("x")
+    out["speedup_mixed_over_f64"] = out["f64"]["ms"] / out["mixed"]["ms"]
+    return out
+
+
+def run_extras(args):
+    """Secondary workloads of the benchmark spec, reported beside the headline."""
+    import torch
+
+    from gooseberry_b200 import workloads as W
+    peak, _ = hbm_peak()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    ex = {}
+    t0 = time.time()
+    A = W.uniform_rows(100_000, 10, seed=1)
+    ex["spmv_uniform_100k"] = spmv_extra("spmv_uniform", A, W.dense_x(A.ncols, 1), peak, flush)
+    A = W.powerlaw_rows(8_000_000, 128_000_000, seed=3, cap=200_000)
+    ex["spmv_powerlaw_8m"] = spmv_extra("spmv_powerlaw", A, W.dense_x(A.ncols, 3), peak, flush)
+    del A
+    ex["mixed_cg_3d_160"] = mixed_extra()
+    ex["seconds"] = time.time() - t0
+    return ex
+
+
 def run_reference_cg(args):
     L, b = cg_laplace_setup()
     ref_it = reference_cg_iterations() or 2966
@@ -379,6 +630,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="cg_laplace2d")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the secondary workloads reported under 'extras'")
     args = ap.parse_args()
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
@@ -394,6 +647,12 @@ def main():
     try:
         if args.workload == "cg_laplace2d":
             out = run_cg_laplace(args, dist)
+            if dist.world == 1 and not args.no_extras:
+                out["extras"] = run_extras(args)
+        elif args.workload in ("spmv_uniform", "spmv_powerlaw"):
+            out = run_spmv(args, dist, args.workload)
+        elif args.workload == "cg_mixed_3d":
+            out = {"extras": {"mixed_cg_3d_160": mixed_extra()}}
         else:
             raise SystemExit(f"unknown workload {args.workload}")
         if dist.rank == 0:

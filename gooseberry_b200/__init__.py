@@ -33,6 +33,7 @@ __all__ = [
     "CsrMatrix", "CgSolver", "CgResult", "dot", "SUCCESS",
     "SCHED_AUTO", "SCHED_THREAD", "SCHED_GROUP4", "SCHED_GROUP8", "SCHED_WARP",
     "SCHED_MERGE", "SCHED_ROW", "SCHED_WTILE", "CG_F64", "CG_MIXED", "plan_tiles",
+    "Server", "ServerResult",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -110,6 +111,12 @@ SIGNATURES = {
     "gb_cg_destroy": (_i, [_vp]),
     "gb_cg_solve": (_i, [_vp, _vp, _vp, _d, _i, _sz, _vp, _sz, _vp, _vp]),
     "gb_cg_profile": (_i, [_vp, _vp, _sz, _vp, _sz, _vp, _vp]),
+    "gb_server_create": (_i, [_vp, _vp]),
+    "gb_server_destroy": (_i, [_vp]),
+    "gb_server_submit": (_i, [_vp, C.c_uint64, _u32, _vp, _vp, _vp, _vp, _vp, _d, _sz]),
+    "gb_server_step": (_i, [_vp, _vp, _vp]),
+    "gb_server_poll": (_i, [_vp, _vp, _sz, _vp]),
+    "gb_server_clock": (_d, [_vp]),
 }
 
 
@@ -415,3 +422,96 @@ class CgSolver:
         _check(lib().gb_cg_profile(self._h, b.data_ptr(), int(iterations), _ptr(ms), 4,
                                    C.addressof(nk), _stream_ptr(stream)), "gb_cg_profile")
         return ms[: nk.value].tolist()
+
+
+# ---- batched solve server ------------------------------------------------------------
+
+class _ServerConfig(C.Structure):
+    _fields_ = [("pool_bytes", C.c_size_t), ("max_slots", C.c_uint32), ("mode", C.c_int),
+                ("iters_per_step", C.c_uint32)]
+
+
+class _ServerResult(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("iterations", C.c_size_t), ("refinements", C.c_size_t),
+                ("rnorm", C.c_double), ("bnorm", C.c_double), ("status", C.c_int),
+                ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double)]
+
+
+@dataclass
+class ServerResult:
+    id: int
+    iterations: int
+    refinements: int
+    rnorm: float
+    bnorm: float
+    status: str
+    t_submit: float
+    t_admit: float
+    t_done: float
+    x: np.ndarray
+
+
+class Server:
+    """Continuous-batching CG server (``gb_server_t``): submit host CSR
+    systems, call ``step()`` repeatedly, collect results with ``poll()``."""
+
+    def __init__(self, pool_bytes: int = 16 << 30, max_slots: int = 128,
+                 mode: int = CG_MIXED, iters_per_step: int = 16):
+        cfg = _ServerConfig(pool_bytes, max_slots, mode, iters_per_step)
+        h = C.c_void_p()
+        _check(lib().gb_server_create(C.addressof(cfg), C.addressof(h)), "gb_server_create")
+        self._h = h
+        self._out = {}  # id -> x buffer kept alive until reported
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().gb_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, rid: int, csr, b, tol: float = 1e-10, niter: int = 0, x_out=None):
+        rowptr = np.ascontiguousarray(csr.rowptr, dtype=np.uint32)
+        rowind = np.ascontiguousarray(csr.rowind, dtype=np.uint32)
+        rowval = np.ascontiguousarray(csr.rowval, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(len(b)) if x_out is None else x_out
+        _check(lib().gb_server_submit(self._h, int(rid), len(b), _ptr(rowptr), _ptr(rowind),
+                                      _ptr(rowval), _ptr(b), _ptr(x), float(tol), int(niter)),
+               "gb_server_submit")
+        self._out[int(rid)] = x
+
+    def step(self):
+        a, q = C.c_size_t(0), C.c_size_t(0)
+        _check(lib().gb_server_step(self._h, C.addressof(a), C.addressof(q)), "gb_server_step")
+        return a.value, q.value
+
+    def poll(self, max_results: int = 4096):
+        buf = (_ServerResult * max_results)()
+        cnt = C.c_size_t(0)
+        _check(lib().gb_server_poll(self._h, C.addressof(buf), max_results, C.addressof(cnt)),
+               "gb_server_poll")
+        out = []
+        for i in range(cnt.value):
+            r = buf[i]
+            out.append(ServerResult(r.id, r.iterations, r.refinements, r.rnorm, r.bnorm,
+                                    CG_STATUS.get(r.status, str(r.status)), r.t_submit,
+                                    r.t_admit, r.t_done, self._out.pop(int(r.id))))
+        return out
+
+    def clock(self) -> float:
+        return float(lib().gb_server_clock(self._h))
+
+    def drain(self, timeout_s: float = 600.0):
+        """Step until every submitted request is reported."""
+        import time
+        res = []
+        t0 = time.time()
+        while self._out and time.time() - t0 < timeout_s:
+            self.step()
+            res += self.poll()
+        return res

@@ -188,41 +188,59 @@ def _assemble_stencil(shape, coef_of_face, bcoef_of_face):
     last axis fastest).  ``coef_of_face(axis)`` gives the coefficient of every
     interior face normal to ``axis`` (array of shape with that axis one
     shorter); ``bcoef_of_face(axis, side)`` the Dirichlet boundary faces.
-    Off-diagonals are -c; the diagonal sums every adjacent face coefficient."""
+    Off-diagonals are -c; the diagonal sums every adjacent face coefficient.
+
+    The CSR is written directly, without sorting: with strides s_0 > s_1 >
+    ... the columns of a row in increasing order are r - s_0, ..., r - s_{d-1},
+    r, r + s_{d-1}, ..., r + s_0 (the ones that exist)."""
     dims = len(shape)
     n = int(np.prod(shape))
-    idx = np.arange(n, dtype=np.int64).reshape(shape)
     diag = np.zeros(shape, dtype=np.float64)
-    rows, cols, vals = [], [], []
+    coefs = []
     for ax in range(dims):
         c = coef_of_face(ax)
+        coefs.append(c)
         lo = [slice(None)] * dims
         hi = [slice(None)] * dims
         lo[ax] = slice(0, shape[ax] - 1)
         hi[ax] = slice(1, shape[ax])
-        a = idx[tuple(lo)].ravel()
-        b = idx[tuple(hi)].ravel()
-        cv = c.ravel()
-        rows += [a, b]
-        cols += [b, a]
-        vals += [-cv, -cv]
         diag[tuple(lo)] += c
         diag[tuple(hi)] += c
         for side in (0, 1):
             sl = [slice(None)] * dims
             sl[ax] = slice(0, 1) if side == 0 else slice(shape[ax] - 1, shape[ax])
             diag[tuple(sl)] += bcoef_of_face(ax, side)
-    rows.append(idx.ravel())
-    cols.append(idx.ravel())
+    strides = [int(np.prod(shape[ax + 1:])) for ax in range(dims)]
+    ridx = np.arange(n, dtype=np.int64)
+    coords = np.unravel_index(ridx, shape)
+    cols, vals, valid = [], [], []
+    # lower neighbours, slowest axis first (largest stride -> smallest column)
+    for ax in range(dims):
+        ok = coords[ax] > 0
+        face = np.zeros(n)
+        sub = tuple(np.where(ok, coords[a] - (1 if a == ax else 0), 0) for a in range(dims))
+        face[ok] = -coefs[ax][tuple(s_[ok] for s_ in sub)]
+        cols.append(ridx - strides[ax])
+        vals.append(face)
+        valid.append(ok)
+    cols.append(ridx)
     vals.append(diag.ravel())
-    r = np.concatenate(rows)
-    c = np.concatenate(cols)
-    v = np.concatenate(vals)
-    order = np.lexsort((c, r))
-    r, c, v = r[order], c[order], v[order]
+    valid.append(np.ones(n, dtype=bool))
+    # upper neighbours, fastest axis first
+    for ax in reversed(range(dims)):
+        ok = coords[ax] < shape[ax] - 1
+        face = np.zeros(n)
+        sub = tuple(np.where(ok, coords[a], 0) for a in range(dims))
+        face[ok] = -coefs[ax][tuple(s_[ok] for s_ in sub)]
+        cols.append(ridx + strides[ax])
+        vals.append(face)
+        valid.append(ok)
+    C = np.stack(cols, axis=1)
+    V = np.stack(vals, axis=1)
+    M = np.stack(valid, axis=1)
     rowptr = np.zeros(n + 1, dtype=np.int64)
-    rowptr[1:] = np.cumsum(np.bincount(r, minlength=n))
-    return Csr(n, n, rowptr.astype(np.uint32), c.astype(np.uint32), v)
+    rowptr[1:] = np.cumsum(M.sum(axis=1))
+    return Csr(n, n, rowptr.astype(np.uint32), C[M].astype(np.uint32), V[M])
 
 
 def laplacian_2d(side: int = 1024) -> Csr:

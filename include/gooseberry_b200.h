@@ -246,6 +246,63 @@ GOOSEBERRY_API int gb_cg_solve(gb_cg_t * s, const double * b, double * x, double
 GOOSEBERRY_API int gb_cg_profile(gb_cg_t * s, const double * b, size_t iterations,
     double * ms, size_t ms_len, size_t * nkernels, gb_stream_t stream);
 
+/* ---- batched solve server (continuous batching) ---------------------------- */
+
+/*
+ * Many independent CG solves of uneven sizes resident on one GPU at once.
+ * Every gb_server_step runs `iters_per_step` CG iterations of EVERY resident
+ * solve with one replay of a captured CUDA graph (the kernels walk a global
+ * list of small row tiles covering all resident solves, so a 1k-row and a
+ * 262k-row system advance together), retires the solves that finished
+ * (their x is copied to the caller's buffer) and admits queued requests into
+ * the freed slots and device memory.  Admission is by device-memory
+ * footprint, bounded by pool_bytes.  No reference counterpart (the reference
+ * runs one cgd call at a time, src/gooseberry_bin.c:2078-2091).
+ */
+typedef struct gb_server gb_server_t;
+
+typedef struct gb_server_config {
+  size_t pool_bytes;        /* device memory for resident solves             */
+  uint32_t max_slots;       /* resident solves at most                       */
+  int mode;                 /* GB_CG_MIXED or GB_CG_F64                      */
+  uint32_t iters_per_step;  /* CG iterations per gb_server_step (>= 1)       */
+} gb_server_config_t;
+
+typedef struct gb_server_result {
+  uint64_t id;
+  size_t iterations;
+  size_t refinements;
+  double rnorm;             /* final ||b - A x||_2 (FP64, true residual for
+                               GB_CG_MIXED; recurrence residual for F64)     */
+  double bnorm;
+  int status;               /* gb_cg_status_t                                */
+  double t_submit, t_admit, t_done;  /* seconds on the server clock        */
+} gb_server_result_t;
+
+GOOSEBERRY_API int gb_server_create(const gb_server_config_t * cfg, gb_server_t ** out);
+GOOSEBERRY_API int gb_server_destroy(gb_server_t * s);
+
+/* Queue one solve of A x = b (square CSR, host arrays, copied at once) to
+ * relative residual tol_rel or niter iterations.  x_out (host, n doubles)
+ * must stay valid until the result is reported by gb_server_poll.  Rows may
+ * hold at most 255 nonzeros.  Returns INVALIDINPUT for malformed input or a
+ * request that could never fit the pool. */
+GOOSEBERRY_API int gb_server_submit(gb_server_t * s, uint64_t id, dim_t n,
+    const ind_t * rowptr, const dim_t * rowind, const double * rowval, const double * b,
+    double * x_out, double tol_rel, size_t niter);
+
+/* One scheduling step (see above).  Returns at once after queueing the
+ * step's GPU work; *active / *queued (optional) receive the resident and
+ * waiting request counts. */
+GOOSEBERRY_API int gb_server_step(gb_server_t * s, size_t * active, size_t * queued);
+
+/* Move up to `max` finished results into `out`; *count receives how many. */
+GOOSEBERRY_API int gb_server_poll(gb_server_t * s, gb_server_result_t * out, size_t max,
+    size_t * count);
+
+/* Seconds since the server was created (the clock of the result stamps). */
+GOOSEBERRY_API double gb_server_clock(const gb_server_t * s);
+
 #ifdef __cplusplus
 }
 #endif

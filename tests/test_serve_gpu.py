@@ -1,0 +1,105 @@
+"""Continuous-batching solve server: every request converges to its
+tolerance (true FP64 residual measured on the host), the result of a request
+is the same whether it runs alone or in a mix of uneven solves (bitwise: each
+solve's reductions run over its own tiles in a fixed order), and admission
+respects the device-memory pool."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import gooseberry_b200 as gb
+from gooseberry_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests(sides, seed0):
+    out = []
+    for k, s in enumerate(sides):
+        A = W.diffusion_2d(int(s), seed=seed0 + k)
+        out.append((k, A, W.rhs(A.nrows, seed0 + k)))
+    return out
+
+
+def _rel(A, x, b):
+    return float(np.linalg.norm(b - A.to_scipy() @ x) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("mode", [gb.CG_MIXED, gb.CG_F64])
+def test_mix_converges_and_matches_alone(mode):
+    reqs = _requests([16, 40, 9, 64, 23, 100, 31, 8, 57], 100)
+    tol = 1e-10
+    srv = gb.Server(pool_bytes=1 << 30, max_slots=4, mode=mode, iters_per_step=8)
+    for rid, A, b in reqs:
+        srv.submit(rid, A, b, tol=tol, niter=20000)
+    res = {r.id: r for r in srv.drain()}
+    assert sorted(res) == [r[0] for r in reqs]
+    for rid, A, b in reqs:
+        r = res[rid]
+        assert r.status == "converged", (rid, r)
+        rel = _rel(A, r.x, b)
+        if mode == gb.CG_MIXED:
+            assert rel <= 1.05 * tol, (rid, rel)  # converged on the true residual
+            assert r.rnorm == pytest.approx(rel * np.linalg.norm(b), rel=1e-3)
+        else:
+            assert rel <= 2 * tol, (rid, rel)
+        assert r.t_submit <= r.t_admit <= r.t_done
+    # alone, in a fresh server, the same requests give the same bits
+    for rid, A, b in (reqs[1], reqs[5]):
+        alone = gb.Server(pool_bytes=1 << 30, max_slots=1, mode=mode, iters_per_step=3)
+        alone.submit(rid, A, b, tol=tol, niter=20000)
+        r1 = alone.drain()[0]
+        assert r1.iterations == res[rid].iterations
+        assert np.array_equal(r1.x, res[rid].x), rid
+        alone.close()
+
+
+def test_fp64_server_matches_single_solver():
+    rid, A, b = _requests([48], 300)[0]
+    srv = gb.Server(pool_bytes=1 << 28, max_slots=2, mode=gb.CG_F64, iters_per_step=5)
+    srv.submit(rid, A, b, tol=1e-8, niter=5000)
+    r = srv.drain()[0]
+    e = 1e-8 * np.linalg.norm(b)
+    x, it, rn = gb.cgd(A.rowptr, A.rowind, A.rowval, b, e, 5000)
+    assert abs(r.iterations - it) <= 2
+    assert np.linalg.norm(r.x - x) <= 1e-6 * np.linalg.norm(x)
+
+
+def _footprint_mixed(n, nnz):
+    """Device bytes of one mixed-precision solve (256-byte granules): rowptr,
+    rowind, FP64 and FP32 values, b, two x buffers, y, r, two p, Ap."""
+    a = lambda v: (v + 255) // 256 * 256  # noqa: E731
+    return (a(4 * (n + 1)) + a(4 * nnz) + a(8 * nnz) + a(4 * nnz) + 3 * a(8 * n)
+            + 5 * a(4 * n))
+
+
+def test_pool_admission_and_limits():
+    reqs = _requests([96, 96, 96, 96], 400)
+    fp = _footprint_mixed(reqs[0][1].nrows, reqs[0][1].nnz)
+    # a pool that holds two of these at once but not three
+    srv = gb.Server(pool_bytes=2 * fp + fp // 2, max_slots=8, mode=gb.CG_MIXED,
+                    iters_per_step=4)
+    for rid, A, b in reqs:
+        srv.submit(rid, A, b, tol=1e-10)
+    active, queued = srv.step()
+    assert active <= 2 and queued >= 2
+    res = srv.drain()
+    assert sorted(r.id for r in res) == [0, 1, 2, 3]
+    assert all(r.status == "converged" for r in res)
+    # requests that can never fit, or have too-long rows, are refused up front
+    big = W.diffusion_2d(512, seed=1)
+    with pytest.raises(gb.GooseberryError):
+        srv.submit(99, big, W.rhs(big.nrows, 1))
+    dense = W.uniform_rows(300, 280, seed=2)
+    with pytest.raises(gb.GooseberryError):
+        srv.submit(98, dense, W.rhs(300, 2))
+
+
+def test_iteration_limit_reports_true_residual():
+    rid, A, b = _requests([80], 500)[0]
+    srv = gb.Server(pool_bytes=1 << 28, max_slots=2, mode=gb.CG_MIXED, iters_per_step=7)
+    srv.submit(rid, A, b, tol=1e-14, niter=30)
+    r = srv.drain()[0]
+    assert r.status == "maxiter" and r.iterations == 30
+    assert r.rnorm == pytest.approx(_rel(A, r.x, b) * np.linalg.norm(b), rel=1e-6)
