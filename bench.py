@@ -573,6 +573,93 @@ def mixed_extra(side=160, rtol=1e-10, reps=2):
     return out
 
 
+def serving_extra(nreq=400, seed=5, rtol=1e-10, pool=16 << 30, slots=256, ips=16,
+                  load=0.8):
+    """Serving stream of 2D 5-point variable-coefficient SPD systems (side
+    log-uniform in [32, 512], coefficients log-uniform in [0.1, 10], b in
+    [-1, 1], per-request seeds), each to rel-res `rtol`.
+
+    Baseline: plain FP64 CG served one solve at a time through the drop-in
+    gooseberry_cgd_f64 (upload, solve, download per request); its latencies
+    under Poisson arrivals are the exact FIFO single-server replay of the
+    measured service times.  Ours: the continuous-batching server (mixed
+    precision, 16 GB pool), driven in real time by the same arrival times.
+    Arrival rate = `load` x the baseline's saturation throughput."""
+    import gooseberry_b200 as gb
+    from gooseberry_b200 import workloads as W
+    sides = W.serving_sides(nreq, seed)
+    reqs = []
+    for k, side in enumerate(sides):
+        rs = seed * 1_000_003 + k
+        A = W.diffusion_2d(int(side), seed=rs)
+        reqs.append((k, A, W.rhs(A.nrows, rs)))
+    # --- baseline: FP64, one at a time
+    svc, base_iters, base_ok = [], [], 0
+    for k, A, b in reqs[:2]:  # warm-up
+        gb.cgd(A.rowptr, A.rowind, A.rowval, b, rtol * float(np.linalg.norm(b)), 0)
+    for k, A, b in reqs:
+        t0 = time.perf_counter()
+        x, it, rn = gb.cgd(A.rowptr, A.rowind, A.rowval, b, rtol * float(np.linalg.norm(b)), 0)
+        svc.append(time.perf_counter() - t0)
+        base_iters.append(it)
+        base_ok += int(rn <= rtol * float(np.linalg.norm(b)) * (1 + 1e-12))
+    base_thr = nreq / sum(svc)
+    # --- ours at saturation (everything queued at t = 0)
+    srv = gb.Server(pool_bytes=pool, max_slots=slots, mode=gb.CG_MIXED, iters_per_step=ips)
+    t0 = time.perf_counter()
+    for k, A, b in reqs:
+        srv.submit(k, A, b, tol=rtol)
+    res = srv.drain(timeout_s=3600)
+    makespan = time.perf_counter() - t0
+    srv.close()
+    sat_thr = len(res) / makespan
+    worst = 0.0
+    for r in res:
+        A, b = reqs[r.id][1], reqs[r.id][2]
+        worst = max(worst, float(np.linalg.norm(b - A.to_scipy() @ r.x) / np.linalg.norm(b)))
+    # --- latency at load x baseline throughput
+    lam = load * base_thr
+    arr = W.poisson_arrivals(nreq, lam, seed)
+    end, base_lat = 0.0, []
+    for a, s_ in zip(arr, svc):
+        start = max(a, end)
+        end = start + s_
+        base_lat.append(end - a)
+    srv = gb.Server(pool_bytes=pool, max_slots=slots, mode=gb.CG_MIXED, iters_per_step=ips)
+    c0 = srv.clock()
+    i, got = 0, []
+    t_start = time.perf_counter()
+    while len(got) < nreq and time.perf_counter() - t_start < 3600:
+        now = time.perf_counter() - t_start
+        while i < nreq and arr[i] <= now:
+            srv.submit(i, reqs[i][1], reqs[i][2], tol=rtol)
+            i += 1
+        active, queued = srv.step()
+        got += srv.poll()
+        if active == 0 and queued == 0 and i < nreq:
+            time.sleep(max(0.0, min(0.01, arr[i] - (time.perf_counter() - t_start))))
+    srv.close()
+    lat = [r.t_done - c0 - arr[r.id] for r in got]
+
+    def pct(v, q):
+        return float(np.percentile(np.asarray(v), q))
+    return {
+        "requests": nreq, "rtol": rtol, "pool_bytes": pool, "slots": slots,
+        "iters_per_step": ips,
+        "rows_min_median_max": [int(min(sides) ** 2), int(np.median(sides) ** 2),
+                                int(max(sides) ** 2)],
+        "fp64_one_at_a_time": {"solves_per_s": base_thr, "converged": base_ok,
+                               "iterations_median": float(np.median(base_iters)),
+                               "p50_s": pct(base_lat, 50), "p99_s": pct(base_lat, 99)},
+        "mixed_batched": {"solves_per_s_saturated": sat_thr, "converged": sum(
+            r.status == "converged" for r in res), "worst_true_rel_residual": worst,
+            "iterations_median": float(np.median([r.iterations for r in res])),
+            "p50_s": pct(lat, 50), "p99_s": pct(lat, 99), "completed_at_load": len(got)},
+        "arrival_rate_per_s": lam,
+        "speedup_solves_per_s": sat_thr / base_thr,
+    }
+
+
 def run_extras(args):
     """Secondary workloads of the benchmark spec, reported beside the headline."""
     import torch
@@ -588,6 +675,7 @@ def run_extras(args):
     ex["spmv_powerlaw_8m"] = spmv_extra("spmv_powerlaw", A, W.dense_x(A.ncols, 3), peak, flush)
     del A
     ex["mixed_cg_3d_160"] = mixed_extra()
+    ex["serving_stream"] = serving_extra(nreq=args.requests)
     ex["seconds"] = time.time() - t0
     return ex
 
@@ -632,6 +720,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the secondary workloads reported under 'extras'")
+    ap.add_argument("--requests", type=int, default=300,
+                    help="requests of the serving stream (extras / --workload serving)")
     args = ap.parse_args()
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
@@ -653,6 +743,8 @@ def main():
             out = run_spmv(args, dist, args.workload)
         elif args.workload == "cg_mixed_3d":
             out = {"extras": {"mixed_cg_3d_160": mixed_extra()}}
+        elif args.workload == "serving":
+            out = {"extras": {"serving_stream": serving_extra(nreq=args.requests)}}
         else:
             raise SystemExit(f"unknown workload {args.workload}")
         if dist.rank == 0:
