@@ -6,28 +6,36 @@
 // its CSR matrix and Krylov vectors live in one device pool (first-fit
 // allocator, bounded by pool_bytes), and all slots advance together.
 //
-// Work list: every slot's rows are cut into row-aligned tiles of at most
-// kTileItems rows + nonzeros; the tiles of all resident slots form ONE global
-// list.  Each kernel is persistent over that list, one warp per tile at a
-// time, lane per row (rows hold at most 255 nonzeros).  A tile leaves a
-// partial sum; the warp that finishes a slot's last tile (per-slot atomic
-// ticket) adds the slot's partials in tile order (deterministic) and updates
-// that slot's alpha / beta / stop decision.  So one launch advances a 1k-row
-// and a 262k-row solve by one phase each, and the launch cost is shared by
-// the whole batch.
+// Work list: every slot's rows are cut into row tiles of 256..2048 rows (a
+// power of two chosen from the slot's size alone); the tiles of all resident
+// slots form ONE global list.  Each kernel is persistent over that list, one
+// CTA tile at a time: eight compute warps run the pipelined thread-per-row
+// loop of the single-solve kernels over the tile (coalesced row vectors,
+// reference summation order), while a ninth, control warp prefetches the
+// next tile's descriptor and slot record into the other half of a shared
+// double buffer and finishes the previous tile: it publishes the tile's dot
+// partial, takes the slot's ticket, and when it is the slot's last tile adds
+// the slot's partials in tile order (deterministic) and advances that slot's
+// scalar state (alpha / beta / stop decision).  So one launch moves a
+// 1k-row and a 262k-row solve forward by one phase each, and the launch
+// cost is shared by the whole batch.
 //
-// Per step (one graph replay): init of newly admitted slots, then
-// iters_per_step x { A: SpMV + direction update + p.Ap;  B: x/y, r update +
-// r.r;  R (mixed only): reliable FP64 residual update }.  Slot state lives in
-// device memory, so the captured graph never changes; between steps the host
-// reads the slot table back, retires finished solves (x copied out), admits
-// queued requests into freed slots and memory, rebuilds the tile list and
-// uploads the table.
+// Per step (one graph replay): iters_per_step x { A, B }.
+//   A: per slot one of  CG   -- SpMV + direction update + p.Ap
+//                       INIT -- x = 0, r = b, p = 0, b.b (newly admitted)
+//                       R    -- reliable FP64 residual update (mixed)
+//   B: x/y and r update + r.r, stop or update decision; skipped for a slot
+//      whose A launch did INIT or R.
+// Slot state lives in device memory, so the captured graph never changes;
+// between steps the host reads the slot table back, retires finished solves
+// (x copied out), admits queued requests into freed slots and memory,
+// rebuilds the tile list and uploads the table.
 //
 // Mixed mode is the algorithm of cg_mixed.cu (FP32 values and vectors, FP64
 // dots, reliable FP64 updates, convergence on the true residual); F64 mode
 // is plain CG like cg.cu (convergence on the recurrence residual, as the
-// reference).
+// reference).  A solve's arithmetic depends only on its own rows and tiles,
+// so its result is bitwise the same alone or in any mix.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -43,11 +51,20 @@
 namespace gb {
 namespace {
 
-constexpr uint32_t kTileItems = 256;  // rows + nonzeros per warp tile
-constexpr int kSrvBlock = 256;
-constexpr int kSrvWarps = kSrvBlock / 32;
-constexpr double kSrvDelta = 0.1;     // reliable update trigger (see cg_mixed.cu)
-constexpr size_t kMaxTiles = 2u << 20;
+constexpr int kSrvComputeWarps = 8;
+constexpr int kSrvCompute = kSrvComputeWarps * 32;  // row threads per CTA
+constexpr int kSrvThreads = kSrvCompute + 32;       // + the control warp
+constexpr int kSrvMinBlocks = 2;
+constexpr int kSrvMaxRegs = 112;  // 2 CTAs of 288 threads per SM
+constexpr uint32_t kTileRowsMin = 256;
+constexpr uint32_t kTileRowsMax = 2048;
+constexpr int kRowsPerThread = kTileRowsMax / kSrvCompute;  // 8
+constexpr uint32_t kTilesPerSolve = 256;  // tile size target: n / 256 rows
+constexpr uint32_t kMaxRowNnz = 255;      // longer rows belong to the single-solve CG
+constexpr double kSrvDelta = 0.1;         // reliable update trigger (see cg_mixed.cu)
+constexpr size_t kMaxTiles = 1u << 20;
+
+enum : int { kWorkCg = 0, kWorkInit = 1, kWorkReliable = 2 };  // what A does for a slot
 
 struct SrvTile {
   uint32_t slot;
@@ -56,7 +73,8 @@ struct SrvTile {
   uint32_t pad;
 };
 
-struct SrvSlot {
+struct __align__(16) SrvSlot {
+  // written by the host at admission
   const uint32_t * rowptr;
   const uint32_t * rowind;
   const double * val64;
@@ -69,29 +87,35 @@ struct SrvSlot {
   void * p0;  // T[n]
   void * p1;  // T[n]
   void * ap;  // T[n]
-  uint32_t n, ntiles, tile0, pad;
-  double rr_hat, rr_hat_old, alpha, beta, tol, tol_rel, bnorm, rmax, rr_true;
-  unsigned long long iter, niter, refinements;
+  uint32_t n, ntiles, tile0, pad0;
+  double tol_rel;
+  unsigned long long niter;
+  // written by the kernels (the slot's last tile of a launch)
+  double rr_hat, rr_hat_old, alpha, beta, tol, bnorm, rmax, rr_true;
+  unsigned long long iter, refinements;
   int live;     // slot holds a solve
-  int init;     // needs the init kernel
+  int a_work;   // kWorkCg / kWorkInit / kWorkReliable
+  int b_skip;   // the next B launch leaves this slot alone
   int done;     // finished (converged / maxiter / breakdown / nonfinite)
   int status;
-  int update;   // reliable update pending
-  int final;    // the update is the last one (iteration limit)
   int y_reset;
   int xpar;
-  unsigned ticket_a, ticket_b, ticket_r, ticket_i;
+  int final_update;  // the pending reliable update is the last one (iteration limit)
+  unsigned ticket_a, ticket_b, pad1, pad2;
+};
+static_assert(sizeof(SrvSlot) == 256, "slot record is sixteen 16-byte words");
+
+struct __align__(16) SrvCtx {
+  SrvTile tile;
+  SrvSlot slot;
 };
 
 struct SrvDev {
   SrvSlot * slots;
   const SrvTile * tiles;
   const uint32_t * ntiles;  // device word: tiles in the list
-  double * pa;
-  double * pb;
-  double * pr;
-  double * pi0;
-  double * pi1;
+  double2 * pa;             // per tile: A partial sums
+  double2 * pb;             // per tile: B partial sums
 };
 
 __device__ __forceinline__ double warp_sum_d(double v) {
@@ -100,95 +124,81 @@ __device__ __forceinline__ double warp_sum_d(double v) {
   return v;
 }
 
-// True in every lane of the warp that completes the slot's last tile.
-__device__ __forceinline__ bool slot_arrive(unsigned * ticket, unsigned ntiles, int lane) {
+// Control warp: tile t's descriptor and its slot record into shared memory.
+// L2-coherent loads: the record was written by other SMs in earlier launches.
+__device__ __forceinline__ void load_ctx(const SrvDev & d, uint32_t t, SrvCtx & c, int lane) {
+  const uint4 tv = __ldcg(reinterpret_cast<const uint4 *>(d.tiles + t));
+  if (lane == 0) *reinterpret_cast<uint4 *>(&c.tile) = tv;
+  if (lane < 16)
+    reinterpret_cast<uint4 *>(&c.slot)[lane] =
+        __ldcg(reinterpret_cast<const uint4 *>(d.slots + tv.x) + lane);
+}
+
+// Control warp, after the tile's rows: publish the tile's sums and take the
+// slot's ticket.  True (in every lane) for the slot's last tile; `tot` is
+// then the slot's sum over its tiles in tile order.
+__device__ __forceinline__ bool slot_finish(double2 * part, uint32_t t, double2 mine,
+    unsigned * ticket, uint32_t t0, uint32_t nt, int lane, double2 * tot) {
   unsigned tk = 0;
-  __syncwarp();
   if (lane == 0) {
+    part[t] = mine;
     __threadfence();
     tk = atomicAdd(ticket, 1u);
   }
   tk = __shfl_sync(0xffffffffu, tk, 0);
-  return tk == ntiles - 1;
-}
-
-// Sum of part[t0 .. t0+nt) in a fixed order, in every lane.
-__device__ __forceinline__ double slot_sum(const double * part, uint32_t t0, uint32_t nt,
-    int lane) {
+  if (tk != nt - 1) return false;
   __threadfence();
-  double acc = 0.0;
-  for (uint32_t i = lane; i < nt; i += 32) acc += __ldcg(part + t0 + i);
-  return warp_sum_d(acc);
+  double sx = 0.0, sy = 0.0;
+  for (uint32_t i = lane; i < nt; i += 32) {
+    const double2 v = __ldcg(part + t0 + i);
+    sx += v.x;
+    sy += v.y;
+  }
+  tot->x = warp_sum_d(sx);
+  tot->y = warp_sum_d(sy);
+  return true;
 }
 
-template <typename T>
-__device__ __forceinline__ T ldv(const T * p, uint64_t pol) { return ld_keep(p, pol); }
-
-// ---- init: x = 0, r = b, p = 0 ---------------------------------------------------
-
-template <typename T, bool MIXED>
-__global__ void __launch_bounds__(kSrvBlock) srv_init_kernel(const SrvDev d) {
-  pdl_wait_and_release();
-  const int lane = threadIdx.x & 31;
-  const uint32_t nt = *d.ntiles;
-  const uint32_t gw = blockIdx.x * kSrvWarps + (threadIdx.x >> 5);
-  for (uint32_t t = gw; t < nt; t += gridDim.x * kSrvWarps) {
-    const SrvTile tl = d.tiles[t];
-    SrvSlot & S = d.slots[tl.slot];
-    if (!S.live || !S.init) continue;
-    T * r = static_cast<T *>(S.r);
-    T * p0 = static_cast<T *>(S.p0);
-    double sb = 0.0, sr = 0.0;
-    for (uint32_t q = lane; q < tl.row_count; q += 32) {
-      const uint32_t i = tl.row_begin + q;
-      const double bv = S.b[i];
-      const T rv = static_cast<T>(bv);
-      S.x0[i] = 0.0;
-      r[i] = rv;
-      p0[i] = T(0);
-      sb += bv * bv;
-      sr += static_cast<double>(rv) * static_cast<double>(rv);
-    }
-    sb = warp_sum_d(sb);
-    sr = warp_sum_d(sr);
-    if (lane == 0) {
-      d.pi0[t] = sb;
-      d.pi1[t] = sr;
-    }
-    if (slot_arrive(&S.ticket_i, S.ntiles, lane)) {
-      const double bb = slot_sum(d.pi0, S.tile0, S.ntiles, lane);
-      const double rr = slot_sum(d.pi1, S.tile0, S.ntiles, lane);
+// The persistent tile loop shared by both kernels.  Work supplies
+// active(slot), rows(ctx, tid, s0, s1) and finish(d, t, ctx, sums, lane).
+template <class Work>
+__device__ __forceinline__ void srv_loop(const SrvDev & d, Work & w) {
+  __shared__ SrvCtx ctx[2];
+  __shared__ double red[2][kSrvComputeWarps][2];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t nt = __ldcg(d.ntiles);
+  uint32_t t = blockIdx.x;
+  if (t >= nt) return;
+  if (warp == kSrvComputeWarps) load_ctx(d, t, ctx[0], lane);
+  __syncthreads();
+  for (int buf = 0; t < nt; t += gridDim.x, buf ^= 1) {
+    const SrvCtx & c = ctx[buf];
+    const bool act = Work::active(c.slot);
+    if (warp == kSrvComputeWarps) {
+      if (t + gridDim.x < nt) load_ctx(d, t + gridDim.x, ctx[buf ^ 1], lane);
+    } else if (act) {
+      double s0 = 0.0, s1 = 0.0;
+      w.rows(c, threadIdx.x, s0, s1);
+      s0 = warp_sum_d(s0);
+      s1 = warp_sum_d(s1);
       if (lane == 0) {
-        S.ticket_i = 0;
-        S.bnorm = sqrt(bb);
-        S.tol = S.tol_rel * S.bnorm;
-        S.rr_true = bb;
-        S.rr_hat = MIXED ? rr : bb;
-        S.rr_hat_old = S.rr_hat;
-        S.rmax = sqrt(S.rr_hat);
-        S.alpha = 0.0;
-        S.beta = 0.0;
-        S.iter = 0;
-        S.refinements = 0;
-        S.xpar = 0;
-        S.y_reset = 1;
-        S.update = 0;
-        S.final = 0;
-        S.status = GB_CG_MAXITER;
-        S.init = 0;
-        if (bb == 0.0) {
-          S.done = 1;
-          S.status = GB_CG_CONVERGED;
-        } else if (!(bb == bb) || isinf(bb)) {
-          S.done = 1;
-          S.status = GB_CG_NONFINITE;
-        }
+        red[buf][warp][0] = s0;
+        red[buf][warp][1] = s1;
       }
+    }
+    __syncthreads();
+    if (warp == kSrvComputeWarps && act) {
+      double2 s = make_double2(0.0, 0.0);
+      if (lane == 0)
+        for (int k = 0; k < kSrvComputeWarps; ++k) {
+          s.x += red[buf][k][0];
+          s.y += red[buf][k][1];
+        }
+      w.finish(d, t, c, s, lane);
+      __syncwarp();  // lane 0 is done reading ctx[buf] before it is refilled
     }
   }
 }
-
-// ---- A: SpMV + direction update + p.Ap --------------------------------------------
 
 template <typename T>
 __device__ __forceinline__ const T * values_of(const SrvSlot & S);
@@ -199,83 +209,203 @@ __device__ __forceinline__ const double * values_of<double>(const SrvSlot & S) {
   return S.val64;
 }
 
+// ---- A: CG step / init / reliable update --------------------------------------------
+
 template <typename T>
-__global__ void __launch_bounds__(kSrvBlock) srv_a_kernel(const SrvDev d) {
-  pdl_wait_and_release();
-  const int lane = threadIdx.x & 31;
-  const uint64_t pol = policy_evict_last();
-  const uint32_t nt = *d.ntiles;
-  const uint32_t gw = blockIdx.x * kSrvWarps + (threadIdx.x >> 5);
-  for (uint32_t t = gw; t < nt; t += gridDim.x * kSrvWarps) {
-    const SrvTile tl = d.tiles[t];
-    SrvSlot & S = d.slots[tl.slot];
-    if (!S.live || S.init || S.done) continue;
-    const T beta = static_cast<T>(S.beta);
-    const bool par = (S.iter & 1ull) != 0;
-    const T * pold = static_cast<const T *>(par ? S.p1 : S.p0);
-    T * pnew = static_cast<T *>(par ? S.p0 : S.p1);
-    const T * r = static_cast<const T *>(S.r);
-    T * ap = static_cast<T *>(S.ap);
-    const T * val = values_of<T>(S);
-    const uint32_t * rowptr = S.rowptr;
-    const uint32_t * rowind = S.rowind;
-    double part = 0.0;
-    for (uint32_t q = lane; q < tl.row_count; q += 32) {
-      const uint32_t i = tl.row_begin + q;
-      const uint32_t b = __ldg(rowptr + i), e = __ldg(rowptr + i + 1);
-      const T ri = r[i], pi = pold[i];
-      T sum = T(0);
-      for (uint32_t base = b; base < e; base += 8) {
-        uint32_t c[8];
-        T v[8], g[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j)
-          if (base + j < e) {
-            c[j] = __ldg(rowind + base + j);
-            v[j] = __ldg(val + base + j);
-          }
-#pragma unroll
-        for (int j = 0; j < 8; ++j)
-          if (base + j < e) g[j] = fma(beta, ldv(pold + c[j], pol), ldv(r + c[j], pol));
-#pragma unroll
-        for (int j = 0; j < 8; ++j)
-          if (base + j < e) sum = fma(v[j], g[j], sum);
+struct SrvGatherP {  // direction p = r + beta * p_old, rebuilt inside the gather
+  const T * r;
+  const T * pold;
+  T beta;
+  __device__ __forceinline__ T operator()(uint32_t c, uint64_t pol) const {
+    return fma(beta, ld_keep(pold + c, pol), ld_keep(r + c, pol));
+  }
+};
+
+template <typename T>
+struct SrvOutA {
+  T * ap;
+  T * pnew;
+  const T * r;
+  const T * pold;
+  T beta;
+  double local;
+  struct Pre {
+    T r, pold;
+  };
+  __device__ __forceinline__ Pre pre(uint32_t i) const { return Pre{r[i], pold[i]}; }
+  __device__ __forceinline__ void row_pre(uint32_t i, T v, const Pre & q) {
+    ap[i] = v;
+    const T pn = fma(beta, q.pold, q.r);
+    pnew[i] = pn;
+    local += static_cast<double>(pn) * static_cast<double>(v);
+  }
+};
+
+struct SrvGatherXY {  // x + y in FP64
+  const double * x;
+  const float * y;
+  bool use_y;
+  __device__ __forceinline__ double operator()(uint32_t c, uint64_t pol) const {
+    const double xc = ld_keep(x + c, pol);
+    return use_y ? xc + static_cast<double>(ld_keep(y + c, pol)) : xc;
+  }
+};
+
+struct SrvOutR {  // x_new = x + y;  r = b - A (x + y) rounded to FP32
+  double * xnew;
+  float * r32;
+  const double * xold;
+  const float * y;
+  const double * b;
+  bool use_y;
+  double local;
+  struct Pre {
+    double x, b;
+    float y;
+  };
+  __device__ __forceinline__ Pre pre(uint32_t i) const {
+    return Pre{xold[i], b[i], use_y ? y[i] : 0.0f};
+  }
+  __device__ __forceinline__ void row_pre(uint32_t i, double v, const Pre & q) {
+    xnew[i] = use_y ? q.x + static_cast<double>(q.y) : q.x;
+    const double rt = q.b - v;
+    r32[i] = static_cast<float>(rt);
+    local += rt * rt;
+  }
+};
+
+// Rare (a few times per solve), so kept out of line: its FP64 row pipeline
+// does not add to the register demand of the CG path.
+__device__ __noinline__ double reliable_rows(const SrvSlot & S, uint32_t first, uint32_t end,
+    uint64_t pol_m, uint64_t pol_x) {
+  const bool use_y = S.y_reset == 0;
+  const double * xold = S.xpar ? S.x1 : S.x0;
+  double * xnew = S.xpar ? S.x0 : S.x1;
+  const float * y = static_cast<const float *>(S.y);
+  SrvGatherXY g{xold, y, use_y};
+  SrvOutR o{xnew, static_cast<float *>(S.r), xold, y, S.b, use_y, 0.0};
+  spmv_row_loop<double, double>(first, end, kSrvCompute, S.n, S.rowptr, S.rowind, S.val64, g,
+      o, pol_m, pol_x);
+  return o.local;
+}
+
+template <typename T, bool MIXED>
+struct WorkA {
+  uint64_t pol_m, pol_x;
+  __device__ __forceinline__ static bool active(const SrvSlot & S) { return S.live && !S.done; }
+
+  __device__ __forceinline__ void rows(const SrvCtx & c, int tid, double & s0, double & s1) {
+    const SrvSlot & S = c.slot;
+    const uint32_t r0 = c.tile.row_begin, r1 = r0 + c.tile.row_count;
+    if (S.a_work == kWorkCg) {
+      const bool par = (S.iter & 1ull) != 0;
+      const T * pold = static_cast<const T *>(par ? S.p1 : S.p0);
+      T * pnew = static_cast<T *>(par ? S.p0 : S.p1);
+      const T * r = static_cast<const T *>(S.r);
+      const T beta = static_cast<T>(S.beta);
+      SrvGatherP<T> g{r, pold, beta};
+      SrvOutA<T> o{static_cast<T *>(S.ap), pnew, r, pold, beta, 0.0};
+      spmv_row_loop<T, T>(r0 + tid, r1, kSrvCompute, S.n, S.rowptr, S.rowind, values_of<T>(S),
+          g, o, pol_m, pol_x);
+      s0 = o.local;
+    } else if (S.a_work == kWorkInit) {
+      T * r = static_cast<T *>(S.r);
+      T * p0 = static_cast<T *>(S.p0);
+      for (uint32_t i = r0 + tid; i < r1; i += kSrvCompute) {
+        const double bv = S.b[i];
+        const T rv = static_cast<T>(bv);
+        S.x0[i] = 0.0;
+        r[i] = rv;
+        p0[i] = T(0);
+        s0 += bv * bv;
+        s1 += static_cast<double>(rv) * static_cast<double>(rv);
       }
-      ap[i] = sum;
-      const T pn = fma(beta, pi, ri);
-      pnew[i] = pn;
-      part += static_cast<double>(pn) * static_cast<double>(sum);
+    } else if (MIXED) {
+      s0 = reliable_rows(S, r0 + tid, r1, pol_m, pol_x);
     }
-    part = warp_sum_d(part);
-    if (lane == 0) d.pa[t] = part;
-    if (slot_arrive(&S.ticket_a, S.ntiles, lane)) {
-      const double pap = slot_sum(d.pa, S.tile0, S.ntiles, lane);
-      if (lane == 0) {
-        S.ticket_a = 0;
-        const double rr = S.rr_hat;
-        if (!(pap > 0.0)) {
-          S.done = 1;
-          S.status = (pap == pap && rr == rr) ? GB_CG_BREAKDOWN : GB_CG_NONFINITE;
-        } else {
-          S.alpha = rr / pap;
-        }
+  }
+
+  __device__ __forceinline__ void finish(const SrvDev & d, uint32_t t, const SrvCtx & c,
+      double2 mine, int lane) {
+    const SrvSlot & C = c.slot;
+    SrvSlot * S = d.slots + c.tile.slot;
+    double2 tot;
+    if (!slot_finish(d.pa, t, mine, &S->ticket_a, C.tile0, C.ntiles, lane, &tot)) return;
+    if (lane != 0) return;
+    S->ticket_a = 0;
+    if (C.a_work == kWorkCg) {
+      const double pap = tot.x;
+      S->b_skip = 0;
+      if (!(pap > 0.0)) {
+        S->done = 1;
+        S->status = (pap == pap && C.rr_hat == C.rr_hat) ? GB_CG_BREAKDOWN : GB_CG_NONFINITE;
+        S->rr_true = C.rr_hat;
+      } else {
+        S->alpha = C.rr_hat / pap;
+      }
+    } else if (C.a_work == kWorkInit) {
+      const double bb = tot.x, rr = MIXED ? tot.y : tot.x;
+      S->bnorm = sqrt(bb);
+      S->tol = C.tol_rel * sqrt(bb);
+      S->rr_true = bb;
+      S->rr_hat = rr;
+      S->rr_hat_old = rr;
+      S->rmax = sqrt(rr);
+      S->alpha = 0.0;
+      S->beta = 0.0;
+      S->iter = 0;
+      S->refinements = 0;
+      S->xpar = 0;
+      S->y_reset = 1;
+      S->final_update = 0;
+      S->status = GB_CG_MAXITER;
+      S->a_work = kWorkCg;
+      S->b_skip = 1;
+      if (bb == 0.0) {
+        S->done = 1;
+        S->status = GB_CG_CONVERGED;
+      } else if (!(bb == bb) || isinf(bb)) {
+        S->done = 1;
+        S->status = GB_CG_NONFINITE;
+      }
+    } else {  // reliable update: r is now the true residual of x
+      const double rr = tot.x;
+      const double rnorm = sqrt(rr);
+      S->rr_true = rr;
+      S->refinements = C.refinements + 1;
+      S->xpar = C.xpar ^ 1;
+      S->y_reset = 1;
+      S->a_work = kWorkCg;
+      S->b_skip = 1;
+      if (!(rnorm == rnorm) || isinf(rnorm)) {
+        S->done = 1;
+        S->status = GB_CG_NONFINITE;
+      } else if (rnorm <= C.tol) {
+        S->done = 1;
+        S->status = GB_CG_CONVERGED;
+      } else if (C.final_update) {
+        S->done = 1;
+        S->status = GB_CG_MAXITER;
+      } else {
+        S->beta = rr / C.rr_hat_old;
+        S->rr_hat = rr;
+        S->rmax = rnorm;
       }
     }
   }
-}
+};
 
 // ---- B: solution / residual update, r.r, stop or update decision --------------------
 
 template <typename T, bool MIXED>
-__global__ void __launch_bounds__(kSrvBlock) srv_b_kernel(const SrvDev d) {
-  pdl_wait_and_release();
-  const int lane = threadIdx.x & 31;
-  const uint32_t nt = *d.ntiles;
-  const uint32_t gw = blockIdx.x * kSrvWarps + (threadIdx.x >> 5);
-  for (uint32_t t = gw; t < nt; t += gridDim.x * kSrvWarps) {
-    const SrvTile tl = d.tiles[t];
-    SrvSlot & S = d.slots[tl.slot];
-    if (!S.live || S.init || S.done) continue;
+struct WorkB {
+  __device__ __forceinline__ static bool active(const SrvSlot & S) {
+    return S.live && !S.done && !S.b_skip;
+  }
+
+  __device__ __forceinline__ void rows(const SrvCtx & c, int tid, double & s0, double &) {
+    const SrvSlot & S = c.slot;
+    const uint32_t r0 = c.tile.row_begin, cnt = c.tile.row_count;
     const T alpha = static_cast<T>(S.alpha);
     const bool fresh = S.y_reset != 0;
     const bool par = (S.iter & 1ull) != 0;
@@ -283,120 +413,88 @@ __global__ void __launch_bounds__(kSrvBlock) srv_b_kernel(const SrvDev d) {
     const T * ap = static_cast<const T *>(S.ap);
     T * r = static_cast<T *>(S.r);
     T * y = static_cast<T *>(S.y);
-    double part = 0.0;
-    for (uint32_t q = lane; q < tl.row_count; q += 32) {
-      const uint32_t i = tl.row_begin + q;
-      const T pn = pnew[i], av = ap[i], rv = r[i];
-      if (MIXED) {
-        const T yv = fresh ? T(0) : y[i];
-        y[i] = fma(alpha, pn, yv);
-      } else {
-        S.x0[i] = fma(static_cast<double>(alpha), static_cast<double>(pn), S.x0[i]);
+    T pv[kRowsPerThread], av[kRowsPerThread], rv[kRowsPerThread];
+    double xv[kRowsPerThread];
+#pragma unroll
+    for (int j = 0; j < kRowsPerThread; ++j) {
+      const uint32_t q = tid + j * kSrvCompute;
+      if (q < cnt) {
+        const uint32_t i = r0 + q;
+        pv[j] = pnew[i];
+        av[j] = ap[i];
+        rv[j] = r[i];
+        if (MIXED) xv[j] = fresh ? 0.0 : static_cast<double>(y[i]);
+        else xv[j] = S.x0[i];
       }
-      const T rn = fma(-alpha, av, rv);
-      r[i] = rn;
-      part += static_cast<double>(rn) * static_cast<double>(rn);
     }
-    part = warp_sum_d(part);
-    if (lane == 0) d.pb[t] = part;
-    if (slot_arrive(&S.ticket_b, S.ntiles, lane)) {
-      const double rr = slot_sum(d.pb, S.tile0, S.ntiles, lane);
-      if (lane == 0) {
-        S.ticket_b = 0;
-        S.y_reset = 0;
-        S.rr_hat_old = S.rr_hat;
-        S.beta = rr / S.rr_hat;
-        S.rr_hat = rr;
-        const unsigned long long it = S.iter + 1;
-        S.iter = it;
-        const double rnorm = sqrt(rr);
-        S.rmax = fmax(S.rmax, rnorm);
-        if (!(rnorm == rnorm) || isinf(rnorm)) {
-          S.done = 1;
-          S.status = GB_CG_NONFINITE;
-        } else if (MIXED) {
-          const bool last = S.niter && it >= S.niter;
-          if (rnorm <= S.tol || rnorm < kSrvDelta * S.rmax || last) {
-            S.update = 1;
-            S.final = last ? 1 : 0;
-          }
+#pragma unroll
+    for (int j = 0; j < kRowsPerThread; ++j) {
+      const uint32_t q = tid + j * kSrvCompute;
+      if (q < cnt) {
+        const uint32_t i = r0 + q;
+        if (MIXED) {
+          y[i] = fma(alpha, pv[j], static_cast<T>(xv[j]));
         } else {
-          if (rnorm <= S.tol) {
-            S.done = 1;
-            S.status = GB_CG_CONVERGED;
-            S.rr_true = rr;
-          } else if (S.niter && it >= S.niter) {
-            S.done = 1;
-            S.status = GB_CG_MAXITER;
-            S.rr_true = rr;
-          }
+          S.x0[i] = fma(static_cast<double>(alpha), static_cast<double>(pv[j]), xv[j]);
         }
+        const T rn = fma(-alpha, av[j], rv[j]);
+        r[i] = rn;
+        s0 += static_cast<double>(rn) * static_cast<double>(rn);
       }
     }
   }
+
+  __device__ __forceinline__ void finish(const SrvDev & d, uint32_t t, const SrvCtx & c,
+      double2 mine, int lane) {
+    const SrvSlot & C = c.slot;
+    SrvSlot * S = d.slots + c.tile.slot;
+    double2 tot;
+    if (!slot_finish(d.pb, t, mine, &S->ticket_b, C.tile0, C.ntiles, lane, &tot)) return;
+    if (lane != 0) return;
+    const double rr = tot.x;
+    S->ticket_b = 0;
+    S->y_reset = 0;
+    S->rr_hat_old = C.rr_hat;
+    S->beta = rr / C.rr_hat;
+    S->rr_hat = rr;
+    const unsigned long long it = C.iter + 1;
+    S->iter = it;
+    const double rnorm = sqrt(rr);
+    S->rmax = fmax(C.rmax, rnorm);
+    if (!(rnorm == rnorm) || isinf(rnorm)) {
+      S->done = 1;
+      S->status = GB_CG_NONFINITE;
+      S->rr_true = rr;
+    } else if (MIXED) {
+      const bool last = C.niter && it >= C.niter;
+      if (rnorm <= C.tol || rnorm < kSrvDelta * fmax(C.rmax, rnorm) || last) {
+        S->a_work = kWorkReliable;
+        S->final_update = last ? 1 : 0;
+      }
+    } else if (rnorm <= C.tol) {
+      S->done = 1;
+      S->status = GB_CG_CONVERGED;
+      S->rr_true = rr;
+    } else if (C.niter && it >= C.niter) {
+      S->done = 1;
+      S->status = GB_CG_MAXITER;
+      S->rr_true = rr;
+    }
+  }
+};
+
+template <typename T, bool MIXED>
+__global__ void __maxnreg__(kSrvMaxRegs) srv_a_kernel(const SrvDev d) {
+  pdl_wait_and_release();
+  WorkA<T, MIXED> w{policy_evict_first(), policy_evict_last()};
+  srv_loop(d, w);
 }
 
-// ---- R: reliable update (mixed) ---------------------------------------------------
-
-__global__ void __launch_bounds__(kSrvBlock) srv_r_kernel(const SrvDev d) {
+template <typename T, bool MIXED>
+__global__ void __maxnreg__(kSrvMaxRegs) srv_b_kernel(const SrvDev d) {
   pdl_wait_and_release();
-  const int lane = threadIdx.x & 31;
-  const uint64_t pol = policy_evict_last();
-  const uint32_t nt = *d.ntiles;
-  const uint32_t gw = blockIdx.x * kSrvWarps + (threadIdx.x >> 5);
-  for (uint32_t t = gw; t < nt; t += gridDim.x * kSrvWarps) {
-    const SrvTile tl = d.tiles[t];
-    SrvSlot & S = d.slots[tl.slot];
-    if (!S.live || S.init || S.done || !S.update) continue;
-    const bool use_y = S.y_reset == 0;
-    const double * xold = S.xpar ? S.x1 : S.x0;
-    double * xnew = S.xpar ? S.x0 : S.x1;
-    const float * y = static_cast<const float *>(S.y);
-    float * r32 = static_cast<float *>(S.r);
-    double part = 0.0;
-    for (uint32_t q = lane; q < tl.row_count; q += 32) {
-      const uint32_t i = tl.row_begin + q;
-      const uint32_t b = __ldg(S.rowptr + i), e = __ldg(S.rowptr + i + 1);
-      double sum = 0.0;
-      for (uint32_t k = b; k < e; ++k) {
-        const uint32_t c = __ldg(S.rowind + k);
-        const double xc = ldv(xold + c, pol) + (use_y ? static_cast<double>(ldv(y + c, pol)) : 0.0);
-        sum = fma(__ldg(S.val64 + k), xc, sum);
-      }
-      xnew[i] = xold[i] + (use_y ? static_cast<double>(y[i]) : 0.0);
-      const double rt = S.b[i] - sum;
-      r32[i] = static_cast<float>(rt);
-      part += rt * rt;
-    }
-    part = warp_sum_d(part);
-    if (lane == 0) d.pr[t] = part;
-    if (slot_arrive(&S.ticket_r, S.ntiles, lane)) {
-      const double tot = slot_sum(d.pr, S.tile0, S.ntiles, lane);
-      if (lane == 0) {
-        S.ticket_r = 0;
-        S.rr_true = tot;
-        S.refinements += 1;
-        S.xpar ^= 1;
-        S.y_reset = 1;
-        S.update = 0;
-        const double rnorm = sqrt(tot);
-        if (!(rnorm == rnorm) || isinf(rnorm)) {
-          S.done = 1;
-          S.status = GB_CG_NONFINITE;
-        } else if (rnorm <= S.tol) {
-          S.done = 1;
-          S.status = GB_CG_CONVERGED;
-        } else if (S.final) {
-          S.done = 1;
-          S.status = GB_CG_MAXITER;
-        } else {
-          S.beta = tot / S.rr_hat_old;
-          S.rr_hat = tot;
-          S.rmax = rnorm;
-        }
-      }
-    }
-  }
+  WorkB<T, MIXED> w;
+  srv_loop(d, w);
 }
 
 // ---- host side --------------------------------------------------------------------
@@ -490,7 +588,7 @@ struct gb_server {
   uint32_t * d_ntiles = nullptr;
   uint32_t * h_ntiles = nullptr;    // pinned
   gb::SrvTile * h_tiles = nullptr;  // pinned staging of the tile list
-  double * d_part = nullptr;        // 5 * kMaxTiles
+  double2 * d_part = nullptr;       // 2 * kMaxTiles (A and B partial sums)
   std::vector<gb::SlotHost> slots;
   std::deque<gb::Request> queue;
   std::vector<gb_server_result_t> results;
@@ -516,9 +614,6 @@ SrvDev dev_view(gb_server & s) {
   d.ntiles = s.d_ntiles;
   d.pa = s.d_part;
   d.pb = s.d_part + kMaxTiles;
-  d.pr = s.d_part + 2 * kMaxTiles;
-  d.pi0 = s.d_part + 3 * kMaxTiles;
-  d.pi1 = s.d_part + 4 * kMaxTiles;
   return d;
 }
 
@@ -527,19 +622,16 @@ int capture_graph(gb_server & s) {
   GB_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
   cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
   const SrvDev d = dev_view(s);
-  if (e == cudaSuccess) {
-    e = s.mixed ? launch_k(srv_init_kernel<float, true>, s.grid, kSrvBlock, 0, cs, false, d)
-                : launch_k(srv_init_kernel<double, false>, s.grid, kSrvBlock, 0, cs, false, d);
-    for (uint32_t k = 0; k < s.cfg.iters_per_step && e == cudaSuccess; ++k) {
-      if (s.mixed) {
-        e = launch_k(srv_a_kernel<float>, s.grid, kSrvBlock, 0, cs, true, d);
-        if (e == cudaSuccess) e = launch_k(srv_b_kernel<float, true>, s.grid, kSrvBlock, 0, cs, true, d);
-        if (e == cudaSuccess) e = launch_k(srv_r_kernel, s.grid, kSrvBlock, 0, cs, true, d);
-      } else {
-        e = launch_k(srv_a_kernel<double>, s.grid, kSrvBlock, 0, cs, true, d);
-        if (e == cudaSuccess)
-          e = launch_k(srv_b_kernel<double, false>, s.grid, kSrvBlock, 0, cs, true, d);
-      }
+  for (uint32_t k = 0; k < s.cfg.iters_per_step && e == cudaSuccess; ++k) {
+    const bool pdl = k > 0;
+    if (s.mixed) {
+      e = launch_k(srv_a_kernel<float, true>, s.grid, kSrvThreads, 0, cs, pdl, d);
+      if (e == cudaSuccess)
+        e = launch_k(srv_b_kernel<float, true>, s.grid, kSrvThreads, 0, cs, true, d);
+    } else {
+      e = launch_k(srv_a_kernel<double, false>, s.grid, kSrvThreads, 0, cs, pdl, d);
+      if (e == cudaSuccess)
+        e = launch_k(srv_b_kernel<double, false>, s.grid, kSrvThreads, 0, cs, true, d);
     }
   }
   cudaGraph_t g = nullptr;
@@ -581,9 +673,9 @@ int create_server(const gb_server_config_t & cfg, gb_server * s) {
   GB_TRY(sm_count_of_current_device(&s->sm_count));
   int occ = 0;
   GB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ,
-      s->mixed ? reinterpret_cast<const void *>(srv_a_kernel<float>)
-               : reinterpret_cast<const void *>(srv_a_kernel<double>), kSrvBlock, 0));
-  s->grid = static_cast<unsigned>(s->sm_count * std::max(1, std::min(occ, 4)));
+      s->mixed ? reinterpret_cast<const void *>(srv_a_kernel<float, true>)
+               : reinterpret_cast<const void *>(srv_a_kernel<double, false>), kSrvThreads, 0));
+  s->grid = static_cast<unsigned>(s->sm_count * std::max(1, std::min(occ, kSrvMinBlocks)));
   GB_CUDA_TRY(cudaMalloc(&s->pool, cfg.pool_bytes));
   s->alloc.reset(cfg.pool_bytes);
   GB_CUDA_TRY(cudaMalloc(&s->d_slots, cfg.max_slots * sizeof(SrvSlot)));
@@ -596,7 +688,7 @@ int create_server(const gb_server_config_t & cfg, gb_server * s) {
   GB_CUDA_TRY(cudaMemset(s->d_ntiles, 0, sizeof(uint32_t)));
   GB_CUDA_TRY(cudaMallocHost(&s->h_ntiles, sizeof(uint32_t)));
   *s->h_ntiles = 0;
-  GB_CUDA_TRY(cudaMalloc(&s->d_part, 5 * kMaxTiles * sizeof(double)));
+  GB_CUDA_TRY(cudaMalloc(&s->d_part, 2 * kMaxTiles * sizeof(double2)));
   s->slots.resize(cfg.max_slots);
   GB_CUDA_TRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
   GB_CUDA_TRY(cudaEventCreateWithFlags(&s->step_done, cudaEventDisableTiming));
@@ -628,23 +720,18 @@ int submit(gb_server & s, uint64_t id, dim_t n, const ind_t * rowptr, const dim_
   q.t_submit = now_s(s);
   q.rowptr.assign(rowptr, rowptr + n + 1);
   GB_CHECK_INPUT(q.rowptr[0] == 0, "rowptr[0] must be 0");
-  // row-aligned warp tiles; rows longer than a tile are refused
-  uint32_t r = 0;
-  while (r < n) {
-    SrvTile t{0, r, 0, 0};
-    uint32_t items = 0;
-    while (r < n) {
-      GB_CHECK_INPUT(q.rowptr[r + 1] >= q.rowptr[r], "rowptr decreases at row %u", r);
-      const uint32_t l = q.rowptr[r + 1] - q.rowptr[r];
-      GB_CHECK_INPUT(l < kTileItems, "row %u has %u nonzeros; the solve server takes at most %u",
-          r, l, kTileItems - 1);
-      if (items + l + 1 > kTileItems) break;
-      items += l + 1;
-      ++r;
-    }
-    t.row_count = r - t.row_begin;
-    q.tiles.push_back(t);
+  for (uint32_t r = 0; r < n; ++r) {
+    GB_CHECK_INPUT(q.rowptr[r + 1] >= q.rowptr[r], "rowptr decreases at row %u", r);
+    const uint32_t l = q.rowptr[r + 1] - q.rowptr[r];
+    GB_CHECK_INPUT(l <= kMaxRowNnz, "row %u has %u nonzeros; the solve server takes at most %u",
+        r, l, kMaxRowNnz);
   }
+  // row tiles: a power of two in [256, 2048] rows, about n / 256 (from n alone,
+  // so a solve is cut the same way whatever else is resident)
+  uint32_t tile_rows = kTileRowsMin;
+  while (tile_rows < kTileRowsMax && tile_rows * kTilesPerSolve < n) tile_rows *= 2;
+  for (uint32_t r = 0; r < n; r += tile_rows)
+    q.tiles.push_back(SrvTile{0, r, std::min(tile_rows, n - r), 0});
   GB_CHECK_INPUT(q.tiles.size() <= kMaxTiles, "request needs %zu tiles, more than %zu",
       q.tiles.size(), kMaxTiles);
   q.rowind.assign(rowind, rowind + nnz);
@@ -732,7 +819,8 @@ int admit(gb_server & s, Request & q, uint32_t k) {
   S.tol_rel = q.tol_rel;
   S.niter = q.niter;
   S.live = 1;
-  S.init = 1;
+  S.a_work = kWorkInit;
+  S.b_skip = 1;
   S.status = GB_CG_MAXITER;
   s.h_slots[k] = S;
   s.dirty = true;
