@@ -573,7 +573,7 @@ def mixed_extra(side=160, rtol=1e-10, reps=2):
     return out
 
 
-def serving_extra(nreq=400, seed=5, rtol=1e-10, pool=16 << 30, slots=256, ips=16,
+def serving_extra(nreq=400, seed=5, rtol=1e-10, pool=16 << 30, slots=256, ips=8,
                   load=0.8):
     """Serving stream of 2D 5-point variable-coefficient SPD systems (side
     log-uniform in [32, 512], coefficients log-uniform in [0.1, 10], b in

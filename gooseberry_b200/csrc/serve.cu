@@ -6,9 +6,8 @@
 // its CSR matrix and Krylov vectors live in one device pool (first-fit
 // allocator, bounded by pool_bytes), and all slots advance together.
 //
-// Work list: every slot's rows are cut into row tiles of 256..2048 rows (a
-// power of two chosen from the slot's size alone); the tiles of all resident
-// slots form ONE global list.  Each kernel is persistent over that list, one
+// Work list: every slot's rows are cut into row tiles of 2048 rows (the last
+// one shorter); the tiles of all resident slots form ONE global list.  Each kernel is persistent over that list, one
 // CTA tile at a time: eight compute warps run the pipelined thread-per-row
 // loop of the single-solve kernels over the tile (coalesced row vectors,
 // reference summation order), while a ninth, control warp prefetches the
@@ -23,9 +22,14 @@
 // Per step (one graph replay): iters_per_step x { A, B }.
 //   A: per slot one of  CG   -- SpMV + direction update + p.Ap
 //                       INIT -- x = 0, r = b, p = 0, b.b (newly admitted)
-//                       R    -- reliable FP64 residual update (mixed)
-//   B: x/y and r update + r.r, stop or update decision; skipped for a slot
-//      whose A launch did INIT or R.
+//   B: per slot one of  UPDATE   -- x/y and r update + r.r, stop or
+//                                   reliable-update decision
+//                       RELIABLE -- reliable FP64 residual update (mixed):
+//                                   x += y, r = b - A x, true r.r
+// A slot idles in the B launch after its INIT and in the A launch before its
+// RELIABLE step.  The rare FP64 step rides in the lighter B kernel so that it
+// adds nothing to the register demand of the SpMV kernel A, which sets the
+// occupancy (3 CTAs of 288 threads per SM).
 // Slot state lives in device memory, so the captured graph never changes;
 // between steps the host reads the slot table back, retires finished solves
 // (x copied out), admits queued requests into freed slots and memory,
@@ -54,17 +58,36 @@ namespace {
 constexpr int kSrvComputeWarps = 8;
 constexpr int kSrvCompute = kSrvComputeWarps * 32;  // row threads per CTA
 constexpr int kSrvThreads = kSrvCompute + 32;       // + the control warp
-constexpr int kSrvMinBlocks = 2;
-constexpr int kSrvMaxRegs = 112;  // 2 CTAs of 288 threads per SM
-constexpr uint32_t kTileRowsMin = 256;
-constexpr uint32_t kTileRowsMax = 2048;
-constexpr int kRowsPerThread = kTileRowsMax / kSrvCompute;  // 8
-constexpr uint32_t kTilesPerSolve = 256;  // tile size target: n / 256 rows
+#ifndef GB_SRV_MIN_BLOCKS
+#define GB_SRV_MIN_BLOCKS 3
+#endif
+#ifndef GB_SRV_MAX_REGS
+#define GB_SRV_MAX_REGS 72
+#endif
+#ifndef GB_SRV_ROW_STAGE
+#define GB_SRV_ROW_STAGE 5
+#endif
+#ifndef GB_SRV_TILE_ROWS
+#define GB_SRV_TILE_ROWS 2048
+#endif
+constexpr int kSrvMinBlocks = GB_SRV_MIN_BLOCKS;
+constexpr int kSrvMaxRegs = GB_SRV_MAX_REGS;  // 3 CTAs of 288 threads per SM at 72
+// Row entries loaded ahead per thread: 5 holds a whole row of a 2-D 5-point
+// stencil (longer rows finish in the loop's tail); measured 1.3x the solves/s
+// of 6 at this register budget.
+constexpr int kSrvRowStage = GB_SRV_ROW_STAGE;
+constexpr uint32_t kTileRows = GB_SRV_TILE_ROWS;
+#ifndef GB_SRV_B_ROWS
+#define GB_SRV_B_ROWS 4
+#endif
+constexpr int kBRows = GB_SRV_B_ROWS;  // rows per thread per pass of the update kernel
 constexpr uint32_t kMaxRowNnz = 255;      // longer rows belong to the single-solve CG
 constexpr double kSrvDelta = 0.1;         // reliable update trigger (see cg_mixed.cu)
 constexpr size_t kMaxTiles = 1u << 20;
 
-enum : int { kWorkCg = 0, kWorkInit = 1, kWorkReliable = 2 };  // what A does for a slot
+// What a launch does for a slot.  A: kWorkCg, kWorkInit or kWorkIdle;
+// B: kWorkUpdate, kWorkReliable or kWorkIdle.
+enum : int { kWorkIdle = 0, kWorkCg = 1, kWorkInit = 2, kWorkUpdate = 3, kWorkReliable = 4 };
 
 struct SrvTile {
   uint32_t slot;
@@ -94,8 +117,8 @@ struct __align__(16) SrvSlot {
   double rr_hat, rr_hat_old, alpha, beta, tol, bnorm, rmax, rr_true;
   unsigned long long iter, refinements;
   int live;     // slot holds a solve
-  int a_work;   // kWorkCg / kWorkInit / kWorkReliable
-  int b_skip;   // the next B launch leaves this slot alone
+  int a_work;   // what the next A launch does for this slot
+  int b_work;   // what the next B launch does for this slot
   int done;     // finished (converged / maxiter / breakdown / nonfinite)
   int status;
   int y_reset;
@@ -274,25 +297,12 @@ struct SrvOutR {  // x_new = x + y;  r = b - A (x + y) rounded to FP32
   }
 };
 
-// Rare (a few times per solve), so kept out of line: its FP64 row pipeline
-// does not add to the register demand of the CG path.
-__device__ __noinline__ double reliable_rows(const SrvSlot & S, uint32_t first, uint32_t end,
-    uint64_t pol_m, uint64_t pol_x) {
-  const bool use_y = S.y_reset == 0;
-  const double * xold = S.xpar ? S.x1 : S.x0;
-  double * xnew = S.xpar ? S.x0 : S.x1;
-  const float * y = static_cast<const float *>(S.y);
-  SrvGatherXY g{xold, y, use_y};
-  SrvOutR o{xnew, static_cast<float *>(S.r), xold, y, S.b, use_y, 0.0};
-  spmv_row_loop<double, double>(first, end, kSrvCompute, S.n, S.rowptr, S.rowind, S.val64, g,
-      o, pol_m, pol_x);
-  return o.local;
-}
-
 template <typename T, bool MIXED>
 struct WorkA {
   uint64_t pol_m, pol_x;
-  __device__ __forceinline__ static bool active(const SrvSlot & S) { return S.live && !S.done; }
+  __device__ __forceinline__ static bool active(const SrvSlot & S) {
+    return S.live && !S.done && S.a_work != kWorkIdle;
+  }
 
   __device__ __forceinline__ void rows(const SrvCtx & c, int tid, double & s0, double & s1) {
     const SrvSlot & S = c.slot;
@@ -305,10 +315,10 @@ struct WorkA {
       const T beta = static_cast<T>(S.beta);
       SrvGatherP<T> g{r, pold, beta};
       SrvOutA<T> o{static_cast<T *>(S.ap), pnew, r, pold, beta, 0.0};
-      spmv_row_loop<T, T>(r0 + tid, r1, kSrvCompute, S.n, S.rowptr, S.rowind, values_of<T>(S),
+      spmv_row_loop<T, T, kSrvRowStage>(r0 + tid, r1, kSrvCompute, S.n, S.rowptr, S.rowind, values_of<T>(S),
           g, o, pol_m, pol_x);
       s0 = o.local;
-    } else if (S.a_work == kWorkInit) {
+    } else {  // kWorkInit
       T * r = static_cast<T *>(S.r);
       T * p0 = static_cast<T *>(S.p0);
       for (uint32_t i = r0 + tid; i < r1; i += kSrvCompute) {
@@ -320,8 +330,6 @@ struct WorkA {
         s0 += bv * bv;
         s1 += static_cast<double>(rv) * static_cast<double>(rv);
       }
-    } else if (MIXED) {
-      s0 = reliable_rows(S, r0 + tid, r1, pol_m, pol_x);
     }
   }
 
@@ -335,7 +343,7 @@ struct WorkA {
     S->ticket_a = 0;
     if (C.a_work == kWorkCg) {
       const double pap = tot.x;
-      S->b_skip = 0;
+      S->b_work = kWorkUpdate;
       if (!(pap > 0.0)) {
         S->done = 1;
         S->status = (pap == pap && C.rr_hat == C.rr_hat) ? GB_CG_BREAKDOWN : GB_CG_NONFINITE;
@@ -343,7 +351,7 @@ struct WorkA {
       } else {
         S->alpha = C.rr_hat / pap;
       }
-    } else if (C.a_work == kWorkInit) {
+    } else {  // kWorkInit
       const double bb = tot.x, rr = MIXED ? tot.y : tot.x;
       S->bnorm = sqrt(bb);
       S->tol = C.tol_rel * sqrt(bb);
@@ -360,7 +368,7 @@ struct WorkA {
       S->final_update = 0;
       S->status = GB_CG_MAXITER;
       S->a_work = kWorkCg;
-      S->b_skip = 1;
+      S->b_work = kWorkIdle;
       if (bb == 0.0) {
         S->done = 1;
         S->status = GB_CG_CONVERGED;
@@ -368,7 +376,85 @@ struct WorkA {
         S->done = 1;
         S->status = GB_CG_NONFINITE;
       }
-    } else {  // reliable update: r is now the true residual of x
+    }
+  }
+};
+
+// ---- B: solution / residual update, r.r, stop or update decision;  or the
+//      reliable FP64 residual update (mixed) ----------------------------------------------
+
+template <typename T, bool MIXED>
+struct WorkB {
+  uint64_t pol_m, pol_x;
+  __device__ __forceinline__ static bool active(const SrvSlot & S) {
+    return S.live && !S.done && S.b_work != kWorkIdle;
+  }
+
+  __device__ __forceinline__ void rows(const SrvCtx & c, int tid, double & s0, double &) {
+    const SrvSlot & S = c.slot;
+    const uint32_t r0 = c.tile.row_begin, cnt = c.tile.row_count;
+    if (MIXED && S.b_work == kWorkReliable) {
+      const bool use_y = S.y_reset == 0;
+      const double * xold = S.xpar ? S.x1 : S.x0;
+      double * xnew = S.xpar ? S.x0 : S.x1;
+      const float * y = static_cast<const float *>(S.y);
+      SrvGatherXY g{xold, y, use_y};
+      SrvOutR o{xnew, static_cast<float *>(S.r), xold, y, S.b, use_y, 0.0};
+      spmv_row_loop<double, double, kSrvRowStage>(r0 + tid, r0 + cnt, kSrvCompute, S.n, S.rowptr, S.rowind,
+          S.val64, g, o, pol_m, pol_x);
+      s0 = o.local;
+      return;
+    }
+    const T alpha = static_cast<T>(S.alpha);
+    const bool fresh = S.y_reset != 0;
+    const bool par = (S.iter & 1ull) != 0;
+    const T * pnew = static_cast<const T *>(par ? S.p0 : S.p1);
+    const T * ap = static_cast<const T *>(S.ap);
+    T * r = static_cast<T *>(S.r);
+    T * y = static_cast<T *>(S.y);
+    // passes of kBRows rows per thread: every load of a pass is in flight at once
+    for (uint32_t base = tid; base < cnt; base += kBRows * kSrvCompute) {
+      T pv[kBRows], av[kBRows], rv[kBRows];
+      double xv[kBRows];
+#pragma unroll
+      for (int j = 0; j < kBRows; ++j) {
+        const uint32_t q = base + j * kSrvCompute;
+        if (q < cnt) {
+          const uint32_t i = r0 + q;
+          pv[j] = pnew[i];
+          av[j] = ap[i];
+          rv[j] = r[i];
+          if (MIXED) xv[j] = fresh ? 0.0 : static_cast<double>(y[i]);
+          else xv[j] = S.x0[i];
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kBRows; ++j) {
+        const uint32_t q = base + j * kSrvCompute;
+        if (q < cnt) {
+          const uint32_t i = r0 + q;
+          if (MIXED) {
+            y[i] = fma(alpha, pv[j], static_cast<T>(xv[j]));
+          } else {
+            S.x0[i] = fma(static_cast<double>(alpha), static_cast<double>(pv[j]), xv[j]);
+          }
+          const T rn = fma(-alpha, av[j], rv[j]);
+          r[i] = rn;
+          s0 += static_cast<double>(rn) * static_cast<double>(rn);
+        }
+      }
+    }
+  }
+
+  __device__ __forceinline__ void finish(const SrvDev & d, uint32_t t, const SrvCtx & c,
+      double2 mine, int lane) {
+    const SrvSlot & C = c.slot;
+    SrvSlot * S = d.slots + c.tile.slot;
+    double2 tot;
+    if (!slot_finish(d.pb, t, mine, &S->ticket_b, C.tile0, C.ntiles, lane, &tot)) return;
+    if (lane != 0) return;
+    S->ticket_b = 0;
+    if (MIXED && C.b_work == kWorkReliable) {  // r is now the true residual of x
       const double rr = tot.x;
       const double rnorm = sqrt(rr);
       S->rr_true = rr;
@@ -376,7 +462,7 @@ struct WorkA {
       S->xpar = C.xpar ^ 1;
       S->y_reset = 1;
       S->a_work = kWorkCg;
-      S->b_skip = 1;
+      S->b_work = kWorkIdle;
       if (!(rnorm == rnorm) || isinf(rnorm)) {
         S->done = 1;
         S->status = GB_CG_NONFINITE;
@@ -391,68 +477,9 @@ struct WorkA {
         S->rr_hat = rr;
         S->rmax = rnorm;
       }
+      return;
     }
-  }
-};
-
-// ---- B: solution / residual update, r.r, stop or update decision --------------------
-
-template <typename T, bool MIXED>
-struct WorkB {
-  __device__ __forceinline__ static bool active(const SrvSlot & S) {
-    return S.live && !S.done && !S.b_skip;
-  }
-
-  __device__ __forceinline__ void rows(const SrvCtx & c, int tid, double & s0, double &) {
-    const SrvSlot & S = c.slot;
-    const uint32_t r0 = c.tile.row_begin, cnt = c.tile.row_count;
-    const T alpha = static_cast<T>(S.alpha);
-    const bool fresh = S.y_reset != 0;
-    const bool par = (S.iter & 1ull) != 0;
-    const T * pnew = static_cast<const T *>(par ? S.p0 : S.p1);
-    const T * ap = static_cast<const T *>(S.ap);
-    T * r = static_cast<T *>(S.r);
-    T * y = static_cast<T *>(S.y);
-    T pv[kRowsPerThread], av[kRowsPerThread], rv[kRowsPerThread];
-    double xv[kRowsPerThread];
-#pragma unroll
-    for (int j = 0; j < kRowsPerThread; ++j) {
-      const uint32_t q = tid + j * kSrvCompute;
-      if (q < cnt) {
-        const uint32_t i = r0 + q;
-        pv[j] = pnew[i];
-        av[j] = ap[i];
-        rv[j] = r[i];
-        if (MIXED) xv[j] = fresh ? 0.0 : static_cast<double>(y[i]);
-        else xv[j] = S.x0[i];
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < kRowsPerThread; ++j) {
-      const uint32_t q = tid + j * kSrvCompute;
-      if (q < cnt) {
-        const uint32_t i = r0 + q;
-        if (MIXED) {
-          y[i] = fma(alpha, pv[j], static_cast<T>(xv[j]));
-        } else {
-          S.x0[i] = fma(static_cast<double>(alpha), static_cast<double>(pv[j]), xv[j]);
-        }
-        const T rn = fma(-alpha, av[j], rv[j]);
-        r[i] = rn;
-        s0 += static_cast<double>(rn) * static_cast<double>(rn);
-      }
-    }
-  }
-
-  __device__ __forceinline__ void finish(const SrvDev & d, uint32_t t, const SrvCtx & c,
-      double2 mine, int lane) {
-    const SrvSlot & C = c.slot;
-    SrvSlot * S = d.slots + c.tile.slot;
-    double2 tot;
-    if (!slot_finish(d.pb, t, mine, &S->ticket_b, C.tile0, C.ntiles, lane, &tot)) return;
-    if (lane != 0) return;
     const double rr = tot.x;
-    S->ticket_b = 0;
     S->y_reset = 0;
     S->rr_hat_old = C.rr_hat;
     S->beta = rr / C.rr_hat;
@@ -468,7 +495,9 @@ struct WorkB {
     } else if (MIXED) {
       const bool last = C.niter && it >= C.niter;
       if (rnorm <= C.tol || rnorm < kSrvDelta * fmax(C.rmax, rnorm) || last) {
-        S->a_work = kWorkReliable;
+        // next launch pair: A idles, B folds y into x and takes the true residual
+        S->a_work = kWorkIdle;
+        S->b_work = kWorkReliable;
         S->final_update = last ? 1 : 0;
       }
     } else if (rnorm <= C.tol) {
@@ -483,17 +512,26 @@ struct WorkB {
   }
 };
 
+// Register budgets: the FP32 kernels are held to 72 so that 3 CTAs fit per
+// SM (the rare FP64 reliable step in B spills there, which costs little);
+// the FP64 forms get 96 and run with their own grid.
 template <typename T, bool MIXED>
-__global__ void __maxnreg__(kSrvMaxRegs) srv_a_kernel(const SrvDev d) {
+struct SrvRegs {
+  static constexpr int a = sizeof(T) == 4 ? kSrvMaxRegs : 96;
+  static constexpr int b = sizeof(T) == 4 ? kSrvMaxRegs : 96;
+};
+
+template <typename T, bool MIXED>
+__global__ void __maxnreg__((SrvRegs<T, MIXED>::a)) srv_a_kernel(const SrvDev d) {
   pdl_wait_and_release();
   WorkA<T, MIXED> w{policy_evict_first(), policy_evict_last()};
   srv_loop(d, w);
 }
 
 template <typename T, bool MIXED>
-__global__ void __maxnreg__(kSrvMaxRegs) srv_b_kernel(const SrvDev d) {
+__global__ void __maxnreg__((SrvRegs<T, MIXED>::b)) srv_b_kernel(const SrvDev d) {
   pdl_wait_and_release();
-  WorkB<T, MIXED> w;
+  WorkB<T, MIXED> w{policy_evict_first(), policy_evict_last()};
   srv_loop(d, w);
 }
 
@@ -578,7 +616,7 @@ struct gb_server {
   gb_server_config_t cfg{};
   bool mixed = true;
   int sm_count = 0;
-  unsigned grid = 0;
+  unsigned grid_a = 0, grid_b = 0;
   std::chrono::steady_clock::time_point t0;
   char * pool = nullptr;
   gb::Pool alloc;
@@ -625,13 +663,13 @@ int capture_graph(gb_server & s) {
   for (uint32_t k = 0; k < s.cfg.iters_per_step && e == cudaSuccess; ++k) {
     const bool pdl = k > 0;
     if (s.mixed) {
-      e = launch_k(srv_a_kernel<float, true>, s.grid, kSrvThreads, 0, cs, pdl, d);
+      e = launch_k(srv_a_kernel<float, true>, s.grid_a, kSrvThreads, 0, cs, pdl, d);
       if (e == cudaSuccess)
-        e = launch_k(srv_b_kernel<float, true>, s.grid, kSrvThreads, 0, cs, true, d);
+        e = launch_k(srv_b_kernel<float, true>, s.grid_b, kSrvThreads, 0, cs, true, d);
     } else {
-      e = launch_k(srv_a_kernel<double, false>, s.grid, kSrvThreads, 0, cs, pdl, d);
+      e = launch_k(srv_a_kernel<double, false>, s.grid_a, kSrvThreads, 0, cs, pdl, d);
       if (e == cudaSuccess)
-        e = launch_k(srv_b_kernel<double, false>, s.grid, kSrvThreads, 0, cs, true, d);
+        e = launch_k(srv_b_kernel<double, false>, s.grid_b, kSrvThreads, 0, cs, true, d);
     }
   }
   cudaGraph_t g = nullptr;
@@ -671,11 +709,16 @@ int create_server(const gb_server_config_t & cfg, gb_server * s) {
   s->mixed = cfg.mode == GB_CG_MIXED;
   s->t0 = std::chrono::steady_clock::now();
   GB_TRY(sm_count_of_current_device(&s->sm_count));
-  int occ = 0;
-  GB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ,
+  // each kernel: one resident wave (it is persistent over the tile list)
+  int occ_a = 0, occ_b = 0;
+  GB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a,
       s->mixed ? reinterpret_cast<const void *>(srv_a_kernel<float, true>)
                : reinterpret_cast<const void *>(srv_a_kernel<double, false>), kSrvThreads, 0));
-  s->grid = static_cast<unsigned>(s->sm_count * std::max(1, std::min(occ, kSrvMinBlocks)));
+  GB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b,
+      s->mixed ? reinterpret_cast<const void *>(srv_b_kernel<float, true>)
+               : reinterpret_cast<const void *>(srv_b_kernel<double, false>), kSrvThreads, 0));
+  s->grid_a = static_cast<unsigned>(s->sm_count * std::max(1, std::min(occ_a, kSrvMinBlocks)));
+  s->grid_b = static_cast<unsigned>(s->sm_count * std::max(1, std::min(occ_b, kSrvMinBlocks)));
   GB_CUDA_TRY(cudaMalloc(&s->pool, cfg.pool_bytes));
   s->alloc.reset(cfg.pool_bytes);
   GB_CUDA_TRY(cudaMalloc(&s->d_slots, cfg.max_slots * sizeof(SrvSlot)));
@@ -726,12 +769,10 @@ int submit(gb_server & s, uint64_t id, dim_t n, const ind_t * rowptr, const dim_
     GB_CHECK_INPUT(l <= kMaxRowNnz, "row %u has %u nonzeros; the solve server takes at most %u",
         r, l, kMaxRowNnz);
   }
-  // row tiles: a power of two in [256, 2048] rows, about n / 256 (from n alone,
-  // so a solve is cut the same way whatever else is resident)
-  uint32_t tile_rows = kTileRowsMin;
-  while (tile_rows < kTileRowsMax && tile_rows * kTilesPerSolve < n) tile_rows *= 2;
-  for (uint32_t r = 0; r < n; r += tile_rows)
-    q.tiles.push_back(SrvTile{0, r, std::min(tile_rows, n - r), 0});
+  // row tiles of kTileRows rows (from n alone, so a solve is cut the same way
+  // whatever else is resident)
+  for (uint32_t r = 0; r < n; r += kTileRows)
+    q.tiles.push_back(SrvTile{0, r, std::min(kTileRows, n - r), 0});
   GB_CHECK_INPUT(q.tiles.size() <= kMaxTiles, "request needs %zu tiles, more than %zu",
       q.tiles.size(), kMaxTiles);
   q.rowind.assign(rowind, rowind + nnz);
@@ -820,7 +861,7 @@ int admit(gb_server & s, Request & q, uint32_t k) {
   S.niter = q.niter;
   S.live = 1;
   S.a_work = kWorkInit;
-  S.b_skip = 1;
+  S.b_work = kWorkIdle;
   S.status = GB_CG_MAXITER;
   s.h_slots[k] = S;
   s.dirty = true;

@@ -439,18 +439,18 @@ struct MinBlocks {
   static constexpr int value = SCHED == SCHED_ROW ? GB_ROW_MIN_BLOCKS : kSpmvMinBlocks;
 };
 
-template <typename V>
+template <typename V, int STAGE>
 struct RowStage {
   uint32_t b = 0, e = 0;
-  uint32_t c[kRowStage];
-  V v[kRowStage];
+  uint32_t c[STAGE];
+  V v[STAGE];
 };
 
-template <typename V>
-__device__ __forceinline__ void row_stage_load(RowStage<V> & s, const uint32_t * rowind,
+template <typename V, int STAGE>
+__device__ __forceinline__ void row_stage_load(RowStage<V, STAGE> & s, const uint32_t * rowind,
     const V * val, uint64_t pol) {
 #pragma unroll
-  for (int j = 0; j < kRowStage; ++j) {
+  for (int j = 0; j < STAGE; ++j) {
     if (s.b + j < s.e) {
       s.c[j] = ld_l1(rowind + s.b + j, pol);
       s.v[j] = ld_l1(val + s.b + j, pol);
@@ -458,7 +458,7 @@ __device__ __forceinline__ void row_stage_load(RowStage<V> & s, const uint32_t *
   }
 }
 
-template <typename V, typename Acc, class Gather, class Out>
+template <typename V, typename Acc, int STAGE = kRowStage, class Gather, class Out>
 __device__ __forceinline__ void spmv_row_loop(uint32_t first, uint32_t end, uint32_t step,
     uint32_t ncols, const uint32_t * __restrict__ rowptr,
     const uint32_t * __restrict__ rowind, const V * __restrict__ val, const Gather & gather,
@@ -466,7 +466,7 @@ __device__ __forceinline__ void spmv_row_loop(uint32_t first, uint32_t end, uint
   const uint32_t cmax = ncols - 1;
   if (first >= end) return;
   // stage L: row `first`; stage P: rowptr pair of row first + step
-  RowStage<V> cur;
+  RowStage<V, STAGE> cur;
   cur.b = __ldg(rowptr + first);
   cur.e = __ldg(rowptr + first + 1);
   typename Out::Pre cur_pre = out.pre(first);
@@ -478,7 +478,7 @@ __device__ __forceinline__ void spmv_row_loop(uint32_t first, uint32_t end, uint
   }
   for (uint32_t i = first; i < end; i += step) {
     // issue the next row's indices/values/operands and the rowptr two ahead
-    RowStage<V> nxt;
+    RowStage<V, STAGE> nxt;
     typename Out::Pre nxt_pre{};
     const uint32_t i1 = i + step, i2 = i + 2 * step;
     if (i1 < end) {
@@ -492,15 +492,15 @@ __device__ __forceinline__ void spmv_row_loop(uint32_t first, uint32_t end, uint
       ne = __ldg(rowptr + i2 + 1);
     }
     // gather and sum the current row (reference order)
-    Acc xv[kRowStage];
+    Acc xv[STAGE];
 #pragma unroll
-    for (int j = 0; j < kRowStage; ++j)
+    for (int j = 0; j < STAGE; ++j)
       if (cur.b + j < cur.e) xv[j] = gather(min(cur.c[j], cmax), pol_x);
     Acc sum = Acc(0);
 #pragma unroll
-    for (int j = 0; j < kRowStage; ++j)
+    for (int j = 0; j < STAGE; ++j)
       if (cur.b + j < cur.e) sum = add_rn(sum, mul_rn(static_cast<Acc>(cur.v[j]), xv[j]));
-    for (uint32_t k = cur.b + kRowStage; k < cur.e; ++k)  // long-row tail
+    for (uint32_t k = cur.b + STAGE; k < cur.e; ++k)  // long-row tail
       sum = add_rn(sum, mul_rn(static_cast<Acc>(ld_l1(val + k, pol_matrix)),
                                gather(min(ld_l1(rowind + k, pol_matrix), cmax), pol_x)));
     out.row_pre(i, sum, cur_pre);
