@@ -32,7 +32,7 @@ __all__ = [
     "GooseberryError", "lib", "spmult", "scale", "add_scalar", "cgd",
     "CsrMatrix", "CgSolver", "CgResult", "dot", "SUCCESS",
     "SCHED_AUTO", "SCHED_THREAD", "SCHED_GROUP4", "SCHED_GROUP8", "SCHED_WARP",
-    "SCHED_MERGE", "SCHED_ROW", "SCHED_WTILE", "CG_F64", "CG_MIXED", "plan_tiles",
+    "SCHED_MERGE", "SCHED_ROW", "SCHED_WTILE", "SCHED_WMERGE", "CG_F64", "CG_MIXED", "plan_tiles",
     "Server", "ServerResult",
 ]
 
@@ -46,9 +46,9 @@ ERROR_NAMES = {
 }
 VALUES_F64, VALUES_F32, DEVICE_POINTERS = 0x1, 0x2, 0x4
 (SCHED_AUTO, SCHED_THREAD, SCHED_GROUP4, SCHED_GROUP8, SCHED_WARP, SCHED_MERGE, SCHED_ROW,
- SCHED_WTILE) = range(8)
+ SCHED_WTILE, SCHED_WMERGE) = range(9)
 SCHED_NAMES = {0: "auto", 1: "thread", 2: "group4", 3: "group8", 4: "warp", 5: "merge",
-               6: "row", 7: "wtile"}
+               6: "row", 7: "wtile", 8: "wmerge"}
 CG_F64, CG_MIXED = 0, 1
 CG_PERSISTENT = 0x100
 CG_STATUS = {0: "converged", 1: "maxiter", 2: "breakdown", 3: "nonfinite"}

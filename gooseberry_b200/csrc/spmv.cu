@@ -163,11 +163,14 @@ struct OutStore {
   __device__ __forceinline__ void row_pre(uint32_t r, Acc v, const Pre &) { row(r, v); }
 };
 
-template <typename V, typename Acc, int SCHED, class Gather, class Out>
-__global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) spmv_tiles_kernel(const PlanView plan,
-    const uint32_t * __restrict__ rowptr, const uint32_t * __restrict__ rowind,
-    const V * __restrict__ val, const Gather gather, Out out) {
-  spmv_tiles_body<V, Acc, SCHED, kSpmvBlock>(plan, rowptr, rowind, val, gather, out);
+template <typename V, typename Acc, int SCHED, class Gather, class Out, bool DIRECT>
+__global__ void __launch_bounds__(DIRECT ? kDirectBlock : kSpmvBlock,
+    DIRECT ? kDirectMinBlocks : MinBlocks<SCHED>::value)
+spmv_tiles_kernel(const PlanView plan, const uint32_t * __restrict__ rowptr,
+    const uint32_t * __restrict__ rowind, const V * __restrict__ val, const Gather gather,
+    Out out) {
+  spmv_tiles_body<V, Acc, SCHED, DIRECT ? kDirectBlock : kSpmvBlock, Gather, Out, DIRECT>(
+      plan, rowptr, rowind, val, gather, out);
 }
 
 __global__ void max_index_kernel(const uint32_t * __restrict__ ind, uint32_t n,
@@ -190,7 +193,7 @@ __global__ void round_f32_kernel(const double * __restrict__ in, float * __restr
 // ---- launch helpers ---------------------------------------------------------
 
 // Resident CTAs per SM of a kernel at a dynamic shared-memory size (cached).
-int occupancy(const void * func, size_t smem, int * out) {
+int occupancy(const void * func, size_t smem, int * out, int block = kSpmvBlock) {
   static std::mutex mu;
   static std::map<std::pair<const void *, size_t>, int> cache;
   std::lock_guard<std::mutex> lock(mu);
@@ -210,7 +213,7 @@ int occupancy(const void * func, size_t smem, int * out) {
     GB_CUDA_TRY(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize,
         static_cast<int>(smem)));
   int n = 0;
-  GB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, func, kSpmvBlock, smem));
+  GB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, func, block, smem));
   if (n < 1) {
     set_error("SpMV kernel cannot be resident with %zu bytes of shared memory", smem);
     return GOOSEBERRY_ERROR_UNKNOWN;
@@ -224,14 +227,25 @@ template <typename V, typename Acc, int SCHED, class Gather, class Out>
 int launch_tiles(const gb_csr & a, const V * val, const Gather & g, const Out & o,
     cudaStream_t stream) {
   if (a.plan.tiles.empty()) return GOOSEBERRY_SUCCESS;
-  auto kern = spmv_tiles_kernel<V, Acc, SCHED, Gather, Out>;
-  const size_t smem = spmv_smem_bytes<V, Acc>(SCHED, a.plan.tile_items, kSpmvBlock);
+  auto kern = spmv_tiles_kernel<V, Acc, SCHED, Gather, Out, false>;
+  size_t smem = spmv_smem_bytes<V, Acc>(SCHED, a.plan.tile_items, kSpmvBlock);
+  int block = kSpmvBlock;
+  if constexpr (IsPlainGather<Gather>::value && SCHED != SCHED_ROW && SCHED != SCHED_WTILE &&
+                SCHED != SCHED_WMERGE) {
+    // plain y = A x on CTA tiles: the direct register pipeline when the tile
+    // fits its per-thread item budget
+    if (a.plan.tile_items <= static_cast<uint32_t>(kDirectKt * kDirectBlock)) {
+      kern = spmv_tiles_kernel<V, Acc, SCHED, Gather, Out, true>;
+      smem = DirectSmem<Acc>::bytes(a.plan.tile_items);
+      block = kDirectBlock;
+    }
+  }
   int occ = 0;
-  GB_TRY(occupancy(reinterpret_cast<const void *>(kern), smem, &occ));
+  GB_TRY(occupancy(reinterpret_cast<const void *>(kern), smem, &occ, block));
   const uint32_t units = spmv_work_units(SCHED, a.nrows,
-      static_cast<uint32_t>(a.plan.tiles.size()), kSpmvBlock);
+      static_cast<uint32_t>(a.plan.tiles.size()), block);
   const uint32_t grid = std::min<uint32_t>(units, static_cast<uint32_t>(a.sm_count * occ));
-  kern<<<grid, kSpmvBlock, smem, stream>>>(plan_view(a), a.rowptr, a.rowind, val, g, o);
+  kern<<<grid, block, smem, stream>>>(plan_view(a), a.rowptr, a.rowind, val, g, o);
   GB_CUDA_TRY(cudaGetLastError());
   return GOOSEBERRY_SUCCESS;
 }
@@ -247,6 +261,7 @@ int launch_sched(const gb_csr & a, int sched, const V * val, const Gather & g,
     case GB_SCHED_MERGE: return launch_tiles<V, Acc, SCHED_MERGE>(a, val, g, o, stream);
     case GB_SCHED_ROW: return launch_tiles<V, Acc, SCHED_ROW>(a, val, g, o, stream);
     case GB_SCHED_WTILE: return launch_tiles<V, Acc, SCHED_WTILE>(a, val, g, o, stream);
+    case GB_SCHED_WMERGE: return launch_tiles<V, Acc, SCHED_WMERGE>(a, val, g, o, stream);
     default:
       set_error("unknown SpMV schedule %d", sched);
       return GOOSEBERRY_ERROR_INVALIDINPUT;
@@ -371,7 +386,8 @@ int autotune(gb_csr & a, unsigned width, cudaStream_t stream) {
   const bool short_rows = a.plan.p99 <= 64 && a.plan.max_row <= 4096;
   if (short_rows) cands.push_back({1024, GB_SCHED_ROW});
   for (uint32_t t : {128u, 256u, 512u}) cands.push_back({t, GB_SCHED_WTILE});
-  for (uint32_t t : {1024u, 2048u, 4096u}) {
+  cands.push_back({static_cast<uint32_t>(32 * kWmKt), GB_SCHED_WMERGE});
+  for (uint32_t t : {512u, 1024u, 2048u, 4096u}) {
     if (a.plan.p90 <= 64) cands.push_back({t, GB_SCHED_THREAD});
     cands.push_back({t, GB_SCHED_GROUP4});
     cands.push_back({t, GB_SCHED_GROUP8});
@@ -593,7 +609,7 @@ int gb_csr_get_info(const gb_csr_t * a, gb_csr_info_t * info) {
 int gb_csr_set_schedule(gb_csr_t * a, unsigned value_width, int schedule,
     uint32_t tile_items) {
   GB_CHECK_INPUT(a != nullptr, "matrix is NULL");
-  GB_CHECK_INPUT(schedule >= GB_SCHED_AUTO && schedule <= GB_SCHED_WTILE,
+  GB_CHECK_INPUT(schedule >= GB_SCHED_AUTO && schedule <= GB_SCHED_WMERGE,
       "unknown schedule %d", schedule);
   GB_CHECK_INPUT(value_width == GB_CSR_VALUES_F64 || value_width == GB_CSR_VALUES_F32,
       "value_width must be GB_CSR_VALUES_F64 or GB_CSR_VALUES_F32");
@@ -603,6 +619,13 @@ int gb_csr_set_schedule(gb_csr_t * a, unsigned value_width, int schedule,
     tile_items = 256;
   GB_CHECK_INPUT(schedule != GB_SCHED_WTILE || (tile_items ? tile_items : a->plan.tile_items) <= 512,
       "per-warp tiles need tile_items <= 512");
+  // per-warp merge tiles: at most kWmKt items per lane
+  constexpr uint32_t wm_max = 32 * gb::kWmKt;
+  if (schedule == GB_SCHED_WMERGE && tile_items == 0 && a->plan.tile_items > wm_max)
+    tile_items = wm_max;
+  GB_CHECK_INPUT(schedule != GB_SCHED_WMERGE ||
+                     (tile_items ? tile_items : a->plan.tile_items) <= wm_max,
+      "per-warp merge tiles need tile_items <= %u", wm_max);
   if (tile_items) GB_TRY(gb::rebuild_plan(*a, tile_items, nullptr));
   const int s = schedule == GB_SCHED_AUTO ? gb::default_schedule(a->plan) : schedule;
   (value_width == GB_CSR_VALUES_F32 ? a->sched32 : a->sched64) = s;

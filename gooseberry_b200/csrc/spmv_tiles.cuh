@@ -40,7 +40,8 @@ enum : int {
   SCHED_WARP = GB_SCHED_WARP,
   SCHED_MERGE = GB_SCHED_MERGE,
   SCHED_ROW = GB_SCHED_ROW,
-  SCHED_WTILE = GB_SCHED_WTILE
+  SCHED_WTILE = GB_SCHED_WTILE,
+  SCHED_WMERGE = GB_SCHED_WMERGE
 };
 
 constexpr int kSpmvBlock = 256;
@@ -434,9 +435,14 @@ __device__ __forceinline__ void spmv_tile_loop(const PlanView & plan, uint32_t t
 #endif
 constexpr int kRowStage = GB_ROW_STAGE;
 // resident CTAs per SM the register budget of a kernel is sized for
+#ifndef GB_WMERGE_MIN_BLOCKS
+#define GB_WMERGE_MIN_BLOCKS 3
+#endif
 template <int SCHED>
 struct MinBlocks {
-  static constexpr int value = SCHED == SCHED_ROW ? GB_ROW_MIN_BLOCKS : kSpmvMinBlocks;
+  static constexpr int value = SCHED == SCHED_ROW      ? GB_ROW_MIN_BLOCKS
+                               : SCHED == SCHED_WMERGE ? GB_WMERGE_MIN_BLOCKS
+                                                       : kSpmvMinBlocks;
 };
 
 template <typename V, int STAGE>
@@ -515,10 +521,13 @@ __device__ __forceinline__ void spmv_row_loop(uint32_t first, uint32_t end, uint
 // while its lanes sum tile t, cp.async already streams tile t + step (rowptr
 // slice, indices, values) into the warp's other shared-memory stage.  Only
 // warp-level synchronisation is needed, so every warp of the SM keeps its own
-// tile in flight (the CTA-wide tile loop above has one per CTA).  A lane sums
-// whole rows, k ascending with unfused multiply and add, exactly like the
-// reference (src/blas.c:85-88): the result is bit-identical to blas_spmult.
-// kStage x values are gathered per lane before any is consumed.
+// tile in flight (the CTA-wide tile loop above has one per CTA).  Per tile
+// the products are formed nonzero-parallel (lane k, k + 32, ...; kStage x
+// gathers in flight per lane whatever the row lengths, each product rounded
+// on its own and written over its value in shared memory), then a lane sums
+// whole rows of products, k ascending, exactly like the reference's
+// unfused multiply-then-add loop (src/blas.c:85-88): the result is
+// bit-identical to blas_spmult.
 
 template <typename V>
 struct WarpSmem {
@@ -613,21 +622,31 @@ __device__ __forceinline__ void spmv_warp_loop(const PlanView & plan, uint32_t t
     } else {
       const uint32_t * so = offs_of(s);
       const uint32_t * si = ind_of(s);
-      const V * sv = val_of(s);
+      V * sv = val_of(s);
+      // products, nonzero-parallel: every lane keeps kStage gathers in flight
+      // whatever the row lengths; each product replaces its value in place
+      const int N = static_cast<int>(d.nnz_count);
+      for (int base = 0; base < N; base += kStage * 32) {
+        Acc xv[kStage];
+#pragma unroll
+        for (int j = 0; j < kStage; ++j) {
+          const int k = base + lane + j * 32;
+          if (k < N) xv[j] = gather(min(si[k], cmax), pol_x);
+        }
+#pragma unroll
+        for (int j = 0; j < kStage; ++j) {
+          const int k = base + lane + j * 32;
+          if (k < N) sv[k] = static_cast<V>(mul_rn(static_cast<Acc>(sv[k]), xv[j]));
+        }
+      }
+      __syncwarp();
+      // row sums, one row per lane, k ascending (the reference's order)
       for (uint32_t r = lane; r < d.row_count; r += 32) {
         const uint32_t i = d.row_begin + r;
         const typename Out::Pre pre = out.pre(i);
         const uint32_t b = so[r] - nb, e = so[r + 1] - nb;
         Acc sum = Acc(0);
-        for (uint32_t base = b; base < e; base += kStage) {
-          Acc xv[kStage];
-#pragma unroll
-          for (int j = 0; j < kStage; ++j)
-            if (base + j < e) xv[j] = gather(min(si[base + j], cmax), pol_x);
-#pragma unroll
-          for (int j = 0; j < kStage; ++j)
-            if (base + j < e) sum = add_rn(sum, mul_rn(static_cast<Acc>(sv[base + j]), xv[j]));
-        }
+        for (uint32_t k = b; k < e; ++k) sum = add_rn(sum, static_cast<Acc>(sv[k]));
         out.row_pre(i, sum, pre);
       }
     }
@@ -637,25 +656,435 @@ __device__ __forceinline__ void spmv_warp_loop(const PlanView & plan, uint32_t t
   cp_async_wait<0>();
 }
 
+// ---- plain SpMV: direct register pipeline -------------------------------------
+//
+// For y = A x the tile's column indices and values are used only by the
+// thread that gathers for them, so they need no shared-memory staging: each
+// thread owns the items k = tid + j * BLOCK of a tile and loads their indices
+// and values straight into registers (coalesced), one tile ahead.  Per tile:
+// the x gathers of the current tile are issued first, then the next tile's
+// index/value loads and the current tile's rowptr slice; the products go to
+// shared memory only for the row reduction (the same reduce_tile as the staged
+// loop, so rows are summed in the same order).  This keeps the L1 traffic to
+// the gathers, the matrix stream and one product write + read per nonzero
+// (the staged loop also writes and reads indices and values through shared
+// memory), and it holds fewer registers, so more CTAs stay resident.
+template <typename X>
+struct IsPlainGather {
+  static constexpr bool value = false;
+};
+template <typename X>
+struct IsPlainGather<GatherPlain<X>> {
+  static constexpr bool value = true;
+};
+
+// Shared memory of the direct loop: rowptr slice (tile_items + 1) and products.
+template <typename Acc>
+struct DirectSmem {
+  static __host__ __device__ size_t offs_bytes(uint32_t t) {
+    return (sizeof(uint32_t) * (t + 1) + 15) & ~size_t(15);
+  }
+  static __host__ __device__ size_t bytes(uint32_t t) {
+    return offs_bytes(t) + ((sizeof(Acc) * t + 15) & ~size_t(15));
+  }
+};
+
+#ifndef GB_DIRECT_KT
+#define GB_DIRECT_KT 4
+#endif
+#ifndef GB_DIRECT_MIN_BLOCKS
+#define GB_DIRECT_MIN_BLOCKS 6
+#endif
+#ifndef GB_DIRECT_BLOCK
+#define GB_DIRECT_BLOCK 128
+#endif
+constexpr int kDirectKt = GB_DIRECT_KT;  // items per thread per tile (tile <= kDirectKt * BLOCK)
+constexpr int kDirectMinBlocks = GB_DIRECT_MIN_BLOCKS;
+constexpr int kDirectBlock = GB_DIRECT_BLOCK;  // threads per CTA of the direct loop
+
+template <typename V, typename Acc, int SCHED, int BLOCK, class Out>
+__device__ __forceinline__ void spmv_direct_loop(const PlanView & plan, uint32_t t_begin,
+    uint32_t t_end, uint32_t t_step, const uint32_t * __restrict__ rowptr,
+    const uint32_t * __restrict__ rowind, const V * __restrict__ val,
+    const Acc * __restrict__ x, Out & out, uint64_t pol_matrix, uint64_t pol_x) {
+  extern __shared__ __align__(16) unsigned char gb_smem[];
+  __shared__ Acc scan_v[BLOCK / 32];
+  __shared__ uint32_t scan_k[BLOCK / 32];
+  __shared__ Acc red[32];
+  constexpr int KT = kDirectKt;
+  const uint32_t T = plan.tile_items;
+  uint32_t * offs = reinterpret_cast<uint32_t *>(gb_smem);
+  Acc * prod = reinterpret_cast<Acc *>(gb_smem + DirectSmem<Acc>::offs_bytes(T));
+  const uint32_t cmax = plan.ncols - 1;
+  const int tid = threadIdx.x;
+
+  // per-tile register state: indices (loaded two tiles ahead), values and
+  // rowptr slice (one tile ahead), gathered x (issued one tile ahead)
+  uint32_t c[KT];
+  V v[KT];
+  Acc xv[KT];
+  uint32_t o[KT + 1];
+  auto load_ind = [&](const TileDesc & d) {
+    if (d.row_count == 0) return;  // long-row chunks stream when they run
+#pragma unroll
+    for (int j = 0; j < KT; ++j) {
+      const uint32_t k = tid + j * BLOCK;
+      if (k < d.nnz_count) c[j] = ld_stream(rowind + d.nnz_begin + k, pol_matrix);
+    }
+  };
+  auto load_rest = [&](const TileDesc & d) {  // values and rowptr slice
+    if (d.row_count == 0) return;
+#pragma unroll
+    for (int j = 0; j < KT; ++j) {
+      const uint32_t k = tid + j * BLOCK;
+      if (k < d.nnz_count) v[j] = ld_stream(val + d.nnz_begin + k, pol_matrix);
+    }
+#pragma unroll
+    for (int j = 0; j <= KT; ++j) {
+      const uint32_t r = tid + j * BLOCK;
+      if (r <= d.row_count) o[j] = __ldg(rowptr + d.row_begin + r);
+    }
+  };
+  auto gather_all = [&](const TileDesc & d) {
+    if (d.row_count == 0) return;
+#pragma unroll
+    for (int j = 0; j < KT; ++j) {
+      const uint32_t k = tid + j * BLOCK;
+      if (k < d.nnz_count) xv[j] = ld_keep(x + min(c[j], cmax), pol_x);
+    }
+  };
+  auto tile_at = [&](uint32_t t) { return t < t_end ? plan.tiles[t] : TileDesc{0, 1, 0, 0}; };
+
+  if (t_begin >= t_end) return;
+  TileDesc d_cur = plan.tiles[t_begin];
+  TileDesc d_nxt = tile_at(t_begin + t_step);
+  TileDesc d_nn = tile_at(t_begin + 2 * t_step);
+  load_ind(d_cur);
+  load_rest(d_cur);
+  gather_all(d_cur);
+  load_ind(d_nxt);
+  for (uint32_t t = t_begin; t < t_end; t += t_step) {
+    const bool has_next = t + t_step < t_end;
+    const uint32_t nb = d_cur.nnz_begin;
+    const int N = static_cast<int>(d_cur.nnz_count);
+    if (d_cur.row_count == 0) {
+      // ---- chunk of a long row (up to kChunkTiles tiles of nonzeros): stream
+      // indices and values, KT gathers in flight per thread
+      Acc sum = Acc(0);
+      for (int base = 0; base < N; base += KT * BLOCK) {
+        uint32_t cc[KT];
+        V vv[KT];
+#pragma unroll
+        for (int j = 0; j < KT; ++j) {
+          const int k = base + tid + j * BLOCK;
+          if (k < N) {
+            cc[j] = ld_stream(rowind + nb + k, pol_matrix);
+            vv[j] = ld_stream(val + nb + k, pol_matrix);
+          }
+        }
+        Acc xx[KT];
+#pragma unroll
+        for (int j = 0; j < KT; ++j) {
+          const int k = base + tid + j * BLOCK;
+          if (k < N) xx[j] = ld_keep(x + min(cc[j], cmax), pol_x);
+        }
+#pragma unroll
+        for (int j = 0; j < KT; ++j) {
+          const int k = base + tid + j * BLOCK;
+          if (k < N) sum += static_cast<Acc>(vv[j]) * xx[j];
+        }
+      }
+      // start the next tile (its indices are in c) before this chunk's reduction
+      if (has_next) {
+        load_rest(d_nxt);
+        gather_all(d_nxt);
+        load_ind(d_nn);
+      }
+      const TileDesc d_n3 = tile_at(t + 3 * t_step);
+      sum = block_sum(sum, red);
+      if (tid == 0) {
+        plan.chunk_partial[t] = static_cast<double>(sum);
+        __threadfence();
+        const LongRowDesc L = plan.longrows[d_cur.row_begin];
+        const unsigned prev = atomicAdd(plan.long_count + d_cur.row_begin, 1u);
+        if (prev == L.nchunks - 1) {
+          __threadfence();
+          Acc tot = Acc(0);
+          for (uint32_t q = 0; q < L.nchunks; ++q)
+            tot += static_cast<Acc>(__ldcg(plan.chunk_partial + L.first_tile + q));
+          plan.long_count[d_cur.row_begin] = 0u;  // ready for the next launch
+          out.long_row(d_cur.row_begin, L.row, tot);
+        }
+      }
+      __syncthreads();
+      d_cur = d_nxt;
+      d_nxt = d_nn;
+      d_nn = d_n3;
+      continue;
+    }
+    // ---- row tile: products and rowptr slice into shared memory
+    const int R = static_cast<int>(d_cur.row_count);
+#pragma unroll
+    for (int j = 0; j < KT; ++j) {
+      const int k = tid + j * BLOCK;
+      if (k < N) prod[k] = static_cast<Acc>(v[j]) * xv[j];
+    }
+#pragma unroll
+    for (int j = 0; j <= KT; ++j) {
+      const int r = tid + j * BLOCK;
+      if (r <= R) offs[r] = o[j] - nb;
+    }
+    __syncthreads();
+    // the next tile's gathers and loads are in flight during this reduction
+    if (has_next) {
+      gather_all(d_nxt);
+      load_rest(d_nxt);
+      load_ind(d_nn);
+    }
+    const TileDesc d_n3 = tile_at(t + 3 * t_step);
+    reduce_tile<SCHED, BLOCK, Acc>(prod, offs, d_cur.row_begin, R, N, out, scan_v, scan_k);
+    __syncthreads();  // offs / prod are free again
+    d_cur = d_nxt;
+    d_nxt = d_nn;
+    d_nn = d_n3;
+  }
+}
+
+// ---- per-warp merge tiles ------------------------------------------------------
+//
+// Per-warp tiles of at most 32 * kWmKt items (rows + nonzeros), no CTA-wide
+// barrier anywhere: every warp is its own pipeline.  Lanes own the items
+// lane + 32 j of a tile; their column indices are loaded two tiles ahead,
+// values and the rowptr slice one tile ahead, and the x gathers of tile t + 1
+// are issued before tile t is reduced, so gathers stay in flight while the
+// warp reduces.  The products and the rowptr slice go to the warp's own
+// shared memory; the reduction walks the merge path of (row ends, nonzeros):
+// each lane takes an equal share of it whatever the row lengths, sums its run
+// of products sequentially, and a segmented shuffle scan carries the partial
+// sums of rows that span lanes.  A row's sum is thus a short left-to-right
+// sum per lane plus a tree over at most 32 lanes (within the condition-scaled
+// tolerance of the reference's sequential sum, not bit-identical).  Long rows
+// are chunks as in the other schedules.
+#ifndef GB_WMERGE_KT
+#define GB_WMERGE_KT 4
+#endif
+constexpr int kWmKt = GB_WMERGE_KT;  // items per lane per tile: tile_items <= 32 * kWmKt
+
+template <typename Acc>
+struct WMergeSmem {
+  static __host__ __device__ size_t offs_bytes(uint32_t t) {
+    return (sizeof(uint32_t) * (t + 1) + 15) & ~size_t(15);
+  }
+  static __host__ __device__ size_t warp_bytes(uint32_t t) {
+    return offs_bytes(t) + ((sizeof(Acc) * t + 15) & ~size_t(15));
+  }
+  static __host__ __device__ size_t bytes(uint32_t t, int warps) {
+    return static_cast<size_t>(warps) * warp_bytes(t);
+  }
+};
+
+template <typename V, typename Acc, class Gather, class Out>
+__device__ __forceinline__ void spmv_wmerge_loop(const PlanView & plan, uint32_t t_first,
+    uint32_t t_end, uint32_t t_step, const uint32_t * __restrict__ rowptr,
+    const uint32_t * __restrict__ rowind, const V * __restrict__ val, const Gather & gather,
+    Out & out, uint64_t pol_matrix, uint64_t pol_x) {
+  extern __shared__ __align__(16) unsigned char gb_smem[];
+  constexpr int KT = kWmKt;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t T = plan.tile_items;
+  unsigned char * mine = gb_smem + static_cast<size_t>(warp) * WMergeSmem<Acc>::warp_bytes(T);
+  uint32_t * offs = reinterpret_cast<uint32_t *>(mine);
+  Acc * prod = reinterpret_cast<Acc *>(mine + WMergeSmem<Acc>::offs_bytes(T));
+  const uint32_t cmax = plan.ncols - 1;
+
+  uint32_t c[KT];
+  V v[KT];
+  Acc xv[KT];
+  uint32_t o[KT + 1];
+  auto load_ind = [&](const TileDesc & d) {
+    if (d.row_count == 0) return;  // long-row chunks stream when they run
+#pragma unroll
+    for (int j = 0; j < KT; ++j) {
+      const uint32_t k = lane + j * 32;
+      if (k < d.nnz_count) c[j] = ld_stream(rowind + d.nnz_begin + k, pol_matrix);
+    }
+  };
+  auto load_rest = [&](const TileDesc & d) {  // values and rowptr slice
+    if (d.row_count == 0) return;
+#pragma unroll
+    for (int j = 0; j < KT; ++j) {
+      const uint32_t k = lane + j * 32;
+      if (k < d.nnz_count) v[j] = ld_stream(val + d.nnz_begin + k, pol_matrix);
+    }
+#pragma unroll
+    for (int j = 0; j <= KT; ++j) {
+      const uint32_t r = lane + j * 32;
+      if (r <= d.row_count) o[j] = __ldg(rowptr + d.row_begin + r);
+    }
+  };
+  auto gather_all = [&](const TileDesc & d) {
+    if (d.row_count == 0) return;
+#pragma unroll
+    for (int j = 0; j < KT; ++j) {
+      const uint32_t k = lane + j * 32;
+      if (k < d.nnz_count) xv[j] = gather(min(c[j], cmax), pol_x);
+    }
+  };
+  auto tile_at = [&](uint32_t t) { return t < t_end ? plan.tiles[t] : TileDesc{0, 1, 0, 0}; };
+
+  if (t_first >= t_end) return;
+  TileDesc d_cur = plan.tiles[t_first];
+  TileDesc d_nxt = tile_at(t_first + t_step);
+  TileDesc d_nn = tile_at(t_first + 2 * t_step);
+  load_ind(d_cur);
+  load_rest(d_cur);
+  gather_all(d_cur);
+  load_ind(d_nxt);
+  for (uint32_t t = t_first; t < t_end; t += t_step) {
+    const bool has_next = t + t_step < t_end;
+    const uint32_t nb = d_cur.nnz_begin;
+    const int N = static_cast<int>(d_cur.nnz_count);
+    if (d_cur.row_count == 0) {
+      // ---- chunk of a long row: the warp streams it, KT gathers per lane
+      Acc sum = Acc(0);
+      for (int base = 0; base < N; base += KT * 32) {
+        uint32_t cc[KT];
+        V vv[KT];
+#pragma unroll
+        for (int j = 0; j < KT; ++j) {
+          const int k = base + lane + j * 32;
+          if (k < N) {
+            cc[j] = ld_stream(rowind + nb + k, pol_matrix);
+            vv[j] = ld_stream(val + nb + k, pol_matrix);
+          }
+        }
+        Acc xx[KT];
+#pragma unroll
+        for (int j = 0; j < KT; ++j) {
+          const int k = base + lane + j * 32;
+          if (k < N) xx[j] = gather(min(cc[j], cmax), pol_x);
+        }
+#pragma unroll
+        for (int j = 0; j < KT; ++j) {
+          const int k = base + lane + j * 32;
+          if (k < N) sum += static_cast<Acc>(vv[j]) * xx[j];
+        }
+      }
+      if (has_next) {
+        load_rest(d_nxt);
+        gather_all(d_nxt);
+        load_ind(d_nn);
+      }
+      const TileDesc d_n3 = tile_at(t + 3 * t_step);
+      sum = group_sum<32>(sum);
+      if (lane == 0) {
+        plan.chunk_partial[t] = static_cast<double>(sum);
+        __threadfence();
+        const LongRowDesc L = plan.longrows[d_cur.row_begin];
+        const unsigned prev = atomicAdd(plan.long_count + d_cur.row_begin, 1u);
+        if (prev == L.nchunks - 1) {
+          __threadfence();
+          Acc tot = Acc(0);
+          for (uint32_t q = 0; q < L.nchunks; ++q)
+            tot += static_cast<Acc>(__ldcg(plan.chunk_partial + L.first_tile + q));
+          plan.long_count[d_cur.row_begin] = 0u;  // ready for the next launch
+          out.long_row(d_cur.row_begin, L.row, tot);
+        }
+      }
+      __syncwarp();
+      d_cur = d_nxt;
+      d_nxt = d_nn;
+      d_nn = d_n3;
+      continue;
+    }
+    // ---- row tile: products and rowptr slice into the warp's shared memory
+    const int R = static_cast<int>(d_cur.row_count);
+    const uint32_t row0 = d_cur.row_begin;
+#pragma unroll
+    for (int j = 0; j < KT; ++j) {
+      const int k = lane + j * 32;
+      if (k < N) prod[k] = static_cast<Acc>(v[j]) * xv[j];
+    }
+#pragma unroll
+    for (int j = 0; j <= KT; ++j) {
+      const int r = lane + j * 32;
+      if (r <= R) offs[r] = o[j] - nb;
+    }
+    __syncwarp();
+    // the next tile's gathers and loads are in flight during this reduction
+    if (has_next) {
+      gather_all(d_nxt);
+      load_rest(d_nxt);
+      load_ind(d_nn);
+    }
+    const TileDesc d_n3 = tile_at(t + 3 * t_step);
+    // merge path over (R row ends, N products): lane share [m0, m1)
+    const int items = R + N;
+    const int per = (items + 31) >> 5;
+    const int m0 = min(lane * per, items);
+    const int m1 = min(m0 + per, items);
+    int lo = max(0, m0 - N), hi = min(m0, R);
+    while (lo < hi) {  // smallest i with offs[i + 1] > m0 - i - 1
+      const int mid = (lo + hi) >> 1;
+      if (static_cast<int>(offs[mid + 1]) > m0 - mid - 1) hi = mid; else lo = mid + 1;
+    }
+    int i = lo, j = m0 - lo;
+    const int i0 = i;
+    Acc run = Acc(0), head = Acc(0);
+    bool head_done = false;
+    for (int m = m0; m < m1; ++m) {
+      if (i < R && static_cast<int>(offs[i + 1]) <= j) {
+        if (i == i0) { head = run; head_done = true; }
+        else out.row(row0 + i, run);
+        run = Acc(0);
+        ++i;
+      } else {
+        run += prod[j];
+        ++j;
+      }
+    }
+    // segmented inclusive scan of (row, partial) over the lanes
+    uint32_t key = static_cast<uint32_t>(i);
+    Acc sc = run;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const Acc vu = __shfl_up_sync(0xffffffffu, sc, off);
+      const uint32_t ku = __shfl_up_sync(0xffffffffu, key, off);
+      if (lane >= off && ku == key) sc += vu;
+    }
+    Acc pv = __shfl_up_sync(0xffffffffu, sc, 1);
+    const uint32_t pk = __shfl_up_sync(0xffffffffu, key, 1);
+    if (head_done)
+      out.row(row0 + i0, (lane > 0 && pk == static_cast<uint32_t>(i0) ? pv : Acc(0)) + head);
+    __syncwarp();  // offs / prod are free again
+    d_cur = d_nxt;
+    d_nxt = d_nn;
+    d_nn = d_n3;
+  }
+}
+
 // Dynamic shared memory a schedule needs per CTA.
 template <typename V, typename Acc>
 __host__ __device__ inline size_t spmv_smem_bytes(int sched, uint32_t tile_items, int block) {
   if (sched == SCHED_ROW) return 0;
   if (sched == SCHED_WTILE) return WarpSmem<V>::bytes(tile_items, block / 32);
+  if (sched == SCHED_WMERGE) return WMergeSmem<Acc>::bytes(tile_items, block / 32);
   return TileSmem<V, Acc>::bytes(tile_items);
 }
 
 // Work units a schedule distributes over CTAs (for the grid size).
 inline uint32_t spmv_work_units(int sched, uint32_t nrows, uint32_t ntiles, int block) {
   if (sched == SCHED_ROW) return (nrows + block - 1) / block;
-  if (sched == SCHED_WTILE) return (ntiles + block / 32 - 1) / (block / 32);
+  if (sched == SCHED_WTILE || sched == SCHED_WMERGE)
+    return (ntiles + block / 32 - 1) / (block / 32);
   return ntiles;
 }
 
 // Round-robin driver: CTA b runs tiles b, b + gridDim.x, ... (for the row
 // schedule rows in a grid-stride loop, for per-warp tiles warp w of CTA b
 // runs tiles b * warps + w, ...); then out.finish() once per thread.
-template <typename V, typename Acc, int SCHED, int BLOCK, class Gather, class Out>
+template <typename V, typename Acc, int SCHED, int BLOCK, class Gather, class Out,
+    bool DIRECT = false>
 __device__ __forceinline__ void spmv_tiles_body(const PlanView plan,
     const uint32_t * __restrict__ rowptr, const uint32_t * __restrict__ rowind,
     const V * __restrict__ val, const Gather gather, Out & out) {
@@ -668,6 +1097,14 @@ __device__ __forceinline__ void spmv_tiles_body(const PlanView plan,
     spmv_warp_loop<V, Acc>(plan, blockIdx.x * W + (threadIdx.x >> 5), plan.ntiles,
         gridDim.x * W, rowptr, rowind, val, gather, out, policy_evict_first(),
         policy_evict_last());
+  } else if constexpr (SCHED == SCHED_WMERGE) {
+    constexpr int W = BLOCK / 32;
+    spmv_wmerge_loop<V, Acc>(plan, blockIdx.x * W + (threadIdx.x >> 5), plan.ntiles,
+        gridDim.x * W, rowptr, rowind, val, gather, out, policy_evict_first(),
+        policy_evict_last());
+  } else if constexpr (DIRECT && IsPlainGather<Gather>::value) {
+    spmv_direct_loop<V, Acc, SCHED, BLOCK>(plan, blockIdx.x, plan.ntiles, gridDim.x, rowptr,
+        rowind, val, gather.x, out, policy_evict_first(), policy_evict_last());
   } else {
     spmv_tile_loop<V, Acc, SCHED, BLOCK>(plan, blockIdx.x, plan.ntiles, gridDim.x, rowptr,
         rowind, val, gather, out, policy_evict_first(), policy_evict_last());

@@ -75,11 +75,18 @@ typedef enum gb_schedule {
                             no tile staging; sums each row in the reference's
                             order (k ascending, unfused multiply and add), so
                             its SpMV is bit-identical to the reference       */
-  GB_SCHED_WTILE = 7     /* per-WARP tiles (small tile_items, ~256): each
+  GB_SCHED_WTILE = 7,    /* per-WARP tiles (small tile_items, ~256): each
                             warp streams its next tile into its own shared
                             memory stage with cp.async while its lanes sum
                             the current tile's rows, one row per lane, in
                             the reference's order (bit-identical, like ROW) */
+  GB_SCHED_WMERGE = 8    /* per-WARP tiles of at most 128 items, no CTA
+                            barrier: indices, values and x gathers are
+                            prefetched into registers one tile ahead, and
+                            rows are reduced along the merge path of (row
+                            ends, nonzeros) with equal work per lane (for
+                            skewed row lengths).  The CG solvers run a
+                            matrix set to this schedule with MERGE. */
 } gb_schedule_t;
 
 /*
@@ -103,7 +110,8 @@ GOOSEBERRY_API int gb_csr_destroy(gb_csr_t * a);
 GOOSEBERRY_API int gb_csr_get_info(const gb_csr_t * a, gb_csr_info_t * info);
 
 /* Fix the SpMV schedule of one value width (GB_CSR_VALUES_F64 or _F32).
- * tile_items == 0 keeps the current tile size. */
+ * tile_items == 0 keeps the current tile size (for the per-warp schedules a
+ * plan built for CTA tiles is rebuilt at their default tile size). */
 GOOSEBERRY_API int gb_csr_set_schedule(gb_csr_t * a, unsigned value_width, int schedule,
     uint32_t tile_items);
 

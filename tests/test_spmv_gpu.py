@@ -20,7 +20,16 @@ pytestmark = pytest.mark.gpu
 TOL64 = 1e-13
 TOL32 = 64 * 2.0 ** -24
 SCHEDS = [gb.SCHED_THREAD, gb.SCHED_GROUP4, gb.SCHED_GROUP8, gb.SCHED_WARP, gb.SCHED_MERGE,
-          gb.SCHED_ROW, gb.SCHED_WTILE]
+          gb.SCHED_ROW, gb.SCHED_WTILE, gb.SCHED_WMERGE]
+
+
+def _tile_for(sched, tile):
+    """Per-warp schedules take small tiles (WTILE <= 512, WMERGE <= 128)."""
+    if sched == gb.SCHED_WTILE:
+        return max(64, tile // 8)
+    if sched == gb.SCHED_WMERGE:
+        return min(128, max(64, tile // 8))
+    return tile
 
 
 @pytest.fixture(scope="module")
@@ -43,7 +52,7 @@ def test_golden_cases_all_schedules_f64(torch, spmv_golden):
         x = _dev(torch, c["x"])
         for tile in (256, 2048):
             for s in SCHEDS:
-                A.set_schedule(s, tile_items=tile if s != gb.SCHED_WTILE else max(64, tile // 8))
+                A.set_schedule(s, tile_items=_tile_for(s, tile))
                 y = A.spmv(x).cpu().numpy()
                 err = cond_scaled_err(y, c["y64"], c["rowptr"], c["rowind"], c["rowval"], c["x"])
                 assert err <= TOL64, (name, s, tile, err)
@@ -151,7 +160,7 @@ def test_powerlaw_long_rows(torch):
     assert M.info().nlong > 0
     xd = _dev(torch, x)
     for s, t in ((gb.SCHED_MERGE, 2048), (gb.SCHED_GROUP8, 2048), (gb.SCHED_THREAD, 2048),
-                 (gb.SCHED_WTILE, 256)):
+                 (gb.SCHED_WTILE, 256), (gb.SCHED_WMERGE, 128), (gb.SCHED_WMERGE, 64)):
         M.set_schedule(s, tile_items=t)
         y = M.spmv(xd).cpu().numpy()
         assert cond_scaled_err(y, y_ref, A.rowptr, A.rowind, A.rowval, x) <= TOL64, s
