@@ -387,6 +387,44 @@ def measure_spmv(A, x, reps=20, f32=False, flush=None, schedule=None):
                                                       "nlong": info.nlong}
 
 
+def measure_spdot(A, x, reps=20, f32=False, flush=None):
+    """Device time of gb_spdot over the matrix's own (rowind, rowval) and x: it
+    streams the same bytes and gathers the same x entries as the SpMV, without
+    the row reductions and the y writes -- a floor for the SpMV on this GPU.
+    Timed through the C-ABI with a preallocated result (no host sync inside)."""
+    import torch
+
+    import gooseberry_b200 as gb
+    dt = np.float32 if f32 else np.float64
+    ind = torch.from_numpy(A.rowind.astype(np.int32)).cuda()
+    val = torch.from_numpy(A.rowval.astype(dt)).cuda()
+    xd = torch.from_numpy(x.astype(dt)).cuda()
+    out = torch.empty(1, dtype=torch.float64, device="cuda")
+    fn = gb.lib().gb_spdot_f32 if f32 else gb.lib().gb_spdot_f64
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def run():
+        rc = fn(A.nnz, ind.data_ptr(), val.data_ptr(), xd.data_ptr(), A.ncols,
+                out.data_ptr(), stream)
+        if rc != 1:
+            raise RuntimeError(gb.last_error())
+    for _ in range(3):
+        run()
+    times = []
+    for _ in range(reps):
+        if flush is not None:
+            flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        run()
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    del ind, val, xd
+    return float(np.median(times))
+
+
 def spmv_extra(name, A, x, peak, flush, rows_check=200_000):
     """SpMV GB/s for one matrix, FP64 and FP32, with parity on the first
     `rows_check` rows against the oracle (FP64 oracle for both widths)."""
@@ -401,9 +439,11 @@ def spmv_extra(name, A, x, peak, flush, rows_check=200_000):
         ms, y, info = measure_spmv(A, x, f32=f32, flush=flush)
         b = _spmv_bytes(A.nrows, A.nnz, 4 if f32 else 8, 4 if f32 else 8)
         gbs = b / (ms * 1e-3) / 1e9
+        floor = measure_spdot(A, x, f32=f32, flush=flush)
         out["f32" if f32 else "f64"] = {
             "ms": ms, "GB/s": gbs, "frac_of_peak": gbs / peak, "bytes": b, **info,
             "max_cond_err_vs_fp64_oracle_first_rows": _cond_err(y[:k], y_ref, sub, x),
+            "stream_gather_floor_ms": floor, "frac_of_floor": floor / ms,
         }
     return out
 
@@ -461,6 +501,7 @@ def run_spmv(args, dist: Dist, which: str):
                         threads=os.cpu_count() or 1)
     sub = type(A)(k, A.ncols, A.rowptr[: k + 1], A.rowind[:nnz_k], A.rowval[:nnz_k])
     err = _cond_err(y.cpu().numpy()[:k], y_ref, sub, x)
+    floor_ms = measure_spdot(A, x, flush=flush)
     # end to end: gooseberry_spmult_f64 with pinned host buffers
     def pinned(a):
         t = torch.empty(a.shape, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
@@ -491,7 +532,9 @@ def run_spmv(args, dist: Dist, which: str):
         "roofline": {"bound": "hbm", "kernel": "spmv_tiles_kernel",
                      "achieved": b / (ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": b / (ms * 1e-3) / 1e9 / peak, "traffic": ncu_traffic(which),
-                     "peak_source": peak_src},
+                     "peak_source": peak_src,
+                     "stream_gather_floor_ms": floor_ms,
+                     "frac_of_stream_gather_floor": floor_ms / ms},
         "e2e": {"value": e2e_steps * b / t_e2e / 1e9, "unit": "GB/s",
                 "h2d_bytes_per_step": 4 * (n + 1) + 12 * nnz + 8 * n,
                 "d2h_bytes_per_step": 8 * n, "api": "gooseberry_spmult_f64 (pinned host)"},

@@ -30,7 +30,7 @@ import numpy as np
 
 __all__ = [
     "GooseberryError", "lib", "spmult", "scale", "add_scalar", "cgd",
-    "CsrMatrix", "CgSolver", "CgResult", "dot", "SUCCESS",
+    "CsrMatrix", "CgSolver", "CgResult", "dot", "spdot", "SUCCESS",
     "SCHED_AUTO", "SCHED_THREAD", "SCHED_GROUP4", "SCHED_GROUP8", "SCHED_WARP",
     "SCHED_MERGE", "SCHED_ROW", "SCHED_WTILE", "SCHED_WMERGE", "CG_F64", "CG_MIXED", "plan_tiles",
     "Server", "ServerResult",
@@ -100,6 +100,8 @@ SIGNATURES = {
     "gb_spmm_f64": (_i, [_vp, _u32, _vp, _vp, _vp]),
     "gb_dot_f64": (_i, [_sz, _vp, _vp, _vp, _vp]),
     "gb_dot_f32": (_i, [_sz, _vp, _vp, _vp, _vp]),
+    "gb_spdot_f64": (_i, [_sz, _vp, _vp, _vp, _sz, _vp, _vp]),
+    "gb_spdot_f32": (_i, [_sz, _vp, _vp, _vp, _sz, _vp, _vp]),
     "gb_dot_f64_noalloc": (_i, [_sz, _vp, _vp, _vp, _vp]),
     "gb_scale_f64": (_i, [_sz, _vp, _d, _vp]),
     "gb_add_scalar_f64": (_i, [_sz, _vp, _d, _vp]),
@@ -276,6 +278,17 @@ def dot(a, b, stream=None) -> float:
     fn = lib().gb_dot_f64 if a.dtype == torch.float64 else lib().gb_dot_f32
     _check(fn(a.numel(), a.data_ptr(), b.data_ptr(), out.data_ptr(), _stream_ptr(stream)),
            "gb_dot")
+    return float(out.item())
+
+
+def spdot(ind, val, x, stream=None) -> float:
+    """sum val[k] * x[ind[k]] for CUDA tensors (ind uint32/int32, val and x of
+    one float type; float64 accumulation, fixed order)."""
+    torch = _torch()
+    out = torch.empty(1, dtype=torch.float64, device=x.device)
+    fn = lib().gb_spdot_f64 if x.dtype == torch.float64 else lib().gb_spdot_f32
+    _check(fn(ind.numel(), ind.data_ptr(), val.data_ptr(), x.data_ptr(), x.numel(),
+              out.data_ptr(), _stream_ptr(stream)), "gb_spdot")
     return float(out.item())
 
 

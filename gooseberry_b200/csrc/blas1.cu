@@ -1,5 +1,5 @@
-// blas1.cu -- dense vector BLAS-1 on device vectors: dot, scale, add_scalar,
-// add, sub (reference src/blas.c:244-336, 397-430).
+// blas1.cu -- BLAS-1 on device vectors: dot, sparse . dense dot, scale,
+// add_scalar, add, sub (reference src/blas.c:244-336, 397-451).
 //
 // All are HBM-streaming grid-stride kernels with grids a multiple of the SM
 // count.  The CG solver does not call them: it fuses the same vector work into
@@ -53,6 +53,50 @@ __global__ void __launch_bounds__(kBlock) dot_final_kernel(unsigned g,
   if (threadIdx.x == 0) *out = acc;
 }
 
+// Sparse . dense: each CTA owns a fixed contiguous chunk of the nonzeros;
+// its threads stream indices and values (evict-first) and keep kSpdotK
+// gathers of x in flight each, accumulating in double.  This is the streaming
+// and gather work of a CSR SpMV without its row reductions, so its time on a
+// matrix's own (rowind, rowval, x) is a floor for that SpMV on this GPU.
+constexpr int kSpdotK = 8;
+
+template <typename T>
+__global__ void __launch_bounds__(kBlock) spdot_partial_kernel(size_t nnz,
+    const uint32_t * __restrict__ ind, const T * __restrict__ val, const T * __restrict__ x,
+    size_t nx, double * __restrict__ partial) {
+  __shared__ double red[32];
+  size_t s, e;
+  chunk_of(nnz, blockIdx.x, gridDim.x, s, e);
+  const NoHint pol_m, pol_x;  // plain loads: faster than L2-policy loads on this pattern
+  const uint32_t cmax = static_cast<uint32_t>(nx - 1);
+  double acc = 0.0;
+  for (size_t base = s + threadIdx.x; base < e; base += static_cast<size_t>(kSpdotK) * kBlock) {
+    uint32_t c[kSpdotK];
+    T v[kSpdotK];
+#pragma unroll
+    for (int j = 0; j < kSpdotK; ++j) {
+      const size_t i = base + static_cast<size_t>(j) * kBlock;
+      if (i < e) {
+        c[j] = ld_stream(ind + i, pol_m);
+        v[j] = ld_stream(val + i, pol_m);
+      }
+    }
+    T xv[kSpdotK];
+#pragma unroll
+    for (int j = 0; j < kSpdotK; ++j) {
+      const size_t i = base + static_cast<size_t>(j) * kBlock;
+      if (i < e) xv[j] = ld_keep(x + min(c[j], cmax), pol_x);
+    }
+#pragma unroll
+    for (int j = 0; j < kSpdotK; ++j) {
+      const size_t i = base + static_cast<size_t>(j) * kBlock;
+      if (i < e) acc += static_cast<double>(v[j]) * static_cast<double>(xv[j]);
+    }
+  }
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) partial[blockIdx.x] = acc;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kBlock) scale_kernel(size_t n, T * __restrict__ v, T s) {
   for (size_t i = blockIdx.x * static_cast<size_t>(kBlock) + threadIdx.x; i < n;
@@ -92,11 +136,27 @@ int dot_impl(size_t n, const T * a, const T * b, double * result, cudaStream_t s
   GB_CHECK_INPUT(n == 0 || (a && b), "NULL vector");
   const unsigned g = grid_for(n, 4);
   double * partial = nullptr;
-  GB_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&partial), g * sizeof(double), s));
+  GB_TRY(scratch_alloc(reinterpret_cast<void **>(&partial), g * sizeof(double), s));
   dot_partial_kernel<T><<<g, kBlock, 0, s>>>(n, a, b, partial);
   dot_final_kernel<<<1, kBlock, 0, s>>>(g, partial, result);
   cudaError_t e = cudaGetLastError();
-  cudaFreeAsync(partial, s);
+  scratch_free(partial, s);
+  GB_CUDA_TRY(e);
+  return GOOSEBERRY_SUCCESS;
+}
+
+template <typename T>
+int spdot_impl(size_t nnz, const uint32_t * ind, const T * val, const T * x, size_t nx,
+    double * result, cudaStream_t s) {
+  GB_CHECK_INPUT(result != nullptr, "result is NULL");
+  GB_CHECK_INPUT(nnz == 0 || (ind && val && x && nx > 0), "NULL vector or empty x");
+  const unsigned g = grid_for(nnz, 4);
+  double * partial = nullptr;
+  GB_TRY(scratch_alloc(reinterpret_cast<void **>(&partial), g * sizeof(double), s));
+  spdot_partial_kernel<T><<<g, kBlock, 0, s>>>(nnz, ind, val, x, nx, partial);
+  dot_final_kernel<<<1, kBlock, 0, s>>>(g, partial, result);
+  cudaError_t e = cudaGetLastError();
+  scratch_free(partial, s);
   GB_CUDA_TRY(e);
   return GOOSEBERRY_SUCCESS;
 }
@@ -216,6 +276,17 @@ int gb_dot_f64(size_t n, const double * a, const double * b, double * result,
 int gb_dot_f32(size_t n, const float * a, const float * b, double * result,
     gb_stream_t stream) {
   return gb::dot_impl<float>(n, a, b, result, static_cast<cudaStream_t>(stream));
+}
+
+int gb_spdot_f64(size_t nnz, const dim_t * ind, const double * val, const double * x,
+    size_t nx, double * result, gb_stream_t stream) {
+  return gb::spdot_impl<double>(nnz, ind, val, x, nx, result,
+      static_cast<cudaStream_t>(stream));
+}
+
+int gb_spdot_f32(size_t nnz, const dim_t * ind, const float * val, const float * x,
+    size_t nx, double * result, gb_stream_t stream) {
+  return gb::spdot_impl<float>(nnz, ind, val, x, nx, result, static_cast<cudaStream_t>(stream));
 }
 
 int gb_scale_f64(size_t n, double * v, double s, gb_stream_t stream) {

@@ -74,7 +74,8 @@ struct GatherP {
   const double * r;
   const double * pold;
   double beta;
-  __device__ __forceinline__ double operator()(uint32_t c, uint64_t pol) const {
+  template <class P>
+  __device__ __forceinline__ double operator()(uint32_t c, P pol) const {
     return fma(beta, ld_keep(pold + c, pol), ld_keep(r + c, pol));
   }
 };
@@ -136,7 +137,7 @@ struct OutCgA {
   }
 };
 
-template <int SCHED>
+template <int SCHED, bool HINT>
 __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_a_kernel(const PlanView plan,
     const uint32_t * __restrict__ rowptr, const uint32_t * __restrict__ rowind,
     const double * __restrict__ val, const double * __restrict__ r,
@@ -150,7 +151,8 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_a_kern
   // the row schedule finishes long rows through row() like any other row
   OutCgA o{ap, pnew, r, pold, longdot, partial, st, beta,
            SCHED == SCHED_ROW ? 0u : plan.nlong, 0.0};
-  spmv_tiles_body<double, double, SCHED, kSpmvBlock>(plan, rowptr, rowind, val, g, o);
+  spmv_tiles_body<double, double, SCHED, kSpmvBlock, GatherP, OutCgA, false, HINT>(plan, rowptr,
+      rowind, val, g, o);
 }
 
 // ---- B: x / r update and r.r ----------------------------------------------------
@@ -289,12 +291,12 @@ size_t spmv_smem(int sched, uint32_t tile_items) {
   return spmv_smem_bytes<double, double>(sched, tile_items, kSpmvBlock);
 }
 
-template <int SCHED>
+template <int SCHED, bool HINT>
 int launch_cg_a_t(const gb_csr & a, const double * r, const double * pold, double * pnew,
     double * ap, double * longdot, double * partial, CgState * st, unsigned grid,
     cudaStream_t s, bool pdl) {
   const size_t smem = spmv_smem(SCHED, a.plan.tile_items);
-  auto kern = cg_a_kernel<SCHED>;
+  auto kern = cg_a_kernel<SCHED, HINT>;
   if (smem > 48 * 1024)
     GB_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void *>(kern),
         cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
@@ -303,37 +305,48 @@ int launch_cg_a_t(const gb_csr & a, const double * r, const double * pold, doubl
   return GOOSEBERRY_SUCCESS;
 }
 
-int launch_cg_a(const gb_csr & a, int sched, const double * r, const double * pold,
+template <bool HINT>
+int launch_cg_a_h(const gb_csr & a, int sched, const double * r, const double * pold,
     double * pnew, double * ap, double * longdot, double * partial, CgState * st,
     unsigned grid, cudaStream_t s, bool pdl) {
   switch (sched) {
     case GB_SCHED_THREAD:
-      return launch_cg_a_t<SCHED_THREAD>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
+      return launch_cg_a_t<SCHED_THREAD, HINT>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
           pdl);
     case GB_SCHED_GROUP4:
-      return launch_cg_a_t<SCHED_GROUP4>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
+      return launch_cg_a_t<SCHED_GROUP4, HINT>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
           pdl);
     case GB_SCHED_GROUP8:
-      return launch_cg_a_t<SCHED_GROUP8>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
+      return launch_cg_a_t<SCHED_GROUP8, HINT>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
           pdl);
     case GB_SCHED_WARP:
-      return launch_cg_a_t<SCHED_WARP>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
+      return launch_cg_a_t<SCHED_WARP, HINT>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
           pdl);
     case GB_SCHED_ROW:
-      return launch_cg_a_t<SCHED_ROW>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
+      return launch_cg_a_t<SCHED_ROW, HINT>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
           pdl);
     case GB_SCHED_WTILE:
-      return launch_cg_a_t<SCHED_WTILE>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
+      return launch_cg_a_t<SCHED_WTILE, HINT>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
           pdl);
     default:
-      return launch_cg_a_t<SCHED_MERGE>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
+      return launch_cg_a_t<SCHED_MERGE, HINT>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
           pdl);
   }
 }
 
+// The A kernel with L2-policy loads (hint) or plain loads.
+int launch_cg_a(const gb_csr & a, int sched, bool hint, const double * r, const double * pold,
+    double * pnew, double * ap, double * longdot, double * partial, CgState * st,
+    unsigned grid, cudaStream_t s, bool pdl) {
+  return hint ? launch_cg_a_h<true>(a, sched, r, pold, pnew, ap, longdot, partial, st, grid, s,
+                                    pdl)
+              : launch_cg_a_h<false>(a, sched, r, pold, pnew, ap, longdot, partial, st, grid,
+                                     s, pdl);
+}
+
 template <int SCHED>
 int occupancy_cg_a(size_t smem, int * out) {
-  auto kern = cg_a_kernel<SCHED>;
+  auto kern = cg_a_kernel<SCHED, false>;
   if (smem > 48 * 1024)
     GB_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void *>(kern),
         cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
@@ -667,6 +680,7 @@ struct gb_cg {
   uint32_t * cta_tiles = nullptr;
   unsigned * sync = nullptr;  // [0] barrier counter, [1] abort flag
   int keep_l2 = 0;
+  bool l2_hint = false;  // A kernel with L2-policy loads (working set fits in L2)
   gb::MixedCg * mixed = nullptr;  // GB_CG_MIXED solver (owns its workspace)
 };
 
@@ -702,7 +716,7 @@ int capture_chunk(gb_cg * s, int slot) {
   for (int k = 0; k < s->chunk && rc == GOOSEBERRY_SUCCESS; ++k) {
     const double * pold = s->p[k & 1];
     double * pnew = s->p[(k + 1) & 1];
-    rc = launch_cg_a(*s->a, s->sched, s->r, pold, pnew, s->ap, s->longdot, s->partial_a,
+    rc = launch_cg_a(*s->a, s->sched, s->l2_hint, s->r, pold, pnew, s->ap, s->longdot, s->partial_a,
         s->st, s->grid_a, cs, k > 0);
     if (rc != GOOSEBERRY_SUCCESS) break;
     if (launch_k(cg_b_kernel, s->grid_b, kVecBlock, 0, cs, true, s->n, s->x, s->r,
@@ -832,6 +846,9 @@ int create_cg(const gb_csr * a, int mode, gb_cg * s) {
   GB_CUDA_TRY(cudaMalloc(&s->ap, n * sizeof(double)));
   s->sched = a->sched64;
   s->tile_items = a->plan.tile_items;
+  // evict-first/evict-last hints keep an L2-sized working set (matrix, rowptr,
+  // r, both p, Ap, x) resident across iterations; beyond L2 the plain loads win
+  GB_TRY(l2_fits(4ull * (s->n + 1) + 12ull * a->nnz + 40ull * s->n, &s->l2_hint));
   const size_t smem = spmv_smem(s->sched, a->plan.tile_items);
   int occ = 0;
   GB_TRY(occupancy_cg_a_sched(s->sched, smem, &occ));
@@ -902,8 +919,7 @@ int solve_cg(gb_cg * s, const double * b, double * x, double tol, int tol_relati
   }
   double * dhist = nullptr;
   const size_t hl = history ? std::min(history_len, niter ? niter : history_len) : 0;
-  if (hl) GB_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&dhist), hl * sizeof(double),
-      stream));
+  if (hl) GB_TRY(scratch_alloc(reinterpret_cast<void **>(&dhist), hl * sizeof(double), stream));
   GB_TRY(start_solve(s, b, tol, tol_relative, niter, dhist, hl, stream));
   size_t launches = 1;
 
@@ -973,7 +989,7 @@ int solve_cg(gb_cg * s, const double * b, double * x, double tol, int tol_relati
       res->kernel_launches = launches;
     }
   }
-  if (dhist) cudaFreeAsync(dhist, stream);
+  if (dhist) scratch_free(dhist, stream);
   return rc;
 }
 
@@ -1010,7 +1026,7 @@ int profile_cg(gb_cg * s, const double * b, size_t iterations, double * ms, size
     const double * pold = s->p[k & 1];
     double * pnew = s->p[(k + 1) & 1];
     cudaEventRecord(ev[3 * k], stream);
-    rc = launch_cg_a(*s->a, s->sched, s->r, pold, pnew, s->ap, s->longdot, s->partial_a,
+    rc = launch_cg_a(*s->a, s->sched, s->l2_hint, s->r, pold, pnew, s->ap, s->longdot, s->partial_a,
         s->st, s->grid_a, stream, false);
     cudaEventRecord(ev[3 * k + 1], stream);
     cg_b_kernel<<<s->grid_b, kVecBlock, 0, stream>>>(s->n, s->x, s->r, pnew, s->ap,

@@ -71,7 +71,8 @@ struct GatherP32 {
   const float * r;
   const float * pold;
   float beta;
-  __device__ __forceinline__ float operator()(uint32_t c, uint64_t pol) const {
+  template <class P>
+  __device__ __forceinline__ float operator()(uint32_t c, P pol) const {
     return fmaf(beta, ld_keep(pold + c, pol), ld_keep(r + c, pol));
   }
 };
@@ -132,7 +133,7 @@ struct OutA32 {
   }
 };
 
-template <int SCHED>
+template <int SCHED, bool HINT>
 __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_a32_kernel(
     const PlanView plan, const uint32_t * __restrict__ rowptr,
     const uint32_t * __restrict__ rowind, const float * __restrict__ val,
@@ -145,7 +146,8 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_a32_ke
   GatherP32 g{r, pold, beta};
   OutA32 o{ap, pnew, r, pold, longdot, partial, st, beta,
            SCHED == SCHED_ROW ? 0u : plan.nlong, 0.0};
-  spmv_tiles_body<float, float, SCHED, kSpmvBlock>(plan, rowptr, rowind, val, g, o);
+  spmv_tiles_body<float, float, SCHED, kSpmvBlock, GatherP32, OutA32, false, HINT>(plan, rowptr,
+      rowind, val, g, o);
 }
 
 // ---- B32 ----------------------------------------------------------------------
@@ -222,7 +224,8 @@ struct GatherXY {
   const double * x;
   const float * y;
   bool use_y;
-  __device__ __forceinline__ double operator()(uint32_t c, uint64_t pol) const {
+  template <class P>
+  __device__ __forceinline__ double operator()(uint32_t c, P pol) const {
     const double xv = ld_keep(x + c, pol);
     return use_y ? xv + static_cast<double>(ld_keep(y + c, pol)) : xv;
   }
@@ -294,7 +297,7 @@ struct OutR {
   }
 };
 
-template <int SCHED>
+template <int SCHED, bool HINT>
 __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_r_kernel(
     const PlanView plan, const uint32_t * __restrict__ rowptr,
     const uint32_t * __restrict__ rowind, const double * __restrict__ val,
@@ -314,7 +317,8 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_r_kern
   GatherXY g{xold, y, use_y};
   OutR o{b, xold, xnew, y, r32, longdot, partial, st, use_y,
          SCHED == SCHED_ROW ? 0u : plan.nlong, 0.0};
-  spmv_tiles_body<double, double, SCHED, kSpmvBlock>(plan, rowptr, rowind, val, g, o);
+  spmv_tiles_body<double, double, SCHED, kSpmvBlock, GatherXY, OutR, false, HINT>(plan, rowptr,
+      rowind, val, g, o);
 }
 
 // ---- init -----------------------------------------------------------------------
@@ -396,24 +400,24 @@ int prep_kernel(K kern, size_t smem, int * occ) {
   return GOOSEBERRY_SUCCESS;
 }
 
-template <int SCHED>
+template <int SCHED, bool HINT>
 int launch_a32_t(const gb_csr & a, unsigned grid, cudaStream_t s, bool pdl,
     const float * r, const float * pold, float * pnew, float * ap, double * longdot,
     double * partial, MixState * st) {
   const size_t smem = smem_of(SCHED, a.plan.tile_items, 4);
-  auto kern = cg_a32_kernel<SCHED>;
+  auto kern = cg_a32_kernel<SCHED, HINT>;
   GB_TRY(prep_kernel(kern, smem, nullptr));
   GB_CUDA_TRY(launch_k(kern, grid, kSpmvBlock, smem, s, pdl, plan_view(a), a.rowptr,
       a.rowind, a.val32, r, pold, pnew, ap, longdot, partial, st));
   return GOOSEBERRY_SUCCESS;
 }
 
-template <int SCHED>
+template <int SCHED, bool HINT>
 int launch_r_t(const gb_csr & a, unsigned grid, cudaStream_t s, bool pdl, const double * b,
     const double * x0, double * x1, const float * y, float * r32, double * longdot,
     double * partial, MixState * st) {
   const size_t smem = smem_of(SCHED, a.plan.tile_items, 8);
-  auto kern = cg_r_kernel<SCHED>;
+  auto kern = cg_r_kernel<SCHED, HINT>;
   GB_TRY(prep_kernel(kern, smem, nullptr));
   GB_CUDA_TRY(launch_k(kern, grid, kSpmvBlock, smem, s, pdl, plan_view(a), a.rowptr,
       a.rowind, a.val64, b, x0, x1, y, r32, longdot, partial, st));
@@ -432,9 +436,11 @@ int launch_r_t(const gb_csr & a, unsigned grid, cudaStream_t s, bool pdl, const 
   }
 
 template <int SCHED>
-int occ_a32_t(size_t smem, int * occ) { return prep_kernel(cg_a32_kernel<SCHED>, smem, occ); }
+int occ_a32_t(size_t smem, int * occ) {
+  return prep_kernel(cg_a32_kernel<SCHED, false>, smem, occ);
+}
 template <int SCHED>
-int occ_r_t(size_t smem, int * occ) { return prep_kernel(cg_r_kernel<SCHED>, smem, occ); }
+int occ_r_t(size_t smem, int * occ) { return prep_kernel(cg_r_kernel<SCHED, false>, smem, occ); }
 
 }  // namespace
 
@@ -459,6 +465,7 @@ struct MixedCg {
   MixState * st = nullptr;
   MixStatus * host_status = nullptr;
   unsigned grid_a = 0, grid_b = 0, grid_r = 0;
+  bool l2_hint = false;  // L2-policy loads (the FP32 working set fits in L2)
   int chunk = 32;
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -469,15 +476,21 @@ namespace {
 int launch_a32(MixedCg * m, cudaStream_t s, bool pdl, int k) {
   const float * pold = m->p[k & 1];
   float * pnew = m->p[(k + 1) & 1];
-#define GB_CALL(S) launch_a32_t<S>(*m->a, m->grid_a, s, pdl, m->r, pold, pnew, m->ap, \
-                                   m->longdot, m->partial_a, m->st)
+#define GB_CALL(S)                                                                      \
+  (m->l2_hint ? launch_a32_t<S, true>(*m->a, m->grid_a, s, pdl, m->r, pold, pnew, m->ap,   \
+                                      m->longdot, m->partial_a, m->st)                     \
+              : launch_a32_t<S, false>(*m->a, m->grid_a, s, pdl, m->r, pold, pnew, m->ap,  \
+                                       m->longdot, m->partial_a, m->st))
   GB_SCHED_SWITCH(m->sched32, GB_CALL)
 #undef GB_CALL
 }
 
 int launch_r(MixedCg * m, cudaStream_t s, bool pdl) {
-#define GB_CALL(S) launch_r_t<S>(*m->a, m->grid_r, s, pdl, m->b, m->x[0], m->x[1], m->y, \
-                                 m->r, m->longdot, m->partial_r, m->st)
+#define GB_CALL(S)                                                                      \
+  (m->l2_hint ? launch_r_t<S, true>(*m->a, m->grid_r, s, pdl, m->b, m->x[0], m->x[1], m->y,  \
+                                    m->r, m->longdot, m->partial_r, m->st)                  \
+              : launch_r_t<S, false>(*m->a, m->grid_r, s, pdl, m->b, m->x[0], m->x[1], m->y, \
+                                     m->r, m->longdot, m->partial_r, m->st))
   GB_SCHED_SWITCH(m->sched64, GB_CALL)
 #undef GB_CALL
 }
@@ -595,6 +608,9 @@ int mixed_create(const gb_csr * a, MixedCg ** out) {
   m->sched32 = a->sched32;
   m->sched64 = a->sched64;
   m->tile_items = a->plan.tile_items;
+  // L2-policy loads only when the FP32 iteration's working set (rowptr,
+  // indices, float values, r, both p, Ap, y) fits in L2
+  GB_TRY(l2_fits(4ull * (m->n + 1) + 8ull * a->nnz + 24ull * m->n, &m->l2_hint));
   const size_t n = std::max<size_t>(m->n, 2);
   GB_CUDA_TRY(cudaMalloc(&m->x[0], n * sizeof(double)));
   GB_CUDA_TRY(cudaMalloc(&m->x[1], n * sizeof(double)));
@@ -660,8 +676,7 @@ int mixed_solve(MixedCg * m, const double * b, double * x, double tol, int tol_r
   }
   double * dhist = nullptr;
   const size_t hl = history ? std::min(history_len, niter ? niter : history_len) : 0;
-  if (hl) GB_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&dhist), hl * sizeof(double),
-      stream));
+  if (hl) GB_TRY(scratch_alloc(reinterpret_cast<void **>(&dhist), hl * sizeof(double), stream));
   GB_TRY(mixed_start(m, b, tol, tol_relative, niter, dhist, hl, stream));
   size_t launches = 1;
   cudaEvent_t ev[2];
@@ -737,7 +752,7 @@ int mixed_solve(MixedCg * m, const double * b, double * x, double tol, int tol_r
     res->status = fin.status;
     res->kernel_launches = launches;
   }
-  if (dhist) cudaFreeAsync(dhist, stream);
+  if (dhist) scratch_free(dhist, stream);
   return rc;
 }
 

@@ -156,6 +156,12 @@ int launch_max_index(const uint32_t * rowind, uint32_t nnz, unsigned int * d_out
 int launch_round_f32(const double * in, float * out, size_t n, cudaStream_t stream);
 
 int sm_count_of_current_device(int * out);
+// Whether `bytes` of working set fit in the current device's L2 (the CG
+// kernels use L2-policy loads only then).
+int l2_fits(size_t bytes, bool * out);
+// Stream-ordered scratch from a library-owned pool that keeps its memory.
+int scratch_alloc(void ** p, size_t bytes, cudaStream_t s);
+void scratch_free(void * p, cudaStream_t s);
 
 // Mixed-precision CG (cg_mixed.cu), owned by a gb_cg created with GB_CG_MIXED.
 struct MixedCg;

@@ -239,7 +239,8 @@ struct SrvGatherP {  // direction p = r + beta * p_old, rebuilt inside the gathe
   const T * r;
   const T * pold;
   T beta;
-  __device__ __forceinline__ T operator()(uint32_t c, uint64_t pol) const {
+  template <class P>
+  __device__ __forceinline__ T operator()(uint32_t c, P pol) const {
     return fma(beta, ld_keep(pold + c, pol), ld_keep(r + c, pol));
   }
 };
@@ -268,7 +269,8 @@ struct SrvGatherXY {  // x + y in FP64
   const double * x;
   const float * y;
   bool use_y;
-  __device__ __forceinline__ double operator()(uint32_t c, uint64_t pol) const {
+  template <class P>
+  __device__ __forceinline__ double operator()(uint32_t c, P pol) const {
     const double xc = ld_keep(x + c, pol);
     return use_y ? xc + static_cast<double>(ld_keep(y + c, pol)) : xc;
   }

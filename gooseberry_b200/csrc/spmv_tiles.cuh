@@ -69,53 +69,55 @@ __device__ __forceinline__ uint64_t policy_evict_last() {
   return p;
 }
 
-__device__ __forceinline__ uint32_t ld_stream(const uint32_t * p, uint64_t pol) {
-  uint32_t v;
-  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;"
-               : "=r"(v) : "l"(p), "l"(pol));
-  return v;
-}
-__device__ __forceinline__ double ld_stream(const double * p, uint64_t pol) {
-  double v;
-  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;"
-               : "=d"(v) : "l"(p), "l"(pol));
-  return v;
-}
-__device__ __forceinline__ float ld_stream(const float * p, uint64_t pol) {
-  float v;
-  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;"
-               : "=f"(v) : "l"(p), "l"(pol));
-  return v;
-}
-// Read-only loads that DO allocate in L1 (for access patterns where several
-// instructions of a warp touch the same sector, e.g. one row per lane).
-__device__ __forceinline__ uint32_t ld_l1(const uint32_t * p, uint64_t pol) {
-  uint32_t v;
-  asm volatile("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
-  return v;
-}
-__device__ __forceinline__ double ld_l1(const double * p, uint64_t pol) {
-  double v;
-  asm volatile("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
-  return v;
-}
-__device__ __forceinline__ float ld_l1(const float * p, uint64_t pol) {
-  float v;
-  asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
-  return v;
-}
-__device__ __forceinline__ double ld_keep(const double * p, uint64_t pol) {
-  double v;
-  asm volatile("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;"
-               : "=d"(v) : "l"(p), "l"(pol));
-  return v;
-}
-__device__ __forceinline__ float ld_keep(const float * p, uint64_t pol) {
-  float v;
-  asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;"
-               : "=f"(v) : "l"(p), "l"(pol));
-  return v;
-}
+// Each load exists twice: with an L2 eviction policy (a uint64_t from
+// createpolicy: evict-first for a matrix stream, evict-last for gathered
+// vectors) and plain (a NoHint tag).  The hinted form keeps an L2-sized
+// working set resident across launches; on streams much larger than L2 and
+// on random gathers it is slower than the plain form, so kernels take the
+// policy as a type and the host picks per launch.
+struct NoHint {};
+
+#define GB_LD(NAME, T, REG, SUFFIX, HINTED, PLAIN)                                   \
+  __device__ __forceinline__ T NAME(const T * p, uint64_t pol) {                   \
+    T v;                                                                           \
+    asm volatile(HINTED "." SUFFIX " %0, [%1], %2;" : "=" REG(v) : "l"(p), "l"(pol)); \
+    return v;                                                                      \
+  }                                                                                \
+  __device__ __forceinline__ T NAME(const T * p, NoHint) {                         \
+    T v;                                                                           \
+    asm volatile(PLAIN "." SUFFIX " %0, [%1];" : "=" REG(v) : "l"(p));             \
+    return v;                                                                      \
+  }
+// streamed once: no L1 allocation
+GB_LD(ld_stream, uint32_t, "r", "u32", "ld.global.nc.L1::no_allocate.L2::cache_hint",
+      "ld.global.nc.L1::no_allocate")
+GB_LD(ld_stream, double, "d", "f64", "ld.global.nc.L1::no_allocate.L2::cache_hint",
+      "ld.global.nc.L1::no_allocate")
+GB_LD(ld_stream, float, "f", "f32", "ld.global.nc.L1::no_allocate.L2::cache_hint",
+      "ld.global.nc.L1::no_allocate")
+// read-only loads that DO allocate in L1 (for access patterns where several
+// instructions of a warp touch the same sector, e.g. one row per lane)
+GB_LD(ld_l1, uint32_t, "r", "u32", "ld.global.nc.L2::cache_hint", "ld.global.nc")
+GB_LD(ld_l1, double, "d", "f64", "ld.global.nc.L2::cache_hint", "ld.global.nc")
+GB_LD(ld_l1, float, "f", "f32", "ld.global.nc.L2::cache_hint", "ld.global.nc")
+// gathered vector entries
+GB_LD(ld_keep, double, "d", "f64", "ld.global.nc.L2::cache_hint", "ld.global.nc")
+GB_LD(ld_keep, float, "f", "f32", "ld.global.nc.L2::cache_hint", "ld.global.nc")
+#undef GB_LD
+
+// The policy pair a kernel built with (HINT) or without L2 hints passes down.
+template <bool HINT>
+struct L2Pol;
+template <>
+struct L2Pol<true> {
+  __device__ static uint64_t stream() { return policy_evict_first(); }
+  __device__ static uint64_t keep() { return policy_evict_last(); }
+};
+template <>
+struct L2Pol<false> {
+  __device__ static NoHint stream() { return NoHint{}; }
+  __device__ static NoHint keep() { return NoHint{}; }
+};
 
 // Round-to-nearest multiply and add that the compiler may not contract into
 // a fused multiply-add (the reference's x86-64 build never fuses).
@@ -154,7 +156,8 @@ __device__ __forceinline__ T block_sum(T v, T * red /* >= 32 entries */) {
 template <typename X>
 struct GatherPlain {
   const X * x;
-  __device__ __forceinline__ X operator()(uint32_t c, uint64_t pol) const {
+  template <class P>
+  __device__ __forceinline__ X operator()(uint32_t c, P pol) const {
     return ld_keep(x + c, pol);
   }
 };
@@ -183,15 +186,25 @@ __device__ __forceinline__ void cp_async4(void * smem, const void * gmem, uint64
   asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 4, %2;"
                :: "r"(s), "l"(gmem), "l"(pol) : "memory");
 }
+__device__ __forceinline__ void cp_async4(void * smem, const void * gmem, NoHint) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" :: "r"(s), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async8(void * smem, const void * gmem, uint64_t pol) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
   asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 8, %2;"
                :: "r"(s), "l"(gmem), "l"(pol) : "memory");
 }
-__device__ __forceinline__ void cp_async_v(void * smem, const double * g, uint64_t pol) {
+__device__ __forceinline__ void cp_async8(void * smem, const void * gmem, NoHint) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" :: "r"(s), "l"(gmem) : "memory");
+}
+template <class P>
+__device__ __forceinline__ void cp_async_v(void * smem, const double * g, P pol) {
   cp_async8(smem, g, pol);
 }
-__device__ __forceinline__ void cp_async_v(void * smem, const float * g, uint64_t pol) {
+template <class P>
+__device__ __forceinline__ void cp_async_v(void * smem, const float * g, P pol) {
   cp_async4(smem, g, pol);
 }
 __device__ __forceinline__ void cp_async_commit() {
@@ -299,11 +312,12 @@ __device__ __forceinline__ void reduce_tile(const Acc * prod, const uint32_t * o
 //   long_row(lid, row, Acc)      -- a finished long row (called by one thread)
 // `pol_matrix` is the L2 policy of the matrix stream (evict-first when the
 // matrix cannot stay in L2, evict-normal/last when it can).
-template <typename V, typename Acc, int SCHED, int BLOCK, class Gather, class Out>
+template <typename V, typename Acc, int SCHED, int BLOCK, class Gather, class Out, class PM,
+    class PX>
 __device__ __forceinline__ void spmv_tile_loop(const PlanView & plan, uint32_t t_begin,
     uint32_t t_end, uint32_t t_step, const uint32_t * __restrict__ rowptr,
     const uint32_t * __restrict__ rowind, const V * __restrict__ val,
-    const Gather & gather, Out & out, uint64_t pol_matrix, uint64_t pol_x) {
+    const Gather & gather, Out & out, PM pol_matrix, PX pol_x) {
   extern __shared__ __align__(16) unsigned char gb_smem[];
   __shared__ Acc scan_v[BLOCK / 32];
   __shared__ uint32_t scan_k[BLOCK / 32];
@@ -452,9 +466,9 @@ struct RowStage {
   V v[STAGE];
 };
 
-template <typename V, int STAGE>
+template <typename V, int STAGE, class P>
 __device__ __forceinline__ void row_stage_load(RowStage<V, STAGE> & s, const uint32_t * rowind,
-    const V * val, uint64_t pol) {
+    const V * val, P pol) {
 #pragma unroll
   for (int j = 0; j < STAGE; ++j) {
     if (s.b + j < s.e) {
@@ -464,11 +478,12 @@ __device__ __forceinline__ void row_stage_load(RowStage<V, STAGE> & s, const uin
   }
 }
 
-template <typename V, typename Acc, int STAGE = kRowStage, class Gather, class Out>
+template <typename V, typename Acc, int STAGE = kRowStage, class Gather, class Out, class PM,
+    class PX>
 __device__ __forceinline__ void spmv_row_loop(uint32_t first, uint32_t end, uint32_t step,
     uint32_t ncols, const uint32_t * __restrict__ rowptr,
     const uint32_t * __restrict__ rowind, const V * __restrict__ val, const Gather & gather,
-    Out & out, uint64_t pol_matrix, uint64_t pol_x) {
+    Out & out, PM pol_matrix, PX pol_x) {
   const uint32_t cmax = ncols - 1;
   if (first >= end) return;
   // stage L: row `first`; stage P: rowptr pair of row first + step
@@ -540,11 +555,11 @@ struct WarpSmem {
   }
 };
 
-template <typename V, typename Acc, class Gather, class Out>
+template <typename V, typename Acc, class Gather, class Out, class PM, class PX>
 __device__ __forceinline__ void spmv_warp_loop(const PlanView & plan, uint32_t t_first,
     uint32_t t_end, uint32_t t_step, const uint32_t * __restrict__ rowptr,
     const uint32_t * __restrict__ rowind, const V * __restrict__ val, const Gather & gather,
-    Out & out, uint64_t pol_matrix, uint64_t pol_x) {
+    Out & out, PM pol_matrix, PX pol_x) {
   extern __shared__ __align__(16) unsigned char gb_smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t T = plan.tile_items;
@@ -702,11 +717,11 @@ constexpr int kDirectKt = GB_DIRECT_KT;  // items per thread per tile (tile <= k
 constexpr int kDirectMinBlocks = GB_DIRECT_MIN_BLOCKS;
 constexpr int kDirectBlock = GB_DIRECT_BLOCK;  // threads per CTA of the direct loop
 
-template <typename V, typename Acc, int SCHED, int BLOCK, class Out>
+template <typename V, typename Acc, int SCHED, int BLOCK, class Out, class PM, class PX>
 __device__ __forceinline__ void spmv_direct_loop(const PlanView & plan, uint32_t t_begin,
     uint32_t t_end, uint32_t t_step, const uint32_t * __restrict__ rowptr,
     const uint32_t * __restrict__ rowind, const V * __restrict__ val,
-    const Acc * __restrict__ x, Out & out, uint64_t pol_matrix, uint64_t pol_x) {
+    const Acc * __restrict__ x, Out & out, PM pol_matrix, PX pol_x) {
   extern __shared__ __align__(16) unsigned char gb_smem[];
   __shared__ Acc scan_v[BLOCK / 32];
   __shared__ uint32_t scan_k[BLOCK / 32];
@@ -883,11 +898,11 @@ struct WMergeSmem {
   }
 };
 
-template <typename V, typename Acc, class Gather, class Out>
+template <typename V, typename Acc, class Gather, class Out, class PM, class PX>
 __device__ __forceinline__ void spmv_wmerge_loop(const PlanView & plan, uint32_t t_first,
     uint32_t t_end, uint32_t t_step, const uint32_t * __restrict__ rowptr,
     const uint32_t * __restrict__ rowind, const V * __restrict__ val, const Gather & gather,
-    Out & out, uint64_t pol_matrix, uint64_t pol_x) {
+    Out & out, PM pol_matrix, PX pol_x) {
   extern __shared__ __align__(16) unsigned char gb_smem[];
   constexpr int KT = kWmKt;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1082,32 +1097,32 @@ inline uint32_t spmv_work_units(int sched, uint32_t nrows, uint32_t ntiles, int 
 
 // Round-robin driver: CTA b runs tiles b, b + gridDim.x, ... (for the row
 // schedule rows in a grid-stride loop, for per-warp tiles warp w of CTA b
-// runs tiles b * warps + w, ...); then out.finish() once per thread.
+// runs tiles b * warps + w, ...); then out.finish() once per thread.  HINT
+// selects the L2-policy loads (L2Pol).
 template <typename V, typename Acc, int SCHED, int BLOCK, class Gather, class Out,
-    bool DIRECT = false>
+    bool DIRECT = false, bool HINT = false>
 __device__ __forceinline__ void spmv_tiles_body(const PlanView plan,
     const uint32_t * __restrict__ rowptr, const uint32_t * __restrict__ rowind,
     const V * __restrict__ val, const Gather gather, Out & out) {
-  if (SCHED == SCHED_ROW) {
+  const auto pm = L2Pol<HINT>::stream();
+  const auto px = L2Pol<HINT>::keep();
+  if constexpr (SCHED == SCHED_ROW) {
     spmv_row_loop<V, Acc>(blockIdx.x * BLOCK + threadIdx.x, plan.nrows, gridDim.x * BLOCK,
-        plan.ncols, rowptr, rowind, val, gather, out, policy_evict_first(),
-        policy_evict_last());
-  } else if (SCHED == SCHED_WTILE) {
+        plan.ncols, rowptr, rowind, val, gather, out, pm, px);
+  } else if constexpr (SCHED == SCHED_WTILE) {
     constexpr int W = BLOCK / 32;
     spmv_warp_loop<V, Acc>(plan, blockIdx.x * W + (threadIdx.x >> 5), plan.ntiles,
-        gridDim.x * W, rowptr, rowind, val, gather, out, policy_evict_first(),
-        policy_evict_last());
+        gridDim.x * W, rowptr, rowind, val, gather, out, pm, px);
   } else if constexpr (SCHED == SCHED_WMERGE) {
     constexpr int W = BLOCK / 32;
     spmv_wmerge_loop<V, Acc>(plan, blockIdx.x * W + (threadIdx.x >> 5), plan.ntiles,
-        gridDim.x * W, rowptr, rowind, val, gather, out, policy_evict_first(),
-        policy_evict_last());
+        gridDim.x * W, rowptr, rowind, val, gather, out, pm, px);
   } else if constexpr (DIRECT && IsPlainGather<Gather>::value) {
     spmv_direct_loop<V, Acc, SCHED, BLOCK>(plan, blockIdx.x, plan.ntiles, gridDim.x, rowptr,
-        rowind, val, gather.x, out, policy_evict_first(), policy_evict_last());
+        rowind, val, gather.x, out, pm, px);
   } else {
     spmv_tile_loop<V, Acc, SCHED, BLOCK>(plan, blockIdx.x, plan.ntiles, gridDim.x, rowptr,
-        rowind, val, gather, out, policy_evict_first(), policy_evict_last());
+        rowind, val, gather, out, pm, px);
   }
   out.finish();
 }

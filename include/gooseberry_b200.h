@@ -156,6 +156,17 @@ GOOSEBERRY_API int gb_dot_f64(size_t n, const double * a, const double * b, doub
 GOOSEBERRY_API int gb_dot_f32(size_t n, const float * a, const float * b, double * result,
     gb_stream_t stream);
 
+/* *result = sum_k val[k] * x[ind[k]] (a sparse vector . a dense vector of nx
+ * entries), accumulated in double, deterministic (fixed reduction order).
+ * Indices must be < nx.  result is a DEVICE pointer.  blas_spdot, reference
+ * src/blas.c:433-451.  Run on a matrix's own (rowind, rowval) and x it streams
+ * the same bytes and gathers the same x entries as that matrix's SpMV, without
+ * the row reductions: its time is a floor for the SpMV on this GPU. */
+GOOSEBERRY_API int gb_spdot_f64(size_t nnz, const dim_t * ind, const double * val,
+    const double * x, size_t nx, double * result, gb_stream_t stream);
+GOOSEBERRY_API int gb_spdot_f32(size_t nnz, const dim_t * ind, const float * val,
+    const float * x, size_t nx, double * result, gb_stream_t stream);
+
 /*
  * Allocation-free form of gb_dot_f64, for callers that must not allocate
  * device memory during a call: code whose device memory is entirely owned by

@@ -57,6 +57,9 @@ def _lib():
             f = getattr(lib, f"oracle_dot_{real}")
             f.argtypes = [C.c_size_t, p, p]
             f.restype = ctype
+            f = getattr(lib, f"oracle_spdot_{real}")
+            f.argtypes = [C.c_size_t, _u32p, p, p]
+            f.restype = ctype
             for nm in ("scale", "add_scalar"):
                 f = getattr(lib, f"oracle_{nm}_{real}")
                 f.argtypes = [C.c_size_t, p, ctype]
@@ -88,6 +91,8 @@ def _ref(real: str = "f64"):
         lib.gbref_spmult.restype = C.c_int
         lib.gbref_dot.argtypes = [C.c_uint32, p, p]
         lib.gbref_dot.restype = C.c_double
+        lib.gbref_spdot.argtypes = [C.c_uint32, _u32p, p, p]
+        lib.gbref_spdot.restype = C.c_double
         lib.gbref_cgd.argtypes = [C.c_uint32, _u32p, _u32p, p, p, p, C.c_double,
                                   C.c_size_t, C.POINTER(C.c_size_t),
                                   C.POINTER(C.c_double), C.c_void_p, C.c_size_t]
@@ -146,6 +151,15 @@ def dot(a, b, real="f64"):
     return float(getattr(_lib(), f"oracle_dot_{real}")(len(a), a, b))
 
 
+def spdot(ind, val, x, real="f64"):
+    """Restated blas_spdot (src/blas.c:433-451): sum val[k]*x[ind[k]], k ascending."""
+    dt = _dt(real)
+    ind = np.ascontiguousarray(ind, dtype=np.uint32)
+    val = np.ascontiguousarray(val, dtype=dt)
+    x = np.ascontiguousarray(x, dtype=dt)
+    return float(getattr(_lib(), f"oracle_spdot_{real}")(len(ind), ind, val, x))
+
+
 def scale(v, s, real="f64"):
     v = np.array(v, dtype=_dt(real), copy=True)
     getattr(_lib(), f"oracle_scale_{real}")(len(v), v, s)
@@ -202,6 +216,15 @@ def ref_dot(a, b, real="f64"):
     a = np.ascontiguousarray(a, dtype=dt)
     b = np.ascontiguousarray(b, dtype=dt)
     return float(_ref(real).gbref_dot(len(a), a, b))
+
+
+def ref_spdot(ind, val, x, real="f64"):
+    """The reference's own blas_spdot (src/blas.c:433-451)."""
+    dt = _dt(real)
+    ind = np.ascontiguousarray(ind, dtype=np.uint32)
+    val = np.ascontiguousarray(val, dtype=dt)
+    x = np.ascontiguousarray(x, dtype=dt)
+    return float(_ref(real).gbref_spdot(len(ind), ind, val, x))
 
 
 def ref_cgd(rowptr, rowind, rowval, b, error, niter, real="f64", history=False):

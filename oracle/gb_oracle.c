@@ -97,6 +97,23 @@ GB_ORACLE_SPMM(oracle_spmm_f32, float)
 GB_ORACLE_DOT(oracle_dot_f64, double)
 GB_ORACLE_DOT(oracle_dot_f32, float)
 
+/* sum_k val[k]*x[ind[k]], k ascending, accumulated in REAL -- src/blas.c:433-451
+ * (blas_spdot) as it runs on one OpenMP thread.  The reference passes the
+ * indices as real_t values (src/blas.h:218-222); here they are integers. */
+#define GB_ORACLE_SPDOT(NAME, REAL)                                            \
+  REAL NAME(size_t nnz, const uint32_t * ind, const REAL * val, const REAL * x); \
+  REAL NAME(size_t nnz, const uint32_t * ind, const REAL * val, const REAL * x)  \
+  {                                                                            \
+    size_t i;                                                                  \
+    REAL s = 0;                                                                \
+    for (i = 0; i < nnz; ++i) {                                                \
+      s += val[i] * x[ind[i]];                                                 \
+    }                                                                          \
+    return s;                                                                  \
+  }
+GB_ORACLE_SPDOT(oracle_spdot_f64, double)
+GB_ORACLE_SPDOT(oracle_spdot_f32, float)
+
 /* v[i] *= s -- src/blas.c:244-257 (blas_scale); v[i] += s --
  * src/blas.c:397-410 (blas_add_scalar). */
 void oracle_scale_f64(size_t n, double * v, double s);

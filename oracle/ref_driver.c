@@ -12,6 +12,7 @@
  * - gbref_spmult: forwards to blas_spmult (src/blas.c:552-606), the body of
  *   gooseberry_spmult (src/gooseberry.c:53-67).
  * - gbref_dot:    forwards to blas_dot (src/blas.c:413-430).
+ * - gbref_spdot:  forwards to blas_spdot (src/blas.c:433-451).
  * - gbref_cgd:    wraps cgd (src/cgd.c:40-129) for raw CSR arrays.  cgd prints
  *   one "ITER: k RMSE: v" line per iteration (src/cgd.c:116) and returns no
  *   iteration count, so stdout is redirected to a temporary file for the call
@@ -59,6 +60,7 @@ int gbref_spmult(dim_t anrows, dim_t ancols, dim_t bncols,
     const real_t * bcolval, real_t * crowval, const dim_t * blocks,
     dim_t nblocks);
 double gbref_dot(dim_t n, const real_t * a, const real_t * b);
+double gbref_spdot(dim_t nnz, const dim_t * ind, const real_t * val, const real_t * x);
 int gbref_cgd(dim_t n, ind_t * rowptr, dim_t * rowind, real_t * rowval,
     real_t * b, real_t * x, double error, size_t niter, size_t * iters,
     double * last_norm, double * history, size_t history_len);
@@ -87,6 +89,24 @@ int gbref_spmult(dim_t anrows, dim_t ancols, dim_t bncols,
 double gbref_dot(dim_t n, const real_t * a, const real_t * b)
 {
   return (double)blas_dot(n, a, b);
+}
+
+/* blas_spdot (src/blas.c:433-451) takes its indices as real_t values; they
+ * are converted here (exact below 2^24 for the float build, 2^53 for double). */
+double gbref_spdot(dim_t nnz, const dim_t * ind, const real_t * val, const real_t * x)
+{
+  dim_t i;
+  double s;
+  real_t * rind = malloc(sizeof(real_t) * (nnz ? nnz : 1));
+  if (!rind) {
+    return 0.0;
+  }
+  for (i = 0; i < nnz; ++i) {
+    rind[i] = (real_t)ind[i];
+  }
+  s = (double)blas_spdot(nnz, rind, val, x);
+  free(rind);
+  return s;
 }
 
 int gbref_cgd(dim_t n, ind_t * rowptr, dim_t * rowind, real_t * rowval,

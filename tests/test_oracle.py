@@ -91,3 +91,26 @@ def test_dot_scale_add_scalar():
     assert np.array_equal(s, a * 3.0)
     t = oracle.add_scalar(a, -0.5)
     assert np.array_equal(t, a - 0.5)
+
+
+def test_spdot_restatement():
+    A = W.powerlaw_rows(2000, 30000, seed=7, cap=2000)
+    x = W.dense_x(2000, 7)
+    s = oracle.spdot(A.rowind, A.rowval, x)
+    acc = 0.0
+    for k in range(A.nnz):  # the loop of src/blas.c:445-448, k ascending
+        acc += A.rowval[k] * x[A.rowind[k]]
+    assert s == acc
+    assert oracle.spdot(A.rowind[:0], A.rowval[:0], x) == 0.0
+
+
+@pytest.mark.skipif(not oracle.ref_available("f64"), reason="reference build absent")
+def test_spdot_matches_reference_build():
+    A = W.powerlaw_rows(2000, 30000, seed=8, cap=2000)
+    x = W.dense_x(2000, 8)
+    oracle.ref_set_threads(1)  # one OpenMP thread: k ascending
+    assert oracle.ref_spdot(A.rowind, A.rowval, x) == oracle.spdot(A.rowind, A.rowval, x)
+    x32 = x.astype(np.float32)
+    v32 = A.rowval.astype(np.float32)
+    assert (oracle.ref_spdot(A.rowind, v32, x32, real="f32")
+            == oracle.spdot(A.rowind, v32, x32, real="f32"))

@@ -221,3 +221,23 @@ def test_blas1_device(torch):
     w = np.arange(10, dtype=np.float32)
     gb.scale(w, 0.5)
     assert np.array_equal(w, np.arange(10, dtype=np.float32) * np.float32(0.5))
+
+
+def test_spdot_matches_oracle(torch):
+    """gb_spdot (blas_spdot, src/blas.c:433-451) on a power-law matrix's own
+    indices/values: FP64 within the condition-scaled bound of the sequential
+    oracle sum; FP32 inputs are multiplied and summed in double, so they are
+    checked against the FP64 oracle of the same float values."""
+    A = W.powerlaw_rows(300_000, 4_800_000, seed=41, cap=50_000)
+    x = W.dense_x(A.ncols, 41)
+    ind = _dev(torch, A.rowind.astype(np.int32))
+    ref = oracle.spdot(A.rowind, A.rowval, x)
+    scale = float(np.sum(np.abs(A.rowval * x[A.rowind])))
+    got = gb.spdot(ind, _dev(torch, A.rowval), _dev(torch, x))
+    assert abs(got - ref) <= 1e-13 * scale
+    assert got == gb.spdot(ind, _dev(torch, A.rowval), _dev(torch, x))  # fixed order
+    v32, x32 = A.rowval.astype(np.float32), x.astype(np.float32)
+    ref32 = oracle.spdot(A.rowind, v32.astype(np.float64), x32.astype(np.float64))
+    got32 = gb.spdot(ind, _dev(torch, v32), _dev(torch, x32))
+    assert abs(got32 - ref32) <= 1e-13 * scale
+    assert gb.spdot(ind[:0], _dev(torch, A.rowval[:0]), _dev(torch, x)) == 0.0
