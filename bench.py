@@ -104,6 +104,12 @@ class Dist:
         self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
         return float(t.item())
 
+    def aggregate(self, units_local: float, t_local: float):
+        """Replicas: every rank times its own units of work; the job's rate is
+        all ranks' units over the slowest rank's time.  Returns (rate, t_max)."""
+        t_max = self.max(t_local)
+        return self.sum(units_local) / t_max, t_max
+
     def close(self):
         if self.pg:
             self.pg.destroy_process_group()
@@ -262,8 +268,7 @@ def run_cg_laplace(args, dist: Dist):
     dist.barrier()
     clk = clocks.stop()
     t_local = sum(a.elapsed_time(b_) for a, b_ in evs) / 1e3
-    t_max = dist.max(t_local)
-    solves_total = dist.sum(float(args.steps))
+    rate, t_max = dist.aggregate(float(args.steps), t_local)
     iters = results[-1].iterations
     assert all(r.status == "converged" for r in results), [r.status for r in results]
 
@@ -289,7 +294,7 @@ def run_cg_laplace(args, dist: Dist):
     ach_a = bytes_a / (ms_a * 1e-3) / 1e9
     out = {
         "metric": "CG solves/s (FP64, 2D 5-point Laplacian 1024x1024, rel-res 1e-8)",
-        "value": solves_total / t_max,
+        "value": rate,
         "unit": "solves/s",
         "n_gpus": dist.world,
         "steps": args.steps,
@@ -491,8 +496,8 @@ def run_spmv(args, dist: Dist, which: str):
     dist.barrier()
     clk = clocks.stop()
     t_local = sum(a.elapsed_time(b) for a, b in times) / 1e3
-    t_max = dist.max(t_local)
     b = _spmv_bytes(n, nnz, 8, 8)
+    rate, t_max = dist.aggregate(args.steps * b / 1e9, t_local)
     ms = t_local / args.steps * 1e3
     # parity on the first rows against the oracle
     k = min(200_000, n)
@@ -520,7 +525,7 @@ def run_spmv(args, dist: Dist, which: str):
     info = M.info()
     out = {
         "metric": f"SpMV GB/s (FP64, {label})",
-        "value": dist.world * args.steps * b / t_max / 1e9,
+        "value": rate,
         "unit": "GB/s", "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic, seeded (gooseberry_b200.workloads)",
