@@ -29,7 +29,7 @@ from dataclasses import dataclass
 import numpy as np
 
 __all__ = [
-    "GooseberryError", "lib", "spmult", "scale", "add_scalar", "cgd",
+    "GooseberryError", "lib", "spmult", "scale", "add_scalar", "cgd", "pagerank",
     "CsrMatrix", "CgSolver", "CgResult", "dot", "spdot", "SUCCESS",
     "SCHED_AUTO", "SCHED_THREAD", "SCHED_GROUP4", "SCHED_GROUP8", "SCHED_WARP",
     "SCHED_MERGE", "SCHED_ROW", "SCHED_WTILE", "SCHED_WMERGE", "CG_F64", "CG_MIXED", "plan_tiles",
@@ -89,6 +89,8 @@ SIGNATURES = {
     "gooseberry_spmult_f64": (_i, [_u32, _u32, _u32, _vp, _vp, _vp, _vp, _vp, _vp, _u32]),
     "gooseberry_cgd": (_i, [_u32, _vp, _vp, _vp, _vp, _vp, _f, _sz, _vp, _vp, _vp, _sz]),
     "gooseberry_cgd_f64": (_i, [_u32, _vp, _vp, _vp, _vp, _vp, _d, _sz, _vp, _vp, _vp, _sz]),
+    "gooseberry_pagerank": (_i, [_u32, _vp, _vp, _vp, _f, _f, _sz, _vp, _vp, _vp]),
+    "gooseberry_pagerank_f64": (_i, [_u32, _vp, _vp, _vp, _d, _d, _sz, _vp, _vp, _vp]),
     "gb_csr_create": (_i, [_u32, _u32, _u32, _vp, _vp, _vp, _vp, C.c_uint, _vp, _vp]),
     "gb_csr_destroy": (_i, [_vp]),
     "gb_csr_get_info": (_i, [_vp, _vp]),
@@ -245,6 +247,24 @@ def cgd(rowptr, rowind, rowval, b, error: float, niter: int, history: bool = Fal
     if history:
         return x, int(it.value), rn.value, hist[: it.value]
     return x, int(it.value), rn.value
+
+
+def pagerank(rowptr, rowind, rowval, damping: float = 0.85, minerror: float = 0.0,
+             niter: int = 0):
+    """PageRank with the reference's contract (``src/gooseberry_bin.c:2610-2741``,
+    see ``gooseberry_pagerank``).  Returns ``(rank, iterations, error)``."""
+    rowval = np.ascontiguousarray(rowval)
+    real = _real(rowval.dtype)
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+    rowind = np.ascontiguousarray(rowind, dtype=np.uint32)
+    n = len(rowptr) - 1
+    rank = np.zeros(n, dtype=rowval.dtype)
+    it = C.c_size_t(0)
+    err = C.c_double(0)
+    fn = lib().gooseberry_pagerank_f64 if real == "f64" else lib().gooseberry_pagerank
+    _check(fn(n, _ptr(rowptr), _ptr(rowind), _ptr(rowval), damping, minerror, int(niter),
+              _ptr(rank), C.addressof(it), C.addressof(err)), "gooseberry_pagerank")
+    return rank, int(it.value), err.value
 
 
 def plan_tiles(rowptr, tile_items: int = 2048):

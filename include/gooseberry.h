@@ -86,6 +86,7 @@ extern "C" {
 #define gooseberry_add_scalar gooseberry_add_scalar_f64
 #define gooseberry_spmult gooseberry_spmult_f64
 #define gooseberry_cgd gooseberry_cgd_f64
+#define gooseberry_pagerank gooseberry_pagerank_f64
 #endif
 
 /*
@@ -146,6 +147,28 @@ GOOSEBERRY_API int gooseberry_cgd_f64(dim_t n, const ind_t * rowptr, const dim_t
     const double * rowval, const double * b, double * x, double error,
     size_t niter, size_t * iterations, double * rnorm, double * history,
     size_t history_len);
+
+/*
+ * PageRank of the square n x n CSR graph (rowptr/rowind/rowval), the
+ * reference's `pagerank` command (src/gooseberry_bin.c:2610-2741) over arrays
+ * already in memory.  Values are normalised by their column sums; rows with no
+ * entries are sinks.  Starting from rank = 1/n, every iteration computes
+ * out = damping * (A rank) + (1 - damping)/n + (sum of rank over the sinks); on
+ * iterations 0, 10, 20, ... the squared change sum (rank - out)^2 is compared
+ * with minerror^2 and the run stops when it is not larger.  niter == 0 means
+ * no iteration limit (a graph with sinks never converges: the reference adds
+ * the whole sink mass to every entry).  On return rank[n] holds the result --
+ * the newest iterate on convergence, the one before it when niter ended the
+ * run, as the reference writes -- *iterations (if non-NULL) the iteration
+ * count and *error (if non-NULL) the 2-norm of the last change.  The float
+ * form computes in double and rounds rank to float.
+ */
+GOOSEBERRY_API int gooseberry_pagerank(dim_t n, const ind_t * rowptr, const dim_t * rowind,
+    const real_t * rowval, real_t damping, real_t minerror, size_t niter, real_t * rank,
+    size_t * iterations, double * error);
+GOOSEBERRY_API int gooseberry_pagerank_f64(dim_t n, const ind_t * rowptr,
+    const dim_t * rowind, const double * rowval, double damping, double minerror,
+    size_t niter, double * rank, size_t * iterations, double * error);
 
 #ifdef __cplusplus
 }

@@ -64,6 +64,11 @@ def _lib():
                 f = getattr(lib, f"oracle_{nm}_{real}")
                 f.argtypes = [C.c_size_t, p, ctype]
                 f.restype = None
+            if real == "f64":
+                f = lib.oracle_pagerank_f64
+                f.argtypes = [C.c_uint32, _u32p, _u32p, p, C.c_double, C.c_double,
+                              C.c_size_t, p, C.POINTER(C.c_double)]
+                f.restype = C.c_size_t
             f = getattr(lib, f"oracle_cgd_{real}")
             f.argtypes = [C.c_uint32, _u32p, _u32p, p, p, p, ctype, C.c_size_t,
                           C.c_void_p, C.c_size_t, C.POINTER(C.c_double), C.c_int]
@@ -93,6 +98,9 @@ def _ref(real: str = "f64"):
         lib.gbref_dot.restype = C.c_double
         lib.gbref_spdot.argtypes = [C.c_uint32, _u32p, p, p]
         lib.gbref_spdot.restype = C.c_double
+        lib.gbref_pagerank.argtypes = [C.c_uint32, _u32p, _u32p, p, C.c_double, C.c_double,
+                                       C.c_size_t, p, C.POINTER(C.c_double)]
+        lib.gbref_pagerank.restype = C.c_size_t
         lib.gbref_cgd.argtypes = [C.c_uint32, _u32p, _u32p, p, p, p, C.c_double,
                                   C.c_size_t, C.POINTER(C.c_size_t),
                                   C.POINTER(C.c_double), C.c_void_p, C.c_size_t]
@@ -216,6 +224,35 @@ def ref_dot(a, b, real="f64"):
     a = np.ascontiguousarray(a, dtype=dt)
     b = np.ascontiguousarray(b, dtype=dt)
     return float(_ref(real).gbref_dot(len(a), a, b))
+
+
+def pagerank(rowptr, rowind, rowval, damping=0.85, minerror=0.0, niter=0):
+    """Restated pagerank command (src/gooseberry_bin.c:2610-2741), FP64.
+    Returns (result, iterations, error)."""
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+    rowind = np.ascontiguousarray(rowind, dtype=np.uint32)
+    rowval = np.ascontiguousarray(rowval, dtype=np.float64)
+    n = len(rowptr) - 1
+    out = np.zeros(n)
+    err = C.c_double(0)
+    it = _lib().oracle_pagerank_f64(n, rowptr, rowind, rowval, damping, minerror, niter, out,
+                                    C.byref(err))
+    return out, int(it), err.value
+
+
+def ref_pagerank(rowptr, rowind, rowval, damping=0.85, minerror=0.0, niter=0, real="f64"):
+    """The pagerank loop around the reference's own blas_spmult / blas_scale /
+    blas_add_scalar.  Returns (result, iterations, error)."""
+    dt = _dt(real)
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+    rowind = np.ascontiguousarray(rowind, dtype=np.uint32)
+    rowval = np.ascontiguousarray(rowval, dtype=dt)
+    n = len(rowptr) - 1
+    out = np.zeros(n, dtype=dt)
+    err = C.c_double(0)
+    it = _ref(real).gbref_pagerank(n, rowptr, rowind, rowval, damping, minerror, niter, out,
+                                   C.byref(err))
+    return out, int(it), err.value
 
 
 def ref_spdot(ind, val, x, real="f64"):

@@ -215,3 +215,86 @@ void oracle_add_scalar_f32(size_t n, float * v, float s)
   }
 GB_ORACLE_CGD(oracle_cgd_f64, double, oracle_spmm_f64, oracle_dot_f64)
 GB_ORACLE_CGD(oracle_cgd_f32, float, oracle_spmm_f32, oracle_dot_f32)
+
+/* PageRank power iteration -- the reference's `pagerank` command,
+ * src/gooseberry_bin.c:2610-2741, for a square CSR matrix already read in
+ * (no permutation file, one run), with sequential sums (one OpenMP thread):
+ *   - normalise: indeg[c] = sum of the values in column c, accumulated in row
+ *     order; every value is divided by its column's indeg; rows without
+ *     entries are sinks (2611-2630);
+ *   - rank = 1/n; per iteration i: out = A rank; out *= damping;
+ *     dist = sum of rank over the sinks, in sink order; out += (1-damping)/n
+ *     + dist (2668-2689);
+ *   - when i % 10 == 0: err = sum (rank - out)^2; err <= minerror^2 stops
+ *     with i + 1 iterations and out the newest iterate (2691-2712);
+ *   - otherwise rank and out swap (2714); niter == 0 means no limit;
+ *   - at the limit err is taken between rank (newest) and out (the iterate
+ *     before), and out -- the second-to-last iterate -- is the result
+ *     (2716-2737, the output written at 2767).
+ * rowval is not modified (the reference normalises its own copy in place).
+ * Writes the result to result[n]; returns the iteration count. */
+size_t oracle_pagerank_f64(uint32_t n, const uint32_t * rowptr, const uint32_t * rowind,
+    const double * rowval, double damping, double minerror, size_t niter,
+    double * result, double * error);
+size_t oracle_pagerank_f64(uint32_t n, const uint32_t * rowptr, const uint32_t * rowind,
+    const double * rowval, double damping, double minerror, size_t niter,
+    double * result, double * error)
+{
+  uint32_t k, nsinks = 0;
+  size_t l, i;
+  double err = 0.0, dist, diff;
+  const uint32_t nnz = rowptr[n];
+  double * indeg = calloc(n ? n : 1, sizeof(double));
+  double * val = malloc(sizeof(double) * (nnz ? nnz : 1));
+  uint32_t * sinks = malloc(sizeof(uint32_t) * (n ? n : 1));
+  double * rank = malloc(sizeof(double) * (n ? n : 1));
+  double * out = malloc(sizeof(double) * (n ? n : 1));
+  double * tmp;
+  int done = 0;
+  for (k = 0; k < n; ++k) {
+    if (rowptr[k] == rowptr[k + 1]) {
+      sinks[nsinks++] = k;
+    } else {
+      for (l = rowptr[k]; l < rowptr[k + 1]; ++l) indeg[rowind[l]] += rowval[l];
+    }
+  }
+  for (l = 0; l < nnz; ++l) val[l] = rowval[l] / indeg[rowind[l]];
+  for (k = 0; k < n; ++k) rank[k] = 1.0 / n;
+  for (i = 0; niter == 0 || i < niter; ++i) {
+    oracle_spmm_f64(n, n, 1, rowptr, rowind, val, rank, out, NULL, 0, 1);
+    oracle_scale_f64(n, out, damping);
+    dist = 0;
+    for (k = 0; k < nsinks; ++k) dist += rank[sinks[k]];
+    oracle_add_scalar_f64(n, out, ((1.0 - damping) / n) + dist);
+    if (i % 10 == 0) {
+      err = 0.0;
+      for (k = 0; k < n; ++k) {
+        diff = rank[k] - out[k];
+        err += diff * diff;
+      }
+      if (err <= minerror * minerror) {
+        ++i;
+        done = 1;
+        break;
+      }
+    }
+    tmp = rank;
+    rank = out;
+    out = tmp;
+  }
+  if (!done) {
+    err = 0.0;
+    for (k = 0; k < n; ++k) {
+      diff = rank[k] - out[k];
+      err += diff * diff;
+    }
+  }
+  *error = sqrt(err);
+  memcpy(result, out, sizeof(double) * n);
+  free(indeg);
+  free(val);
+  free(sinks);
+  free(rank);
+  free(out);
+  return i;
+}

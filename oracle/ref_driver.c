@@ -13,6 +13,11 @@
  *   gooseberry_spmult (src/gooseberry.c:53-67).
  * - gbref_dot:    forwards to blas_dot (src/blas.c:413-430).
  * - gbref_spdot:  forwards to blas_spdot (src/blas.c:433-451).
+ * - gbref_pagerank: the pagerank command's loop (src/gooseberry_bin.c:
+ *   2610-2741) lives in the CLI's main file, which does not build as a
+ *   library; it is restated here around the reference's own blas_spmult,
+ *   blas_scale and blas_add_scalar -- the calls the command makes through
+ *   gooseberry_spmult / _scale / _add_scalar (src/gooseberry.c:35-67).
  * - gbref_cgd:    wraps cgd (src/cgd.c:40-129) for raw CSR arrays.  cgd prints
  *   one "ITER: k RMSE: v" line per iteration (src/cgd.c:116) and returns no
  *   iteration count, so stdout is redirected to a temporary file for the call
@@ -20,6 +25,7 @@
  * - permute_* stubs: src/matrix.c:256-373 references them for permutations,
  *   which nothing on the SpMV/CG path calls.
  */
+#include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -64,6 +70,9 @@ double gbref_spdot(dim_t nnz, const dim_t * ind, const real_t * val, const real_
 int gbref_cgd(dim_t n, ind_t * rowptr, dim_t * rowind, real_t * rowval,
     real_t * b, real_t * x, double error, size_t niter, size_t * iters,
     double * last_norm, double * history, size_t history_len);
+size_t gbref_pagerank(dim_t n, const ind_t * rowptr, const dim_t * rowind,
+    const real_t * rowval, double damping, double minerror, size_t niter, real_t * result,
+    double * error);
 
 /* OpenMP thread count of the reference's parallel regions.  With 1 thread
  * blas_dot sums in index order, which makes cgd bit-reproducible. */
@@ -167,4 +176,68 @@ int gbref_cgd(dim_t n, ind_t * rowptr, dim_t * rowind, real_t * rowval,
   *iters = count;
   *last_norm = last;
   return rv;
+}
+
+size_t gbref_pagerank(dim_t n, const ind_t * rowptr, const dim_t * rowind,
+    const real_t * rowval, double damping, double minerror, size_t niter, real_t * result,
+    double * error)
+{
+  dim_t k, nsinks = 0;
+  ind_t l;
+  size_t i;
+  real_t err = 0.0, dist, diff;
+  const ind_t nnz = rowptr[n];
+  real_t * indeg = calloc(n ? n : 1, sizeof(real_t));
+  real_t * val = malloc(sizeof(real_t) * (nnz ? nnz : 1));
+  dim_t * sinks = malloc(sizeof(dim_t) * (n ? n : 1));
+  real_t * rank = malloc(sizeof(real_t) * (n ? n : 1));
+  real_t * out = malloc(sizeof(real_t) * (n ? n : 1));
+  real_t * tmp;
+  int done = 0;
+  for (k = 0; k < n; ++k) {
+    if (rowptr[k] == rowptr[k + 1]) {
+      sinks[nsinks++] = k;
+    } else {
+      for (l = rowptr[k]; l < rowptr[k + 1]; ++l) indeg[rowind[l]] += rowval[l];
+    }
+  }
+  for (l = 0; l < nnz; ++l) val[l] = rowval[l] / indeg[rowind[l]];
+  for (k = 0; k < n; ++k) rank[k] = 1.0 / n;
+  for (i = 0; niter == 0 || i < niter; ++i) {
+    blas_spmult(n, n, 1, rowptr, rowind, val, rank, out, NULL, 0);
+    blas_scale(n, out, damping);
+    dist = 0;
+    for (k = 0; k < nsinks; ++k) dist += rank[sinks[k]];
+    blas_add_scalar(n, out, ((1.0 - damping) / n) + dist);
+    if (i % 10 == 0) {
+      err = 0.0;
+      for (k = 0; k < n; ++k) {
+        diff = rank[k] - out[k];
+        err += diff * diff;
+      }
+      if (err <= minerror * minerror) {
+        ++i;
+        done = 1;
+        break;
+      }
+    }
+    tmp = rank;
+    rank = out;
+    out = tmp;
+  }
+  if (!done) {
+    err = 0.0;
+    for (k = 0; k < n; ++k) {
+      diff = rank[k] - out[k];
+      err += diff * diff;
+    }
+  }
+  *error = sqrt(err);
+  memcpy(result, out, sizeof(real_t) * n);
+  free(indeg);
+  free(val);
+  free(sinks);
+  free(rank);
+  free(out);
+  return i;
 }

@@ -114,3 +114,35 @@ def test_spdot_matches_reference_build():
     v32 = A.rowval.astype(np.float32)
     assert (oracle.ref_spdot(A.rowind, v32, x32, real="f32")
             == oracle.spdot(A.rowind, v32, x32, real="f32"))
+
+
+def _pr_graph(n, nnz, seed, nsinks=0):
+    A = W.powerlaw_rows(n, nnz, seed=seed, cap=n)
+    rv = np.abs(A.rowval) + 0.1
+    if not nsinks:
+        return A.rowptr, A.rowind, rv
+    rp = A.rowptr.astype(np.int64)
+    keep = np.ones(A.nnz, bool)
+    L = np.diff(rp)
+    for k in range(nsinks):
+        keep[rp[k]:rp[k + 1]] = False
+        L[k] = 0
+    return (np.concatenate([[0], np.cumsum(L)]).astype(np.uint32), A.rowind[keep], rv[keep])
+
+
+@pytest.mark.skipif(not oracle.ref_available("f64"), reason="reference build absent")
+def test_pagerank_restatement_matches_reference_loop():
+    """The restated pagerank command equals the same loop around the
+    reference's own blas_spmult / blas_scale / blas_add_scalar, bit for bit:
+    converging (no sinks) and at an iteration limit (with sinks, whose mass the
+    reference adds whole to every entry)."""
+    oracle.ref_set_threads(1)
+    rp, ri, rv = _pr_graph(3000, 30000, 5)
+    a = oracle.pagerank(rp, ri, rv, 0.85, 1e-10, 0)
+    b = oracle.ref_pagerank(rp, ri, rv, 0.85, 1e-10, 0)
+    assert a[1] == b[1] and a[1] % 10 == 1 and a[2] == b[2] and np.array_equal(a[0], b[0])
+    assert abs(a[0].sum() - 1.0) < 1e-9
+    rp, ri, rv = _pr_graph(3000, 30000, 6, nsinks=7)
+    a = oracle.pagerank(rp, ri, rv, 0.9, 0.0, 13)
+    b = oracle.ref_pagerank(rp, ri, rv, 0.9, 0.0, 13)
+    assert a[1] == b[1] == 13 and a[2] == b[2] and np.array_equal(a[0], b[0])
