@@ -708,6 +708,40 @@ def serving_extra(nreq=400, seed=5, rtol=1e-10, pool=16 << 30, slots=256, ips=8,
     }
 
 
+def pagerank_extra(n=2_000_000, nnz=32_000_000, seed=7, tol=1e-10, cpu_iters=5):
+    """PageRank (the reference's pagerank command) on a power-law directed graph
+    (n nodes, nnz weighted edges, Zipf-2.1 out-degrees, weights |U[-1,1]| + 0.1),
+    damping 0.85, to a change of at most `tol`.  Ours: gooseberry_pagerank_f64
+    end to end (host normalisation as the reference, upload, device iterations,
+    download).  CPU: the reference's loop (blas_spmult etc., all host threads) on
+    a bounded sample of `cpu_iters` iterations, scaled to the same count."""
+    import gooseberry_b200 as gb
+    import oracle
+    from gooseberry_b200 import workloads as W
+    A = W.powerlaw_rows(n, nnz, seed=seed, cap=200_000)
+    rv = np.abs(A.rowval) + 0.1
+    gb.pagerank(A.rowptr, A.rowind, rv, 0.85, 0.0, 2)  # warm
+    t0 = time.perf_counter()
+    r, it, err = gb.pagerank(A.rowptr, A.rowind, rv, 0.85, tol, 0)
+    t_ours = time.perf_counter() - t0
+    out = {"n": n, "nnz": nnz, "tol": tol, "iterations": it, "error": err,
+           "ms": t_ours * 1e3, "solves_per_s": 1.0 / t_ours,
+           "rank_sum": float(r.sum())}
+    if oracle.ref_available("f64"):
+        threads = os.cpu_count() or 1
+        oracle.ref_set_threads(threads)
+        t0 = time.perf_counter()
+        r5, _, _ = oracle.ref_pagerank(A.rowptr, A.rowind, rv, 0.85, 0.0, cpu_iters)
+        t_cpu = time.perf_counter() - t0
+        g5, _, _ = gb.pagerank(A.rowptr, A.rowind, rv, 0.85, 0.0, cpu_iters)
+        out["cpu_reference"] = {"cores": threads, "sample_iterations": cpu_iters,
+                                "sample_s": t_cpu,
+                                "ms_scaled_to_iterations": t_cpu / cpu_iters * it * 1e3}
+        out["max_rel_diff_vs_reference_at_sample"] = float(
+            np.max(np.abs(g5 - r5)) / np.max(np.abs(r5)))
+    return out
+
+
 def run_extras(args):
     """Secondary workloads of the benchmark spec, reported beside the headline."""
     import torch
@@ -724,6 +758,7 @@ def run_extras(args):
     del A
     ex["mixed_cg_3d_160"] = mixed_extra()
     ex["serving_stream"] = serving_extra(nreq=args.requests)
+    ex["pagerank_powerlaw_2m"] = pagerank_extra()
     ex["seconds"] = time.time() - t0
     return ex
 
@@ -793,6 +828,8 @@ def main():
             out = {"extras": {"mixed_cg_3d_160": mixed_extra()}}
         elif args.workload == "serving":
             out = {"extras": {"serving_stream": serving_extra(nreq=args.requests)}}
+        elif args.workload == "pagerank":
+            out = {"extras": {"pagerank_powerlaw_2m": pagerank_extra()}}
         else:
             raise SystemExit(f"unknown workload {args.workload}")
         if dist.rank == 0:

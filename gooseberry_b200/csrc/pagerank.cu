@@ -16,6 +16,7 @@
 // second-to-last iterate (the buffer the last swap left in `out`).
 #include <algorithm>
 #include <cmath>
+#include <thread>
 #include <vector>
 
 #include "gb_internal.h"
@@ -131,22 +132,36 @@ int pagerank_f64(dim_t n, const ind_t * rowptr, const dim_t * rowind, const doub
   const uint32_t nnz = rowptr[n];
   GB_CHECK_INPUT(nnz == 0 || (rowind && rowval), "NULL array");
   GB_CHECK_INPUT(rowptr[0] == 0, "rowptr[0] must be 0");
-  // normalise like src/gooseberry_bin.c:2611-2630 (row order, sequential)
-  std::vector<double> indeg(n, 0.0), val(nnz ? nnz : 1);
+  // normalise like src/gooseberry_bin.c:2611-2630.  Host threads split the
+  // COLUMNS: each scans all entries in row order and sums only its own
+  // columns, so every column sum is accumulated in the reference's order.
   std::vector<uint32_t> sinks;
   for (dim_t k = 0; k < n; ++k) {
     GB_CHECK_INPUT(rowptr[k + 1] >= rowptr[k], "rowptr decreases at row %u", k);
-    if (rowptr[k] == rowptr[k + 1]) {
-      sinks.push_back(k);
-    } else {
-      for (ind_t l = rowptr[k]; l < rowptr[k + 1]; ++l) {
-        GB_CHECK_INPUT(rowind[l] < n, "column index %u out of range for %u columns", rowind[l],
-            n);
-        indeg[rowind[l]] += rowval[l];
-      }
-    }
+    if (rowptr[k] == rowptr[k + 1]) sinks.push_back(k);
   }
-  for (ind_t l = 0; l < nnz; ++l) val[l] = rowval[l] / indeg[rowind[l]];
+  for (ind_t l = 0; l < nnz; ++l)
+    GB_CHECK_INPUT(rowind[l] < n, "column index %u out of range for %u columns", rowind[l], n);
+  std::vector<double> indeg(n, 0.0), val(nnz ? nnz : 1);
+  const unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  auto parallel = [&](auto && body) {
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; ++t) th.emplace_back(body, t);
+    for (auto & x : th) x.join();
+  };
+  parallel([&](unsigned t) {
+    const uint32_t c0 = static_cast<uint32_t>(static_cast<uint64_t>(n) * t / nt);
+    const uint32_t c1 = static_cast<uint32_t>(static_cast<uint64_t>(n) * (t + 1) / nt);
+    for (ind_t l = 0; l < nnz; ++l) {
+      const uint32_t c = rowind[l];
+      if (c >= c0 && c < c1) indeg[c] += rowval[l];
+    }
+  });
+  parallel([&](unsigned t) {
+    const ind_t l0 = static_cast<ind_t>(static_cast<uint64_t>(nnz) * t / nt);
+    const ind_t l1 = static_cast<ind_t>(static_cast<uint64_t>(nnz) * (t + 1) / nt);
+    for (ind_t l = l0; l < l1; ++l) val[l] = rowval[l] / indeg[rowind[l]];
+  });
 
   PrBuffers B;
   GB_CUDA_TRY(cudaStreamCreateWithFlags(&B.st, cudaStreamNonBlocking));
