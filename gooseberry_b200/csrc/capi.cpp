@@ -45,11 +45,14 @@ cudaStream_t dropin_stream(int * rc) {
   return streams[dev];
 }
 
-// Device buffer freed at scope exit.
+// Device buffer (library pool) freed at scope exit, after the device is idle.
 struct DevBuf {
   void * p = nullptr;
   ~DevBuf() {
-    if (p) cudaFree(p);
+    if (p) {
+      cudaDeviceSynchronize();
+      gb::dev_free(p);
+    }
   }
 };
 
@@ -61,7 +64,7 @@ int vec_op(ind_t n, T * val, T s, bool add) {
   cudaStream_t st = dropin_stream(&rc);
   GB_TRY(rc);
   DevBuf d;
-  GB_CUDA_TRY(cudaMalloc(&d.p, n * sizeof(T)));
+  GB_TRY(gb::dev_alloc(&d.p, n * sizeof(T)));
   GB_CUDA_TRY(cudaMemcpyAsync(d.p, val, n * sizeof(T), cudaMemcpyHostToDevice, st));
   if (sizeof(T) == 8) {
     rc = add ? gb::launch_add_scalar_f64(n, static_cast<double *>(d.p), s, st)
@@ -109,8 +112,8 @@ int spmult_impl(dim_t anrows, dim_t ancols, dim_t bncols, const ind_t * rowptr,
   DevBuf db, dc;
   const size_t bsz = static_cast<size_t>(ancols) * bncols;
   const size_t csz = static_cast<size_t>(anrows) * bncols;
-  GB_CUDA_TRY(cudaMalloc(&db.p, std::max<size_t>(bsz, 1) * sizeof(T)));
-  GB_CUDA_TRY(cudaMalloc(&dc.p, csz * sizeof(T)));
+  GB_TRY(gb::dev_alloc(&db.p, std::max<size_t>(bsz, 1) * sizeof(T)));
+  GB_TRY(gb::dev_alloc(&dc.p, csz * sizeof(T)));
   if (bsz) GB_CUDA_TRY(cudaMemcpyAsync(db.p, bcolval, bsz * sizeof(T), cudaMemcpyHostToDevice, st));
   for (dim_t j = 0; j < bncols; ++j) {
     if (f64) {
@@ -154,12 +157,13 @@ int cgd_f64(dim_t n, const ind_t * rowptr, const dim_t * rowind, const double * 
   GB_TRY(gb_csr_create(n, n, nnz, rowptr, rowind, rowval, nullptr, GB_CSR_VALUES_F64, st,
       &g.a));
   gb_cg_t * s = nullptr;
-  GB_TRY(gb_cg_create(g.a, GB_CG_F64, &s));
+  GB_TRY(gb_cg_create(g.a, GB_CG_F64 | GB_CG_DIRECT, &s));
   DevBuf db, dx;
   rc = GOOSEBERRY_SUCCESS;
   gb_cg_result_t res{};
-  if (cudaMalloc(&db.p, n * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&dx.p, n * sizeof(double)) != cudaSuccess ||
+  rc = gb::dev_alloc(&db.p, n * sizeof(double));
+  if (rc == GOOSEBERRY_SUCCESS) rc = gb::dev_alloc(&dx.p, n * sizeof(double));
+  if (rc == GOOSEBERRY_SUCCESS &&
       cudaMemcpyAsync(db.p, b, n * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess) {
     gb::set_error("CG buffers: %s", cudaGetErrorString(cudaGetLastError()));
     rc = GOOSEBERRY_ERROR_UNKNOWN;

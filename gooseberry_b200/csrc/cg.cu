@@ -680,6 +680,7 @@ struct gb_cg {
   uint32_t * cta_tiles = nullptr;
   unsigned * sync = nullptr;  // [0] barrier counter, [1] abort flag
   int keep_l2 = 0;
+  bool direct = false;   // GB_CG_DIRECT: kernels launched one by one, no graphs
   bool l2_hint = false;  // A kernel with L2-policy loads (working set fits in L2)
   gb::MixedCg * mixed = nullptr;  // GB_CG_MIXED solver (owns its workspace)
 };
@@ -689,29 +690,30 @@ namespace {
 
 void destroy_cg(gb_cg * s) {
   if (!s) return;
+  cudaDeviceSynchronize();  // its memory goes back to the pool below
   mixed_destroy(s->mixed);
   for (auto & g : s->graph)
     if (g) cudaGraphExecDestroy(g);
   if (s->cap_stream) cudaStreamDestroy(s->cap_stream);
-  cudaFree(s->x);
-  cudaFree(s->r);
-  cudaFree(s->p[0]);
-  cudaFree(s->p[1]);
-  cudaFree(s->ap);
-  cudaFree(s->partial_a);
-  cudaFree(s->partial_b);
-  cudaFree(s->partial_i);
-  cudaFree(s->longdot);
-  cudaFree(s->st);
-  cudaFree(s->cta_tiles);
-  cudaFree(s->sync);
+  dev_free(s->x);
+  dev_free(s->r);
+  dev_free(s->p[0]);
+  dev_free(s->p[1]);
+  dev_free(s->ap);
+  dev_free(s->partial_a);
+  dev_free(s->partial_b);
+  dev_free(s->partial_i);
+  dev_free(s->longdot);
+  dev_free(s->st);
+  dev_free(s->cta_tiles);
+  dev_free(s->sync);
   if (s->host_status) cudaFreeHost(s->host_status);
   delete s;
 }
 
-int capture_chunk(gb_cg * s, int slot) {
-  cudaStream_t cs = s->cap_stream;
-  GB_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+// One chunk of iterations (A, B per iteration) and the status mirror into
+// host_status[slot], on stream cs: captured into a graph, or launched directly.
+int enqueue_chunk(gb_cg * s, int slot, cudaStream_t cs) {
   int rc = GOOSEBERRY_SUCCESS;
   for (int k = 0; k < s->chunk && rc == GOOSEBERRY_SUCCESS; ++k) {
     const double * pold = s->p[k & 1];
@@ -737,6 +739,13 @@ int capture_chunk(gb_cg * s, int slot) {
     cudaMemcpyAsync(&s->host_status[slot].bnorm, &s->st->bnorm, sizeof(double),
         cudaMemcpyDeviceToHost, cs);
   }
+  return rc;
+}
+
+int capture_chunk(gb_cg * s, int slot) {
+  cudaStream_t cs = s->cap_stream;
+  GB_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+  const int rc = enqueue_chunk(s, slot, cs);
   cudaGraph_t g = nullptr;
   cudaError_t e = cudaStreamEndCapture(cs, &g);
   if (rc != GOOSEBERRY_SUCCESS) {
@@ -777,10 +786,10 @@ int setup_persistent(const gb_csr * a, gb_cg * s) {
     bounds[g] = static_cast<uint32_t>(std::max<size_t>(t, bounds[g - 1]));
   }
   bounds[G] = static_cast<uint32_t>(ntiles);
-  GB_CUDA_TRY(cudaMalloc(&s->cta_tiles, (G + 1) * sizeof(uint32_t)));
+  GB_TRY(dev_alloc(&s->cta_tiles, (G + 1) * sizeof(uint32_t)));
   GB_CUDA_TRY(cudaMemcpy(s->cta_tiles, bounds.data(), (G + 1) * sizeof(uint32_t),
       cudaMemcpyHostToDevice));
-  GB_CUDA_TRY(cudaMalloc(&s->sync, 2 * sizeof(unsigned)));
+  GB_TRY(dev_alloc(&s->sync, 2 * sizeof(unsigned)));
   // the matrix stays L2-resident across iterations when the working set of
   // one iteration fits in about 3/4 of L2
   int l2 = 0;
@@ -826,7 +835,8 @@ int create_cg(const gb_csr * a, int mode, gb_cg * s) {
   GB_CHECK_INPUT(a->nrows == a->ncols, "CG needs a square matrix, got %ux%u", a->nrows,
       a->ncols);
   const bool want_persistent = (mode & GB_CG_PERSISTENT) != 0;
-  mode &= ~GB_CG_PERSISTENT;
+  const bool direct = (mode & GB_CG_DIRECT) != 0;
+  mode &= ~(GB_CG_PERSISTENT | GB_CG_DIRECT);
   GB_CHECK_INPUT(mode == GB_CG_F64 || mode == GB_CG_MIXED, "unknown CG mode %d", mode);
   if (mode == GB_CG_MIXED) {
     s->a = a;
@@ -839,11 +849,11 @@ int create_cg(const gb_csr * a, int mode, gb_cg * s) {
   s->mode = mode;
   s->n = a->nrows;
   const size_t n = std::max<size_t>(s->n, 2);
-  GB_CUDA_TRY(cudaMalloc(&s->x, n * sizeof(double)));
-  GB_CUDA_TRY(cudaMalloc(&s->r, n * sizeof(double)));
-  GB_CUDA_TRY(cudaMalloc(&s->p[0], n * sizeof(double)));
-  GB_CUDA_TRY(cudaMalloc(&s->p[1], n * sizeof(double)));
-  GB_CUDA_TRY(cudaMalloc(&s->ap, n * sizeof(double)));
+  GB_TRY(dev_alloc(&s->x, n * sizeof(double)));
+  GB_TRY(dev_alloc(&s->r, n * sizeof(double)));
+  GB_TRY(dev_alloc(&s->p[0], n * sizeof(double)));
+  GB_TRY(dev_alloc(&s->p[1], n * sizeof(double)));
+  GB_TRY(dev_alloc(&s->ap, n * sizeof(double)));
   s->sched = a->sched64;
   s->tile_items = a->plan.tile_items;
   // evict-first/evict-last hints keep an L2-sized working set (matrix, rowptr,
@@ -868,16 +878,17 @@ int create_cg(const gb_csr * a, int mode, gb_cg * s) {
   const unsigned gmax = std::max<unsigned>(std::max(s->grid_a, s->grid_b),
       static_cast<unsigned>(std::min<size_t>(a->plan.tiles.size() + 1,
           static_cast<size_t>(a->sm_count) * 32)));
-  GB_CUDA_TRY(cudaMalloc(&s->partial_a, gmax * sizeof(double)));
-  GB_CUDA_TRY(cudaMalloc(&s->partial_b, gmax * sizeof(double)));
-  GB_CUDA_TRY(cudaMalloc(&s->partial_i, gmax * sizeof(double)));
-  GB_CUDA_TRY(cudaMalloc(&s->longdot,
+  GB_TRY(dev_alloc(&s->partial_a, gmax * sizeof(double)));
+  GB_TRY(dev_alloc(&s->partial_b, gmax * sizeof(double)));
+  GB_TRY(dev_alloc(&s->partial_i, gmax * sizeof(double)));
+  GB_TRY(dev_alloc(&s->longdot,
       std::max<size_t>(a->plan.longrows.size(), 1) * sizeof(double)));
-  GB_CUDA_TRY(cudaMalloc(&s->st, sizeof(CgState)));
+  GB_TRY(dev_alloc(&s->st, sizeof(CgState)));
   GB_CUDA_TRY(cudaMemset(s->st, 0, sizeof(CgState)));
   GB_CUDA_TRY(cudaMallocHost(&s->host_status, 2 * sizeof(CgStatus)));
   if (want_persistent) GB_TRY(setup_persistent(a, s));
-  if (!s->persistent) {
+  s->direct = direct && !s->persistent;
+  if (!s->persistent && !s->direct) {
     GB_CUDA_TRY(cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking));
     GB_TRY(capture_chunk(s, 0));
     GB_TRY(capture_chunk(s, 1));
@@ -930,6 +941,16 @@ int solve_cg(gb_cg * s, const double * b, double * x, double tol, int tol_relati
   int rc = GOOSEBERRY_SUCCESS;
   s->host_status[0].done = s->host_status[1].done = 0;
   auto launch = [&](int slot) -> int {
+    if (s->direct) {  // the same kernels and status copies, launched one by one
+      const int r2 = enqueue_chunk(s, slot, stream);
+      const cudaError_t e2 = cudaEventRecord(ev[slot], stream);
+      launches += 2 * static_cast<size_t>(s->chunk);
+      if (r2 != GOOSEBERRY_SUCCESS || e2 != cudaSuccess) {
+        set_error("CG launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+        return GOOSEBERRY_ERROR_UNKNOWN;
+      }
+      return GOOSEBERRY_SUCCESS;
+    }
     cudaError_t e = cudaGraphLaunch(s->graph[slot], stream);
     if (e == cudaSuccess) e = cudaEventRecord(ev[slot], stream);
     launches += 2 * static_cast<size_t>(s->chunk);

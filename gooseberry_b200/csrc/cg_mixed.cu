@@ -576,23 +576,24 @@ int grid_of(const gb_csr * a, int sched, size_t smem, bool f32, unsigned * grid)
 
 void mixed_destroy(MixedCg * m) {
   if (!m) return;
+  cudaDeviceSynchronize();  // its memory goes back to the pool below
   for (auto & g : m->graph)
     if (g) cudaGraphExecDestroy(g);
   if (m->cap_stream) cudaStreamDestroy(m->cap_stream);
-  cudaFree(m->x[0]);
-  cudaFree(m->x[1]);
-  cudaFree(m->b);
-  cudaFree(m->y);
-  cudaFree(m->r);
-  cudaFree(m->p[0]);
-  cudaFree(m->p[1]);
-  cudaFree(m->ap);
-  cudaFree(m->partial_a);
-  cudaFree(m->partial_b);
-  cudaFree(m->partial_r);
-  cudaFree(m->partial_i);
-  cudaFree(m->longdot);
-  cudaFree(m->st);
+  dev_free(m->x[0]);
+  dev_free(m->x[1]);
+  dev_free(m->b);
+  dev_free(m->y);
+  dev_free(m->r);
+  dev_free(m->p[0]);
+  dev_free(m->p[1]);
+  dev_free(m->ap);
+  dev_free(m->partial_a);
+  dev_free(m->partial_b);
+  dev_free(m->partial_r);
+  dev_free(m->partial_i);
+  dev_free(m->longdot);
+  dev_free(m->st);
   if (m->host_status) cudaFreeHost(m->host_status);
   delete m;
 }
@@ -612,14 +613,14 @@ int mixed_create(const gb_csr * a, MixedCg ** out) {
   // indices, float values, r, both p, Ap, y) fits in L2
   GB_TRY(l2_fits(4ull * (m->n + 1) + 8ull * a->nnz + 24ull * m->n, &m->l2_hint));
   const size_t n = std::max<size_t>(m->n, 2);
-  GB_CUDA_TRY(cudaMalloc(&m->x[0], n * sizeof(double)));
-  GB_CUDA_TRY(cudaMalloc(&m->x[1], n * sizeof(double)));
-  GB_CUDA_TRY(cudaMalloc(&m->b, n * sizeof(double)));
-  GB_CUDA_TRY(cudaMalloc(&m->y, n * sizeof(float)));
-  GB_CUDA_TRY(cudaMalloc(&m->r, n * sizeof(float)));
-  GB_CUDA_TRY(cudaMalloc(&m->p[0], n * sizeof(float)));
-  GB_CUDA_TRY(cudaMalloc(&m->p[1], n * sizeof(float)));
-  GB_CUDA_TRY(cudaMalloc(&m->ap, n * sizeof(float)));
+  GB_TRY(dev_alloc(&m->x[0], n * sizeof(double)));
+  GB_TRY(dev_alloc(&m->x[1], n * sizeof(double)));
+  GB_TRY(dev_alloc(&m->b, n * sizeof(double)));
+  GB_TRY(dev_alloc(&m->y, n * sizeof(float)));
+  GB_TRY(dev_alloc(&m->r, n * sizeof(float)));
+  GB_TRY(dev_alloc(&m->p[0], n * sizeof(float)));
+  GB_TRY(dev_alloc(&m->p[1], n * sizeof(float)));
+  GB_TRY(dev_alloc(&m->ap, n * sizeof(float)));
   GB_TRY(grid_of(a, m->sched32, smem_of(m->sched32, m->tile_items, 4), true, &m->grid_a));
   GB_TRY(grid_of(a, m->sched64, smem_of(m->sched64, m->tile_items, 8), false, &m->grid_r));
   int occ_b = 0;
@@ -627,13 +628,13 @@ int mixed_create(const gb_csr * a, MixedCg ** out) {
   m->grid_b = static_cast<unsigned>(std::max<size_t>(1, std::min<size_t>(
       (m->n + kVecBlock - 1) / kVecBlock, static_cast<size_t>(a->sm_count) * std::max(occ_b, 1))));
   const unsigned gmax = std::max({m->grid_a, m->grid_b, m->grid_r, 1u});
-  GB_CUDA_TRY(cudaMalloc(&m->partial_a, gmax * sizeof(double)));
-  GB_CUDA_TRY(cudaMalloc(&m->partial_b, gmax * sizeof(double)));
-  GB_CUDA_TRY(cudaMalloc(&m->partial_r, gmax * sizeof(double)));
-  GB_CUDA_TRY(cudaMalloc(&m->partial_i, 2 * gmax * sizeof(double)));
-  GB_CUDA_TRY(cudaMalloc(&m->longdot,
+  GB_TRY(dev_alloc(&m->partial_a, gmax * sizeof(double)));
+  GB_TRY(dev_alloc(&m->partial_b, gmax * sizeof(double)));
+  GB_TRY(dev_alloc(&m->partial_r, gmax * sizeof(double)));
+  GB_TRY(dev_alloc(&m->partial_i, 2 * gmax * sizeof(double)));
+  GB_TRY(dev_alloc(&m->longdot,
       std::max<size_t>(a->plan.longrows.size(), 1) * sizeof(double)));
-  GB_CUDA_TRY(cudaMalloc(&m->st, sizeof(MixState)));
+  GB_TRY(dev_alloc(&m->st, sizeof(MixState)));
   GB_CUDA_TRY(cudaMemset(m->st, 0, sizeof(MixState)));
   GB_CUDA_TRY(cudaMallocHost(&m->host_status, 2 * sizeof(MixStatus)));
   GB_CUDA_TRY(cudaStreamCreateWithFlags(&m->cap_stream, cudaStreamNonBlocking));

@@ -159,9 +159,18 @@ int sm_count_of_current_device(int * out);
 // Whether `bytes` of working set fit in the current device's L2 (the CG
 // kernels use L2-policy loads only then).
 int l2_fits(size_t bytes, bool * out);
-// Stream-ordered scratch from a library-owned pool that keeps its memory.
+// Stream-ordered scratch from the library-owned memory pool.
 int scratch_alloc(void ** p, size_t bytes, cudaStream_t s);
 void scratch_free(void * p, cudaStream_t s);
+// Object memory from the same pool: dev_alloc returns memory usable from any
+// stream; dev_free may only be called once no work that uses the memory can
+// still run (the destroy paths synchronise the device first).
+int dev_alloc(void ** p, size_t bytes);
+void dev_free(void * p);
+template <typename T>
+int dev_alloc(T ** p, size_t bytes) {
+  return dev_alloc(reinterpret_cast<void **>(p), bytes);
+}
 
 // Mixed-precision CG (cg_mixed.cu), owned by a gb_cg created with GB_CG_MIXED.
 struct MixedCg;

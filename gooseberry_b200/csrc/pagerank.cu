@@ -114,11 +114,11 @@ struct PrBuffers {
   gb_csr_t * a = nullptr;
   ~PrBuffers() {
     if (st) cudaStreamSynchronize(st);
-    cudaFree(rank);
-    cudaFree(out);
-    cudaFree(partial);
-    cudaFree(scal);
-    cudaFree(sinks);
+    dev_free(rank);
+    dev_free(out);
+    dev_free(partial);
+    dev_free(scal);
+    dev_free(sinks);
     if (h_err) cudaFreeHost(h_err);
     if (a) gb_csr_destroy(a);
     if (st) cudaStreamDestroy(st);
@@ -173,14 +173,14 @@ int pagerank_f64(dim_t n, const ind_t * rowptr, const dim_t * rowind, const doub
       (n + kPrBlock * 4 - 1) / (kPrBlock * 4), static_cast<size_t>(sms) * 4)));
   const unsigned gs = static_cast<unsigned>(std::max<size_t>(1, std::min<size_t>(
       (sinks.size() + kPrBlock * 4 - 1) / (kPrBlock * 4), static_cast<size_t>(sms) * 4)));
-  GB_CUDA_TRY(cudaMalloc(&B.rank, n * sizeof(double)));
-  GB_CUDA_TRY(cudaMalloc(&B.out, n * sizeof(double)));
-  GB_CUDA_TRY(cudaMalloc(&B.partial, std::max(g, gs) * sizeof(double)));
-  GB_CUDA_TRY(cudaMalloc(&B.scal, 2 * sizeof(double)));
+  GB_TRY(dev_alloc(&B.rank, n * sizeof(double)));
+  GB_TRY(dev_alloc(&B.out, n * sizeof(double)));
+  GB_TRY(dev_alloc(&B.partial, std::max(g, gs) * sizeof(double)));
+  GB_TRY(dev_alloc(&B.scal, 2 * sizeof(double)));
   GB_CUDA_TRY(cudaMemsetAsync(B.scal, 0, 2 * sizeof(double), B.st));
   GB_CUDA_TRY(cudaMallocHost(&B.h_err, sizeof(double)));
   if (!sinks.empty()) {
-    GB_CUDA_TRY(cudaMalloc(&B.sinks, sinks.size() * sizeof(uint32_t)));
+    GB_TRY(dev_alloc(&B.sinks, sinks.size() * sizeof(uint32_t)));
     GB_CUDA_TRY(cudaMemcpyAsync(B.sinks, sinks.data(), sinks.size() * sizeof(uint32_t),
         cudaMemcpyHostToDevice, B.st));
   }

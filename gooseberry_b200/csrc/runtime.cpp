@@ -43,41 +43,68 @@ int l2_fits(size_t bytes, bool * out) {
 }
 
 namespace {
+struct DevicePool {
+  cudaMemPool_t pool = nullptr;
+  cudaStream_t alloc_stream = nullptr;  // orders the pool's own allocations and frees
+};
 std::mutex g_pool_mu;
-std::vector<cudaMemPool_t> g_pools;  // per device, created on first use
-}  // namespace
+std::vector<DevicePool> g_pools;  // per device, created on first use
+// Memory the pool keeps for reuse after frees; beyond this it returns memory
+// to the device at synchronisation points.
+constexpr uint64_t kPoolKeepBytes = 4ull << 30;
 
-// Small per-call scratch (reduction partials, histories) comes from a memory
-// pool the library owns: it keeps its memory between calls (release threshold
-// = all), so a stream-ordered allocation costs no driver mapping after the
-// first one, and the device's default pool and its settings stay untouched.
-int scratch_alloc(void ** p, size_t bytes, cudaStream_t s) {
+int pool_of_current_device(DevicePool * out) {
   int dev = 0;
   GB_CUDA_TRY(cudaGetDevice(&dev));
-  cudaMemPool_t pool = nullptr;
-  {
-    std::lock_guard<std::mutex> lock(g_pool_mu);
-    if (g_pools.size() <= static_cast<size_t>(dev)) g_pools.resize(dev + 1, nullptr);
-    if (!g_pools[dev]) {
-      cudaMemPoolProps props = {};
-      props.allocType = cudaMemAllocationTypePinned;
-      props.handleTypes = cudaMemHandleTypeNone;
-      props.location.type = cudaMemLocationTypeDevice;
-      props.location.id = dev;
-      cudaMemPool_t np = nullptr;
-      GB_CUDA_TRY(cudaMemPoolCreate(&np, &props));
-      uint64_t keep = UINT64_MAX;
-      GB_CUDA_TRY(cudaMemPoolSetAttribute(np, cudaMemPoolAttrReleaseThreshold, &keep));
-      g_pools[dev] = np;
-    }
-    pool = g_pools[dev];
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  if (g_pools.size() <= static_cast<size_t>(dev)) g_pools.resize(dev + 1);
+  DevicePool & d = g_pools[dev];
+  if (!d.pool) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t np = nullptr;
+    GB_CUDA_TRY(cudaMemPoolCreate(&np, &props));
+    uint64_t keep = kPoolKeepBytes;
+    GB_CUDA_TRY(cudaMemPoolSetAttribute(np, cudaMemPoolAttrReleaseThreshold, &keep));
+    GB_CUDA_TRY(cudaStreamCreateWithFlags(&d.alloc_stream, cudaStreamNonBlocking));
+    d.pool = np;
   }
-  GB_CUDA_TRY(cudaMallocFromPoolAsync(p, bytes, pool, s));
+  *out = d;
+  return GOOSEBERRY_SUCCESS;
+}
+}  // namespace
+
+// Device memory of the library's objects and per-call scratch comes from a
+// memory pool the library owns: after the first use an allocation costs no
+// driver mapping and a free no device-wide synchronisation, and the device's
+// default pool and its settings stay untouched.
+int scratch_alloc(void ** p, size_t bytes, cudaStream_t s) {
+  DevicePool d;
+  GB_TRY(pool_of_current_device(&d));
+  GB_CUDA_TRY(cudaMallocFromPoolAsync(p, bytes, d.pool, s));
   return GOOSEBERRY_SUCCESS;
 }
 
 void scratch_free(void * p, cudaStream_t s) {
   if (p) cudaFreeAsync(p, s);
+}
+
+int dev_alloc(void ** p, size_t bytes) {
+  DevicePool d;
+  GB_TRY(pool_of_current_device(&d));
+  GB_CUDA_TRY(cudaMallocFromPoolAsync(p, bytes ? bytes : 1, d.pool, d.alloc_stream));
+  GB_CUDA_TRY(cudaStreamSynchronize(d.alloc_stream));  // usable from any stream now
+  return GOOSEBERRY_SUCCESS;
+}
+
+void dev_free(void * p) {
+  if (!p) return;
+  DevicePool d;
+  if (pool_of_current_device(&d) != GOOSEBERRY_SUCCESS) return;
+  cudaFreeAsync(p, d.alloc_stream);
 }
 
 }  // namespace gb

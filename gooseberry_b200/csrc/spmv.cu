@@ -109,10 +109,12 @@ int build_plan(uint32_t nrows, const uint32_t * rowptr, uint32_t nnz,
 }
 
 void free_plan(Plan & plan) {
-  if (plan.d_tiles) cudaFree(plan.d_tiles);
-  if (plan.d_longrows) cudaFree(plan.d_longrows);
-  if (plan.d_chunk_partial) cudaFree(plan.d_chunk_partial);
-  if (plan.d_long_count) cudaFree(plan.d_long_count);
+  if (plan.d_tiles || plan.d_longrows || plan.d_chunk_partial || plan.d_long_count)
+    cudaDeviceSynchronize();  // no kernel may still read the old plan
+  if (plan.d_tiles) dev_free(plan.d_tiles);
+  if (plan.d_longrows) dev_free(plan.d_longrows);
+  if (plan.d_chunk_partial) dev_free(plan.d_chunk_partial);
+  if (plan.d_long_count) dev_free(plan.d_long_count);
   plan.d_tiles = nullptr;
   plan.d_longrows = nullptr;
   plan.d_chunk_partial = nullptr;
@@ -123,10 +125,10 @@ int upload_plan(Plan & plan, cudaStream_t stream) {
   free_plan(plan);
   const size_t nt = std::max<size_t>(plan.tiles.size(), 1);
   const size_t nl = std::max<size_t>(plan.longrows.size(), 1);
-  GB_CUDA_TRY(cudaMalloc(&plan.d_tiles, nt * sizeof(TileDesc)));
-  GB_CUDA_TRY(cudaMalloc(&plan.d_longrows, nl * sizeof(LongRowDesc)));
-  GB_CUDA_TRY(cudaMalloc(&plan.d_chunk_partial, nt * sizeof(double)));
-  GB_CUDA_TRY(cudaMalloc(&plan.d_long_count, nl * sizeof(unsigned int)));
+  GB_TRY(dev_alloc(&plan.d_tiles, nt * sizeof(TileDesc)));
+  GB_TRY(dev_alloc(&plan.d_longrows, nl * sizeof(LongRowDesc)));
+  GB_TRY(dev_alloc(&plan.d_chunk_partial, nt * sizeof(double)));
+  GB_TRY(dev_alloc(&plan.d_long_count, nl * sizeof(unsigned int)));
   if (!plan.tiles.empty())
     GB_CUDA_TRY(cudaMemcpyAsync(plan.d_tiles, plan.tiles.data(),
         plan.tiles.size() * sizeof(TileDesc), cudaMemcpyHostToDevice, stream));
@@ -370,8 +372,8 @@ int autotune(gb_csr & a, unsigned width, cudaStream_t stream) {
   const size_t yb = static_cast<size_t>(a.nrows) * (width == GB_CSR_VALUES_F32 ? 4 : 8);
   void * x = nullptr;
   void * y = nullptr;
-  GB_CUDA_TRY(cudaMalloc(&x, std::max<size_t>(xb, 8)));
-  GB_CUDA_TRY(cudaMalloc(&y, std::max<size_t>(yb, 8)));
+  GB_TRY(dev_alloc(&x, std::max<size_t>(xb, 8)));
+  GB_TRY(dev_alloc(&y, std::max<size_t>(yb, 8)));
   GB_CUDA_TRY(cudaMemsetAsync(x, 0, std::max<size_t>(xb, 8), stream));
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
@@ -433,8 +435,8 @@ int autotune(gb_csr & a, unsigned width, cudaStream_t stream) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  cudaFree(x);
-  cudaFree(y);
+  dev_free(x);
+  dev_free(y);
   GB_TRY(rc);
   GB_TRY(rebuild_plan(a, choice.tile_items, stream));
   (width == GB_CSR_VALUES_F32 ? a.sched32 : a.sched64) = choice.sched;
@@ -447,13 +449,15 @@ int autotune(gb_csr & a, unsigned width, cudaStream_t stream) {
 
 // ---- C ABI ------------------------------------------------------------------
 
+using gb::dev_alloc;
+using gb::dev_free;
 using gb::set_error;
 
 namespace {
 
 template <typename T>
 int alloc_copy(void ** dst, const T * src, size_t n, bool device_src, cudaStream_t s) {
-  GB_CUDA_TRY(cudaMalloc(dst, std::max<size_t>(n, 1) * sizeof(T)));
+  GB_TRY(dev_alloc(dst, std::max<size_t>(n, 1) * sizeof(T)));
   if (n)
     GB_CUDA_TRY(cudaMemcpyAsync(*dst, src, n * sizeof(T),
         device_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
@@ -463,10 +467,10 @@ int alloc_copy(void ** dst, const T * src, size_t n, bool device_src, cudaStream
 void release(gb_csr * a) {
   if (!a) return;
   gb::free_plan(a->plan);
-  if (a->own_rowptr) cudaFree(a->own_rowptr);
-  if (a->own_rowind) cudaFree(a->own_rowind);
-  if (a->own_val64) cudaFree(a->own_val64);
-  if (a->own_val32) cudaFree(a->own_val32);
+  if (a->own_rowptr) dev_free(a->own_rowptr);
+  if (a->own_rowind) dev_free(a->own_rowind);
+  if (a->own_val64) dev_free(a->own_val64);
+  if (a->own_val32) dev_free(a->own_val32);
   delete a;
 }
 
@@ -529,11 +533,11 @@ int create_impl(dim_t nrows, dim_t ncols, ind_t nnz, const ind_t * rowptr,
       GB_TRY(alloc_copy(&tmp, rowval64, nnz, dev, stream));
       src = static_cast<const double *>(tmp);
     }
-    GB_CUDA_TRY(cudaMalloc(&a->own_val32, std::max<size_t>(nnz, 1) * sizeof(float)));
+    GB_TRY(dev_alloc(&a->own_val32, std::max<size_t>(nnz, 1) * sizeof(float)));
     int rc = gb::launch_round_f32(src, static_cast<float *>(a->own_val32), nnz, stream);
     if (tmp) {
       cudaStreamSynchronize(stream);
-      cudaFree(tmp);
+      dev_free(tmp);
     }
     GB_TRY(rc);
     a->val32 = static_cast<const float *>(a->own_val32);
@@ -542,7 +546,7 @@ int create_impl(dim_t nrows, dim_t ncols, ind_t nnz, const ind_t * rowptr,
   // validate column indices on the device
   if (nnz > 0) {
     unsigned int * d_max = nullptr;
-    GB_CUDA_TRY(cudaMalloc(&d_max, sizeof(unsigned int)));
+    GB_TRY(dev_alloc(&d_max, sizeof(unsigned int)));
     unsigned int hmax = 0;
     int rc = gb::launch_max_index(a->rowind, nnz, d_max, stream);
     if (rc == GOOSEBERRY_SUCCESS) {
@@ -553,7 +557,7 @@ int create_impl(dim_t nrows, dim_t ncols, ind_t nnz, const ind_t * rowptr,
         rc = GOOSEBERRY_ERROR_UNKNOWN;
       }
     }
-    cudaFree(d_max);
+    dev_free(d_max);
     GB_TRY(rc);
     GB_CHECK_INPUT(hmax < ncols, "column index %u out of range for %u columns", hmax, ncols);
   }
