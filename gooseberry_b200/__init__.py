@@ -51,7 +51,6 @@ SCHED_NAMES = {0: "auto", 1: "thread", 2: "group4", 3: "group8", 4: "warp", 5: "
                6: "row", 7: "wtile", 8: "wmerge"}
 CG_F64, CG_MIXED = 0, 1
 CG_PERSISTENT = 0x100
-CG_DIRECT = 0x200
 CG_STATUS = {0: "converged", 1: "maxiter", 2: "breakdown", 3: "nonfinite"}
 
 
@@ -414,11 +413,10 @@ class CgResult:
 class CgSolver:
     """CG workspace bound to one matrix (``gb_cg_t``)."""
 
-    def __init__(self, A: CsrMatrix, mode: int = CG_F64, persistent: bool = False,
-                 direct: bool = False):
+    def __init__(self, A: CsrMatrix, mode: int = CG_F64, persistent: bool = False):
         self.A = A
         h = C.c_void_p()
-        flags = mode | (CG_PERSISTENT if persistent else 0) | (CG_DIRECT if direct else 0)
+        flags = mode | (CG_PERSISTENT if persistent else 0)
         _check(lib().gb_cg_create(A._h, flags, C.addressof(h)), "gb_cg_create")
         self._h = h
 

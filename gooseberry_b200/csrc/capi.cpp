@@ -157,7 +157,7 @@ int cgd_f64(dim_t n, const ind_t * rowptr, const dim_t * rowind, const double * 
   GB_TRY(gb_csr_create(n, n, nnz, rowptr, rowind, rowval, nullptr, GB_CSR_VALUES_F64, st,
       &g.a));
   gb_cg_t * s = nullptr;
-  GB_TRY(gb_cg_create(g.a, GB_CG_F64 | GB_CG_DIRECT, &s));
+  GB_TRY(gb_cg_create(g.a, GB_CG_F64, &s));
   DevBuf db, dx;
   rc = GOOSEBERRY_SUCCESS;
   gb_cg_result_t res{};

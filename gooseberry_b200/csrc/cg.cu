@@ -680,7 +680,6 @@ struct gb_cg {
   uint32_t * cta_tiles = nullptr;
   unsigned * sync = nullptr;  // [0] barrier counter, [1] abort flag
   int keep_l2 = 0;
-  bool direct = false;   // GB_CG_DIRECT: kernels launched one by one, no graphs
   bool l2_hint = false;  // A kernel with L2-policy loads (working set fits in L2)
   gb::MixedCg * mixed = nullptr;  // GB_CG_MIXED solver (owns its workspace)
 };
@@ -712,7 +711,7 @@ void destroy_cg(gb_cg * s) {
 }
 
 // One chunk of iterations (A, B per iteration) and the status mirror into
-// host_status[slot], on stream cs: captured into a graph, or launched directly.
+// host_status[slot], on the capture stream cs.
 int enqueue_chunk(gb_cg * s, int slot, cudaStream_t cs) {
   int rc = GOOSEBERRY_SUCCESS;
   for (int k = 0; k < s->chunk && rc == GOOSEBERRY_SUCCESS; ++k) {
@@ -835,8 +834,7 @@ int create_cg(const gb_csr * a, int mode, gb_cg * s) {
   GB_CHECK_INPUT(a->nrows == a->ncols, "CG needs a square matrix, got %ux%u", a->nrows,
       a->ncols);
   const bool want_persistent = (mode & GB_CG_PERSISTENT) != 0;
-  const bool direct = (mode & GB_CG_DIRECT) != 0;
-  mode &= ~(GB_CG_PERSISTENT | GB_CG_DIRECT);
+  mode &= ~GB_CG_PERSISTENT;
   GB_CHECK_INPUT(mode == GB_CG_F64 || mode == GB_CG_MIXED, "unknown CG mode %d", mode);
   if (mode == GB_CG_MIXED) {
     s->a = a;
@@ -887,8 +885,7 @@ int create_cg(const gb_csr * a, int mode, gb_cg * s) {
   GB_CUDA_TRY(cudaMemset(s->st, 0, sizeof(CgState)));
   GB_CUDA_TRY(cudaMallocHost(&s->host_status, 2 * sizeof(CgStatus)));
   if (want_persistent) GB_TRY(setup_persistent(a, s));
-  s->direct = direct && !s->persistent;
-  if (!s->persistent && !s->direct) {
+  if (!s->persistent) {
     GB_CUDA_TRY(cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking));
     GB_TRY(capture_chunk(s, 0));
     GB_TRY(capture_chunk(s, 1));
@@ -941,16 +938,6 @@ int solve_cg(gb_cg * s, const double * b, double * x, double tol, int tol_relati
   int rc = GOOSEBERRY_SUCCESS;
   s->host_status[0].done = s->host_status[1].done = 0;
   auto launch = [&](int slot) -> int {
-    if (s->direct) {  // the same kernels and status copies, launched one by one
-      const int r2 = enqueue_chunk(s, slot, stream);
-      const cudaError_t e2 = cudaEventRecord(ev[slot], stream);
-      launches += 2 * static_cast<size_t>(s->chunk);
-      if (r2 != GOOSEBERRY_SUCCESS || e2 != cudaSuccess) {
-        set_error("CG launch failed: %s", cudaGetErrorString(cudaGetLastError()));
-        return GOOSEBERRY_ERROR_UNKNOWN;
-      }
-      return GOOSEBERRY_SUCCESS;
-    }
     cudaError_t e = cudaGraphLaunch(s->graph[slot], stream);
     if (e == cudaSuccess) e = cudaEventRecord(ev[slot], stream);
     launches += 2 * static_cast<size_t>(s->chunk);

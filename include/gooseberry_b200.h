@@ -217,12 +217,6 @@ typedef enum gb_cg_mode {
  * only when every row fits a tile and the grid can be co-resident; it holds
  * every SM until the solve ends. */
 #define GB_CG_PERSISTENT 0x100
-/* OR-ed into the mode of gb_cg_create (GB_CG_F64 only): launch the two
- * kernels of every iteration directly instead of replaying captured CUDA
- * graphs.  Same kernels, same results; creating the solver is cheaper (no
- * capture or instantiation), which suits one-shot solves such as the drop-in
- * gooseberry_cgd. */
-#define GB_CG_DIRECT 0x200
 
 typedef enum gb_cg_status {
   GB_CG_CONVERGED = 0,  /* ||r|| <= tolerance                                 */

@@ -110,20 +110,3 @@ def test_persistent_and_graph_paths_agree(torch, cg_golden):
         for k, x in out.items():
             assert np.linalg.norm(x - ref) <= 1e-4 * np.linalg.norm(ref), (name, k)
 
-
-def test_direct_launch_equals_graph_replay(torch, cg_golden):
-    """GB_CG_DIRECT launches the same kernels one by one instead of replaying
-    captured graphs: the result is the same bit for bit."""
-    for name in ("laplace64", "diffusion3d12"):
-        c = cg_golden[name]
-        b = torch.from_numpy(c["b"]).cuda()
-        A = gb.CsrMatrix.from_host(rowptr=c["rowptr"], rowind=c["rowind"], rowval=c["rowval"])
-        res = []
-        for direct in (False, True):
-            S = gb.CgSolver(A, direct=direct)
-            x, r = S.solve(b, tol=float(c["error"]), relative=False, niter=int(c["niter"]))
-            res.append((x.cpu().numpy(), r.iterations, r.rnorm))
-            S.close()
-        assert res[0][1] == res[1][1] and res[0][2] == res[1][2], name
-        assert np.array_equal(res[0][0], res[1][0]), name
-        A.close()
