@@ -710,6 +710,50 @@ def serving_extra(nreq=400, seed=5, rtol=1e-10, pool=16 << 30, slots=256, ips=8,
     }
 
 
+def spmm_extra(k=8, flush=None, peak=None, reps=20):
+    """C = A B with k right-hand sides on the 2D 5-point Laplacian 1024^2 (the
+    CG configuration's matrix): the fused kernel (A read once, B transposed
+    row-major) against k separate SpMVs.  Algorithmic bytes: A once, B and C
+    once each: 4(n+1) + 12 nnz + 16 n k."""
+    import torch
+
+    import gooseberry_b200 as gb
+    from gooseberry_b200 import workloads as W
+    L = W.laplacian_2d(1024)
+    n, nnz = L.nrows, L.nnz
+    M = gb.CsrMatrix.from_host(L)
+    M.set_schedule(gb.SCHED_ROW)
+    B = torch.from_numpy(np.random.default_rng(8).uniform(-1, 1, n * k)).cuda()
+    C = M.spmm(B, k)
+    y = torch.empty(n, dtype=torch.float64, device="cuda")
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        ts = []
+        for _ in range(reps):
+            if flush is not None:
+                flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts))
+    t_fused = timed(lambda: M.spmm(B, k, out=C))
+    t_cols = timed(lambda: [M.spmv(B[j * n:(j + 1) * n], y) for j in range(k)])
+    b = 4 * (n + 1) + 12 * nnz + 16 * n * k
+    out = {"k": k, "n": n, "nnz": nnz, "fused_ms": t_fused, "per_column_spmv_ms": t_cols,
+           "speedup": t_cols / t_fused, "GB/s": b / (t_fused * 1e-3) / 1e9,
+           "bytes": b}
+    if peak:
+        out["frac_of_peak"] = out["GB/s"] / peak
+    M.close()
+    return out
+
+
 def pagerank_extra(n=2_000_000, nnz=32_000_000, seed=7, tol=1e-10, cpu_iters=5):
     """PageRank (the reference's pagerank command) on a power-law directed graph
     (n nodes, nnz weighted edges, Zipf-2.1 out-degrees, weights |U[-1,1]| + 0.1),
@@ -760,6 +804,7 @@ def run_extras(args):
     del A
     ex["mixed_cg_3d_160"] = mixed_extra()
     ex["serving_stream"] = serving_extra(nreq=args.requests)
+    ex["spmm_laplace1024_k8"] = spmm_extra(flush=flush, peak=peak)
     ex["pagerank_powerlaw_2m"] = pagerank_extra()
     ex["seconds"] = time.time() - t0
     return ex
@@ -830,6 +875,8 @@ def main():
             out = {"extras": {"mixed_cg_3d_160": mixed_extra()}}
         elif args.workload == "serving":
             out = {"extras": {"serving_stream": serving_extra(nreq=args.requests)}}
+        elif args.workload == "spmm":
+            out = {"extras": {"spmm_laplace1024_k8": spmm_extra(peak=hbm_peak()[0])}}
         elif args.workload == "pagerank":
             out = {"extras": {"pagerank_powerlaw_2m": pagerank_extra()}}
         else:

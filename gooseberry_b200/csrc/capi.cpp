@@ -115,7 +115,11 @@ int spmult_impl(dim_t anrows, dim_t ancols, dim_t bncols, const ind_t * rowptr,
   GB_TRY(gb::dev_alloc(&db.p, std::max<size_t>(bsz, 1) * sizeof(T)));
   GB_TRY(gb::dev_alloc(&dc.p, csz * sizeof(T)));
   if (bsz) GB_CUDA_TRY(cudaMemcpyAsync(db.p, bcolval, bsz * sizeof(T), cudaMemcpyHostToDevice, st));
-  for (dim_t j = 0; j < bncols; ++j) {
+  bool fused = false;
+  GB_TRY(gb::launch_spmm_fused<T>(*g.a, bncols,
+      f64 ? reinterpret_cast<const T *>(g.a->val64) : reinterpret_cast<const T *>(g.a->val32),
+      static_cast<const T *>(db.p), static_cast<T *>(dc.p), st, &fused));
+  for (dim_t j = 0; j < bncols && !fused; ++j) {
     if (f64) {
       GB_TRY(gb::launch_spmv_f64(*g.a, g.a->sched64,
           static_cast<const double *>(db.p) + static_cast<size_t>(j) * ancols,

@@ -150,6 +150,12 @@ int launch_spmv_f64(const gb_csr & a, int sched, const double * x, double * y,
     uint32_t stride, cudaStream_t stream);
 int launch_spmv_f32(const gb_csr & a, int sched, const float * x, float * y,
     uint32_t stride, cudaStream_t stream);
+// C = A B for k >= 2 right-hand sides in one pass over A (spmm.cu); B
+// column-major ncols x k, C row-major nrows x k.  Sets *done = false (and does
+// nothing) when the matrix has rows too long for the fused kernel.
+template <typename T>
+int launch_spmm_fused(const gb_csr & a, uint32_t k, const T * vals, const T * b, T * c,
+    cudaStream_t stream, bool * done);
 // max(rowind) over nnz into *d_out (device), for validation.
 int launch_max_index(const uint32_t * rowind, uint32_t nnz, unsigned int * d_out,
     cudaStream_t stream);

@@ -701,7 +701,12 @@ int gb_spmm_f64(const gb_csr_t * a, dim_t bncols, const double * b, double * c,
   GB_CHECK_INPUT(a != nullptr, "matrix is NULL");
   GB_CHECK_INPUT(a->nrows == 0 || bncols == 0 || c != nullptr, "c is NULL");
   GB_CHECK_INPUT(a->nnz == 0 || bncols == 0 || b != nullptr, "b is NULL");
-  for (dim_t j = 0; j < bncols; ++j)
+  GB_CHECK_INPUT(a->val64 != nullptr, "matrix holds no double values");
+  bool fused = false;
+  GB_TRY(gb::launch_spmm_fused<double>(*a, bncols, a->val64, b, c,
+      static_cast<cudaStream_t>(stream), &fused));
+  if (fused) return GOOSEBERRY_SUCCESS;
+  for (dim_t j = 0; j < bncols; ++j)  // one SpMV per column (long rows, or one column)
     GB_TRY(gb::launch_spmv_f64(*a, a->sched64, b + static_cast<size_t>(j) * a->ncols, c + j,
         bncols, static_cast<cudaStream_t>(stream)));
   return GOOSEBERRY_SUCCESS;

@@ -118,7 +118,8 @@ def test_dropin_spmult_f64_and_f32(spmv_golden):
 def test_dropin_spmm_and_blocks(spmv_golden):
     u = spmv_golden["uniform300"]
     C = gb.spmult(u["rowptr"], u["rowind"], u["rowval"], spmv_golden["spmm3"]["B"], bncols=3)
-    np.testing.assert_allclose(C, spmv_golden["spmm3"]["C"], rtol=1e-13, atol=1e-13)
+    # the fused multi-column kernel sums in the reference's order: bitwise
+    assert np.array_equal(C, spmv_golden["spmm3"]["C"])
     bl = spmv_golden["blocks"]
     out = bl["init"].copy()
     gb.spmult(u["rowptr"], u["rowind"], u["rowval"], u["x"], blocks=bl["blocks_partial"],
@@ -241,3 +242,28 @@ def test_spdot_matches_oracle(torch):
     got32 = gb.spdot(ind, _dev(torch, v32), _dev(torch, x32))
     assert abs(got32 - ref32) <= 1e-13 * scale
     assert gb.spdot(ind[:0], _dev(torch, A.rowval[:0]), _dev(torch, x)) == 0.0
+
+
+@pytest.mark.parametrize("k", [2, 3, 5, 8, 13])
+def test_fused_spmm_bitwise(torch, k):
+    """gb_spmm_f64 reads A once for all k columns; every output is summed
+    k ascending with unfused multiply and add, so C equals the reference
+    order bit for bit (stencil, uniform and short power-law rows).  Rows too
+    long for the fused kernel take the per-column SpMV, within the SpMV bound."""
+    mats = [W.diffusion_2d(90, seed=3), W.uniform_rows(20_000, 10, seed=4),
+            W.powerlaw_rows(30_000, 240_000, seed=5, cap=200)]
+    for A in mats:
+        B = np.random.default_rng(k).uniform(-1, 1, A.ncols * k)
+        ref = oracle.spmm(A.rowptr, A.rowind, A.rowval, B, ncols=A.ncols, bncols=k)
+        M = gb.CsrMatrix.from_host(A)
+        C = M.spmm(_dev(torch, B), k).cpu().numpy()
+        assert np.array_equal(C, ref), (A.nrows, k)
+        M.close()
+    A = W.powerlaw_rows(30_000, 480_000, seed=6, cap=20_000)
+    B = np.random.default_rng(k).uniform(-1, 1, A.ncols * k)
+    ref = oracle.spmm(A.rowptr, A.rowind, A.rowval, B, ncols=A.ncols, bncols=k)
+    M = gb.CsrMatrix.from_host(A)
+    C = M.spmm(_dev(torch, B), k).cpu().numpy()
+    for j in range(k):
+        assert cond_scaled_err(C[j::k], ref[j::k], A.rowptr, A.rowind, A.rowval,
+                               B[j * A.ncols:(j + 1) * A.ncols]) <= TOL64
