@@ -754,6 +754,50 @@ def spmm_extra(k=8, flush=None, peak=None, reps=20):
     return out
 
 
+def loader_extra(n=2_000_000, nnz=32_000_000, seed=9):
+    """CSR text loader: a power-law matrix written in the reference's CSR
+    format (%g values), then read by gooseberry_read_sparse_matrix_f64 (all
+    host threads) and by gb_csr_read (parse + upload to a device matrix),
+    against the reference's own single-threaded reader (src/io.c) on the same
+    file."""
+    import shutil
+    import tempfile
+
+    import gooseberry_b200 as gb
+    import oracle
+    from gooseberry_b200 import workloads as W
+    A = W.powerlaw_rows(n, nnz, seed=seed, cap=200_000)
+    d = tempfile.mkdtemp(prefix="gb_loader_")
+    try:
+        path = os.path.join(d, "a.csr")
+        t0 = time.perf_counter()
+        gb.write_csr(path, A.rowptr, A.rowind, A.rowval, A.ncols)
+        t_write = time.perf_counter() - t0
+        size = os.path.getsize(path)
+        t0 = time.perf_counter()
+        rp, ri, rv, nc = gb.read_csr(path)
+        t_read = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        M = gb.CsrMatrix.read(path)
+        t_dev = time.perf_counter() - t0
+        M.close()
+        out = {"rows": n, "nnz": nnz, "file_bytes": size, "threads": os.cpu_count(),
+               "write_s": t_write, "read_s": t_read, "read_to_device_s": t_dev,
+               "read_GB/s": size / t_read / 1e9}
+        if oracle.ref_available("f64"):
+            t0 = time.perf_counter()
+            rc, rn, rnc, rrp, rri, rrv = oracle.ref_read_csr(path)
+            t_ref = time.perf_counter() - t0
+            out["reference_read_s"] = t_ref
+            out["speedup_vs_reference_read"] = t_ref / t_read
+            out["same_arrays_as_reference"] = bool(
+                rc == 1 and rnc == nc and np.array_equal(rrp, rp) and np.array_equal(rri, ri)
+                and np.array_equal(rrv, rv))
+        return out
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
 def pagerank_extra(n=2_000_000, nnz=32_000_000, seed=7, tol=1e-10, cpu_iters=5):
     """PageRank (the reference's pagerank command) on a power-law directed graph
     (n nodes, nnz weighted edges, Zipf-2.1 out-degrees, weights |U[-1,1]| + 0.1),
@@ -806,6 +850,7 @@ def run_extras(args):
     ex["serving_stream"] = serving_extra(nreq=args.requests)
     ex["spmm_laplace1024_k8"] = spmm_extra(flush=flush, peak=peak)
     ex["pagerank_powerlaw_2m"] = pagerank_extra()
+    ex["csr_loader_2m"] = loader_extra()
     ex["seconds"] = time.time() - t0
     return ex
 
@@ -877,6 +922,8 @@ def main():
             out = {"extras": {"serving_stream": serving_extra(nreq=args.requests)}}
         elif args.workload == "spmm":
             out = {"extras": {"spmm_laplace1024_k8": spmm_extra(peak=hbm_peak()[0])}}
+        elif args.workload == "loader":
+            out = {"extras": {"csr_loader_2m": loader_extra()}}
         elif args.workload == "pagerank":
             out = {"extras": {"pagerank_powerlaw_2m": pagerank_extra()}}
         else:

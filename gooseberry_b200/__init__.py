@@ -30,6 +30,7 @@ import numpy as np
 
 __all__ = [
     "GooseberryError", "lib", "spmult", "scale", "add_scalar", "cgd", "pagerank",
+    "read_csr", "read_grid", "write_csr", "write_grid",
     "CsrMatrix", "CgSolver", "CgResult", "dot", "spdot", "SUCCESS",
     "SCHED_AUTO", "SCHED_THREAD", "SCHED_GROUP4", "SCHED_GROUP8", "SCHED_WARP",
     "SCHED_MERGE", "SCHED_ROW", "SCHED_WTILE", "SCHED_WMERGE", "CG_F64", "CG_MIXED", "plan_tiles",
@@ -91,7 +92,16 @@ SIGNATURES = {
     "gooseberry_cgd_f64": (_i, [_u32, _vp, _vp, _vp, _vp, _vp, _d, _sz, _vp, _vp, _vp, _sz]),
     "gooseberry_pagerank": (_i, [_u32, _vp, _vp, _vp, _f, _f, _sz, _vp, _vp, _vp]),
     "gooseberry_pagerank_f64": (_i, [_u32, _vp, _vp, _vp, _d, _d, _sz, _vp, _vp, _vp]),
+    "gooseberry_read_sparse_matrix": (_i, [_i, C.c_char_p, _vp, _vp, _vp, _vp, _vp]),
+    "gooseberry_read_sparse_matrix_f64": (_i, [_i, C.c_char_p, _vp, _vp, _vp, _vp, _vp]),
+    "gooseberry_read_dense_matrix": (_i, [_i, C.c_char_p, _vp, _vp, _vp]),
+    "gooseberry_read_dense_matrix_f64": (_i, [_i, C.c_char_p, _vp, _vp, _vp]),
+    "gooseberry_write_dense_matrix": (_i, [_i, C.c_char_p, _u32, _u32, _vp]),
+    "gooseberry_write_dense_matrix_f64": (_i, [_i, C.c_char_p, _u32, _u32, _vp]),
+    "gooseberry_write_sparse_matrix": (_i, [_i, C.c_char_p, _u32, _u32, _vp, _vp, _vp]),
+    "gooseberry_write_sparse_matrix_f64": (_i, [_i, C.c_char_p, _u32, _u32, _vp, _vp, _vp]),
     "gb_csr_create": (_i, [_u32, _u32, _u32, _vp, _vp, _vp, _vp, C.c_uint, _vp, _vp]),
+    "gb_csr_read": (_i, [C.c_char_p, C.c_uint, _vp, _vp]),
     "gb_csr_destroy": (_i, [_vp]),
     "gb_csr_get_info": (_i, [_vp, _vp]),
     "gb_csr_set_schedule": (_i, [_vp, C.c_uint, _i, _u32]),
@@ -267,6 +277,74 @@ def pagerank(rowptr, rowind, rowval, damping: float = 0.85, minerror: float = 0.
     return rank, int(it.value), err.value
 
 
+FORMAT_GRID, FORMAT_CSR = 1, 2  # gooseberry_format_t
+_libc = C.CDLL(None)
+_libc.free.argtypes = [C.c_void_p]
+_libc.free.restype = None
+
+
+def _take(ptr, ctype, n, dtype):
+    """Copy n elements out of a malloc'ed C array and free it."""
+    if n:
+        a = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ctype)), (n,)).copy()
+    else:
+        a = np.zeros(0, dtype=dtype)
+    _libc.free(ptr)
+    return a
+
+
+def read_csr(path, f64: bool = True):
+    """Read a CSR text file (``gooseberry_read_sparse_matrix``, the reference's
+    format, src/io.c:369-498).  Returns ``(rowptr, rowind, rowval, ncols)``."""
+    nr, nc = C.c_uint32(0), C.c_uint32(0)
+    rp, ri, rv = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    fn = lib().gooseberry_read_sparse_matrix_f64 if f64 else lib().gooseberry_read_sparse_matrix
+    _check(fn(FORMAT_CSR, str(path).encode(), C.addressof(nr), C.addressof(nc),
+              C.addressof(rp), C.addressof(ri), C.addressof(rv)), "gooseberry_read_sparse_matrix")
+    n = nr.value
+    rowptr = _take(rp, C.c_uint32, n + 1, np.uint32)
+    nnz = int(rowptr[-1])
+    rowind = _take(ri, C.c_uint32, nnz, np.uint32)
+    rowval = _take(rv, C.c_double if f64 else C.c_float, nnz,
+                   np.float64 if f64 else np.float32)
+    return rowptr, rowind, rowval, nc.value
+
+
+def read_grid(path, f64: bool = True):
+    """Read a grid (dense) text file (src/io.c:145-239).  Returns a 2-D array."""
+    nr, nc = C.c_uint32(0), C.c_uint32(0)
+    rv = C.c_void_p()
+    fn = lib().gooseberry_read_dense_matrix_f64 if f64 else lib().gooseberry_read_dense_matrix
+    _check(fn(FORMAT_GRID, str(path).encode(), C.addressof(nr), C.addressof(nc),
+              C.addressof(rv)), "gooseberry_read_dense_matrix")
+    vals = _take(rv, C.c_double if f64 else C.c_float, nr.value * nc.value,
+                 np.float64 if f64 else np.float32)
+    return vals.reshape(nr.value, nc.value)
+
+
+def write_grid(path, values):
+    """Write a 2-D array as a grid text file (src/io.c:1195-1229)."""
+    v = np.ascontiguousarray(values)
+    if v.ndim == 1:
+        v = v.reshape(-1, 1)
+    f64 = _real(v.dtype) == "f64"
+    fn = lib().gooseberry_write_dense_matrix_f64 if f64 else lib().gooseberry_write_dense_matrix
+    _check(fn(FORMAT_GRID, str(path).encode(), v.shape[0], v.shape[1], _ptr(v)),
+           "gooseberry_write_dense_matrix")
+
+
+def write_csr(path, rowptr, rowind, rowval, ncols: int = 0):
+    """Write a CSR text file (src/io.c:1233-1275)."""
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+    rowind = np.ascontiguousarray(rowind, dtype=np.uint32)
+    rowval = np.ascontiguousarray(rowval)
+    f64 = _real(rowval.dtype) == "f64"
+    fn = (lib().gooseberry_write_sparse_matrix_f64 if f64
+          else lib().gooseberry_write_sparse_matrix)
+    _check(fn(FORMAT_CSR, str(path).encode(), len(rowptr) - 1, ncols, _ptr(rowptr),
+              _ptr(rowind), _ptr(rowval)), "gooseberry_write_sparse_matrix")
+
+
 def plan_tiles(rowptr, tile_items: int = 2048):
     """Run the SpMV tile planner on a host rowptr (no GPU).  Returns
     ``(tiles[ntiles, 4], nlong, info)``; see ``gb_plan_tiles_host``."""
@@ -319,6 +397,18 @@ class CsrMatrix:
         self._h = C.c_void_p(handle)
         self.nrows, self.ncols, self.nnz = nrows, ncols, nnz
         self._keep = keep  # borrowed device tensors must outlive the handle
+
+    @classmethod
+    def read(cls, path, f64: bool = True, f32: bool = False, stream=None) -> "CsrMatrix":
+        """Read a CSR text file straight into a device matrix (``gb_csr_read``)."""
+        h = C.c_void_p()
+        flags = (VALUES_F64 if f64 else 0) | (VALUES_F32 if f32 else 0)
+        _check(lib().gb_csr_read(str(path).encode(), flags, _stream_ptr(stream),
+                                 C.addressof(h)), "gb_csr_read")
+        info = CsrInfo()
+        _check(lib().gb_csr_get_info(h, C.addressof(info)), "gb_csr_get_info")
+        m = cls(h.value, info.nrows, info.ncols, info.nnz)
+        return m
 
     @classmethod
     def from_host(cls, csr=None, *, rowptr=None, rowind=None, rowval=None, ncols=None,

@@ -1,0 +1,512 @@
+// io.cpp -- CSR and grid text files: the reference's readers and writers
+// (src/io.c:145-239 __read_grid, 369-498 __read_csr, 1195-1229 __write_grid,
+// 1233-1275 __write_csr) with the same format rules, parsed by all host
+// threads, plus gb_csr_read, which parses straight into a device matrix.
+//
+// Format rules kept from the reference:
+//  - lines end at '\n'; the newline that ends the file opens no extra line;
+//  - a line whose first character is one of  # % ' " /  is a comment;
+//  - CSR: every other line is a row of "column value" pairs read with
+//    strtoull / strtod until a value fails to parse; a blank line is an empty
+//    row; columns are 1-based unless a 0 appears (the smallest column seen,
+//    capped at 1, is subtracted); ncols = largest - smallest + 1;
+//  - grid: every non-comment line is a row of values; the first line fixes the
+//    column count (a leading blank line leaves it open), a later line with no
+//    values or a different count is an error;
+//  - writers print values with %g and CSR columns 1-based, one row per line.
+//
+// The file is read into memory once; newlines become terminators so strtod
+// never runs into the next line, lines are found by parallel chunk scans, and
+// rows are parsed by contiguous line ranges per thread and concatenated in
+// order, so the arrays are exactly the sequential reader's.
+#include <algorithm>
+#include <cerrno>
+#include <charconv>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include <sys/stat.h>
+#include <thread>
+#include <vector>
+
+#include "gb_internal.h"
+
+namespace gb {
+namespace {
+
+bool is_comment(char c) {
+  return c == '#' || c == '%' || c == '\'' || c == '"' || c == '/';
+}
+
+unsigned n_threads() {
+  return std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+}
+
+template <class F>
+void parallel_for(unsigned nt, F && body) {
+  std::vector<std::thread> th;
+  for (unsigned t = 1; t < nt; ++t) th.emplace_back(body, t);
+  body(0u);
+  for (auto & x : th) x.join();
+}
+
+int open_error(const char * path, const char * mode) {
+  if (errno == ENOENT || errno == ENOTDIR) {
+    set_error("file not found '%s'", path);
+    return GOOSEBERRY_ERROR_FILENOTFOUND;
+  }
+  if (errno == EACCES) {
+    set_error("permission denied '%s'", path);
+    return GOOSEBERRY_ERROR_PERMISSIONDENIED;
+  }
+  set_error("cannot open '%s' (%s) for %s", path, std::strerror(errno),
+      mode[0] == 'r' ? "reading" : "writing");
+  return GOOSEBERRY_ERROR_UNKNOWN;
+}
+
+// The whole file, newlines replaced by '\0', and the start of every line.
+struct Lines {
+  std::unique_ptr<char[]> buf;  // not zero-filled: every byte is read from the file
+  std::vector<size_t> start;    // line i spans buf[start[i]] .. its '\0'
+};
+
+int read_lines(const char * path, Lines & L) {
+  GB_CHECK_INPUT(path != nullptr, "file name is NULL");
+  FILE * f = std::fopen(path, "rb");
+  if (!f) return open_error(path, "r");
+  struct stat st;
+  size_t cap = (fstat(fileno(f), &st) == 0 && st.st_size > 0)
+                   ? static_cast<size_t>(st.st_size) : (1u << 20);
+  L.buf.reset(new char[cap + 1]);
+  size_t got = 0;
+  for (;;) {  // the size is a hint: read to the end whatever it is
+    got += std::fread(L.buf.get() + got, 1, cap - got, f);
+    if (got < cap || std::feof(f)) break;
+    int c = std::fgetc(f);
+    if (c == EOF) break;
+    std::unique_ptr<char[]> bigger(new char[2 * cap + 1]);
+    std::memcpy(bigger.get(), L.buf.get(), got);
+    bigger[got++] = static_cast<char>(c);
+    L.buf = std::move(bigger);
+    cap *= 2;
+  }
+  const bool bad = std::ferror(f) != 0;
+  std::fclose(f);
+  if (bad) {
+    set_error("read error on '%s'", path);
+    return GOOSEBERRY_ERROR_READ;
+  }
+  const size_t n = got;
+  char * buf = L.buf.get();
+  buf[n] = '\0';
+  // newline positions, chunk-parallel, in order
+  const unsigned nt = n_threads();
+  std::vector<std::vector<size_t>> nl(nt);
+  parallel_for(nt, [&](unsigned t) {
+    const size_t a = n * t / nt, b = n * (t + 1) / nt;
+    for (size_t i = a; i < b; ++i)
+      if (buf[i] == '\n') nl[t].push_back(i);
+  });
+  size_t total = 0;
+  for (auto & v : nl) total += v.size();
+  const bool tail = n > 0 && buf[n - 1] != '\n';  // last line without a newline
+  L.start.resize(total + (tail ? 1 : 0));
+  size_t k = 0, prev = 0;
+  for (auto & v : nl)
+    for (size_t pos : v) {
+      L.start[k++] = prev;
+      buf[pos] = '\0';
+      prev = pos + 1;
+    }
+  if (tail) L.start[k] = prev;
+  return GOOSEBERRY_SUCCESS;
+}
+
+template <typename T>
+struct CsrPart {
+  std::vector<uint32_t> count;  // entries per row, in line order
+  std::vector<uint32_t> ind;
+  std::vector<T> val;
+  uint32_t mincol = 1, maxcol = 0;
+};
+
+bool is_space(char c) {
+  return c == ' ' || c == '\t' || c == '\r' || c == '\n' || c == '\v' || c == '\f';
+}
+
+// strtoull(s, &end, 10) with a fast path for [spaces] digits (no sign, no
+// overflow); anything else goes to strtoull itself.
+unsigned long long parse_ull(const char * s, char ** end) {
+  const char * q = s;
+  while (is_space(*q)) ++q;
+  const char * d = q;
+  unsigned long long v = 0;
+  int nd = 0;
+  while (*q >= '0' && *q <= '9' && nd < 19) {
+    v = v * 10 + static_cast<unsigned>(*q - '0');
+    ++q;
+    ++nd;
+  }
+  if (nd == 0 || (*q >= '0' && *q <= '9')) return std::strtoull(s, end, 10);
+  (void)d;
+  *end = const_cast<char *>(q);
+  return v;
+}
+
+// strtod(s, &end) with a fast path: a plain decimal token ([+-] digits, '.',
+// exponent) is converted by std::from_chars, which rounds correctly like
+// strtod; hex, inf, nan and anything odd go to strtod itself.
+double parse_double(const char * s, char ** end) {
+  const char * q = s;
+  while (is_space(*q)) ++q;
+  const char * t = q;
+  bool neg = false;
+  if (*t == '+' || *t == '-') {
+    neg = *t == '-';
+    ++t;
+  }
+  if (!((*t >= '0' && *t <= '9') || (*t == '.' && t[1] >= '0' && t[1] <= '9')) ||
+      (t[0] == '0' && (t[1] == 'x' || t[1] == 'X')))
+    return std::strtod(s, end);
+  const char * e = t;
+  while (*e && !is_space(*e)) ++e;
+  double v = 0.0;
+  const auto r = std::from_chars(t, e, v, std::chars_format::general);
+  if (r.ec != std::errc() || r.ptr != e) return std::strtod(s, end);
+  *end = const_cast<char *>(e);
+  return neg ? -v : v;
+}
+
+// One CSR row: "col val" pairs until a value does not parse (src/io.c:417-437).
+template <typename T>
+void parse_csr_row(const char * line, CsrPart<T> & p) {
+  const char * sptr = line;
+  char * eptr = nullptr;
+  uint32_t n = 0;
+  uint32_t i = static_cast<uint32_t>(parse_ull(sptr, &eptr));
+  sptr = eptr;
+  double f = parse_double(sptr, &eptr);
+  while (eptr != sptr) {
+    p.maxcol = std::max(p.maxcol, i);
+    p.mincol = std::min(p.mincol, i);
+    p.ind.push_back(i);
+    p.val.push_back(static_cast<T>(f));
+    ++n;
+    sptr = eptr;
+    i = static_cast<uint32_t>(parse_ull(sptr, &eptr));
+    sptr = eptr;
+    f = parse_double(sptr, &eptr);
+  }
+  p.count.push_back(n);
+}
+
+template <typename T>
+T * malloc_n(size_t n) {
+  return static_cast<T *>(std::malloc(sizeof(T) * (n ? n : 1)));
+}
+
+// Parses a CSR file into caller-owned arrays made by `alloc`.
+template <typename T, class Alloc>
+int read_csr(const char * path, dim_t * nrows, dim_t * ncols, ind_t ** r_rowptr,
+    dim_t ** r_rowind, T ** r_rowval, Alloc && alloc) {
+  GB_CHECK_INPUT(nrows && ncols && r_rowptr && r_rowind && r_rowval, "NULL output");
+  Lines L;
+  GB_TRY(read_lines(path, L));
+  const size_t nl = L.start.size();
+  const unsigned nt = static_cast<unsigned>(std::min<size_t>(n_threads(),
+      std::max<size_t>(nl / 1024, 1)));
+  std::vector<CsrPart<T>> part(nt);
+  parallel_for(nt, [&](unsigned t) {
+    const size_t a = nl * t / nt, b = nl * (t + 1) / nt;
+    CsrPart<T> & p = part[t];
+    for (size_t l = a; l < b; ++l) {
+      const char * line = L.buf.get() + L.start[l];
+      if (line[0] != '\0' && is_comment(line[0])) continue;  // blank lines are empty rows
+      parse_csr_row(line, p);
+    }
+  });
+  size_t n = 0, nnz = 0;
+  uint32_t mincol = 1, maxcol = 0;
+  for (auto & p : part) {
+    n += p.count.size();
+    nnz += p.ind.size();
+    mincol = std::min(mincol, p.mincol);
+    maxcol = std::max(maxcol, p.maxcol);
+  }
+  GB_CHECK_INPUT(n < 0xffffffffu && nnz <= 0xffffffffu,
+      "'%s' holds %zu rows / %zu entries, beyond 32-bit indices", path, n, nnz);
+  ind_t * rowptr = nullptr;
+  dim_t * rowind = nullptr;
+  T * rowval = nullptr;
+  if (!alloc(&rowptr, n + 1) || !alloc(&rowind, nnz) || !alloc(&rowval, nnz)) {
+    set_error("out of host memory reading '%s'", path);
+    return GOOSEBERRY_ERROR_UNKNOWN;
+  }
+  std::vector<size_t> row0(nt + 1, 0), ent0(nt + 1, 0);
+  for (unsigned t = 0; t < nt; ++t) {
+    row0[t + 1] = row0[t] + part[t].count.size();
+    ent0[t + 1] = ent0[t] + part[t].ind.size();
+  }
+  rowptr[0] = 0;
+  parallel_for(nt, [&](unsigned t) {
+    const CsrPart<T> & p = part[t];
+    size_t j = ent0[t];
+    for (size_t r = 0; r < p.count.size(); ++r) {
+      j += p.count[r];
+      rowptr[row0[t] + r + 1] = static_cast<ind_t>(j);
+    }
+    for (size_t e = 0; e < p.ind.size(); ++e) {
+      rowind[ent0[t] + e] = p.ind[e] - mincol;  // mincol is at most 1
+      rowval[ent0[t] + e] = p.val[e];
+    }
+  });
+  *r_rowptr = rowptr;
+  *r_rowind = rowind;
+  *r_rowval = rowval;
+  *nrows = static_cast<dim_t>(n);
+  *ncols = maxcol - mincol + 1;
+  return GOOSEBERRY_SUCCESS;
+}
+
+template <typename T>
+int read_grid(const char * path, dim_t * r_nrows, dim_t * r_ncols, T ** r_rowval) {
+  GB_CHECK_INPUT(r_nrows && r_ncols && r_rowval, "NULL output");
+  Lines L;
+  GB_TRY(read_lines(path, L));
+  const size_t nl = L.start.size();
+  // values per line (comments: ~0)
+  const size_t kComment = ~size_t(0);
+  std::vector<size_t> cnt(nl);
+  const unsigned nt = static_cast<unsigned>(std::min<size_t>(n_threads(),
+      std::max<size_t>(nl / 256, 1)));
+  parallel_for(nt, [&](unsigned t) {
+    for (size_t l = nl * t / nt; l < nl * (t + 1) / nt; ++l) {
+      const char * line = L.buf.get() + L.start[l];
+      if (is_comment(line[0])) {
+        cnt[l] = kComment;
+        continue;
+      }
+      size_t j = 0;
+      const char * sptr = line;
+      char * eptr = nullptr;
+      parse_double(sptr, &eptr);
+      while (eptr != sptr) {
+        ++j;
+        sptr = eptr;
+        parse_double(sptr, &eptr);
+      }
+      cnt[l] = j;
+    }
+  });
+  // the column-count rule of src/io.c:171-199, in line order
+  size_t nrows = 0, ncols = 0;
+  std::vector<size_t> off(nl, 0);
+  size_t k = 0;
+  for (size_t l = 0; l < nl; ++l) {
+    if (cnt[l] == kComment) continue;
+    const size_t j = cnt[l];
+    if (ncols == 0) {
+      ncols = j;
+    } else if (j == 0) {
+      set_error("invalid line in grid matrix file: %zu", nrows + 1);
+      return GOOSEBERRY_ERROR_INVALIDINPUT;
+    } else if (j != ncols) {
+      set_error("different number of columns (%zu) for line %zu when previous had %zu columns",
+          j, nrows, ncols);
+      return GOOSEBERRY_ERROR_INVALIDINPUT;
+    }
+    off[l] = k;
+    k += j;
+    ++nrows;
+  }
+  GB_CHECK_INPUT(nrows < 0xffffffffu && ncols < 0xffffffffu, "grid too large for 32-bit sizes");
+  T * rowval = static_cast<T *>(std::calloc(nrows * ncols ? nrows * ncols : 1, sizeof(T)));
+  if (!rowval) {
+    set_error("out of host memory reading '%s'", path);
+    return GOOSEBERRY_ERROR_UNKNOWN;
+  }
+  parallel_for(nt, [&](unsigned t) {
+    for (size_t l = nl * t / nt; l < nl * (t + 1) / nt; ++l) {
+      if (cnt[l] == kComment || cnt[l] == 0) continue;
+      const char * sptr = L.buf.get() + L.start[l];
+      char * eptr = nullptr;
+      size_t q = off[l];
+      double f = parse_double(sptr, &eptr);
+      while (eptr != sptr) {
+        rowval[q++] = static_cast<T>(f);
+        sptr = eptr;
+        f = parse_double(sptr, &eptr);
+      }
+    }
+  });
+  *r_rowval = rowval;
+  *r_nrows = static_cast<dim_t>(nrows);
+  *r_ncols = static_cast<dim_t>(ncols);
+  return GOOSEBERRY_SUCCESS;
+}
+
+// Rows formatted by all threads into per-thread strings, written in order.
+template <class Fmt>
+int write_rows(const char * path, size_t nrows, Fmt && fmt) {
+  GB_CHECK_INPUT(path != nullptr, "file name is NULL");
+  FILE * f = std::fopen(path, "wb");
+  if (!f) return open_error(path, "w");
+  const unsigned nt = static_cast<unsigned>(std::min<size_t>(n_threads(),
+      std::max<size_t>(nrows / 1024, 1)));
+  std::vector<std::string> out(nt);
+  parallel_for(nt, [&](unsigned t) {
+    char tmp[64];
+    for (size_t i = nrows * t / nt; i < nrows * (t + 1) / nt; ++i) fmt(i, out[t], tmp);
+  });
+  bool ok = true;
+  for (auto & s : out) ok = ok && std::fwrite(s.data(), 1, s.size(), f) == s.size();
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) {
+    set_error("write error on '%s'", path);
+    return GOOSEBERRY_ERROR_WRITE;
+  }
+  return GOOSEBERRY_SUCCESS;
+}
+
+template <typename T>
+int write_grid(const char * path, dim_t nrows, dim_t ncols, const T * rowval) {
+  GB_CHECK_INPUT(nrows == 0 || ncols == 0 || rowval, "NULL values");
+  return write_rows(path, nrows, [&](size_t i, std::string & s, char * tmp) {
+    for (dim_t j = 0; j < ncols; ++j) {
+      const int m = std::snprintf(tmp, 64, j ? " %g" : "%g",
+          static_cast<double>(rowval[i * ncols + j]));
+      s.append(tmp, m);
+    }
+    s.push_back('\n');
+  });
+}
+
+template <typename T>
+int write_csr(const char * path, dim_t nrows, const ind_t * rowptr, const dim_t * rowind,
+    const T * rowval) {
+  GB_CHECK_INPUT(nrows == 0 || rowptr, "NULL rowptr");
+  GB_CHECK_INPUT(nrows == 0 || rowptr[nrows] == 0 || (rowind && rowval), "NULL arrays");
+  return write_rows(path, nrows, [&](size_t i, std::string & s, char * tmp) {
+    for (ind_t k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+      const int m = std::snprintf(tmp, 64, k == rowptr[i] ? "%u %g" : " %u %g",
+          rowind[k] + 1, static_cast<double>(rowval[k]));
+      s.append(tmp, m);
+    }
+    s.push_back('\n');
+  });
+}
+
+// The formats the reference reads and writes (src/io.c:1467-1545): CSR and
+// GRID here; the others are recognised and reported as unimplemented.
+int other_format(int type, bool sparse) {
+  if (type == GOOSEBERRY_FORMAT_RAW || type == GOOSEBERRY_FORMAT_POINT ||
+      type == GOOSEBERRY_FORMAT_SVM || type == GOOSEBERRY_FORMAT_GRAPH ||
+      type == GOOSEBERRY_FORMAT_CLU || type == GOOSEBERRY_FORMAT_MATRIXMARKET ||
+      type == (sparse ? GOOSEBERRY_FORMAT_GRID : GOOSEBERRY_FORMAT_CSR)) {
+    set_error("%s matrix format %d is not implemented here (CSR and GRID are)",
+        sparse ? "sparse" : "dense", type);
+    return GOOSEBERRY_ERROR_UNIMPLEMENTED;
+  }
+  set_error("unrecognized %s matrix format '%d'", sparse ? "sparse" : "dense", type);
+  return GOOSEBERRY_ERROR_INVALIDINPUT;
+}
+
+template <typename T>
+int read_sparse(int type, const char * file, dim_t * nrows, dim_t * ncols, ind_t ** rowptr,
+    dim_t ** rowind, T ** rowval) {
+  if (type != GOOSEBERRY_FORMAT_CSR) return other_format(type, true);
+  return read_csr<T>(file, nrows, ncols, rowptr, rowind, rowval, [](auto ** p, size_t n) {
+    *p = malloc_n<std::remove_pointer_t<std::remove_pointer_t<decltype(p)>>>(n);
+    return *p != nullptr;
+  });
+}
+
+}  // namespace
+}  // namespace gb
+
+extern "C" {
+
+int gooseberry_read_sparse_matrix(int type, const char * file, dim_t * nrows, dim_t * ncols,
+    ind_t ** rowptr, dim_t ** rowind, float ** rowval) {
+  return gb::read_sparse<float>(type, file, nrows, ncols, rowptr, rowind, rowval);
+}
+
+int gooseberry_read_sparse_matrix_f64(int type, const char * file, dim_t * nrows,
+    dim_t * ncols, ind_t ** rowptr, dim_t ** rowind, double ** rowval) {
+  return gb::read_sparse<double>(type, file, nrows, ncols, rowptr, rowind, rowval);
+}
+
+int gooseberry_read_dense_matrix(int type, const char * file, dim_t * nrows, dim_t * ncols,
+    float ** rowval) {
+  if (type != GOOSEBERRY_FORMAT_GRID) return gb::other_format(type, false);
+  return gb::read_grid<float>(file, nrows, ncols, rowval);
+}
+
+int gooseberry_read_dense_matrix_f64(int type, const char * file, dim_t * nrows,
+    dim_t * ncols, double ** rowval) {
+  if (type != GOOSEBERRY_FORMAT_GRID) return gb::other_format(type, false);
+  return gb::read_grid<double>(file, nrows, ncols, rowval);
+}
+
+int gooseberry_write_dense_matrix(int type, const char * file, dim_t nrows, dim_t ncols,
+    const float * rowval) {
+  if (type != GOOSEBERRY_FORMAT_GRID) return gb::other_format(type, false);
+  return gb::write_grid<float>(file, nrows, ncols, rowval);
+}
+
+int gooseberry_write_dense_matrix_f64(int type, const char * file, dim_t nrows, dim_t ncols,
+    const double * rowval) {
+  if (type != GOOSEBERRY_FORMAT_GRID) return gb::other_format(type, false);
+  return gb::write_grid<double>(file, nrows, ncols, rowval);
+}
+
+int gooseberry_write_sparse_matrix(int type, const char * file, dim_t nrows, dim_t ncols,
+    const ind_t * rowptr, const dim_t * rowind, const float * rowval) {
+  (void)ncols;
+  if (type != GOOSEBERRY_FORMAT_CSR) return gb::other_format(type, true);
+  return gb::write_csr<float>(file, nrows, rowptr, rowind, rowval);
+}
+
+int gooseberry_write_sparse_matrix_f64(int type, const char * file, dim_t nrows, dim_t ncols,
+    const ind_t * rowptr, const dim_t * rowind, const double * rowval) {
+  (void)ncols;
+  if (type != GOOSEBERRY_FORMAT_CSR) return gb::other_format(type, true);
+  return gb::write_csr<double>(file, nrows, rowptr, rowind, rowval);
+}
+
+// Parse a CSR file into host memory and upload it as a device matrix.
+int gb_csr_read(const char * file, unsigned flags, gb_stream_t stream, gb_csr_t ** out) {
+  GB_CHECK_INPUT(out != nullptr, "out is NULL");
+  *out = nullptr;
+  const bool want64 = (flags & GB_CSR_VALUES_F64) != 0;
+  const bool want32 = (flags & GB_CSR_VALUES_F32) != 0;
+  GB_CHECK_INPUT(want64 || want32, "flags must ask for GB_CSR_VALUES_F64 and/or _F32");
+  GB_CHECK_INPUT((flags & GB_CSR_DEVICE_POINTERS) == 0,
+      "gb_csr_read uploads its own copy; GB_CSR_DEVICE_POINTERS does not apply");
+  std::vector<void *> held;
+  auto alloc = [&](auto ** p, size_t n) {
+    using E = std::remove_pointer_t<std::remove_pointer_t<decltype(p)>>;
+    void * q = std::malloc(sizeof(E) * (n ? n : 1));
+    if (!q) return false;
+    held.push_back(q);
+    *p = static_cast<E *>(q);
+    return true;
+  };
+  dim_t nrows = 0, ncols = 0;
+  ind_t * rowptr = nullptr;
+  dim_t * rowind = nullptr;
+  double * rowval = nullptr;
+  int rc = gb::read_csr<double>(file, &nrows, &ncols, &rowptr, &rowind, &rowval, alloc);
+  if (rc == GOOSEBERRY_SUCCESS)
+    rc = gb_csr_create(nrows, ncols, rowptr[nrows], rowptr, rowind, rowval, nullptr,
+        (want64 ? GB_CSR_VALUES_F64 : 0u) | (want32 ? GB_CSR_VALUES_F32 : 0u), stream, out);
+  if (rc == GOOSEBERRY_SUCCESS) cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+  for (void * q : held) std::free(q);
+  return rc;
+}
+
+}  // extern "C"

@@ -70,6 +70,20 @@ typedef enum gooseberry_error_t {
   GOOSEBERRY_ERROR_UNKNOWN
 } gooseberry_error_t;
 
+/* File formats, numbered as the reference (include/gooseberry.h:97-106).
+ * CSR and GRID are read and written here; the others are reported as
+ * GOOSEBERRY_ERROR_UNIMPLEMENTED. */
+typedef enum gooseberry_format_t {
+  GOOSEBERRY_FORMAT_RAW,
+  GOOSEBERRY_FORMAT_GRID,
+  GOOSEBERRY_FORMAT_CSR,
+  GOOSEBERRY_FORMAT_POINT,
+  GOOSEBERRY_FORMAT_SVM,
+  GOOSEBERRY_FORMAT_GRAPH,
+  GOOSEBERRY_FORMAT_CLU,
+  GOOSEBERRY_FORMAT_MATRIXMARKET
+} gooseberry_format_t;
+
 /* Symbols exported by the shared library (hidden visibility otherwise). */
 #if defined(__GNUC__)
 #define GOOSEBERRY_API __attribute__((visibility("default")))
@@ -87,6 +101,10 @@ extern "C" {
 #define gooseberry_spmult gooseberry_spmult_f64
 #define gooseberry_cgd gooseberry_cgd_f64
 #define gooseberry_pagerank gooseberry_pagerank_f64
+#define gooseberry_read_sparse_matrix gooseberry_read_sparse_matrix_f64
+#define gooseberry_read_dense_matrix gooseberry_read_dense_matrix_f64
+#define gooseberry_write_sparse_matrix gooseberry_write_sparse_matrix_f64
+#define gooseberry_write_dense_matrix gooseberry_write_dense_matrix_f64
 #endif
 
 /*
@@ -169,6 +187,35 @@ GOOSEBERRY_API int gooseberry_pagerank(dim_t n, const ind_t * rowptr, const dim_
 GOOSEBERRY_API int gooseberry_pagerank_f64(dim_t n, const ind_t * rowptr,
     const dim_t * rowind, const double * rowval, double damping, double minerror,
     size_t niter, double * rank, size_t * iterations, double * error);
+
+/*
+ * Text files (reference include/gooseberry.h:389-421, src/io.c:1467-1545),
+ * parsed by all host threads with the reference's rules: CSR rows of
+ * "column value" pairs (1-based columns unless a 0 appears; ncols = largest -
+ * smallest column + 1; blank lines are empty rows; lines starting with
+ * # % ' " / are comments) and GRID rows of values.  Output arrays are
+ * malloc'ed; the caller frees them with free().  Writers print values with
+ * %g, CSR columns 1-based.  Errors: GOOSEBERRY_ERROR_FILENOTFOUND /
+ * _PERMISSIONDENIED / _READ / _WRITE, _INVALIDINPUT for a ragged grid or an
+ * unknown format, _UNIMPLEMENTED for the formats other than CSR and GRID.
+ */
+GOOSEBERRY_API int gooseberry_read_sparse_matrix(int type, const char * file, dim_t * nrows,
+    dim_t * ncols, ind_t ** rowptr, dim_t ** rowind, real_t ** rowval);
+GOOSEBERRY_API int gooseberry_read_sparse_matrix_f64(int type, const char * file,
+    dim_t * nrows, dim_t * ncols, ind_t ** rowptr, dim_t ** rowind, double ** rowval);
+GOOSEBERRY_API int gooseberry_read_dense_matrix(int type, const char * file, dim_t * nrows,
+    dim_t * ncols, real_t ** rowval);
+GOOSEBERRY_API int gooseberry_read_dense_matrix_f64(int type, const char * file,
+    dim_t * nrows, dim_t * ncols, double ** rowval);
+GOOSEBERRY_API int gooseberry_write_dense_matrix(int type, const char * file, dim_t nrows,
+    dim_t ncols, const real_t * rowval);
+GOOSEBERRY_API int gooseberry_write_dense_matrix_f64(int type, const char * file,
+    dim_t nrows, dim_t ncols, const double * rowval);
+GOOSEBERRY_API int gooseberry_write_sparse_matrix(int type, const char * file, dim_t nrows,
+    dim_t ncols, const ind_t * rowptr, const dim_t * rowind, const real_t * rowval);
+GOOSEBERRY_API int gooseberry_write_sparse_matrix_f64(int type, const char * file,
+    dim_t nrows, dim_t ncols, const ind_t * rowptr, const dim_t * rowind,
+    const double * rowval);
 
 #ifdef __cplusplus
 }

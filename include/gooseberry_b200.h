@@ -104,6 +104,13 @@ GOOSEBERRY_API int gb_csr_create(dim_t nrows, dim_t ncols, ind_t nnz, const ind_
     const dim_t * rowind, const double * rowval64, const float * rowval32,
     unsigned flags, gb_stream_t stream, gb_csr_t ** out);
 
+/* Read a CSR text file (the format of gooseberry_read_sparse_matrix with
+ * GOOSEBERRY_FORMAT_CSR, reference src/io.c:369-498) with all host threads
+ * into host memory and create a device matrix from it (flags: the
+ * value widths to keep, GB_CSR_VALUES_F64 and/or _F32).  Synchronous. */
+GOOSEBERRY_API int gb_csr_read(const char * file, unsigned flags, gb_stream_t stream,
+    gb_csr_t ** out);
+
 /* Release a matrix (matrix_free, reference src/matrix.c:483-535). */
 GOOSEBERRY_API int gb_csr_destroy(gb_csr_t * a);
 

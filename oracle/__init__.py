@@ -101,6 +101,18 @@ def _ref(real: str = "f64"):
         lib.gbref_pagerank.argtypes = [C.c_uint32, _u32p, _u32p, p, C.c_double, C.c_double,
                                        C.c_size_t, p, C.POINTER(C.c_double)]
         lib.gbref_pagerank.restype = C.c_size_t
+        vp = C.c_void_p
+        lib.gbref_read_sparse.argtypes = [C.c_int, C.c_char_p, vp, vp, vp, vp, vp]
+        lib.gbref_read_sparse.restype = C.c_int
+        lib.gbref_read_dense.argtypes = [C.c_int, C.c_char_p, vp, vp, vp]
+        lib.gbref_read_dense.restype = C.c_int
+        lib.gbref_write_sparse.argtypes = [C.c_int, C.c_char_p, C.c_uint32, C.c_uint32,
+                                           _u32p, _u32p, p]
+        lib.gbref_write_sparse.restype = C.c_int
+        lib.gbref_write_dense.argtypes = [C.c_int, C.c_char_p, C.c_uint32, C.c_uint32, p]
+        lib.gbref_write_dense.restype = C.c_int
+        lib.gbref_free.argtypes = [vp]
+        lib.gbref_free.restype = None
         lib.gbref_cgd.argtypes = [C.c_uint32, _u32p, _u32p, p, p, p, C.c_double,
                                   C.c_size_t, C.POINTER(C.c_size_t),
                                   C.POINTER(C.c_double), C.c_void_p, C.c_size_t]
@@ -253,6 +265,64 @@ def ref_pagerank(rowptr, rowind, rowval, damping=0.85, minerror=0.0, niter=0, re
     it = _ref(real).gbref_pagerank(n, rowptr, rowind, rowval, damping, minerror, niter, out,
                                    C.byref(err))
     return out, int(it), err.value
+
+
+FORMAT_GRID, FORMAT_CSR = 1, 2  # gooseberry_format_t (include/gooseberry.h:97-106)
+
+
+def ref_read_csr(path, real="f64"):
+    """The reference's CSR reader (src/io.c:369-498).  Returns
+    (rc, nrows, ncols, rowptr, rowind, rowval) -- arrays copied out."""
+    L = _ref(real)
+    nr, nc = C.c_uint32(0), C.c_uint32(0)
+    rp, ri, rv = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    rc = L.gbref_read_sparse(FORMAT_CSR, str(path).encode(), C.addressof(nr), C.addressof(nc),
+                             C.addressof(rp), C.addressof(ri), C.addressof(rv))
+    if rc != 1:
+        return rc, 0, 0, None, None, None
+    n = nr.value
+    nnz = C.cast(rp, C.POINTER(C.c_uint32))[n] if rp.value else 0
+    rowptr = np.ctypeslib.as_array(C.cast(rp, C.POINTER(C.c_uint32)), (n + 1,)).copy()
+    rowind = (np.ctypeslib.as_array(C.cast(ri, C.POINTER(C.c_uint32)), (nnz,)).copy()
+              if nnz else np.zeros(0, np.uint32))
+    ct = C.c_double if real == "f64" else C.c_float
+    rowval = (np.ctypeslib.as_array(C.cast(rv, C.POINTER(ct)), (nnz,)).copy()
+              if nnz else np.zeros(0, _dt(real)))
+    for q in (rp, ri, rv):
+        L.gbref_free(q)
+    return rc, n, nc.value, rowptr, rowind, rowval
+
+
+def ref_read_grid(path, real="f64"):
+    """The reference's grid reader (src/io.c:145-239): (rc, nrows, ncols, values)."""
+    L = _ref(real)
+    nr, nc = C.c_uint32(0), C.c_uint32(0)
+    rv = C.c_void_p()
+    rc = L.gbref_read_dense(FORMAT_GRID, str(path).encode(), C.addressof(nr), C.addressof(nc),
+                            C.addressof(rv))
+    if rc != 1:
+        return rc, 0, 0, None
+    m = nr.value * nc.value
+    ct = C.c_double if real == "f64" else C.c_float
+    vals = (np.ctypeslib.as_array(C.cast(rv, C.POINTER(ct)), (m,)).copy()
+            if m else np.zeros(0, _dt(real)))
+    L.gbref_free(rv)
+    return rc, nr.value, nc.value, vals
+
+
+def ref_write_grid(path, vals, nrows, ncols, real="f64"):
+    """The reference's grid writer (src/io.c:1195-1229)."""
+    v = np.ascontiguousarray(vals, dtype=_dt(real))
+    return _ref(real).gbref_write_dense(FORMAT_GRID, str(path).encode(), nrows, ncols, v)
+
+
+def ref_write_csr(path, rowptr, rowind, rowval, ncols, real="f64"):
+    """The reference's CSR writer (src/io.c:1233-1275)."""
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+    rowind = np.ascontiguousarray(rowind, dtype=np.uint32)
+    rowval = np.ascontiguousarray(rowval, dtype=_dt(real))
+    return _ref(real).gbref_write_sparse(FORMAT_CSR, str(path).encode(), len(rowptr) - 1,
+                                         ncols, rowptr, rowind, rowval)
 
 
 def ref_spdot(ind, val, x, real="f64"):

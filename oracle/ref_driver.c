@@ -13,6 +13,9 @@
  *   gooseberry_spmult (src/gooseberry.c:53-67).
  * - gbref_dot:    forwards to blas_dot (src/blas.c:413-430).
  * - gbref_spdot:  forwards to blas_spdot (src/blas.c:433-451).
+ * - gbref_read_sparse / _read_dense / _write_sparse / _write_dense: forward
+ *   to the reference's src/io.c readers and writers (CSR and grid formats,
+ *   src/io.c:145-239,369-498,1195-1275); gbref_free releases their arrays.
  * - gbref_pagerank: the pagerank command's loop (src/gooseberry_bin.c:
  *   2610-2741) lives in the CLI's main file, which does not build as a
  *   library; it is restated here around the reference's own blas_spmult,
@@ -34,6 +37,7 @@
 #include "matrix.h"
 #include "blas.h"
 #include "cgd.h"
+#include "io.h"
 #include "permute.h"
 #include <omp.h>
 
@@ -73,6 +77,15 @@ int gbref_cgd(dim_t n, ind_t * rowptr, dim_t * rowind, real_t * rowval,
 size_t gbref_pagerank(dim_t n, const ind_t * rowptr, const dim_t * rowind,
     const real_t * rowval, double damping, double minerror, size_t niter, real_t * result,
     double * error);
+int gbref_read_sparse(int type, const char * file, dim_t * nrows, dim_t * ncols,
+    ind_t ** rowptr, dim_t ** rowind, real_t ** rowval);
+int gbref_read_dense(int type, const char * file, dim_t * nrows, dim_t * ncols,
+    real_t ** rowval);
+int gbref_write_sparse(int type, const char * file, dim_t nrows, dim_t ncols,
+    const ind_t * rowptr, const dim_t * rowind, const real_t * rowval);
+int gbref_write_dense(int type, const char * file, dim_t nrows, dim_t ncols,
+    const real_t * rowval);
+void gbref_free(void * p);
 
 /* OpenMP thread count of the reference's parallel regions.  With 1 thread
  * blas_dot sums in index order, which makes cgd bit-reproducible. */
@@ -240,4 +253,33 @@ size_t gbref_pagerank(dim_t n, const ind_t * rowptr, const dim_t * rowind,
   free(rank);
   free(out);
   return i;
+}
+
+int gbref_read_sparse(int type, const char * file, dim_t * nrows, dim_t * ncols,
+    ind_t ** rowptr, dim_t ** rowind, real_t ** rowval)
+{
+  return read_sparse_matrix(type, file, nrows, ncols, rowptr, rowind, rowval);
+}
+
+int gbref_read_dense(int type, const char * file, dim_t * nrows, dim_t * ncols,
+    real_t ** rowval)
+{
+  return read_dense_matrix(type, file, nrows, ncols, rowval);
+}
+
+int gbref_write_sparse(int type, const char * file, dim_t nrows, dim_t ncols,
+    const ind_t * rowptr, const dim_t * rowind, const real_t * rowval)
+{
+  return write_sparse_matrix(type, file, nrows, ncols, rowptr, rowind, rowval);
+}
+
+int gbref_write_dense(int type, const char * file, dim_t nrows, dim_t ncols,
+    const real_t * rowval)
+{
+  return write_dense_matrix(type, file, nrows, ncols, rowval);
+}
+
+void gbref_free(void * p)
+{
+  free(p);
 }

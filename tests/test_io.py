@@ -1,0 +1,123 @@
+"""CSR and grid text files (gooseberry_read_* / _write_*, the reference's
+src/io.c formats) against the reference's own readers and writers compiled
+into oracle/_ref: the same arrays bit for bit on edge-case and large files,
+byte-identical written files, the same error classes.  Host-only (no GPU)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import gooseberry_b200 as gb
+import oracle
+from gooseberry_b200 import workloads as W
+
+pytestmark = pytest.mark.skipif(not oracle.ref_available("f64"), reason="reference build absent")
+
+CSR_CASES = {
+    "basic": "1 2.5 3 -1\n\n% comment\n2 4e-3\n3 1.5 1 7",
+    "zero_based": "0 1.0 2 2.0\n1 3.5\n",
+    "comments": "# head\n' q\n\" d\n/ s\n1 1\n% mm\n",
+    "crlf": "1 1.5 2 2.5\r\n3 3.5\r\n",
+    "odd_tokens": "1 2 3\n4 5.5 6\n",
+    "signs_exp": "1 +1e3 2 -2.5E-2 5 .5\n",
+    "blank_only": "\n\n\n",
+    "empty": "",
+    "no_trailing_newline": "2 1\n1 2",
+    "tabs": "1\t2.0\t3\t4.0\n",
+}
+
+
+def _csr_equal(path, f64=True):
+    real = "f64" if f64 else "f32"
+    rc, n, nc, rp, ri, rv = oracle.ref_read_csr(path, real=real)
+    assert rc == 1
+    grp, gri, grv, gnc = gb.read_csr(path, f64=f64)
+    assert gnc == nc and len(grp) == n + 1
+    assert np.array_equal(grp, rp) and np.array_equal(gri, ri)
+    assert np.array_equal(grv, rv)
+
+
+@pytest.mark.parametrize("name", sorted(CSR_CASES))
+def test_csr_edge_cases_match_reference(tmp_path, name):
+    p = tmp_path / f"{name}.csr"
+    p.write_text(CSR_CASES[name])
+    _csr_equal(p, f64=True)
+    _csr_equal(p, f64=False)
+
+
+def test_large_csr_round_trip_matches_reference(tmp_path):
+    """A 20k-row power-law matrix with some empty rows, written by both writers
+    (byte-identical) and read back by both readers (the same arrays)."""
+    A = W.powerlaw_rows(20_000, 200_000, seed=21, cap=2000)
+    lengths = np.diff(A.rowptr.astype(np.int64))
+    keep = np.ones(A.nnz, bool)
+    for r in range(0, A.nrows, 997):  # empty rows
+        keep[A.rowptr[r]:A.rowptr[r + 1]] = False
+        lengths[r] = 0
+    rp = np.concatenate([[0], np.cumsum(lengths)]).astype(np.uint32)
+    ri, rv = A.rowind[keep], A.rowval[keep]
+    p_ref, p_ours = tmp_path / "ref.csr", tmp_path / "ours.csr"
+    assert oracle.ref_write_csr(p_ref, rp, ri, rv, A.ncols) == 1
+    gb.write_csr(p_ours, rp, ri, rv, A.ncols)
+    assert p_ref.read_bytes() == p_ours.read_bytes()
+    _csr_equal(p_ref)
+    _csr_equal(p_ref, f64=False)
+
+
+GRID_CASES = {
+    "basic": "1 2 3\n# c\n4 5 6\n",
+    "leading_blank": "\n1 2\n3 4\n",
+    "one_col": "1\n2\n3",
+    "exp": "1e-3 -2E+4\n+5 .25\n",
+}
+
+
+@pytest.mark.parametrize("name", sorted(GRID_CASES))
+def test_grid_cases_match_reference(tmp_path, name):
+    p = tmp_path / f"{name}.grid"
+    p.write_text(GRID_CASES[name])
+    rc, n, nc, vals = oracle.ref_read_grid(p)
+    assert rc == 1
+    g = gb.read_grid(p)
+    assert g.shape == (n, nc)
+    # values fill the grid in order; a leading blank line counts as a row
+    # whose slots the reference leaves unwritten, so compare what was read
+    nvals = sum(len(line.split()) for line in GRID_CASES[name].splitlines()
+                if line and line[0] not in "#%'\"/")
+    assert np.array_equal(g.reshape(-1)[:nvals], vals[:nvals])
+
+
+def test_ragged_grid_is_invalid_like_reference(tmp_path):
+    for text in ("1 2\n3\n", "1 2\n\n3 4\n"):
+        p = tmp_path / "bad.grid"
+        p.write_text(text)
+        assert oracle.ref_read_grid(p)[0] == 3  # GOOSEBERRY_ERROR_INVALIDINPUT
+        with pytest.raises(gb.GooseberryError) as e:
+            gb.read_grid(p)
+        assert e.value.code == 3
+
+
+def test_grid_writer_is_byte_identical(tmp_path):
+    v = np.random.default_rng(3).uniform(-1e6, 1e6, (57, 13))
+    v[3, 4] = 0.0
+    v[5, 6] = 1e-300
+    pr, po = tmp_path / "ref.grid", tmp_path / "ours.grid"
+    assert oracle.ref_write_grid(pr, v.reshape(-1), 57, 13) == 1
+    gb.write_grid(po, v)
+    assert pr.read_bytes() == po.read_bytes()
+    back = gb.read_grid(po)
+    assert np.allclose(back, v, rtol=1e-5)  # %g keeps 6 significant digits
+
+
+def test_error_codes(tmp_path):
+    with pytest.raises(gb.GooseberryError) as e:
+        gb.read_csr(tmp_path / "missing.csr")
+    assert e.value.code == 6  # GOOSEBERRY_ERROR_FILENOTFOUND
+    p = tmp_path / "a.csr"
+    p.write_text("1 1\n")
+    L = gb.lib()
+    out = [np.zeros(1, np.uint64) for _ in range(5)]
+    rc = L.gooseberry_read_sparse_matrix_f64(5, str(p).encode(), *[o.ctypes.data for o in out])
+    assert rc == 2  # GOOSEBERRY_ERROR_UNIMPLEMENTED (GRAPH format)
+    rc = L.gooseberry_read_sparse_matrix_f64(42, str(p).encode(), *[o.ctypes.data for o in out])
+    assert rc == 3  # unknown format

@@ -267,3 +267,19 @@ def test_fused_spmm_bitwise(torch, k):
     for j in range(k):
         assert cond_scaled_err(C[j::k], ref[j::k], A.rowptr, A.rowind, A.rowval,
                                B[j * A.ncols:(j + 1) * A.ncols]) <= TOL64
+
+
+def test_csr_read_to_device(torch, tmp_path):
+    """gb_csr_read parses a CSR text file into a device matrix; its SpMV equals
+    the one of the same arrays uploaded from the host reader's output."""
+    A = W.powerlaw_rows(50_000, 600_000, seed=51, cap=5000)
+    p = tmp_path / "a.csr"
+    gb.write_csr(p, A.rowptr, A.rowind, A.rowval, A.ncols)
+    rp, ri, rv, nc = gb.read_csr(p)
+    M1 = gb.CsrMatrix.read(p)
+    M2 = gb.CsrMatrix.from_host(rowptr=rp, rowind=ri, rowval=rv, ncols=nc)
+    assert (M1.nrows, M1.ncols, M1.nnz) == (len(rp) - 1, nc, len(ri))
+    x = _dev(torch, W.dense_x(nc, 51))
+    M1.set_schedule(gb.SCHED_ROW)
+    M2.set_schedule(gb.SCHED_ROW)
+    assert np.array_equal(M1.spmv(x).cpu().numpy(), M2.spmv(x).cpu().numpy())
