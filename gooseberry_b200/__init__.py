@@ -30,7 +30,8 @@ import numpy as np
 
 __all__ = [
     "GooseberryError", "lib", "spmult", "scale", "add_scalar", "cgd", "pagerank",
-    "read_csr", "read_grid", "write_csr", "write_grid",
+    "read_csr", "read_grid", "write_csr", "write_grid", "cuthillmckee", "permute_sparse",
+    "permute_vector",
     "CsrMatrix", "CgSolver", "CgResult", "dot", "spdot", "SUCCESS",
     "SCHED_AUTO", "SCHED_THREAD", "SCHED_GROUP4", "SCHED_GROUP8", "SCHED_WARP",
     "SCHED_MERGE", "SCHED_ROW", "SCHED_WTILE", "SCHED_WMERGE", "CG_F64", "CG_MIXED", "plan_tiles",
@@ -100,6 +101,12 @@ SIGNATURES = {
     "gooseberry_write_dense_matrix_f64": (_i, [_i, C.c_char_p, _u32, _u32, _vp]),
     "gooseberry_write_sparse_matrix": (_i, [_i, C.c_char_p, _u32, _u32, _vp, _vp, _vp]),
     "gooseberry_write_sparse_matrix_f64": (_i, [_i, C.c_char_p, _u32, _u32, _vp, _vp, _vp]),
+    "gooseberry_permute_cuthillmckee": (_i, [_u32, _u32, _vp, _vp, _vp, _vp, _u32, _vp]),
+    "gooseberry_permute_sparse": (_i, [_u32, _u32, _vp, _vp, _vp, _vp, _vp]),
+    "gooseberry_permute_sparse_f64": (_i, [_u32, _u32, _vp, _vp, _vp, _vp, _vp]),
+    "gb_csr_cuthillmckee": (_i, [_vp, _vp, _u32, _vp, _vp]),
+    "gb_csr_permute": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "gb_permute_vector_f64": (_i, [_sz, _vp, _vp, _i, _vp, _vp]),
     "gb_csr_create": (_i, [_u32, _u32, _u32, _vp, _vp, _vp, _vp, C.c_uint, _vp, _vp]),
     "gb_csr_read": (_i, [C.c_char_p, C.c_uint, _vp, _vp]),
     "gb_csr_destroy": (_i, [_vp]),
@@ -345,6 +352,49 @@ def write_csr(path, rowptr, rowind, rowval, ncols: int = 0):
               _ptr(rowind), _ptr(rowval)), "gooseberry_write_sparse_matrix")
 
 
+def cuthillmckee(rowptr, rowind, nrows: int, ncols: int | None = None, blocks=None):
+    """Cuthill-McKee order of a host CSR (``gooseberry_permute_cuthillmckee``,
+    reference src/permute.c:288-337), computed on the GPU: ``perm[new] = old``.
+    ``blocks`` (nblocks+1 row boundaries) orders each diagonal block alone."""
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+    rowind = np.ascontiguousarray(rowind, dtype=np.uint32)
+    ncols = nrows if ncols is None else int(ncols)
+    perm = np.zeros(max(nrows, 1), dtype=np.uint32)
+    b = None if blocks is None else np.ascontiguousarray(blocks, dtype=np.uint32)
+    nb = 0 if b is None else len(b) - 1
+    _check(lib().gooseberry_permute_cuthillmckee(nrows, ncols, _ptr(rowptr), _ptr(rowind), None,
+                                                 _ptr(b), nb, _ptr(perm)),
+           "gooseberry_permute_cuthillmckee")
+    return perm[:nrows]
+
+
+def permute_sparse(rowptr, rowind, rowval, ncols: int, rowperm=None, colperm=None):
+    """Permuted copy of a host CSR (``gooseberry_permute_sparse[_f64]``, reference
+    src/permute.c:120-205): new row i is row ``rowperm[i]``, column
+    ``colperm[j]`` becomes j.  Returns ``(rowptr, rowind, rowval)``."""
+    rowptr = np.array(rowptr, dtype=np.uint32)
+    rowind = np.array(rowind, dtype=np.uint32)
+    real = _real(np.asarray(rowval).dtype)
+    rowval = np.array(rowval, dtype=np.float64 if real == "f64" else np.float32)
+    rp = None if rowperm is None else np.ascontiguousarray(rowperm, dtype=np.uint32)
+    cp = None if colperm is None else np.ascontiguousarray(colperm, dtype=np.uint32)
+    fn = lib().gooseberry_permute_sparse_f64 if real == "f64" else lib().gooseberry_permute_sparse
+    _check(fn(len(rowptr) - 1, ncols, _ptr(rowptr), _ptr(rowind), _ptr(rowval), _ptr(rp),
+              _ptr(cp)), "gooseberry_permute_sparse")
+    return rowptr, rowind, rowval
+
+
+def permute_vector(x, perm, reverse: bool = False, stream=None):
+    """``y[i] = x[perm[i]]`` (or ``y[perm[i]] = x[i]`` with ``reverse``) for
+    float64 CUDA tensors; ``perm`` a uint32/int32 CUDA tensor."""
+    torch = _torch()
+    y = torch.empty_like(x)
+    _check(lib().gb_permute_vector_f64(x.numel(), x.data_ptr(), perm.data_ptr(), int(reverse),
+                                       y.data_ptr(), _stream_ptr(stream)),
+           "gb_permute_vector_f64")
+    return y
+
+
 def plan_tiles(rowptr, tile_items: int = 2048):
     """Run the SpMV tile planner on a host rowptr (no GPU).  Returns
     ``(tiles[ntiles, 4], nlong, info)``; see ``gb_plan_tiles_host``."""
@@ -480,6 +530,25 @@ class CsrMatrix:
         fn = lib().gb_spmv_f64 if x.dtype == torch.float64 else lib().gb_spmv_f32
         _check(fn(self._h, x.data_ptr(), y.data_ptr(), _stream_ptr(stream)), "gb_spmv")
         return y
+
+    def cuthillmckee(self, blocks=None, stream=None):
+        """Cuthill-McKee order on the device (``gb_csr_cuthillmckee``): an int32
+        CUDA tensor ``perm`` with ``perm[new] = old``."""
+        torch = _torch()
+        perm = torch.empty(max(self.nrows, 1), dtype=torch.int32, device="cuda")
+        b = None if blocks is None else np.ascontiguousarray(blocks, dtype=np.uint32)
+        nb = 0 if b is None else len(b) - 1
+        _check(lib().gb_csr_cuthillmckee(self._h, _ptr(b), nb, perm.data_ptr(),
+                                         _stream_ptr(stream)), "gb_csr_cuthillmckee")
+        return perm[: self.nrows]
+
+    def permute(self, rowperm=None, colperm=None, stream=None) -> "CsrMatrix":
+        """A new matrix with rows ``rowperm`` and columns renamed by ``colperm``
+        (int32/uint32 CUDA tensors or None; ``gb_csr_permute``)."""
+        h = C.c_void_p()
+        _check(lib().gb_csr_permute(self._h, _ptr(rowperm), _ptr(colperm), _stream_ptr(stream),
+                                    C.addressof(h)), "gb_csr_permute")
+        return CsrMatrix(h.value, self.nrows, self.ncols, self.nnz)
 
     def spmm(self, B, bncols: int, out=None, stream=None):
         torch = _torch()

@@ -178,6 +178,11 @@ int dev_alloc(T ** p, size_t bytes) {
   return dev_alloc(reinterpret_cast<void **>(p), bytes);
 }
 
+// Wrap device arrays allocated with dev_alloc into a matrix that owns them
+// (gb_csr_destroy frees them).  On failure the arrays stay the caller's.
+int csr_adopt(uint32_t nrows, uint32_t ncols, uint32_t nnz, uint32_t * rowptr,
+    uint32_t * rowind, double * val64, float * val32, cudaStream_t stream, gb_csr ** out);
+
 // Mixed-precision CG (cg_mixed.cu), owned by a gb_cg created with GB_CG_MIXED.
 struct MixedCg;
 int mixed_create(const gb_csr * a, MixedCg ** out);

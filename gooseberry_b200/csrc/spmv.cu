@@ -569,6 +569,29 @@ int create_impl(dim_t nrows, dim_t ncols, ind_t nnz, const ind_t * rowptr,
 
 }  // namespace
 
+namespace gb {
+
+int csr_adopt(uint32_t nrows, uint32_t ncols, uint32_t nnz, uint32_t * rowptr,
+    uint32_t * rowind, double * val64, float * val32, cudaStream_t stream, gb_csr ** out) {
+  *out = nullptr;
+  const unsigned flags = GB_CSR_DEVICE_POINTERS | (val64 ? GB_CSR_VALUES_F64 : 0u) |
+                         (val32 ? GB_CSR_VALUES_F32 : 0u);
+  gb_csr * a = new gb_csr();
+  int rc = create_impl(nrows, ncols, nnz, rowptr, rowind, val64, val32, flags, stream, a);
+  if (rc != GOOSEBERRY_SUCCESS) {
+    release(a);  // frees only what create_impl allocated itself
+    return rc;
+  }
+  a->own_rowptr = rowptr;
+  a->own_rowind = rowind;
+  a->own_val64 = val64;
+  if (val32) a->own_val32 = val32;
+  *out = a;
+  return GOOSEBERRY_SUCCESS;
+}
+
+}  // namespace gb
+
 extern "C" {
 
 int gb_csr_create(dim_t nrows, dim_t ncols, ind_t nnz, const ind_t * rowptr,

@@ -105,6 +105,7 @@ extern "C" {
 #define gooseberry_read_dense_matrix gooseberry_read_dense_matrix_f64
 #define gooseberry_write_sparse_matrix gooseberry_write_sparse_matrix_f64
 #define gooseberry_write_dense_matrix gooseberry_write_dense_matrix_f64
+#define gooseberry_permute_sparse gooseberry_permute_sparse_f64
 #endif
 
 /*
@@ -216,6 +217,35 @@ GOOSEBERRY_API int gooseberry_write_sparse_matrix(int type, const char * file, d
 GOOSEBERRY_API int gooseberry_write_sparse_matrix_f64(int type, const char * file,
     dim_t nrows, dim_t ncols, const ind_t * rowptr, const dim_t * rowind,
     const double * rowval);
+
+/*
+ * Bandwidth-reducing order: replaces permute_cuthillmckee (reference
+ * src/permute.h:40-48, src/permute.c:288-337), which the CLI calls for
+ * `permute -p bandwidth` (src/gooseberry_bin.c:986-993) and `blas -b`
+ * (:1655-1676).  perm[new] = old.  With `blocks` (nblocks+1 row boundaries)
+ * every diagonal block is ordered on its own within its slice of perm; edges
+ * leaving a block are ignored.  Equal degrees go smaller row first.  rowval is
+ * not read.  nrows != ncols gives GOOSEBERRY_ERROR_INVALIDINPUT as in the
+ * reference; so do blocks that do not cover [0, nrows) (the reference leaves
+ * the uncovered part of perm unwritten).  Runs on the GPU; host arrays.
+ */
+GOOSEBERRY_API int gooseberry_permute_cuthillmckee(dim_t nrows, dim_t ncols,
+    const ind_t * rowptr, const dim_t * rowind, const void * rowval, const dim_t * blocks,
+    dim_t nblocks, dim_t * perm);
+
+/*
+ * In-place sparse permutation: replaces permute_sparse (reference
+ * src/permute.h:30-37, src/permute.c:120-205).  New row i is old row
+ * rowperm[i]; old column colperm[j] becomes column j; either may be NULL (no
+ * change); the entries of a row keep their stored order.  Differences: a
+ * rowperm / colperm that is not a permutation, a decreasing rowptr or a column
+ * >= ncols gives GOOSEBERRY_ERROR_INVALIDINPUT and leaves the arrays as they
+ * were (the reference reads or writes out of bounds).  Runs on the GPU.
+ */
+GOOSEBERRY_API int gooseberry_permute_sparse(dim_t nrows, dim_t ncols, ind_t * rowptr,
+    dim_t * rowind, real_t * rowval, const dim_t * rowperm, const dim_t * colperm);
+GOOSEBERRY_API int gooseberry_permute_sparse_f64(dim_t nrows, dim_t ncols, ind_t * rowptr,
+    dim_t * rowind, double * rowval, const dim_t * rowperm, const dim_t * colperm);
 
 #ifdef __cplusplus
 }

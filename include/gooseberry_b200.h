@@ -153,6 +153,31 @@ GOOSEBERRY_API int gb_spmv_f32(const gb_csr_t * a, const float * x, float * y,
 GOOSEBERRY_API int gb_spmm_f64(const gb_csr_t * a, dim_t bncols, const double * b, double * c,
     gb_stream_t stream);
 
+/* ---- reordering ------------------------------------------------------------ */
+
+/* Cuthill-McKee order of a square device matrix into the DEVICE array perm
+ * (perm[new] = old), as permute_cuthillmckee (reference src/permute.c:
+ * 288-337) computes it; equal degrees go smaller row first.  blocks: HOST
+ * array of nblocks+1 row boundaries covering [0, nrows) (each diagonal block
+ * ordered on its own, edges leaving it ignored), or NULL.  Synchronous. */
+GOOSEBERRY_API int gb_csr_cuthillmckee(const gb_csr_t * a, const dim_t * blocks, dim_t nblocks,
+    dim_t * perm, gb_stream_t stream);
+
+/* A new device matrix P_r A P_c^T: new row i is row rowperm[i] of a, old
+ * column colperm[j] becomes column j (permute_sparse, reference
+ * src/permute.c:120-205); both DEVICE arrays, NULL for identity; rows keep
+ * their entry order.  The result holds the same value widths as a, owns its
+ * memory and gets the default schedule.  Synchronous. */
+GOOSEBERRY_API int gb_csr_permute(const gb_csr_t * a, const dim_t * rowperm,
+    const dim_t * colperm, gb_stream_t stream, gb_csr_t ** out);
+
+/* y[i] = x[perm[i]] (reverse = 0; permute_dense with one column, reference
+ * src/permute.c:208-242) or y[perm[i]] = x[i] (reverse != 0;
+ * permute_dense_rev, :245-280).  Device arrays; perm must be a permutation
+ * of 0..n-1; x and y must not overlap. */
+GOOSEBERRY_API int gb_permute_vector_f64(size_t n, const double * x, const dim_t * perm,
+    int reverse, double * y, gb_stream_t stream);
+
 /* ---- BLAS-1 on device vectors --------------------------------------------- */
 
 /* *result = sum a[i]*b[i], accumulated in double, deterministic (fixed

@@ -69,6 +69,14 @@ def _lib():
                 f.argtypes = [C.c_uint32, _u32p, _u32p, p, C.c_double, C.c_double,
                               C.c_size_t, p, C.POINTER(C.c_double)]
                 f.restype = C.c_size_t
+            if real == "f64":
+                lib.oracle_cuthillmckee.argtypes = [C.c_uint32, C.c_uint32, _u32p, _u32p,
+                                                    C.c_void_p, C.c_uint32, _u32p]
+                lib.oracle_cuthillmckee.restype = C.c_int
+                lib.oracle_permute_sparse_f64.argtypes = [C.c_uint32, C.c_uint32, _u32p,
+                                                          _u32p, p, C.c_void_p, C.c_void_p,
+                                                          _u32p, _u32p, p]
+                lib.oracle_permute_sparse_f64.restype = None
             f = getattr(lib, f"oracle_cgd_{real}")
             f.argtypes = [C.c_uint32, _u32p, _u32p, p, p, p, ctype, C.c_size_t,
                           C.c_void_p, C.c_size_t, C.POINTER(C.c_double), C.c_int]
@@ -113,6 +121,11 @@ def _ref(real: str = "f64"):
         lib.gbref_write_dense.restype = C.c_int
         lib.gbref_free.argtypes = [vp]
         lib.gbref_free.restype = None
+        lib.gbref_cuthillmckee.argtypes = [C.c_uint32, C.c_uint32, _u32p, _u32p, vp,
+                                           C.c_uint32, _u32p]
+        lib.gbref_cuthillmckee.restype = C.c_int
+        lib.gbref_permute_sparse.argtypes = [C.c_uint32, C.c_uint32, _u32p, _u32p, p, vp, vp]
+        lib.gbref_permute_sparse.restype = C.c_int
         lib.gbref_cgd.argtypes = [C.c_uint32, _u32p, _u32p, p, p, p, C.c_double,
                                   C.c_size_t, C.POINTER(C.c_size_t),
                                   C.POINTER(C.c_double), C.c_void_p, C.c_size_t]
@@ -354,3 +367,73 @@ def ref_cgd(rowptr, rowind, rowval, b, error, niter, real="f64", history=False):
     if history:
         return x, int(it.value), last.value, hist[: it.value]
     return x, int(it.value), last.value
+
+
+def _perm_arg(perm):
+    if perm is None:
+        return None, None
+    a = np.ascontiguousarray(perm, dtype=np.uint32)
+    return a.ctypes.data_as(C.c_void_p), a
+
+
+def cuthillmckee(rowptr, rowind, nrows, ncols=None, blocks=None):
+    """Restated Cuthill-McKee order (src/permute.c:45-104,288-337); equal
+    degrees smaller id first.  Returns perm (perm[new] = old), or None when the
+    matrix is not square (the reference's INVALIDINPUT)."""
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+    rowind = np.ascontiguousarray(rowind, dtype=np.uint32)
+    ncols = nrows if ncols is None else ncols
+    perm = np.zeros(max(nrows, 1), dtype=np.uint32)
+    bp, nb, keep = _blocks_arg(blocks)
+    rc = _lib().oracle_cuthillmckee(nrows, ncols, rowptr, rowind, bp, nb, perm)
+    del keep
+    return None if rc != 0 else perm[:nrows]
+
+
+def ref_cuthillmckee(rowptr, rowind, nrows, ncols=None, blocks=None, real="f64"):
+    """The reference's own permute_cuthillmckee (src/permute.c:288-337), with
+    the oracle shim's priority queue.  Returns (rc, perm)."""
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+    rowind = np.ascontiguousarray(rowind, dtype=np.uint32)
+    ncols = nrows if ncols is None else ncols
+    perm = np.zeros(max(nrows, 1), dtype=np.uint32)
+    bp, nb, keep = _blocks_arg(blocks)
+    rc = _ref(real).gbref_cuthillmckee(nrows, ncols, rowptr, rowind, bp, nb, perm)
+    del keep
+    return rc, perm[:nrows]
+
+
+def permute_sparse(rowptr, rowind, rowval, ncols, rowperm=None, colperm=None):
+    """Restated permute_sparse (src/permute.c:120-205), FP64, out of place:
+    returns (rowptr, rowind, rowval) of the permuted matrix."""
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+    rowind = np.ascontiguousarray(rowind, dtype=np.uint32)
+    rowval = np.ascontiguousarray(rowval, dtype=np.float64)
+    n = len(rowptr) - 1
+    nnz = int(rowptr[-1])
+    prp = np.zeros(n + 1, dtype=np.uint32)
+    pri = np.zeros(max(nnz, 1), dtype=np.uint32)
+    prv = np.zeros(max(nnz, 1), dtype=np.float64)
+    rp, rk = _perm_arg(rowperm)
+    cp, ck = _perm_arg(colperm)
+    _lib().oracle_permute_sparse_f64(n, ncols, rowptr, rowind, rowval, rp, cp, prp, pri, prv)
+    del rk, ck
+    return prp, pri[:nnz], prv[:nnz]
+
+
+def ref_permute_sparse(rowptr, rowind, rowval, ncols, rowperm=None, colperm=None, real="f64"):
+    """The reference's own permute_sparse (src/permute.c:120-205), applied to
+    copies: returns (rc, rowptr, rowind, rowval)."""
+    rowptr = np.array(rowptr, dtype=np.uint32)
+    rowind = np.array(rowind, dtype=np.uint32)
+    rowval = np.array(rowval, dtype=_dt(real))
+    if len(rowind) == 0:
+        rowind = np.zeros(1, np.uint32)
+        rowval = np.zeros(1, _dt(real))
+    rp, rk = _perm_arg(rowperm)
+    cp, ck = _perm_arg(colperm)
+    rc = _ref(real).gbref_permute_sparse(len(rowptr) - 1, ncols, rowptr, rowind, rowval, rp, cp)
+    del rk, ck
+    nnz = int(rowptr[-1])
+    return rc, rowptr, rowind[:nnz], rowval[:nnz]
+

@@ -298,3 +298,125 @@ size_t oracle_pagerank_f64(uint32_t n, const uint32_t * rowptr, const uint32_t *
   free(out);
   return i;
 }
+
+/*
+ * Cuthill-McKee order -- src/permute.c:45-104 (__cuthillmckee_block) and
+ * :288-337 (permute_cuthillmckee).  perm[new] = old.
+ *
+ * Per diagonal block [start, end) (the whole matrix when blocks is NULL):
+ *   - deg[v] = entries of row v whose column lies in [start, end) (:66-77);
+ *   - a new component starts at the remaining vertex of least degree
+ *     (:81-84, the `rem` queue);
+ *   - breadth-first from it: for each ordered vertex in turn, its still
+ *     remaining in-block columns are taken out of `rem` and appended in
+ *     ascending degree (:86-101, the `q` queue).
+ * Positions start at `start`, so each block orders its own slice of perm.
+ * Equal degrees are taken smaller vertex id first.  The reference's queues
+ * come from domlib's dlpq (not vendored); this tie order is the one the oracle
+ * shim's queue gives the compiled reference, so the two agree exactly.
+ *
+ * Written as a sort, not a queue: the least-degree remaining vertex is the
+ * first unvisited entry of all vertices sorted by (degree, id), and a
+ * vertex's children leave `q` in (degree, id) order.  Returns 0, or -1 when
+ * nrows != ncols (the reference's GOOSEBERRY_ERROR_INVALIDINPUT).
+ */
+static int oracle_u64_cmp(const void * a, const void * b)
+{
+  const uint64_t x = *(const uint64_t *)a, y = *(const uint64_t *)b;
+  return x < y ? -1 : (x > y ? 1 : 0);
+}
+
+static void oracle_cm_block(uint32_t start, uint32_t end, const uint32_t * rowptr,
+    const uint32_t * rowind, uint32_t * perm)
+{
+  const uint32_t m = end - start;
+  uint32_t v, j, nordered = start, sr = start, next = 0, maxdeg = 0, nc;
+  uint32_t * deg = calloc(m ? m : 1, sizeof(uint32_t));
+  uint32_t * order = malloc(sizeof(uint32_t) * (m ? m : 1));
+  uint32_t * count;
+  unsigned char * seen = calloc(m ? m : 1, 1);
+  uint64_t * child = malloc(sizeof(uint64_t) * (m ? m : 1));
+  for (v = start; v < end; ++v) {
+    uint32_t d = 0;
+    for (j = rowptr[v]; j < rowptr[v + 1]; ++j) {
+      if (rowind[j] >= start && rowind[j] < end) ++d;
+    }
+    deg[v - start] = d;
+    if (d > maxdeg) maxdeg = d;
+  }
+  /* stable counting sort by degree: (degree, id) order */
+  count = calloc((size_t)maxdeg + 2, sizeof(uint32_t));
+  for (v = 0; v < m; ++v) ++count[deg[v] + 1];
+  for (v = 0; v <= maxdeg; ++v) count[v + 1] += count[v];
+  for (v = 0; v < m; ++v) order[count[deg[v]]++] = start + v;
+  free(count);
+  while (nordered < end) {
+    while (seen[order[next] - start]) ++next;
+    v = order[next];
+    seen[v - start] = 1;
+    perm[nordered++] = v;
+    while (sr < nordered) {
+      v = perm[sr++];
+      nc = 0;
+      for (j = rowptr[v]; j < rowptr[v + 1]; ++j) {
+        const uint32_t k = rowind[j];
+        if (k >= start && k < end && !seen[k - start]) {
+          seen[k - start] = 1;
+          child[nc++] = ((uint64_t)deg[k - start] << 32) | k;
+        }
+      }
+      qsort(child, nc, sizeof(uint64_t), oracle_u64_cmp);
+      for (j = 0; j < nc; ++j) perm[nordered++] = (uint32_t)child[j];
+    }
+  }
+  free(deg);
+  free(order);
+  free(seen);
+  free(child);
+}
+
+int oracle_cuthillmckee(uint32_t nrows, uint32_t ncols, const uint32_t * rowptr,
+    const uint32_t * rowind, const uint32_t * blocks, uint32_t nblocks, uint32_t * perm);
+int oracle_cuthillmckee(uint32_t nrows, uint32_t ncols, const uint32_t * rowptr,
+    const uint32_t * rowind, const uint32_t * blocks, uint32_t nblocks, uint32_t * perm)
+{
+  uint32_t c;
+  if (nrows != ncols) return -1;
+  if (blocks) {
+    for (c = 0; c < nblocks; ++c) oracle_cm_block(blocks[c], blocks[c + 1], rowptr, rowind, perm);
+  } else {
+    oracle_cm_block(0, nrows, rowptr, rowind, perm);
+  }
+  return 0;
+}
+
+/*
+ * Sparse permutation -- src/permute.c:120-205 (permute_sparse), out of place:
+ * new row i is old row rowperm[i] (identity when NULL) with its entries in
+ * their stored order; an old column c becomes the j with colperm[j] == c
+ * (unchanged when colperm is NULL).  Columns are not re-sorted.
+ */
+void oracle_permute_sparse_f64(uint32_t nrows, uint32_t ncols, const uint32_t * rowptr,
+    const uint32_t * rowind, const double * rowval, const uint32_t * rowperm,
+    const uint32_t * colperm, uint32_t * prowptr, uint32_t * prowind, double * prowval);
+void oracle_permute_sparse_f64(uint32_t nrows, uint32_t ncols, const uint32_t * rowptr,
+    const uint32_t * rowind, const double * rowval, const uint32_t * rowperm,
+    const uint32_t * colperm, uint32_t * prowptr, uint32_t * prowind, double * prowval)
+{
+  uint32_t i, j, v, k = 0;
+  uint32_t * rename = NULL;
+  if (colperm) {
+    rename = malloc(sizeof(uint32_t) * (ncols ? ncols : 1));
+    for (j = 0; j < ncols; ++j) rename[colperm[j]] = j;
+  }
+  prowptr[0] = 0;
+  for (i = 0; i < nrows; ++i) {
+    v = rowperm ? rowperm[i] : i;
+    for (j = rowptr[v]; j < rowptr[v + 1]; ++j, ++k) {
+      prowind[k] = rename ? rename[rowind[j]] : rowind[j];
+      prowval[k] = rowval[j];
+    }
+    prowptr[i + 1] = k;
+  }
+  free(rename);
+}

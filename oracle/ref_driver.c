@@ -25,8 +25,11 @@
  *   one "ITER: k RMSE: v" line per iteration (src/cgd.c:116) and returns no
  *   iteration count, so stdout is redirected to a temporary file for the call
  *   and the ITER lines are parsed back into (iterations, last norm, history).
- * - permute_* stubs: src/matrix.c:256-373 references them for permutations,
- *   which nothing on the SpMV/CG path calls.
+ * - gbref_cuthillmckee / gbref_permute_sparse: forward to
+ *   permute_cuthillmckee (src/permute.c:288-337) and permute_sparse
+ *   (src/permute.c:120-205), compiled from src/permute.c against the shim's
+ *   priority queue (oracle/shim/dlpq_headers.h), which breaks equal-degree
+ *   ties by the smaller vertex id.
  */
 #include <math.h>
 #include <stdio.h>
@@ -40,28 +43,6 @@
 #include "io.h"
 #include "permute.h"
 #include <omp.h>
-
-int permute_sparse(dim_t nrows, dim_t ncols, ind_t * rowptr, dim_t * rowind,
-    real_t * rowval, const dim_t * rowperm, const dim_t * colperm)
-{
-  (void)nrows; (void)ncols; (void)rowptr; (void)rowind; (void)rowval;
-  (void)rowperm; (void)colperm;
-  return GOOSEBERRY_ERROR_UNIMPLEMENTED;
-}
-
-int permute_dense(dim_t nrows, dim_t ncols, real_t * rowval,
-    const dim_t * rowperm, const dim_t * colperm)
-{
-  (void)nrows; (void)ncols; (void)rowval; (void)rowperm; (void)colperm;
-  return GOOSEBERRY_ERROR_UNIMPLEMENTED;
-}
-
-int permute_dense_rev(dim_t nrows, dim_t ncols, real_t * rowval,
-    const dim_t * rowperm, const dim_t * colperm)
-{
-  (void)nrows; (void)ncols; (void)rowval; (void)rowperm; (void)colperm;
-  return GOOSEBERRY_ERROR_UNIMPLEMENTED;
-}
 
 int gbref_real_size(void);
 void gbref_set_threads(int n);
@@ -86,6 +67,11 @@ int gbref_write_sparse(int type, const char * file, dim_t nrows, dim_t ncols,
 int gbref_write_dense(int type, const char * file, dim_t nrows, dim_t ncols,
     const real_t * rowval);
 void gbref_free(void * p);
+int gbref_cuthillmckee(dim_t nrows, dim_t ncols, const ind_t * rowptr,
+    const dim_t * rowind, const dim_t * blocks, dim_t nblocks, dim_t * perm);
+int gbref_permute_sparse(dim_t nrows, dim_t ncols, ind_t * rowptr,
+    dim_t * rowind, real_t * rowval, const dim_t * rowperm,
+    const dim_t * colperm);
 
 /* OpenMP thread count of the reference's parallel regions.  With 1 thread
  * blas_dot sums in index order, which makes cgd bit-reproducible. */
@@ -282,4 +268,23 @@ int gbref_write_dense(int type, const char * file, dim_t nrows, dim_t ncols,
 void gbref_free(void * p)
 {
   free(p);
+}
+
+/* The bandwidth-reducing order (src/permute.c:288-337): perm[new] = old; per
+ * block when `blocks` (nblocks+1 boundaries) is given.  The values are not
+ * read by the ordering. */
+int gbref_cuthillmckee(dim_t nrows, dim_t ncols, const ind_t * rowptr,
+    const dim_t * rowind, const dim_t * blocks, dim_t nblocks, dim_t * perm)
+{
+  return permute_cuthillmckee(nrows, ncols, rowptr, rowind, NULL, blocks,
+      nblocks, perm);
+}
+
+/* In-place sparse permutation (src/permute.c:120-205): new row i is old row
+ * rowperm[i]; old column colperm[j] becomes column j. */
+int gbref_permute_sparse(dim_t nrows, dim_t ncols, ind_t * rowptr,
+    dim_t * rowind, real_t * rowval, const dim_t * rowperm,
+    const dim_t * colperm)
+{
+  return permute_sparse(nrows, ncols, rowptr, rowind, rowval, rowperm, colperm);
 }

@@ -54,6 +54,11 @@ def cg_golden():
 
 
 @pytest.fixture(scope="session")
+def rcm_golden():
+    return _cases(np.load(os.path.join(GOLDEN, "rcm_cases.npz")))
+
+
+@pytest.fixture(scope="session")
 def full_golden():
     with open(os.path.join(GOLDEN, "full_sizes.json")) as f:
         return json.load(f)

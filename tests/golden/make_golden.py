@@ -7,11 +7,15 @@ pin: the oracle restatement and the CUDA path are both checked against them.
 Run from the repo root (needs the reference sources at build time only):
 
     make -C oracle ref && OMP_NUM_THREADS=8 python tests/golden/make_golden.py
+    python tests/golden/make_golden.py --only rcm     # just rcm_cases.npz
 
 Fixtures
   spmv_cases.npz  small SpMV cases (inputs + reference outputs, f64 and f32)
   cg_cases.npz    small CG cases (inputs + reference x, iteration counts;
                   reference run on one OpenMP thread)
+  rcm_cases.npz   Cuthill-McKee orders (src/permute.c:288-337, compiled with
+                  the oracle shim's priority queue: equal degrees smaller
+                  id first) and permute_sparse results (src/permute.c:120-205)
   full_sizes.json checksums of the reference SpMV on the full 100k x 100k
                   uniform matrix, and the reference CG iteration count /
                   final ||r|| on the full 1024x1024 Laplacian
@@ -133,6 +137,96 @@ def cg_cases():
     return sorted(cases)
 
 
+def scrambled_band(n, half, seed):
+    """A symmetric band matrix (|i-j| <= half) with its rows and columns
+    renumbered by a seeded permutation: bandwidth ~n until reordered."""
+    p = np.argsort(W.rand_u64(seed, 30, 0, n), kind="stable").astype(np.int64)
+    inv = np.empty(n, np.int64)
+    inv[p] = np.arange(n)
+    rows, cols = [], []
+    for d in range(-half, half + 1):
+        i = np.arange(max(0, -d), min(n, n - d))
+        rows.append(inv[i])
+        cols.append(inv[i + d])
+    r = np.concatenate(rows)
+    c = np.concatenate(cols)
+    o = np.lexsort((c, r))
+    r, c = r[o], c[o]
+    rp = np.zeros(n + 1, np.int64)
+    np.add.at(rp, r + 1, 1)
+    vals = W.rand_uniform(seed, W.S_VALS, len(c), -1.0, 1.0)
+    return W.Csr(n, n, np.cumsum(rp).astype(np.uint32), c.astype(np.uint32), vals)
+
+
+def isolated(n, seed):
+    """Mostly isolated vertices (diagonal only) with a few short chains: many
+    one-vertex components."""
+    rows, cols = list(range(n)), list(range(n))
+    for a in range(0, n - 3, 97):
+        rows += [a, a + 1, a + 1, a + 2]
+        cols += [a + 1, a, a + 2, a + 1]
+    r = np.array(rows)
+    c = np.array(cols)
+    o = np.lexsort((c, r))
+    r, c = r[o], c[o]
+    rp = np.zeros(n + 1, np.int64)
+    np.add.at(rp, r + 1, 1)
+    vals = W.rand_uniform(seed, W.S_VALS, len(c), -1.0, 1.0)
+    return W.Csr(n, n, np.cumsum(rp).astype(np.uint32), c.astype(np.uint32), vals)
+
+
+def rcm_cases():
+    cases = {
+        "laplace16": (W.laplacian_2d(16), None),
+        "band2000": (scrambled_band(2000, 4, 31), None),
+        "uniform300": (W.uniform_rows(300, 10, seed=11), None),
+        "uniform300_blocks": (W.uniform_rows(300, 10, seed=11),
+                              np.array([0, 50, 50, 120, 300], np.uint32)),
+        "powerlaw4k": (W.powerlaw_rows(4000, 64000, seed=13, cap=4000), None),
+        "ragged5k": (ragged(14), None),
+        "isolated3000": (isolated(3000, 32), None),
+    }
+    out = {}
+    for name, (A, blocks) in cases.items():
+        # values = entry numbers: distinct, so a permuted copy shows where
+        # every entry went (and the file compresses)
+        A = W.Csr(A.nrows, A.ncols, A.rowptr, A.rowind,
+                  np.arange(len(A.rowind), dtype=np.float64))
+        cases[name] = (A, blocks)
+        rc, perm = oracle.ref_cuthillmckee(A.rowptr, A.rowind, A.nrows, blocks=blocks)
+        assert rc == 1, (name, rc)
+        out[f"{name}/rowptr"] = A.rowptr
+        out[f"{name}/rowind"] = A.rowind
+        if blocks is not None:
+            out[f"{name}/blocks"] = blocks
+        out[f"{name}/perm"] = perm
+        # the reordered matrix P A P^T (the CLI's `permute -p bandwidth`)
+        rc, prp, pri, prv = oracle.ref_permute_sparse(A.rowptr, A.rowind, A.rowval, A.ncols,
+                                                      perm, perm)
+        assert rc == 1, (name, rc)
+        assert np.array_equal(prv, A.rowval[prv.astype(np.int64)])
+        out[f"{name}/p_rowptr"] = prp
+        out[f"{name}/p_rowind"] = pri
+        out[f"{name}/p_source"] = prv.astype(np.uint32)  # entry numbers
+    # rows only, and columns only, with seeded permutations
+    A = cases["uniform300"][0]
+    rperm = np.argsort(W.rand_u64(33, 30, 0, 300), kind="stable").astype(np.uint32)
+    cperm = np.argsort(W.rand_u64(34, 30, 0, 300), kind="stable").astype(np.uint32)
+    for tag, rp_, cp_ in (("rows", rperm, None), ("cols", None, cperm)):
+        rc, prp, pri, prv = oracle.ref_permute_sparse(A.rowptr, A.rowind, A.rowval, A.ncols,
+                                                      rp_, cp_)
+        assert rc == 1
+        out[f"perm_{tag}/rowptr"] = A.rowptr
+        out[f"perm_{tag}/rowind"] = A.rowind
+        out[f"perm_{tag}/rowperm"] = rp_ if rp_ is not None else np.zeros(0, np.uint32)
+        out[f"perm_{tag}/colperm"] = cp_ if cp_ is not None else np.zeros(0, np.uint32)
+        out[f"perm_{tag}/p_rowptr"] = prp
+        out[f"perm_{tag}/p_rowind"] = pri
+        out[f"perm_{tag}/p_source"] = prv.astype(np.uint32)
+    np.savez_compressed(os.path.join(OUT, "rcm_cases.npz"), **out)
+    return sorted(cases)
+
+
 def full_sizes():
     res = {}
     t = time.time()
@@ -167,7 +261,11 @@ def full_sizes():
 if __name__ == "__main__":
     if not oracle.ref_available("f64") or not oracle.ref_available("f32"):
         sys.exit("build the reference oracle first: make -C oracle ref")
+    if "--only" in sys.argv and sys.argv[sys.argv.index("--only") + 1] == "rcm":
+        print("rcm:", rcm_cases())
+        sys.exit(0)
     print("spmv:", spmv_cases())
+    print("rcm:", rcm_cases())
     print("cg:", cg_cases())
     if "--skip-full" not in sys.argv:
         full_sizes()
