@@ -754,6 +754,102 @@ def spmm_extra(k=8, flush=None, peak=None, reps=20):
     return out
 
 
+def _device_spmv_ms(M, xd, flush, reps=20):
+    """Median device time of one autotuned FP64 SpMV of a device matrix."""
+    import torch
+
+    import gooseberry_b200 as gb
+    M.autotune()
+    y = M.spmv(xd)
+    for _ in range(3):
+        M.spmv(xd, y)
+    ts = []
+    for _ in range(reps):
+        if flush is not None:
+            flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        M.spmv(xd, y)
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return {"ms": float(np.median(ts)), "schedule": gb.SCHED_NAMES[M.info().schedule]}
+
+
+def rcm_extra(powerlaw=None, flush=None):
+    """Bandwidth-reducing reorder (Cuthill-McKee, src/permute.c:288-337; the
+    CLI's `permute -p bandwidth` and `blas -b`).  Ours: the drop-in
+    gooseberry_permute_cuthillmckee on host arrays (upload, device ordering,
+    download) and the device-resident gb_csr_cuthillmckee; reference: its own
+    permute.c on one host core (the unblocked call is serial), same graphs,
+    equal orders required.  Then what the order buys the SpMV: the power-law
+    matrix and a 2D Laplacian whose numbering was scrambled, each timed
+    before and after P A P^T."""
+    import torch
+
+    import gooseberry_b200 as gb
+    import oracle
+    from gooseberry_b200 import workloads as W
+    graphs = [("uniform_100k", W.uniform_rows(100_000, 10, seed=1)),
+              ("laplace_1024", W.laplacian_2d(1024))]
+    if powerlaw is not None:
+        graphs.append(("powerlaw_8m", powerlaw))
+    out = {}
+    for name, A in graphs:
+        gb.cuthillmckee(A.rowptr, A.rowind, A.nrows)  # warm
+        t0 = time.perf_counter()
+        perm = gb.cuthillmckee(A.rowptr, A.rowind, A.nrows)
+        t_drop = time.perf_counter() - t0
+        M = gb.CsrMatrix.from_host(A)
+        M.cuthillmckee()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dperm = M.cuthillmckee()
+        torch.cuda.synchronize()
+        t_dev = time.perf_counter() - t0
+        r = {"n": A.nrows, "nnz": A.nnz, "dropin_ms": t_drop * 1e3, "device_ms": t_dev * 1e3}
+        if oracle.ref_available("f64"):
+            t0 = time.perf_counter()
+            rc, ref = oracle.ref_cuthillmckee(A.rowptr, A.rowind, A.nrows)
+            t_ref = time.perf_counter() - t0
+            r.update({"reference_ms": t_ref * 1e3, "reference_cores": 1,
+                      "speedup_dropin_vs_reference": t_ref / t_drop,
+                      "same_order_as_reference": bool(np.array_equal(perm, ref)) and bool(
+                          np.array_equal(dperm.cpu().numpy().astype(np.uint32), ref))})
+        if name == "powerlaw_8m":
+            xd = torch.from_numpy(W.dense_x(A.nrows, 3)).cuda()
+            R = M.permute(dperm, dperm)
+            px = gb.permute_vector(xd, dperm)
+            r["spmv_f64_before"] = _device_spmv_ms(M, xd, flush)
+            r["spmv_f64_after"] = _device_spmv_ms(R, px, flush)
+            R.close()
+        M.close()
+        out[name] = r
+    # a mesh with a scrambled numbering: the order gives its locality back
+    L = W.laplacian_2d(2048)
+    M = gb.CsrMatrix.from_host(L)
+    sp = torch.from_numpy(np.argsort(W.rand_u64(9, 30, 0, L.nrows), kind="stable")
+                          .astype(np.int32)).cuda()
+    S = M.permute(sp, sp)
+    S.cuthillmckee()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    p = S.cuthillmckee()
+    torch.cuda.synchronize()
+    t_dev = time.perf_counter() - t0
+    R = S.permute(p, p)
+    xd = torch.from_numpy(W.dense_x(L.nrows, 4)).cuda()
+    out["laplace_2048_scrambled"] = {
+        "n": L.nrows, "nnz": L.nnz, "device_ms": t_dev * 1e3,
+        "spmv_f64_natural": _device_spmv_ms(M, xd, flush),
+        "spmv_f64_scrambled": _device_spmv_ms(S, xd, flush),
+        "spmv_f64_reordered": _device_spmv_ms(R, xd, flush)}
+    for X in (R, S, M):
+        X.close()
+    return out
+
+
 def loader_extra(n=2_000_000, nnz=32_000_000, seed=9):
     """CSR text loader: a power-law matrix written in the reference's CSR
     format (%g values), then read by gooseberry_read_sparse_matrix_f64 (all
@@ -845,6 +941,7 @@ def run_extras(args):
     ex["spmv_uniform_100k"] = spmv_extra("spmv_uniform", A, W.dense_x(A.ncols, 1), peak, flush)
     A = W.powerlaw_rows(8_000_000, 128_000_000, seed=3, cap=200_000)
     ex["spmv_powerlaw_8m"] = spmv_extra("spmv_powerlaw", A, W.dense_x(A.ncols, 3), peak, flush)
+    ex["rcm_reorder"] = rcm_extra(A, flush)
     del A
     ex["mixed_cg_3d_160"] = mixed_extra()
     ex["serving_stream"] = serving_extra(nreq=args.requests)
@@ -926,6 +1023,12 @@ def main():
             out = {"extras": {"csr_loader_2m": loader_extra()}}
         elif args.workload == "pagerank":
             out = {"extras": {"pagerank_powerlaw_2m": pagerank_extra()}}
+        elif args.workload == "rcm":
+            import torch
+            flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+            from gooseberry_b200 import workloads as W
+            A = W.powerlaw_rows(8_000_000, 128_000_000, seed=3, cap=200_000)
+            out = {"extras": {"rcm_reorder": rcm_extra(A, flush)}}
         else:
             raise SystemExit(f"unknown workload {args.workload}")
         if dist.rank == 0:

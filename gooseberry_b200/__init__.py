@@ -34,7 +34,8 @@ __all__ = [
     "permute_vector",
     "CsrMatrix", "CgSolver", "CgResult", "dot", "spdot", "SUCCESS",
     "SCHED_AUTO", "SCHED_THREAD", "SCHED_GROUP4", "SCHED_GROUP8", "SCHED_WARP",
-    "SCHED_MERGE", "SCHED_ROW", "SCHED_WTILE", "SCHED_WMERGE", "CG_F64", "CG_MIXED", "plan_tiles",
+    "SCHED_MERGE", "SCHED_ROW", "SCHED_WTILE", "SCHED_WMERGE", "CG_F64", "CG_MIXED",
+    "CG_PLAIN_ENTRIES", "plan_tiles",
     "Server", "ServerResult",
 ]
 
@@ -53,6 +54,7 @@ SCHED_NAMES = {0: "auto", 1: "thread", 2: "group4", 3: "group8", 4: "warp", 5: "
                6: "row", 7: "wtile", 8: "wmerge"}
 CG_F64, CG_MIXED = 0, 1
 CG_PERSISTENT = 0x100
+CG_PLAIN_ENTRIES = 0x200
 CG_STATUS = {0: "converged", 1: "maxiter", 2: "breakdown", 3: "nonfinite"}
 
 
@@ -132,6 +134,7 @@ SIGNATURES = {
     "gb_cg_destroy": (_i, [_vp]),
     "gb_cg_solve": (_i, [_vp, _vp, _vp, _d, _i, _sz, _vp, _sz, _vp, _vp]),
     "gb_cg_profile": (_i, [_vp, _vp, _sz, _vp, _sz, _vp, _vp]),
+    "gb_cg_entry_bytes": (_i, [_vp, _vp]),
     "gb_server_create": (_i, [_vp, _vp]),
     "gb_server_destroy": (_i, [_vp]),
     "gb_server_submit": (_i, [_vp, C.c_uint64, _u32, _vp, _vp, _vp, _vp, _vp, _d, _sz]),
@@ -572,10 +575,12 @@ class CgResult:
 class CgSolver:
     """CG workspace bound to one matrix (``gb_cg_t``)."""
 
-    def __init__(self, A: CsrMatrix, mode: int = CG_F64, persistent: bool = False):
+    def __init__(self, A: CsrMatrix, mode: int = CG_F64, persistent: bool = False,
+                 plain_entries: bool = False):
         self.A = A
         h = C.c_void_p()
-        flags = mode | (CG_PERSISTENT if persistent else 0)
+        flags = mode | (CG_PERSISTENT if persistent else 0) | (
+            CG_PLAIN_ENTRIES if plain_entries else 0)
         _check(lib().gb_cg_create(A._h, flags, C.addressof(h)), "gb_cg_create")
         self._h = h
 
@@ -605,6 +610,12 @@ class CgSolver:
         if history:
             return x, out, hist[: res.iterations]
         return x, out
+
+    def entry_bytes(self) -> int:
+        """Bytes per matrix entry the solver's SpMV streams (12 = plain CSR)."""
+        v = C.c_size_t(0)
+        _check(lib().gb_cg_entry_bytes(self._h, C.addressof(v)), "gb_cg_entry_bytes")
+        return int(v.value)
 
     def profile(self, b, iterations: int = 20, stream=None):
         """Mean device time (ms) of each kernel of one iteration, timed launch

@@ -11,13 +11,18 @@
 //        partial  += p_new[i] * Ap[i]
 //      The gathered p values are recomputed from r and p_old with the same
 //      fma, so they equal p_new bit for bit; p is double-buffered so no CTA
-//      reads a p value another CTA has already overwritten.  The last CTA to
-//      finish (atomic ticket) sums the per-CTA partials in CTA order and
-//      sets alpha = rr / p.Ap.
+//      reads a p value another CTA has already overwritten.
 //   B  (solution / residual update + r.r)
 //        x += alpha p_new;  r -= alpha Ap;  partial += r.r
-//      The last CTA sets rr, beta = rr_new / rr, records ||r|| and decides
-//      whether to stop (||r|| <= tol, iteration limit, breakdown, NaN).
+//
+// Each kernel ends by writing one partial sum per CTA, and EVERY CTA of the
+// next kernel sums the previous kernel's partials itself, in CTA order:
+// B forms p.Ap and alpha = rr / p.Ap; A forms rr from the last B (and the rr
+// before it from the B before, kept in a second partial buffer), beta,
+// records ||r|| and decides whether to stop (||r|| <= tol, iteration limit,
+// NaN; B: breakdown).  All CTAs hold the same numbers because they add the
+// same partials in the same order, so no kernel has a serial last-CTA step
+// on the critical path.
 //
 // Both kernels return at once when the device-side stop flag is set, so a
 // CUDA graph of K iterations can be replayed blindly: the host only reads
@@ -30,6 +35,7 @@
 // (src/cgd.c:87,115-119).
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "gb_internal.h"
@@ -47,8 +53,10 @@ struct CgState {
   double tol;        // absolute bound on ||r||_2
   double bnorm;      // ||b||_2
   double pap;
-  unsigned long long iter;   // iterations done
+  unsigned long long iter;   // iterations done (written by B, read by A)
   unsigned long long niter;  // limit (0 = none)
+  unsigned long long kb;     // iteration of the running B (written by A)
+  double rrk[2];             // r.r of iteration k in rrk[k & 1] (written by A)
   int done;          // 1: stop
   int status;        // gb_cg_status_t
   unsigned int ticket_a;
@@ -67,6 +75,60 @@ struct CgStatus {
   double rr;
   double bnorm;
 };
+
+// Where A finds the r.r partials: B of iteration j writes buf[j & 1]
+// (stride entries apart), the init kernel writes buf[1]; count per buffer.
+struct RrPartials {
+  const double * buf;
+  unsigned count;
+  unsigned stride;
+};
+
+// The stop flag, read once per CTA so that all of its threads agree.
+__device__ __forceinline__ bool cta_done(const CgState * st) {
+  __shared__ int s_done;
+  if (threadIdx.x == 0) s_done = *reinterpret_cast<const volatile int *>(&st->done);
+  __syncthreads();
+  return s_done != 0;
+}
+
+// Start of A for iteration k = st->iter: rr_k from the last B, beta =
+// rr_k / rr_{k-1} (0 at k = 0; rr_{k-1} as the previous A recorded it), the
+// history entry and the stop test, which the reference makes after each
+// update (src/cgd.c:115-119).  CTA 0 records the outcome.  Returns false when
+// the solve stops here.
+__device__ __forceinline__ bool cg_a_begin(CgState * st, RrPartials rp, double * beta) {
+  __shared__ double red[32];
+  __shared__ double s_rr[2];
+  const unsigned long long k = *reinterpret_cast<const volatile unsigned long long *>(&st->iter);
+  const double rr = ordered_sum(rp.buf + ((k + 1) & 1) * rp.stride, rp.count, red);
+  if (threadIdx.x == 0) {
+    s_rr[0] = rr;
+    s_rr[1] = k > 0 ? __ldcg(&st->rrk[(k + 1) & 1]) : 0.0;
+  }
+  __syncthreads();
+  const double rrk = s_rr[0];
+  int stop = -1;
+  if (k > 0) {
+    const double rnorm = sqrt(rrk);
+    if (!(rnorm == rnorm) || isinf(rnorm)) stop = GB_CG_NONFINITE;
+    else if (rnorm <= st->tol) stop = GB_CG_CONVERGED;
+    else if (st->niter && k >= st->niter) stop = GB_CG_MAXITER;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && st->hist && k <= st->hist_len)
+      st->hist[k - 1] = rnorm;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->rr = rrk;
+    st->rrk[k & 1] = rrk;
+    st->kb = k;
+    if (stop >= 0) {
+      st->status = stop;
+      st->done = 1;
+    }
+  }
+  *beta = k > 0 ? rrk / s_rr[1] : 0.0;
+  return stop < 0;
+}
 
 // ---- A: SpMV with fused direction update and p.Ap -----------------------------
 
@@ -115,25 +177,8 @@ struct OutCgA {
   }
   __device__ __forceinline__ void finish() {
     __shared__ double red[32];
-    __shared__ bool last;
     const double s = block_sum(local, red);
     if (threadIdx.x == 0) partial[blockIdx.x] = s;
-    if (!arrive_last(&st->ticket_a, &last)) return;
-    __threadfence();
-    double tot = ordered_sum(partial, gridDim.x, red);
-    if (threadIdx.x == 0) {
-      for (unsigned q = 0; q < nlong; ++q) tot += __ldcg(longdot + q);
-      st->ticket_a = 0;
-      st->pap = tot;
-      const double rr = st->rr;
-      if (!(tot > 0.0)) {
-        st->done = 1;
-        st->status = (tot == tot && rr == rr) ? GB_CG_BREAKDOWN : GB_CG_NONFINITE;
-        st->alpha = 0.0;
-      } else {
-        st->alpha = rr / tot;
-      }
-    }
   }
 };
 
@@ -143,10 +188,11 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_a_kern
     const double * __restrict__ val, const double * __restrict__ r,
     const double * __restrict__ pold, double * __restrict__ pnew,
     double * __restrict__ ap, double * __restrict__ longdot,
-    double * __restrict__ partial, CgState * st) {
+    double * __restrict__ partial, CgState * st, RrPartials rp) {
   pdl_wait_and_release();
-  if (*reinterpret_cast<volatile int *>(&st->done)) return;
-  const double beta = st->beta;
+  if (cta_done(st)) return;
+  double beta;
+  if (!cg_a_begin(st, rp, &beta)) return;
   GatherP g{r, pold, beta};
   // the row schedule finishes long rows through row() like any other row
   OutCgA o{ap, pnew, r, pold, longdot, partial, st, beta,
@@ -155,16 +201,62 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_a_kern
       rowind, val, g, o);
 }
 
+// The row-schedule A kernel over compressed entries (RowCodec): the same
+// sums, products and epilogue as cg_a_kernel<SCHED_ROW>, fewer bytes.
+template <class IC, class VC, bool HINT>
+__global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED_ROW>::value) cg_a_codec_kernel(
+    const PlanView plan, const uint32_t * __restrict__ rowptr, IC ic, VC vc,
+    const double * __restrict__ table, uint32_t ntable, const double * __restrict__ r,
+    const double * __restrict__ pold, double * __restrict__ pnew, double * __restrict__ ap,
+    double * __restrict__ longdot, double * __restrict__ partial, CgState * st, RrPartials rp) {
+  __shared__ double s_table[256];
+  if constexpr (std::is_same<VC, ValCode8>::value) {
+    for (uint32_t i = threadIdx.x; i < ntable; i += kSpmvBlock) s_table[i] = table[i];
+    __syncthreads();
+    vc.table = s_table;
+  }
+  pdl_wait_and_release();
+  if (cta_done(st)) return;
+  double beta;
+  if (!cg_a_begin(st, rp, &beta)) return;
+  GatherP g{r, pold, beta};
+  OutCgA o{ap, pnew, r, pold, longdot, partial, st, beta, 0u, 0.0};
+  spmv_row_loop_c<double, kRowStage>(blockIdx.x * kSpmvBlock + threadIdx.x, plan.nrows,
+      gridDim.x * kSpmvBlock, plan.ncols, rowptr, ic, vc, g, o, L2Pol<HINT>::stream(),
+      L2Pol<HINT>::keep());
+  o.finish();
+}
+
 // ---- B: x / r update and r.r ----------------------------------------------------
 
+// Every CTA first sums A's p.Ap partials (then the long-row terms) in order
+// and forms alpha = rr / p.Ap; CTA 0 records a breakdown (p.Ap <= 0) or NaN.
 __global__ void __launch_bounds__(kVecBlock, kSpmvMinBlocks) cg_b_kernel(size_t n,
     double * __restrict__ x, double * __restrict__ r, const double * __restrict__ p,
-    const double * __restrict__ ap, double * __restrict__ partial, CgState * st) {
+    const double * __restrict__ ap, const double * __restrict__ partial_a, unsigned na,
+    const double * __restrict__ longdot, unsigned nlong, double * __restrict__ partial_b,
+    unsigned stride, CgState * st) {
   pdl_wait_and_release();
-  if (*reinterpret_cast<volatile int *>(&st->done)) return;
+  if (cta_done(st)) return;
   __shared__ double red[32];
-  __shared__ bool last;
-  const double alpha = st->alpha;
+  __shared__ double s_pap;
+  const unsigned long long k = st->kb;
+  const double rr_cur = st->rr;
+  double tot = ordered_sum(partial_a, na, red);
+  if (threadIdx.x == 0) {
+    for (unsigned q = 0; q < nlong; ++q) tot += __ldcg(longdot + q);
+    s_pap = tot;
+  }
+  __syncthreads();
+  const double pap = s_pap;
+  if (!(pap > 0.0)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      st->status = (pap == pap && rr_cur == rr_cur) ? GB_CG_BREAKDOWN : GB_CG_NONFINITE;
+      st->done = 1;
+    }
+    return;
+  }
+  const double alpha = rr_cur / pap;
   // contiguous chunk per CTA (2-element units, 16-byte aligned pairs)
   const size_t units = (n + 1) / 2;
   const size_t q = units / gridDim.x, rem = units % gridDim.x;
@@ -212,30 +304,8 @@ __global__ void __launch_bounds__(kVecBlock, kSpmvMinBlocks) cg_b_kernel(size_t 
     acc += rn * rn;
   }
   const double s = block_sum(acc, red);
-  if (threadIdx.x == 0) partial[blockIdx.x] = s;
-  if (!arrive_last(&st->ticket_b, &last)) return;
-  __threadfence();
-  const double rr = ordered_sum(partial, gridDim.x, red);
-  if (threadIdx.x == 0) {
-    st->ticket_b = 0;
-    const double rr_old = st->rr;
-    st->beta = rr / rr_old;
-    st->rr = rr;
-    const unsigned long long it = st->iter + 1;
-    st->iter = it;
-    const double rnorm = sqrt(rr);
-    if (st->hist && it <= st->hist_len) st->hist[it - 1] = rnorm;
-    if (!(rnorm == rnorm) || isinf(rnorm)) {
-      st->done = 1;
-      st->status = GB_CG_NONFINITE;
-    } else if (rnorm <= st->tol) {
-      st->done = 1;
-      st->status = GB_CG_CONVERGED;
-    } else if (st->niter && it >= st->niter) {
-      st->done = 1;
-      st->status = GB_CG_MAXITER;
-    }
-  }
+  if (threadIdx.x == 0) partial_b[(k & 1) * stride + blockIdx.x] = s;
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->iter = k + 1;
 }
 
 // ---- init: x = 0, r = b, p = 0, rr = b.b -----------------------------------------
@@ -293,7 +363,7 @@ size_t spmv_smem(int sched, uint32_t tile_items) {
 
 template <int SCHED, bool HINT>
 int launch_cg_a_t(const gb_csr & a, const double * r, const double * pold, double * pnew,
-    double * ap, double * longdot, double * partial, CgState * st, unsigned grid,
+    double * ap, double * longdot, double * partial, CgState * st, RrPartials rp, unsigned grid,
     cudaStream_t s, bool pdl) {
   const size_t smem = spmv_smem(SCHED, a.plan.tile_items);
   auto kern = cg_a_kernel<SCHED, HINT>;
@@ -301,47 +371,104 @@ int launch_cg_a_t(const gb_csr & a, const double * r, const double * pold, doubl
     GB_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void *>(kern),
         cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   GB_CUDA_TRY(launch_k(kern, grid, kSpmvBlock, smem, s, pdl, plan_view(a), a.rowptr,
-      a.rowind, a.val64, r, pold, pnew, ap, longdot, partial, st));
+      a.rowind, a.val64, r, pold, pnew, ap, longdot, partial, st, rp));
   return GOOSEBERRY_SUCCESS;
 }
 
 template <bool HINT>
 int launch_cg_a_h(const gb_csr & a, int sched, const double * r, const double * pold,
     double * pnew, double * ap, double * longdot, double * partial, CgState * st,
-    unsigned grid, cudaStream_t s, bool pdl) {
+    RrPartials rp, unsigned grid, cudaStream_t s, bool pdl) {
   switch (sched) {
     case GB_SCHED_THREAD:
-      return launch_cg_a_t<SCHED_THREAD, HINT>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
-          pdl);
+      return launch_cg_a_t<SCHED_THREAD, HINT>(a, r, pold, pnew, ap, longdot, partial, st, rp, grid,
+          s, pdl);
     case GB_SCHED_GROUP4:
-      return launch_cg_a_t<SCHED_GROUP4, HINT>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
-          pdl);
+      return launch_cg_a_t<SCHED_GROUP4, HINT>(a, r, pold, pnew, ap, longdot, partial, st, rp, grid,
+          s, pdl);
     case GB_SCHED_GROUP8:
-      return launch_cg_a_t<SCHED_GROUP8, HINT>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
-          pdl);
+      return launch_cg_a_t<SCHED_GROUP8, HINT>(a, r, pold, pnew, ap, longdot, partial, st, rp, grid,
+          s, pdl);
     case GB_SCHED_WARP:
-      return launch_cg_a_t<SCHED_WARP, HINT>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
-          pdl);
+      return launch_cg_a_t<SCHED_WARP, HINT>(a, r, pold, pnew, ap, longdot, partial, st, rp, grid,
+          s, pdl);
     case GB_SCHED_ROW:
-      return launch_cg_a_t<SCHED_ROW, HINT>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
-          pdl);
+      return launch_cg_a_t<SCHED_ROW, HINT>(a, r, pold, pnew, ap, longdot, partial, st, rp, grid,
+          s, pdl);
     case GB_SCHED_WTILE:
-      return launch_cg_a_t<SCHED_WTILE, HINT>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
-          pdl);
+      return launch_cg_a_t<SCHED_WTILE, HINT>(a, r, pold, pnew, ap, longdot, partial, st, rp, grid,
+          s, pdl);
     default:
-      return launch_cg_a_t<SCHED_MERGE, HINT>(a, r, pold, pnew, ap, longdot, partial, st, grid, s,
-          pdl);
+      return launch_cg_a_t<SCHED_MERGE, HINT>(a, r, pold, pnew, ap, longdot, partial, st, rp, grid,
+          s, pdl);
   }
 }
 
 // The A kernel with L2-policy loads (hint) or plain loads.
 int launch_cg_a(const gb_csr & a, int sched, bool hint, const double * r, const double * pold,
     double * pnew, double * ap, double * longdot, double * partial, CgState * st,
-    unsigned grid, cudaStream_t s, bool pdl) {
-  return hint ? launch_cg_a_h<true>(a, sched, r, pold, pnew, ap, longdot, partial, st, grid, s,
-                                    pdl)
-              : launch_cg_a_h<false>(a, sched, r, pold, pnew, ap, longdot, partial, st, grid,
-                                     s, pdl);
+    RrPartials rp, unsigned grid, cudaStream_t s, bool pdl) {
+  return hint ? launch_cg_a_h<true>(a, sched, r, pold, pnew, ap, longdot, partial, st, rp, grid,
+                                    s, pdl)
+              : launch_cg_a_h<false>(a, sched, r, pold, pnew, ap, longdot, partial, st, rp,
+                                     grid, s, pdl);
+}
+
+template <class IC, class VC, bool HINT>
+int launch_cg_a_codec_t(const gb_csr & a, const RowCodec & c, const double * r,
+    const double * pold, double * pnew, double * ap, double * longdot, double * partial,
+    CgState * st, RrPartials rp, unsigned grid, cudaStream_t s, bool pdl, int * occ) {
+  IC ic{};
+  VC vc{};
+  if constexpr (std::is_same<IC, ColD16>::value) ic.p = c.col16; else ic.p = a.rowind;
+  if constexpr (std::is_same<VC, ValCode8>::value) {
+    vc.p = c.code8;
+    vc.table = nullptr;
+  } else if constexpr (std::is_same<VC, ValPlain<float>>::value) {
+    vc.p = c.val32;
+  } else {
+    vc.p = a.val64;
+  }
+  auto kern = cg_a_codec_kernel<IC, VC, HINT>;
+  if (occ) {  // occupancy query only
+    GB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, kSpmvBlock, 0));
+    return GOOSEBERRY_SUCCESS;
+  }
+  GB_CUDA_TRY(launch_k(kern, grid, kSpmvBlock, 0, s, pdl, plan_view(a), a.rowptr, ic, vc,
+      static_cast<const double *>(c.table), c.ntable, r, pold, pnew, ap, longdot, partial, st,
+      rp));
+  return GOOSEBERRY_SUCCESS;
+}
+
+template <class IC, bool HINT>
+int launch_cg_a_codec_v(const gb_csr & a, const RowCodec & c, const double * r,
+    const double * pold, double * pnew, double * ap, double * longdot, double * partial,
+    CgState * st, RrPartials rp, unsigned grid, cudaStream_t s, bool pdl, int * occ) {
+  if (c.code8)
+    return launch_cg_a_codec_t<IC, ValCode8, HINT>(a, c, r, pold, pnew, ap, longdot, partial,
+        st, rp, grid, s, pdl, occ);
+  if (c.val32)
+    return launch_cg_a_codec_t<IC, ValPlain<float>, HINT>(a, c, r, pold, pnew, ap, longdot,
+        partial, st, rp, grid, s, pdl, occ);
+  return launch_cg_a_codec_t<IC, ValPlain<double>, HINT>(a, c, r, pold, pnew, ap, longdot,
+      partial, st, rp, grid, s, pdl, occ);
+}
+
+// The row-schedule A kernel over the solver's compressed entries (occ != null:
+// only its occupancy).
+int launch_cg_a_codec(const gb_csr & a, const RowCodec & c, bool hint, const double * r,
+    const double * pold, double * pnew, double * ap, double * longdot, double * partial,
+    CgState * st, RrPartials rp, unsigned grid, cudaStream_t s, bool pdl,
+    int * occ = nullptr) {
+  if (c.col16)
+    return hint ? launch_cg_a_codec_v<ColD16, true>(a, c, r, pold, pnew, ap, longdot, partial,
+                                                     st, rp, grid, s, pdl, occ)
+                : launch_cg_a_codec_v<ColD16, false>(a, c, r, pold, pnew, ap, longdot,
+                                                      partial, st, rp, grid, s, pdl, occ);
+  return hint ? launch_cg_a_codec_v<ColU32, true>(a, c, r, pold, pnew, ap, longdot, partial, st,
+                                                   rp, grid, s, pdl, occ)
+              : launch_cg_a_codec_v<ColU32, false>(a, c, r, pold, pnew, ap, longdot, partial,
+                                                    st, rp, grid, s, pdl, occ);
 }
 
 template <int SCHED>
@@ -661,8 +788,8 @@ struct gb_cg {
   double * p[2] = {nullptr, nullptr};
   double * ap = nullptr;
   double * partial_a = nullptr;
-  double * partial_b = nullptr;
-  double * partial_i = nullptr;
+  double * partial_b = nullptr;  // two buffers of pstride (B of even / odd iterations)
+  unsigned pstride = 0;
   double * longdot = nullptr;
   gb::CgState * st = nullptr;
   gb::CgStatus * host_status = nullptr;  // pinned, [2] slots
@@ -681,6 +808,8 @@ struct gb_cg {
   unsigned * sync = nullptr;  // [0] barrier counter, [1] abort flag
   int keep_l2 = 0;
   bool l2_hint = false;  // A kernel with L2-policy loads (working set fits in L2)
+  bool use_codec = false;  // row schedule over compressed entries
+  gb::RowCodec codec;
   gb::MixedCg * mixed = nullptr;  // GB_CG_MIXED solver (owns its workspace)
 };
 
@@ -691,6 +820,7 @@ void destroy_cg(gb_cg * s) {
   if (!s) return;
   cudaDeviceSynchronize();  // its memory goes back to the pool below
   mixed_destroy(s->mixed);
+  free_row_codec(s->codec);
   for (auto & g : s->graph)
     if (g) cudaGraphExecDestroy(g);
   if (s->cap_stream) cudaStreamDestroy(s->cap_stream);
@@ -701,13 +831,34 @@ void destroy_cg(gb_cg * s) {
   dev_free(s->ap);
   dev_free(s->partial_a);
   dev_free(s->partial_b);
-  dev_free(s->partial_i);
   dev_free(s->longdot);
   dev_free(s->st);
   dev_free(s->cta_tiles);
   dev_free(s->sync);
   if (s->host_status) cudaFreeHost(s->host_status);
   delete s;
+}
+
+RrPartials rr_partials(const gb_cg * s) {
+  return RrPartials{s->partial_b, s->grid_b, s->pstride};
+}
+
+int launch_a(gb_cg * s, const double * pold, double * pnew, cudaStream_t cs, bool pdl) {
+  return s->use_codec
+             ? launch_cg_a_codec(*s->a, s->codec, s->l2_hint, s->r, pold, pnew, s->ap,
+                   s->longdot, s->partial_a, s->st, rr_partials(s), s->grid_a, cs, pdl)
+             : launch_cg_a(*s->a, s->sched, s->l2_hint, s->r, pold, pnew, s->ap, s->longdot,
+                   s->partial_a, s->st, rr_partials(s), s->grid_a, cs, pdl);
+}
+
+int launch_b(gb_cg * s, const double * pnew, cudaStream_t cs, bool pdl) {
+  // the row schedule sums long rows like any other row: no long-row terms
+  const unsigned nlong = s->sched == GB_SCHED_ROW ? 0u
+                         : static_cast<unsigned>(s->a->plan.longrows.size());
+  GB_CUDA_TRY(launch_k(cg_b_kernel, s->grid_b, kVecBlock, 0, cs, pdl, s->n, s->x, s->r, pnew,
+      static_cast<const double *>(s->ap), static_cast<const double *>(s->partial_a), s->grid_a,
+      static_cast<const double *>(s->longdot), nlong, s->partial_b, s->pstride, s->st));
+  return GOOSEBERRY_SUCCESS;
 }
 
 // One chunk of iterations (A, B per iteration) and the status mirror into
@@ -717,13 +868,9 @@ int enqueue_chunk(gb_cg * s, int slot, cudaStream_t cs) {
   for (int k = 0; k < s->chunk && rc == GOOSEBERRY_SUCCESS; ++k) {
     const double * pold = s->p[k & 1];
     double * pnew = s->p[(k + 1) & 1];
-    rc = launch_cg_a(*s->a, s->sched, s->l2_hint, s->r, pold, pnew, s->ap, s->longdot, s->partial_a,
-        s->st, s->grid_a, cs, k > 0);
+    rc = launch_a(s, pold, pnew, cs, k > 0);
     if (rc != GOOSEBERRY_SUCCESS) break;
-    if (launch_k(cg_b_kernel, s->grid_b, kVecBlock, 0, cs, true, s->n, s->x, s->r,
-            static_cast<const double *>(pnew), static_cast<const double *>(s->ap),
-            s->partial_b, s->st) != cudaSuccess)
-      rc = GOOSEBERRY_ERROR_UNKNOWN;
+    rc = launch_b(s, pnew, cs, true);
   }
   if (rc == GOOSEBERRY_SUCCESS) {
     // status mirror: done, status, iter, rr, bnorm
@@ -834,7 +981,8 @@ int create_cg(const gb_csr * a, int mode, gb_cg * s) {
   GB_CHECK_INPUT(a->nrows == a->ncols, "CG needs a square matrix, got %ux%u", a->nrows,
       a->ncols);
   const bool want_persistent = (mode & GB_CG_PERSISTENT) != 0;
-  mode &= ~GB_CG_PERSISTENT;
+  const bool plain_entries = (mode & GB_CG_PLAIN_ENTRIES) != 0;
+  mode &= ~(GB_CG_PERSISTENT | GB_CG_PLAIN_ENTRIES);
   GB_CHECK_INPUT(mode == GB_CG_F64 || mode == GB_CG_MIXED, "unknown CG mode %d", mode);
   if (mode == GB_CG_MIXED) {
     s->a = a;
@@ -854,12 +1002,24 @@ int create_cg(const gb_csr * a, int mode, gb_cg * s) {
   GB_TRY(dev_alloc(&s->ap, n * sizeof(double)));
   s->sched = a->sched64;
   s->tile_items = a->plan.tile_items;
+  // the row schedule reads compressed entries when the matrix allows it
+  // (banded columns, few distinct or float-exact values)
+  size_t entry_bytes = 12;
+  if (s->sched == GB_SCHED_ROW && !want_persistent && !plain_entries) {
+    GB_TRY(build_row_codec(*a, &s->codec, nullptr));
+    s->use_codec = s->codec.col16 || s->codec.code8 || s->codec.val32;
+    entry_bytes = s->codec.entry_bytes();
+  }
   // evict-first/evict-last hints keep an L2-sized working set (matrix, rowptr,
   // r, both p, Ap, x) resident across iterations; beyond L2 the plain loads win
-  GB_TRY(l2_fits(4ull * (s->n + 1) + 12ull * a->nnz + 40ull * s->n, &s->l2_hint));
+  GB_TRY(l2_fits(4ull * (s->n + 1) + entry_bytes * a->nnz + 40ull * s->n, &s->l2_hint));
   const size_t smem = spmv_smem(s->sched, a->plan.tile_items);
   int occ = 0;
-  GB_TRY(occupancy_cg_a_sched(s->sched, smem, &occ));
+  if (s->use_codec)
+    GB_TRY(launch_cg_a_codec(*a, s->codec, false, nullptr, nullptr, nullptr, nullptr, nullptr,
+        nullptr, nullptr, RrPartials{}, 0, nullptr, false, &occ));
+  else
+    GB_TRY(occupancy_cg_a_sched(s->sched, smem, &occ));
   GB_CHECK_INPUT(occ > 0, "CG kernel cannot be resident");
   const unsigned ntiles = static_cast<unsigned>(std::max<size_t>(a->plan.tiles.size(), 1));
   const unsigned work_a = spmv_work_units(s->sched, static_cast<uint32_t>(s->n), ntiles,
@@ -877,8 +1037,8 @@ int create_cg(const gb_csr * a, int mode, gb_cg * s) {
       static_cast<unsigned>(std::min<size_t>(a->plan.tiles.size() + 1,
           static_cast<size_t>(a->sm_count) * 32)));
   GB_TRY(dev_alloc(&s->partial_a, gmax * sizeof(double)));
-  GB_TRY(dev_alloc(&s->partial_b, gmax * sizeof(double)));
-  GB_TRY(dev_alloc(&s->partial_i, gmax * sizeof(double)));
+  GB_TRY(dev_alloc(&s->partial_b, 2 * static_cast<size_t>(gmax) * sizeof(double)));
+  s->pstride = gmax;
   GB_TRY(dev_alloc(&s->longdot,
       std::max<size_t>(a->plan.longrows.size(), 1) * sizeof(double)));
   GB_TRY(dev_alloc(&s->st, sizeof(CgState)));
@@ -906,8 +1066,9 @@ int start_solve(gb_cg * s, const double * b, double tol, int tol_relative, size_
   init.hist_len = hl;
   GB_CUDA_TRY(cudaMemcpyAsync(s->st, &init, sizeof(CgState), cudaMemcpyHostToDevice, stream));
   if (s->persistent) return launch_persistent(s, b, tol_relative, stream);
+  // its r.r partials land where A of iteration 0 looks (the odd B buffer)
   cg_init_kernel<<<s->grid_b, kVecBlock, 0, stream>>>(s->n, b, s->x, s->r, s->p[0],
-      s->partial_i, s->st, tol_relative);
+      s->partial_b + s->pstride, s->st, tol_relative);
   GB_CUDA_TRY(cudaGetLastError());
   return GOOSEBERRY_SUCCESS;
 }
@@ -1034,11 +1195,9 @@ int profile_cg(gb_cg * s, const double * b, size_t iterations, double * ms, size
     const double * pold = s->p[k & 1];
     double * pnew = s->p[(k + 1) & 1];
     cudaEventRecord(ev[3 * k], stream);
-    rc = launch_cg_a(*s->a, s->sched, s->l2_hint, s->r, pold, pnew, s->ap, s->longdot, s->partial_a,
-        s->st, s->grid_a, stream, false);
+    rc = launch_a(s, pold, pnew, stream, false);
     cudaEventRecord(ev[3 * k + 1], stream);
-    cg_b_kernel<<<s->grid_b, kVecBlock, 0, stream>>>(s->n, s->x, s->r, pnew, s->ap,
-        s->partial_b, s->st);
+    if (rc == GOOSEBERRY_SUCCESS) rc = launch_b(s, pnew, stream, false);
     cudaEventRecord(ev[3 * k + 2], stream);
   }
   cudaError_t e = cudaStreamSynchronize(stream);
@@ -1091,6 +1250,12 @@ int gb_cg_solve(gb_cg_t * s, const double * b, double * x, double tol, int tol_r
   GB_CHECK_INPUT(s != nullptr, "solver is NULL");
   return gb::solve_cg(s, b, x, tol, tol_relative, niter, history, history_len, result,
       static_cast<cudaStream_t>(stream));
+}
+
+int gb_cg_entry_bytes(const gb_cg_t * s, size_t * bytes) {
+  GB_CHECK_INPUT(s != nullptr && bytes != nullptr, "NULL argument");
+  *bytes = s->mixed ? 8 : (s->use_codec ? s->codec.entry_bytes() : 12);
+  return GOOSEBERRY_SUCCESS;
 }
 
 int gb_cg_profile(gb_cg_t * s, const double * b, size_t iterations, double * ms,

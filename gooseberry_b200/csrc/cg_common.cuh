@@ -49,15 +49,24 @@ __device__ __forceinline__ bool arrive_last(unsigned int * ticket, bool * flag) 
   return *flag;
 }
 
-// Sum of partial[0..n) in index order, by one CTA; result valid in thread 0.
+// Sum of partial[0..n) in a fixed order (for a given n and CTA size), by one
+// CTA; result valid in thread 0.  Thread t adds entries t, t + blockDim.x,
+// ... (all loads of a batch issued before the adds), then the warp tree and
+// the per-warp sums in warp order.
 __device__ __forceinline__ double ordered_sum(const double * partial, unsigned n,
     double * red) {
-  // each thread sums a contiguous run, then runs are summed in thread order
-  const unsigned per = (n + blockDim.x - 1) / blockDim.x;
-  const unsigned s = min(n, threadIdx.x * per), e = min(n, s + per);
+  constexpr int U = 8;
   double acc = 0.0;
-  for (unsigned i = s; i < e; ++i) acc += __ldcg(partial + i);
-  // ordered combine: warp tree is order-fixed as well
+  for (unsigned base = 0; base < n; base += U * blockDim.x) {
+    double v[U];
+#pragma unroll
+    for (int j = 0; j < U; ++j) {
+      const unsigned i = base + j * blockDim.x + threadIdx.x;
+      v[j] = i < n ? __ldcg(partial + i) : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < U; ++j) acc += v[j];
+  }
   return block_sum(acc, red);
 }
 

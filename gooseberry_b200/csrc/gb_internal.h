@@ -183,6 +183,22 @@ int dev_alloc(T ** p, size_t bytes) {
 int csr_adopt(uint32_t nrows, uint32_t ncols, uint32_t nnz, uint32_t * rowptr,
     uint32_t * rowind, double * val64, float * val32, cudaStream_t stream, gb_csr ** out);
 
+// Lossless compressed entries for the row schedule (codec.cu): columns as
+// int16 distances from the row, values as 8-bit codes into a table of the
+// distinct values or as exact floats.  Null members are not available.
+struct RowCodec {
+  int16_t * col16 = nullptr;  // col - row
+  uint8_t * code8 = nullptr;  // code of each value
+  double * table = nullptr;   // [ntable] distinct values
+  uint32_t ntable = 0;
+  float * val32 = nullptr;    // (float)value, equal to the double
+  size_t entry_bytes() const {
+    return (col16 ? 2 : 4) + (code8 ? 1 : (val32 ? 4 : 8));
+  }
+};
+int build_row_codec(const gb_csr & a, RowCodec * c, cudaStream_t s);
+void free_row_codec(RowCodec & c);
+
 // Mixed-precision CG (cg_mixed.cu), owned by a gb_cg created with GB_CG_MIXED.
 struct MixedCg;
 int mixed_create(const gb_csr * a, MixedCg ** out);

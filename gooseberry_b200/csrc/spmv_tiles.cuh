@@ -459,39 +459,110 @@ struct MinBlocks {
                                                        : kSpmvMinBlocks;
 };
 
-template <typename V, int STAGE>
-struct RowStage {
-  uint32_t b = 0, e = 0;
-  uint32_t c[STAGE];
-  V v[STAGE];
+// ---- entry codecs of the row schedule ------------------------------------------
+//
+// How a row-schedule kernel reads entry k of the matrix.  Besides the plain
+// CSR arrays, two lossless encodings shrink the matrix stream (after the
+// index and value compression of Kourtis, Goumas and Koziris, "Optimizing
+// sparse matrix-vector multiplication using index and value compression",
+// CF 2008): a column stored as its signed 16-bit distance from the row
+// (when every entry lies within 32767 of the diagonal), and a value stored as
+// an 8-bit code into a table of the matrix's distinct values (when it has at
+// most 256).  A value stored as float when the float equals the double
+// exactly is ValPlain<float> widened to double.  Decoding gives back the exact
+// column and double, so results are bit-identical to the plain arrays.
+
+__device__ __forceinline__ int32_t ld_l1_s16(const int16_t * p, uint64_t pol) {
+  int32_t v;
+  asm volatile("ld.global.nc.L2::cache_hint.s16 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ int32_t ld_l1_s16(const int16_t * p, NoHint) {
+  int32_t v;
+  asm volatile("ld.global.nc.s16 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ uint32_t ld_l1_u8(const uint8_t * p, uint64_t pol) {
+  uint32_t v;
+  asm volatile("ld.global.nc.L2::cache_hint.u8 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ uint32_t ld_l1_u8(const uint8_t * p, NoHint) {
+  uint32_t v;
+  asm volatile("ld.global.nc.u8 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+
+struct ColU32 {  // the CSR column array
+  const uint32_t * p;
+  using Raw = uint32_t;
+  template <class P>
+  __device__ __forceinline__ Raw load(uint32_t k, P pol) const { return ld_l1(p + k, pol); }
+  __device__ __forceinline__ uint32_t col(Raw r, uint32_t) const { return r; }
 };
 
-template <typename V, int STAGE, class P>
-__device__ __forceinline__ void row_stage_load(RowStage<V, STAGE> & s, const uint32_t * rowind,
-    const V * val, P pol) {
+struct ColD16 {  // column - row, 16-bit
+  const int16_t * p;
+  using Raw = int32_t;
+  template <class P>
+  __device__ __forceinline__ Raw load(uint32_t k, P pol) const { return ld_l1_s16(p + k, pol); }
+  __device__ __forceinline__ uint32_t col(Raw r, uint32_t row) const {
+    return row + static_cast<uint32_t>(r);
+  }
+};
+
+template <typename V>
+struct ValPlain {  // values as stored (float widens exactly to double)
+  const V * p;
+  using Raw = V;
+  template <class P>
+  __device__ __forceinline__ Raw load(uint32_t k, P pol) const { return ld_l1(p + k, pol); }
+  template <typename Acc>
+  __device__ __forceinline__ Acc value(Raw r) const { return static_cast<Acc>(r); }
+};
+
+struct ValCode8 {  // 8-bit code into the distinct-value table (shared memory)
+  const uint8_t * p;
+  const double * table;
+  using Raw = uint32_t;
+  template <class P>
+  __device__ __forceinline__ Raw load(uint32_t k, P pol) const { return ld_l1_u8(p + k, pol); }
+  template <typename Acc>
+  __device__ __forceinline__ Acc value(Raw r) const { return static_cast<Acc>(table[r]); }
+};
+
+template <class IC, class VC, int STAGE>
+struct RowStage {
+  uint32_t b = 0, e = 0;
+  typename IC::Raw c[STAGE];
+  typename VC::Raw v[STAGE];
+};
+
+template <class IC, class VC, int STAGE, class P>
+__device__ __forceinline__ void row_stage_load(RowStage<IC, VC, STAGE> & s, const IC & ic,
+    const VC & vc, P pol) {
 #pragma unroll
   for (int j = 0; j < STAGE; ++j) {
     if (s.b + j < s.e) {
-      s.c[j] = ld_l1(rowind + s.b + j, pol);
-      s.v[j] = ld_l1(val + s.b + j, pol);
+      s.c[j] = ic.load(s.b + j, pol);
+      s.v[j] = vc.load(s.b + j, pol);
     }
   }
 }
 
-template <typename V, typename Acc, int STAGE = kRowStage, class Gather, class Out, class PM,
+template <typename Acc, int STAGE, class IC, class VC, class Gather, class Out, class PM,
     class PX>
-__device__ __forceinline__ void spmv_row_loop(uint32_t first, uint32_t end, uint32_t step,
-    uint32_t ncols, const uint32_t * __restrict__ rowptr,
-    const uint32_t * __restrict__ rowind, const V * __restrict__ val, const Gather & gather,
-    Out & out, PM pol_matrix, PX pol_x) {
+__device__ __forceinline__ void spmv_row_loop_c(uint32_t first, uint32_t end, uint32_t step,
+    uint32_t ncols, const uint32_t * __restrict__ rowptr, const IC & ic, const VC & vc,
+    const Gather & gather, Out & out, PM pol_matrix, PX pol_x) {
   const uint32_t cmax = ncols - 1;
   if (first >= end) return;
   // stage L: row `first`; stage P: rowptr pair of row first + step
-  RowStage<V, STAGE> cur;
+  RowStage<IC, VC, STAGE> cur;
   cur.b = __ldg(rowptr + first);
   cur.e = __ldg(rowptr + first + 1);
   typename Out::Pre cur_pre = out.pre(first);
-  row_stage_load(cur, rowind, val, pol_matrix);
+  row_stage_load(cur, ic, vc, pol_matrix);
   uint32_t nb = 0, ne = 0;
   if (first + step < end) {
     nb = __ldg(rowptr + first + step);
@@ -499,14 +570,14 @@ __device__ __forceinline__ void spmv_row_loop(uint32_t first, uint32_t end, uint
   }
   for (uint32_t i = first; i < end; i += step) {
     // issue the next row's indices/values/operands and the rowptr two ahead
-    RowStage<V, STAGE> nxt;
+    RowStage<IC, VC, STAGE> nxt;
     typename Out::Pre nxt_pre{};
     const uint32_t i1 = i + step, i2 = i + 2 * step;
     if (i1 < end) {
       nxt.b = nb;
       nxt.e = ne;
       nxt_pre = out.pre(i1);
-      row_stage_load(nxt, rowind, val, pol_matrix);
+      row_stage_load(nxt, ic, vc, pol_matrix);
     }
     if (i2 < end) {
       nb = __ldg(rowptr + i2);
@@ -516,18 +587,30 @@ __device__ __forceinline__ void spmv_row_loop(uint32_t first, uint32_t end, uint
     Acc xv[STAGE];
 #pragma unroll
     for (int j = 0; j < STAGE; ++j)
-      if (cur.b + j < cur.e) xv[j] = gather(min(cur.c[j], cmax), pol_x);
+      if (cur.b + j < cur.e) xv[j] = gather(min(ic.col(cur.c[j], i), cmax), pol_x);
     Acc sum = Acc(0);
 #pragma unroll
     for (int j = 0; j < STAGE; ++j)
-      if (cur.b + j < cur.e) sum = add_rn(sum, mul_rn(static_cast<Acc>(cur.v[j]), xv[j]));
+      if (cur.b + j < cur.e)
+        sum = add_rn(sum, mul_rn(vc.template value<Acc>(cur.v[j]), xv[j]));
     for (uint32_t k = cur.b + STAGE; k < cur.e; ++k)  // long-row tail
-      sum = add_rn(sum, mul_rn(static_cast<Acc>(ld_l1(val + k, pol_matrix)),
-                               gather(min(ld_l1(rowind + k, pol_matrix), cmax), pol_x)));
+      sum = add_rn(sum, mul_rn(vc.template value<Acc>(vc.load(k, pol_matrix)),
+                               gather(min(ic.col(ic.load(k, pol_matrix), i), cmax), pol_x)));
     out.row_pre(i, sum, cur_pre);
     cur = nxt;
     cur_pre = nxt_pre;
   }
+}
+
+// The row loop over the plain CSR arrays.
+template <typename V, typename Acc, int STAGE = kRowStage, class Gather, class Out, class PM,
+    class PX>
+__device__ __forceinline__ void spmv_row_loop(uint32_t first, uint32_t end, uint32_t step,
+    uint32_t ncols, const uint32_t * __restrict__ rowptr,
+    const uint32_t * __restrict__ rowind, const V * __restrict__ val, const Gather & gather,
+    Out & out, PM pol_matrix, PX pol_x) {
+  spmv_row_loop_c<Acc, STAGE>(first, end, step, ncols, rowptr, ColU32{rowind},
+      ValPlain<V>{val}, gather, out, pol_matrix, pol_x);
 }
 
 // ---- per-warp tiles -----------------------------------------------------------

@@ -250,6 +250,16 @@ typedef enum gb_cg_mode {
  * every SM until the solve ends. */
 #define GB_CG_PERSISTENT 0x100
 
+/* The FP64 solver's SpMV on the row schedule normally reads a compressed copy
+ * of the matrix entries that it builds at create time when the matrix allows:
+ * columns as 16-bit distances from the row (every entry within 32767 of the
+ * diagonal) and values as 8-bit codes into a table (at most 256 distinct
+ * values) or as floats (every value exactly a float).  Decoding is exact, so
+ * results are bit-identical to the plain arrays; only the bytes streamed per
+ * iteration shrink.  OR this flag into the mode to read the plain CSR arrays
+ * instead. */
+#define GB_CG_PLAIN_ENTRIES 0x200
+
 typedef enum gb_cg_status {
   GB_CG_CONVERGED = 0,  /* ||r|| <= tolerance                                 */
   GB_CG_MAXITER = 1,    /* iteration limit reached first                      */
@@ -296,6 +306,12 @@ GOOSEBERRY_API int gb_cg_solve(gb_cg_t * s, const double * b, double * x, double
  */
 GOOSEBERRY_API int gb_cg_profile(gb_cg_t * s, const double * b, size_t iterations,
     double * ms, size_t ms_len, size_t * nkernels, gb_stream_t stream);
+
+/* Bytes per matrix entry the solver's SpMV streams: 12 for the plain arrays
+ * (4-byte column, 8-byte value), down to 3 for 16-bit columns with 8-bit value
+ * codes (see GB_CG_PLAIN_ENTRIES), 8 for the mixed solver's float values.
+ * No reference counterpart. */
+GOOSEBERRY_API int gb_cg_entry_bytes(const gb_cg_t * s, size_t * bytes);
 
 /* ---- batched solve server (continuous batching) ---------------------------- */
 
