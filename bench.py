@@ -241,7 +241,12 @@ def run_cg_laplace(args, dist: Dist):
 
     # live per-kernel timing (first iterations of a real solve)
     ms_a, ms_b = S.profile(bd, iterations=40)
-    bytes_a = 4 * (n + 1) + 12 * nnz + 32 * n   # rowptr, ind+val, r & p gathered, p & Ap written
+    # bytes per matrix entry the A kernel streams: 12 for plain CSR, 3 when the
+    # solver reads its lossless compressed copy (16-bit column distances,
+    # 8-bit codes into the table of distinct values)
+    entry_bytes = S.entry_bytes()
+    bytes_a = 4 * (n + 1) + entry_bytes * nnz + 32 * n  # rowptr, entries, r & p gathered, p & Ap written
+    bytes_a_csr = 4 * (n + 1) + 12 * nnz + 32 * n
     bytes_b = 48 * n                             # x, p, r, Ap read; x, r written
     bytes_textbook = 4 * (n + 1) + 12 * nnz + 14 * 8 * n
 
@@ -311,19 +316,26 @@ def run_cg_laplace(args, dist: Dist):
             "reference_iterations": reference_cg_iterations(),
             "schedule": gb.SCHED_NAMES[A.info().schedule],
             "tile_items": A.info().tile_items,
+            "matrix_bytes_per_entry": entry_bytes,
             "l2": "flushed between steps (256 MB write, outside the timed events)",
             "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "single GPU",
         },
         "roofline": {
-            "bound": "hbm", "kernel": "cg_a_kernel (SpMV + p update + p.Ap)",
+            "bound": "hbm",
+            "kernel": ("cg_a_codec_kernel (row schedule over the compressed entries; SpMV + "
+                       "p update + p.Ap)" if entry_bytes < 12 else
+                       "cg_a_kernel (SpMV + p update + p.Ap)"),
             "achieved": ach_a, "peak": peak, "unit": "GB/s", "frac": ach_a / peak,
-            "traffic": ncu_traffic("cg_a_laplace1024"),
+            "traffic": ncu_traffic("cg_a_codec_laplace1024" if entry_bytes < 12
+                                   else "cg_a_row_laplace1024"),
             "bytes_per_launch": bytes_a, "launch_ms": ms_a, "peak_source": peak_src,
+            "bytes_per_launch_as_plain_csr": bytes_a_csr,
         },
         "kernels": {
             "cg_a_ms": ms_a, "cg_b_ms": ms_b,
             "cg_b_gbs": bytes_b / (ms_b * 1e-3) / 1e9,
             "iteration_ms": (t_local / args.steps) / iters * 1e3,
+            "iteration_fused_gbs": (bytes_a + bytes_b) * iters * args.steps / t_local / 1e9,
             "iteration_textbook_gbs": bytes_textbook * iters * args.steps / t_local / 1e9,
             "bytes_per_iteration_fused": bytes_a + bytes_b,
             "bytes_per_iteration_textbook": bytes_textbook,

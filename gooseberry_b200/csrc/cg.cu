@@ -202,8 +202,10 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_a_kern
 }
 
 // The row-schedule A kernel over compressed entries (RowCodec): the same
-// sums, products and epilogue as cg_a_kernel<SCHED_ROW>, fewer bytes.
-template <class IC, class VC, bool HINT>
+// sums, products and epilogue as cg_a_kernel<SCHED_ROW>, fewer bytes.  STAGE
+// entries of a row ride in the register pipeline (sized to the longest row
+// when that is short: fewer predicated slots per row).
+template <class IC, class VC, bool HINT, int STAGE>
 __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED_ROW>::value) cg_a_codec_kernel(
     const PlanView plan, const uint32_t * __restrict__ rowptr, IC ic, VC vc,
     const double * __restrict__ table, uint32_t ntable, const double * __restrict__ r,
@@ -221,7 +223,7 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED_ROW>::value) cg_a_
   if (!cg_a_begin(st, rp, &beta)) return;
   GatherP g{r, pold, beta};
   OutCgA o{ap, pnew, r, pold, longdot, partial, st, beta, 0u, 0.0};
-  spmv_row_loop_c<double, kRowStage>(blockIdx.x * kSpmvBlock + threadIdx.x, plan.nrows,
+  spmv_row_loop_c<double, STAGE>(blockIdx.x * kSpmvBlock + threadIdx.x, plan.nrows,
       gridDim.x * kSpmvBlock, plan.ncols, rowptr, ic, vc, g, o, L2Pol<HINT>::stream(),
       L2Pol<HINT>::keep());
   o.finish();
@@ -429,7 +431,9 @@ int launch_cg_a_codec_t(const gb_csr & a, const RowCodec & c, const double * r,
   } else {
     vc.p = a.val64;
   }
-  auto kern = cg_a_codec_kernel<IC, VC, HINT>;
+  auto kern = c.stage == 5   ? cg_a_codec_kernel<IC, VC, HINT, 5>
+              : c.stage == 7 ? cg_a_codec_kernel<IC, VC, HINT, 7>
+                             : cg_a_codec_kernel<IC, VC, HINT, kRowStage>;
   if (occ) {  // occupancy query only
     GB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, kSpmvBlock, 0));
     return GOOSEBERRY_SUCCESS;

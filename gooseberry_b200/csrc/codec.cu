@@ -201,6 +201,7 @@ int build_values(const gb_csr & a, RowCodec * c, unsigned * flags, cudaStream_t 
 
 int build_row_codec(const gb_csr & a, RowCodec * c, cudaStream_t s) {
   *c = RowCodec{};
+  c->stage = a.plan.max_row <= 5 ? 5 : (a.plan.max_row <= 7 ? 7 : 6);
   if (a.nnz == 0 || !a.val64) return GOOSEBERRY_SUCCESS;
   unsigned * flags = nullptr;
   GB_TRY(scratch_alloc(reinterpret_cast<void **>(&flags), 16, s));
@@ -228,7 +229,9 @@ void free_row_codec(RowCodec & c) {
   if (c.code8) dev_free(c.code8);
   if (c.table) dev_free(c.table);
   if (c.val32) dev_free(c.val32);
+  const int stage = c.stage;
   c = RowCodec{};
+  c.stage = stage;
 }
 
 }  // namespace gb

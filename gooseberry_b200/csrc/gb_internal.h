@@ -192,6 +192,7 @@ struct RowCodec {
   double * table = nullptr;   // [ntable] distinct values
   uint32_t ntable = 0;
   float * val32 = nullptr;    // (float)value, equal to the double
+  int stage = 6;              // row entries held in the pipeline (5, 6 or 7)
   size_t entry_bytes() const {
     return (col16 ? 2 : 4) + (code8 ? 1 : (val32 ? 4 : 8));
   }

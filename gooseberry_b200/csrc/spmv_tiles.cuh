@@ -496,6 +496,7 @@ __device__ __forceinline__ uint32_t ld_l1_u8(const uint8_t * p, NoHint) {
 struct ColU32 {  // the CSR column array
   const uint32_t * p;
   using Raw = uint32_t;
+  static constexpr bool kInRange = false;  // clamp before gathering
   template <class P>
   __device__ __forceinline__ Raw load(uint32_t k, P pol) const { return ld_l1(p + k, pol); }
   __device__ __forceinline__ uint32_t col(Raw r, uint32_t) const { return r; }
@@ -504,6 +505,7 @@ struct ColU32 {  // the CSR column array
 struct ColD16 {  // column - row, 16-bit
   const int16_t * p;
   using Raw = int32_t;
+  static constexpr bool kInRange = true;  // built from validated columns
   template <class P>
   __device__ __forceinline__ Raw load(uint32_t k, P pol) const { return ld_l1_s16(p + k, pol); }
   __device__ __forceinline__ uint32_t col(Raw r, uint32_t row) const {
@@ -586,8 +588,12 @@ __device__ __forceinline__ void spmv_row_loop_c(uint32_t first, uint32_t end, ui
     // gather and sum the current row (reference order)
     Acc xv[STAGE];
 #pragma unroll
-    for (int j = 0; j < STAGE; ++j)
-      if (cur.b + j < cur.e) xv[j] = gather(min(ic.col(cur.c[j], i), cmax), pol_x);
+    for (int j = 0; j < STAGE; ++j) {
+      if (cur.b + j < cur.e) {
+        const uint32_t c = ic.col(cur.c[j], i);
+        xv[j] = gather(IC::kInRange ? c : min(c, cmax), pol_x);
+      }
+    }
     Acc sum = Acc(0);
 #pragma unroll
     for (int j = 0; j < STAGE; ++j)
@@ -595,7 +601,9 @@ __device__ __forceinline__ void spmv_row_loop_c(uint32_t first, uint32_t end, ui
         sum = add_rn(sum, mul_rn(vc.template value<Acc>(cur.v[j]), xv[j]));
     for (uint32_t k = cur.b + STAGE; k < cur.e; ++k)  // long-row tail
       sum = add_rn(sum, mul_rn(vc.template value<Acc>(vc.load(k, pol_matrix)),
-                               gather(min(ic.col(ic.load(k, pol_matrix), i), cmax), pol_x)));
+                               gather(IC::kInRange ? ic.col(ic.load(k, pol_matrix), i)
+                                                   : min(ic.col(ic.load(k, pol_matrix), i), cmax),
+                                      pol_x)));
     out.row_pre(i, sum, cur_pre);
     cur = nxt;
     cur_pre = nxt_pre;
