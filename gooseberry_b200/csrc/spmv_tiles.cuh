@@ -534,14 +534,14 @@ struct ValCode8 {  // 8-bit code into the distinct-value table (shared memory)
 };
 
 template <class IC, class VC, int STAGE>
-struct RowStage {
+struct RowStageC {
   uint32_t b = 0, e = 0;
   typename IC::Raw c[STAGE];
   typename VC::Raw v[STAGE];
 };
 
 template <class IC, class VC, int STAGE, class P>
-__device__ __forceinline__ void row_stage_load(RowStage<IC, VC, STAGE> & s, const IC & ic,
+__device__ __forceinline__ void row_stage_load_c(RowStageC<IC, VC, STAGE> & s, const IC & ic,
     const VC & vc, P pol) {
 #pragma unroll
   for (int j = 0; j < STAGE; ++j) {
@@ -560,11 +560,11 @@ __device__ __forceinline__ void spmv_row_loop_c(uint32_t first, uint32_t end, ui
   const uint32_t cmax = ncols - 1;
   if (first >= end) return;
   // stage L: row `first`; stage P: rowptr pair of row first + step
-  RowStage<IC, VC, STAGE> cur;
+  RowStageC<IC, VC, STAGE> cur;
   cur.b = __ldg(rowptr + first);
   cur.e = __ldg(rowptr + first + 1);
   typename Out::Pre cur_pre = out.pre(first);
-  row_stage_load(cur, ic, vc, pol_matrix);
+  row_stage_load_c(cur, ic, vc, pol_matrix);
   uint32_t nb = 0, ne = 0;
   if (first + step < end) {
     nb = __ldg(rowptr + first + step);
@@ -572,14 +572,14 @@ __device__ __forceinline__ void spmv_row_loop_c(uint32_t first, uint32_t end, ui
   }
   for (uint32_t i = first; i < end; i += step) {
     // issue the next row's indices/values/operands and the rowptr two ahead
-    RowStage<IC, VC, STAGE> nxt;
+    RowStageC<IC, VC, STAGE> nxt;
     typename Out::Pre nxt_pre{};
     const uint32_t i1 = i + step, i2 = i + 2 * step;
     if (i1 < end) {
       nxt.b = nb;
       nxt.e = ne;
       nxt_pre = out.pre(i1);
-      row_stage_load(nxt, ic, vc, pol_matrix);
+      row_stage_load_c(nxt, ic, vc, pol_matrix);
     }
     if (i2 < end) {
       nb = __ldg(rowptr + i2);
@@ -610,15 +610,78 @@ __device__ __forceinline__ void spmv_row_loop_c(uint32_t first, uint32_t end, ui
   }
 }
 
-// The row loop over the plain CSR arrays.
+// The row loop over the plain CSR arrays: the same pipeline written for the
+// two arrays directly (kept separate from spmv_row_loop_c, whose generic form
+// costs the FP32 kernels registers and occupancy).
+template <typename V, int STAGE>
+struct RowStage {
+  uint32_t b = 0, e = 0;
+  uint32_t c[STAGE];
+  V v[STAGE];
+};
+
+template <typename V, int STAGE, class P>
+__device__ __forceinline__ void row_stage_load(RowStage<V, STAGE> & s, const uint32_t * rowind,
+    const V * val, P pol) {
+#pragma unroll
+  for (int j = 0; j < STAGE; ++j) {
+    if (s.b + j < s.e) {
+      s.c[j] = ld_l1(rowind + s.b + j, pol);
+      s.v[j] = ld_l1(val + s.b + j, pol);
+    }
+  }
+}
+
 template <typename V, typename Acc, int STAGE = kRowStage, class Gather, class Out, class PM,
     class PX>
 __device__ __forceinline__ void spmv_row_loop(uint32_t first, uint32_t end, uint32_t step,
     uint32_t ncols, const uint32_t * __restrict__ rowptr,
     const uint32_t * __restrict__ rowind, const V * __restrict__ val, const Gather & gather,
     Out & out, PM pol_matrix, PX pol_x) {
-  spmv_row_loop_c<Acc, STAGE>(first, end, step, ncols, rowptr, ColU32{rowind},
-      ValPlain<V>{val}, gather, out, pol_matrix, pol_x);
+  const uint32_t cmax = ncols - 1;
+  if (first >= end) return;
+  // stage L: row `first`; stage P: rowptr pair of row first + step
+  RowStage<V, STAGE> cur;
+  cur.b = __ldg(rowptr + first);
+  cur.e = __ldg(rowptr + first + 1);
+  typename Out::Pre cur_pre = out.pre(first);
+  row_stage_load(cur, rowind, val, pol_matrix);
+  uint32_t nb = 0, ne = 0;
+  if (first + step < end) {
+    nb = __ldg(rowptr + first + step);
+    ne = __ldg(rowptr + first + step + 1);
+  }
+  for (uint32_t i = first; i < end; i += step) {
+    // issue the next row's indices/values/operands and the rowptr two ahead
+    RowStage<V, STAGE> nxt;
+    typename Out::Pre nxt_pre{};
+    const uint32_t i1 = i + step, i2 = i + 2 * step;
+    if (i1 < end) {
+      nxt.b = nb;
+      nxt.e = ne;
+      nxt_pre = out.pre(i1);
+      row_stage_load(nxt, rowind, val, pol_matrix);
+    }
+    if (i2 < end) {
+      nb = __ldg(rowptr + i2);
+      ne = __ldg(rowptr + i2 + 1);
+    }
+    // gather and sum the current row (reference order)
+    Acc xv[STAGE];
+#pragma unroll
+    for (int j = 0; j < STAGE; ++j)
+      if (cur.b + j < cur.e) xv[j] = gather(min(cur.c[j], cmax), pol_x);
+    Acc sum = Acc(0);
+#pragma unroll
+    for (int j = 0; j < STAGE; ++j)
+      if (cur.b + j < cur.e) sum = add_rn(sum, mul_rn(static_cast<Acc>(cur.v[j]), xv[j]));
+    for (uint32_t k = cur.b + STAGE; k < cur.e; ++k)  // long-row tail
+      sum = add_rn(sum, mul_rn(static_cast<Acc>(ld_l1(val + k, pol_matrix)),
+                               gather(min(ld_l1(rowind + k, pol_matrix), cmax), pol_x)));
+    out.row_pre(i, sum, cur_pre);
+    cur = nxt;
+    cur_pre = nxt_pre;
+  }
 }
 
 // ---- per-warp tiles -----------------------------------------------------------
