@@ -992,7 +992,7 @@ int create_cg(const gb_csr * a, int mode, gb_cg * s) {
     s->a = a;
     s->mode = mode;
     s->n = a->nrows;
-    return mixed_create(a, &s->mixed);
+    return mixed_create(a, plain_entries, &s->mixed);
   }
   GB_CHECK_INPUT(a->val64 != nullptr, "CG (FP64) needs double values on the matrix");
   s->a = a;
@@ -1258,7 +1258,7 @@ int gb_cg_solve(gb_cg_t * s, const double * b, double * x, double tol, int tol_r
 
 int gb_cg_entry_bytes(const gb_cg_t * s, size_t * bytes) {
   GB_CHECK_INPUT(s != nullptr && bytes != nullptr, "NULL argument");
-  *bytes = s->mixed ? 8 : (s->use_codec ? s->codec.entry_bytes() : 12);
+  *bytes = s->mixed ? mixed_entry_bytes(s->mixed) : (s->use_codec ? s->codec.entry_bytes() : 12);
   return GOOSEBERRY_SUCCESS;
 }
 

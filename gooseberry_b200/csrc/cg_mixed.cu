@@ -150,6 +150,26 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_a32_ke
       rowind, val, g, o);
 }
 
+// A32 on the row schedule over 16-bit column distances (ColD16): the same
+// products and sums as cg_a32_kernel<SCHED_ROW>, 2 bytes less per nonzero.
+template <bool HINT, int STAGE>
+__global__ void __launch_bounds__(kSpmvBlock, 3) cg_a32_d16_kernel(
+    const PlanView plan, const uint32_t * __restrict__ rowptr,
+    const int16_t * __restrict__ col16, const float * __restrict__ val,
+    const float * __restrict__ r, const float * __restrict__ pold, float * __restrict__ pnew,
+    float * __restrict__ ap, double * __restrict__ longdot, double * __restrict__ partial,
+    MixState * st) {
+  pdl_wait_and_release();
+  if (*reinterpret_cast<volatile int *>(&st->done)) return;
+  const float beta = static_cast<float>(st->beta);
+  GatherP32 g{r, pold, beta};
+  OutA32 o{ap, pnew, r, pold, longdot, partial, st, beta, 0u, 0.0};
+  spmv_row_loop_c<float, STAGE>(blockIdx.x * kSpmvBlock + threadIdx.x, plan.nrows,
+      gridDim.x * kSpmvBlock, plan.ncols, rowptr, ColD16{col16}, ValPlain<float>{val}, g, o,
+      L2Pol<HINT>::stream(), L2Pol<HINT>::keep());
+  o.finish();
+}
+
 // ---- B32 ----------------------------------------------------------------------
 
 __global__ void __launch_bounds__(kVecBlock, kSpmvMinBlocks) cg_b32_kernel(size_t n,
@@ -435,6 +455,19 @@ int launch_r_t(const gb_csr & a, unsigned grid, cudaStream_t s, bool pdl, const 
     default: return CALL(SCHED_MERGE);                                          \
   }
 
+template <bool HINT>
+int launch_a32_d16_t(const gb_csr & a, const int16_t * col16, int stage, unsigned grid,
+    cudaStream_t s, bool pdl, const float * r, const float * pold, float * pnew, float * ap,
+    double * longdot, double * partial, MixState * st, int * occ) {
+  auto kern = stage == 5   ? cg_a32_d16_kernel<HINT, 5>
+              : stage == 7 ? cg_a32_d16_kernel<HINT, 7>
+                           : cg_a32_d16_kernel<HINT, kRowStage>;
+  if (occ) return prep_kernel(kern, 0, occ);
+  GB_CUDA_TRY(launch_k(kern, grid, kSpmvBlock, 0, s, pdl, plan_view(a), a.rowptr, col16, a.val32,
+      r, pold, pnew, ap, longdot, partial, st));
+  return GOOSEBERRY_SUCCESS;
+}
+
 template <int SCHED>
 int occ_a32_t(size_t smem, int * occ) {
   return prep_kernel(cg_a32_kernel<SCHED, false>, smem, occ);
@@ -466,6 +499,8 @@ struct MixedCg {
   MixStatus * host_status = nullptr;
   unsigned grid_a = 0, grid_b = 0, grid_r = 0;
   bool l2_hint = false;  // L2-policy loads (the FP32 working set fits in L2)
+  int16_t * col16 = nullptr;  // row schedule: column - row, 16-bit (else null)
+  int stage = 6;
   int chunk = 32;
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -476,6 +511,11 @@ namespace {
 int launch_a32(MixedCg * m, cudaStream_t s, bool pdl, int k) {
   const float * pold = m->p[k & 1];
   float * pnew = m->p[(k + 1) & 1];
+  if (m->col16)
+    return m->l2_hint ? launch_a32_d16_t<true>(*m->a, m->col16, m->stage, m->grid_a, s, pdl,
+                            m->r, pold, pnew, m->ap, m->longdot, m->partial_a, m->st, nullptr)
+                      : launch_a32_d16_t<false>(*m->a, m->col16, m->stage, m->grid_a, s, pdl,
+                            m->r, pold, pnew, m->ap, m->longdot, m->partial_a, m->st, nullptr);
 #define GB_CALL(S)                                                                      \
   (m->l2_hint ? launch_a32_t<S, true>(*m->a, m->grid_a, s, pdl, m->r, pold, pnew, m->ap,   \
                                       m->longdot, m->partial_a, m->st)                     \
@@ -594,11 +634,14 @@ void mixed_destroy(MixedCg * m) {
   dev_free(m->partial_i);
   dev_free(m->longdot);
   dev_free(m->st);
+  if (m->col16) dev_free(m->col16);
   if (m->host_status) cudaFreeHost(m->host_status);
   delete m;
 }
 
-int mixed_create(const gb_csr * a, MixedCg ** out) {
+size_t mixed_entry_bytes(const MixedCg * m) { return m->col16 ? 6 : 8; }
+
+int mixed_create(const gb_csr * a, bool plain_entries, MixedCg ** out) {
   GB_CHECK_INPUT(a->val64 && a->val32,
       "mixed-precision CG needs both double and float values on the matrix "
       "(GB_CSR_VALUES_F64 | GB_CSR_VALUES_F32)");
@@ -609,9 +652,16 @@ int mixed_create(const gb_csr * a, MixedCg ** out) {
   m->sched32 = a->sched32;
   m->sched64 = a->sched64;
   m->tile_items = a->plan.tile_items;
+  // the row schedule reads 16-bit column distances when every entry lies
+  // within 32767 of the diagonal (stencils, banded matrices)
+  if (m->sched32 == GB_SCHED_ROW && !plain_entries) {
+    GB_TRY(build_col16(*a, &m->col16, nullptr));
+    m->stage = row_stage_for(*a);
+  }
   // L2-policy loads only when the FP32 iteration's working set (rowptr,
   // indices, float values, r, both p, Ap, y) fits in L2
-  GB_TRY(l2_fits(4ull * (m->n + 1) + 8ull * a->nnz + 24ull * m->n, &m->l2_hint));
+  GB_TRY(l2_fits(4ull * (m->n + 1) + (m->col16 ? 6ull : 8ull) * a->nnz + 24ull * m->n,
+      &m->l2_hint));
   const size_t n = std::max<size_t>(m->n, 2);
   GB_TRY(dev_alloc(&m->x[0], n * sizeof(double)));
   GB_TRY(dev_alloc(&m->x[1], n * sizeof(double)));
@@ -621,7 +671,17 @@ int mixed_create(const gb_csr * a, MixedCg ** out) {
   GB_TRY(dev_alloc(&m->p[0], n * sizeof(float)));
   GB_TRY(dev_alloc(&m->p[1], n * sizeof(float)));
   GB_TRY(dev_alloc(&m->ap, n * sizeof(float)));
-  GB_TRY(grid_of(a, m->sched32, smem_of(m->sched32, m->tile_items, 4), true, &m->grid_a));
+  if (m->col16) {
+    int occ = 0;
+    GB_TRY(launch_a32_d16_t<false>(*a, m->col16, m->stage, 0, nullptr, false, nullptr, nullptr,
+        nullptr, nullptr, nullptr, nullptr, nullptr, &occ));
+    GB_CHECK_INPUT(occ > 0, "CG kernel cannot be resident");
+    const size_t rows_units = (m->n + kSpmvBlock - 1) / kSpmvBlock;
+    m->grid_a = static_cast<unsigned>(std::max<size_t>(1, std::min<size_t>(rows_units,
+        static_cast<size_t>(a->sm_count) * occ)));
+  } else {
+    GB_TRY(grid_of(a, m->sched32, smem_of(m->sched32, m->tile_items, 4), true, &m->grid_a));
+  }
   GB_TRY(grid_of(a, m->sched64, smem_of(m->sched64, m->tile_items, 8), false, &m->grid_r));
   int occ_b = 0;
   GB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, cg_b32_kernel, kVecBlock, 0));

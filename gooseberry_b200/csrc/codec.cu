@@ -199,27 +199,46 @@ int build_values(const gb_csr & a, RowCodec * c, unsigned * flags, cudaStream_t 
 
 }  // namespace
 
-int build_row_codec(const gb_csr & a, RowCodec * c, cudaStream_t s) {
-  *c = RowCodec{};
-  c->stage = a.plan.max_row <= 5 ? 5 : (a.plan.max_row <= 7 ? 7 : 6);
-  if (a.nnz == 0 || !a.val64) return GOOSEBERRY_SUCCESS;
+int row_stage_for(const gb_csr & a) {
+  return a.plan.max_row <= 5 ? 5 : (a.plan.max_row <= 7 ? 7 : 6);
+}
+
+int build_col16(const gb_csr & a, int16_t ** out, cudaStream_t s) {
+  *out = nullptr;
+  if (a.nnz == 0) return GOOSEBERRY_SUCCESS;
   unsigned * flags = nullptr;
   GB_TRY(scratch_alloc(reinterpret_cast<void **>(&flags), 16, s));
   unsigned bad = 1;
-  int rc = dev_alloc(&c->col16, static_cast<size_t>(a.nnz) * 2);
+  int16_t * col16 = nullptr;
+  int rc = dev_alloc(&col16, static_cast<size_t>(a.nnz) * 2);
   if (rc == GOOSEBERRY_SUCCESS && cudaMemsetAsync(flags, 0, 4, s) != cudaSuccess)
     rc = GOOSEBERRY_ERROR_UNKNOWN;
   if (rc == GOOSEBERRY_SUCCESS) {
-    codec_delta_kernel<<<grid_of(a, a.nrows), 256, 0, s>>>(a.rowptr, a.rowind, a.nrows, c->col16,
+    codec_delta_kernel<<<grid_of(a, a.nrows), 256, 0, s>>>(a.rowptr, a.rowind, a.nrows, col16,
         flags);
     rc = read_flag(flags, &bad, s);
   }
-  if (rc == GOOSEBERRY_SUCCESS && bad) {
-    dev_free(c->col16);
-    c->col16 = nullptr;
-  }
-  if (rc == GOOSEBERRY_SUCCESS) rc = build_values(a, c, flags, s);
   scratch_free(flags, s);
+  if (rc != GOOSEBERRY_SUCCESS || bad) {
+    if (col16) dev_free(col16);
+    return rc;
+  }
+  *out = col16;
+  return GOOSEBERRY_SUCCESS;
+}
+
+int build_row_codec(const gb_csr & a, RowCodec * c, cudaStream_t s) {
+  *c = RowCodec{};
+  c->stage = row_stage_for(a);
+  if (a.nnz == 0 || !a.val64) return GOOSEBERRY_SUCCESS;
+  int rc = build_col16(a, &c->col16, s);
+  unsigned * flags = nullptr;
+  if (rc == GOOSEBERRY_SUCCESS)
+    rc = scratch_alloc(reinterpret_cast<void **>(&flags), 16, s);
+  if (rc == GOOSEBERRY_SUCCESS) {
+    rc = build_values(a, c, flags, s);
+    scratch_free(flags, s);
+  }
   if (rc != GOOSEBERRY_SUCCESS) free_row_codec(*c);
   return rc;
 }

@@ -199,10 +199,16 @@ struct RowCodec {
 };
 int build_row_codec(const gb_csr & a, RowCodec * c, cudaStream_t s);
 void free_row_codec(RowCodec & c);
+// The int16 column distances alone (*out stays null when some entry is
+// farther than 32767 from the diagonal); free with dev_free.
+int build_col16(const gb_csr & a, int16_t ** out, cudaStream_t s);
+// Register stage of the row loop for this matrix's longest row (5, 6 or 7).
+int row_stage_for(const gb_csr & a);
 
 // Mixed-precision CG (cg_mixed.cu), owned by a gb_cg created with GB_CG_MIXED.
 struct MixedCg;
-int mixed_create(const gb_csr * a, MixedCg ** out);
+int mixed_create(const gb_csr * a, bool plain_entries, MixedCg ** out);
+size_t mixed_entry_bytes(const MixedCg * m);
 void mixed_destroy(MixedCg * m);
 int mixed_solve(MixedCg * m, const double * b, double * x, double tol, int tol_relative,
     size_t niter, double * history, size_t history_len, gb_cg_result_t * res,

@@ -75,3 +75,25 @@ def test_compressed_entries_are_bit_identical(name):
     S.close()
     P.close()
     M.close()
+
+
+def test_mixed_solver_16bit_columns_are_bit_identical():
+    """The mixed solver's FP32 SpMV over 16-bit column distances gives the
+    same iterates, refinements and solution as over the plain columns."""
+    import torch
+    A = W.diffusion_3d(24, seed=11)
+    M = gb.CsrMatrix.from_host(A, f64=True, f32=True)
+    M.set_schedule(gb.SCHED_ROW)
+    M.set_schedule(gb.SCHED_ROW, f32=True)
+    S = gb.CgSolver(M, gb.CG_MIXED)
+    P = gb.CgSolver(M, gb.CG_MIXED, plain_entries=True)
+    assert S.entry_bytes() == 6 and P.entry_bytes() == 8
+    b = torch.from_numpy(W.rhs(A.nrows, 12)).cuda()
+    x1, r1 = S.solve(b, tol=1e-10)
+    x2, r2 = P.solve(b, tol=1e-10)
+    assert r1.status == r2.status == "converged"
+    assert (r1.iterations, r1.refinements) == (r2.iterations, r2.refinements)
+    assert torch.equal(x1, x2)
+    S.close()
+    P.close()
+    M.close()
