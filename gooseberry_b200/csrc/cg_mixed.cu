@@ -17,11 +17,18 @@
 // Per iteration three kernels, graph-captured 32 iterations at a time with
 // programmatic dependent launch:
 //   A32  SpMV (FP32) with the fused direction update, p.Ap in FP64
-//   B32  y += alpha p, r -= alpha Ap, r.r in FP64, update decision
-//   R    only when an update is pending (returns at once otherwise): FP64
-//        SpMV of b - A (x + y) fused with x <- x + y (into the other x
-//        buffer, so no CTA reads an x another CTA already changed) and the
-//        FP32 rounding of r; true ||r||, convergence test.
+//   B32  alpha from A32's partials; y += alpha p, r -= alpha Ap, r.r in FP64
+//   R    beta, ||r|| and the update decision from B32's partials; then, only
+//        when an update is pending: FP64 SpMV of b - A (x + y) fused with
+//        x <- x + y (into the other x buffer, so no CTA reads an x another CTA
+//        already changed) and the FP32 rounding of r; true ||r||,
+//        convergence test.
+// A32 and B32 have no serial last-CTA step: every CTA of the next kernel sums
+// their per-CTA partials itself in the same fixed order, so all CTAs hold the
+// same alpha / beta / decision.  The scalars that change every iteration are
+// kept in two versions (iteration k reads version k & 1, R of iteration k
+// writes version (k + 1) & 1), so no CTA reads a value another CTA of the
+// same kernel is rewriting.  R's own step (rare) keeps its last-CTA tail.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -36,28 +43,45 @@ namespace {
 
 constexpr double kDelta = 0.1;  // reliable update when ||r|| < kDelta * max ||r||
 
-struct MixState {
+// The scalars of one iteration (two versions, see above).
+struct MixScalars {
   double rr_hat;      // ||r||^2 of the FP32 residual the directions are built on
   double rr_hat_old;  // its value one iteration earlier
-  double alpha;
   double beta;
+  double rmax;        // largest ||r|| since the last reliable update
+  unsigned long long iter;
+  int update;         // a reliable update is pending
+  int y_reset;        // y was folded into x: the next B starts y afresh
+};
+
+struct MixState {
+  MixScalars sv[2];
   double tol;         // absolute bound on the true ||b - A x||
   double bnorm;
-  double rmax;        // largest ||r|| since the last reliable update
   double rr_true;     // ||b - A x||^2 at the last reliable update
-  unsigned long long iter;
+  unsigned long long iter;  // iterations done (host mirror; written by R's CTA 0)
   unsigned long long niter;
   unsigned long long refinements;
   int done;
   int status;
-  int update;         // a reliable update is pending
-  int y_reset;        // y was folded into x: the next B starts y afresh
   int xpar;           // index of the current x buffer
-  int force;          // run R even without a pending update (final fold)
-  unsigned ticket_a, ticket_b, ticket_r, ticket_i;
+  unsigned ticket_r, ticket_i;
   double * hist;
   unsigned long long hist_len;
 };
+
+// R launch modes: the iteration's step, the final fold the host requests when
+// a solve stops with a pending FP32 correction, and the profiler's (the step,
+// then the FP64 residual whether or not an update is pending).
+enum : int { kRStep = 0, kRFold = 1, kRProfile = 2 };
+
+// The stop flag, read once per CTA so that all of its threads agree.
+__device__ __forceinline__ bool mix_cta_done(const MixState * st) {
+  __shared__ int s_done;
+  if (threadIdx.x == 0) s_done = *reinterpret_cast<const volatile int *>(&st->done);
+  __syncthreads();
+  return s_done != 0;
+}
 
 struct MixStatus {
   int done;
@@ -112,24 +136,8 @@ struct OutA32 {
   }
   __device__ __forceinline__ void finish() {
     __shared__ double red[32];
-    __shared__ bool last;
     const double s = block_sum(local, red);
     if (threadIdx.x == 0) partial[blockIdx.x] = s;
-    if (!arrive_last(&st->ticket_a, &last)) return;
-    __threadfence();
-    double tot = ordered_sum(partial, gridDim.x, red);
-    if (threadIdx.x == 0) {
-      for (unsigned q = 0; q < nlong; ++q) tot += __ldcg(longdot + q);
-      st->ticket_a = 0;
-      const double rr = st->rr_hat;
-      if (!(tot > 0.0)) {
-        st->done = 1;
-        st->status = (tot == tot && rr == rr) ? GB_CG_BREAKDOWN : GB_CG_NONFINITE;
-        st->alpha = 0.0;
-      } else {
-        st->alpha = rr / tot;
-      }
-    }
   }
 };
 
@@ -139,10 +147,10 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_a32_ke
     const uint32_t * __restrict__ rowind, const float * __restrict__ val,
     const float * __restrict__ r, const float * __restrict__ pold, float * __restrict__ pnew,
     float * __restrict__ ap, double * __restrict__ longdot, double * __restrict__ partial,
-    MixState * st) {
+    MixState * st, int par) {
   pdl_wait_and_release();
-  if (*reinterpret_cast<volatile int *>(&st->done)) return;
-  const float beta = static_cast<float>(st->beta);
+  if (mix_cta_done(st)) return;
+  const float beta = static_cast<float>(st->sv[par].beta);
   GatherP32 g{r, pold, beta};
   OutA32 o{ap, pnew, r, pold, longdot, partial, st, beta,
            SCHED == SCHED_ROW ? 0u : plan.nlong, 0.0};
@@ -158,10 +166,10 @@ __global__ void __launch_bounds__(kSpmvBlock, 3) cg_a32_d16_kernel(
     const int16_t * __restrict__ col16, const float * __restrict__ val,
     const float * __restrict__ r, const float * __restrict__ pold, float * __restrict__ pnew,
     float * __restrict__ ap, double * __restrict__ longdot, double * __restrict__ partial,
-    MixState * st) {
+    MixState * st, int par) {
   pdl_wait_and_release();
-  if (*reinterpret_cast<volatile int *>(&st->done)) return;
-  const float beta = static_cast<float>(st->beta);
+  if (mix_cta_done(st)) return;
+  const float beta = static_cast<float>(st->sv[par].beta);
   GatherP32 g{r, pold, beta};
   OutA32 o{ap, pnew, r, pold, longdot, partial, st, beta, 0u, 0.0};
   spmv_row_loop_c<float, STAGE>(blockIdx.x * kSpmvBlock + threadIdx.x, plan.nrows,
@@ -172,15 +180,35 @@ __global__ void __launch_bounds__(kSpmvBlock, 3) cg_a32_d16_kernel(
 
 // ---- B32 ----------------------------------------------------------------------
 
+// Every CTA first sums A32's p.Ap partials (then the long-row terms) in order
+// and forms alpha = rr_hat / p.Ap; a breakdown (p.Ap <= 0) or NaN stops the
+// solve before anything is updated.
 __global__ void __launch_bounds__(kVecBlock, kSpmvMinBlocks) cg_b32_kernel(size_t n,
     float * __restrict__ y, float * __restrict__ r, const float * __restrict__ p,
-    const float * __restrict__ ap, double * __restrict__ partial, MixState * st) {
+    const float * __restrict__ ap, const double * __restrict__ partial_a, unsigned na,
+    const double * __restrict__ longdot, unsigned nlong, double * __restrict__ partial,
+    MixState * st, int par) {
   pdl_wait_and_release();
-  if (*reinterpret_cast<volatile int *>(&st->done)) return;
+  if (mix_cta_done(st)) return;
   __shared__ double red[32];
-  __shared__ bool last;
-  const float alpha = static_cast<float>(st->alpha);
-  const bool fresh = st->y_reset != 0;
+  __shared__ double s_pap;
+  double tot = ordered_sum(partial_a, na, red);
+  if (threadIdx.x == 0) {
+    for (unsigned q = 0; q < nlong; ++q) tot += __ldcg(longdot + q);
+    s_pap = tot;
+  }
+  __syncthreads();
+  const double pap = s_pap;
+  const double rr_hat = st->sv[par].rr_hat;
+  if (!(pap > 0.0)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      st->status = (pap == pap && rr_hat == rr_hat) ? GB_CG_BREAKDOWN : GB_CG_NONFINITE;
+      st->done = 1;
+    }
+    return;
+  }
+  const float alpha = static_cast<float>(rr_hat / pap);
+  const bool fresh = st->sv[par].y_reset != 0;
   const size_t q = n / gridDim.x, rem = n % gridDim.x;
   const size_t b = blockIdx.x;
   const size_t s = b * q + min(b, rem);
@@ -212,30 +240,6 @@ __global__ void __launch_bounds__(kVecBlock, kSpmvMinBlocks) cg_b32_kernel(size_
   }
   const double bs = block_sum(acc, red);
   if (threadIdx.x == 0) partial[blockIdx.x] = bs;
-  if (!arrive_last(&st->ticket_b, &last)) return;
-  __threadfence();
-  const double rr = ordered_sum(partial, gridDim.x, red);
-  if (threadIdx.x == 0) {
-    st->ticket_b = 0;
-    st->y_reset = 0;
-    st->rr_hat_old = st->rr_hat;
-    st->beta = rr / st->rr_hat;
-    st->rr_hat = rr;
-    const unsigned long long it = st->iter + 1;
-    st->iter = it;
-    const double rnorm = sqrt(rr);
-    if (st->hist && it <= st->hist_len) st->hist[it - 1] = rnorm;
-    st->rmax = fmax(st->rmax, rnorm);
-    if (!(rnorm == rnorm) || isinf(rnorm)) {
-      st->done = 1;
-      st->status = GB_CG_NONFINITE;
-    } else if (rnorm <= st->tol || rnorm < kDelta * st->rmax) {
-      st->update = 1;  // R folds y into x and checks the true residual
-    } else if (st->niter && it >= st->niter) {
-      st->done = 1;
-      st->status = GB_CG_MAXITER;
-    }
-  }
 }
 
 // ---- R: reliable update -------------------------------------------------------
@@ -263,6 +267,8 @@ struct OutR {
   bool use_y;
   unsigned nlong;
   double local;
+  MixScalars * sv;  // the version this R step writes
+  bool forced;      // fold and measure only: the iteration does not continue
   __device__ __forceinline__ double fold(uint32_t i, double ax) {
     xnew[i] = use_y ? xold[i] + static_cast<double>(y[i]) : xold[i];
     const double rt = b[i] - ax;
@@ -290,12 +296,11 @@ struct OutR {
       st->rr_true = tot;
       st->refinements += 1;
       st->xpar ^= 1;
-      st->y_reset = 1;
-      st->update = 0;
-      const bool forced = st->force != 0;
-      st->force = 0;
+      sv->y_reset = 1;
+      sv->update = 0;
       const double rnorm = sqrt(tot);
-      const unsigned long long it = st->iter;
+      // written by CTA 0 during this launch: read through L2
+      const unsigned long long it = __ldcg(&st->iter);
       if (st->hist && it >= 1 && it <= st->hist_len) st->hist[it - 1] = rnorm;
       if (!(rnorm == rnorm) || isinf(rnorm)) {
         st->done = 1;
@@ -305,9 +310,9 @@ struct OutR {
         st->status = GB_CG_CONVERGED;
       } else if (!forced) {
         // continue from the true residual, keeping the search direction
-        st->beta = tot / st->rr_hat_old;
-        st->rr_hat = tot;
-        st->rmax = rnorm;
+        sv->beta = tot / __ldcg(&sv->rr_hat_old);
+        sv->rr_hat = tot;
+        sv->rmax = rnorm;
         if (st->niter && it >= st->niter) {
           st->done = 1;
           st->status = GB_CG_MAXITER;
@@ -323,20 +328,56 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_r_kern
     const uint32_t * __restrict__ rowind, const double * __restrict__ val,
     const double * __restrict__ b, const double * __restrict__ x0, double * __restrict__ x1,
     const float * __restrict__ y, float * __restrict__ r32, double * __restrict__ longdot,
-    double * __restrict__ partial, MixState * st) {
+    double * __restrict__ partial, MixState * st, const double * __restrict__ partial_b,
+    unsigned nb, int par, int mode) {
   pdl_wait_and_release();
-  const int force = *reinterpret_cast<volatile int *>(&st->force);
-  if (!force) {
-    if (*reinterpret_cast<volatile int *>(&st->done)) return;
-    if (!*reinterpret_cast<volatile int *>(&st->update)) return;
+  MixScalars * sv = &st->sv[par];  // kRFold: the current version, in place
+  if (mode != kRFold) {
+    // the iteration's scalar step from B32's r.r partials (src/cgd.c:109-119
+    // for beta and the stop test), identical in every CTA; CTA 0 records it
+    // as the next version
+    if (mix_cta_done(st)) return;
+    __shared__ double red[32];
+    __shared__ double s_rr;
+    const double rr_sum = ordered_sum(partial_b, nb, red);
+    if (threadIdx.x == 0) s_rr = rr_sum;
+    __syncthreads();
+    const double rr = s_rr;
+    const MixScalars cur = st->sv[par];
+    MixScalars nv = cur;
+    nv.y_reset = 0;
+    nv.rr_hat_old = cur.rr_hat;
+    nv.beta = rr / cur.rr_hat;
+    nv.rr_hat = rr;
+    const unsigned long long it = cur.iter + 1;
+    nv.iter = it;
+    const double rnorm = sqrt(rr);
+    nv.rmax = fmax(cur.rmax, rnorm);
+    int stop = -1;
+    if (!(rnorm == rnorm) || isinf(rnorm)) stop = GB_CG_NONFINITE;
+    else if (rnorm <= st->tol || rnorm < kDelta * nv.rmax) nv.update = 1;
+    else if (st->niter && it >= st->niter) stop = GB_CG_MAXITER;
+    sv = &st->sv[par ^ 1];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      *sv = nv;
+      st->iter = it;
+      if (st->hist && it <= st->hist_len) st->hist[it - 1] = rnorm;
+      if (stop >= 0) {
+        st->status = stop;
+        st->done = 1;
+      }
+    }
+    if (stop >= 0 || (!nv.update && mode != kRProfile)) return;
   }
   const int xpar = st->xpar;
-  const bool use_y = st->y_reset == 0;
+  // after the step y holds this iteration's correction; a fold on request
+  // uses it only if no update has consumed it yet
+  const bool use_y = mode != kRFold || sv->y_reset == 0;
   const double * xold = xpar ? x1 : x0;
   double * xnew = xpar ? const_cast<double *>(x0) : x1;
   GatherXY g{xold, y, use_y};
   OutR o{b, xold, xnew, y, r32, longdot, partial, st, use_y,
-         SCHED == SCHED_ROW ? 0u : plan.nlong, 0.0};
+         SCHED == SCHED_ROW ? 0u : plan.nlong, 0.0, sv, mode != kRStep};
   spmv_tiles_body<double, double, SCHED, kSpmvBlock, GatherXY, OutR, false, HINT>(plan, rowptr,
       rowind, val, g, o);
 }
@@ -379,17 +420,18 @@ __global__ void __launch_bounds__(kVecBlock) cg_mixed_init_kernel(size_t n,
     st->ticket_i = 0;
     st->bnorm = sqrt(bb);
     st->rr_true = bb;
-    st->rr_hat = rr;
-    st->rr_hat_old = rr;
-    st->rmax = sqrt(rr);
-    st->beta = 0.0;
-    st->alpha = 0.0;
+    MixScalars v0;
+    v0.rr_hat = rr;
+    v0.rr_hat_old = rr;
+    v0.rmax = sqrt(rr);
+    v0.beta = 0.0;
+    v0.iter = 0;
+    v0.y_reset = 1;
+    v0.update = 0;
+    st->sv[0] = v0;
     st->iter = 0;
     st->refinements = 0;
     st->xpar = 0;
-    st->y_reset = 1;
-    st->update = 0;
-    st->force = 0;
     if (tol_relative) st->tol = st->tol * st->bnorm;
     st->done = 0;
     st->status = GB_CG_MAXITER;
@@ -423,24 +465,25 @@ int prep_kernel(K kern, size_t smem, int * occ) {
 template <int SCHED, bool HINT>
 int launch_a32_t(const gb_csr & a, unsigned grid, cudaStream_t s, bool pdl,
     const float * r, const float * pold, float * pnew, float * ap, double * longdot,
-    double * partial, MixState * st) {
+    double * partial, MixState * st, int par) {
   const size_t smem = smem_of(SCHED, a.plan.tile_items, 4);
   auto kern = cg_a32_kernel<SCHED, HINT>;
   GB_TRY(prep_kernel(kern, smem, nullptr));
   GB_CUDA_TRY(launch_k(kern, grid, kSpmvBlock, smem, s, pdl, plan_view(a), a.rowptr,
-      a.rowind, a.val32, r, pold, pnew, ap, longdot, partial, st));
+      a.rowind, a.val32, r, pold, pnew, ap, longdot, partial, st, par));
   return GOOSEBERRY_SUCCESS;
 }
 
 template <int SCHED, bool HINT>
 int launch_r_t(const gb_csr & a, unsigned grid, cudaStream_t s, bool pdl, const double * b,
     const double * x0, double * x1, const float * y, float * r32, double * longdot,
-    double * partial, MixState * st) {
+    double * partial, MixState * st, const double * partial_b, unsigned nb, int par,
+    int mode) {
   const size_t smem = smem_of(SCHED, a.plan.tile_items, 8);
   auto kern = cg_r_kernel<SCHED, HINT>;
   GB_TRY(prep_kernel(kern, smem, nullptr));
   GB_CUDA_TRY(launch_k(kern, grid, kSpmvBlock, smem, s, pdl, plan_view(a), a.rowptr,
-      a.rowind, a.val64, b, x0, x1, y, r32, longdot, partial, st));
+      a.rowind, a.val64, b, x0, x1, y, r32, longdot, partial, st, partial_b, nb, par, mode));
   return GOOSEBERRY_SUCCESS;
 }
 
@@ -458,13 +501,13 @@ int launch_r_t(const gb_csr & a, unsigned grid, cudaStream_t s, bool pdl, const 
 template <bool HINT>
 int launch_a32_d16_t(const gb_csr & a, const int16_t * col16, int stage, unsigned grid,
     cudaStream_t s, bool pdl, const float * r, const float * pold, float * pnew, float * ap,
-    double * longdot, double * partial, MixState * st, int * occ) {
+    double * longdot, double * partial, MixState * st, int par, int * occ) {
   auto kern = stage == 5   ? cg_a32_d16_kernel<HINT, 5>
               : stage == 7 ? cg_a32_d16_kernel<HINT, 7>
                            : cg_a32_d16_kernel<HINT, kRowStage>;
   if (occ) return prep_kernel(kern, 0, occ);
   GB_CUDA_TRY(launch_k(kern, grid, kSpmvBlock, 0, s, pdl, plan_view(a), a.rowptr, col16, a.val32,
-      r, pold, pnew, ap, longdot, partial, st));
+      r, pold, pnew, ap, longdot, partial, st, par));
   return GOOSEBERRY_SUCCESS;
 }
 
@@ -513,40 +556,49 @@ int launch_a32(MixedCg * m, cudaStream_t s, bool pdl, int k) {
   float * pnew = m->p[(k + 1) & 1];
   if (m->col16)
     return m->l2_hint ? launch_a32_d16_t<true>(*m->a, m->col16, m->stage, m->grid_a, s, pdl,
-                            m->r, pold, pnew, m->ap, m->longdot, m->partial_a, m->st, nullptr)
+                            m->r, pold, pnew, m->ap, m->longdot, m->partial_a, m->st, k & 1,
+                            nullptr)
                       : launch_a32_d16_t<false>(*m->a, m->col16, m->stage, m->grid_a, s, pdl,
-                            m->r, pold, pnew, m->ap, m->longdot, m->partial_a, m->st, nullptr);
+                            m->r, pold, pnew, m->ap, m->longdot, m->partial_a, m->st, k & 1,
+                            nullptr);
 #define GB_CALL(S)                                                                      \
   (m->l2_hint ? launch_a32_t<S, true>(*m->a, m->grid_a, s, pdl, m->r, pold, pnew, m->ap,   \
-                                      m->longdot, m->partial_a, m->st)                     \
+                                      m->longdot, m->partial_a, m->st, k & 1)              \
               : launch_a32_t<S, false>(*m->a, m->grid_a, s, pdl, m->r, pold, pnew, m->ap,  \
-                                       m->longdot, m->partial_a, m->st))
+                                       m->longdot, m->partial_a, m->st, k & 1))
   GB_SCHED_SWITCH(m->sched32, GB_CALL)
 #undef GB_CALL
 }
 
-int launch_r(MixedCg * m, cudaStream_t s, bool pdl) {
+// R of iteration parity par (kRFold: par = the current version).
+int launch_r(MixedCg * m, cudaStream_t s, bool pdl, int par, int mode) {
 #define GB_CALL(S)                                                                      \
   (m->l2_hint ? launch_r_t<S, true>(*m->a, m->grid_r, s, pdl, m->b, m->x[0], m->x[1], m->y,  \
-                                    m->r, m->longdot, m->partial_r, m->st)                  \
+                                    m->r, m->longdot, m->partial_r, m->st, m->partial_b,    \
+                                    m->grid_b, par, mode)                                   \
               : launch_r_t<S, false>(*m->a, m->grid_r, s, pdl, m->b, m->x[0], m->x[1], m->y, \
-                                     m->r, m->longdot, m->partial_r, m->st))
+                                     m->r, m->longdot, m->partial_r, m->st, m->partial_b,   \
+                                     m->grid_b, par, mode))
   GB_SCHED_SWITCH(m->sched64, GB_CALL)
 #undef GB_CALL
 }
 
 int launch_b32(MixedCg * m, cudaStream_t s, bool pdl, int k) {
   float * pnew = m->p[(k + 1) & 1];
+  // the row schedule sums long rows like any other row: no long-row terms
+  const unsigned nlong = m->sched32 == GB_SCHED_ROW ? 0u
+                         : static_cast<unsigned>(m->a->plan.longrows.size());
   GB_CUDA_TRY(launch_k(cg_b32_kernel, m->grid_b, kVecBlock, 0, s, pdl, m->n, m->y, m->r,
-      static_cast<const float *>(pnew), static_cast<const float *>(m->ap), m->partial_b,
-      m->st));
+      static_cast<const float *>(pnew), static_cast<const float *>(m->ap),
+      static_cast<const double *>(m->partial_a), m->grid_a,
+      static_cast<const double *>(m->longdot), nlong, m->partial_b, m->st, k & 1));
   return GOOSEBERRY_SUCCESS;
 }
 
 int iteration(MixedCg * m, cudaStream_t s, bool pdl_first, int k) {
   GB_TRY(launch_a32(m, s, pdl_first, k));
   GB_TRY(launch_b32(m, s, true, k));
-  GB_TRY(launch_r(m, s, true));
+  GB_TRY(launch_r(m, s, true, k & 1, kRStep));
   return GOOSEBERRY_SUCCESS;
 }
 
@@ -674,7 +726,7 @@ int mixed_create(const gb_csr * a, bool plain_entries, MixedCg ** out) {
   if (m->col16) {
     int occ = 0;
     GB_TRY(launch_a32_d16_t<false>(*a, m->col16, m->stage, 0, nullptr, false, nullptr, nullptr,
-        nullptr, nullptr, nullptr, nullptr, nullptr, &occ));
+        nullptr, nullptr, nullptr, nullptr, nullptr, 0, &occ));
     GB_CHECK_INPUT(occ > 0, "CG kernel cannot be resident");
     const size_t rows_units = (m->n + kSpmvBlock - 1) / kSpmvBlock;
     m->grid_a = static_cast<unsigned>(std::max<size_t>(1, std::min<size_t>(rows_units,
@@ -780,15 +832,11 @@ int mixed_solve(MixedCg * m, const double * b, double * x, double tol, int tol_r
   if (rc == GOOSEBERRY_SUCCESS) {
     e = cudaMemcpy(&fin, m->st, sizeof(MixState), cudaMemcpyDeviceToHost);
     if (e == cudaSuccess && fin.status != GB_CG_CONVERGED && fin.status != GB_CG_NONFINITE &&
-        fin.y_reset == 0) {
+        fin.sv[fin.iter & 1].y_reset == 0) {
       // stopped on the iteration limit (or breakdown) with a pending FP32
       // correction: fold it into x once more and measure the true residual
-      const int one = 1;
-      e = cudaMemcpyAsync(&m->st->force, &one, sizeof(int), cudaMemcpyHostToDevice, stream);
-      if (e == cudaSuccess) {
-        rc = launch_r(m, stream, false);
-        launches += 1;
-      }
+      rc = launch_r(m, stream, false, static_cast<int>(fin.iter & 1), kRFold);
+      launches += 1;
       if (e == cudaSuccess && rc == GOOSEBERRY_SUCCESS) e = cudaStreamSynchronize(stream);
       if (e == cudaSuccess && rc == GOOSEBERRY_SUCCESS)
         e = cudaMemcpy(&fin, m->st, sizeof(MixState), cudaMemcpyDeviceToHost);
@@ -826,16 +874,14 @@ int mixed_profile(MixedCg * m, const double * b, size_t iterations, double * ms,
   std::vector<cudaEvent_t> ev(4 * iterations);
   for (auto & e : ev) GB_CUDA_TRY(cudaEventCreate(&e));
   int rc = GOOSEBERRY_SUCCESS;
-  const int one = 1;
   for (size_t k = 0; k < iterations && rc == GOOSEBERRY_SUCCESS; ++k) {
-    // the FP64 refinement kernel is forced to run so every iteration times it
-    cudaMemcpyAsync(&m->st->force, &one, sizeof(int), cudaMemcpyHostToDevice, stream);
     cudaEventRecord(ev[4 * k], stream);
     rc = launch_a32(m, stream, false, static_cast<int>(k));
     cudaEventRecord(ev[4 * k + 1], stream);
     if (rc == GOOSEBERRY_SUCCESS) rc = launch_b32(m, stream, false, static_cast<int>(k));
     cudaEventRecord(ev[4 * k + 2], stream);
-    if (rc == GOOSEBERRY_SUCCESS) rc = launch_r(m, stream, false);
+    // the FP64 refinement runs every iteration here, so every iteration times it
+    if (rc == GOOSEBERRY_SUCCESS) rc = launch_r(m, stream, false, static_cast<int>(k & 1), kRProfile);
     cudaEventRecord(ev[4 * k + 3], stream);
   }
   cudaError_t e = cudaStreamSynchronize(stream);
