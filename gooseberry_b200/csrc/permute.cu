@@ -54,6 +54,7 @@ constexpr int kCmThreads = 1024;
 constexpr uint32_t kCmSmallFrontier = 4096;  // frontier vertices the CTA expands
 constexpr uint32_t kCmSmallEdges = 32768;    // frontier entries the CTA expands
 constexpr uint32_t kCmSmallLevel = 4096;     // candidates the CTA sorts
+constexpr int kCmUnroll = 4;                 // frontier entries in flight per thread
 constexpr int kCmExpandThreads = 256;
 constexpr uint32_t kCmLaneEdges = 8;         // entries per lane per warp chunk
 
@@ -82,8 +83,13 @@ struct CmSmem {
   uint32_t hi[kCmSmallFrontier];
   unsigned long long key[kCmSmallLevel];
   uint32_t warp_sum[kCmThreads / 32];
-  uint32_t count, found;
+  uint32_t count, found, maxb;
 };
+
+// Children one parent may have for the bucket ordering of a small level
+// (larger families take the bitonic sort).
+constexpr uint32_t kCmBucketMax = 32;
+constexpr int kCmHeld = kCmSmallLevel / kCmThreads;  // candidates per thread
 
 __device__ __forceinline__ void cm_block_range(const CmGraph & g, uint32_t v, uint32_t & lo,
     uint32_t & hi) {
@@ -261,18 +267,39 @@ cm_small_kernel(CmGraph g, const uint32_t * __restrict__ order,
     }
     __syncthreads();
 
-    // expand: one thread per frontier entry
-    for (uint32_t e = tid; e < total; e += kCmThreads) {
-      uint32_t lo = 0, hi = L;  // largest i with off[i] <= e
-      while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) / 2;
-        if (sm.off[mid] <= e) lo = mid; else hi = mid;
+    // expand: one thread per frontier entry, kCmUnroll entries in flight per
+    // thread (their loads and atomics are issued before any result is used)
+    for (uint32_t e0 = tid; e0 < total; e0 += kCmUnroll * kCmThreads) {
+      uint32_t k[kCmUnroll], p[kCmUnroll];
+      bool in[kCmUnroll];
+#pragma unroll
+      for (int u = 0; u < kCmUnroll; ++u) {
+        const uint32_t e = e0 + u * kCmThreads;
+        in[u] = false;
+        k[u] = 0;
+        p[u] = 0;
+        if (e < total) {
+          uint32_t lo = 0, hi = L;  // largest i with off[i] <= e
+          while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) / 2;
+            if (sm.off[mid] <= e) lo = mid; else hi = mid;
+          }
+          k[u] = __ldg(g.rowind + sm.rs[lo] + (e - sm.off[lo]));
+          p[u] = lo;
+          in[u] = true;
+        }
       }
-      const uint32_t k = __ldg(g.rowind + sm.rs[lo] + (e - sm.off[lo]));
-      if (k >= sm.lo[lo] && k < sm.hi[lo]) {
-        if (atomicMin(claim + k, a + lo) == kUnvisited) {
+      uint32_t old[kCmUnroll];
+#pragma unroll
+      for (int u = 0; u < kCmUnroll; ++u) {
+        in[u] = in[u] && k[u] >= sm.lo[p[u]] && k[u] < sm.hi[p[u]];
+        old[u] = in[u] ? atomicMin(claim + k[u], a + p[u]) : 0u;
+      }
+#pragma unroll
+      for (int u = 0; u < kCmUnroll; ++u) {
+        if (in[u] && old[u] == kUnvisited) {
           const uint32_t slot = atomicAdd(&sm.count, 1u);
-          cand[slot] = k;
+          cand[slot] = k[u];
         }
       }
     }
@@ -287,7 +314,76 @@ cm_small_kernel(CmGraph g, const uint32_t * __restrict__ order,
       continue;
     }
 
-    // order the level by (first parent, degree, id) in shared memory
+    // order the level by (first parent, degree, id) in shared memory.
+    // Usually each parent has a few children: bucket the candidates by parent
+    // (counts, scan, scatter), then sort each bucket by rank in one thread.
+    uint32_t hk[kCmHeld], hp[kCmHeld], hpos[kCmHeld];
+#pragma unroll
+    for (int q = 0; q < kCmHeld; ++q) {
+      const uint32_t i = tid * kCmHeld + q;
+      if (i < L) sm.rs[i] = 0;  // bucket counts (the row starts are spent)
+    }
+    if (tid == 0) sm.maxb = 0;
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kCmHeld; ++q) {
+      const uint32_t i = tid + q * kCmThreads;
+      if (i < count) {
+        hk[q] = __ldcg(cand + i);
+        hp[q] = __ldcg(claim + hk[q]) - a;
+        hpos[q] = atomicAdd(&sm.rs[hp[q]], 1u);
+        atomicMax(&sm.maxb, hpos[q] + 1);
+      }
+    }
+    __syncthreads();
+    if (sm.maxb <= kCmBucketMax) {
+      uint32_t cnt[kCmHeld], csum = 0;
+#pragma unroll
+      for (int q = 0; q < kCmHeld; ++q) {
+        const uint32_t i = tid * kCmHeld + q;
+        cnt[q] = i < L ? sm.rs[i] : 0u;
+        csum += cnt[q];
+      }
+      uint32_t tot;
+      uint32_t o = cm_block_scan(csum, sm.warp_sum, &tot);
+#pragma unroll
+      for (int q = 0; q < kCmHeld; ++q) {
+        const uint32_t i = tid * kCmHeld + q;
+        if (i < L) sm.lo[i] = o;  // bucket starts (the block ranges are spent)
+        o += cnt[q];
+      }
+      __syncthreads();
+      uint32_t * slot_rank = reinterpret_cast<uint32_t *>(sm.key);
+#pragma unroll
+      for (int q = 0; q < kCmHeld; ++q) {
+        const uint32_t i = tid + q * kCmThreads;
+        if (i < count) slot_rank[sm.lo[hp[q]] + hpos[q]] = __ldg(rank + hk[q]);
+      }
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < kCmHeld; ++q) {  // insertion sort of each bucket
+        const uint32_t i = tid * kCmHeld + q;
+        if (i < L) {
+          const uint32_t s0 = sm.lo[i], c = sm.rs[i];
+          for (uint32_t x = 1; x < c; ++x) {
+            const uint32_t v = slot_rank[s0 + x];
+            uint32_t y = x;
+            while (y > 0 && slot_rank[s0 + y - 1] > v) {
+              slot_rank[s0 + y] = slot_rank[s0 + y - 1];
+              --y;
+            }
+            slot_rank[s0 + y] = v;
+          }
+        }
+      }
+      __syncthreads();
+      for (uint32_t i = tid; i < count; i += kCmThreads)
+        perm[b + i] = __ldg(order + slot_rank[i]);
+      a = b;
+      b += count;
+      __syncthreads();
+      continue;
+    }
     uint32_t P = 1;
     while (P < count) P <<= 1;
     for (uint32_t i = tid; i < P; i += kCmThreads) {
