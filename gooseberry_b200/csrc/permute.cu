@@ -547,16 +547,20 @@ int grid_for(size_t items, int threads) {
 // device array perm (perm[new] = old).  blocks: host array of nblocks+1
 // boundaries covering [0, n), or null for one block.  max_row bounds the
 // degree.  Synchronises `stream` once per large level.
+int check_blocks(uint32_t n, const uint32_t * blocks, uint32_t nblocks) {
+  if (!blocks) return GOOSEBERRY_SUCCESS;
+  GB_CHECK_INPUT(blocks[0] == 0 && blocks[nblocks] == n,
+      "row blocks must cover [0, %u): got [%u, %u)", n, blocks[0], blocks[nblocks]);
+  for (uint32_t c = 0; c < nblocks; ++c)
+    GB_CHECK_INPUT(blocks[c] <= blocks[c + 1], "row block %u has a negative size", c);
+  return GOOSEBERRY_SUCCESS;
+}
+
 int cuthillmckee_device(uint32_t n, const uint32_t * rowptr, const uint32_t * rowind,
     uint32_t max_row, const uint32_t * blocks, uint32_t nblocks, uint32_t * perm,
     cudaStream_t stream) {
   if (n == 0) return GOOSEBERRY_SUCCESS;
-  if (blocks) {
-    GB_CHECK_INPUT(blocks[0] == 0 && blocks[nblocks] == n,
-        "row blocks must cover [0, %u): got [%u, %u)", n, blocks[0], blocks[nblocks]);
-    for (uint32_t c = 0; c < nblocks; ++c)
-      GB_CHECK_INPUT(blocks[c] <= blocks[c + 1], "row block %u has a negative size", c);
-  }
+  GB_TRY(check_blocks(n, blocks, nblocks));
   ScratchSet sc(stream);
   uint32_t *deg, *iota, *order, *rank, *claim, *cand, *len, *off;
   unsigned long long *keys, *keys_alt;
@@ -871,6 +875,7 @@ int gooseberry_permute_cuthillmckee(dim_t nrows, dim_t ncols, const ind_t * rowp
   GB_CHECK_INPUT(perm != nullptr, "perm is NULL");
   uint32_t max_row = 0;
   GB_TRY(check_rowptr(nrows, rowptr, &max_row));
+  GB_TRY(gb::check_blocks(nrows, blocks, nblocks));
   const uint32_t nnz = rowptr[nrows];
   GB_CHECK_INPUT(nnz == 0 || rowind, "rowind is NULL");
   cudaStream_t s = nullptr;

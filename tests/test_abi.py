@@ -87,3 +87,32 @@ def test_planner_rejects_bad_rowptr():
     with pytest.raises(gb.GooseberryError) as e:
         gb.plan_tiles(np.array([0, 5, 3, 8], np.uint32), 64)
     assert e.value.code == 3 and "decreases" in str(e.value)
+
+
+def test_reordering_entry_points_reject_bad_input_before_any_device_work():
+    """Shape and argument errors of the Cuthill-McKee and permutation drop-ins
+    (src/permute.c:120-205,288-337) come back as GOOSEBERRY_ERROR_INVALIDINPUT
+    from host-side checks, with no GPU needed."""
+    rowptr = np.array([0, 2, 3, 5], np.uint32)
+    rowind = np.array([0, 1, 1, 0, 2], np.uint32)
+    vals = np.ones(5)
+    with pytest.raises(gb.GooseberryError) as e:
+        gb.cuthillmckee(rowptr, rowind, 3, 4)  # not square, as the reference
+    assert e.value.code == 3 and "symmetric" in str(e.value)
+    with pytest.raises(gb.GooseberryError) as e:
+        gb.cuthillmckee(rowptr, rowind, 3, blocks=[0, 2])  # blocks miss row 2
+    assert e.value.code == 3
+    with pytest.raises(gb.GooseberryError) as e:
+        gb.cuthillmckee(np.array([0, 2, 1, 5], np.uint32), rowind, 3)
+    assert e.value.code == 3
+    with pytest.raises(gb.GooseberryError) as e:
+        gb.permute_sparse(np.array([0, 3, 2, 5], np.uint32), rowind, vals, 3,
+                          np.array([2, 1, 0], np.uint32))
+    assert e.value.code == 3
+    with pytest.raises(gb.GooseberryError) as e:  # a column past ncols with colperm
+        gb.permute_sparse(rowptr, np.array([0, 1, 1, 0, 7], np.uint32), vals, 3, None,
+                          np.array([2, 1, 0], np.uint32))
+    assert e.value.code == 3
+    # no permutation: nothing to do, arrays come back unchanged
+    rp, ri, rv = gb.permute_sparse(rowptr, rowind, vals, 3)
+    assert np.array_equal(rp, rowptr) and np.array_equal(ri, rowind)
