@@ -48,20 +48,15 @@ namespace {
 
 struct CgState {
   double rr;         // r.r of the current residual
-  double alpha;
-  double beta;
   double tol;        // absolute bound on ||r||_2
   double bnorm;      // ||b||_2
-  double pap;
   unsigned long long iter;   // iterations done (written by B, read by A)
   unsigned long long niter;  // limit (0 = none)
   unsigned long long kb;     // iteration of the running B (written by A)
   double rrk[2];             // r.r of iteration k in rrk[k & 1] (written by A)
   int done;          // 1: stop
   int status;        // gb_cg_status_t
-  unsigned int ticket_a;
-  unsigned int ticket_b;
-  unsigned int ticket_i;
+  unsigned int ticket_i;     // the init kernel's last-CTA ticket
   unsigned int pad;
   double * hist;     // optional device history
   unsigned long long hist_len;
@@ -342,8 +337,6 @@ __global__ void __launch_bounds__(kVecBlock) cg_init_kernel(size_t n,
     st->ticket_i = 0;
     st->rr = rr;
     st->bnorm = sqrt(rr);
-    st->beta = 0.0;
-    st->alpha = 0.0;
     st->iter = 0;
     if (tol_relative) st->tol = st->tol * st->bnorm;
     st->done = 0;
