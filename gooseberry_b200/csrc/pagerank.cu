@@ -2,9 +2,12 @@
 // `pagerank` command (src/gooseberry_bin.c:2610-2741) for a square CSR graph
 // already in memory (no permutation file, one run).
 //
-// Normalisation is done on the host exactly like the reference (column sums
-// accumulated in row order, every value divided by its column's sum, rows
-// without entries are the sinks), so the device matrix holds the same values.
+// Normalisation is done on the device with the reference's arithmetic (column
+// sums accumulated in row order, every value divided by its column's sum,
+// rows without entries are the sinks), so the device matrix holds the same
+// values: a stable radix sort of the entries by column keeps each column's
+// entries in row order, one thread per column adds them in that order, and
+// each value is divided by its column's sum.
 // Per iteration on the device: out = A rank (the library SpMV, its matrix's
 // schedule); dist = sum of rank over the sinks (fixed-order reduction);
 // out = out * damping, then out += (1 - damping)/n + dist (two roundings, as
@@ -14,9 +17,11 @@
 // are, quirks included: the whole sink mass is added to every entry (not
 // spread over n), and when the iteration limit ends the run the result is the
 // second-to-last iterate (the buffer the last swap left in `out`).
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
 #include <algorithm>
 #include <cmath>
-#include <thread>
 #include <vector>
 
 #include "gb_internal.h"
@@ -97,6 +102,95 @@ __global__ void __launch_bounds__(kPrBlock) pr_diff_kernel(size_t n,
   if (threadIdx.x == 0) partial[blockIdx.x] = acc;
 }
 
+// ---- normalisation (src/gooseberry_bin.c:2611-2630) --------------------------
+
+__global__ void pr_iota_count_kernel(uint32_t nnz, const uint32_t * __restrict__ rowind,
+    uint32_t * __restrict__ iota, uint32_t * __restrict__ count) {
+  for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < nnz; l += gridDim.x * blockDim.x) {
+    iota[l] = l;
+    atomicAdd(count + rowind[l], 1u);
+  }
+}
+
+// indeg[c] = sum of the values of column c, entries in row order (the sorted
+// entry numbers of a column ascend); the reference's loop adds them in the
+// same order without fusing (src/gooseberry_bin.c:2611-2621).
+__global__ void pr_colsum_kernel(uint32_t n, const uint32_t * __restrict__ colptr,
+    const uint32_t * __restrict__ entry, const double * __restrict__ val,
+    double * __restrict__ indeg) {
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (uint32_t j = colptr[c]; j < colptr[c + 1]; ++j) s = __dadd_rn(s, val[entry[j]]);
+    indeg[c] = s;
+  }
+}
+
+// val[l] /= indeg[rowind[l]] (src/gooseberry_bin.c:2622-2630)
+__global__ void pr_divide_kernel(uint32_t nnz, const uint32_t * __restrict__ rowind,
+    const double * __restrict__ indeg, double * __restrict__ val) {
+  for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < nnz; l += gridDim.x * blockDim.x)
+    val[l] = __ddiv_rn(val[l], indeg[rowind[l]]);
+}
+
+// Scratch of the normalisation, released together.
+struct PrScratch {
+  cudaStream_t s;
+  std::vector<void *> p;
+  explicit PrScratch(cudaStream_t st) : s(st) {}
+  template <typename T>
+  int get(T ** out, size_t count) {
+    void * q = nullptr;
+    GB_TRY(scratch_alloc(&q, std::max<size_t>(count, 1) * sizeof(T), s));
+    p.push_back(q);
+    *out = static_cast<T *>(q);
+    return GOOSEBERRY_SUCCESS;
+  }
+  ~PrScratch() {
+    for (void * q : p) scratch_free(q, s);
+  }
+};
+
+// Normalise the device matrix's values in place.
+int normalise_device(gb_csr & a, cudaStream_t st) {
+  const uint32_t n = a.nrows, nnz = a.nnz;
+  if (nnz == 0) return GOOSEBERRY_SUCCESS;
+  double * val = static_cast<double *>(a.own_val64);
+  GB_CHECK_INPUT(val != nullptr, "matrix holds no values of its own");
+  PrScratch sc(st);
+  uint32_t *iota, *keys, *entry, *count, *colptr;
+  double * indeg;
+  GB_TRY(sc.get(&iota, nnz));
+  GB_TRY(sc.get(&keys, nnz));
+  GB_TRY(sc.get(&entry, nnz));
+  GB_TRY(sc.get(&count, static_cast<size_t>(n) + 1));
+  GB_TRY(sc.get(&colptr, static_cast<size_t>(n) + 1));
+  GB_TRY(sc.get(&indeg, n));
+  int sms = 148;
+  GB_TRY(sm_count_of_current_device(&sms));
+  const int grid = sms * 8;
+  int bits = 1;
+  while (bits < 32 && (1ull << bits) < n) ++bits;
+  size_t t_sort = 0, t_scan = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, t_sort, a.rowind, keys, iota, entry, nnz, 0, bits,
+      st);
+  cub::DeviceScan::ExclusiveSum(nullptr, t_scan, count, colptr, n + 1, st);
+  unsigned char * tmp;
+  GB_TRY(sc.get(&tmp, std::max(t_sort, t_scan)));
+  GB_CUDA_TRY(cudaMemsetAsync(count, 0, (static_cast<size_t>(n) + 1) * 4, st));
+  pr_iota_count_kernel<<<grid, kPrBlock, 0, st>>>(nnz, a.rowind, iota, count);
+  GB_CUDA_TRY(cudaGetLastError());
+  // stable: the entries of a column keep their (row) order
+  GB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, t_sort, a.rowind, keys, iota, entry, nnz, 0,
+      bits, st));
+  GB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, t_scan, count, colptr, n + 1, st));
+  pr_colsum_kernel<<<grid, kPrBlock, 0, st>>>(n, colptr, entry, val, indeg);
+  GB_CUDA_TRY(cudaGetLastError());
+  pr_divide_kernel<<<grid, kPrBlock, 0, st>>>(nnz, a.rowind, indeg, val);
+  GB_CUDA_TRY(cudaGetLastError());
+  GB_CUDA_TRY(cudaStreamSynchronize(st));
+  return GOOSEBERRY_SUCCESS;
+}
+
 __global__ void pr_fill_kernel(size_t n, double * __restrict__ v, double value) {
   for (size_t k = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; k < n;
        k += static_cast<size_t>(gridDim.x) * blockDim.x)
@@ -132,41 +226,19 @@ int pagerank_f64(dim_t n, const ind_t * rowptr, const dim_t * rowind, const doub
   const uint32_t nnz = rowptr[n];
   GB_CHECK_INPUT(nnz == 0 || (rowind && rowval), "NULL array");
   GB_CHECK_INPUT(rowptr[0] == 0, "rowptr[0] must be 0");
-  // normalise like src/gooseberry_bin.c:2611-2630.  Host threads split the
-  // COLUMNS: each scans all entries in row order and sums only its own
-  // columns, so every column sum is accumulated in the reference's order.
+  // the sinks: rows without entries (src/gooseberry_bin.c:2611-2618)
   std::vector<uint32_t> sinks;
   for (dim_t k = 0; k < n; ++k) {
     GB_CHECK_INPUT(rowptr[k + 1] >= rowptr[k], "rowptr decreases at row %u", k);
     if (rowptr[k] == rowptr[k + 1]) sinks.push_back(k);
   }
-  for (ind_t l = 0; l < nnz; ++l)
-    GB_CHECK_INPUT(rowind[l] < n, "column index %u out of range for %u columns", rowind[l], n);
-  std::vector<double> indeg(n, 0.0), val(nnz ? nnz : 1);
-  const unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-  auto parallel = [&](auto && body) {
-    std::vector<std::thread> th;
-    for (unsigned t = 0; t < nt; ++t) th.emplace_back(body, t);
-    for (auto & x : th) x.join();
-  };
-  parallel([&](unsigned t) {
-    const uint32_t c0 = static_cast<uint32_t>(static_cast<uint64_t>(n) * t / nt);
-    const uint32_t c1 = static_cast<uint32_t>(static_cast<uint64_t>(n) * (t + 1) / nt);
-    for (ind_t l = 0; l < nnz; ++l) {
-      const uint32_t c = rowind[l];
-      if (c >= c0 && c < c1) indeg[c] += rowval[l];
-    }
-  });
-  parallel([&](unsigned t) {
-    const ind_t l0 = static_cast<ind_t>(static_cast<uint64_t>(nnz) * t / nt);
-    const ind_t l1 = static_cast<ind_t>(static_cast<uint64_t>(nnz) * (t + 1) / nt);
-    for (ind_t l = l0; l < l1; ++l) val[l] = rowval[l] / indeg[rowind[l]];
-  });
-
+  // upload the raw values (gb_csr_create checks the column indices) and
+  // normalise them on the device
   PrBuffers B;
   GB_CUDA_TRY(cudaStreamCreateWithFlags(&B.st, cudaStreamNonBlocking));
-  GB_TRY(gb_csr_create(n, n, nnz, rowptr, rowind, val.data(), nullptr, GB_CSR_VALUES_F64, B.st,
+  GB_TRY(gb_csr_create(n, n, nnz, rowptr, rowind, rowval, nullptr, GB_CSR_VALUES_F64, B.st,
       &B.a));
+  GB_TRY(normalise_device(*B.a, B.st));
   int sms = 148;
   GB_TRY(sm_count_of_current_device(&sms));
   const unsigned g = static_cast<unsigned>(std::max<size_t>(1, std::min<size_t>(
