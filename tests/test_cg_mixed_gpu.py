@@ -73,3 +73,25 @@ def test_mixed_needs_both_value_widths():
     A = W.laplacian_2d(8)
     with pytest.raises(gb.GooseberryError):
         gb.CgSolver(gb.CsrMatrix.from_host(A, f64=True, f32=False), mode=gb.CG_MIXED)
+
+
+@pytest.mark.parametrize("mode", [gb.CG_F64, gb.CG_MIXED])
+def test_profile_times_each_kernel_and_leaves_the_solver_ready(torch, mode):
+    """gb_cg_profile runs the first iterations launch by launch (the mixed
+    solver's FP64 step every time) and reports one mean time per kernel; a
+    solve afterwards equals a solve on a fresh solver bit for bit."""
+    A = W.diffusion_3d(20, seed=33)
+    M = gb.CsrMatrix.from_host(A, f64=True, f32=True)
+    b = torch.from_numpy(W.rhs(A.nrows, 34)).cuda()
+    S = gb.CgSolver(M, mode)
+    ms = S.profile(b, iterations=7)
+    assert len(ms) == (2 if mode == gb.CG_F64 else 3)
+    assert all(t > 0 for t in ms)
+    x1, r1 = S.solve(b, tol=1e-10)
+    F = gb.CgSolver(M, mode)
+    x2, r2 = F.solve(b, tol=1e-10)
+    assert r1.status == r2.status == "converged" and r1.iterations == r2.iterations
+    assert torch.equal(x1, x2)
+    S.close()
+    F.close()
+    M.close()
