@@ -108,6 +108,10 @@ extern "C" {
 #define gooseberry_permute_sparse gooseberry_permute_sparse_f64
 #endif
 
+/* Message of the last failed call on this thread (no reference counterpart:
+ * the reference prints its errors).  Also declared in gooseberry_b200.h. */
+GOOSEBERRY_API const char * gb_last_error(void);
+
 /*
  * val[i] *= s for i < n.
  * Replaces gooseberry_scale (reference include/gooseberry.h:134-137,
