@@ -158,3 +158,39 @@ def test_invalid_inputs_are_rejected():
     # empty block list: nothing ordered, as in the reference
     perm = gb.cuthillmckee(A.rowptr, A.rowind, 1000, blocks=[0])
     assert perm.shape == (1000,)
+
+
+@pytest.mark.parametrize("case", ["one", "no_entries", "two_components", "anti_diagonal",
+                                  "empty_blocks", "outside_columns"])
+def test_edge_cases_match_oracle(case):
+    """Degenerate graphs: one vertex, rows without entries (every vertex its own
+    component, taken in id order), two components, an anti-diagonal (vertex i
+    joined to n-1-i), empty row
+    blocks, columns outside the matrix (ignored, as the reference's range
+    test ignores them)."""
+    blocks = None
+    if case == "one":
+        rp, ri, n = np.array([0, 1], np.uint32), np.array([0], np.uint32), 1
+    elif case == "no_entries":
+        n = 50
+        rp, ri = np.zeros(n + 1, np.uint32), np.zeros(0, np.uint32)
+    elif case == "two_components":
+        n = 6  # 0-1-2 and 3-4-5 paths, listed backwards
+        rows = [[1], [0, 2], [1], [4], [3, 5], [4]]
+        rp = np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.uint32)
+        ri = np.array([c for r in rows for c in r], np.uint32)
+    elif case == "anti_diagonal":
+        n = 40
+        rp, ri = np.arange(n + 1, dtype=np.uint32), np.arange(n, dtype=np.uint32)[::-1].copy()
+    elif case == "empty_blocks":
+        A = W.uniform_rows(2000, 6, seed=47)
+        rp, ri, n = A.rowptr, A.rowind, A.nrows
+        blocks = np.array([0, 0, 700, 700, 700, 2000, 2000], np.uint32)
+    else:
+        A = W.uniform_rows(3000, 6, seed=48)
+        rp, ri, n = A.rowptr, A.rowind, A.nrows
+        blocks = np.array([0, 1000, 3000], np.uint32)  # columns past a block are outside it
+    want = oracle.cuthillmckee(rp, ri, n, blocks=blocks)
+    got = gb.cuthillmckee(rp, ri, n, blocks=blocks)
+    assert np.array_equal(got, want)
+    assert np.array_equal(np.sort(got), np.arange(n))

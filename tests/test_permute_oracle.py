@@ -89,3 +89,18 @@ def test_permute_sparse_matches_reference_random():
         rc, *r = oracle.ref_permute_sparse(A.rowptr, A.rowind, A.rowval, 5000, a, b)
         assert rc == 1
         assert all(np.array_equal(x, y) for x, y in zip(o, r))
+
+
+@pytest.mark.skipif(not oracle.ref_available("f64"), reason="reference build absent")
+def test_degenerate_graphs_match_reference():
+    cases = [
+        (np.array([0, 1], np.uint32), np.array([0], np.uint32), 1, None),
+        (np.zeros(51, np.uint32), np.zeros(0, np.uint32), 50, None),
+        (np.arange(41, dtype=np.uint32), np.arange(40, dtype=np.uint32)[::-1].copy(), 40, None),
+        (np.zeros(11, np.uint32), np.zeros(0, np.uint32), 10, np.array([0, 0, 5, 5, 10], np.uint32)),
+    ]
+    for rp, ri, n, blocks in cases:
+        rc, ref = oracle.ref_cuthillmckee(rp, ri if len(ri) else np.zeros(1, np.uint32), n,
+                                          blocks=blocks)
+        assert rc == 1
+        assert np.array_equal(oracle.cuthillmckee(rp, ri, n, blocks=blocks), ref)
