@@ -649,7 +649,9 @@ def serving_extra(nreq=400, seed=5, rtol=1e-10, pool=16 << 30, slots=256, ips=16
     under Poisson arrivals are the exact FIFO single-server replay of the
     measured service times.  Ours: the continuous-batching server (mixed
     precision, 16 GB pool), driven in real time by the same arrival times.
-    Arrival rate = `load` x the baseline's saturation throughput."""
+    Arrival rate = `load` x the baseline's saturation throughput.  A second
+    FP64 reference point: the same server in FP64 with one slot (one solve at
+    a time without the drop-in's per-request setup), at saturation."""
     import gooseberry_b200 as gb
     from gooseberry_b200 import workloads as W
     sides = W.serving_sides(nreq, seed)
@@ -689,6 +691,18 @@ def serving_extra(nreq=400, seed=5, rtol=1e-10, pool=16 << 30, slots=256, ips=16
     for r in res:
         A, b = reqs[r.id][1], reqs[r.id][2]
         worst = max(worst, float(np.linalg.norm(b - A.to_scipy() @ r.x) / np.linalg.norm(b)))
+    # --- a second FP64 reference point: the same server in FP64 with one slot
+    # (one solve at a time, no per-request setup), at saturation after a warm pass
+    one = gb.Server(pool_bytes=pool, max_slots=1, mode=gb.CG_F64, iters_per_step=ips)
+    for k, A, b in reqs[::10]:
+        one.submit(k, A, b, tol=rtol)
+    one.drain(timeout_s=3600)
+    t0 = time.perf_counter()
+    for k, A, b in reqs:
+        one.submit(k, A, b, tol=rtol)
+    res_one = one.drain(timeout_s=3600)
+    one_thr = len(res_one) / (time.perf_counter() - t0)
+    one.close()
     # --- latency at load x baseline throughput
     lam = load * base_thr
     arr = W.poisson_arrivals(nreq, lam, seed)
@@ -726,6 +740,9 @@ def serving_extra(nreq=400, seed=5, rtol=1e-10, pool=16 << 30, slots=256, ips=16
             r.status == "converged" for r in res), "worst_true_rel_residual": worst,
             "iterations_median": float(np.median([r.iterations for r in res])),
             "p50_s": pct(lat, 50), "p99_s": pct(lat, 99), "completed_at_load": len(got)},
+        "fp64_server_one_slot": {"solves_per_s": one_thr, "converged": sum(
+            r.status == "converged" for r in res_one),
+            "speedup_mixed_batched_over_it": sat_thr / one_thr},
         "arrival_rate_per_s": lam,
         "speedup_solves_per_s": sat_thr / base_thr,
     }
