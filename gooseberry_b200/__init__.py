@@ -31,7 +31,7 @@ import numpy as np
 __all__ = [
     "GooseberryError", "lib", "spmult", "scale", "add_scalar", "cgd", "pagerank",
     "read_csr", "read_grid", "write_csr", "write_grid", "cuthillmckee", "permute_sparse",
-    "permute_vector",
+    "permute_dense", "permute_vector",
     "CsrMatrix", "CgSolver", "CgResult", "dot", "spdot", "SUCCESS",
     "SCHED_AUTO", "SCHED_THREAD", "SCHED_GROUP4", "SCHED_GROUP8", "SCHED_WARP",
     "SCHED_MERGE", "SCHED_ROW", "SCHED_WTILE", "SCHED_WMERGE", "CG_F64", "CG_MIXED",
@@ -106,6 +106,10 @@ SIGNATURES = {
     "gooseberry_permute_cuthillmckee": (_i, [_u32, _u32, _vp, _vp, _vp, _vp, _u32, _vp]),
     "gooseberry_permute_sparse": (_i, [_u32, _u32, _vp, _vp, _vp, _vp, _vp]),
     "gooseberry_permute_sparse_f64": (_i, [_u32, _u32, _vp, _vp, _vp, _vp, _vp]),
+    "gooseberry_permute_dense": (_i, [_u32, _u32, _vp, _vp, _vp]),
+    "gooseberry_permute_dense_f64": (_i, [_u32, _u32, _vp, _vp, _vp]),
+    "gooseberry_permute_dense_rev": (_i, [_u32, _u32, _vp, _vp, _vp]),
+    "gooseberry_permute_dense_rev_f64": (_i, [_u32, _u32, _vp, _vp, _vp]),
     "gb_csr_cuthillmckee": (_i, [_vp, _vp, _u32, _vp, _vp]),
     "gb_csr_permute": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "gb_permute_vector_f64": (_i, [_sz, _vp, _vp, _i, _vp, _vp]),
@@ -385,6 +389,22 @@ def permute_sparse(rowptr, rowind, rowval, ncols: int, rowperm=None, colperm=Non
     _check(fn(len(rowptr) - 1, ncols, _ptr(rowptr), _ptr(rowind), _ptr(rowval), _ptr(rp),
               _ptr(cp)), "gooseberry_permute_sparse")
     return rowptr, rowind, rowval
+
+
+def permute_dense(vals, nrows: int, ncols: int, rowperm=None, colperm=None,
+                  reverse: bool = False):
+    """Permuted copy of a row-major host matrix (``gooseberry_permute_dense``
+    / ``_rev``, reference src/permute.c:208-283): forward ``out[i][j] =
+    in[rowperm[i]][colperm[j]]``, reverse ``out[rowperm[i]][colperm[j]] =
+    in[i][j]``."""
+    real = _real(np.asarray(vals).dtype)
+    a = np.array(vals, dtype=np.float64 if real == "f64" else np.float32).reshape(-1)
+    rp = None if rowperm is None else np.ascontiguousarray(rowperm, dtype=np.uint32)
+    cp = None if colperm is None else np.ascontiguousarray(colperm, dtype=np.uint32)
+    name = "gooseberry_permute_dense" + ("_rev" if reverse else "") + (
+        "_f64" if real == "f64" else "")
+    _check(getattr(lib(), name)(nrows, ncols, _ptr(a), _ptr(rp), _ptr(cp)), name)
+    return a
 
 
 def permute_vector(x, perm, reverse: bool = False, stream=None):

@@ -730,6 +730,23 @@ __global__ void pm_copy_kernel(const uint32_t * __restrict__ rowptr,
   }
 }
 
+// Dense row-major nrows x ncols: out[i][j] = in[rowperm[i]][colperm[j]], or
+// out[rowperm[i]][colperm[j]] = in[i][j] when reverse (null: identity).
+template <typename T>
+__global__ void pm_dense_kernel(uint32_t nrows, uint32_t ncols, const T * __restrict__ in,
+    T * __restrict__ out, const uint32_t * __restrict__ rowperm,
+    const uint32_t * __restrict__ colperm, int reverse) {
+  const size_t total = static_cast<size_t>(nrows) * ncols;
+  for (size_t q = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; q < total;
+       q += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const uint32_t i = static_cast<uint32_t>(q / ncols), j = static_cast<uint32_t>(q % ncols);
+    const size_t v = rowperm ? rowperm[i] : i;
+    const size_t u = colperm ? colperm[j] : j;
+    if (reverse) out[v * ncols + u] = in[q];
+    else out[q] = in[v * ncols + u];
+  }
+}
+
 __global__ void pm_vector_kernel(const double * x, const uint32_t * perm, uint32_t n, int reverse,
     double * y) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -818,6 +835,43 @@ int upload(gb::ScratchSet & sc, T ** d, const T * h, size_t count, cudaStream_t 
   return GOOSEBERRY_SUCCESS;
 }
 
+// A permutation of 0..n-1 (checked on the host: the caller's arrays).
+int check_perm_host(const uint32_t * perm, uint32_t n, const char * what) {
+  if (!perm) return GOOSEBERRY_SUCCESS;
+  std::vector<unsigned char> seen(n, 0);
+  for (uint32_t i = 0; i < n; ++i) {
+    GB_CHECK_INPUT(perm[i] < n && !seen[perm[i]], "%s is not a permutation of 0..%u", what,
+        n - 1);
+    seen[perm[i]] = 1;
+  }
+  return GOOSEBERRY_SUCCESS;
+}
+
+template <typename T>
+int permute_dense_host(dim_t nrows, dim_t ncols, T * rowval, const dim_t * rowperm,
+    const dim_t * colperm, int reverse) {
+  if (!rowperm && !colperm) return GOOSEBERRY_SUCCESS;
+  const size_t total = static_cast<size_t>(nrows) * ncols;
+  if (total == 0) return GOOSEBERRY_SUCCESS;
+  GB_CHECK_INPUT(rowval != nullptr, "rowval is NULL");
+  GB_TRY(check_perm_host(rowperm, nrows, "rowperm"));
+  GB_TRY(check_perm_host(colperm, ncols, "colperm"));
+  cudaStream_t s = nullptr;
+  gb::ScratchSet sc(s);
+  T *in, *out;
+  uint32_t *rpm = nullptr, *cpm = nullptr;
+  GB_TRY(upload(sc, &in, rowval, total, s));
+  GB_TRY(sc.get(&out, total));
+  if (rowperm) GB_TRY(upload(sc, &rpm, rowperm, nrows, s));
+  if (colperm) GB_TRY(upload(sc, &cpm, colperm, ncols, s));
+  gb::pm_dense_kernel<T><<<gb::grid_for(total, 256), 256, 0, s>>>(nrows, ncols, in, out, rpm, cpm,
+      reverse);
+  GB_CUDA_TRY(cudaGetLastError());
+  GB_CUDA_TRY(cudaMemcpyAsync(rowval, out, total * sizeof(T), cudaMemcpyDeviceToHost, s));
+  GB_CUDA_TRY(cudaStreamSynchronize(s));
+  return GOOSEBERRY_SUCCESS;
+}
+
 template <typename T>
 int permute_sparse_host(dim_t nrows, dim_t ncols, ind_t * rowptr, dim_t * rowind, T * rowval,
     const dim_t * rowperm, const dim_t * colperm) {
@@ -900,6 +954,30 @@ int gooseberry_permute_sparse_f64(dim_t nrows, dim_t ncols, ind_t * rowptr, dim_
     double * rowval, const dim_t * rowperm, const dim_t * colperm) {
   gb::clear_error();
   return permute_sparse_host(nrows, ncols, rowptr, rowind, rowval, rowperm, colperm);
+}
+
+int gooseberry_permute_dense(dim_t nrows, dim_t ncols, float * rowval, const dim_t * rowperm,
+    const dim_t * colperm) {
+  gb::clear_error();
+  return permute_dense_host(nrows, ncols, rowval, rowperm, colperm, 0);
+}
+
+int gooseberry_permute_dense_f64(dim_t nrows, dim_t ncols, double * rowval,
+    const dim_t * rowperm, const dim_t * colperm) {
+  gb::clear_error();
+  return permute_dense_host(nrows, ncols, rowval, rowperm, colperm, 0);
+}
+
+int gooseberry_permute_dense_rev(dim_t nrows, dim_t ncols, float * rowval,
+    const dim_t * rowperm, const dim_t * colperm) {
+  gb::clear_error();
+  return permute_dense_host(nrows, ncols, rowval, rowperm, colperm, 1);
+}
+
+int gooseberry_permute_dense_rev_f64(dim_t nrows, dim_t ncols, double * rowval,
+    const dim_t * rowperm, const dim_t * colperm) {
+  gb::clear_error();
+  return permute_dense_host(nrows, ncols, rowval, rowperm, colperm, 1);
 }
 
 int gb_csr_cuthillmckee(const gb_csr_t * a, const dim_t * blocks, dim_t nblocks, dim_t * perm,

@@ -106,6 +106,8 @@ extern "C" {
 #define gooseberry_write_sparse_matrix gooseberry_write_sparse_matrix_f64
 #define gooseberry_write_dense_matrix gooseberry_write_dense_matrix_f64
 #define gooseberry_permute_sparse gooseberry_permute_sparse_f64
+#define gooseberry_permute_dense gooseberry_permute_dense_f64
+#define gooseberry_permute_dense_rev gooseberry_permute_dense_rev_f64
 #endif
 
 /* Message of the last failed call on this thread (no reference counterpart:
@@ -250,6 +252,26 @@ GOOSEBERRY_API int gooseberry_permute_sparse(dim_t nrows, dim_t ncols, ind_t * r
     dim_t * rowind, real_t * rowval, const dim_t * rowperm, const dim_t * colperm);
 GOOSEBERRY_API int gooseberry_permute_sparse_f64(dim_t nrows, dim_t ncols, ind_t * rowptr,
     dim_t * rowind, double * rowval, const dim_t * rowperm, const dim_t * colperm);
+
+/*
+ * In-place dense permutation of a row-major nrows x ncols matrix: replaces
+ * permute_dense (reference src/permute.h:51-56, src/permute.c:208-242;
+ * row[i][j] <- row[rowperm[i]][colperm[j]]) and permute_dense_rev (:59-64,
+ * :248-283; row[rowperm[i]][colperm[j]] <- row[i][j]), which matrix_permute
+ * applies to dense vectors and matrices (src/matrix.c:256-342), e.g. the
+ * right-hand side after a Cuthill-McKee reorder (src/gooseberry_bin.c:1674).
+ * NULL permutations mean identity.  A rowperm / colperm that is not a
+ * permutation gives GOOSEBERRY_ERROR_INVALIDINPUT (the reference does not
+ * check).  Runs on the GPU.
+ */
+GOOSEBERRY_API int gooseberry_permute_dense(dim_t nrows, dim_t ncols, real_t * rowval,
+    const dim_t * rowperm, const dim_t * colperm);
+GOOSEBERRY_API int gooseberry_permute_dense_f64(dim_t nrows, dim_t ncols, double * rowval,
+    const dim_t * rowperm, const dim_t * colperm);
+GOOSEBERRY_API int gooseberry_permute_dense_rev(dim_t nrows, dim_t ncols, real_t * rowval,
+    const dim_t * rowperm, const dim_t * colperm);
+GOOSEBERRY_API int gooseberry_permute_dense_rev_f64(dim_t nrows, dim_t ncols, double * rowval,
+    const dim_t * rowperm, const dim_t * colperm);
 
 #ifdef __cplusplus
 }

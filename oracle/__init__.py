@@ -77,6 +77,9 @@ def _lib():
                                                           _u32p, p, C.c_void_p, C.c_void_p,
                                                           _u32p, _u32p, p]
                 lib.oracle_permute_sparse_f64.restype = None
+                lib.oracle_permute_dense_f64.argtypes = [C.c_uint32, C.c_uint32, p, p,
+                                                         C.c_void_p, C.c_void_p, C.c_int]
+                lib.oracle_permute_dense_f64.restype = None
             f = getattr(lib, f"oracle_cgd_{real}")
             f.argtypes = [C.c_uint32, _u32p, _u32p, p, p, p, ctype, C.c_size_t,
                           C.c_void_p, C.c_size_t, C.POINTER(C.c_double), C.c_int]
@@ -126,6 +129,8 @@ def _ref(real: str = "f64"):
         lib.gbref_cuthillmckee.restype = C.c_int
         lib.gbref_permute_sparse.argtypes = [C.c_uint32, C.c_uint32, _u32p, _u32p, p, vp, vp]
         lib.gbref_permute_sparse.restype = C.c_int
+        lib.gbref_permute_dense.argtypes = [C.c_uint32, C.c_uint32, p, vp, vp, C.c_int]
+        lib.gbref_permute_dense.restype = C.c_int
         lib.gbref_cgd.argtypes = [C.c_uint32, _u32p, _u32p, p, p, p, C.c_double,
                                   C.c_size_t, C.POINTER(C.c_size_t),
                                   C.POINTER(C.c_double), C.c_void_p, C.c_size_t]
@@ -436,4 +441,27 @@ def ref_permute_sparse(rowptr, rowind, rowval, ncols, rowperm=None, colperm=None
     del rk, ck
     nnz = int(rowptr[-1])
     return rc, rowptr, rowind[:nnz], rowval[:nnz]
+
+
+def permute_dense(vals, nrows, ncols, rowperm=None, colperm=None, reverse=False):
+    """Restated permute_dense / permute_dense_rev (src/permute.c:208-283), FP64,
+    row-major, out of place."""
+    a = np.ascontiguousarray(vals, dtype=np.float64)
+    out = np.zeros_like(a) if reverse else np.empty_like(a)
+    rp, rk = _perm_arg(rowperm)
+    cp, ck = _perm_arg(colperm)
+    _lib().oracle_permute_dense_f64(nrows, ncols, a, out, rp, cp, int(reverse))
+    del rk, ck
+    return out
+
+
+def ref_permute_dense(vals, nrows, ncols, rowperm=None, colperm=None, reverse=False,
+                      real="f64"):
+    """The reference's own permute_dense / permute_dense_rev on a copy."""
+    a = np.array(vals, dtype=_dt(real))
+    rp, rk = _perm_arg(rowperm)
+    cp, ck = _perm_arg(colperm)
+    rc = _ref(real).gbref_permute_dense(nrows, ncols, a, rp, cp, int(reverse))
+    del rk, ck
+    return rc, a
 

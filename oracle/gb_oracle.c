@@ -420,3 +420,26 @@ void oracle_permute_sparse_f64(uint32_t nrows, uint32_t ncols, const uint32_t * 
   }
   free(rename);
 }
+
+/*
+ * Dense permutation -- src/permute.c:208-242 (permute_dense) and :248-283
+ * (permute_dense_rev), out of place, row-major nrows x ncols:
+ *   forward: out[i][j] = in[rowperm[i]][colperm[j]]
+ *   reverse: out[rowperm[i]][colperm[j]] = in[i][j]
+ * with a NULL permutation meaning identity.
+ */
+void oracle_permute_dense_f64(uint32_t nrows, uint32_t ncols, const double * in, double * out,
+    const uint32_t * rowperm, const uint32_t * colperm, int reverse);
+void oracle_permute_dense_f64(uint32_t nrows, uint32_t ncols, const double * in, double * out,
+    const uint32_t * rowperm, const uint32_t * colperm, int reverse)
+{
+  uint32_t i, j;
+  for (i = 0; i < nrows; ++i) {
+    const size_t v = rowperm ? rowperm[i] : i;
+    for (j = 0; j < ncols; ++j) {
+      const size_t u = colperm ? colperm[j] : j;
+      if (reverse) out[v * ncols + u] = in[(size_t)i * ncols + j];
+      else out[(size_t)i * ncols + j] = in[v * ncols + u];
+    }
+  }
+}

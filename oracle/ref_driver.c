@@ -25,9 +25,10 @@
  *   one "ITER: k RMSE: v" line per iteration (src/cgd.c:116) and returns no
  *   iteration count, so stdout is redirected to a temporary file for the call
  *   and the ITER lines are parsed back into (iterations, last norm, history).
- * - gbref_cuthillmckee / gbref_permute_sparse: forward to
- *   permute_cuthillmckee (src/permute.c:288-337) and permute_sparse
- *   (src/permute.c:120-205), compiled from src/permute.c against the shim's
+ * - gbref_cuthillmckee / gbref_permute_sparse / gbref_permute_dense: forward
+ *   to permute_cuthillmckee (src/permute.c:288-337), permute_sparse
+ *   (src/permute.c:120-205) and permute_dense / permute_dense_rev
+ *   (src/permute.c:208-283), compiled from src/permute.c against the shim's
  *   priority queue (oracle/shim/dlpq_headers.h), which breaks equal-degree
  *   ties by the smaller vertex id.
  */
@@ -72,6 +73,8 @@ int gbref_cuthillmckee(dim_t nrows, dim_t ncols, const ind_t * rowptr,
 int gbref_permute_sparse(dim_t nrows, dim_t ncols, ind_t * rowptr,
     dim_t * rowind, real_t * rowval, const dim_t * rowperm,
     const dim_t * colperm);
+int gbref_permute_dense(dim_t nrows, dim_t ncols, real_t * rowval,
+    const dim_t * rowperm, const dim_t * colperm, int reverse);
 
 /* OpenMP thread count of the reference's parallel regions.  With 1 thread
  * blas_dot sums in index order, which makes cgd bit-reproducible. */
@@ -288,3 +291,13 @@ int gbref_permute_sparse(dim_t nrows, dim_t ncols, ind_t * rowptr,
 {
   return permute_sparse(nrows, ncols, rowptr, rowind, rowval, rowperm, colperm);
 }
+
+/* In-place dense permutation (src/permute.c:208-242) or its reverse
+ * (src/permute.c:248-283), row-major nrows x ncols. */
+int gbref_permute_dense(dim_t nrows, dim_t ncols, real_t * rowval,
+    const dim_t * rowperm, const dim_t * colperm, int reverse)
+{
+  return reverse ? permute_dense_rev(nrows, ncols, rowval, rowperm, colperm)
+                 : permute_dense(nrows, ncols, rowval, rowperm, colperm);
+}
+

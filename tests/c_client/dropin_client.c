@@ -3,7 +3,7 @@
  * gooseberry would (include/gooseberry.h names, argument order, status
  * codes), linked with libgooseberry_b200.so instead of libgooseberry:
  * SpMV with one and with three right-hand sides, CG, the Cuthill-McKee order
- * and a sparse permutation on a small tridiagonal system.  Exits 0 and prints
+ * and sparse and dense permutations on a small tridiagonal system.  Exits 0 and prints
  * "dropin ok" when every result is right.
  */
 #define GOOSEBERRY_DOUBLE_REALS 1
@@ -67,6 +67,12 @@ int main(void) {
     for (k = rowptr[i]; k < rowptr[i + 1]; ++k)
       if (rowind[k] + 1 < i || rowind[k] > i + 1) { fprintf(stderr, "band\n"); return 1; }
   }
+  /* the right-hand side follows the reorder and comes back with its reverse */
+  rc = gooseberry_permute_dense(N, 1, b, perm, NULL);
+  if (rc != GOOSEBERRY_SUCCESS) return fail("gooseberry_permute_dense", rc);
+  rc = gooseberry_permute_dense_rev(N, 1, b, perm, NULL);
+  if (rc != GOOSEBERRY_SUCCESS) return fail("gooseberry_permute_dense_rev", rc);
+  if (b[0] != 1.0 || b[N - 1] != 1.0 || b[1] != 0.0) { fprintf(stderr, "dense\n"); return 1; }
   /* a bad call comes back as the reference's error code */
   if (gooseberry_permute_cuthillmckee(N, N + 1, rowptr, rowind, rowval, NULL, 0, perm) !=
       GOOSEBERRY_ERROR_INVALIDINPUT) { fprintf(stderr, "error code\n"); return 1; }

@@ -113,6 +113,10 @@ def test_reordering_entry_points_reject_bad_input_before_any_device_work():
         gb.permute_sparse(rowptr, np.array([0, 1, 1, 0, 7], np.uint32), vals, 3, None,
                           np.array([2, 1, 0], np.uint32))
     assert e.value.code == 3
+    with pytest.raises(gb.GooseberryError) as e:  # not a permutation
+        gb.permute_dense(np.ones(6), 3, 2, np.array([0, 0, 1], np.uint32))
+    assert e.value.code == 3
+    assert np.array_equal(gb.permute_dense(np.arange(6.0), 3, 2), np.arange(6.0))
     # no permutation: nothing to do, arrays come back unchanged
     rp, ri, rv = gb.permute_sparse(rowptr, rowind, vals, 3)
     assert np.array_equal(rp, rowptr) and np.array_equal(ri, rowind)

@@ -194,3 +194,19 @@ def test_edge_cases_match_oracle(case):
     got = gb.cuthillmckee(rp, ri, n, blocks=blocks)
     assert np.array_equal(got, want)
     assert np.array_equal(np.sort(got), np.arange(n))
+
+
+def test_drop_in_permute_dense_matches_oracle():
+    """gooseberry_permute_dense[_rev] (src/permute.c:208-283) on a row-major
+    matrix and on a vector (one column), both widths, both directions."""
+    rng = np.random.default_rng(49)
+    for nr, nc in ((1000, 1), (257, 33)):
+        a = rng.random(nr * nc)
+        rp = rng.permutation(nr).astype(np.uint32)
+        cp = rng.permutation(nc).astype(np.uint32)
+        for r, c in ((rp, cp), (rp, None), (None, cp)):
+            for rev in (False, True):
+                want = oracle.permute_dense(a, nr, nc, r, c, rev)
+                assert np.array_equal(gb.permute_dense(a, nr, nc, r, c, rev), want)
+                got32 = gb.permute_dense(a.astype(np.float32), nr, nc, r, c, rev)
+                assert np.array_equal(got32, want.astype(np.float32))

@@ -104,3 +104,20 @@ def test_degenerate_graphs_match_reference():
                                           blocks=blocks)
         assert rc == 1
         assert np.array_equal(oracle.cuthillmckee(rp, ri, n, blocks=blocks), ref)
+
+
+@pytest.mark.skipif(not oracle.ref_available("f64"), reason="reference build absent")
+def test_permute_dense_restatement_matches_reference():
+    rng = np.random.default_rng(9)
+    nr, nc = 31, 7
+    a = rng.random(nr * nc)
+    rp = rng.permutation(nr).astype(np.uint32)
+    cp = rng.permutation(nc).astype(np.uint32)
+    for r, c in ((rp, cp), (rp, None), (None, cp)):
+        for rev in (False, True):
+            rc, ref = oracle.ref_permute_dense(a, nr, nc, r, c, rev)
+            assert rc == 1
+            assert np.array_equal(oracle.permute_dense(a, nr, nc, r, c, rev), ref)
+    # the reverse undoes the forward permutation
+    f = oracle.permute_dense(a, nr, nc, rp, cp)
+    assert np.array_equal(oracle.permute_dense(f, nr, nc, rp, cp, reverse=True), a)
