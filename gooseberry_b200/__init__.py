@@ -297,14 +297,25 @@ _libc.free.argtypes = [C.c_void_p]
 _libc.free.restype = None
 
 
+class _MallocBuffer:
+    """A malloc'ed C array seen as a numpy array without a copy; freed when the
+    last array that uses it goes away."""
+
+    def __init__(self, addr: int, n: int, dtype):
+        self._addr = addr
+        self.__array_interface__ = {"shape": (n,), "typestr": np.dtype(dtype).str,
+                                    "data": (addr, False), "version": 3}
+
+    def __del__(self):
+        _libc.free(C.c_void_p(self._addr))
+
+
 def _take(ptr, ctype, n, dtype):
-    """Copy n elements out of a malloc'ed C array and free it."""
-    if n:
-        a = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ctype)), (n,)).copy()
-    else:
-        a = np.zeros(0, dtype=dtype)
+    """n elements of a malloc'ed C array as a numpy array that owns it."""
+    if n and ptr.value:
+        return np.asarray(_MallocBuffer(ptr.value, n, dtype))
     _libc.free(ptr)
-    return a
+    return np.zeros(0, dtype=dtype)
 
 
 def read_csr(path, f64: bool = True):
