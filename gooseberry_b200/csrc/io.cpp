@@ -175,7 +175,6 @@ bool is_space(char c) {
 unsigned long long parse_ull(const char * s, char ** end) {
   const char * q = s;
   while (is_space(*q)) ++q;
-  const char * d = q;
   unsigned long long v = 0;
   int nd = 0;
   while (*q >= '0' && *q <= '9' && nd < 19) {
@@ -184,7 +183,6 @@ unsigned long long parse_ull(const char * s, char ** end) {
     ++nd;
   }
   if (nd == 0 || (*q >= '0' && *q <= '9')) return std::strtoull(s, end, 10);
-  (void)d;
   *end = const_cast<char *>(q);
   return v;
 }
