@@ -114,6 +114,9 @@ GOOSEBERRY_API int gb_csr_read(const char * file, unsigned flags, gb_stream_t st
 /* Release a matrix (matrix_free, reference src/matrix.c:483-535). */
 GOOSEBERRY_API int gb_csr_destroy(gb_csr_t * a);
 
+/* Shape, row-length summary, tile plan and current schedules of a matrix
+ * (host struct; no GPU work).  The reference's matrix_t exposes only the
+ * shape and the arrays (src/matrix.h:37-45). */
 GOOSEBERRY_API int gb_csr_get_info(const gb_csr_t * a, gb_csr_info_t * info);
 
 /* Fix the SpMV schedule of one value width (GB_CSR_VALUES_F64 or _F32).
