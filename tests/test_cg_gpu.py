@@ -110,3 +110,30 @@ def test_persistent_and_graph_paths_agree(torch, cg_golden):
         for k, x in out.items():
             assert np.linalg.norm(x - ref) <= 1e-4 * np.linalg.norm(ref), (name, k)
 
+
+
+def test_float_abi_cgd_matches_float_reference(cg_golden):
+    """The float drop-in (gooseberry_cgd, the reference's default real_t build)
+    solves in double on the device and rounds x to float.  Against the FP64
+    oracle on the same float-rounded matrix, right-hand side and threshold:
+    iterations +-2, x to CG accuracy.  Against the reference's own float build
+    (iterations parsed from its ITER lines): iterations +-2, x to 1e-4."""
+    import oracle
+    c = cg_golden["laplace64"]
+    v32 = c["rowval"].astype(np.float32)
+    b32 = c["b"].astype(np.float32)
+    err = float(np.float32(c["error"]))
+    niter = int(c["niter"])
+    x, it, rn = gb.cgd(c["rowptr"], c["rowind"], v32, b32, err, niter)
+    assert x.dtype == np.float32
+    assert rn <= err
+    xo, ito, _ = oracle.cgd(c["rowptr"], c["rowind"], v32.astype(np.float64),
+                            b32.astype(np.float64), err, niter)
+    assert abs(it - ito) <= 2, (it, ito)
+    assert np.linalg.norm(x - xo) <= 1e-4 * np.linalg.norm(xo)
+    if oracle.ref_available("f32"):
+        oracle.ref_set_threads(1)
+        xr, itr, _ = oracle.ref_cgd(c["rowptr"], c["rowind"], v32, b32, err, niter,
+                                    real="f32")
+        assert abs(it - itr) <= 2, (it, itr)
+        assert np.linalg.norm(x - xr) <= 1e-4 * np.linalg.norm(xr)
