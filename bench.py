@@ -1010,7 +1010,8 @@ def run_reference_cg(args):
     return {
         "impl": "reference",
         "metric": "CG solves/s (FP64, 2D 5-point Laplacian 1024x1024, rel-res 1e-8)",
-        "value": v, "unit": "solves/s", "n_gpus": 0, "steps": args.steps,
+        "value": v, "unit": "solves/s", "n_gpus": args.gpus, "gpus_used": 0,
+        "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic: seeded b ~ U[-1,1] (seed 2), exact 5-point Laplacian",
