@@ -121,3 +121,57 @@ def test_error_codes(tmp_path):
     assert rc == 2  # GOOSEBERRY_ERROR_UNIMPLEMENTED (GRAPH format)
     rc = L.gooseberry_read_sparse_matrix_f64(42, str(p).encode(), *[o.ctypes.data for o in out])
     assert rc == 3  # unknown format
+
+
+def _odd_values(rng, m):
+    """Values whose %g spelling has edge cases: non-finite, signed zero,
+    subnormal, rounding ties at the sixth digit, the %f/%e switch points."""
+    v = rng.uniform(-1, 1, m) * 10.0 ** rng.integers(-12, 12, m)
+    special = [np.nan, -np.nan, np.inf, -np.inf, 0.0, -0.0, 5e-324, 2.2250738585072014e-308,
+               1.7976931348623157e308, 999999.5, 9999995.0, 1e-5, 9.999995e-5, 0.0001,
+               123456.5, 1e6, 100000.0, 0.5, 2.5]
+    v[: len(special)] = special
+    return v
+
+
+def test_writers_byte_identical_on_odd_values_and_shapes(tmp_path):
+    """A row longer than the writer's 8 MiB formatting chunk, empty rows,
+    non-finite / subnormal / tie values, both value widths; and empty files."""
+    rng = np.random.default_rng(17)
+    lengths = np.array([0, 3, 400_000, 0, 1, 25, 0], np.int64)
+    rp = np.concatenate([[0], np.cumsum(lengths)]).astype(np.uint32)
+    nnz = int(rp[-1])
+    ri = rng.integers(0, 2**32 - 2, nnz, dtype=np.uint64).astype(np.uint32)
+    rv = _odd_values(rng, nnz)
+    with np.errstate(over="ignore"):  # DBL_MAX becomes inf in float
+        rv32 = rv.astype(np.float32)
+    for real, vals in (("f64", rv), ("f32", rv32)):
+        pr, po = tmp_path / f"ref_{real}.csr", tmp_path / f"ours_{real}.csr"
+        assert oracle.ref_write_csr(pr, rp, ri, vals, 2**32 - 1, real=real) == 1
+        gb.write_csr(po, rp, ri, vals, 2**32 - 1)
+        assert pr.read_bytes() == po.read_bytes(), real
+    g = _odd_values(rng, 300 * 7).reshape(300, 7)
+    with np.errstate(over="ignore"):
+        g32 = g.astype(np.float32)
+    for real, vals in (("f64", g), ("f32", g32)):
+        pr, po = tmp_path / f"ref_{real}.grid", tmp_path / f"ours_{real}.grid"
+        assert oracle.ref_write_grid(pr, vals.reshape(-1), 300, 7, real=real) == 1
+        gb.write_grid(po, vals)
+        assert pr.read_bytes() == po.read_bytes(), real
+    # nothing to write: an empty file, like the reference
+    pe = tmp_path / "empty.csr"
+    gb.write_csr(pe, np.zeros(1, np.uint32), np.zeros(0, np.uint32), np.zeros(0), 0)
+    assert pe.read_bytes() == b""
+    pe = tmp_path / "empty_rows.csr"
+    gb.write_csr(pe, np.zeros(4, np.uint32), np.zeros(0, np.uint32), np.zeros(0), 0)
+    assert pe.read_bytes() == b"\n\n\n"
+
+
+@pytest.mark.skipif(not __import__("os").path.exists("/dev/full"), reason="no /dev/full")
+def test_writer_reports_a_full_device():
+    """Every formatting chunk still takes its turn after a failed write, so the
+    call returns GOOSEBERRY_ERROR_WRITE instead of blocking."""
+    A = W.powerlaw_rows(50_000, 1_000_000, seed=4, cap=5000)
+    with pytest.raises(gb.GooseberryError) as e:
+        gb.write_csr("/dev/full", A.rowptr, A.rowind, A.rowval, A.ncols)
+    assert e.value.code == 5  # GOOSEBERRY_ERROR_WRITE
