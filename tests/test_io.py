@@ -175,3 +175,111 @@ def test_writer_reports_a_full_device():
     with pytest.raises(gb.GooseberryError) as e:
         gb.write_csr("/dev/full", A.rowptr, A.rowind, A.rowval, A.ncols)
     assert e.value.code == 5  # GOOSEBERRY_ERROR_WRITE
+
+
+# Tokens strtoull (indices) and strtod (values) read whole.  On these the
+# reference's CSR reader is well defined: it sizes each row by its token count
+# over two (src/io.c:414) and copies that many entries (:457), which equals
+# the pairs it parsed only when every token reads whole.
+_IDX_TOKENS = ["1", "2", "3", "17", "0", "+3", "-1", "007", "4294967295", "4294967296",
+               "99999999999999999999", "5"]
+_VAL_TOKENS = ["1.5", "-2e-3", ".5", "5.", "1e400", "-1e400", "1e-400", "inf", "-inf", "nan",
+               "NaN", "-INF", "infinity", "nan(123)", "0x1p3", "+.5", "1E5", "0.1",
+               "123456789012345678901234567890", "4.9e-324", "-0", "7"]
+_SEPS = [" ", "  ", "\t", " \t "]
+
+
+def _fuzz_csr_text(rng):
+    lines = []
+    for _ in range(int(rng.integers(0, 30))):
+        kind = rng.random()
+        if kind < 0.1:
+            lines.append(str(rng.choice(list("#%'\"/"))) + " note 1 2")
+        elif kind < 0.15:
+            lines.append(str(rng.choice(["", " ", "\t"])))
+        else:
+            toks = []
+            for _ in range(int(rng.integers(0, 9))):
+                toks.append(str(rng.choice(_IDX_TOKENS if len(toks) % 2 == 0 else _VAL_TOKENS)))
+            sep = [str(rng.choice(_SEPS)) for _ in toks]
+            line = "".join(s + t for s, t in zip(sep, toks))
+            if rng.random() < 0.7:
+                line = line.lstrip(" \t")
+            if rng.random() < 0.2:
+                line += str(rng.choice([" ", "\r", " \r", "\t"]))
+            lines.append(line)
+    text = "\n".join(lines)
+    if rng.random() < 0.5:
+        text += "\n"
+    return text
+
+
+def test_csr_reader_fuzz_matches_reference(tmp_path):
+    """Seeded random CSR text (odd token counts, signs, wrap-around and
+    overflowing indices, 0-based files, inf/nan/hex/subnormal values,
+    comments, blank and whitespace-only lines, CR line ends): the same status,
+    shape and arrays (bytes, so NaN payloads count) as the reference's reader,
+    both widths."""
+    rng = np.random.default_rng(2024)
+    p = tmp_path / "fuzz.csr"
+    for case in range(400):
+        p.write_text(_fuzz_csr_text(rng))
+        for f64, real in ((True, "f64"), (False, "f32")):
+            rc, n, nc, rp, ri, rv = oracle.ref_read_csr(p, real=real)
+            ctx = (case, real, p.read_text())
+            assert rc == 1, ctx
+            grp, gri, grv, gnc = gb.read_csr(p, f64=f64)
+            assert gnc == nc and len(grp) == n + 1, ctx
+            assert grp.tobytes() == rp.tobytes() and gri.tobytes() == ri.tobytes(), ctx
+            assert grv.tobytes() == rv.tobytes(), ctx
+
+
+def test_csr_reader_keeps_the_pairs_that_parse(tmp_path):
+    """Tokens that do not read whole.  The reference overruns its arrays on
+    these (rows sized by token count, src/io.c:414,457); here a row holds the
+    pairs strtoull/strtod read, in the reference's loop order (src/io.c:423-437):
+    the row ends at the first value that does not parse."""
+    cases = {
+        "1 2.5 12abc 3.0 4 5\n": ([0, 1], [0], [2.5]),          # value "abc" fails
+        "0x1f 2.0\n": ([0, 0], [], []),                         # index 0, value "x1f" fails
+        "3-1 4 5\n": ([0, 2], [2, 3], [-1.0, 5.0]),             # one token, one pair
+        "2 1e 3 4\n": ([0, 1], [1], [1.0]),                     # "e" ends the row
+        "1 1\n2 abc\n3 3\n": ([0, 1, 1, 2], [0, 2], [1.0, 3.0]),
+    }
+    p = tmp_path / "bad.csr"
+    for text, (rp, ri, rv) in cases.items():
+        p.write_text(text)
+        grp, gri, grv, _ = gb.read_csr(p)
+        assert grp.tolist() == rp and gri.tolist() == ri and grv.tolist() == rv, text
+
+
+def test_grid_reader_fuzz_matches_reference(tmp_path):
+    """Seeded random grids, some ragged, with any of the tokens above or
+    tokens that read in part ("2.5e+3x", "1e", "abc"): the same status and
+    values as the reference's reader (whose two passes parse alike)."""
+    partial = ["2.5e+3x", "1e", "abc", "-.e1", "3-1", "1,5", "12abc", "0x1f"]
+    rng = np.random.default_rng(7)
+    p = tmp_path / "fuzz.grid"
+    for case in range(300):
+        ncols = int(rng.integers(1, 5))
+        lines = [" ".join(str(rng.choice(_VAL_TOKENS)) for _ in range(ncols))]
+        for _ in range(int(rng.integers(0, 7))):
+            if rng.random() < 0.1:
+                lines.append("# c")
+                continue
+            k = ncols if rng.random() < 0.85 else int(rng.integers(0, ncols + 2))
+            toks = [str(rng.choice(_VAL_TOKENS if rng.random() < 0.9 else partial))
+                    for _ in range(k)]
+            lines.append(str(rng.choice(_SEPS)).join(toks))
+        p.write_text("\n".join(lines) + ("\n" if rng.random() < 0.5 else ""))
+        for f64, real in ((True, "f64"), (False, "f32")):
+            rc, n, nc, vals = oracle.ref_read_grid(p, real=real)
+            ctx = (case, real, p.read_text())
+            if rc != 1:
+                with pytest.raises(gb.GooseberryError) as e:
+                    gb.read_grid(p, f64=f64)
+                assert e.value.code == rc, ctx
+                continue
+            g = gb.read_grid(p, f64=f64)
+            assert g.shape == (n, nc), ctx
+            assert g.reshape(-1).tobytes() == vals[: n * nc].tobytes(), ctx
