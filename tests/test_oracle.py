@@ -146,3 +146,36 @@ def test_pagerank_restatement_matches_reference_loop():
     a = oracle.pagerank(rp, ri, rv, 0.9, 0.0, 13)
     b = oracle.ref_pagerank(rp, ri, rv, 0.9, 0.0, 13)
     assert a[1] == b[1] == 13 and a[2] == b[2] and np.array_equal(a[0], b[0])
+
+
+@pytest.mark.skipif(not oracle.ref_available("f64"), reason="reference build absent")
+def test_spmm_blocks_fuzz_matches_reference_build():
+    """Random matrices with empty rows, 1-4 right-hand columns and random
+    block lists (increasing, decreasing = empty, overlapping, not covering
+    every row): the restatement and the reference's blas_spmult write the same
+    rows with the same bits and leave the others alone (src/blas.c:576-595),
+    both value widths."""
+    rng = np.random.default_rng(31)
+    for case in range(60):
+        n = int(rng.integers(1, 300))
+        ncols = int(rng.integers(1, 300))
+        lengths = rng.integers(0, 12, n) * (rng.random(n) < 0.8)
+        rp = np.concatenate([[0], np.cumsum(lengths)]).astype(np.uint32)
+        nnz = int(rp[-1])
+        ri = rng.integers(0, ncols, nnz).astype(np.uint32)
+        rv = rng.uniform(-1, 1, nnz)
+        k = int(rng.integers(1, 5))
+        B = rng.uniform(-1, 1, ncols * k)
+        blocks = None
+        if rng.random() < 0.75:
+            blocks = rng.integers(0, n + 1, int(rng.integers(1, 7)))
+            if rng.random() < 0.5:
+                blocks = np.sort(blocks)
+        for real in ("f64", "f32"):
+            dt = np.float64 if real == "f64" else np.float32
+            init = np.full(n * k, 7.0, dt)
+            a = oracle.spmm(rp, ri, rv.astype(dt), B.astype(dt), ncols=ncols, bncols=k,
+                            blocks=blocks, out=init.copy(), real=real)
+            b = oracle.ref_spmm(rp, ri, rv.astype(dt), B.astype(dt), ncols=ncols, bncols=k,
+                                blocks=blocks, out=init.copy(), real=real)
+            assert a.tobytes() == b.tobytes(), (case, real, blocks)
