@@ -179,3 +179,38 @@ def test_spmm_blocks_fuzz_matches_reference_build():
             b = oracle.ref_spmm(rp, ri, rv.astype(dt), B.astype(dt), ncols=ncols, bncols=k,
                                 blocks=blocks, out=init.copy(), real=real)
             assert a.tobytes() == b.tobytes(), (case, real, blocks)
+
+
+@pytest.mark.skipif(not oracle.ref_available("f64"), reason="reference build absent")
+def test_cgd_fuzz_matches_reference_build():
+    """Random symmetric diagonally dominant systems (random sparsity, sizes
+    1-400, tolerances from loose to unreachable, iteration limits that stop
+    early): the restatement's iterations, last norm and x equal the reference
+    cgd's bit for bit, both value widths (one OpenMP thread, so the
+    reference's dot products add in index order)."""
+    rng = np.random.default_rng(5)
+    oracle.ref_set_threads(1)
+    for case in range(40):
+        n = int(rng.integers(1, 400))
+        m = int(rng.integers(0, 4 * n + 1))
+        r = rng.integers(0, n, m)
+        c = rng.integers(0, n, m)
+        w = rng.uniform(-1, 1, m)
+        A = np.zeros((n, n))
+        np.add.at(A, (r, c), w)
+        A = A + A.T
+        A[np.arange(n), np.arange(n)] = np.abs(A).sum(axis=1) + rng.uniform(0.1, 2, n)
+        rows, cols = np.nonzero(A)
+        rp = np.concatenate([[0], np.cumsum(np.bincount(rows, minlength=n))]).astype(np.uint32)
+        ri, rv = cols.astype(np.uint32), A[rows, cols]
+        b = rng.uniform(-1, 1, n)
+        err = float(10.0 ** rng.uniform(-14, -1)) * float(np.linalg.norm(b))
+        niter = int(rng.choice([3, 10, 1000]))
+        for real in ("f64", "f32"):
+            dt = np.float64 if real == "f64" else np.float32
+            xo, ito, _ = oracle.cgd(rp, ri, rv.astype(dt), b.astype(dt), err, niter, real=real)
+            xr, itr, _ = oracle.ref_cgd(rp, ri, rv.astype(dt), b.astype(dt), err, niter,
+                                         real=real)
+            ctx = (case, real, n, niter, err)
+            assert ito == itr, ctx
+            assert xo.tobytes() == xr.tobytes(), ctx
