@@ -244,13 +244,135 @@ T * malloc_n(size_t n) {
   return static_cast<T *>(std::malloc(sizeof(T) * (n ? n : 1)));
 }
 
-// Parses a CSR file into caller-owned arrays made by `alloc`.
+// Whitespace-separated tokens of a line: the reference sizes a CSR row as
+// this over two (src/io.c:414).
+uint32_t count_tokens(const char * s) {
+  uint32_t n = 0;
+  bool in = false;
+  for (; *s; ++s) {
+    const bool sp = is_space(*s);
+    n += (!sp && !in) ? 1u : 0u;
+    in = !sp;
+  }
+  return n;
+}
+
+constexpr uint32_t kCommentLine = 0xffffffffu;
+
+// The common case, in two passes over the lines: every line's token count
+// over two sizes its row (one pass, by all threads), then every row is parsed
+// straight into the caller's arrays at its offset.  Exact only when each row
+// parses into exactly that many pairs, which holds whenever every token reads
+// whole as a number; returns false (arrays released) when a row does not, and
+// the caller falls back to read_csr_rows.  Columns are stored 1-based minus
+// one and shifted back when a 0 column makes the file 0-based (mincol,
+// src/io.c:464).
+template <typename T, class Alloc, class Release>
+bool read_csr_sized(const Lines & L, dim_t * nrows, dim_t * ncols, ind_t ** r_rowptr,
+    dim_t ** r_rowind, T ** r_rowval, Alloc && alloc, Release && release, int * rc) {
+  const size_t nl = L.start.size();
+  const unsigned nt = static_cast<unsigned>(std::min<size_t>(n_threads(),
+      std::max<size_t>(nl / 1024, 1)));
+  std::vector<uint32_t> pairs(nl);
+  std::vector<size_t> rows(nt + 1, 0), ents(nt + 1, 0);
+  parallel_for(nt, [&](unsigned t) {
+    size_t r = 0, e = 0;
+    for (size_t l = nl * t / nt; l < nl * (t + 1) / nt; ++l) {
+      const char * line = L.buf.get() + L.start[l];
+      if (line[0] != '\0' && is_comment(line[0])) {
+        pairs[l] = kCommentLine;
+        continue;
+      }
+      pairs[l] = count_tokens(line) / 2;
+      ++r;
+      e += pairs[l];
+    }
+    rows[t + 1] = r;
+    ents[t + 1] = e;
+  });
+  for (unsigned t = 0; t < nt; ++t) {
+    rows[t + 1] += rows[t];
+    ents[t + 1] += ents[t];
+  }
+  const size_t n = rows[nt], nnz = ents[nt];
+  if (n >= 0xffffffffu || nnz > 0xffffffffu) return false;  // the general path reports it
+  ind_t * rowptr = nullptr;
+  dim_t * rowind = nullptr;
+  T * rowval = nullptr;
+  if (!alloc(&rowptr, n + 1) || !alloc(&rowind, nnz) || !alloc(&rowval, nnz)) {
+    set_error("out of host memory reading CSR rows");
+    *rc = GOOSEBERRY_ERROR_UNKNOWN;
+    return true;
+  }
+  std::vector<uint32_t> lo(nt, 1), hi(nt, 0);
+  std::vector<char> bad(nt, 0);
+  rowptr[0] = 0;
+  parallel_for(nt, [&](unsigned t) {
+    size_t r = rows[t], j = ents[t];
+    uint32_t mn = 1, mx = 0;
+    bool b = false;
+    for (size_t l = nl * t / nt; l < nl * (t + 1) / nt && !b; ++l) {
+      const uint32_t want = pairs[l];
+      if (want == kCommentLine) continue;
+      // the loop of src/io.c:423-437, stopped at the row's size
+      const char * sptr = L.buf.get() + L.start[l];
+      char * eptr = nullptr;
+      uint32_t k = 0;
+      uint32_t i = static_cast<uint32_t>(parse_ull(sptr, &eptr));
+      sptr = eptr;
+      double f = parse_double(sptr, &eptr);
+      while (eptr != sptr) {
+        if (k == want) break;
+        mx = std::max(mx, i);
+        mn = std::min(mn, i);
+        rowind[j + k] = i - 1u;
+        rowval[j + k] = static_cast<T>(f);
+        ++k;
+        sptr = eptr;
+        i = static_cast<uint32_t>(parse_ull(sptr, &eptr));
+        sptr = eptr;
+        f = parse_double(sptr, &eptr);
+      }
+      b = k != want || eptr != sptr;
+      j += want;
+      rowptr[++r] = static_cast<ind_t>(j);
+    }
+    lo[t] = mn;
+    hi[t] = mx;
+    bad[t] = b;
+  });
+  uint32_t mincol = 1, maxcol = 0;
+  bool exact = true;
+  for (unsigned t = 0; t < nt; ++t) {
+    mincol = std::min(mincol, lo[t]);
+    maxcol = std::max(maxcol, hi[t]);
+    exact = exact && !bad[t];
+  }
+  if (!exact) {
+    release(rowptr);
+    release(rowind);
+    release(rowval);
+    return false;
+  }
+  if (mincol == 0) {  // a 0-based file: undo the 1-based shift
+    parallel_for(nt, [&](unsigned t) {
+      for (size_t e = nnz * t / nt; e < nnz * (t + 1) / nt; ++e) rowind[e] += 1u;
+    });
+  }
+  *r_rowptr = rowptr;
+  *r_rowind = rowind;
+  *r_rowval = rowval;
+  *nrows = static_cast<dim_t>(n);
+  *ncols = maxcol - mincol + 1;
+  *rc = GOOSEBERRY_SUCCESS;
+  return true;
+}
+
+// The general case: rows parsed by all threads into per-thread lists, then
+// gathered into caller-owned arrays made by `alloc`.
 template <typename T, class Alloc>
-int read_csr(const char * path, dim_t * nrows, dim_t * ncols, ind_t ** r_rowptr,
-    dim_t ** r_rowind, T ** r_rowval, Alloc && alloc) {
-  GB_CHECK_INPUT(nrows && ncols && r_rowptr && r_rowind && r_rowval, "NULL output");
-  Lines L;
-  GB_TRY(read_lines(path, L));
+int read_csr_rows(const char * path, const Lines & L, dim_t * nrows, dim_t * ncols,
+    ind_t ** r_rowptr, dim_t ** r_rowind, T ** r_rowval, Alloc && alloc) {
   const size_t nl = L.start.size();
   const unsigned nt = static_cast<unsigned>(std::min<size_t>(n_threads(),
       std::max<size_t>(nl / 1024, 1)));
@@ -305,6 +427,20 @@ int read_csr(const char * path, dim_t * nrows, dim_t * ncols, ind_t ** r_rowptr,
   *nrows = static_cast<dim_t>(n);
   *ncols = maxcol - mincol + 1;
   return GOOSEBERRY_SUCCESS;
+}
+
+// Parses a CSR file into caller-owned arrays made by `alloc` (and given back
+// through `release` when the sized pass cannot be used).
+template <typename T, class Alloc, class Release>
+int read_csr(const char * path, dim_t * nrows, dim_t * ncols, ind_t ** r_rowptr,
+    dim_t ** r_rowind, T ** r_rowval, Alloc && alloc, Release && release) {
+  GB_CHECK_INPUT(nrows && ncols && r_rowptr && r_rowind && r_rowval, "NULL output");
+  Lines L;
+  GB_TRY(read_lines(path, L));
+  int rc = GOOSEBERRY_SUCCESS;
+  if (read_csr_sized<T>(L, nrows, ncols, r_rowptr, r_rowind, r_rowval, alloc, release, &rc))
+    return rc;
+  return read_csr_rows<T>(path, L, nrows, ncols, r_rowptr, r_rowind, r_rowval, alloc);
 }
 
 template <typename T>
@@ -528,10 +664,12 @@ template <typename T>
 int read_sparse(int type, const char * file, dim_t * nrows, dim_t * ncols, ind_t ** rowptr,
     dim_t ** rowind, T ** rowval) {
   if (type != GOOSEBERRY_FORMAT_CSR) return other_format(type, true);
-  return read_csr<T>(file, nrows, ncols, rowptr, rowind, rowval, [](auto ** p, size_t n) {
-    *p = malloc_n<std::remove_pointer_t<std::remove_pointer_t<decltype(p)>>>(n);
-    return *p != nullptr;
-  });
+  return read_csr<T>(file, nrows, ncols, rowptr, rowind, rowval,
+      [](auto ** p, size_t n) {
+        *p = malloc_n<std::remove_pointer_t<std::remove_pointer_t<decltype(p)>>>(n);
+        return *p != nullptr;
+      },
+      [](void * p) { std::free(p); });
 }
 
 }  // namespace
@@ -609,7 +747,12 @@ int gb_csr_read(const char * file, unsigned flags, gb_stream_t stream, gb_csr_t 
   ind_t * rowptr = nullptr;
   dim_t * rowind = nullptr;
   double * rowval = nullptr;
-  int rc = gb::read_csr<double>(file, &nrows, &ncols, &rowptr, &rowind, &rowval, alloc);
+  auto release = [&](void * q) {
+    held.erase(std::find(held.begin(), held.end(), q));
+    std::free(q);
+  };
+  int rc = gb::read_csr<double>(file, &nrows, &ncols, &rowptr, &rowind, &rowval, alloc,
+      release);
   if (rc == GOOSEBERRY_SUCCESS)
     rc = gb_csr_create(nrows, ncols, rowptr[nrows], rowptr, rowind, rowval, nullptr,
         (want64 ? GB_CSR_VALUES_F64 : 0u) | (want32 ? GB_CSR_VALUES_F32 : 0u), stream, out);
