@@ -300,6 +300,8 @@ bool read_csr_sized(const Lines & L, dim_t * nrows, dim_t * ncols, ind_t ** r_ro
   dim_t * rowind = nullptr;
   T * rowval = nullptr;
   if (!alloc(&rowptr, n + 1) || !alloc(&rowind, nnz) || !alloc(&rowval, nnz)) {
+    if (rowptr) release(rowptr);
+    if (rowind) release(rowind);
     set_error("out of host memory reading CSR rows");
     *rc = GOOSEBERRY_ERROR_UNKNOWN;
     return true;
@@ -370,9 +372,9 @@ bool read_csr_sized(const Lines & L, dim_t * nrows, dim_t * ncols, ind_t ** r_ro
 
 // The general case: rows parsed by all threads into per-thread lists, then
 // gathered into caller-owned arrays made by `alloc`.
-template <typename T, class Alloc>
+template <typename T, class Alloc, class Release>
 int read_csr_rows(const char * path, const Lines & L, dim_t * nrows, dim_t * ncols,
-    ind_t ** r_rowptr, dim_t ** r_rowind, T ** r_rowval, Alloc && alloc) {
+    ind_t ** r_rowptr, dim_t ** r_rowind, T ** r_rowval, Alloc && alloc, Release && release) {
   const size_t nl = L.start.size();
   const unsigned nt = static_cast<unsigned>(std::min<size_t>(n_threads(),
       std::max<size_t>(nl / 1024, 1)));
@@ -400,6 +402,8 @@ int read_csr_rows(const char * path, const Lines & L, dim_t * nrows, dim_t * nco
   dim_t * rowind = nullptr;
   T * rowval = nullptr;
   if (!alloc(&rowptr, n + 1) || !alloc(&rowind, nnz) || !alloc(&rowval, nnz)) {
+    if (rowptr) release(rowptr);
+    if (rowind) release(rowind);
     set_error("out of host memory reading '%s'", path);
     return GOOSEBERRY_ERROR_UNKNOWN;
   }
@@ -440,7 +444,8 @@ int read_csr(const char * path, dim_t * nrows, dim_t * ncols, ind_t ** r_rowptr,
   int rc = GOOSEBERRY_SUCCESS;
   if (read_csr_sized<T>(L, nrows, ncols, r_rowptr, r_rowind, r_rowval, alloc, release, &rc))
     return rc;
-  return read_csr_rows<T>(path, L, nrows, ncols, r_rowptr, r_rowind, r_rowval, alloc);
+  return read_csr_rows<T>(path, L, nrows, ncols, r_rowptr, r_rowind, r_rowval, alloc,
+      release);
 }
 
 template <typename T>
