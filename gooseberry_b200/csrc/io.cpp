@@ -148,18 +148,27 @@ int read_lines(const char * path, Lines & L) {
       p = q + 1;
     }
   });
-  size_t total = 0;
-  for (auto & v : nl) total += v.size();
+  // line starts, filled by every thread for its own newlines: thread t's
+  // first line starts after the last newline any earlier thread found
+  std::vector<size_t> first(nt + 1, 0), from(nt, 0);
+  size_t prev = 0;
+  for (unsigned t = 0; t < nt; ++t) {
+    first[t + 1] = first[t] + nl[t].size();
+    from[t] = prev;
+    if (!nl[t].empty()) prev = nl[t].back() + 1;
+  }
+  const size_t total = first[nt];
   const bool tail = n > 0 && buf[n - 1] != '\n';  // last line without a newline
   L.start.resize(total + (tail ? 1 : 0));
-  size_t k = 0, prev = 0;
-  for (auto & v : nl)
-    for (size_t pos : v) {
-      L.start[k++] = prev;
+  parallel_for(nt, [&](unsigned t) {
+    size_t k = first[t], p = from[t];
+    for (size_t pos : nl[t]) {
+      L.start[k++] = p;
       buf[pos] = '\0';
-      prev = pos + 1;
+      p = pos + 1;
     }
-  if (tail) L.start[k] = prev;
+  });
+  if (tail) L.start[total] = prev;
   return GOOSEBERRY_SUCCESS;
 }
 
