@@ -120,3 +120,64 @@ def test_reordering_entry_points_reject_bad_input_before_any_device_work():
     # no permutation: nothing to do, arrays come back unchanged
     rp, ri, rv = gb.permute_sparse(rowptr, rowind, vals, 3)
     assert np.array_equal(rp, rowptr) and np.array_equal(ri, rowind)
+
+
+def _plan_model(rp, T):
+    """The planner's greedy rule, restated: tiles of whole rows while rows +
+    nonzeros fit in T; a row with more than T - 1 nonzeros becomes a long row
+    cut into chunks of 4T nonzeros.  Tiles are {first row | long-row id, row
+    count (0 for a chunk), first nonzero, nonzero count}."""
+    rp = rp.astype(np.int64)
+    n, chunk = len(rp) - 1, 4 * T
+    tiles, nlong, r = [], 0, 0
+    while r < n:
+        b, L = rp[r], rp[r + 1] - rp[r]
+        if L + 1 > T:
+            for q in range((L + chunk - 1) // chunk):
+                tiles.append((nlong, 0, b + q * chunk, min(chunk, L - q * chunk)))
+            nlong += 1
+            r += 1
+            continue
+        r0, items = r, 0
+        while r < n:
+            l = rp[r + 1] - rp[r]
+            if l + 1 > T or items + l + 1 > T:
+                break
+            items += l + 1
+            r += 1
+        tiles.append((r0, r - r0, b, rp[r] - b))
+    return np.array(tiles, np.int64).reshape(-1, 4), nlong
+
+
+def _quantile_model(lengths, q):
+    """Row-length quantile as the planner reports it: exact below 1024, the
+    top of the row's power-of-two bucket above."""
+    want = int(np.ceil(q * len(lengths)))
+    if want == 0:
+        return 0
+    v = int(np.sort(lengths)[want - 1])
+    return v if v < 1024 else (1 << int(v).bit_length()) - 1
+
+
+def test_planner_fuzz_matches_greedy_rule():
+    """Random row-length mixes (empty rows, short rows, rows just under and
+    over a tile, rows of several chunks, lengths past 1024) and tile sizes:
+    the planner's tiles, long-row count and row-length summary equal the
+    restated rule exactly."""
+    rng = np.random.default_rng(12)
+    for case in range(80):
+        T = int(rng.choice([64, 100, 256, 1000, 2048, 4096]))
+        n = int(rng.integers(0, 3000))
+        kind = rng.random(n)
+        L = np.where(kind < 0.2, 0,
+            np.where(kind < 0.8, rng.integers(1, 40, n),
+            np.where(kind < 0.9, rng.integers(T - 3, T + 3, n),
+                     rng.integers(1, 9 * T, n)))).astype(np.int64)
+        rp = np.concatenate([[0], np.cumsum(L)]).astype(np.uint32)
+        tiles, nlong, info = gb.plan_tiles(rp, T)
+        mt, mlong = _plan_model(rp, T)
+        assert nlong == mlong and np.array_equal(tiles.astype(np.int64), mt), (case, T, n)
+        if n:
+            assert info.max_row == L.max(), case
+            for q, got in ((0.5, info.row_p50), (0.9, info.row_p90), (0.99, info.row_p99)):
+                assert got == _quantile_model(L, q), (case, q)
