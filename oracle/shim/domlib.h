@@ -3,9 +3,10 @@
  * gooseberry (reference .gitmodules:1-3, src/base.h:19).
  *
  * TEST INFRASTRUCTURE ONLY.  It exists so the reference's own hot-path sources
- * (src/blas.c, src/cgd.c, src/matrix.c, and src/io.c with dlfile_shim.h) can
- * be compiled unmodified into the CPU oracle under oracle/_ref.  It supplies only the helpers those three files
- * call: typed alloc/calloc/set/copy/init_alloc, exclusive prefix sums, even
+ * (src/blas.c, src/cgd.c, src/matrix.c, src/io.c with dlfile_shim.h, and
+ * src/permute.c with dlpq_headers.h) can be compiled unmodified into the CPU
+ * oracle under oracle/_ref.  It supplies only the helpers those files call:
+ * typed alloc/calloc/set/copy/init_alloc, exclusive prefix sums, even
  * chunking of an index range over threads, free/swap/min and the
  * eprintf/wprintf message macros.  Written for this project from the call
  * sites; it is not domlib's code.
