@@ -11,6 +11,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -26,6 +27,91 @@ constexpr uint32_t kDefaultTileItems = 2048;
 constexpr uint32_t kChunkTiles = 4;  // a long-row chunk is 4 tiles of nonzeros
 }  // namespace
 
+namespace {
+
+// The tiles that start at row r under the greedy rule, appended to `tiles`,
+// and the row after them.  A row with more than tile_items - 1 nonzeros is a
+// long row: chunk tiles of chunk_nnz nonzeros carrying `lid`, its long-row
+// id (*nchunks > 0).  Otherwise one tile of whole rows while rows + nonzeros
+// fit in tile_items (*nchunks = 0).  rowptr must be non-decreasing.
+uint32_t tile_from(uint32_t r, uint32_t nrows, const uint32_t * rowptr, uint32_t tile_items,
+    uint32_t chunk_nnz, uint32_t lid, std::vector<TileDesc> & tiles, uint32_t * nchunks) {
+  const uint32_t b = rowptr[r], len = rowptr[r + 1] - b;
+  if (static_cast<uint64_t>(len) + 1 > tile_items) {
+    const uint32_t nch = (len + chunk_nnz - 1) / chunk_nnz;
+    for (uint32_t q = 0; q < nch; ++q)
+      tiles.push_back({lid, 0, b + q * chunk_nnz, std::min(chunk_nnz, len - q * chunk_nnz)});
+    *nchunks = nch;
+    return r + 1;
+  }
+  uint32_t items = 0, e = r;
+  while (e < nrows) {
+    const uint32_t l = rowptr[e + 1] - rowptr[e];
+    if (static_cast<uint64_t>(l) + 1 > tile_items || items + l + 1 > tile_items) break;
+    items += l + 1;
+    ++e;
+  }
+  tiles.push_back({r, e - r, b, rowptr[e] - b});
+  *nchunks = 0;
+  return e;
+}
+
+// Greedy tiles of one segment of rows, planned from its first row as if a
+// tile started there; the last step may run past the segment's end.
+struct PlanSegment {
+  uint32_t begin = 0, end = 0, stop = 0;  // rows [begin, end); steps end at row `stop`
+  std::vector<TileDesc> tiles;            // chunk tiles carry segment-local long-row ids
+  std::vector<uint32_t> step_row;         // first row of each step (a row tile or a long row)
+  std::vector<uint32_t> step_tile;        // its first tile in `tiles`
+  std::vector<uint32_t> step_long;        // long rows of the segment before the step
+  std::vector<uint32_t> long_step;        // step of each long row
+};
+
+void plan_segment(PlanSegment & g, const uint32_t * rowptr, uint32_t nrows,
+    uint32_t tile_items, uint32_t chunk_nnz) {
+  uint32_t r = g.begin, nlong = 0;
+  while (r < g.end) {
+    g.step_row.push_back(r);
+    g.step_tile.push_back(static_cast<uint32_t>(g.tiles.size()));
+    g.step_long.push_back(nlong);
+    uint32_t nch = 0;
+    r = tile_from(r, nrows, rowptr, tile_items, chunk_nnz, nlong, g.tiles, &nch);
+    if (nch) {
+      g.long_step.push_back(static_cast<uint32_t>(g.step_row.size() - 1));
+      ++nlong;
+    }
+  }
+  g.stop = r;
+}
+
+// One tile step of the true plan, at row r; returns the next row.
+uint32_t plan_step(Plan & plan, uint32_t r, const uint32_t * rowptr, uint32_t nrows) {
+  const uint32_t first = static_cast<uint32_t>(plan.tiles.size());
+  uint32_t nch = 0;
+  const uint32_t lid = static_cast<uint32_t>(plan.longrows.size());
+  const uint32_t next = tile_from(r, nrows, rowptr, plan.tile_items, plan.chunk_nnz, lid,
+      plan.tiles, &nch);
+  if (nch) plan.longrows.push_back({r, first, nch, 0});
+  return next;
+}
+
+template <class F>
+void run_threads(unsigned nt, F && body) {
+  std::vector<std::thread> th;
+  for (unsigned t = 1; t < nt; ++t) th.emplace_back(body, t);
+  body(0u);
+  for (auto & x : th) x.join();
+}
+
+}  // namespace
+
+// Tiles in the greedy order from row 0, computed by all host threads for
+// large matrices: each thread plans its segment of rows from the segment's
+// first row; a sequential pass then follows the true chain of tiles, takes
+// over a segment's tiles from the first tile start the chain lands on (from a
+// given row the greedy tiles are always the same, and every long row starts
+// afresh), and plans tile by tile wherever it does not land on one.  The
+// result is the plan the sequential rule gives.
 int build_plan(uint32_t nrows, const uint32_t * rowptr, uint32_t nnz,
     uint32_t tile_items, Plan & plan) {
   if (tile_items < 64 || tile_items > 16384)
@@ -37,55 +123,88 @@ int build_plan(uint32_t nrows, const uint32_t * rowptr, uint32_t nnz,
   plan.tiles.clear();
   plan.longrows.clear();
 
-  // exact counts of lengths < 1024, log2 buckets above, for quantiles
-  std::vector<uint64_t> small(1024, 0), big(33, 0);
-  uint32_t maxlen = 0;
-  uint32_t r = 0;
-  while (r < nrows) {
-    const uint32_t b = rowptr[r], e = rowptr[r + 1];
-    GB_CHECK_INPUT(e >= b, "rowptr decreases at row %u (%u > %u)", r, b, e);
-    const uint32_t len = e - b;
-    if (static_cast<uint64_t>(len) + 1 > tile_items) {
-      // long row -> chunk tiles
-      LongRowDesc L;
-      L.row = r;
-      L.first_tile = static_cast<uint32_t>(plan.tiles.size());
-      L.nchunks = (len + plan.chunk_nnz - 1) / plan.chunk_nnz;
-      L.pad = 0;
-      const uint32_t lid = static_cast<uint32_t>(plan.longrows.size());
-      for (uint32_t q = 0; q < L.nchunks; ++q) {
-        TileDesc t;
-        t.row_begin = lid;
-        t.row_count = 0;
-        t.nnz_begin = b + q * plan.chunk_nnz;
-        t.nnz_count = std::min(plan.chunk_nnz, len - q * plan.chunk_nnz);
-        plan.tiles.push_back(t);
+  constexpr uint32_t kSegmentRows = 32768;  // > the most rows one tile can hold
+  const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  const unsigned nt = static_cast<unsigned>(std::max<uint64_t>(1,
+      std::min<uint64_t>(hw, nrows / kSegmentRows)));
+
+  // row-length histogram (exact counts below 1024, log2 buckets above), the
+  // longest row and the first row where rowptr decreases
+  struct Hist {
+    std::vector<uint64_t> small = std::vector<uint64_t>(1024, 0), big = std::vector<uint64_t>(33, 0);
+    uint32_t maxlen = 0, bad = 0xffffffffu;
+  };
+  std::vector<Hist> hist(nt);
+  run_threads(nt, [&](unsigned t) {
+    Hist h;  // thread-local until the end: the per-thread slots share cache lines
+    const uint32_t a = static_cast<uint32_t>(uint64_t(nrows) * t / nt);
+    const uint32_t z = static_cast<uint32_t>(uint64_t(nrows) * (t + 1) / nt);
+    uint32_t mx = 0;
+    for (uint32_t r = a; r < z; ++r) {
+      const uint32_t b = rowptr[r], e = rowptr[r + 1];
+      if (e < b) {
+        h.bad = r;
+        break;
       }
-      plan.longrows.push_back(L);
-      maxlen = std::max(maxlen, len);
-      if (len < 1024) ++small[len]; else ++big[32 - __builtin_clz(len)];
-      ++r;
-      continue;
+      const uint32_t len = e - b;
+      mx = std::max(mx, len);
+      if (len < 1024) ++h.small[len]; else ++h.big[32 - __builtin_clz(len)];
     }
-    TileDesc t;
-    t.row_begin = r;
-    t.nnz_begin = b;
-    uint32_t items = 0;
-    while (r < nrows) {
-      const uint32_t bb = rowptr[r], ee = rowptr[r + 1];
-      GB_CHECK_INPUT(ee >= bb, "rowptr decreases at row %u (%u > %u)", r, bb, ee);
-      const uint32_t l = ee - bb;
-      if (static_cast<uint64_t>(l) + 1 > tile_items) break;
-      if (items + l + 1 > tile_items) break;
-      items += l + 1;
-      maxlen = std::max(maxlen, l);
-      if (l < 1024) ++small[l]; else ++big[32 - __builtin_clz(l)];
-      ++r;
-    }
-    t.row_count = r - t.row_begin;
-    t.nnz_count = rowptr[r] - b;
-    plan.tiles.push_back(t);
+    h.maxlen = mx;
+    hist[t] = std::move(h);
+  });
+  std::vector<uint64_t> small(1024, 0), big(33, 0);
+  uint32_t maxlen = 0, bad = 0xffffffffu;
+  for (const Hist & h : hist) {
+    for (int l = 0; l < 1024; ++l) small[l] += h.small[l];
+    for (int k = 0; k < 33; ++k) big[k] += h.big[k];
+    maxlen = std::max(maxlen, h.maxlen);
+    bad = std::min(bad, h.bad);
   }
+  GB_CHECK_INPUT(bad == 0xffffffffu, "rowptr decreases at row %u (%u > %u)", bad,
+      bad == 0xffffffffu ? 0u : rowptr[bad], bad == 0xffffffffu ? 0u : rowptr[bad + 1]);
+
+  if (nt == 1) {
+    for (uint32_t r = 0; r < nrows;) r = plan_step(plan, r, rowptr, nrows);
+  } else {
+    std::vector<PlanSegment> seg(nt);
+    run_threads(nt, [&](unsigned t) {
+      PlanSegment g;  // thread-local until the end, as above
+      g.begin = static_cast<uint32_t>(uint64_t(nrows) * t / nt);
+      g.end = static_cast<uint32_t>(uint64_t(nrows) * (t + 1) / nt);
+      plan_segment(g, rowptr, nrows, tile_items, plan.chunk_nnz);
+      seg[t] = std::move(g);
+    });
+    uint32_t r = 0;
+    for (unsigned t = 0; t < nt; ++t) {
+      const PlanSegment & g = seg[t];
+      size_t j = 0;  // first step of g at or after row r
+      for (;;) {
+        while (j < g.step_row.size() && g.step_row[j] < r) ++j;
+        if (r >= g.end || (j < g.step_row.size() && g.step_row[j] == r)) break;
+        r = plan_step(plan, r, rowptr, nrows);
+      }
+      if (r >= g.end) continue;
+      // the chain is at step j of this segment: take its tiles from there
+      const uint32_t tile0 = static_cast<uint32_t>(plan.tiles.size());
+      const uint32_t long0 = static_cast<uint32_t>(plan.longrows.size());
+      const uint32_t from_tile = g.step_tile[j], from_long = g.step_long[j];
+      for (size_t i = from_tile; i < g.tiles.size(); ++i) {
+        TileDesc d = g.tiles[i];
+        if (d.row_count == 0) d.row_begin = d.row_begin - from_long + long0;
+        plan.tiles.push_back(d);
+      }
+      for (size_t L = from_long; L < g.long_step.size(); ++L) {
+        const uint32_t k = g.long_step[L];
+        const uint32_t first = g.step_tile[k];
+        const uint32_t last = k + 1 < g.step_tile.size() ? g.step_tile[k + 1]
+                                                          : static_cast<uint32_t>(g.tiles.size());
+        plan.longrows.push_back({g.step_row[k], tile0 + (first - from_tile), last - first, 0});
+      }
+      r = g.stop;
+    }
+  }
+
   // quantiles (exact below 1024, bucket upper bound above)
   auto quant = [&](double q) -> uint32_t {
     const uint64_t want = static_cast<uint64_t>(std::ceil(q * nrows));

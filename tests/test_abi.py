@@ -181,3 +181,29 @@ def test_planner_fuzz_matches_greedy_rule():
             assert info.max_row == L.max(), case
             for q, got in ((0.5, info.row_p50), (0.9, info.row_p90), (0.99, info.row_p99)):
                 assert got == _quantile_model(L, q), (case, q)
+
+
+def test_planner_parallel_path_matches_greedy_rule():
+    """Matrices large enough for the planner to split the rows over host
+    threads (each plans its segment from the segment's start, then one pass
+    follows the true chain of tiles): the plan equals the sequential rule when
+    the segments' chains never meet the true one (uniform rows), meet it at
+    long rows, or meet it anywhere."""
+    rng = np.random.default_rng(44)
+    n = 140_000
+    mixes = {
+        "uniform": np.full(n, 9),
+        "long_rows": np.where(rng.random(n) < 0.002, 5000, rng.integers(1, 30, n)),
+        "mixed": np.where(rng.random(n) < 0.2, 0, rng.integers(1, 60, n)),
+    }
+    for name, L in mixes.items():
+        rp = np.concatenate([[0], np.cumsum(L)]).astype(np.uint32)
+        for T in (256, 2048):
+            tiles, nlong, info = gb.plan_tiles(rp, T)
+            mt, mlong = _plan_model(rp, T)
+            assert nlong == mlong and np.array_equal(tiles.astype(np.int64), mt), (name, T)
+            assert info.max_row == L.max() and info.row_p50 == _quantile_model(L, 0.5), name
+    A = W.laplacian_2d(300)  # 90k rows
+    tiles, nlong, _ = gb.plan_tiles(A.rowptr, 2048)
+    mt, mlong = _plan_model(A.rowptr, 2048)
+    assert nlong == mlong and np.array_equal(tiles.astype(np.int64), mt)
