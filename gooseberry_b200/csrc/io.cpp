@@ -52,10 +52,19 @@ unsigned n_threads() {
   return std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
 }
 
+// body(t) for t in [0, nt), on nt threads (the caller's among them).  A
+// thread that cannot be started runs its share inline instead: nothing
+// throws through the C interface.
 template <class F>
 void parallel_for(unsigned nt, F && body) {
   std::vector<std::thread> th;
-  for (unsigned t = 1; t < nt; ++t) th.emplace_back(body, t);
+  th.reserve(nt);
+  unsigned t = 1;
+  try {
+    for (; t < nt; ++t) th.emplace_back(body, t);
+  } catch (...) {
+    for (unsigned u = t; u < nt; ++u) body(u);
+  }
   body(0u);
   for (auto & x : th) x.join();
 }
