@@ -196,7 +196,7 @@ def cpu_cg_sample(L, b, rtol, iters_full, budget_s=10.0, threads=None):
     """Time the reference cgd (oracle/_ref, else the restatement) for a bounded
     number of iterations on this host; returns (solves/s, info)."""
     import oracle
-    threads = threads or os.cpu_count() or 1
+    threads = threads or host_cores()
     err = rtol * float(np.linalg.norm(b))
     kind = "reference" if oracle.ref_available("f64") else "port"
     if kind == "reference":
@@ -574,7 +574,7 @@ def cpu_spmv_sample(A, x, nbytes, budget_s=10.0):
     host threads; GB/s over repeated full SpMVs within the time budget.
     Returns (GB/s, info, y) with y the baseline's own result."""
     import oracle
-    threads = os.cpu_count() or 1
+    threads = host_cores()
     kind = "reference" if oracle.ref_available("f64") else "port"
     if kind == "reference":
         oracle.ref_set_threads(threads)
@@ -956,7 +956,7 @@ def pagerank_extra(n=2_000_000, nnz=32_000_000, seed=7, tol=1e-10, cpu_iters=5):
            "ms": t_ours * 1e3, "solves_per_s": 1.0 / t_ours,
            "rank_sum": float(r.sum())}
     if oracle.ref_available("f64"):
-        threads = os.cpu_count() or 1
+        threads = host_cores()
         oracle.ref_set_threads(threads)
         t0 = time.perf_counter()
         r5, _, _ = oracle.ref_pagerank(A.rowptr, A.rowind, rv, 0.85, 0.0, cpu_iters)
@@ -994,28 +994,72 @@ def run_extras(args):
     return ex
 
 
+def host_cores() -> int:
+    """Physical cores of this host (logical CPUs when that cannot be read)."""
+    try:
+        import psutil
+        return int(psutil.cpu_count(logical=False) or os.cpu_count() or 1)
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def pin_openmp() -> None:
+    """OpenMP placement for the reference's CPU code: one thread per physical
+    core, kept close.  Must run before the reference library is loaded (libgomp
+    reads these at start-up)."""
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    os.environ.setdefault("OMP_PLACES", "cores")
+
+
 def run_reference_cg(args):
+    """The reference's own cgd on all physical host cores.  A step is one
+    timed block of `block` iterations of a fresh solve (x0 = 0), about 1.5 s,
+    so ms_per_step x steps is the time the arm really spent; the rate is the
+    block's time per iteration scaled to the reference's full iteration count
+    (CG iterations cost the same from the first to the last)."""
+    import oracle
     L, b = cg_laplace_setup()
     ref_it = reference_cg_iterations() or 2966
-    cores = os.cpu_count() or 1
-    vals = []
-    info = None
+    cores = host_cores()
+    err = 1e-8 * float(np.linalg.norm(b))
+    kind = "reference" if oracle.ref_available("f64") else "port"
+    if kind == "reference":
+        oracle.ref_set_threads(cores)
+
+        def run(k):
+            return oracle.ref_cgd(L.rowptr, L.rowind, L.rowval, b, err, k)
+    else:
+        def run(k):
+            return oracle.cgd(L.rowptr, L.rowind, L.rowval, b, err, k, threads=cores)
+    t0 = time.perf_counter()
+    run(10)
+    t_iter = (time.perf_counter() - t0) / 10
+    block = int(max(20, min(ref_it, 1.5 / max(t_iter, 1e-9))))
+    step_s = []
     for k in range(args.warmup + args.steps):
-        v, info = cpu_cg_sample(L, b, 1e-8, ref_it, budget_s=max(2.0, 60.0 / max(
-            args.steps + args.warmup, 1)), threads=cores)
+        t0 = time.perf_counter()
+        _, done, _ = run(block)
+        dt = time.perf_counter() - t0
         if k >= args.warmup:
-            vals.append(v)
-    v = float(np.median(vals))
+            step_s.append(dt / max(done, 1) * block)
+    s_block = float(np.median(step_s))
+    v = 1.0 / (s_block / block * ref_it)
+    info = {"kind": kind, "cores": cores, "iterations_timed": block}
     return {
         "impl": "reference",
         "metric": "CG solves/s (FP64, 2D 5-point Laplacian 1024x1024, rel-res 1e-8)",
         "value": v, "unit": "solves/s", "n_gpus": args.gpus, "gpus_used": 0,
         "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": 1e3 * s_block, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic: seeded b ~ U[-1,1] (seed 2), exact 5-point Laplacian",
         "config": {"workload": "cg_laplace2d_1024 (plain FP64 CG, x0=0, rel-res 1e-8, max 5000 it)",
-                   "n": L.nrows, "nnz": L.nnz, "reference_iterations": ref_it},
+                   "n": L.nrows, "nnz": L.nnz, "reference_iterations": ref_it,
+                   "step": (f"one timed block of {block} of the {ref_it} iterations of a "
+                            "fresh solve; ms_per_step is that block's time"),
+                   "omp": {"threads": cores, "OMP_PROC_BIND": os.environ.get("OMP_PROC_BIND"),
+                           "OMP_PLACES": os.environ.get("OMP_PLACES"),
+                           "logical_cpus": os.cpu_count()}},
         "cpu_baseline": {"value": v, "unit": "solves/s", "cores": info["cores"],
                          "kind": info["kind"],
                          "sample": (f"per step {info['iterations_timed']} of {ref_it} "
@@ -1038,6 +1082,7 @@ def main():
     ap.add_argument("--requests", type=int, default=300,
                     help="requests of the serving stream (extras / --workload serving)")
     args = ap.parse_args()
+    pin_openmp()
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
 

@@ -32,9 +32,10 @@ __all__ = [
     "GooseberryError", "lib", "spmult", "scale", "add_scalar", "cgd", "pagerank",
     "read_csr", "read_grid", "write_csr", "write_grid", "cuthillmckee", "permute_sparse",
     "permute_dense", "permute_vector",
-    "CsrMatrix", "CgSolver", "CgResult", "dot", "spdot", "SUCCESS",
+    "CsrMatrix", "CgSolver", "CgResult", "dot", "spdot", "add", "sub", "SUCCESS",
     "SCHED_AUTO", "SCHED_THREAD", "SCHED_GROUP4", "SCHED_GROUP8", "SCHED_WARP",
-    "SCHED_MERGE", "SCHED_ROW", "SCHED_WTILE", "SCHED_WMERGE", "CG_F64", "CG_MIXED",
+    "SCHED_MERGE", "SCHED_ROW", "SCHED_WTILE", "SCHED_WMERGE", "SCHED_SEG", "CG_F64",
+    "CG_MIXED",
     "CG_PLAIN_ENTRIES", "plan_tiles",
     "Server", "ServerResult",
 ]
@@ -49,13 +50,13 @@ ERROR_NAMES = {
 }
 VALUES_F64, VALUES_F32, DEVICE_POINTERS = 0x1, 0x2, 0x4
 (SCHED_AUTO, SCHED_THREAD, SCHED_GROUP4, SCHED_GROUP8, SCHED_WARP, SCHED_MERGE, SCHED_ROW,
- SCHED_WTILE, SCHED_WMERGE) = range(9)
+ SCHED_WTILE, SCHED_WMERGE, SCHED_SEG) = range(10)
 SCHED_NAMES = {0: "auto", 1: "thread", 2: "group4", 3: "group8", 4: "warp", 5: "merge",
-               6: "row", 7: "wtile", 8: "wmerge"}
+               6: "row", 7: "wtile", 8: "wmerge", 9: "seg"}
 CG_F64, CG_MIXED = 0, 1
 CG_PERSISTENT = 0x100
 CG_PLAIN_ENTRIES = 0x200
-CG_STATUS = {0: "converged", 1: "maxiter", 2: "breakdown", 3: "nonfinite"}
+CG_STATUS = {0: "converged", 1: "maxiter", 2: "breakdown", 3: "nonfinite", 4: "cancelled"}
 
 
 class GooseberryError(RuntimeError):
@@ -139,6 +140,8 @@ SIGNATURES = {
     "gb_cg_solve": (_i, [_vp, _vp, _vp, _d, _i, _sz, _vp, _sz, _vp, _vp]),
     "gb_cg_profile": (_i, [_vp, _vp, _sz, _vp, _sz, _vp, _vp]),
     "gb_cg_entry_bytes": (_i, [_vp, _vp]),
+    "gb_cg_cancel": (_i, [_vp]),
+    "gb_server_cancel": (_i, [_vp, C.c_uint64]),
     "gb_server_create": (_i, [_vp, _vp]),
     "gb_server_destroy": (_i, [_vp]),
     "gb_server_submit": (_i, [_vp, C.c_uint64, _u32, _vp, _vp, _vp, _vp, _vp, _d, _sz]),
@@ -463,6 +466,30 @@ def dot(a, b, stream=None) -> float:
     return float(out.item())
 
 
+def add(a, b, out=None, stream=None):
+    """out = a + b for float64 CUDA tensors (``gb_add_f64``, the reference's
+    blas_add, ``src/blas.c:275-290``); ``out`` may be ``a`` or ``b``."""
+    return _axpby(a, b, out, "gb_add_f64", stream)
+
+
+def sub(a, b, out=None, stream=None):
+    """out = a - b for float64 CUDA tensors (``gb_sub_f64``, the reference's
+    blas_sub, ``src/blas.c:321-336``); ``out`` may be ``a`` or ``b``."""
+    return _axpby(a, b, out, "gb_sub_f64", stream)
+
+
+def _axpby(a, b, out, name, stream):
+    torch = _torch()
+    if out is None:
+        out = torch.empty_like(a)
+    assert a.dtype == b.dtype == out.dtype == torch.float64
+    assert a.is_contiguous() and b.is_contiguous() and out.is_contiguous()
+    assert a.numel() == b.numel() == out.numel()
+    _check(getattr(lib(), name)(a.numel(), a.data_ptr(), b.data_ptr(), out.data_ptr(),
+                                _stream_ptr(stream)), name)
+    return out
+
+
 def spdot(ind, val, x, stream=None) -> float:
     """sum val[k] * x[ind[k]] for CUDA tensors (ind uint32/int32, val and x of
     one float type; float64 accumulation, fixed order)."""
@@ -642,6 +669,11 @@ class CgSolver:
             return x, out, hist[: res.iterations]
         return x, out
 
+    def cancel(self):
+        """Stop the solve running on another thread (``gb_cg_cancel``); with
+        no solve running, the next solve stops at its first check."""
+        _check(lib().gb_cg_cancel(self._h), "gb_cg_cancel")
+
     def entry_bytes(self) -> int:
         """Bytes per matrix entry the solver's SpMV streams (12 = plain CSR)."""
         v = C.c_size_t(0)
@@ -736,6 +768,11 @@ class Server:
                                     CG_STATUS.get(r.status, str(r.status)), r.t_submit,
                                     r.t_admit, r.t_done, self._out.pop(int(r.id))))
         return out
+
+    def cancel(self, rid: int):
+        """Cancel a queued or resident request (``gb_server_cancel``); it is
+        reported by ``poll`` with status "cancelled" (x_out untouched)."""
+        _check(lib().gb_server_cancel(self._h, int(rid)), "gb_server_cancel")
 
     def clock(self) -> float:
         return float(lib().gb_server_clock(self._h))

@@ -8,6 +8,7 @@
 // reference's OpenMP reduction order varies with the thread count,
 // src/blas.c:423-427).
 #include <algorithm>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -207,7 +208,10 @@ static_assert(GB_DOT_NOALLOC_MAX_N == kNoAllocChunk * kNoAllocMaxChunks,
 static __device__ __align__(256) double g_dot_scratch[kNoAllocMaxChunks];
 
 std::mutex g_dot_scratch_mu;
-std::vector<double *> g_dot_scratch_ptr;  // device address of the array, per device
+// Device address of the array per CUDA context, keyed by the context's unique
+// id: a cudaDeviceReset (or any teardown of a primary context) reloads the
+// module in a new context with a new id, so a stale address is never reused.
+std::map<unsigned long long, double *> g_dot_scratch_ptr;
 
 __global__ void __launch_bounds__(kBlock) dot_chunk_kernel(size_t n,
     const double * __restrict__ a, const double * __restrict__ b,
@@ -221,24 +225,58 @@ __global__ void __launch_bounds__(kBlock) dot_chunk_kernel(size_t n,
   if (threadIdx.x == 0) partial[blockIdx.x] = acc;
 }
 
-// Device address of g_dot_scratch on the current device (looked up once).
+// Unique id of the calling thread's current CUDA context (driver entry
+// points cuCtxGetCurrent / cuCtxGetId, resolved once through the runtime so
+// the library needs no link to the driver library).  False when unavailable.
+bool current_context_id(unsigned long long * id) {
+  using GetCurrent = int (*)(void **);
+  using GetId = int (*)(void *, unsigned long long *);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void * f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess && q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrent>(f);
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess && q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(f);
+  });
+  void * ctx = nullptr;
+  return get_current && get_id && get_current(&ctx) == 0 && ctx && get_id(ctx, id) == 0;
+}
+
+// Device address of g_dot_scratch in the current context: looked up once per
+// context (the first call on a device, with that device current), or on
+// every call if the context id cannot be read.
 int dot_scratch_address(double ** out) {
   int dev = 0;
   GB_CUDA_TRY(cudaGetDevice(&dev));
-  std::lock_guard<std::mutex> lock(g_dot_scratch_mu);
-  if (g_dot_scratch_ptr.size() <= static_cast<size_t>(dev))
-    g_dot_scratch_ptr.resize(dev + 1, nullptr);
-  if (!g_dot_scratch_ptr[dev]) {
-    void * p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_dot_scratch);
-    if (e != cudaSuccess || p == nullptr) {
-      set_error("cudaGetSymbolAddress of the dot scratch array failed on device %d: %s", dev,
-          cudaGetErrorString(e));
-      return GOOSEBERRY_ERROR_UNKNOWN;
-    }
-    g_dot_scratch_ptr[dev] = static_cast<double *>(p);
+  unsigned long long ctx = 0;
+  bool keyed = current_context_id(&ctx);
+  if (!keyed) {  // no context bound to this thread yet: bind the primary one
+    GB_CUDA_TRY(cudaFree(nullptr));
+    keyed = current_context_id(&ctx);
   }
-  *out = g_dot_scratch_ptr[dev];
+  std::lock_guard<std::mutex> lock(g_dot_scratch_mu);
+  if (keyed) {
+    auto it = g_dot_scratch_ptr.find(ctx);
+    if (it != g_dot_scratch_ptr.end()) {
+      *out = it->second;
+      return GOOSEBERRY_SUCCESS;
+    }
+  }
+  void * p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_dot_scratch);
+  if (e != cudaSuccess || p == nullptr) {
+    set_error("cudaGetSymbolAddress of the dot scratch array failed on device %d: %s", dev,
+        cudaGetErrorString(e));
+    return GOOSEBERRY_ERROR_UNKNOWN;
+  }
+  if (keyed) g_dot_scratch_ptr[ctx] = static_cast<double *>(p);
+  *out = static_cast<double *>(p);
   return GOOSEBERRY_SUCCESS;
 }
 

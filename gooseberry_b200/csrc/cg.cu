@@ -505,6 +505,16 @@ int occupancy_cg_a_sched(int sched, size_t smem, int * out) {
 // CTA leaves, and the solve reports GB_CG_NONFINITE with rnorm = NaN.
 
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;
+// Values of the abort flag: a barrier timed out, or the host cancelled.
+constexpr int kAbortTimeout = 1;
+constexpr int kAbortCancel = 2;
+
+// A host-written flag in mapped pinned memory, read past every cache.
+__device__ __forceinline__ int ld_host_flag(const int * p) {
+  int v;
+  asm volatile("ld.volatile.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
 
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
@@ -540,12 +550,15 @@ __device__ __forceinline__ bool grid_barrier(unsigned * counter, int * abort_fla
       if (++polls > 64) {
         __nanosleep(64);
         if (global_ns() - t0 > kBarrierTimeoutNs) {
-          atomicExch(abort_flag, 1);
+          atomicExch(abort_flag, kAbortTimeout);
           ok = 0;
           break;
         }
       }
     }
+    // an abort raised before the last arrival is seen by every CTA here, so
+    // all of them leave at the same barrier
+    if (ok && *reinterpret_cast<volatile int *>(abort_flag)) ok = 0;
     __threadfence();
     *ok_smem = ok;
   }
@@ -621,6 +634,7 @@ struct PersistArgs {
   const uint32_t * cta_tiles;  // [G + 1]
   unsigned * sync;
   int * abort_flag;
+  const int * cancel;  // host-mapped cancel request (gb_cg_cancel)
   CgState * st;
   int tol_relative;
   int keep_matrix_in_l2;
@@ -658,6 +672,10 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_persis
   }
   acc = block_sum(acc, red);
   if (tid == 0) a.partial_b[cta] = acc;
+  // CTA 0 reads the host's cancel request one phase before it acts on it, so
+  // the read's latency hides behind the phase's work
+  int cancel_req = 0;
+  if (cta == 0 && tid == 0) cancel_req = ld_host_flag(a.cancel);
   unsigned epoch = 0;
   int status = GB_CG_MAXITER;
   unsigned long long it = 0;
@@ -689,7 +707,10 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_persis
             a.rowind, a.val, g, o, pol_m, pol_x);
       double s = block_sum(o.local, red);
       if (tid == 0) a.partial_a[cta] = s;
+      // a cancel stops the solve before x moves, so x matches `it`
+      if (cta == 0 && tid == 0 && cancel_req) atomicExch(a.abort_flag, kAbortCancel);
       if (!grid_barrier(a.sync, a.abort_flag, ++epoch, &ok_smem)) { aborted = true; break; }
+      if (cta == 0 && tid == 0) cancel_req = ld_host_flag(a.cancel);
       const double pap = ordered_allsum(a.partial_a, G, red, &bcast);
       if (!(pap > 0.0)) {
         status = (pap == pap && rr == rr) ? GB_CG_BREAKDOWN : GB_CG_NONFINITE;
@@ -738,11 +759,13 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_persis
   }
   if (cta == 0 && tid == 0) {
     CgState * st = a.st;
+    const bool cancelled =
+        aborted && *reinterpret_cast<volatile int *>(a.abort_flag) == kAbortCancel;
     st->iter = it;
-    st->rr = aborted ? __longlong_as_double(0x7ff8000000000000ll) : rr;
+    st->rr = aborted && !cancelled ? __longlong_as_double(0x7ff8000000000000ll) : rr;
     st->bnorm = bnorm;
     st->tol = tol;
-    st->status = aborted ? GB_CG_NONFINITE : status;
+    st->status = cancelled ? GB_CG_CANCELLED : (aborted ? GB_CG_NONFINITE : status);
     st->done = 1;
   }
 }
@@ -803,6 +826,8 @@ struct gb_cg {
   const void * fn_p = nullptr;
   uint32_t * cta_tiles = nullptr;
   unsigned * sync = nullptr;  // [0] barrier counter, [1] abort flag
+  int * cancel_h = nullptr;   // pinned, mapped: set by gb_cg_cancel
+  int * cancel_d = nullptr;   // its device address
   int keep_l2 = 0;
   bool l2_hint = false;  // A kernel with L2-policy loads (working set fits in L2)
   bool use_codec = false;  // row schedule over compressed entries
@@ -833,6 +858,7 @@ void destroy_cg(gb_cg * s) {
   dev_free(s->cta_tiles);
   dev_free(s->sync);
   if (s->host_status) cudaFreeHost(s->host_status);
+  if (s->cancel_h) cudaFreeHost(s->cancel_h);
   delete s;
 }
 
@@ -965,6 +991,7 @@ int launch_persistent(gb_cg * s, const double * b, int tol_relative, cudaStream_
   args.cta_tiles = s->cta_tiles;
   args.sync = s->sync;
   args.abort_flag = reinterpret_cast<int *>(s->sync + 1);
+  args.cancel = s->cancel_d;
   args.st = s->st;
   args.tol_relative = tol_relative;
   args.keep_matrix_in_l2 = s->keep_l2;
@@ -981,6 +1008,10 @@ int create_cg(const gb_csr * a, int mode, gb_cg * s) {
   const bool plain_entries = (mode & GB_CG_PLAIN_ENTRIES) != 0;
   mode &= ~(GB_CG_PERSISTENT | GB_CG_PLAIN_ENTRIES);
   GB_CHECK_INPUT(mode == GB_CG_F64 || mode == GB_CG_MIXED, "unknown CG mode %d", mode);
+  GB_CUDA_TRY(cudaHostAlloc(reinterpret_cast<void **>(&s->cancel_h), sizeof(int),
+      cudaHostAllocMapped));
+  *s->cancel_h = 0;
+  GB_CUDA_TRY(cudaHostGetDevicePointer(reinterpret_cast<void **>(&s->cancel_d), s->cancel_h, 0));
   if (mode == GB_CG_MIXED) {
     s->a = a;
     s->mode = mode;
@@ -1050,6 +1081,11 @@ int create_cg(const gb_csr * a, int mode, gb_cg * s) {
   return GOOSEBERRY_SUCCESS;
 }
 
+bool cancel_requested(const gb_cg * s) {
+  return __atomic_load_n(s->cancel_h, __ATOMIC_ACQUIRE) != 0;
+}
+void clear_cancel(gb_cg * s) { __atomic_store_n(s->cancel_h, 0, __ATOMIC_RELEASE); }
+
 int start_solve(gb_cg * s, const double * b, double tol, int tol_relative, size_t niter,
     double * dhist, size_t hl, cudaStream_t stream) {
   // niter == 0 means "no limit" as in the reference; a solve that can never
@@ -1073,9 +1109,12 @@ int start_solve(gb_cg * s, const double * b, double tol, int tol_relative, size_
 int solve_cg(gb_cg * s, const double * b, double * x, double tol, int tol_relative,
     size_t niter, double * history, size_t history_len, gb_cg_result_t * res,
     cudaStream_t stream) {
-  if (s->mixed)
-    return mixed_solve(s->mixed, b, x, tol, tol_relative, niter, history, history_len, res,
-        stream);
+  if (s->mixed) {
+    const int rc = mixed_solve(s->mixed, b, x, tol, tol_relative, niter, history, history_len,
+        res, stream, s->cancel_h);
+    if (rc == GOOSEBERRY_SUCCESS && res && res->status == GB_CG_CANCELLED) clear_cancel(s);
+    return rc;
+  }
   GB_CHECK_INPUT(s->n == 0 || (b && x), "NULL vector");
   GB_CHECK_INPUT(s->a->sched64 == s->sched && s->a->plan.tile_items == s->tile_items,
       "matrix schedule changed after the solver was created");
@@ -1110,6 +1149,7 @@ int solve_cg(gb_cg * s, const double * b, double * x, double tol, int tol_relati
     if (rc == GOOSEBERRY_SUCCESS) rc = launch(1);
   }
   int slot = 0;
+  bool cancelled = false;
   while (rc == GOOSEBERRY_SUCCESS && !s->persistent) {
     cudaError_t e = cudaEventSynchronize(ev[slot]);
     if (e != cudaSuccess) {
@@ -1118,6 +1158,10 @@ int solve_cg(gb_cg * s, const double * b, double * x, double tol, int tol_relati
       break;
     }
     if (s->host_status[slot].done) break;
+    if (cancel_requested(s)) {  // the graph in flight finishes; no new one starts
+      cancelled = true;
+      break;
+    }
     rc = launch(slot);
     slot ^= 1;
   }
@@ -1140,10 +1184,14 @@ int solve_cg(gb_cg * s, const double * b, double * x, double tol, int tol_relati
     unsigned flags[2] = {0, 0};
     if (e == cudaSuccess && s->persistent)
       e = cudaMemcpy(flags, s->sync, sizeof(flags), cudaMemcpyDeviceToHost);
+    if (flags[1] == kAbortCancel || (cancelled && !fin.done)) {
+      fin.status = GB_CG_CANCELLED;
+      clear_cancel(s);
+    }
     if (e != cudaSuccess) {
       set_error("CG result copy failed: %s", cudaGetErrorString(e));
       rc = GOOSEBERRY_ERROR_UNKNOWN;
-    } else if (flags[1]) {
+    } else if (flags[1] == kAbortTimeout) {
       set_error("CG solve abandoned: a grid barrier timed out");
       rc = GOOSEBERRY_ERROR_UNKNOWN;
     } else if (res) {
@@ -1247,6 +1295,12 @@ int gb_cg_solve(gb_cg_t * s, const double * b, double * x, double tol, int tol_r
   GB_CHECK_INPUT(s != nullptr, "solver is NULL");
   return gb::solve_cg(s, b, x, tol, tol_relative, niter, history, history_len, result,
       static_cast<cudaStream_t>(stream));
+}
+
+int gb_cg_cancel(gb_cg_t * s) {
+  GB_CHECK_INPUT(s != nullptr, "solver is NULL");
+  __atomic_store_n(s->cancel_h, 1, __ATOMIC_RELEASE);
+  return GOOSEBERRY_SUCCESS;
 }
 
 int gb_cg_entry_bytes(const gb_cg_t * s, size_t * bytes) {

@@ -781,7 +781,7 @@ int mixed_start(MixedCg * m, const double * b, double tol, int tol_relative, siz
 
 int mixed_solve(MixedCg * m, const double * b, double * x, double tol, int tol_relative,
     size_t niter, double * history, size_t history_len, gb_cg_result_t * res,
-    cudaStream_t stream) {
+    cudaStream_t stream, const int * cancel) {
   GB_CHECK_INPUT(m->n == 0 || (b && x), "NULL vector");
   GB_CHECK_INPUT(m->a->sched32 == m->sched32 && m->a->sched64 == m->sched64 &&
                  m->a->plan.tile_items == m->tile_items,
@@ -813,6 +813,7 @@ int mixed_solve(MixedCg * m, const double * b, double * x, double tol, int tol_r
   rc = launch(0);
   if (rc == GOOSEBERRY_SUCCESS) rc = launch(1);
   int slot = 0;
+  bool cancelled = false;
   while (rc == GOOSEBERRY_SUCCESS) {
     cudaError_t e = cudaEventSynchronize(ev[slot]);
     if (e != cudaSuccess) {
@@ -821,6 +822,10 @@ int mixed_solve(MixedCg * m, const double * b, double * x, double tol, int tol_r
       break;
     }
     if (m->host_status[slot].done) break;
+    if (cancel && __atomic_load_n(cancel, __ATOMIC_ACQUIRE)) {  // no new graph starts
+      cancelled = true;
+      break;
+    }
     rc = launch(slot);
     slot ^= 1;
   }
@@ -861,7 +866,7 @@ int mixed_solve(MixedCg * m, const double * b, double * x, double tol, int tol_r
     res->refinements = fin.refinements;
     res->rnorm = std::sqrt(fin.rr_true);
     res->bnorm = fin.bnorm;
-    res->status = fin.status;
+    res->status = cancelled && fin.status != GB_CG_CONVERGED ? GB_CG_CANCELLED : fin.status;
     res->kernel_launches = launches;
   }
   if (dhist) scratch_free(dhist, stream);

@@ -81,6 +81,22 @@ struct PlanView {
   uint32_t nrows;
 };
 
+// Segmented plan (the SEG schedule, spmv_seg.cuh): one contiguous range of
+// nonzeros per warp, balanced on rows + nonzeros, every range starting at a
+// multiple of 4.  A row that starts before a warp's range and ends in it is
+// the warp's head row; the row open at the range end continues (tail_last)
+// or ends there.
+struct SegRange {
+  uint32_t nz_begin;    // first nonzero of the range (multiple of 4)
+  uint32_t row_begin;   // first row whose start is >= nz_begin
+  uint32_t head_row;    // row holding nz_begin when it starts earlier, else ~0
+  uint32_t head_first;  // warp holding head_row's first nonzero
+  uint32_t tail_last;   // warp holding the last nonzero of the row open at the range end,
+                        // when that row continues past it, else ~0
+  uint32_t span_count;  // warps with nonzeros of head_row, when head_row ends here
+  uint32_t pad0, pad1;
+};
+
 struct Plan {
   uint32_t tile_items = 0;
   uint32_t chunk_nnz = 0;
@@ -89,17 +105,28 @@ struct Plan {
   // row-length summary
   uint32_t max_row = 0, p50 = 0, p90 = 0, p99 = 0;
   double mean_row = 0.0;
+  // segmented plan ([nwarps + 1] ranges; empty until built)
+  std::vector<SegRange> seg;
   // device copies
   TileDesc * d_tiles = nullptr;
   LongRowDesc * d_longrows = nullptr;
   double * d_chunk_partial = nullptr;
   unsigned int * d_long_count = nullptr;
+  SegRange * d_seg = nullptr;
+  double * d_seg_rec = nullptr;  // [2 nwarps]: head records, then tail records
+  unsigned int * d_seg_count = nullptr;
 };
 
 // Build the tile plan from a HOST copy of rowptr.  Returns INVALIDINPUT if
 // rowptr decreases or does not span nnz.
 int build_plan(uint32_t nrows, const uint32_t * rowptr, uint32_t nnz,
     uint32_t tile_items, Plan & plan);
+// The segmented ranges for at most `max_warps` warps (HOST rowptr, already
+// validated by build_plan).
+void build_seg_plan(uint32_t nrows, const uint32_t * rowptr, uint32_t nnz,
+    uint32_t max_warps, Plan & plan);
+// Warps a segmented plan is built for on the current device.
+uint32_t seg_max_warps(int sm_count);
 int upload_plan(Plan & plan, cudaStream_t stream);
 void free_plan(Plan & plan);
 
@@ -210,9 +237,11 @@ struct MixedCg;
 int mixed_create(const gb_csr * a, bool plain_entries, MixedCg ** out);
 size_t mixed_entry_bytes(const MixedCg * m);
 void mixed_destroy(MixedCg * m);
+// `cancel` (host memory, may be null): a nonzero value stops the solve
+// between graph replays with status GB_CG_CANCELLED.
 int mixed_solve(MixedCg * m, const double * b, double * x, double tol, int tol_relative,
     size_t niter, double * history, size_t history_len, gb_cg_result_t * res,
-    cudaStream_t stream);
+    cudaStream_t stream, const int * cancel = nullptr);
 int mixed_profile(MixedCg * m, const double * b, size_t iterations, double * ms,
     size_t ms_len, size_t * nkernels, cudaStream_t stream);
 

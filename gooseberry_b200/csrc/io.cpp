@@ -58,9 +58,9 @@ unsigned n_threads() {
 template <class F>
 void parallel_for(unsigned nt, F && body) {
   std::vector<std::thread> th;
-  th.reserve(nt);
   unsigned t = 1;
   try {
+    th.reserve(nt);
     for (; t < nt; ++t) th.emplace_back(body, t);
   } catch (...) {
     for (unsigned u = t; u < nt; ++u) body(u);

@@ -601,6 +601,7 @@ struct Request {
 
 struct SlotHost {
   bool used = false;
+  bool cancel = false;  // retire at the next step without copying x out
   uint64_t id = 0;
   uint32_t n = 0;
   size_t off = 0, bytes = 0;
@@ -870,17 +871,39 @@ int admit(gb_server & s, Request & q, uint32_t k) {
   return GOOSEBERRY_SUCCESS;
 }
 
+int cancel(gb_server & s, uint64_t id) {
+  for (auto it = s.queue.begin(); it != s.queue.end(); ++it) {
+    if (it->id != id) continue;
+    gb_server_result_t res{};
+    res.id = id;
+    res.status = GB_CG_CANCELLED;
+    res.t_submit = it->t_submit;
+    res.t_admit = res.t_done = now_s(s);
+    s.results.push_back(res);
+    s.queue.erase(it);
+    return GOOSEBERRY_SUCCESS;
+  }
+  for (auto & h : s.slots) {
+    if (!h.used || h.id != id || h.cancel) continue;
+    h.cancel = true;  // the step in flight may still run it; the next step retires it
+    return GOOSEBERRY_SUCCESS;
+  }
+  set_error("no queued or resident request with id %llu", static_cast<unsigned long long>(id));
+  return GOOSEBERRY_ERROR_INVALIDINPUT;
+}
+
 int step(gb_server & s, size_t * active, size_t * queued) {
   if (s.inflight) {
     GB_CUDA_TRY(cudaEventSynchronize(s.step_done));
     s.inflight = false;
   }
-  // 1. retire finished solves: copy x out, free memory and the slot
+  // 1. retire finished (or cancelled) solves: copy x out, free memory and
+  //    the slot
   bool any_done = false;
   for (uint32_t k = 0; k < s.cfg.max_slots; ++k) {
     SlotHost & h = s.slots[k];
     const SrvSlot & S = s.h_slots[k];
-    if (!h.used || !S.done) continue;
+    if (!h.used || !S.done) continue;  // a solve that finished before its cancel keeps x
     const double * x = (s.mixed && S.xpar) ? S.x1 : S.x0;
     GB_CUDA_TRY(cudaMemcpyAsync(h.x_out, x, 8ull * h.n, cudaMemcpyDeviceToHost, s.stream));
     any_done = true;
@@ -889,14 +912,14 @@ int step(gb_server & s, size_t * active, size_t * queued) {
   for (uint32_t k = 0; k < s.cfg.max_slots; ++k) {
     SlotHost & h = s.slots[k];
     SrvSlot & S = s.h_slots[k];
-    if (!h.used || !S.done) continue;
+    if (!h.used || !(S.done || h.cancel)) continue;
     gb_server_result_t res;
     res.id = h.id;
     res.iterations = S.iter;
     res.refinements = S.refinements;
     res.rnorm = std::sqrt(S.rr_true);
     res.bnorm = S.bnorm;
-    res.status = S.status;
+    res.status = S.done ? S.status : GB_CG_CANCELLED;
     res.t_submit = h.t_submit;
     res.t_admit = h.t_admit;
     res.t_done = now_s(s);
@@ -1002,6 +1025,11 @@ int gb_server_poll(gb_server_t * s, gb_server_result_t * out, size_t max, size_t
   s->results.erase(s->results.begin(), s->results.begin() + m);
   *count = m;
   return GOOSEBERRY_SUCCESS;
+}
+
+int gb_server_cancel(gb_server_t * s, uint64_t id) {
+  GB_CHECK_INPUT(s != nullptr, "server is NULL");
+  return gb::cancel(*s, id);
 }
 
 double gb_server_clock(const gb_server_t * s) { return s ? gb::now_s(*s) : 0.0; }

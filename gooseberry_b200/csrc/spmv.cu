@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "gb_internal.h"
+#include "spmv_seg.cuh"
 #include "spmv_tiles.cuh"
 
 namespace gb {
@@ -101,9 +102,9 @@ uint32_t plan_step(Plan & plan, uint32_t r, const uint32_t * rowptr, uint32_t nr
 template <class F>
 void run_threads(unsigned nt, F && body) {
   std::vector<std::thread> th;
-  th.reserve(nt);
   unsigned t = 1;
   try {
+    th.reserve(nt);
     for (; t < nt; ++t) th.emplace_back(body, t);
   } catch (...) {
     for (unsigned u = t; u < nt; ++u) body(u);
@@ -236,17 +237,86 @@ int build_plan(uint32_t nrows, const uint32_t * rowptr, uint32_t nnz,
   return GOOSEBERRY_SUCCESS;
 }
 
+uint32_t seg_max_warps(int sm_count) {
+  return static_cast<uint32_t>(std::max(sm_count, 1)) * kSegMinBlocks * kSegWarps;
+}
+
+// Ranges of a merge-path split of (row ends, nonzeros) into equal shares of
+// rows + nonzeros, each range start rounded down to a multiple of 4.  At
+// least kSegMinItems items per warp, so small matrices use fewer warps.
+void build_seg_plan(uint32_t nrows, const uint32_t * rowptr, uint32_t nnz,
+    uint32_t max_warps, Plan & plan) {
+  constexpr uint64_t kSegMinItems = 96;
+  const uint64_t total = static_cast<uint64_t>(nrows) + nnz;
+  const uint32_t W = static_cast<uint32_t>(std::max<uint64_t>(1,
+      std::min<uint64_t>(max_warps, total / kSegMinItems)));
+  std::vector<uint32_t> nzb(static_cast<size_t>(W) + 1);
+  for (uint32_t w = 0; w < W; ++w) {
+    const uint64_t d = total * w / W;
+    // rows whose end comes before merge position d: the smallest i with
+    // rowptr[i + 1] + i >= d (row i's end sits at merge position rowptr[i+1] + i)
+    uint64_t lo = d > nnz ? d - nnz : 0, hi = std::min<uint64_t>(d, nrows);
+    while (lo < hi) {
+      const uint64_t mid = (lo + hi) / 2;
+      if (static_cast<uint64_t>(rowptr[mid + 1]) + mid < d) lo = mid + 1; else hi = mid;
+    }
+    nzb[w] = static_cast<uint32_t>(std::min<uint64_t>(d - lo, nnz)) & ~3u;
+  }
+  for (uint32_t w = 1; w < W; ++w) nzb[w] = std::max(nzb[w], nzb[w - 1]);
+  nzb[W] = nnz;
+  // warp holding nonzero p (the last range starting at or before p)
+  auto warp_of = [&](uint32_t p) {
+    return static_cast<uint32_t>(std::upper_bound(nzb.begin(), nzb.begin() + W, p) -
+                                 nzb.begin()) - 1;
+  };
+  // row holding nonzero p < nnz (the last row starting at or before p)
+  auto row_of = [&](uint32_t p) {
+    return static_cast<uint32_t>(std::upper_bound(rowptr, rowptr + nrows + 1, p) - rowptr) - 1;
+  };
+  std::vector<uint32_t> nonempty_before(static_cast<size_t>(W) + 1, 0);
+  for (uint32_t w = 0; w < W; ++w)
+    nonempty_before[w + 1] = nonempty_before[w] + (nzb[w + 1] > nzb[w] ? 1u : 0u);
+  plan.seg.assign(static_cast<size_t>(W) + 1, SegRange{});
+  for (uint32_t w = 0; w <= W; ++w) {
+    SegRange & g = plan.seg[w];
+    g.nz_begin = nzb[w];
+    g.head_row = g.head_first = g.tail_last = kSegNone;
+    g.span_count = 0;
+    if (w == W) continue;
+    g.row_begin = static_cast<uint32_t>(
+        std::lower_bound(rowptr, rowptr + nrows + 1, nzb[w]) - rowptr);
+    if (g.row_begin > nrows) g.row_begin = nrows;
+    if (nzb[w + 1] == nzb[w]) continue;  // no nonzeros: no rows to join
+    const uint32_t hr = row_of(nzb[w]);
+    if (rowptr[hr] < nzb[w]) {
+      g.head_row = hr;
+      g.head_first = warp_of(rowptr[hr]);
+      if (rowptr[hr + 1] <= nzb[w + 1])
+        g.span_count = nonempty_before[w + 1] - nonempty_before[g.head_first];
+    }
+    const uint32_t tr = row_of(nzb[w + 1] - 1);
+    if (rowptr[tr + 1] > nzb[w + 1]) g.tail_last = warp_of(rowptr[tr + 1] - 1);
+  }
+}
+
 void free_plan(Plan & plan) {
-  if (plan.d_tiles || plan.d_longrows || plan.d_chunk_partial || plan.d_long_count)
+  if (plan.d_tiles || plan.d_longrows || plan.d_chunk_partial || plan.d_long_count ||
+      plan.d_seg)
     cudaDeviceSynchronize();  // no kernel may still read the old plan
   if (plan.d_tiles) dev_free(plan.d_tiles);
   if (plan.d_longrows) dev_free(plan.d_longrows);
   if (plan.d_chunk_partial) dev_free(plan.d_chunk_partial);
   if (plan.d_long_count) dev_free(plan.d_long_count);
+  if (plan.d_seg) dev_free(plan.d_seg);
+  if (plan.d_seg_rec) dev_free(plan.d_seg_rec);
+  if (plan.d_seg_count) dev_free(plan.d_seg_count);
   plan.d_tiles = nullptr;
   plan.d_longrows = nullptr;
   plan.d_chunk_partial = nullptr;
   plan.d_long_count = nullptr;
+  plan.d_seg = nullptr;
+  plan.d_seg_rec = nullptr;
+  plan.d_seg_count = nullptr;
 }
 
 int upload_plan(Plan & plan, cudaStream_t stream) {
@@ -264,6 +334,16 @@ int upload_plan(Plan & plan, cudaStream_t stream) {
     GB_CUDA_TRY(cudaMemcpyAsync(plan.d_longrows, plan.longrows.data(),
         plan.longrows.size() * sizeof(LongRowDesc), cudaMemcpyHostToDevice, stream));
   GB_CUDA_TRY(cudaMemsetAsync(plan.d_long_count, 0, nl * sizeof(unsigned int), stream));
+  if (!plan.seg.empty()) {
+    const size_t W = plan.seg.size() - 1;
+    GB_TRY(dev_alloc(&plan.d_seg, plan.seg.size() * sizeof(SegRange)));
+    GB_TRY(dev_alloc(&plan.d_seg_rec, 2 * W * sizeof(double)));
+    GB_TRY(dev_alloc(&plan.d_seg_count, W * sizeof(unsigned int)));
+    GB_CUDA_TRY(cudaMemcpyAsync(plan.d_seg, plan.seg.data(), plan.seg.size() * sizeof(SegRange),
+        cudaMemcpyHostToDevice, stream));
+    GB_CUDA_TRY(cudaMemsetAsync(plan.d_seg_rec, 0, 2 * W * sizeof(double), stream));
+    GB_CUDA_TRY(cudaMemsetAsync(plan.d_seg_count, 0, W * sizeof(unsigned int), stream));
+  }
   GB_CUDA_TRY(cudaStreamSynchronize(stream));  // host vectors may change later
   return GOOSEBERRY_SUCCESS;
 }
@@ -380,10 +460,53 @@ int launch_tiles(const gb_csr & a, const V * val, const Gather & g, const Out & 
   return GOOSEBERRY_SUCCESS;
 }
 
+template <typename V, typename Acc, class Out>
+__global__ void __launch_bounds__(kSegBlock, kSegMinBlocks)
+spmv_seg_kernel(const SegView sv, const uint32_t * __restrict__ rowptr,
+    const uint32_t * __restrict__ rowind, const V * __restrict__ val,
+    const Acc * __restrict__ x, Out out) {
+  spmv_seg_body<V, Acc, GB_SEG_K>(sv, rowptr, rowind, val, x, out);
+}
+
+// Whether the segmented schedule's 16-byte loads can read these arrays.
+bool seg_aligned(const gb_csr & a, const void * val) {
+  return (reinterpret_cast<uintptr_t>(a.rowind) & 15u) == 0 &&
+         (reinterpret_cast<uintptr_t>(val) & 15u) == 0;
+}
+
+template <typename V, typename Acc, class Gather, class Out>
+int launch_seg(const gb_csr & a, const V * val, const Gather & g, const Out & o,
+    cudaStream_t stream) {
+  if constexpr (IsPlainGather<Gather>::value) {
+    if (a.nrows == 0) return GOOSEBERRY_SUCCESS;
+    GB_CHECK_INPUT(a.plan.d_seg != nullptr, "the matrix has no segmented plan");
+    GB_CHECK_INPUT(a.nnz == 0 || seg_aligned(a, val),
+        "the segmented schedule needs rowind and values on 16-byte boundaries");
+    SegView sv;
+    sv.ranges = a.plan.d_seg;
+    sv.nwarps = static_cast<uint32_t>(a.plan.seg.size() - 1);
+    sv.head_rec = a.plan.d_seg_rec;
+    sv.tail_rec = a.plan.d_seg_rec + sv.nwarps;
+    sv.count = a.plan.d_seg_count;
+    sv.nrows = a.nrows;
+    sv.ncols = a.ncols;
+    sv.nnz = a.nnz;
+    const uint32_t grid = (sv.nwarps + kSegWarps - 1) / kSegWarps;
+    spmv_seg_kernel<V, Acc, Out><<<grid, kSegBlock, 0, stream>>>(sv, a.rowptr, a.rowind, val,
+        g.x, o);
+    GB_CUDA_TRY(cudaGetLastError());
+    return GOOSEBERRY_SUCCESS;
+  } else {
+    set_error("the segmented schedule computes plain SpMV only");
+    return GOOSEBERRY_ERROR_INVALIDINPUT;
+  }
+}
+
 template <typename V, typename Acc, class Gather, class Out>
 int launch_sched(const gb_csr & a, int sched, const V * val, const Gather & g,
     const Out & o, cudaStream_t stream) {
   switch (sched) {
+    case GB_SCHED_SEG: return launch_seg<V, Acc>(a, val, g, o, stream);
     case GB_SCHED_THREAD: return launch_tiles<V, Acc, SCHED_THREAD>(a, val, g, o, stream);
     case GB_SCHED_GROUP4: return launch_tiles<V, Acc, SCHED_GROUP4>(a, val, g, o, stream);
     case GB_SCHED_GROUP8: return launch_tiles<V, Acc, SCHED_GROUP8>(a, val, g, o, stream);
@@ -479,6 +602,7 @@ int rebuild_plan(gb_csr & a, uint32_t tile_items, cudaStream_t stream) {
   GB_CUDA_TRY(cudaStreamSynchronize(stream));
   Plan p;
   GB_TRY(build_plan(a.nrows, hrp.data(), a.nnz, tile_items, p));
+  build_seg_plan(a.nrows, hrp.data(), a.nnz, seg_max_warps(a.sm_count), p);
   GB_TRY(upload_plan(p, stream));
   free_plan(a.plan);
   a.plan = std::move(p);
@@ -517,6 +641,9 @@ int autotune(gb_csr & a, unsigned width, cudaStream_t stream) {
   if (short_rows) cands.push_back({1024, GB_SCHED_ROW});
   for (uint32_t t : {128u, 256u, 512u}) cands.push_back({t, GB_SCHED_WTILE});
   cands.push_back({static_cast<uint32_t>(32 * kWmKt), GB_SCHED_WMERGE});
+  const void * vals = width == GB_CSR_VALUES_F32 ? static_cast<const void *>(a.val32)
+                                                  : static_cast<const void *>(a.val64);
+  if (seg_aligned(a, vals)) cands.push_back({kDefaultTileItems, GB_SCHED_SEG});
   for (uint32_t t : {512u, 1024u, 2048u, 4096u}) {
     if (a.plan.p90 <= 64) cands.push_back({t, GB_SCHED_THREAD});
     cands.push_back({t, GB_SCHED_GROUP4});
@@ -633,6 +760,7 @@ int create_impl(dim_t nrows, dim_t ncols, ind_t nnz, const ind_t * rowptr,
     rp_host = hrp.data();
   }
   GB_TRY(gb::build_plan(nrows, rp_host, nnz, gb::kDefaultTileItems, a->plan));
+  gb::build_seg_plan(nrows, rp_host, nnz, gb::seg_max_warps(a->sm_count), a->plan);
 
   if (dev) {
     a->rowptr = rowptr;
@@ -764,8 +892,13 @@ int gb_csr_get_info(const gb_csr_t * a, gb_csr_info_t * info) {
 int gb_csr_set_schedule(gb_csr_t * a, unsigned value_width, int schedule,
     uint32_t tile_items) {
   GB_CHECK_INPUT(a != nullptr, "matrix is NULL");
-  GB_CHECK_INPUT(schedule >= GB_SCHED_AUTO && schedule <= GB_SCHED_WMERGE,
+  GB_CHECK_INPUT(schedule >= GB_SCHED_AUTO && schedule <= GB_SCHED_SEG,
       "unknown schedule %d", schedule);
+  GB_CHECK_INPUT(schedule != GB_SCHED_SEG || a->nnz == 0 ||
+                     gb::seg_aligned(*a, value_width == GB_CSR_VALUES_F32
+                                             ? static_cast<const void *>(a->val32)
+                                             : static_cast<const void *>(a->val64)),
+      "the segmented schedule needs rowind and values on 16-byte boundaries");
   GB_CHECK_INPUT(value_width == GB_CSR_VALUES_F64 || value_width == GB_CSR_VALUES_F32,
       "value_width must be GB_CSR_VALUES_F64 or GB_CSR_VALUES_F32");
   // per-warp tiles keep two stages per warp in shared memory: they need small

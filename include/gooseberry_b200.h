@@ -80,13 +80,22 @@ typedef enum gb_schedule {
                             memory stage with cp.async while its lanes sum
                             the current tile's rows, one row per lane, in
                             the reference's order (bit-identical, like ROW) */
-  GB_SCHED_WMERGE = 8    /* per-WARP tiles of at most 128 items, no CTA
+  GB_SCHED_WMERGE = 8,   /* per-WARP tiles of at most 128 items, no CTA
                             barrier: indices, values and x gathers are
                             prefetched into registers one tile ahead, and
                             rows are reduced along the merge path of (row
                             ends, nonzeros) with equal work per lane (for
                             skewed row lengths).  The CG solvers run a
                             matrix set to this schedule with MERGE. */
+  GB_SCHED_SEG = 9       /* no tiles: one contiguous range of nonzeros per
+                            warp (balanced on rows + nonzeros), read with
+                            16-byte loads; each lane sums 4 consecutive
+                            products and a segmented scan over the lanes
+                            joins rows that span lanes, whatever the row
+                            lengths.  Needs rowind and the values on
+                            16-byte boundaries (always true for matrices
+                            the library uploads).  Plain SpMV only: the CG
+                            solvers run such a matrix with MERGE. */
 } gb_schedule_t;
 
 /*
@@ -215,8 +224,9 @@ GOOSEBERRY_API int gb_spdot_f32(size_t nnz, const dim_t * ind, const float * val
  *   - n may be at most GB_DOT_NOALLOC_MAX_N; larger n is rejected with
  *     GOOSEBERRY_ERROR_INVALIDINPUT before anything runs.
  *   - The first call on each device looks up that array's device address
- *     (with that device current) and remembers it: make that first call
- *     before any stream capture.
+ *     (with that device current) and remembers it for the device's CUDA
+ *     context: make that first call before any stream capture.  After a
+ *     cudaDeviceReset the next call is again a first call (new context).
  *   - Every call on a device shares the one array, and it keeps the previous
  *     call's partial sums (each call writes every entry it reads first), so
  *     calls whose kernels overlap on the GPU (different streams, or threads
@@ -267,7 +277,9 @@ typedef enum gb_cg_status {
   GB_CG_CONVERGED = 0,  /* ||r|| <= tolerance                                 */
   GB_CG_MAXITER = 1,    /* iteration limit reached first                      */
   GB_CG_BREAKDOWN = 2,  /* p.Ap <= 0: matrix not SPD                          */
-  GB_CG_NONFINITE = 3   /* NaN or Inf appeared                                */
+  GB_CG_NONFINITE = 3,  /* NaN or Inf appeared                                */
+  GB_CG_CANCELLED = 4   /* stopped by gb_cg_cancel / gb_server_cancel; x is
+                           the iterate of the last finished iteration        */
 } gb_cg_status_t;
 
 typedef struct gb_cg_result {
@@ -297,6 +309,16 @@ GOOSEBERRY_API int gb_cg_destroy(gb_cg_t * s);
 GOOSEBERRY_API int gb_cg_solve(gb_cg_t * s, const double * b, double * x, double tol,
     int tol_relative, size_t niter, double * history, size_t history_len,
     gb_cg_result_t * result, gb_stream_t stream);
+
+/* Ask the solver's running gb_cg_solve (called on another thread) to stop.
+ * Safe to call from any thread at any time.  The solve ends at its next
+ * check -- between graph replays, or, for a GB_CG_PERSISTENT solve, at the
+ * next iteration's first grid barrier, which every CTA then leaves -- and
+ * reports GB_CG_CANCELLED with the iterations it finished.  A request made
+ * while no solve runs stops the next solve at its first check; a solve that
+ * stopped on a request clears it.  The reference's cgd cannot be stopped
+ * (src/cgd.c:87-119); no counterpart. */
+GOOSEBERRY_API int gb_cg_cancel(gb_cg_t * s);
 
 /*
  * Measurement hook: start a solve of A x = b and run its first `iterations`
@@ -369,6 +391,14 @@ GOOSEBERRY_API int gb_server_step(gb_server_t * s, size_t * active, size_t * que
 /* Move up to `max` finished results into `out`; *count receives how many. */
 GOOSEBERRY_API int gb_server_poll(gb_server_t * s, gb_server_result_t * out, size_t max,
     size_t * count);
+
+/* Cancel request `id`.  A queued request is dropped at once; a resident one
+ * is retired at the next gb_server_step (its slot and memory are freed and
+ * x_out is left as it was).  Either way gb_server_poll then reports it with
+ * status GB_CG_CANCELLED.  INVALIDINPUT if no queued or resident request has
+ * that id (it was never submitted, or has already finished).  The reference
+ * has no server, so no counterpart. */
+GOOSEBERRY_API int gb_server_cancel(gb_server_t * s, uint64_t id);
 
 /* Seconds since the server was created (the clock of the result stamps). */
 GOOSEBERRY_API double gb_server_clock(const gb_server_t * s);

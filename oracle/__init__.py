@@ -32,13 +32,27 @@ _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 
 
-def build(ref_root: str | None = "/root/reference", quiet: bool = True) -> None:
-    """Compile the restatement, and the reference build when its sources exist."""
+def build(ref_root: str | None = None, quiet: bool = True) -> None:
+    """Compile the restatement, and the reference build when its sources exist.
+
+    ``ref_root`` is the reference checkout; None takes the environment
+    variable GOOSEBERRY_REFERENCE, else the default of oracle/Makefile.  The
+    reference build is skipped when that directory has no ``src/``."""
     targets = ["oracle"]
+    cmd = ["make", "-C", _HERE]
+    if ref_root is None:
+        ref_root = os.environ.get("GOOSEBERRY_REFERENCE") or _makefile_reference()
     if ref_root and os.path.isdir(os.path.join(ref_root, "src")):
         targets.append("ref")
-    cmd = ["make", "-C", _HERE, f"REF={ref_root or ''}"] + targets
-    subprocess.run(cmd, check=True, capture_output=quiet)
+        cmd.append(f"REF={ref_root}")
+    subprocess.run(cmd + targets, check=True, capture_output=quiet)
+
+
+def _makefile_reference() -> str | None:
+    """The reference checkout oracle/Makefile defaults to."""
+    r = subprocess.run(["make", "-s", "-C", _HERE, "--no-print-directory", "print-ref"],
+                       capture_output=True, text=True)
+    return r.stdout.strip() or None if r.returncode == 0 else None
 
 
 def _lib():
@@ -107,6 +121,9 @@ def _ref(real: str = "f64"):
         lib.gbref_spmult.restype = C.c_int
         lib.gbref_dot.argtypes = [C.c_uint32, p, p]
         lib.gbref_dot.restype = C.c_double
+        for nm in ("gbref_add", "gbref_sub"):
+            getattr(lib, nm).argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
+            getattr(lib, nm).restype = C.c_int
         lib.gbref_spdot.argtypes = [C.c_uint32, _u32p, p, p]
         lib.gbref_spdot.restype = C.c_double
         lib.gbref_pagerank.argtypes = [C.c_uint32, _u32p, _u32p, p, C.c_double, C.c_double,
@@ -247,6 +264,20 @@ def ref_spmm(rowptr, rowind, rowval, B, ncols=None, bncols=1, blocks=None, out=N
     if rc != 1:
         raise RuntimeError(f"blas_spmult returned {rc}")
     return C_
+
+
+def ref_axpby(a, b, c, subtract=False, real="f64"):
+    """c = a + b (blas_add, src/blas.c:275-290) or c = a - b (blas_sub,
+    src/blas.c:321-336) through the reference build, in place on numpy arrays
+    of the build's real type; c may be the same array as a or b."""
+    dt = _dt(real)
+    for v in (a, b, c):
+        assert v.dtype == dt and v.flags.c_contiguous and len(v) == len(c)
+    fn = _ref(real).gbref_sub if subtract else _ref(real).gbref_add
+    rc = fn(len(c), a.ctypes.data, b.ctypes.data, c.ctypes.data)
+    if rc != 1:
+        raise RuntimeError(f"blas_{'sub' if subtract else 'add'} returned {rc}")
+    return c
 
 
 def ref_dot(a, b, real="f64"):

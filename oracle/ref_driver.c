@@ -12,6 +12,8 @@
  * - gbref_spmult: forwards to blas_spmult (src/blas.c:552-606), the body of
  *   gooseberry_spmult (src/gooseberry.c:53-67).
  * - gbref_dot:    forwards to blas_dot (src/blas.c:413-430).
+ * - gbref_add / gbref_sub: forward to blas_add / blas_sub (src/blas.c:275-290,
+ *   321-336) on an n x 1 dense vector; c may alias a or b, as cgd uses it.
  * - gbref_spdot:  forwards to blas_spdot (src/blas.c:433-451).
  * - gbref_read_sparse / _read_dense / _write_sparse / _write_dense: forward
  *   to the reference's src/io.c readers and writers (CSR and grid formats,
@@ -52,6 +54,8 @@ int gbref_spmult(dim_t anrows, dim_t ancols, dim_t bncols,
     const real_t * bcolval, real_t * crowval, const dim_t * blocks,
     dim_t nblocks);
 double gbref_dot(dim_t n, const real_t * a, const real_t * b);
+int gbref_add(dim_t n, const real_t * a, const real_t * b, real_t * c);
+int gbref_sub(dim_t n, const real_t * a, const real_t * b, real_t * c);
 double gbref_spdot(dim_t nnz, const dim_t * ind, const real_t * val, const real_t * x);
 int gbref_cgd(dim_t n, ind_t * rowptr, dim_t * rowind, real_t * rowval,
     real_t * b, real_t * x, double error, size_t niter, size_t * iters,
@@ -100,6 +104,16 @@ int gbref_spmult(dim_t anrows, dim_t ancols, dim_t bncols,
 double gbref_dot(dim_t n, const real_t * a, const real_t * b)
 {
   return (double)blas_dot(n, a, b);
+}
+
+int gbref_add(dim_t n, const real_t * a, const real_t * b, real_t * c)
+{
+  return blas_add(n, 1, a, b, c);
+}
+
+int gbref_sub(dim_t n, const real_t * a, const real_t * b, real_t * c)
+{
+  return blas_sub(n, 1, a, b, c);
 }
 
 /* blas_spdot (src/blas.c:433-451) takes its indices as real_t values; they

@@ -18,7 +18,11 @@ Fixtures
                   id first) and permute_sparse results (src/permute.c:120-205)
   full_sizes.json checksums of the reference SpMV on the full 100k x 100k
                   uniform matrix, and the reference CG iteration count /
-                  final ||r|| on the full 1024x1024 Laplacian
+                  final ||r|| on the full 1024x1024 Laplacian; with
+                  ``--only large``: the reference SpMV checksums (both
+                  widths) on the full 8M-row power-law matrix, and the
+                  reference CG on the 160^3 3D operator (iterations, norms,
+                  and a sample of x in cg_diffusion_160_xsample.npz)
 """
 from __future__ import annotations
 
@@ -258,11 +262,59 @@ def full_sizes():
         json.dump(res, f, indent=1)
 
 
+def full_sizes_large():
+    """The power-law SpMV (8M rows, 128M nonzeros) through the reference's
+    blas_spmult, both value widths, and the reference cgd on the 160^3
+    variable-coefficient 3D operator.  Merged into full_sizes.json; a sample
+    of the reference CG solution (every (n // 65536)-th entry) goes to
+    cg_diffusion_160_xsample.npz."""
+    path = os.path.join(OUT, "full_sizes.json")
+    res = json.load(open(path)) if os.path.exists(path) else {}
+    t = time.time()
+    A = W.powerlaw_rows(8_000_000, 128_000_000, seed=3, cap=200_000)
+    x = W.dense_x(A.ncols, 3)
+    y = oracle.ref_spmm(A.rowptr, A.rowind, A.rowval, x, real="f64")
+    y32 = oracle.ref_spmm(A.rowptr, A.rowind, A.rowval.astype(np.float32),
+                          x.astype(np.float32), real="f32")
+    res["spmv_powerlaw_8m"] = {
+        "seed": 3, "n": A.nrows, "nnz": int(A.rowptr[-1]), "cap": 200_000,
+        "rowptr_sha256": hashlib.sha256(A.rowptr.tobytes()).hexdigest(),
+        "y_sha256": hashlib.sha256(y.tobytes()).hexdigest(),
+        "y32_sha256": hashlib.sha256(y32.tobytes()).hexdigest(),
+        "y_sum": float(y.sum()), "y_abs_sum": float(np.abs(y).sum()),
+    }
+    print(f"spmv powerlaw 8M: {time.time() - t:.1f}s", flush=True)
+    del A, y, y32
+    t = time.time()
+    A = W.diffusion_3d(160, seed=4)
+    b = W.rhs(A.nrows, 4)
+    bn = float(np.linalg.norm(b))
+    x, it, last = oracle.ref_cgd(A.rowptr, A.rowind, A.rowval, b, 1e-10 * bn, 50000)
+    r = b - A.to_scipy() @ x
+    step = A.nrows // 65536
+    np.savez_compressed(os.path.join(OUT, "cg_diffusion_160_xsample.npz"),
+                        step=step, x=x[::step].copy())
+    res["cg_diffusion_160"] = {
+        "seed": 4, "side": 160, "b_seed": 4, "rtol": 1e-10, "niter": 50000,
+        "iterations": it, "bnorm": bn, "last_rnorm": last,
+        "true_rel_residual": float(np.linalg.norm(r) / bn),
+        "x_norm": float(np.linalg.norm(x)), "x_sum": float(x.sum()),
+        "x_sample_step": step,
+        "omp_threads": int(os.environ.get("OMP_NUM_THREADS", "0") or 0),
+    }
+    print(f"cg 160^3: {it} iterations, {time.time() - t:.1f}s", flush=True)
+    with open(path, "w") as f:
+        json.dump(res, f, indent=1)
+
+
 if __name__ == "__main__":
     if not oracle.ref_available("f64") or not oracle.ref_available("f32"):
         sys.exit("build the reference oracle first: make -C oracle ref")
     if "--only" in sys.argv and sys.argv[sys.argv.index("--only") + 1] == "rcm":
         print("rcm:", rcm_cases())
+        sys.exit(0)
+    if "--only" in sys.argv and sys.argv[sys.argv.index("--only") + 1] == "large":
+        full_sizes_large()
         sys.exit(0)
     print("spmv:", spmv_cases())
     print("rcm:", rcm_cases())

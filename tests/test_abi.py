@@ -207,3 +207,21 @@ def test_planner_parallel_path_matches_greedy_rule():
     tiles, nlong, _ = gb.plan_tiles(A.rowptr, 2048)
     mt, mlong = _plan_model(A.rowptr, 2048)
     assert nlong == mlong and np.array_equal(tiles.astype(np.int64), mt)
+
+
+def test_planner_many_segments_match_greedy_rule():
+    """More than 32 x 32768 rows of mixed lengths: the planner cuts the rows
+    into as many segments as the host has threads (up to 32), so the stitch
+    along the true chain of tiles crosses every segment boundary."""
+    if (os.cpu_count() or 1) < 2:
+        pytest.skip("the host has one thread: the planner takes its sequential path")
+    rng = np.random.default_rng(45)
+    n = 32 * 32768 + 5000
+    L = np.where(rng.random(n) < 0.1, 0,
+        np.where(rng.random(n) < 0.001, rng.integers(2000, 9000, n),
+                 rng.integers(1, 40, n))).astype(np.int64)
+    rp = np.concatenate([[0], np.cumsum(L)]).astype(np.uint32)
+    tiles, nlong, info = gb.plan_tiles(rp, 2048)
+    mt, mlong = _plan_model(rp, 2048)
+    assert nlong == mlong and np.array_equal(tiles.astype(np.int64), mt)
+    assert info.max_row == L.max()

@@ -137,3 +137,42 @@ def test_float_abi_cgd_matches_float_reference(cg_golden):
                                     real="f32")
         assert abs(it - itr) <= 2, (it, itr)
         assert np.linalg.norm(x - xr) <= 1e-4 * np.linalg.norm(xr)
+
+
+@pytest.mark.parametrize("mode,persistent", [(gb.CG_F64, True), (gb.CG_F64, False),
+                                             (gb.CG_MIXED, False)])
+def test_cancel_before_and_during_a_solve(torch, mode, persistent):
+    """gb_cg_cancel stops a solve at its next check with status "cancelled".
+    A request made before the solve stops it at once (the persistent solve at
+    its first grid barrier, which every CTA then leaves, before x moves); a
+    request from another thread stops a solve that could not converge long
+    before its iteration limit.  The solver works normally afterwards."""
+    import threading
+    import time
+    L = W.laplacian_2d(512)
+    A = gb.CsrMatrix.from_host(L, f64=True, f32=(mode == gb.CG_MIXED))
+    b = torch.from_numpy(W.rhs(L.nrows, 5)).cuda()
+    S = gb.CgSolver(A, mode=mode, persistent=persistent)
+    # cancelled before it starts
+    S.cancel()
+    x, r = S.solve(b, tol=1e-12, niter=200_000)
+    assert r.status == "cancelled", r
+    assert r.iterations <= (0 if persistent else 128), r
+    if persistent:
+        assert torch.count_nonzero(x).item() == 0  # stopped before x moved
+    # cancelled while running: an unreachable tolerance, a long iteration limit
+    t = threading.Timer(0.3, S.cancel)
+    t0 = time.time()
+    t.start()
+    x, r = S.solve(b, tol=1e-300, relative=False, niter=2_000_000)
+    dt = time.time() - t0
+    t.join()
+    assert r.status == "cancelled", r
+    assert 0 < r.iterations < 2_000_000 and dt < 30.0, (r, dt)
+    assert np.isfinite(r.rnorm)
+    # the request was consumed: the next solve runs to convergence
+    x, r = S.solve(b, tol=1e-8, niter=20_000)
+    assert r.status == "converged", r
+    res = np.linalg.norm(b.cpu().numpy() - L.to_scipy() @ x.cpu().numpy())
+    assert res <= 2e-8 * np.linalg.norm(b.cpu().numpy())
+    S.close()

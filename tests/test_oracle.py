@@ -93,6 +93,20 @@ def test_dot_scale_add_scalar():
     assert np.array_equal(t, a - 0.5)
 
 
+@pytest.mark.skipif(not oracle.ref_available("f64"), reason="reference build absent")
+def test_reference_add_sub_known_answers():
+    """blas_add / blas_sub through the reference build equal the IEEE sums
+    and differences elementwise, also written in place over either input."""
+    a = W.dense_x(5003, 11)
+    b = W.rhs(5003, 12)
+    assert np.array_equal(oracle.ref_axpby(a, b, np.empty_like(a)), a + b)
+    assert np.array_equal(oracle.ref_axpby(a, b, np.empty_like(a), subtract=True), a - b)
+    c = b.copy()
+    assert np.array_equal(oracle.ref_axpby(a, c, c, subtract=True), a - b)
+    c = a.copy()
+    assert np.array_equal(oracle.ref_axpby(c, b, c), a + b)
+
+
 def test_spdot_restatement():
     A = W.powerlaw_rows(2000, 30000, seed=7, cap=2000)
     x = W.dense_x(2000, 7)

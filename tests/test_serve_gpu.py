@@ -103,3 +103,42 @@ def test_iteration_limit_reports_true_residual():
     r = srv.drain()[0]
     assert r.status == "maxiter" and r.iterations == 30
     assert r.rnorm == pytest.approx(_rel(A, r.x, b) * np.linalg.norm(b), rel=1e-6)
+
+
+def test_cancel_queued_and_resident_requests():
+    """gb_server_cancel drops a queued request at once and retires a resident
+    one at the next step; both are reported as "cancelled" with their x_out
+    untouched, their slot and memory go back to the pool, and the other
+    requests still converge to the same bits as alone."""
+    reqs = _requests([120, 90, 60], 700)
+    srv = gb.Server(pool_bytes=1 << 30, max_slots=2, mode=gb.CG_MIXED, iters_per_step=4)
+    outs = {}
+    for rid, A, b in reqs:
+        outs[rid] = np.full(A.nrows, 7.0)
+        srv.submit(rid, A, b, tol=1e-10, niter=20000, x_out=outs[rid])
+    active, queued = srv.step()
+    assert active == 2 and queued == 1
+    srv.cancel(2)  # still queued
+    srv.cancel(0)  # resident
+    with pytest.raises(gb.GooseberryError):
+        srv.cancel(77)
+    res = {r.id: r for r in srv.drain()}
+    assert sorted(res) == [0, 1, 2]
+    for rid in (0, 2):
+        assert res[rid].status == "cancelled", res[rid]
+        assert np.all(outs[rid] == 7.0)
+    assert res[2].iterations == 0
+    assert res[1].status == "converged"
+    rid, A, b = reqs[1]
+    alone = gb.Server(pool_bytes=1 << 30, max_slots=1, mode=gb.CG_MIXED, iters_per_step=4)
+    alone.submit(rid, A, b, tol=1e-10, niter=20000)
+    r1 = alone.drain()[0]
+    assert r1.iterations == res[1].iterations and np.array_equal(r1.x, res[1].x)
+    with pytest.raises(gb.GooseberryError):
+        srv.cancel(1)  # already finished
+    # the freed slot and memory take new work
+    srv.submit(9, A, b, tol=1e-10, niter=20000)
+    r9 = srv.drain()[0]
+    assert r9.status == "converged" and np.array_equal(r9.x, res[1].x)
+    srv.close()
+    alone.close()

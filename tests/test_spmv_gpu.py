@@ -20,7 +20,7 @@ pytestmark = pytest.mark.gpu
 TOL64 = 1e-13
 TOL32 = 64 * 2.0 ** -24
 SCHEDS = [gb.SCHED_THREAD, gb.SCHED_GROUP4, gb.SCHED_GROUP8, gb.SCHED_WARP, gb.SCHED_MERGE,
-          gb.SCHED_ROW, gb.SCHED_WTILE, gb.SCHED_WMERGE]
+          gb.SCHED_ROW, gb.SCHED_WTILE, gb.SCHED_WMERGE, gb.SCHED_SEG]
 
 
 def _tile_for(sched, tile):
@@ -161,16 +161,85 @@ def test_powerlaw_long_rows(torch):
     assert M.info().nlong > 0
     xd = _dev(torch, x)
     for s, t in ((gb.SCHED_MERGE, 2048), (gb.SCHED_GROUP8, 2048), (gb.SCHED_THREAD, 2048),
-                 (gb.SCHED_WTILE, 256), (gb.SCHED_WMERGE, 128), (gb.SCHED_WMERGE, 64)):
+                 (gb.SCHED_WTILE, 256), (gb.SCHED_WMERGE, 128), (gb.SCHED_WMERGE, 64),
+                 (gb.SCHED_SEG, 2048)):
         M.set_schedule(s, tile_items=t)
         y = M.spmv(xd).cpu().numpy()
         assert cond_scaled_err(y, y_ref, A.rowptr, A.rowind, A.rowval, x) <= TOL64, s
         assert np.array_equal(y, M.spmv(xd).cpu().numpy())
     y32_ref = oracle.spmv(A.rowptr, A.rowind, A.rowval.astype(np.float32),
                           x.astype(np.float32), threads=8, real="f32")
+    for s in (gb.SCHED_MERGE, gb.SCHED_SEG):
+        M.set_schedule(s, f32=True)
+        y32 = M.spmv(_dev(torch, x.astype(np.float32))).cpu().numpy()
+        assert cond_scaled_err(y32, y32_ref, A.rowptr, A.rowind, A.rowval.astype(np.float32),
+                               x.astype(np.float32)) <= TOL32, s
+
+
+def _lens_csr(lens, ncols, seed):
+    """A CSR matrix with the given row lengths, uniform columns and values."""
+    rng = np.random.default_rng(seed)
+    lens = np.asarray(lens, dtype=np.int64)
+    rowptr = np.concatenate([[0], np.cumsum(lens)]).astype(np.uint32)
+    nnz = int(rowptr[-1])
+    rowind = rng.integers(0, ncols, nnz).astype(np.uint32)
+    rowval = rng.uniform(-1, 1, nnz)
+    return rowptr, rowind, rowval
+
+
+@pytest.mark.parametrize("case", ["empty_runs", "one_huge_row", "huge_rows_between_empties",
+                                  "trailing_empties", "leading_empties", "ragged_pareto",
+                                  "tiny"])
+def test_segmented_schedule_edge_cases(torch, case):
+    """The SEG schedule cuts nonzeros into per-warp ranges wherever the
+    merge-path split lands: rows that cross ranges (and runs of empty rows at
+    range starts, or after the last nonzero) must come out once and right,
+    and bitwise the same on every run (the cross-range sums go in warp order)."""
+    rng = np.random.default_rng(7)
+    lens = {
+        "empty_runs": [0] * 3000 + [5] * 20_000 + [0] * 7000 + [3] * 9000 + [0] * 100,
+        "one_huge_row": [300_000],
+        "huge_rows_between_empties": [0, 150_000, 0, 0, 70_001, 1, 0, 90_003, 0],
+        "trailing_empties": [7] * 50_000 + [0] * 40_000,
+        "leading_empties": [0] * 40_000 + [9] * 50_000,
+        "ragged_pareto": list((rng.pareto(1.1, 200_000) * 3).astype(int)),
+        "tiny": [1, 0, 2],
+    }[case]
+    ncols = 50_000
+    rp, ri, rv = _lens_csr(lens, ncols, seed=len(lens))
+    x = W.dense_x(ncols, 3)
+    y_ref = oracle.spmv(rp, ri, rv, x, threads=8)
+    M = gb.CsrMatrix.from_host(rowptr=rp, rowind=ri, rowval=rv, ncols=ncols, f64=True, f32=True)
+    M.set_schedule(gb.SCHED_SEG)
+    M.set_schedule(gb.SCHED_SEG, f32=True)
+    xd = _dev(torch, x)
+    y = M.spmv(xd).cpu().numpy()
+    assert cond_scaled_err(y, y_ref, rp, ri, rv, x) <= TOL64
+    for _ in range(3):
+        assert np.array_equal(y, M.spmv(xd).cpu().numpy())
+    y32_ref = oracle.spmv(rp, ri, rv.astype(np.float32), x.astype(np.float32), threads=8,
+                          real="f32")
     y32 = M.spmv(_dev(torch, x.astype(np.float32))).cpu().numpy()
-    assert cond_scaled_err(y32, y32_ref, A.rowptr, A.rowind, A.rowval.astype(np.float32),
+    assert cond_scaled_err(y32, y32_ref, rp, ri, rv.astype(np.float32),
                            x.astype(np.float32)) <= TOL32
+
+
+def test_segmented_schedule_needs_aligned_arrays(torch):
+    """Borrowed device arrays that do not start on a 16-byte boundary cannot
+    take the SEG schedule's 16-byte loads: choosing it is refused."""
+    A = W.uniform_rows(3000, 7, seed=41)
+    rp = _dev(torch, A.rowptr.view(np.int32))
+    ri = _dev(torch, np.concatenate([[0], A.rowind]).view(np.int32))[1:]
+    v = _dev(torch, A.rowval)
+    M = gb.CsrMatrix.from_device(rp, ri, val64=v)
+    with pytest.raises(gb.GooseberryError) as e:
+        M.set_schedule(gb.SCHED_SEG)
+    assert e.value.code == 3 and "16-byte" in str(e.value)
+    M.set_schedule(gb.SCHED_MERGE)
+    x = W.dense_x(3000, 41)
+    y = M.spmv(_dev(torch, x)).cpu().numpy()
+    y_ref = oracle.spmv(A.rowptr, A.rowind, A.rowval, x)
+    assert cond_scaled_err(y, y_ref, A.rowptr, A.rowind, A.rowval, x) <= TOL64
 
 
 def test_device_pointer_matrix(torch):
@@ -190,8 +259,10 @@ def test_empty_and_degenerate(torch):
     rp = np.zeros(101, np.uint32)
     M = gb.CsrMatrix.from_host(rowptr=rp, rowind=np.zeros(0, np.uint32),
                                rowval=np.zeros(0), ncols=100)
-    y = M.spmv(torch.ones(100, dtype=torch.float64, device="cuda"))
-    assert torch.count_nonzero(y).item() == 0
+    for s in (gb.SCHED_AUTO, gb.SCHED_SEG):
+        M.set_schedule(s)
+        y = M.spmv(torch.ones(100, dtype=torch.float64, device="cuda"))
+        assert torch.count_nonzero(y).item() == 0
     # zero rows: nothing to do
     y = gb.spmult(np.zeros(1, np.uint32), np.zeros(0, np.uint32), np.zeros(0), np.zeros(4),
                   ncols=4)
@@ -222,6 +293,34 @@ def test_blas1_device(torch):
     w = np.arange(10, dtype=np.float32)
     gb.scale(w, 0.5)
     assert np.array_equal(w, np.arange(10, dtype=np.float32) * np.float32(0.5))
+
+
+@pytest.mark.skipif(not oracle.ref_available("f64"), reason="reference build missing")
+def test_add_sub_match_reference_bitwise(torch):
+    """gb_add_f64 / gb_sub_f64 against the reference's own blas_add / blas_sub
+    (src/blas.c:275-290,321-336) on the same vectors, bit for bit, including
+    the aliased forms cgd uses (c = b at src/cgd.c:105, and c = a)."""
+    n = 1_000_003
+    a = W.dense_x(n, 61)
+    b = W.rhs(n, 62) * 1e3
+    for subtract in (False, True):
+        fn = gb.sub if subtract else gb.add
+        ref = oracle.ref_axpby(a, b, np.empty(n), subtract=subtract)
+        got = fn(_dev(torch, a), _dev(torch, b)).cpu().numpy()
+        assert np.array_equal(got, ref), subtract
+        # c aliases b, then a
+        bb = b.copy()
+        oracle.ref_axpby(a, bb, bb, subtract=subtract)
+        bd = _dev(torch, b)
+        fn(_dev(torch, a), bd, out=bd)
+        assert np.array_equal(bd.cpu().numpy(), bb), ("c = b", subtract)
+        aa = a.copy()
+        oracle.ref_axpby(aa, b, aa, subtract=subtract)
+        ad = _dev(torch, a)
+        fn(ad, _dev(torch, b), out=ad)
+        assert np.array_equal(ad.cpu().numpy(), aa), ("c = a", subtract)
+    e = torch.empty(0, dtype=torch.float64, device="cuda")
+    assert gb.add(e, e).numel() == 0
 
 
 def test_spdot_matches_oracle(torch):
