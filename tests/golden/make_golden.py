@@ -289,7 +289,17 @@ def full_sizes_large():
     A = W.diffusion_3d(160, seed=4)
     b = W.rhs(A.nrows, 4)
     bn = float(np.linalg.norm(b))
-    x, it, last = oracle.ref_cgd(A.rowptr, A.rowind, A.rowval, b, 1e-10 * bn, 50000)
+    # the reference's dot products reduce in OpenMP thread order, so on this
+    # ill-conditioned system its iteration count depends on the thread count:
+    # record the range over 1, 2, 4 and 8 threads (the golden x is the 8-thread one)
+    by_threads, xs = {}, {}
+    for nt in (1, 2, 4, 8):
+        oracle.ref_set_threads(nt)
+        xs[nt], by_threads[str(nt)], last = oracle.ref_cgd(A.rowptr, A.rowind, A.rowval, b,
+                                                           1e-10 * bn, 50000)
+    x, it = xs[8], by_threads["8"]
+    spread = max(float(np.linalg.norm(xs[p] - xs[q]) / np.linalg.norm(xs[q]))
+                 for p in xs for q in xs if p < q)
     r = b - A.to_scipy() @ x
     step = A.nrows // 65536
     np.savez_compressed(os.path.join(OUT, "cg_diffusion_160_xsample.npz"),
@@ -300,7 +310,13 @@ def full_sizes_large():
         "true_rel_residual": float(np.linalg.norm(r) / bn),
         "x_norm": float(np.linalg.norm(x)), "x_sum": float(x.sum()),
         "x_sample_step": step,
-        "omp_threads": int(os.environ.get("OMP_NUM_THREADS", "0") or 0),
+        "omp_threads": 8,
+        "reference_iterations_by_threads": by_threads,
+        "reference_iterations_range": [min(by_threads.values()), max(by_threads.values())],
+        "reference_solution_spread": spread,
+        # a solve that stops at rel-res 1e-10 on this operator can sit this far
+        # from another that does (mixed precision takes a different path there)
+        "solution_tolerance": 1e-8,
     }
     print(f"cg 160^3: {it} iterations, {time.time() - t:.1f}s", flush=True)
     with open(path, "w") as f:

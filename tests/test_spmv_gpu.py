@@ -229,7 +229,7 @@ def test_segmented_schedule_needs_aligned_arrays(torch):
     take the SEG schedule's 16-byte loads: choosing it is refused."""
     A = W.uniform_rows(3000, 7, seed=41)
     rp = _dev(torch, A.rowptr.view(np.int32))
-    ri = _dev(torch, np.concatenate([[0], A.rowind]).view(np.int32))[1:]
+    ri = _dev(torch, np.concatenate([np.zeros(1, np.uint32), A.rowind]).view(np.int32))[1:]
     v = _dev(torch, A.rowval)
     M = gb.CsrMatrix.from_device(rp, ri, val64=v)
     with pytest.raises(gb.GooseberryError) as e:
