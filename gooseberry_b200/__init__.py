@@ -56,7 +56,8 @@ SCHED_NAMES = {0: "auto", 1: "thread", 2: "group4", 3: "group8", 4: "warp", 5: "
 CG_F64, CG_MIXED = 0, 1
 CG_PERSISTENT = 0x100
 CG_PLAIN_ENTRIES = 0x200
-CG_STATUS = {0: "converged", 1: "maxiter", 2: "breakdown", 3: "nonfinite", 4: "cancelled"}
+CG_STATUS = {0: "converged", 1: "maxiter", 2: "breakdown", 3: "nonfinite", 4: "cancelled",
+             5: "timeout"}
 
 
 class GooseberryError(RuntimeError):
@@ -141,6 +142,7 @@ SIGNATURES = {
     "gb_cg_profile": (_i, [_vp, _vp, _sz, _vp, _sz, _vp, _vp]),
     "gb_cg_entry_bytes": (_i, [_vp, _vp]),
     "gb_cg_cancel": (_i, [_vp]),
+    "gb_cg_set_barrier_fault": (_i, [_vp, C.c_int, C.c_uint]),
     "gb_server_cancel": (_i, [_vp, C.c_uint64]),
     "gb_server_create": (_i, [_vp, _vp]),
     "gb_server_destroy": (_i, [_vp]),
@@ -673,6 +675,14 @@ class CgSolver:
         """Stop the solve running on another thread (``gb_cg_cancel``); with
         no solve running, the next solve stops at its first check."""
         _check(lib().gb_cg_cancel(self._h), "gb_cg_cancel")
+
+    def set_barrier_fault(self, drop_cta: int = -1, limit_ms: int = 0):
+        """Failure-path hook of a persistent solver (``gb_cg_set_barrier_fault``):
+        CTA ``drop_cta`` skips the first grid barrier of the following solves,
+        which then give up after ``limit_ms`` (0: the 2 s default) and raise
+        (status "timeout"); ``drop_cta < 0`` turns it off."""
+        _check(lib().gb_cg_set_barrier_fault(self._h, int(drop_cta), int(limit_ms)),
+               "gb_cg_set_barrier_fault")
 
     def entry_bytes(self) -> int:
         """Bytes per matrix entry the solver's SpMV streams (12 = plain CSR)."""

@@ -501,8 +501,9 @@ int occupancy_cg_a_sched(int sched, size_t smem, int * out) {
 //   barrier  every CTA sums r.r, forms beta and takes the same stop decision
 // Vectors that other CTAs write during the launch (r, p) are read through L2
 // (ld.global.cg), never the read-only path.  Barriers wait on a global
-// counter with a 2 s limit; on time-out the CTA raises `abort`, every waiting
-// CTA leaves, and the solve reports GB_CG_NONFINITE with rnorm = NaN.
+// counter with a limit (2 s unless a test sets one); on time-out the CTA
+// raises `abort`, every waiting CTA leaves, and the solve reports
+// GB_CG_TIMEOUT with rnorm = NaN.
 
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;
 // Values of the abort flag: a barrier timed out, or the host cancelled.
@@ -535,9 +536,12 @@ __device__ __forceinline__ double ld_cg(const double * p, uint64_t pol) {
 }
 
 // Grid barrier number `epoch` (1, 2, ...): returns false if it was abandoned.
+// A CTA told to skip (`skip`, the failure-path test) does not arrive and
+// leaves as if the barrier had been abandoned.
 __device__ __forceinline__ bool grid_barrier(unsigned * counter, int * abort_flag,
-    unsigned epoch, int * ok_smem) {
+    unsigned epoch, int * ok_smem, unsigned long long limit_ns, bool skip = false) {
   __syncthreads();
+  if (skip) return false;
   if (threadIdx.x == 0) {
     __threadfence();
     atomicAdd(counter, 1u);
@@ -549,7 +553,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned * counter, int * abort_fla
       if (*reinterpret_cast<volatile int *>(abort_flag)) { ok = 0; break; }
       if (++polls > 64) {
         __nanosleep(64);
-        if (global_ns() - t0 > kBarrierTimeoutNs) {
+        if (global_ns() - t0 > limit_ns) {
           atomicExch(abort_flag, kAbortTimeout);
           ok = 0;
           break;
@@ -638,6 +642,8 @@ struct PersistArgs {
   CgState * st;
   int tol_relative;
   int keep_matrix_in_l2;
+  int drop_cta;                       // failure-path test: this CTA skips barrier 1
+  unsigned long long barrier_limit_ns;
 };
 
 template <int SCHED>
@@ -681,7 +687,9 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_persis
   unsigned long long it = 0;
   double rr = 0.0, bnorm = 0.0, tol = tol_in, beta = 0.0;
   bool aborted = false;
-  if (!grid_barrier(a.sync, a.abort_flag, ++epoch, &ok_smem)) {
+  const unsigned long long lim = a.barrier_limit_ns;
+  if (!grid_barrier(a.sync, a.abort_flag, ++epoch, &ok_smem, lim,
+                    static_cast<int>(cta) == a.drop_cta)) {
     aborted = true;
   } else {
     rr = ordered_allsum(a.partial_b, G, red, &bcast);
@@ -709,7 +717,7 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_persis
       if (tid == 0) a.partial_a[cta] = s;
       // a cancel stops the solve before x moves, so x matches `it`
       if (cta == 0 && tid == 0 && cancel_req) atomicExch(a.abort_flag, kAbortCancel);
-      if (!grid_barrier(a.sync, a.abort_flag, ++epoch, &ok_smem)) { aborted = true; break; }
+      if (!grid_barrier(a.sync, a.abort_flag, ++epoch, &ok_smem, lim)) { aborted = true; break; }
       if (cta == 0 && tid == 0) cancel_req = ld_host_flag(a.cancel);
       const double pap = ordered_allsum(a.partial_a, G, red, &bcast);
       if (!(pap > 0.0)) {
@@ -745,7 +753,7 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_persis
       }
       s = block_sum(acc, red);
       if (tid == 0) a.partial_b[cta] = s;
-      if (!grid_barrier(a.sync, a.abort_flag, ++epoch, &ok_smem)) { aborted = true; break; }
+      if (!grid_barrier(a.sync, a.abort_flag, ++epoch, &ok_smem, lim)) { aborted = true; break; }
       const double rr_new = ordered_allsum(a.partial_b, G, red, &bcast);
       beta = rr_new / rr;
       rr = rr_new;
@@ -765,7 +773,9 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_persis
     st->rr = aborted && !cancelled ? __longlong_as_double(0x7ff8000000000000ll) : rr;
     st->bnorm = bnorm;
     st->tol = tol;
-    st->status = cancelled ? GB_CG_CANCELLED : (aborted ? GB_CG_NONFINITE : status);
+    // an abort that is not a cancel is a barrier that timed out (CTA 0 may be
+    // the CTA that left without arriving: it reports the same)
+    st->status = cancelled ? GB_CG_CANCELLED : (aborted ? GB_CG_TIMEOUT : status);
     st->done = 1;
   }
 }
@@ -828,6 +838,8 @@ struct gb_cg {
   unsigned * sync = nullptr;  // [0] barrier counter, [1] abort flag
   int * cancel_h = nullptr;   // pinned, mapped: set by gb_cg_cancel
   int * cancel_d = nullptr;   // its device address
+  int drop_cta = -1;          // gb_cg_set_barrier_fault
+  unsigned long long barrier_limit_ns = gb::kBarrierTimeoutNs;
   int keep_l2 = 0;
   bool l2_hint = false;  // A kernel with L2-policy loads (working set fits in L2)
   bool use_codec = false;  // row schedule over compressed entries
@@ -995,6 +1007,8 @@ int launch_persistent(gb_cg * s, const double * b, int tol_relative, cudaStream_
   args.st = s->st;
   args.tol_relative = tol_relative;
   args.keep_matrix_in_l2 = s->keep_l2;
+  args.drop_cta = s->drop_cta;
+  args.barrier_limit_ns = s->barrier_limit_ns;
   void * kargs[] = {&args};
   GB_CUDA_TRY(cudaLaunchCooperativeKernel(s->fn_p, dim3(s->grid_p), dim3(kSpmvBlock), kargs,
       s->smem_p, stream));
@@ -1191,16 +1205,21 @@ int solve_cg(gb_cg * s, const double * b, double * x, double tol, int tol_relati
     if (e != cudaSuccess) {
       set_error("CG result copy failed: %s", cudaGetErrorString(e));
       rc = GOOSEBERRY_ERROR_UNKNOWN;
-    } else if (flags[1] == kAbortTimeout) {
-      set_error("CG solve abandoned: a grid barrier timed out");
-      rc = GOOSEBERRY_ERROR_UNKNOWN;
-    } else if (res) {
-      res->iterations = fin.iter;
-      res->refinements = 0;
-      res->rnorm = std::sqrt(fin.rr);
-      res->bnorm = fin.bnorm;
-      res->status = fin.status;
-      res->kernel_launches = launches;
+    } else {
+      if (flags[1] == kAbortTimeout || fin.status == GB_CG_TIMEOUT) {
+        // the device is fine (every wait has a limit); the solve is not
+        set_error("CG solve abandoned: a grid barrier timed out");
+        rc = GOOSEBERRY_ERROR_UNKNOWN;
+        fin.status = GB_CG_TIMEOUT;
+      }
+      if (res) {
+        res->iterations = fin.iter;
+        res->refinements = 0;
+        res->rnorm = std::sqrt(fin.rr);
+        res->bnorm = fin.bnorm;
+        res->status = fin.status;
+        res->kernel_launches = launches;
+      }
     }
   }
   if (dhist) scratch_free(dhist, stream);
@@ -1300,6 +1319,18 @@ int gb_cg_solve(gb_cg_t * s, const double * b, double * x, double tol, int tol_r
 int gb_cg_cancel(gb_cg_t * s) {
   GB_CHECK_INPUT(s != nullptr, "solver is NULL");
   __atomic_store_n(s->cancel_h, 1, __ATOMIC_RELEASE);
+  return GOOSEBERRY_SUCCESS;
+}
+
+int gb_cg_set_barrier_fault(gb_cg_t * s, int drop_cta, unsigned limit_ms) {
+  GB_CHECK_INPUT(s != nullptr, "solver is NULL");
+  GB_CHECK_INPUT(drop_cta < 0 || s->persistent,
+      "the barrier fault applies to GB_CG_PERSISTENT solvers only");
+  GB_CHECK_INPUT(drop_cta < 0 || static_cast<unsigned>(drop_cta) < s->grid_p,
+      "drop_cta %d is not a CTA of the %u-CTA solve", drop_cta, s->grid_p);
+  s->drop_cta = drop_cta < 0 ? -1 : drop_cta;
+  s->barrier_limit_ns = limit_ms ? static_cast<unsigned long long>(limit_ms) * 1000000ull
+                                 : gb::kBarrierTimeoutNs;
   return GOOSEBERRY_SUCCESS;
 }
 

@@ -278,8 +278,13 @@ typedef enum gb_cg_status {
   GB_CG_MAXITER = 1,    /* iteration limit reached first                      */
   GB_CG_BREAKDOWN = 2,  /* p.Ap <= 0: matrix not SPD                          */
   GB_CG_NONFINITE = 3,  /* NaN or Inf appeared                                */
-  GB_CG_CANCELLED = 4   /* stopped by gb_cg_cancel / gb_server_cancel; x is
+  GB_CG_CANCELLED = 4,  /* stopped by gb_cg_cancel / gb_server_cancel; x is
                            the iterate of the last finished iteration        */
+  GB_CG_TIMEOUT = 5     /* a GB_CG_PERSISTENT solve gave up at a grid barrier
+                           that not every CTA reached within the limit (2 s
+                           unless set by gb_cg_set_barrier_fault); the call
+                           returns GOOSEBERRY_ERROR_UNKNOWN with this status
+                           in the result, rnorm NaN; x is not meaningful     */
 } gb_cg_status_t;
 
 typedef struct gb_cg_result {
@@ -319,6 +324,15 @@ GOOSEBERRY_API int gb_cg_solve(gb_cg_t * s, const double * b, double * x, double
  * stopped on a request clears it.  The reference's cgd cannot be stopped
  * (src/cgd.c:87-119); no counterpart. */
 GOOSEBERRY_API int gb_cg_cancel(gb_cg_t * s);
+
+/* Failure-path hook for GB_CG_PERSISTENT solves, for tests of the bounded
+ * grid barrier: from the next gb_cg_solve on, CTA `drop_cta` (>= 0) does not
+ * arrive at the solve's first grid barrier and leaves, so the other CTAs
+ * wait out the barrier limit, raise the abort flag and leave too; the solve
+ * returns GOOSEBERRY_ERROR_UNKNOWN with status GB_CG_TIMEOUT.  `limit_ms` sets the barrier limit (0 keeps 2000);
+ * drop_cta < 0 turns the fault off.  Nothing waits without a limit, so the
+ * device stays usable.  No reference counterpart (cgd runs on the host). */
+GOOSEBERRY_API int gb_cg_set_barrier_fault(gb_cg_t * s, int drop_cta, unsigned limit_ms);
 
 /*
  * Measurement hook: start a solve of A x = b and run its first `iterations`

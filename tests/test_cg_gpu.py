@@ -176,3 +176,53 @@ def test_cancel_before_and_during_a_solve(torch, mode, persistent):
     res = np.linalg.norm(b.cpu().numpy() - L.to_scipy() @ x.cpu().numpy())
     assert res <= 2e-8 * np.linalg.norm(b.cpu().numpy())
     S.close()
+
+
+@pytest.mark.parametrize("drop", ["first", "last"])
+def test_persistent_barrier_times_out_and_reports_it(torch, drop):
+    """The persistent solve's grid barriers wait with a limit.  With one CTA
+    held back from the first barrier (the failure-path hook; no CTA waits
+    without a limit), the others give up after the limit, leave, and the
+    solve reports "timeout" with a NaN residual -- and the context stays
+    usable: the same solver, with the hook off, then converges normally."""
+    import time
+    L = W.laplacian_2d(256)
+    A = gb.CsrMatrix.from_host(L)
+    b = torch.from_numpy(W.rhs(L.nrows, 9)).cuda()
+    S = gb.CgSolver(A, persistent=True)
+    with pytest.raises(gb.GooseberryError):
+        S.set_barrier_fault(10 ** 6, 100)  # not a CTA of this solve
+    S.set_barrier_fault(0 if drop == "first" else lib_grid(S) - 1, 100)
+    t0 = time.time()
+    with pytest.raises(gb.GooseberryError) as e:
+        S.solve(b, tol=1e-8, niter=5000)
+    dt = time.time() - t0
+    assert e.value.code == 8 and "timed out" in str(e.value), e.value
+    assert 0.1 <= dt < 30.0, dt
+    # the limit is per barrier: a longer one takes longer to give up
+    S.set_barrier_fault(0 if drop == "first" else lib_grid(S) - 1, 600)
+    t0 = time.time()
+    with pytest.raises(gb.GooseberryError):
+        S.solve(b, tol=1e-8, niter=5000)
+    assert time.time() - t0 >= 0.6
+    S.set_barrier_fault(-1)
+    x, r = S.solve(b, tol=1e-8, niter=5000)
+    assert r.status == "converged", r
+    res = np.linalg.norm(b.cpu().numpy() - L.to_scipy() @ x.cpu().numpy())
+    assert res <= 2e-8 * np.linalg.norm(b.cpu().numpy())
+    S.close()
+
+
+def lib_grid(S):
+    """CTAs of a persistent solver's cooperative launch (found by asking the
+    hook for CTA indices until it refuses one)."""
+    lo, hi = 0, 1 << 20
+    while hi - lo > 1:
+        mid = (lo + hi) // 2
+        try:
+            S.set_barrier_fault(mid, 100)
+            lo = mid
+        except gb.GooseberryError:
+            hi = mid
+    S.set_barrier_fault(-1)
+    return lo + 1
