@@ -248,7 +248,7 @@ def run_cg_laplace(args, dist: Dist):
     # values: entry_bytes = 3 instead of 12), reported beside it
     entry_bytes = S.entry_bytes()
     bytes_a = 4 * (n + 1) + 12 * nnz + 32 * n
-    bytes_a_stored = 4 * (n + 1) + entry_bytes * nnz + 32 * n
+    bytes_a_stored = S.row_bytes() * (n + 1) + entry_bytes * nnz + 32 * n
     bytes_b = 48 * n                             # x, p, r, Ap read; x, r written
     bytes_textbook = 4 * (n + 1) + 12 * nnz + 14 * 8 * n
 
@@ -334,6 +334,12 @@ def run_cg_laplace(args, dist: Dist):
             "bytes_per_launch": bytes_a, "launch_ms": ms_a, "peak_source": peak_src,
             "bytes_per_launch_stored": bytes_a_stored,
             "achieved_stored": ach_a_stored, "frac_stored": ach_a_stored / peak,
+            # one iteration's working set (stored matrix + vectors) fits in
+            # the 126 MB L2, which the solve keeps it in (evict-last hints):
+            # the kernel's bytes mostly come from L2, not HBM
+            "l2_resident": bool(bytes_a_stored + 16 * n <= 126e6),
+            "frac_textbook_per_step": (bytes_textbook * iters * args.steps / t_local / 1e9)
+                                      / peak,
         },
         "kernels": {
             "cg_a_ms": ms_a, "cg_b_ms": ms_b,
@@ -466,6 +472,7 @@ def spmv_extra(name, A, x, peak, flush, rows_check=200_000):
         floor = measure_spdot(A, x, f32=f32, flush=flush)
         out["f32" if f32 else "f64"] = {
             "ms": ms, "GB/s": gbs, "frac_of_peak": gbs / peak, "bytes": b, **info,
+            "working_set_fits_l2": bool(b <= 126e6), "l2": "flushed before every rep",
             "max_cond_err_vs_fp64_reference_first_rows": _cond_err(y[:k], y_ref, sub, x),
             "stream_gather_floor_ms": floor, "frac_of_floor": floor / ms,
         }
@@ -594,21 +601,48 @@ def cpu_spmv_sample(A, x, nbytes, budget_s=10.0):
                                       "sample": f"{reps} full SpMVs in {dt:.1f} s"}, y
 
 
-def mixed_extra(side=160, rtol=1e-10, reps=2):
+def _reference_cg_solution(side):
+    """The reference cgd's solution on the 160^3 operator (every step-th entry)
+    and its golden record, from tests/golden (made by running the reference's
+    own build); None for other sizes."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden")
+    try:
+        with open(os.path.join(path, "full_sizes.json")) as f:
+            g = json.load(f)["cg_diffusion_160"]
+        xs = np.load(os.path.join(path, "cg_diffusion_160_xsample.npz"))
+    except (OSError, KeyError):
+        return None
+    if g["side"] != side:
+        return None
+    return g, int(xs["step"]), xs["x"]
+
+
+def mixed_extra(side=160, rtol=1e-10, reps=2, peak=None):
     """Mixed-precision CG (FP32 inner, FP64 refinement) against plain FP64 CG
     on the 3D 7-point variable-coefficient operator (160^3, coefficients
-    log-uniform in [1e-2, 1e2]); errors are true FP64 residuals on the host."""
+    log-uniform in [1e-2, 1e2]); errors are true FP64 residuals on the host
+    and distances to the reference cgd's solution (tests/golden).  Per-kernel
+    device times come from the solver's profiler (launch by launch, CUDA
+    events); the FP64 solver's SpMV kernel gets a roofline block: its bytes in
+    CSR terms (4(n+1) + 12 nnz + 32 n: rowptr, entries, r and p gathered once,
+    p and Ap written) and in the bytes it stores per entry."""
     import torch
 
     import gooseberry_b200 as gb
     from gooseberry_b200 import workloads as W
     A = W.diffusion_3d(side, seed=4)
     b = W.rhs(A.nrows, 4)
+    n, nnz = A.nrows, A.nnz
     M = gb.CsrMatrix.from_host(A, f64=True, f32=True)
     bd = torch.from_numpy(b).cuda()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     S_ = A.to_scipy()
-    out = {"n": A.nrows, "nnz": A.nnz, "rtol": rtol}
+    ref = _reference_cg_solution(side)
+    out = {"n": n, "nnz": nnz, "rtol": rtol,
+           "l2": "flushed before each timed solve (256 MB write)"}
+    if ref is not None:
+        out["reference"] = {"iterations_by_omp_threads": ref[0]["reference_iterations_by_threads"],
+                            "solution": f"every {ref[1]}-th entry of the reference cgd's x"}
     for name, mode in (("f64", gb.CG_F64), ("mixed", gb.CG_MIXED)):
         S = gb.CgSolver(M, mode=mode)
         x, r = S.solve(bd, tol=rtol, niter=50000)
@@ -622,37 +656,83 @@ def mixed_extra(side=160, rtol=1e-10, reps=2):
             e1.record()
             torch.cuda.synchronize()
             ts.append(e0.elapsed_time(e1))
-        rel = float(np.linalg.norm(b - S_ @ x.cpu().numpy()) / np.linalg.norm(b))
-        out[name] = {"ms": min(ts), "solves_per_s": 1e3 / min(ts), "iterations": r.iterations,
-                     "refinements": r.refinements, "status": r.status,
-                     "true_rel_residual": rel, "schedule": gb.SCHED_NAMES[
-                         M.info().schedule_f32 if mode == gb.CG_MIXED else M.info().schedule]}
+        xh = x.cpu().numpy()
+        rel = float(np.linalg.norm(b - S_ @ xh) / np.linalg.norm(b))
+        prof = S.profile(bd, iterations=20)
+        names = (["spmv_direction_pap", "x_r_update_rr"] if mode == gb.CG_F64 else
+                 ["spmv32_direction_pap", "y_r_update_rr", "fp64_residual_of_a_refinement"])
+        d = {"ms": min(ts), "solves_per_s": 1e3 / min(ts), "iterations": r.iterations,
+             "refinements": r.refinements, "status": r.status, "true_rel_residual": rel,
+             "us_per_iteration": 1e3 * min(ts) / max(r.iterations, 1),
+             "kernels_us": {k: 1e3 * v for k, v in zip(names, prof)},
+             "kernel_launches": r.kernel_launches,
+             "entry_bytes": S.entry_bytes(), "row_bytes": S.row_bytes(),
+             "schedule": gb.SCHED_NAMES[
+                 M.info().schedule_f32 if mode == gb.CG_MIXED else M.info().schedule]}
+        if ref is not None:
+            d["rel_err_vs_reference_solution"] = float(
+                np.linalg.norm(xh[::ref[1]] - ref[2]) / np.linalg.norm(ref[2]))
         if mode == gb.CG_F64:
-            out["f64"]["x"] = None
-            x64 = x.cpu().numpy()
+            x64 = xh
+            if peak:
+                eb, rb = S.entry_bytes(), S.row_bytes()
+                a_ms = prof[0]
+                bytes_csr = 4 * (n + 1) + 12 * nnz + 32 * n
+                bytes_stored = rb * (n + 1) + eb * nnz + 32 * n
+                d["roofline"] = {
+                    "bound": "hbm", "kernel": "cg_a_codec_kernel (FP64 SpMV + p update + p.Ap)",
+                    "launch_ms": a_ms, "bytes_per_launch": bytes_csr,
+                    "achieved": bytes_csr / (a_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                    "frac": bytes_csr / (a_ms * 1e-3) / 1e9 / peak,
+                    "bytes_per_launch_stored": bytes_stored,
+                    "frac_stored": bytes_stored / (a_ms * 1e-3) / 1e9 / peak,
+                    "l2_resident": False}
         else:
-            out["mixed"]["rel_diff_to_fp64_solution"] = float(
-                np.linalg.norm(x.cpu().numpy() - x64) / np.linalg.norm(x64))
+            d["rel_diff_to_fp64_solution"] = float(np.linalg.norm(xh - x64) / np.linalg.norm(x64))
+        out[name] = d
         S.close()
-    out["f64"].pop("x")
     out["speedup_mixed_over_f64"] = out["f64"]["ms"] / out["mixed"]["ms"]
     return out
 
 
-def serving_extra(nreq=400, seed=5, rtol=1e-10, pool=16 << 30, slots=256, ips=16,
+def _serve_live(srv, reqs, arr, rtol, limit_s=3600.0):
+    """Drive a server in real time: request i is submitted at arr[i] seconds
+    after the start; returns the results and their latencies (arrival to
+    result, seconds, on the server's clock)."""
+    n = len(reqs)
+    c0 = srv.clock()
+    i, got = 0, []
+    t_start = time.perf_counter()
+    while len(got) < n and time.perf_counter() - t_start < limit_s:
+        now = time.perf_counter() - t_start
+        while i < n and arr[i] <= now:
+            srv.submit(i, reqs[i][1], reqs[i][2], tol=rtol)
+            i += 1
+        active, queued = srv.step()
+        got += srv.poll()
+        if active == 0 and queued == 0 and i < n:
+            time.sleep(max(0.0, min(0.01, arr[i] - (time.perf_counter() - t_start))))
+    return got, [r.t_done - c0 - arr[r.id] for r in got]
+
+
+def serving_extra(nreq=300, seed=5, rtol=1e-10, pool=16 << 30, slots=256, ips=16,
                   load=0.8):
     """Serving stream of 2D 5-point variable-coefficient SPD systems (side
     log-uniform in [32, 512], coefficients log-uniform in [0.1, 10], b in
     [-1, 1], per-request seeds), each to rel-res `rtol`.
 
-    Baseline: plain FP64 CG served one solve at a time through the drop-in
-    gooseberry_cgd_f64 (upload, solve, download per request); its latencies
-    under Poisson arrivals are the exact FIFO single-server replay of the
-    measured service times.  Ours: the continuous-batching server (mixed
-    precision, 16 GB pool), driven in real time by the same arrival times.
-    Arrival rate = `load` x the baseline's saturation throughput.  A second
-    FP64 reference point: the same server in FP64 with one slot (one solve at
-    a time without the drop-in's per-request setup), at saturation."""
+    Server arms on the same stream (16 GB pool, `ips` iterations per step):
+      mixed_batched      continuous batching, FP32 inner iterations with FP64
+                         refinement, up to `slots` solves resident;
+      fp64_batched       the same server in plain FP64 CG;
+      fp64_one_at_a_time the same server in FP64 with one slot: plain FP64 CG
+                         served one solve at a time (the benchmark's baseline).
+    Each arm: the saturated rate (every request queued at t = 0, after an
+    untimed pass that grows the server to its working size), then a live run
+    under Poisson arrivals at `load` x the one-at-a-time arm's saturated rate,
+    the same arrival times for every arm, with p50/p99 latency from arrival
+    to result.  For context, the drop-in gooseberry_cgd_f64 (upload, solve,
+    download per request) one at a time at saturation."""
     import gooseberry_b200 as gb
     from gooseberry_b200 import workloads as W
     sides = W.serving_sides(nreq, seed)
@@ -661,91 +741,67 @@ def serving_extra(nreq=400, seed=5, rtol=1e-10, pool=16 << 30, slots=256, ips=16
         rs = seed * 1_000_003 + k
         A = W.diffusion_2d(int(side), seed=rs)
         reqs.append((k, A, W.rhs(A.nrows, rs)))
-    # --- baseline: FP64, one at a time
-    svc, base_iters, base_ok = [], [], 0
-    # warm-up over every 10th request in size order: the library's memory pool
-    # and every kernel the stream uses are ready before the timed pass
-    for k, A, b in sorted(reqs, key=lambda q: q[1].nrows)[::10]:
-        gb.cgd(A.rowptr, A.rowind, A.rowval, b, rtol * float(np.linalg.norm(b)), 0)
-    for k, A, b in reqs:
-        t0 = time.perf_counter()
-        x, it, rn = gb.cgd(A.rowptr, A.rowind, A.rowval, b, rtol * float(np.linalg.norm(b)), 0)
-        svc.append(time.perf_counter() - t0)
-        base_iters.append(it)
-        base_ok += int(rn <= rtol * float(np.linalg.norm(b)) * (1 + 1e-12))
-    base_thr = nreq / sum(svc)
-    # --- ours at saturation (everything queued at t = 0).  One long-lived
-    # server in steady state: a first, untimed pass of the stream grows its
-    # pool, slot table and graphs to their working size (once per serving
-    # process), then the stream is timed
-    srv = gb.Server(pool_bytes=pool, max_slots=slots, mode=gb.CG_MIXED, iters_per_step=ips)
-    for k, A, b in reqs:
-        srv.submit(k, A, b, tol=rtol)
-    srv.drain(timeout_s=3600)
-    t0 = time.perf_counter()
-    for k, A, b in reqs:
-        srv.submit(k, A, b, tol=rtol)
-    res = srv.drain(timeout_s=3600)
-    makespan = time.perf_counter() - t0
-    sat_thr = len(res) / makespan
-    worst = 0.0
-    for r in res:
-        A, b = reqs[r.id][1], reqs[r.id][2]
-        worst = max(worst, float(np.linalg.norm(b - A.to_scipy() @ r.x) / np.linalg.norm(b)))
-    # --- a second FP64 reference point: the same server in FP64 with one slot
-    # (one solve at a time, no per-request setup), at saturation after a warm pass
-    one = gb.Server(pool_bytes=pool, max_slots=1, mode=gb.CG_F64, iters_per_step=ips)
-    for k, A, b in reqs[::10]:
-        one.submit(k, A, b, tol=rtol)
-    one.drain(timeout_s=3600)
-    t0 = time.perf_counter()
-    for k, A, b in reqs:
-        one.submit(k, A, b, tol=rtol)
-    res_one = one.drain(timeout_s=3600)
-    one_thr = len(res_one) / (time.perf_counter() - t0)
-    one.close()
-    # --- latency at load x baseline throughput
-    lam = load * base_thr
-    arr = W.poisson_arrivals(nreq, lam, seed)
-    end, base_lat = 0.0, []
-    for a, s_ in zip(arr, svc):
-        start = max(a, end)
-        end = start + s_
-        base_lat.append(end - a)
-    c0 = srv.clock()
-    i, got = 0, []
-    t_start = time.perf_counter()
-    while len(got) < nreq and time.perf_counter() - t_start < 3600:
-        now = time.perf_counter() - t_start
-        while i < nreq and arr[i] <= now:
-            srv.submit(i, reqs[i][1], reqs[i][2], tol=rtol)
-            i += 1
-        active, queued = srv.step()
-        got += srv.poll()
-        if active == 0 and queued == 0 and i < nreq:
-            time.sleep(max(0.0, min(0.01, arr[i] - (time.perf_counter() - t_start))))
-    srv.close()
-    lat = [r.t_done - c0 - arr[r.id] for r in got]
 
     def pct(v, q):
-        return float(np.percentile(np.asarray(v), q))
+        return float(np.percentile(np.asarray(v), q)) if len(v) else None
+
+    arms = {"mixed_batched": (gb.CG_MIXED, slots), "fp64_batched": (gb.CG_F64, slots),
+            "fp64_one_at_a_time": (gb.CG_F64, 1)}
+    servers, out = {}, {}
+    for name, (mode, ns) in arms.items():
+        srv = gb.Server(pool_bytes=pool, max_slots=ns, mode=mode, iters_per_step=ips)
+        warm = reqs if ns > 1 else reqs[::10]
+        for k, A, b in warm:
+            srv.submit(k, A, b, tol=rtol)
+        srv.drain(timeout_s=3600)
+        t0 = time.perf_counter()
+        for k, A, b in reqs:
+            srv.submit(k, A, b, tol=rtol)
+        res = srv.drain(timeout_s=3600)
+        makespan = time.perf_counter() - t0
+        worst = 0.0
+        for r in res:
+            A, b = reqs[r.id][1], reqs[r.id][2]
+            worst = max(worst, float(np.linalg.norm(b - A.to_scipy() @ r.x) /
+                                     np.linalg.norm(b)))
+        out[name] = {"solves_per_s_saturated": len(res) / makespan,
+                     "converged": sum(r.status == "converged" for r in res),
+                     "worst_true_rel_residual": worst,
+                     "iterations_median": float(np.median([r.iterations for r in res]))}
+        servers[name] = srv
+    lam = load * out["fp64_one_at_a_time"]["solves_per_s_saturated"]
+    arr = W.poisson_arrivals(nreq, lam, seed)
+    for name, srv in servers.items():
+        got, lat = _serve_live(srv, reqs, arr, rtol)
+        out[name].update({"p50_s": pct(lat, 50), "p99_s": pct(lat, 99),
+                          "completed_live": len(got),
+                          "converged_live": sum(r.status == "converged" for r in got)})
+        srv.close()
+    # context: the drop-in, one request at a time (upload, solve, download)
+    for k, A, b in sorted(reqs, key=lambda q: q[1].nrows)[::10]:
+        gb.cgd(A.rowptr, A.rowind, A.rowval, b, rtol * float(np.linalg.norm(b)), 0)
+    t0 = time.perf_counter()
+    ok = 0
+    for k, A, b in reqs:
+        x, it, rn = gb.cgd(A.rowptr, A.rowind, A.rowval, b, rtol * float(np.linalg.norm(b)), 0)
+        ok += int(rn <= rtol * float(np.linalg.norm(b)) * (1 + 1e-12))
+    out["fp64_dropin_one_at_a_time"] = {"solves_per_s": nreq / (time.perf_counter() - t0),
+                                        "converged": ok}
+    base = out["fp64_one_at_a_time"]["solves_per_s_saturated"]
     return {
         "requests": nreq, "rtol": rtol, "pool_bytes": pool, "slots": slots,
         "iters_per_step": ips,
         "rows_min_median_max": [int(min(sides) ** 2), int(np.median(sides) ** 2),
                                 int(max(sides) ** 2)],
-        "fp64_one_at_a_time": {"solves_per_s": base_thr, "converged": base_ok,
-                               "iterations_median": float(np.median(base_iters)),
-                               "p50_s": pct(base_lat, 50), "p99_s": pct(base_lat, 99)},
-        "mixed_batched": {"solves_per_s_saturated": sat_thr, "converged": sum(
-            r.status == "converged" for r in res), "worst_true_rel_residual": worst,
-            "iterations_median": float(np.median([r.iterations for r in res])),
-            "p50_s": pct(lat, 50), "p99_s": pct(lat, 99), "completed_at_load": len(got)},
-        "fp64_server_one_slot": {"solves_per_s": one_thr, "converged": sum(
-            r.status == "converged" for r in res_one),
-            "speedup_mixed_batched_over_it": sat_thr / one_thr},
+        **out,
         "arrival_rate_per_s": lam,
-        "speedup_solves_per_s": sat_thr / base_thr,
+        "speedup_mixed_batched_over_fp64_one_at_a_time":
+            out["mixed_batched"]["solves_per_s_saturated"] / base,
+        "speedup_mixed_batched_over_fp64_batched":
+            out["mixed_batched"]["solves_per_s_saturated"] /
+            out["fp64_batched"]["solves_per_s_saturated"],
+        "speedup_fp64_batched_over_fp64_one_at_a_time":
+            out["fp64_batched"]["solves_per_s_saturated"] / base,
     }
 
 
@@ -985,7 +1041,7 @@ def run_extras(args):
     ex["spmv_powerlaw_8m"] = spmv_extra("spmv_powerlaw", A, W.dense_x(A.ncols, 3), peak, flush)
     ex["rcm_reorder"] = rcm_extra(A, flush)
     del A
-    ex["mixed_cg_3d_160"] = mixed_extra()
+    ex["mixed_cg_3d_160"] = mixed_extra(peak=peak)
     ex["serving_stream"] = serving_extra(nreq=args.requests)
     ex["spmm_laplace1024_k8"] = spmm_extra(flush=flush, peak=peak)
     ex["pagerank_powerlaw_2m"] = pagerank_extra()
@@ -1102,7 +1158,7 @@ def main():
         elif args.workload in ("spmv_uniform", "spmv_powerlaw"):
             out = run_spmv(args, dist, args.workload)
         elif args.workload == "cg_mixed_3d":
-            out = {"extras": {"mixed_cg_3d_160": mixed_extra()}}
+            out = {"extras": {"mixed_cg_3d_160": mixed_extra(peak=hbm_peak()[0])}}
         elif args.workload == "serving":
             out = {"extras": {"serving_stream": serving_extra(nreq=args.requests)}}
         elif args.workload == "spmm":

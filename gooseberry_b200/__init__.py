@@ -141,6 +141,7 @@ SIGNATURES = {
     "gb_cg_solve": (_i, [_vp, _vp, _vp, _d, _i, _sz, _vp, _sz, _vp, _vp]),
     "gb_cg_profile": (_i, [_vp, _vp, _sz, _vp, _sz, _vp, _vp]),
     "gb_cg_entry_bytes": (_i, [_vp, _vp]),
+    "gb_cg_row_bytes": (_i, [_vp, _vp]),
     "gb_cg_cancel": (_i, [_vp]),
     "gb_cg_set_barrier_fault": (_i, [_vp, C.c_int, C.c_uint]),
     "gb_server_cancel": (_i, [_vp, C.c_uint64]),
@@ -688,6 +689,13 @@ class CgSolver:
         """Bytes per matrix entry the solver's SpMV streams (12 = plain CSR)."""
         v = C.c_size_t(0)
         _check(lib().gb_cg_entry_bytes(self._h, C.addressof(v)), "gb_cg_entry_bytes")
+        return int(v.value)
+
+    def row_bytes(self) -> int:
+        """Bytes per row the solver's SpMV streams besides the entries (4 =
+        rowptr; 5 with a column-pattern byte)."""
+        v = C.c_size_t(0)
+        _check(lib().gb_cg_row_bytes(self._h, C.addressof(v)), "gb_cg_row_bytes")
         return int(v.value)
 
     def profile(self, b, iterations: int = 20, stream=None):

@@ -1340,6 +1340,12 @@ int gb_cg_entry_bytes(const gb_cg_t * s, size_t * bytes) {
   return GOOSEBERRY_SUCCESS;
 }
 
+int gb_cg_row_bytes(const gb_cg_t * s, size_t * bytes) {
+  GB_CHECK_INPUT(s != nullptr && bytes != nullptr, "NULL argument");
+  *bytes = s->mixed ? mixed_row_bytes(s->mixed) : 4;
+  return GOOSEBERRY_SUCCESS;
+}
+
 int gb_cg_profile(gb_cg_t * s, const double * b, size_t iterations, double * ms,
     size_t ms_len, size_t * nkernels, gb_stream_t stream) {
   GB_CHECK_INPUT(s != nullptr, "solver is NULL");

@@ -14,21 +14,26 @@
 //     so the Krylov process continues instead of restarting, and convergence
 //     is only ever declared on the true FP64 residual.
 //
-// Per iteration three kernels, graph-captured 32 iterations at a time with
-// programmatic dependent launch:
-//   A32  SpMV (FP32) with the fused direction update, p.Ap in FP64
-//   B32  alpha from A32's partials; y += alpha p, r -= alpha Ap, r.r in FP64
-//   R    beta, ||r|| and the update decision from B32's partials; then, only
-//        when an update is pending: FP64 SpMV of b - A (x + y) fused with
-//        x <- x + y (into the other x buffer, so no CTA reads an x another CTA
-//        already changed) and the FP32 rounding of r; true ||r||,
-//        convergence test.
-// A32 and B32 have no serial last-CTA step: every CTA of the next kernel sums
-// their per-CTA partials itself in the same fixed order, so all CTAs hold the
-// same alpha / beta / decision.  The scalars that change every iteration are
-// kept in two versions (iteration k reads version k & 1, R of iteration k
-// writes version (k + 1) & 1), so no CTA reads a value another CTA of the
-// same kernel is rewriting.  R's own step (rare) keeps its last-CTA tail.
+// Per iteration two kernels, graph-captured 32 at a time with programmatic
+// dependent launch:
+//   A32  the iteration's scalar step from B32's r.r partials (beta, ||r||, the
+//        stop test and the reliable-update decision, identical in every CTA),
+//        then the FP32 SpMV with the fused direction update and p.Ap in FP64;
+//   B32  alpha from A32's partials; y += alpha p, r -= alpha Ap, r.r in FP64.
+// A reliable update takes one pair of launches of its own: A32 decides it and
+// does no SpMV, and B32 computes r = b - A (x + y) with the FP64 values and
+// FP64 accumulation over its rows, x <- x + y (into the other x buffer, so no
+// CTA reads an x another CTA already changed), the FP32 rounding of r and the
+// true r.r partials, which the next A32 turns into the true ||r||, the
+// convergence test and beta.  No kernel has a serial last-CTA step: every CTA
+// of the next kernel sums the per-CTA partials itself in the same fixed
+// order, so all CTAs hold the same alpha / beta / decision.  The scalars are
+// kept in two versions: A32 launch k reads version k & 1 and its CTA 0 writes
+// version (k + 1) & 1, which B32 launch k reads, so no CTA reads a value
+// another CTA of the same kernel is rewriting.  The R kernel (FP64 residual
+// over the matrix's SpMV schedule) folds a pending correction into x when a
+// solve stops at its iteration limit, and times the FP64 residual for the
+// profiler.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -44,13 +49,18 @@ namespace {
 constexpr double kDelta = 0.1;  // reliable update when ||r|| < kDelta * max ||r||
 
 // The scalars of one iteration (two versions, see above).
+// What the pair of launches governed by a version does.
+enum : int { kPhaseCg = 0, kPhaseRefresh = 1, kPhaseFirst = 2 };
+
 struct MixScalars {
   double rr_hat;      // ||r||^2 of the FP32 residual the directions are built on
   double rr_hat_old;  // its value one iteration earlier
   double beta;
   double rmax;        // largest ||r|| since the last reliable update
   unsigned long long iter;
-  int update;         // a reliable update is pending
+  int phase;          // kPhaseCg: a CG iteration; kPhaseRefresh: a reliable
+                      // update (B32 recomputes r in FP64); kPhaseFirst: the
+                      // init kernel's version (A32 takes no step from it)
   int y_reset;        // y was folded into x: the next B starts y afresh
 };
 
@@ -59,21 +69,21 @@ struct MixState {
   double tol;         // absolute bound on the true ||b - A x||
   double bnorm;
   double rr_true;     // ||b - A x||^2 at the last reliable update
-  unsigned long long iter;  // iterations done (host mirror; written by R's CTA 0)
+  unsigned long long iter;  // iterations done (host mirror; written by A32's CTA 0)
   unsigned long long niter;
   unsigned long long refinements;
   int done;
   int status;
   int xpar;           // index of the current x buffer
+  int ver;            // the version the last A32 wrote (the current one)
   unsigned ticket_r, ticket_i;
   double * hist;
   unsigned long long hist_len;
 };
 
-// R launch modes: the iteration's step, the final fold the host requests when
-// a solve stops with a pending FP32 correction, and the profiler's (the step,
-// then the FP64 residual whether or not an update is pending).
-enum : int { kRStep = 0, kRFold = 1, kRProfile = 2 };
+// R launch modes: the final fold the host requests when a solve stops with a
+// pending FP32 correction, and the profiler's (the FP64 residual alone).
+enum : int { kRFold = 1, kRProfile = 2 };
 
 // The stop flag, read once per CTA so that all of its threads agree.
 __device__ __forceinline__ bool mix_cta_done(const MixState * st) {
@@ -90,6 +100,74 @@ struct MixStatus {
 };
 
 // ---- A32 ----------------------------------------------------------------------
+
+// The scalar step of A32 launch k from B32 launch k-1's partials: version
+// `par` in, version par ^ 1 out (CTA 0 writes it).  Identical in every CTA.
+// Returns true when this launch runs the CG SpMV (beta in *beta); false when
+// the solve stopped or this pair of launches is a reliable update.
+__device__ __forceinline__ bool mix_a_step(MixState * st, int par,
+    const double * __restrict__ partial_b, unsigned nb, float * beta) {
+  __shared__ double red[32];
+  __shared__ double s_rr;
+  const MixScalars cur = st->sv[par];
+  MixScalars nv = cur;
+  int stop = -1;
+  if (cur.phase != kPhaseFirst) {
+    const double rr_sum = ordered_sum(partial_b, nb, red);
+    if (threadIdx.x == 0) s_rr = rr_sum;
+    __syncthreads();
+    const double rr = s_rr;
+    const double rnorm = sqrt(rr);
+    const bool finite = rnorm == rnorm && !isinf(rnorm);
+    if (cur.phase == kPhaseRefresh) {
+      // B32 recomputed r = b - A x in FP64 (src/cgd.c:115-119 stops on it):
+      // continue from the true residual, keeping the search direction
+      nv.phase = kPhaseCg;
+      nv.y_reset = 1;
+      nv.beta = rr / cur.rr_hat_old;
+      nv.rr_hat = rr;
+      nv.rmax = rnorm;
+      if (!finite) stop = GB_CG_NONFINITE;
+      else if (rnorm <= st->tol) stop = GB_CG_CONVERGED;
+      else if (st->niter && cur.iter >= st->niter) stop = GB_CG_MAXITER;
+      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->rr_true = rr;
+        st->refinements += 1;
+        st->xpar ^= 1;
+        if (st->hist && cur.iter >= 1 && cur.iter <= st->hist_len) st->hist[cur.iter - 1] = rnorm;
+      }
+    } else {
+      // a CG iteration finished: beta, ||r|| and the reliable-update test
+      const unsigned long long it = cur.iter + 1;
+      nv.phase = kPhaseCg;
+      nv.y_reset = 0;
+      nv.iter = it;
+      nv.rr_hat_old = cur.rr_hat;
+      nv.beta = rr / cur.rr_hat;
+      nv.rr_hat = rr;
+      nv.rmax = fmax(cur.rmax, rnorm);
+      if (!finite) stop = GB_CG_NONFINITE;
+      else if (rnorm <= st->tol || rnorm < kDelta * nv.rmax) nv.phase = kPhaseRefresh;
+      else if (st->niter && it >= st->niter) stop = GB_CG_MAXITER;
+      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->iter = it;
+        if (st->hist && it <= st->hist_len) st->hist[it - 1] = rnorm;
+      }
+    }
+  } else {
+    nv.phase = kPhaseCg;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->sv[par ^ 1] = nv;
+    st->ver = par ^ 1;
+    if (stop >= 0) {
+      st->status = stop;
+      st->done = 1;
+    }
+  }
+  *beta = static_cast<float>(nv.beta);
+  return stop < 0 && nv.phase == kPhaseCg;
+}
 
 struct GatherP32 {
   const float * r;
@@ -147,10 +225,11 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_a32_ke
     const uint32_t * __restrict__ rowind, const float * __restrict__ val,
     const float * __restrict__ r, const float * __restrict__ pold, float * __restrict__ pnew,
     float * __restrict__ ap, double * __restrict__ longdot, double * __restrict__ partial,
-    MixState * st, int par) {
+    MixState * st, int par, const double * __restrict__ partial_b, unsigned nb) {
   pdl_wait_and_release();
   if (mix_cta_done(st)) return;
-  const float beta = static_cast<float>(st->sv[par].beta);
+  float beta;
+  if (!mix_a_step(st, par, partial_b, nb, &beta)) return;
   GatherP32 g{r, pold, beta};
   OutA32 o{ap, pnew, r, pold, longdot, partial, st, beta,
            SCHED == SCHED_ROW ? 0u : plan.nlong, 0.0};
@@ -158,43 +237,110 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_a32_ke
       rowind, val, g, o);
 }
 
-// A32 on the row schedule over 16-bit column distances (ColD16): the same
-// products and sums as cg_a32_kernel<SCHED_ROW>, 2 bytes less per nonzero.
-// Four CTAs per SM (64 registers, no spills): the FP32 rows are short chains
-// of dependent loads, and more of them in flight measured 4 % faster than
-// three CTAs (five spill).
-template <bool HINT, int STAGE>
-__global__ void __launch_bounds__(kSpmvBlock, 4) cg_a32_d16_kernel(
-    const PlanView plan, const uint32_t * __restrict__ rowptr,
-    const int16_t * __restrict__ col16, const float * __restrict__ val,
+// A32 on the row schedule over compressed columns: a pattern byte per row
+// (ColPat8, stencils) or 16-bit column distances (ColD16): the same products
+// and sums as cg_a32_kernel<SCHED_ROW>, 4 or 2 bytes less per nonzero.  Four
+// CTAs per SM (64 registers, no spills): the FP32 rows are short chains of
+// dependent loads, and more of them in flight measured 4 % faster than three
+// CTAs (five spill).
+#ifndef GB_MIX_PAT_MIN_BLOCKS
+#define GB_MIX_PAT_MIN_BLOCKS 5
+#endif
+// Over row patterns the stage holds one code per row instead of a column per
+// entry: 48 registers, five CTAs per SM.
+template <class IC>
+struct MixAMinBlocks {
+  static constexpr int value = IC::kPerRow ? GB_MIX_PAT_MIN_BLOCKS : 4;
+};
+
+template <class IC, bool HINT, int STAGE>
+__global__ void __launch_bounds__(kSpmvBlock, MixAMinBlocks<IC>::value) cg_a32_c_kernel(
+    const PlanView plan, const uint32_t * __restrict__ rowptr, IC ic,
+    const int32_t * __restrict__ pat_off, uint32_t npat, const float * __restrict__ val,
     const float * __restrict__ r, const float * __restrict__ pold, float * __restrict__ pnew,
     float * __restrict__ ap, double * __restrict__ longdot, double * __restrict__ partial,
-    MixState * st, int par) {
+    MixState * st, int par, const double * __restrict__ partial_b, unsigned nb) {
+  if constexpr (IC::kPerRow) {
+    __shared__ int32_t s_pat[256 * kPatMax];
+    for (uint32_t i = threadIdx.x; i < npat * kPatMax; i += kSpmvBlock) s_pat[i] = pat_off[i];
+    ic.off = s_pat;
+    __syncthreads();
+  }
   pdl_wait_and_release();
   if (mix_cta_done(st)) return;
-  const float beta = static_cast<float>(st->sv[par].beta);
+  float beta;
+  if (!mix_a_step(st, par, partial_b, nb, &beta)) return;
   GatherP32 g{r, pold, beta};
   OutA32 o{ap, pnew, r, pold, longdot, partial, st, beta, 0u, 0.0};
   spmv_row_loop_c<float, STAGE>(blockIdx.x * kSpmvBlock + threadIdx.x, plan.nrows,
-      gridDim.x * kSpmvBlock, plan.ncols, rowptr, ColD16{col16}, ValPlain<float>{val}, g, o,
+      gridDim.x * kSpmvBlock, plan.ncols, rowptr, ic, ValPlain<float>{val}, g, o,
       L2Pol<HINT>::stream(), L2Pol<HINT>::keep());
   o.finish();
 }
 
 // ---- B32 ----------------------------------------------------------------------
 
+// The reliable update of B32's rows (a kPhaseRefresh pair): r = b - A (x + y)
+// with the FP64 values, each row summed in the reference's order
+// (src/blas.c:82-91, unfused multiply and add), x <- x + y into the other x
+// buffer, r rounded to FP32, and the true r.r partial of the CTA.  The search
+// direction is kept: A32 wrote no new one in this pair, so it is carried into
+// the buffer the next A32 reads (pnew <- pold).  One thread per row: the
+// reliable update is rare, and this keeps the FP64 loop out of the SpMV
+// kernel's register budget.
+__device__ __forceinline__ void mix_refresh_rows(size_t s, size_t e,
+    const uint32_t * __restrict__ rowptr, const uint32_t * __restrict__ rowind,
+    const double * __restrict__ val, const double * __restrict__ b,
+    const double * __restrict__ xold, double * __restrict__ xnew, const float * __restrict__ y,
+    float * __restrict__ r, const float * __restrict__ pold, float * __restrict__ pnew,
+    bool use_y, double * __restrict__ partial, double * red) {
+  double acc = 0.0;
+  for (size_t i = s + threadIdx.x; i < e; i += kVecBlock) {
+    pnew[i] = pold[i];
+    const uint32_t kb = __ldg(rowptr + i), ke = __ldg(rowptr + i + 1);
+    double ax = 0.0;
+    for (uint32_t k = kb; k < ke; ++k) {
+      const uint32_t c = __ldg(rowind + k);
+      const double xc = use_y ? xold[c] + static_cast<double>(y[c]) : xold[c];
+      ax = add_rn(ax, mul_rn(__ldg(val + k), xc));
+    }
+    xnew[i] = use_y ? xold[i] + static_cast<double>(y[i]) : xold[i];
+    const double rt = b[i] - ax;
+    r[i] = static_cast<float>(rt);
+    acc += rt * rt;
+  }
+  const double bs = block_sum(acc, red);
+  if (threadIdx.x == 0) partial[blockIdx.x] = bs;
+}
+
 // Every CTA first sums A32's p.Ap partials (then the long-row terms) in order
 // and forms alpha = rr_hat / p.Ap; a breakdown (p.Ap <= 0) or NaN stops the
-// solve before anything is updated.
-__global__ void __launch_bounds__(kVecBlock, kSpmvMinBlocks) cg_b32_kernel(size_t n,
-    float * __restrict__ y, float * __restrict__ r, const float * __restrict__ p,
+// solve before anything is updated.  In a reliable-update pair it computes
+// the FP64 residual of its rows instead (mix_refresh_rows).  Six CTAs per SM
+// (40 registers, no spills): the update streams six vectors, and at four CTAs
+// (54 registers) it ran 21.2 us instead of 18.6 on the 160^3 operator.
+__global__ void __launch_bounds__(kVecBlock, 6) cg_b32_kernel(size_t n,
+    float * __restrict__ y, float * __restrict__ r, float * __restrict__ p,
+    const float * __restrict__ pold,
     const float * __restrict__ ap, const double * __restrict__ partial_a, unsigned na,
     const double * __restrict__ longdot, unsigned nlong, double * __restrict__ partial,
-    MixState * st, int par) {
+    MixState * st, int par, const uint32_t * __restrict__ rowptr,
+    const uint32_t * __restrict__ rowind, const double * __restrict__ val64,
+    const double * __restrict__ bvec, double * x0, double * x1) {
   pdl_wait_and_release();
   if (mix_cta_done(st)) return;
   __shared__ double red[32];
   __shared__ double s_pap;
+  if (st->sv[par].phase == kPhaseRefresh) {
+    const size_t q = n / gridDim.x, rem = n % gridDim.x;
+    const size_t cb = blockIdx.x;
+    const size_t s = cb * q + min(cb, rem);
+    const size_t e = s + q + (cb < rem ? 1 : 0);
+    const int xp = st->xpar;
+    mix_refresh_rows(s, e, rowptr, rowind, val64, bvec, xp ? x1 : x0, xp ? x0 : x1, y, r,
+        pold, p, st->sv[par].y_reset == 0, partial, red);
+    return;
+  }
   double tot = ordered_sum(partial_a, na, red);
   if (threadIdx.x == 0) {
     for (unsigned q = 0; q < nlong; ++q) tot += __ldcg(longdot + q);
@@ -300,7 +446,7 @@ struct OutR {
       st->refinements += 1;
       st->xpar ^= 1;
       sv->y_reset = 1;
-      sv->update = 0;
+      sv->phase = kPhaseCg;
       const double rnorm = sqrt(tot);
       // written by CTA 0 during this launch: read through L2
       const unsigned long long it = __ldcg(&st->iter);
@@ -325,62 +471,26 @@ struct OutR {
   }
 };
 
+// R: the FP64 residual r = b - A (x + y) over the matrix's SpMV schedule,
+// x <- x + y into the other x buffer; kRFold folds a pending correction when a
+// solve stopped (version `par`, the current one), kRProfile times the step.
 template <int SCHED, bool HINT>
 __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_r_kernel(
     const PlanView plan, const uint32_t * __restrict__ rowptr,
     const uint32_t * __restrict__ rowind, const double * __restrict__ val,
     const double * __restrict__ b, const double * __restrict__ x0, double * __restrict__ x1,
     const float * __restrict__ y, float * __restrict__ r32, double * __restrict__ longdot,
-    double * __restrict__ partial, MixState * st, const double * __restrict__ partial_b,
-    unsigned nb, int par, int mode) {
+    double * __restrict__ partial, MixState * st, int par, int mode) {
   pdl_wait_and_release();
-  MixScalars * sv = &st->sv[par];  // kRFold: the current version, in place
-  if (mode != kRFold) {
-    // the iteration's scalar step from B32's r.r partials (src/cgd.c:109-119
-    // for beta and the stop test), identical in every CTA; CTA 0 records it
-    // as the next version
-    if (mix_cta_done(st)) return;
-    __shared__ double red[32];
-    __shared__ double s_rr;
-    const double rr_sum = ordered_sum(partial_b, nb, red);
-    if (threadIdx.x == 0) s_rr = rr_sum;
-    __syncthreads();
-    const double rr = s_rr;
-    const MixScalars cur = st->sv[par];
-    MixScalars nv = cur;
-    nv.y_reset = 0;
-    nv.rr_hat_old = cur.rr_hat;
-    nv.beta = rr / cur.rr_hat;
-    nv.rr_hat = rr;
-    const unsigned long long it = cur.iter + 1;
-    nv.iter = it;
-    const double rnorm = sqrt(rr);
-    nv.rmax = fmax(cur.rmax, rnorm);
-    int stop = -1;
-    if (!(rnorm == rnorm) || isinf(rnorm)) stop = GB_CG_NONFINITE;
-    else if (rnorm <= st->tol || rnorm < kDelta * nv.rmax) nv.update = 1;
-    else if (st->niter && it >= st->niter) stop = GB_CG_MAXITER;
-    sv = &st->sv[par ^ 1];
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      *sv = nv;
-      st->iter = it;
-      if (st->hist && it <= st->hist_len) st->hist[it - 1] = rnorm;
-      if (stop >= 0) {
-        st->status = stop;
-        st->done = 1;
-      }
-    }
-    if (stop >= 0 || (!nv.update && mode != kRProfile)) return;
-  }
+  MixScalars * sv = &st->sv[par];
   const int xpar = st->xpar;
-  // after the step y holds this iteration's correction; a fold on request
-  // uses it only if no update has consumed it yet
+  // a fold uses y only if no update has consumed it yet
   const bool use_y = mode != kRFold || sv->y_reset == 0;
   const double * xold = xpar ? x1 : x0;
   double * xnew = xpar ? const_cast<double *>(x0) : x1;
   GatherXY g{xold, y, use_y};
   OutR o{b, xold, xnew, y, r32, longdot, partial, st, use_y,
-         SCHED == SCHED_ROW ? 0u : plan.nlong, 0.0, sv, mode != kRStep};
+         SCHED == SCHED_ROW ? 0u : plan.nlong, 0.0, sv, true};
   spmv_tiles_body<double, double, SCHED, kSpmvBlock, GatherXY, OutR, false, HINT>(plan, rowptr,
       rowind, val, g, o);
 }
@@ -430,8 +540,9 @@ __global__ void __launch_bounds__(kVecBlock) cg_mixed_init_kernel(size_t n,
     v0.beta = 0.0;
     v0.iter = 0;
     v0.y_reset = 1;
-    v0.update = 0;
+    v0.phase = kPhaseFirst;
     st->sv[0] = v0;
+    st->ver = 0;
     st->iter = 0;
     st->refinements = 0;
     st->xpar = 0;
@@ -468,25 +579,24 @@ int prep_kernel(K kern, size_t smem, int * occ) {
 template <int SCHED, bool HINT>
 int launch_a32_t(const gb_csr & a, unsigned grid, cudaStream_t s, bool pdl,
     const float * r, const float * pold, float * pnew, float * ap, double * longdot,
-    double * partial, MixState * st, int par) {
+    double * partial, MixState * st, int par, const double * partial_b, unsigned nb) {
   const size_t smem = smem_of(SCHED, a.plan.tile_items, 4);
   auto kern = cg_a32_kernel<SCHED, HINT>;
   GB_TRY(prep_kernel(kern, smem, nullptr));
   GB_CUDA_TRY(launch_k(kern, grid, kSpmvBlock, smem, s, pdl, plan_view(a), a.rowptr,
-      a.rowind, a.val32, r, pold, pnew, ap, longdot, partial, st, par));
+      a.rowind, a.val32, r, pold, pnew, ap, longdot, partial, st, par, partial_b, nb));
   return GOOSEBERRY_SUCCESS;
 }
 
 template <int SCHED, bool HINT>
 int launch_r_t(const gb_csr & a, unsigned grid, cudaStream_t s, bool pdl, const double * b,
     const double * x0, double * x1, const float * y, float * r32, double * longdot,
-    double * partial, MixState * st, const double * partial_b, unsigned nb, int par,
-    int mode) {
+    double * partial, MixState * st, int par, int mode) {
   const size_t smem = smem_of(SCHED, a.plan.tile_items, 8);
   auto kern = cg_r_kernel<SCHED, HINT>;
   GB_TRY(prep_kernel(kern, smem, nullptr));
   GB_CUDA_TRY(launch_k(kern, grid, kSpmvBlock, smem, s, pdl, plan_view(a), a.rowptr,
-      a.rowind, a.val64, b, x0, x1, y, r32, longdot, partial, st, partial_b, nb, par, mode));
+      a.rowind, a.val64, b, x0, x1, y, r32, longdot, partial, st, par, mode));
   return GOOSEBERRY_SUCCESS;
 }
 
@@ -501,17 +611,33 @@ int launch_r_t(const gb_csr & a, unsigned grid, cudaStream_t s, bool pdl, const 
     default: return CALL(SCHED_MERGE);                                          \
   }
 
-template <bool HINT>
-int launch_a32_d16_t(const gb_csr & a, const int16_t * col16, int stage, unsigned grid,
-    cudaStream_t s, bool pdl, const float * r, const float * pold, float * pnew, float * ap,
-    double * longdot, double * partial, MixState * st, int par, int * occ) {
-  auto kern = stage == 5   ? cg_a32_d16_kernel<HINT, 5>
-              : stage == 7 ? cg_a32_d16_kernel<HINT, 7>
-                           : cg_a32_d16_kernel<HINT, kRowStage>;
+template <class IC, bool HINT>
+int launch_a32_c_t(const gb_csr & a, const IC & ic, const RowPatterns & pat, int stage,
+    unsigned grid, cudaStream_t s, bool pdl, const float * r, const float * pold, float * pnew,
+    float * ap, double * longdot, double * partial, MixState * st, int par,
+    const double * partial_b, unsigned nb, int * occ) {
+  auto kern = stage == 5   ? cg_a32_c_kernel<IC, HINT, 5>
+              : stage == 7 ? cg_a32_c_kernel<IC, HINT, 7>
+                           : cg_a32_c_kernel<IC, HINT, kRowStage>;
   if (occ) return prep_kernel(kern, 0, occ);
-  GB_CUDA_TRY(launch_k(kern, grid, kSpmvBlock, 0, s, pdl, plan_view(a), a.rowptr, col16, a.val32,
-      r, pold, pnew, ap, longdot, partial, st, par));
+  GB_CUDA_TRY(launch_k(kern, grid, kSpmvBlock, 0, s, pdl, plan_view(a), a.rowptr, ic,
+      static_cast<const int32_t *>(pat.off), pat.npat, a.val32, r, pold, pnew, ap, longdot,
+      partial, st, par, partial_b, nb));
   return GOOSEBERRY_SUCCESS;
+}
+
+// The row-schedule A32 over the solver's compressed columns (patterns, else
+// 16-bit distances).
+template <bool HINT>
+int launch_a32_d16_t(const gb_csr & a, const RowPatterns & pat, const int16_t * col16,
+    int stage, unsigned grid, cudaStream_t s, bool pdl, const float * r, const float * pold,
+    float * pnew, float * ap, double * longdot, double * partial, MixState * st, int par,
+    const double * partial_b, unsigned nb, int * occ) {
+  if (pat.code8)
+    return launch_a32_c_t<ColPat8, HINT>(a, ColPat8{pat.code8, nullptr}, pat, stage, grid, s,
+        pdl, r, pold, pnew, ap, longdot, partial, st, par, partial_b, nb, occ);
+  return launch_a32_c_t<ColD16, HINT>(a, ColD16{col16}, pat, stage, grid, s, pdl, r, pold, pnew,
+      ap, longdot, partial, st, par, partial_b, nb, occ);
 }
 
 template <int SCHED>
@@ -545,7 +671,9 @@ struct MixedCg {
   MixStatus * host_status = nullptr;
   unsigned grid_a = 0, grid_b = 0, grid_r = 0;
   bool l2_hint = false;  // L2-policy loads (the FP32 working set fits in L2)
-  int16_t * col16 = nullptr;  // row schedule: column - row, 16-bit (else null)
+  // row schedule: columns as row patterns, else column - row in 16 bits
+  RowPatterns pat;
+  int16_t * col16 = nullptr;
   int stage = 6;
   int chunk = 32;
   cudaStream_t cap_stream = nullptr;
@@ -557,51 +685,53 @@ namespace {
 int launch_a32(MixedCg * m, cudaStream_t s, bool pdl, int k) {
   const float * pold = m->p[k & 1];
   float * pnew = m->p[(k + 1) & 1];
-  if (m->col16)
-    return m->l2_hint ? launch_a32_d16_t<true>(*m->a, m->col16, m->stage, m->grid_a, s, pdl,
-                            m->r, pold, pnew, m->ap, m->longdot, m->partial_a, m->st, k & 1,
-                            nullptr)
-                      : launch_a32_d16_t<false>(*m->a, m->col16, m->stage, m->grid_a, s, pdl,
-                            m->r, pold, pnew, m->ap, m->longdot, m->partial_a, m->st, k & 1,
-                            nullptr);
+  if (m->pat.code8 || m->col16)
+    return m->l2_hint ? launch_a32_d16_t<true>(*m->a, m->pat, m->col16, m->stage, m->grid_a, s,
+                            pdl, m->r, pold, pnew, m->ap, m->longdot, m->partial_a, m->st,
+                            k & 1, m->partial_b, m->grid_b, nullptr)
+                      : launch_a32_d16_t<false>(*m->a, m->pat, m->col16, m->stage, m->grid_a, s,
+                            pdl, m->r, pold, pnew, m->ap, m->longdot, m->partial_a, m->st,
+                            k & 1, m->partial_b, m->grid_b, nullptr);
 #define GB_CALL(S)                                                                      \
   (m->l2_hint ? launch_a32_t<S, true>(*m->a, m->grid_a, s, pdl, m->r, pold, pnew, m->ap,   \
-                                      m->longdot, m->partial_a, m->st, k & 1)              \
+                                      m->longdot, m->partial_a, m->st, k & 1,              \
+                                      m->partial_b, m->grid_b)                             \
               : launch_a32_t<S, false>(*m->a, m->grid_a, s, pdl, m->r, pold, pnew, m->ap,  \
-                                       m->longdot, m->partial_a, m->st, k & 1))
+                                       m->longdot, m->partial_a, m->st, k & 1,             \
+                                       m->partial_b, m->grid_b))
   GB_SCHED_SWITCH(m->sched32, GB_CALL)
 #undef GB_CALL
 }
 
-// R of iteration parity par (kRFold: par = the current version).
+// R over version par (kRFold: the current version).
 int launch_r(MixedCg * m, cudaStream_t s, bool pdl, int par, int mode) {
 #define GB_CALL(S)                                                                      \
   (m->l2_hint ? launch_r_t<S, true>(*m->a, m->grid_r, s, pdl, m->b, m->x[0], m->x[1], m->y,  \
-                                    m->r, m->longdot, m->partial_r, m->st, m->partial_b,    \
-                                    m->grid_b, par, mode)                                   \
+                                    m->r, m->longdot, m->partial_r, m->st, par, mode)       \
               : launch_r_t<S, false>(*m->a, m->grid_r, s, pdl, m->b, m->x[0], m->x[1], m->y, \
-                                     m->r, m->longdot, m->partial_r, m->st, m->partial_b,   \
-                                     m->grid_b, par, mode))
+                                     m->r, m->longdot, m->partial_r, m->st, par, mode))
   GB_SCHED_SWITCH(m->sched64, GB_CALL)
 #undef GB_CALL
 }
 
+// B32 of A32 launch k: it reads the version A32 k wrote, (k + 1) & 1.
 int launch_b32(MixedCg * m, cudaStream_t s, bool pdl, int k) {
   float * pnew = m->p[(k + 1) & 1];
   // the row schedule sums long rows like any other row: no long-row terms
   const unsigned nlong = m->sched32 == GB_SCHED_ROW ? 0u
                          : static_cast<unsigned>(m->a->plan.longrows.size());
   GB_CUDA_TRY(launch_k(cg_b32_kernel, m->grid_b, kVecBlock, 0, s, pdl, m->n, m->y, m->r,
-      static_cast<const float *>(pnew), static_cast<const float *>(m->ap),
+      pnew, static_cast<const float *>(m->p[k & 1]), static_cast<const float *>(m->ap),
       static_cast<const double *>(m->partial_a), m->grid_a,
-      static_cast<const double *>(m->longdot), nlong, m->partial_b, m->st, k & 1));
+      static_cast<const double *>(m->longdot), nlong, m->partial_b, m->st, (k + 1) & 1,
+      m->a->rowptr, m->a->rowind, static_cast<const double *>(m->a->val64),
+      static_cast<const double *>(m->b), m->x[0], m->x[1]));
   return GOOSEBERRY_SUCCESS;
 }
 
 int iteration(MixedCg * m, cudaStream_t s, bool pdl_first, int k) {
   GB_TRY(launch_a32(m, s, pdl_first, k));
   GB_TRY(launch_b32(m, s, true, k));
-  GB_TRY(launch_r(m, s, true, k & 1, kRStep));
   return GOOSEBERRY_SUCCESS;
 }
 
@@ -690,11 +820,14 @@ void mixed_destroy(MixedCg * m) {
   dev_free(m->longdot);
   dev_free(m->st);
   if (m->col16) dev_free(m->col16);
+  free_row_patterns(m->pat);
   if (m->host_status) cudaFreeHost(m->host_status);
   delete m;
 }
 
-size_t mixed_entry_bytes(const MixedCg * m) { return m->col16 ? 6 : 8; }
+size_t mixed_entry_bytes(const MixedCg * m) { return m->pat.code8 ? 4 : (m->col16 ? 6 : 8); }
+
+size_t mixed_row_bytes(const MixedCg * m) { return m->pat.code8 ? 5 : 4; }
 
 int mixed_create(const gb_csr * a, bool plain_entries, MixedCg ** out) {
   GB_CHECK_INPUT(a->val64 && a->val32,
@@ -707,16 +840,18 @@ int mixed_create(const gb_csr * a, bool plain_entries, MixedCg ** out) {
   m->sched32 = a->sched32;
   m->sched64 = a->sched64;
   m->tile_items = a->plan.tile_items;
-  // the row schedule reads 16-bit column distances when every entry lies
-  // within 32767 of the diagonal (stencils, banded matrices)
+  // the row schedule reads a pattern byte per row when the rows form at most
+  // 256 column patterns (stencils), else 16-bit column distances when every
+  // entry lies within 32767 of the diagonal (banded matrices)
   if (m->sched32 == GB_SCHED_ROW && !plain_entries) {
-    GB_TRY(build_col16(*a, &m->col16, nullptr));
+    GB_TRY(build_row_patterns(*a, &m->pat, nullptr));
+    if (!m->pat.code8) GB_TRY(build_col16(*a, &m->col16, nullptr));
     m->stage = row_stage_for(*a);
   }
   // L2-policy loads only when the FP32 iteration's working set (rowptr,
   // indices, float values, r, both p, Ap, y) fits in L2
-  GB_TRY(l2_fits(4ull * (m->n + 1) + (m->col16 ? 6ull : 8ull) * a->nnz + 24ull * m->n,
-      &m->l2_hint));
+  GB_TRY(l2_fits(mixed_row_bytes(m) * (m->n + 1) + mixed_entry_bytes(m) * a->nnz +
+      24ull * m->n, &m->l2_hint));
   const size_t n = std::max<size_t>(m->n, 2);
   GB_TRY(dev_alloc(&m->x[0], n * sizeof(double)));
   GB_TRY(dev_alloc(&m->x[1], n * sizeof(double)));
@@ -726,10 +861,10 @@ int mixed_create(const gb_csr * a, bool plain_entries, MixedCg ** out) {
   GB_TRY(dev_alloc(&m->p[0], n * sizeof(float)));
   GB_TRY(dev_alloc(&m->p[1], n * sizeof(float)));
   GB_TRY(dev_alloc(&m->ap, n * sizeof(float)));
-  if (m->col16) {
+  if (m->pat.code8 || m->col16) {
     int occ = 0;
-    GB_TRY(launch_a32_d16_t<false>(*a, m->col16, m->stage, 0, nullptr, false, nullptr, nullptr,
-        nullptr, nullptr, nullptr, nullptr, nullptr, 0, &occ));
+    GB_TRY(launch_a32_d16_t<false>(*a, m->pat, m->col16, m->stage, 0, nullptr, false, nullptr,
+        nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr, 0, &occ));
     GB_CHECK_INPUT(occ > 0, "CG kernel cannot be resident");
     const size_t rows_units = (m->n + kSpmvBlock - 1) / kSpmvBlock;
     m->grid_a = static_cast<unsigned>(std::max<size_t>(1, std::min<size_t>(rows_units,
@@ -803,7 +938,7 @@ int mixed_solve(MixedCg * m, const double * b, double * x, double tol, int tol_r
   auto launch = [&](int slot) -> int {
     cudaError_t e = cudaGraphLaunch(m->graph[slot], stream);
     if (e == cudaSuccess) e = cudaEventRecord(ev[slot], stream);
-    launches += 3 * static_cast<size_t>(m->chunk);
+    launches += 2 * static_cast<size_t>(m->chunk);
     if (e != cudaSuccess) {
       set_error("mixed CG graph launch failed: %s", cudaGetErrorString(e));
       return GOOSEBERRY_ERROR_UNKNOWN;
@@ -840,10 +975,10 @@ int mixed_solve(MixedCg * m, const double * b, double * x, double tol, int tol_r
   if (rc == GOOSEBERRY_SUCCESS) {
     e = cudaMemcpy(&fin, m->st, sizeof(MixState), cudaMemcpyDeviceToHost);
     if (e == cudaSuccess && fin.status != GB_CG_CONVERGED && fin.status != GB_CG_NONFINITE &&
-        fin.sv[fin.iter & 1].y_reset == 0) {
+        fin.sv[fin.ver].y_reset == 0) {
       // stopped on the iteration limit (or breakdown) with a pending FP32
       // correction: fold it into x once more and measure the true residual
-      rc = launch_r(m, stream, false, static_cast<int>(fin.iter & 1), kRFold);
+      rc = launch_r(m, stream, false, fin.ver, kRFold);
       launches += 1;
       if (e == cudaSuccess && rc == GOOSEBERRY_SUCCESS) e = cudaStreamSynchronize(stream);
       if (e == cudaSuccess && rc == GOOSEBERRY_SUCCESS)
@@ -877,7 +1012,7 @@ int mixed_profile(MixedCg * m, const double * b, size_t iterations, double * ms,
     size_t ms_len, size_t * nkernels, cudaStream_t stream) {
   GB_CHECK_INPUT(m->n > 0 && b != nullptr, "profile needs a non-empty system and b");
   GB_CHECK_INPUT(iterations > 0, "iterations must be positive");
-  if (nkernels) *nkernels = 3;
+  if (nkernels) *nkernels = 3;  // A32, B32, and the FP64 residual of a reliable update
   GB_TRY(mixed_start(m, b, 0.0, 0, 0, nullptr, 0, stream));
   std::vector<cudaEvent_t> ev(4 * iterations);
   for (auto & e : ev) GB_CUDA_TRY(cudaEventCreate(&e));
@@ -888,8 +1023,10 @@ int mixed_profile(MixedCg * m, const double * b, size_t iterations, double * ms,
     cudaEventRecord(ev[4 * k + 1], stream);
     if (rc == GOOSEBERRY_SUCCESS) rc = launch_b32(m, stream, false, static_cast<int>(k));
     cudaEventRecord(ev[4 * k + 2], stream);
-    // the FP64 refinement runs every iteration here, so every iteration times it
-    if (rc == GOOSEBERRY_SUCCESS) rc = launch_r(m, stream, false, static_cast<int>(k & 1), kRProfile);
+    // the FP64 residual of a reliable update runs every iteration here, so
+    // every iteration times it (the solve runs it only when an update is due)
+    if (rc == GOOSEBERRY_SUCCESS)
+      rc = launch_r(m, stream, false, static_cast<int>((k + 1) & 1), kRProfile);
     cudaEventRecord(ev[4 * k + 3], stream);
   }
   cudaError_t e = cudaStreamSynchronize(stream);

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "gb_internal.h"
+#include "spmv_tiles.cuh"
 
 namespace gb {
 namespace {
@@ -114,6 +115,97 @@ __global__ void codec_f32_kernel(const double * __restrict__ val, uint32_t nnz,
   }
 }
 
+// ---- row patterns (ColPat8) ---------------------------------------------------
+
+// Hash of a row's column offsets from the diagonal (offsets taken mod 2^32, so
+// row + offset recovers the column exactly); never the empty-slot value.
+__device__ __forceinline__ unsigned long long pattern_hash(const uint32_t * __restrict__ rowind,
+    uint32_t b, uint32_t e, uint32_t row) {
+  unsigned long long h = 0x9e3779b97f4a7c15ull * (e - b + 1);
+  for (uint32_t k = b; k < e; ++k) {
+    const unsigned long long d = __ldg(rowind + k) - row;
+    h ^= d + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2);
+    h *= 0xff51afd7ed558ccdull;
+    h ^= h >> 33;
+  }
+  return h == kEmpty ? h ^ 1ull : h;
+}
+
+// Distinct row patterns into the hash set, with a row holding each; *bad = 1
+// past kMaxCodes patterns or for a row longer than kPatMax.
+__global__ void codec_pattern_set_kernel(const uint32_t * __restrict__ rowptr,
+    const uint32_t * __restrict__ rowind, uint32_t n, unsigned long long * keys,
+    uint32_t * rep, unsigned * count, unsigned * bad) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if ((i & 255u) == 0 && *reinterpret_cast<volatile unsigned *>(bad)) return;
+    const uint32_t b = __ldg(rowptr + i), e = __ldg(rowptr + i + 1);
+    if (e - b > static_cast<uint32_t>(kPatMax)) {
+      atomicExch(bad, 1u);
+      return;
+    }
+    const unsigned long long h0 = pattern_hash(rowind, b, e, i);
+    unsigned h = slot_of(h0);
+    bool placed = false;
+    for (unsigned probe = 0; probe < kSetSlots; ++probe, h = (h + 1) & (kSetSlots - 1)) {
+      unsigned long long cur = *reinterpret_cast<volatile unsigned long long *>(keys + h);
+      if (cur == h0) {
+        placed = true;
+        break;
+      }
+      if (cur == kEmpty) {
+        cur = atomicCAS(keys + h, kEmpty, h0);
+        if (cur == kEmpty) {
+          rep[h] = i;
+          if (atomicAdd(count, 1u) >= kMaxCodes) atomicExch(bad, 1u);
+          placed = true;
+          break;
+        }
+        if (cur == h0) {
+          placed = true;
+          break;
+        }
+      }
+    }
+    if (!placed) {
+      atomicExch(bad, 1u);
+      return;
+    }
+  }
+}
+
+// off[code * kPatMax + j] = offset j of the row that holds each pattern.
+__global__ void codec_pattern_table_kernel(const uint32_t * __restrict__ rowptr,
+    const uint32_t * __restrict__ rowind, const unsigned long long * __restrict__ keys,
+    const uint32_t * __restrict__ rep, const uint8_t * __restrict__ slot_code,
+    int32_t * __restrict__ off) {
+  const unsigned h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= kSetSlots || keys[h] == kEmpty) return;
+  const uint32_t row = rep[h], b = rowptr[row], e = rowptr[row + 1];
+  const uint32_t c = slot_code[h];
+  for (int j = 0; j < kPatMax; ++j)
+    off[c * kPatMax + j] = b + j < e ? static_cast<int32_t>(rowind[b + j] - row) : 0;
+}
+
+// code8[i] = pattern of row i; then every column is checked against it
+// (*bad = 1 on a mismatch, which only a hash collision could cause).
+__global__ void codec_pattern_encode_kernel(const uint32_t * __restrict__ rowptr,
+    const uint32_t * __restrict__ rowind, uint32_t n, const unsigned long long * __restrict__ keys,
+    const uint8_t * __restrict__ slot_code, const int32_t * __restrict__ off,
+    uint8_t * __restrict__ code8, unsigned * bad) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t b = __ldg(rowptr + i), e = __ldg(rowptr + i + 1);
+    const unsigned long long h0 = pattern_hash(rowind, b, e, i);
+    unsigned h = slot_of(h0);
+    for (unsigned probe = 0; probe < kSetSlots; ++probe, h = (h + 1) & (kSetSlots - 1))
+      if (__ldg(keys + h) == h0) break;
+    const uint32_t c = __ldg(slot_code + h);
+    code8[i] = static_cast<uint8_t>(c);
+    for (uint32_t k = b; k < e; ++k)
+      if (__ldg(rowind + k) != i + static_cast<uint32_t>(__ldg(off + c * kPatMax + (k - b))))
+        atomicExch(bad, 1u);
+  }
+}
+
 int grid_of(const gb_csr & a, size_t items) {
   const size_t want = (items + 255) / 256;
   return static_cast<int>(std::max<size_t>(1, std::min<size_t>(want,
@@ -198,6 +290,69 @@ int build_values(const gb_csr & a, RowCodec * c, unsigned * flags, cudaStream_t 
 }
 
 }  // namespace
+
+int build_row_patterns(const gb_csr & a, RowPatterns * out, cudaStream_t s) {
+  *out = RowPatterns{};
+  // rows of at most 7 entries: the row loop's register stage (row_stage_for)
+  // then holds a whole row, and pattern rows need no long-row tail
+  if (a.nrows == 0 || a.plan.max_row > 7u) return GOOSEBERRY_SUCCESS;
+  // set: keys, representative rows, count + flag
+  unsigned long long * keys = nullptr;
+  GB_TRY(scratch_alloc(reinterpret_cast<void **>(&keys), kSetSlots * 12 + kSetSlots + 64, s));
+  uint32_t * rep = reinterpret_cast<uint32_t *>(keys + kSetSlots);
+  uint8_t * d_slot = reinterpret_cast<uint8_t *>(rep + kSetSlots);
+  unsigned * cnt = reinterpret_cast<unsigned *>(d_slot + kSetSlots);
+  unsigned * flags = cnt + 2;
+  std::vector<unsigned long long> hk(kSetSlots, kEmpty);
+  unsigned bad = 1, count = 0;
+  int rc = GOOSEBERRY_SUCCESS;
+  auto done = [&](int r) {
+    scratch_free(keys, s);
+    if (r != GOOSEBERRY_SUCCESS || bad) {
+      if (out->code8) dev_free(out->code8);
+      if (out->off) dev_free(out->off);
+      *out = RowPatterns{};
+    }
+    return r;
+  };
+  if (cudaMemcpyAsync(keys, hk.data(), kSetSlots * 8, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemsetAsync(cnt, 0, 16, s) != cudaSuccess)
+    return done(GOOSEBERRY_ERROR_UNKNOWN);
+  codec_pattern_set_kernel<<<grid_of(a, a.nrows), 256, 0, s>>>(a.rowptr, a.rowind, a.nrows, keys,
+      rep, cnt, flags);
+  if ((rc = read_flag(flags, &bad, s)) != GOOSEBERRY_SUCCESS || bad) return done(rc);
+  if (cudaMemcpyAsync(hk.data(), keys, kSetSlots * 8, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaMemcpyAsync(&count, cnt, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return done(GOOSEBERRY_ERROR_UNKNOWN);
+  std::vector<uint8_t> slot_code(kSetSlots, 0);
+  uint32_t np = 0;
+  for (unsigned h = 0; h < kSetSlots; ++h)
+    if (hk[h] != kEmpty) slot_code[h] = static_cast<uint8_t>(np++);
+  bad = np != count || np > kMaxCodes;
+  if (bad) return done(GOOSEBERRY_SUCCESS);
+  if ((rc = dev_alloc(&out->code8, a.nrows)) != GOOSEBERRY_SUCCESS ||
+      (rc = dev_alloc(&out->off, static_cast<size_t>(std::max(np, 1u)) * kPatMax * 4)) !=
+          GOOSEBERRY_SUCCESS)
+    return done(rc);
+  out->npat = np;
+  if (cudaMemcpyAsync(d_slot, slot_code.data(), kSetSlots, cudaMemcpyHostToDevice, s) !=
+          cudaSuccess ||
+      cudaMemsetAsync(flags, 0, 4, s) != cudaSuccess)
+    return done(GOOSEBERRY_ERROR_UNKNOWN);
+  codec_pattern_table_kernel<<<kSetSlots / 256, 256, 0, s>>>(a.rowptr, a.rowind, keys, rep,
+      d_slot, out->off);
+  codec_pattern_encode_kernel<<<grid_of(a, a.nrows), 256, 0, s>>>(a.rowptr, a.rowind, a.nrows,
+      keys, d_slot, out->off, out->code8, flags);
+  if ((rc = read_flag(flags, &bad, s)) != GOOSEBERRY_SUCCESS) return done(rc);
+  return done(GOOSEBERRY_SUCCESS);
+}
+
+void free_row_patterns(RowPatterns & p) {
+  if (p.code8) dev_free(p.code8);
+  if (p.off) dev_free(p.off);
+  p = RowPatterns{};
+}
 
 int row_stage_for(const gb_csr & a) {
   return a.plan.max_row <= 5 ? 5 : (a.plan.max_row <= 7 ? 7 : 6);

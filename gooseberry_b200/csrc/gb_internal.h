@@ -213,6 +213,18 @@ int csr_adopt(uint32_t nrows, uint32_t ncols, uint32_t nnz, uint32_t * rowptr,
 // Lossless compressed entries for the row schedule (codec.cu): columns as
 // int16 distances from the row, values as 8-bit codes into a table of the
 // distinct values or as exact floats.  Null members are not available.
+// Per-row column patterns (ColPat8, spmv_tiles.cuh): a byte per row naming
+// one of npat offset lists of kPatMax entries.
+struct RowPatterns {
+  uint8_t * code8 = nullptr;  // [nrows]
+  int32_t * off = nullptr;    // [npat * kPatMax]
+  uint32_t npat = 0;
+};
+// Built when every row has at most 7 entries and the matrix has at most 256
+// distinct patterns (checked column by column); else `out` stays empty.
+int build_row_patterns(const gb_csr & a, RowPatterns * out, cudaStream_t s);
+void free_row_patterns(RowPatterns & p);
+
 struct RowCodec {
   int16_t * col16 = nullptr;  // col - row
   uint8_t * code8 = nullptr;  // code of each value
@@ -236,6 +248,7 @@ int row_stage_for(const gb_csr & a);
 struct MixedCg;
 int mixed_create(const gb_csr * a, bool plain_entries, MixedCg ** out);
 size_t mixed_entry_bytes(const MixedCg * m);
+size_t mixed_row_bytes(const MixedCg * m);
 void mixed_destroy(MixedCg * m);
 // `cancel` (host memory, may be null): a nonzero value stops the solve
 // between graph replays with status GB_CG_CANCELLED.

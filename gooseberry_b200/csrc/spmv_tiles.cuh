@@ -497,6 +497,7 @@ struct ColU32 {  // the CSR column array
   const uint32_t * p;
   using Raw = uint32_t;
   static constexpr bool kInRange = false;  // clamp before gathering
+  static constexpr bool kPerRow = false;
   template <class P>
   __device__ __forceinline__ Raw load(uint32_t k, P pol) const { return ld_l1(p + k, pol); }
   __device__ __forceinline__ uint32_t col(Raw r, uint32_t) const { return r; }
@@ -506,8 +507,33 @@ struct ColD16 {  // column - row, 16-bit
   const int16_t * p;
   using Raw = int32_t;
   static constexpr bool kInRange = true;  // built from validated columns
+  static constexpr bool kPerRow = false;
   template <class P>
   __device__ __forceinline__ Raw load(uint32_t k, P pol) const { return ld_l1_s16(p + k, pol); }
+  __device__ __forceinline__ uint32_t col(Raw r, uint32_t row) const {
+    return row + static_cast<uint32_t>(r);
+  }
+};
+
+// Columns from a per-row pattern code.  A row's pattern is the list of its
+// columns' offsets from the diagonal; a matrix whose rows have at most
+// kPatMax entries and form at most 256 distinct patterns (structured-grid
+// stencils: 27 on a 3-D 7-point operator) stores one byte per row instead of
+// a column per entry, and the kernel keeps the pattern table (offsets, row
+// lengths still from rowptr) in shared memory.  The index compression of
+// Kourtis, Goumas and Koziris (CF 2008), taken from entries to whole rows.
+constexpr int kPatMax = 8;
+struct ColPat8 {
+  const uint8_t * code;  // [nrows] pattern of each row
+  const int32_t * off;   // [256 * kPatMax] offsets (the kernel's shared copy)
+  using Raw = int32_t;
+  static constexpr bool kInRange = true;  // built from validated columns
+  static constexpr bool kPerRow = true;
+  template <class P>
+  __device__ __forceinline__ uint32_t row_code(uint32_t i, P pol) const {
+    return ld_l1_u8(code + i, pol);
+  }
+  __device__ __forceinline__ Raw offset(uint32_t c, int j) const { return off[c * kPatMax + j]; }
   __device__ __forceinline__ uint32_t col(Raw r, uint32_t row) const {
     return row + static_cast<uint32_t>(r);
   }
@@ -536,18 +562,26 @@ struct ValCode8 {  // 8-bit code into the distinct-value table (shared memory)
 template <class IC, class VC, int STAGE>
 struct RowStageC {
   uint32_t b = 0, e = 0;
+  uint32_t code = 0;  // per-row column accessors: the row's pattern
   typename IC::Raw c[STAGE];
   typename VC::Raw v[STAGE];
 };
 
 template <class IC, class VC, int STAGE, class P>
-__device__ __forceinline__ void row_stage_load_c(RowStageC<IC, VC, STAGE> & s, const IC & ic,
-    const VC & vc, P pol) {
+__device__ __forceinline__ void row_stage_load_c(RowStageC<IC, VC, STAGE> & s, uint32_t i,
+    const IC & ic, const VC & vc, P pol) {
+  if constexpr (IC::kPerRow) {  // the offsets are read from the table when gathering
+    s.code = ic.row_code(i, pol);
 #pragma unroll
-  for (int j = 0; j < STAGE; ++j) {
-    if (s.b + j < s.e) {
-      s.c[j] = ic.load(s.b + j, pol);
-      s.v[j] = vc.load(s.b + j, pol);
+    for (int j = 0; j < STAGE; ++j)
+      if (s.b + j < s.e) s.v[j] = vc.load(s.b + j, pol);
+  } else {
+#pragma unroll
+    for (int j = 0; j < STAGE; ++j) {
+      if (s.b + j < s.e) {
+        s.c[j] = ic.load(s.b + j, pol);
+        s.v[j] = vc.load(s.b + j, pol);
+      }
     }
   }
 }
@@ -564,7 +598,7 @@ __device__ __forceinline__ void spmv_row_loop_c(uint32_t first, uint32_t end, ui
   cur.b = __ldg(rowptr + first);
   cur.e = __ldg(rowptr + first + 1);
   typename Out::Pre cur_pre = out.pre(first);
-  row_stage_load_c(cur, ic, vc, pol_matrix);
+  row_stage_load_c(cur, first, ic, vc, pol_matrix);
   uint32_t nb = 0, ne = 0;
   if (first + step < end) {
     nb = __ldg(rowptr + first + step);
@@ -579,7 +613,7 @@ __device__ __forceinline__ void spmv_row_loop_c(uint32_t first, uint32_t end, ui
       nxt.b = nb;
       nxt.e = ne;
       nxt_pre = out.pre(i1);
-      row_stage_load_c(nxt, ic, vc, pol_matrix);
+      row_stage_load_c(nxt, i1, ic, vc, pol_matrix);
     }
     if (i2 < end) {
       nb = __ldg(rowptr + i2);
@@ -590,7 +624,9 @@ __device__ __forceinline__ void spmv_row_loop_c(uint32_t first, uint32_t end, ui
 #pragma unroll
     for (int j = 0; j < STAGE; ++j) {
       if (cur.b + j < cur.e) {
-        const uint32_t c = ic.col(cur.c[j], i);
+        uint32_t c;
+        if constexpr (IC::kPerRow) c = ic.col(ic.offset(cur.code, j), i);
+        else c = ic.col(cur.c[j], i);
         xv[j] = gather(IC::kInRange ? c : min(c, cmax), pol_x);
       }
     }
@@ -599,11 +635,14 @@ __device__ __forceinline__ void spmv_row_loop_c(uint32_t first, uint32_t end, ui
     for (int j = 0; j < STAGE; ++j)
       if (cur.b + j < cur.e)
         sum = add_rn(sum, mul_rn(vc.template value<Acc>(cur.v[j]), xv[j]));
-    for (uint32_t k = cur.b + STAGE; k < cur.e; ++k)  // long-row tail
-      sum = add_rn(sum, mul_rn(vc.template value<Acc>(vc.load(k, pol_matrix)),
-                               gather(IC::kInRange ? ic.col(ic.load(k, pol_matrix), i)
-                                                   : min(ic.col(ic.load(k, pol_matrix), i), cmax),
-                                      pol_x)));
+    if constexpr (!IC::kPerRow) {  // pattern rows fit the stage: no tail
+      for (uint32_t k = cur.b + STAGE; k < cur.e; ++k)  // long-row tail
+        sum = add_rn(sum, mul_rn(vc.template value<Acc>(vc.load(k, pol_matrix)),
+                                 gather(IC::kInRange ? ic.col(ic.load(k, pol_matrix), i)
+                                                     : min(ic.col(ic.load(k, pol_matrix), i),
+                                                           cmax),
+                                        pol_x)));
+    }
     out.row_pre(i, sum, cur_pre);
     cur = nxt;
     cur_pre = nxt_pre;

@@ -347,10 +347,17 @@ GOOSEBERRY_API int gb_cg_profile(gb_cg_t * s, const double * b, size_t iteration
     double * ms, size_t ms_len, size_t * nkernels, gb_stream_t stream);
 
 /* Bytes per matrix entry the solver's SpMV streams: 12 for the plain arrays
- * (4-byte column, 8-byte value), down to 3 for 16-bit columns with 8-bit value
- * codes (see GB_CG_PLAIN_ENTRIES), 8 for the mixed solver's float values.
- * No reference counterpart. */
+ * (4-byte column, 8-byte value); 2 + the value bytes with 16-bit column
+ * distances; for MIXED the float value alone when the columns are a pattern
+ * byte per row (rows of at most 7 entries forming at most 256 distinct lists
+ * of column offsets from the diagonal: stencils); F64 values as 8-bit codes
+ * (1), exact floats (4) or doubles (8) (see GB_CG_PLAIN_ENTRIES).  No
+ * reference counterpart. */
 GOOSEBERRY_API int gb_cg_entry_bytes(const gb_cg_t * s, size_t * bytes);
+
+/* Bytes per row the solver's SpMV streams besides the entries: 4 (rowptr), 5
+ * with a column-pattern byte.  No reference counterpart. */
+GOOSEBERRY_API int gb_cg_row_bytes(const gb_cg_t * s, size_t * bytes);
 
 /* ---- batched solve server (continuous batching) ---------------------------- */
 

@@ -44,27 +44,77 @@ def float_exact(A):
                  A.rowval.astype(np.float32).astype(np.float64))
 
 
+def banded(n, offsets, seed):
+    """A symmetric diagonally dominant matrix with the given diagonals: its
+    rows have only a few distinct column patterns until the band is wider than
+    256 patterns allow, then 16-bit distances take over."""
+    rng = np.random.default_rng(seed)
+    rows, cols, vals = [], [], []
+    for d in offsets:
+        i = np.arange(max(0, -d), min(n, n - d))
+        rows.append(i)
+        cols.append(i + d)
+        vals.append(-rng.uniform(0.1, 1.0, len(i)))
+    r = np.concatenate(rows)
+    c = np.concatenate(cols)
+    v = np.concatenate(vals)
+    keep = r < c
+    r, c, v = r[keep], c[keep], v[keep]
+    d = np.ones(n)
+    np.add.at(d, r, -v)
+    np.add.at(d, c, -v)
+    return _csr(n, np.concatenate([r, c, np.arange(n)]), np.concatenate([c, r, np.arange(n)]),
+                np.concatenate([v, v, d + 1.0]))
+
+
+def many_patterns(n, seed):
+    """Rows of up to 7 entries whose column offsets are drawn per row: far
+    more than 256 distinct patterns, all within 16-bit distance."""
+    rng = np.random.default_rng(seed)
+    rows, cols = [np.arange(n)], [np.arange(n)]
+    for k in range(3):
+        off = rng.integers(1, 3000, n)
+        j = np.arange(n) + off
+        ok = j < n
+        rows += [np.arange(n)[ok], j[ok]]
+        cols += [j[ok], np.arange(n)[ok]]
+    r = np.concatenate(rows)
+    c = np.concatenate(cols)
+    e = np.unique(np.stack([r, c], 1), axis=0)
+    r, c = e[:, 0], e[:, 1]
+    v = np.where(r == c, 0.0, -rng.uniform(0.1, 1.0, len(r)))
+    v = np.where(r < c, v, 0.0)
+    # symmetric values: take the upper triangle's
+    up = {(a, b): w for a, b, w in zip(r, c, v) if a < b}
+    v = np.array([up[(a, b)] if a < b else (up[(b, a)] if a > b else 0.0)
+                  for a, b in zip(r, c)])
+    d = np.zeros(n)
+    np.add.at(d, r, -v)
+    v = np.where(r == c, d[r] + 1.0, v)
+    return _csr(n, r, c, v)
+
+
 CASES = {
-    # name: (matrix builder, expected bytes per entry)
-    "laplace64": (lambda: W.laplacian_2d(64), 3),           # 16-bit columns, value codes
-    "diffusion2d": (lambda: W.diffusion_2d(48, seed=5), 10),  # 16-bit columns, doubles
-    "diffusion2d_f32": (lambda: float_exact(W.diffusion_2d(48, seed=6)), 6),
-    "graph": (lambda: graph_laplacian(40000, 4, 7), 5),         # 32-bit columns, codes
-    "graph_weighted": (lambda: graph_laplacian(40000, 4, 8, weights=True), 12),
+    # name: (matrix builder, expected bytes per entry, per row)
+    "laplace64": (lambda: W.laplacian_2d(64), 3, 4),           # 16-bit columns, value codes
+    "diffusion2d": (lambda: W.diffusion_2d(48, seed=5), 10, 4),  # 16-bit columns, doubles
+    "diffusion2d_f32": (lambda: float_exact(W.diffusion_2d(48, seed=6)), 6, 4),
+    "graph": (lambda: graph_laplacian(40000, 4, 7), 5, 4),      # 32-bit columns, codes
+    "graph_weighted": (lambda: graph_laplacian(40000, 4, 8, weights=True), 12, 4),
 }
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_compressed_entries_are_bit_identical(name):
     import torch
-    build, want_bytes = CASES[name]
+    build, want_bytes, want_row = CASES[name]
     A = build()
     M = gb.CsrMatrix.from_host(A)
     M.set_schedule(gb.SCHED_ROW)
     S = gb.CgSolver(M)
     P = gb.CgSolver(M, plain_entries=True)
-    assert S.entry_bytes() == want_bytes
-    assert P.entry_bytes() == 12
+    assert (S.entry_bytes(), S.row_bytes()) == (want_bytes, want_row)
+    assert (P.entry_bytes(), P.row_bytes()) == (12, 4)
     b = torch.from_numpy(W.rhs(A.nrows, 9)).cuda()
     for tol, niter in ((1e-10, 0), (1e-30, 25)):
         x1, r1 = S.solve(b, tol=tol, niter=niter)
@@ -77,17 +127,24 @@ def test_compressed_entries_are_bit_identical(name):
     M.close()
 
 
-def test_mixed_solver_16bit_columns_are_bit_identical():
-    """The mixed solver's FP32 SpMV over 16-bit column distances gives the
-    same iterates, refinements and solution as over the plain columns."""
+@pytest.mark.parametrize("name,want", [("diffusion3d", (4, 5)), ("diffusion2d", (4, 5)),
+                                       ("band", (4, 5)), ("many_patterns", (6, 4))])
+def test_mixed_solver_compressed_columns_are_bit_identical(name, want):
+    """The mixed solver's FP32 SpMV over row patterns (stencils and bands: a
+    byte per row naming one of at most 256 lists of column offsets) or, past
+    that, 16-bit column distances gives the same iterates, refinements and
+    solution as over the plain columns."""
     import torch
-    A = W.diffusion_3d(24, seed=11)
+    A = {"diffusion3d": lambda: W.diffusion_3d(24, seed=11),
+         "diffusion2d": lambda: W.diffusion_2d(70, seed=12),
+         "band": lambda: banded(5000, [-200, -3, -1, 0, 1, 3, 200], 8),
+         "many_patterns": lambda: many_patterns(20000, 10)}[name]()
     M = gb.CsrMatrix.from_host(A, f64=True, f32=True)
     M.set_schedule(gb.SCHED_ROW)
     M.set_schedule(gb.SCHED_ROW, f32=True)
     S = gb.CgSolver(M, gb.CG_MIXED)
     P = gb.CgSolver(M, gb.CG_MIXED, plain_entries=True)
-    assert S.entry_bytes() == 6 and P.entry_bytes() == 8
+    assert (S.entry_bytes(), S.row_bytes()) == want and P.entry_bytes() == 8
     b = torch.from_numpy(W.rhs(A.nrows, 12)).cuda()
     x1, r1 = S.solve(b, tol=1e-10)
     x2, r2 = P.solve(b, tol=1e-10)
