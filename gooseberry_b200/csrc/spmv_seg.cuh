@@ -62,23 +62,37 @@ struct SegView {
 
 // ---- 128-bit streaming loads --------------------------------------------------
 
+#ifndef GB_SEG_STREAM_HINT
+#define GB_SEG_STREAM_HINT 0
+#endif
+#if GB_SEG_STREAM_HINT
+#define GB_SEG_LD "ld.global.nc.L1::no_allocate.L2::cache_hint"
+#define GB_SEG_POL , "l"(policy_evict_first())
+#define GB_SEG_POLA ", %5;"
+#define GB_SEG_POLB ", %3;"
+#else
+#define GB_SEG_LD "ld.global.nc.L1::no_allocate"
+#define GB_SEG_POL
+#define GB_SEG_POLA ";"
+#define GB_SEG_POLB ";"
+#endif
 __device__ __forceinline__ void ld_stream4(const uint32_t * p, uint32_t * o) {
-  asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0, %1, %2, %3}, [%4];"
+  asm volatile(GB_SEG_LD ".v4.u32 {%0, %1, %2, %3}, [%4]" GB_SEG_POLA
                : "=r"(o[0]), "=r"(o[1]), "=r"(o[2]), "=r"(o[3])
-               : "l"(p));
+               : "l"(p) GB_SEG_POL);
 }
 __device__ __forceinline__ void ld_stream4(const double * p, double * o) {
-  asm volatile("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];"
+  asm volatile(GB_SEG_LD ".v2.f64 {%0, %1}, [%2]" GB_SEG_POLB
                : "=d"(o[0]), "=d"(o[1])
-               : "l"(p));
-  asm volatile("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];"
+               : "l"(p) GB_SEG_POL);
+  asm volatile(GB_SEG_LD ".v2.f64 {%0, %1}, [%2]" GB_SEG_POLB
                : "=d"(o[2]), "=d"(o[3])
-               : "l"(p + 2));
+               : "l"(p + 2) GB_SEG_POL);
 }
 __device__ __forceinline__ void ld_stream4(const float * p, float * o) {
-  asm volatile("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+  asm volatile(GB_SEG_LD ".v4.f32 {%0, %1, %2, %3}, [%4]" GB_SEG_POLA
                : "=f"(o[0]), "=f"(o[1]), "=f"(o[2]), "=f"(o[3])
-               : "l"(p));
+               : "l"(p) GB_SEG_POL);
 }
 
 // K consecutive entries from position q (a multiple of 4) of a stream, the
