@@ -731,8 +731,10 @@ def serving_extra(nreq=300, seed=5, rtol=1e-10, pool=16 << 30, slots=256, ips=16
     untimed pass that grows the server to its working size), then a live run
     under Poisson arrivals at `load` x the one-at-a-time arm's saturated rate,
     the same arrival times for every arm, with p50/p99 latency from arrival
-    to result.  For context, the drop-in gooseberry_cgd_f64 (upload, solve,
-    download per request) one at a time at saturation."""
+    to result.  For context (streams of up to 1000 requests), the drop-in
+    gooseberry_cgd_f64 (upload, solve, download per request) one at a time
+    at saturation.  Each server's stats (device time of its graph replays,
+    host time per step and in submit, tile autotuner runs) come with it."""
     import gooseberry_b200 as gb
     from gooseberry_b200 import workloads as W
     sides = W.serving_sides(nreq, seed)
@@ -769,6 +771,7 @@ def serving_extra(nreq=300, seed=5, rtol=1e-10, pool=16 << 30, slots=256, ips=16
             worst = max(worst, float(np.linalg.norm(b - A.to_scipy() @ r.x) /
                                      np.linalg.norm(b)))
         out[name] = {"solves_per_s_saturated": len(res) / makespan,
+                     "server_stats_saturated": srv.stats(),
                      "converged": sum(r.status == "converged" for r in res),
                      "worst_true_rel_residual": worst,
                      "iterations_median": float(np.median([r.iterations for r in res]))}
@@ -784,7 +787,7 @@ def serving_extra(nreq=300, seed=5, rtol=1e-10, pool=16 << 30, slots=256, ips=16
                               "converged_live": sum(r.status == "converged" for r in got)})
     for srv in servers.values():
         srv.close()
-    if dropin:  # context: the drop-in, one request at a time (upload, solve, download)
+    if dropin and nreq <= 1000:  # context: the drop-in, one request at a time
         for k, A, b in sorted(reqs, key=lambda q: q[1].nrows)[::10]:
             gb.cgd(A.rowptr, A.rowind, A.rowval, b, rtol * float(np.linalg.norm(b)), 0)
         t0 = time.perf_counter()

@@ -145,6 +145,8 @@ SIGNATURES = {
     "gb_cg_cancel": (_i, [_vp]),
     "gb_cg_set_barrier_fault": (_i, [_vp, C.c_int, C.c_uint]),
     "gb_server_cancel": (_i, [_vp, C.c_uint64]),
+    "gb_server_stats": (_i, [_vp, _vp]),
+    "gb_server_tuned_tile_rows": (_i, [C.c_int, C.c_uint32, C.c_uint32, _vp]),
     "gb_server_create": (_i, [_vp, _vp]),
     "gb_server_destroy": (_i, [_vp]),
     "gb_server_submit": (_i, [_vp, C.c_uint64, _u32, _vp, _vp, _vp, _vp, _vp, _d, _sz]),
@@ -712,7 +714,12 @@ class CgSolver:
 
 class _ServerConfig(C.Structure):
     _fields_ = [("pool_bytes", C.c_size_t), ("max_slots", C.c_uint32), ("mode", C.c_int),
-                ("iters_per_step", C.c_uint32)]
+                ("iters_per_step", C.c_uint32), ("tile_rows", C.c_uint32)]
+
+
+class _ServerStats(C.Structure):
+    _fields_ = [("steps", C.c_size_t), ("gpu_ms", C.c_double), ("wait_ms", C.c_double),
+                ("host_ms", C.c_double), ("submit_ms", C.c_double), ("tunings", C.c_size_t)]
 
 
 class _ServerResult(C.Structure):
@@ -735,13 +742,22 @@ class ServerResult:
     x: np.ndarray
 
 
+def server_tuned_tile_rows(mode: int, n: int, max_row_nnz: int) -> int:
+    """The serving tile autotuner's cached tile size for requests of this
+    class (``gb_server_tuned_tile_rows``); 0 when not tuned yet."""
+    v = C.c_uint32(0)
+    _check(lib().gb_server_tuned_tile_rows(int(mode), int(n), int(max_row_nnz),
+                                           C.addressof(v)), "gb_server_tuned_tile_rows")
+    return int(v.value)
+
+
 class Server:
     """Continuous-batching CG server (``gb_server_t``): submit host CSR
     systems, call ``step()`` repeatedly, collect results with ``poll()``."""
 
     def __init__(self, pool_bytes: int = 16 << 30, max_slots: int = 128,
-                 mode: int = CG_MIXED, iters_per_step: int = 16):
-        cfg = _ServerConfig(pool_bytes, max_slots, mode, iters_per_step)
+                 mode: int = CG_MIXED, iters_per_step: int = 16, tile_rows: int = 0):
+        cfg = _ServerConfig(pool_bytes, max_slots, mode, iters_per_step, tile_rows)
         h = C.c_void_p()
         _check(lib().gb_server_create(C.addressof(cfg), C.addressof(h)), "gb_server_create")
         self._h = h
@@ -794,6 +810,14 @@ class Server:
 
     def clock(self) -> float:
         return float(lib().gb_server_clock(self._h))
+
+    def stats(self) -> dict:
+        """Where the server's time went (``gb_server_stats``): graph replays and
+        their device ms, host ms waiting for them and doing the rest of each
+        step, host ms in submit, tile autotuner runs."""
+        st = _ServerStats()
+        _check(lib().gb_server_stats(self._h, C.addressof(st)), "gb_server_stats")
+        return {f: getattr(st, f) for f, _ in _ServerStats._fields_}
 
     def drain(self, timeout_s: float = 600.0):
         """Step until every submitted request is reported."""

@@ -46,6 +46,8 @@
 #include <cstring>
 #include <deque>
 #include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "gb_internal.h"
@@ -68,7 +70,7 @@ constexpr int kSrvThreads = kSrvCompute + 32;       // + the control warp
 #define GB_SRV_ROW_STAGE 5
 #endif
 #ifndef GB_SRV_TILE_ROWS
-#define GB_SRV_TILE_ROWS 2048
+#define GB_SRV_TILE_ROWS 2048  // tile rows when the autotuner cannot run
 #endif
 constexpr int kSrvMinBlocks = GB_SRV_MIN_BLOCKS;
 constexpr int kSrvMaxRegs = GB_SRV_MAX_REGS;  // 3 CTAs of 288 threads per SM at 72
@@ -637,8 +639,10 @@ struct gb_server {
   bool dirty = false;
   cudaStream_t stream = nullptr;
   cudaGraphExec_t graph = nullptr;
+  cudaEvent_t step_start = nullptr;
   cudaEvent_t step_done = nullptr;
   bool inflight = false;
+  gb_server_stats_t stats{};
 };
 
 namespace gb {
@@ -690,6 +694,7 @@ void destroy_server(gb_server * s) {
   if (s->stream) cudaStreamSynchronize(s->stream);
   if (s->graph) cudaGraphExecDestroy(s->graph);
   if (s->step_done) cudaEventDestroy(s->step_done);
+  if (s->step_start) cudaEventDestroy(s->step_start);
   if (s->stream) cudaStreamDestroy(s->stream);
   cudaFree(s->pool);
   cudaFree(s->d_slots);
@@ -708,6 +713,9 @@ int create_server(const gb_server_config_t & cfg, gb_server * s) {
   GB_CHECK_INPUT(cfg.mode == GB_CG_MIXED || cfg.mode == GB_CG_F64, "mode must be GB_CG_MIXED or GB_CG_F64");
   GB_CHECK_INPUT(cfg.iters_per_step >= 1 && cfg.iters_per_step <= 1024,
       "iters_per_step must be in [1, 1024]");
+  GB_CHECK_INPUT(cfg.tile_rows == 0 || (cfg.tile_rows >= 256 && cfg.tile_rows <= 65536 &&
+                                        (cfg.tile_rows & (cfg.tile_rows - 1)) == 0),
+      "tile_rows must be 0 (autotuned) or a power of two in [256, 65536]");
   s->cfg = cfg;
   s->mixed = cfg.mode == GB_CG_MIXED;
   s->t0 = std::chrono::steady_clock::now();
@@ -737,7 +745,8 @@ int create_server(const gb_server_config_t & cfg, gb_server * s) {
   GB_CUDA_TRY(cudaMalloc(&s->d_part, 2 * kMaxTiles * sizeof(double2)));
   s->slots.resize(cfg.max_slots);
   GB_CUDA_TRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
-  GB_CUDA_TRY(cudaEventCreateWithFlags(&s->step_done, cudaEventDisableTiming));
+  GB_CUDA_TRY(cudaEventCreate(&s->step_start));
+  GB_CUDA_TRY(cudaEventCreate(&s->step_done));
   GB_TRY(capture_graph(*s));
   return GOOSEBERRY_SUCCESS;
 }
@@ -750,6 +759,8 @@ size_t footprint(bool mixed, uint32_t n, uint32_t nnz) {
   if (mixed) b += align256(4ull * nnz) /* val32 */ + align256(8ull * n) /* x1 */;
   return b;
 }
+
+int tile_rows_for(gb_server & s, const Request & q, uint32_t maxrow, uint32_t * out);
 
 int submit(gb_server & s, uint64_t id, dim_t n, const ind_t * rowptr, const dim_t * rowind,
     const double * rowval, const double * b, double * x_out, double tol_rel, size_t niter) {
@@ -766,23 +777,26 @@ int submit(gb_server & s, uint64_t id, dim_t n, const ind_t * rowptr, const dim_
   q.t_submit = now_s(s);
   q.rowptr.assign(rowptr, rowptr + n + 1);
   GB_CHECK_INPUT(q.rowptr[0] == 0, "rowptr[0] must be 0");
+  uint32_t maxrow = 0;
   for (uint32_t r = 0; r < n; ++r) {
     GB_CHECK_INPUT(q.rowptr[r + 1] >= q.rowptr[r], "rowptr decreases at row %u", r);
     const uint32_t l = q.rowptr[r + 1] - q.rowptr[r];
     GB_CHECK_INPUT(l <= kMaxRowNnz, "row %u has %u nonzeros; the solve server takes at most %u",
         r, l, kMaxRowNnz);
+    maxrow = std::max(maxrow, l);
   }
-  // row tiles of kTileRows rows (from n alone, so a solve is cut the same way
-  // whatever else is resident)
-  for (uint32_t r = 0; r < n; r += kTileRows)
-    q.tiles.push_back(SrvTile{0, r, std::min(kTileRows, n - r), 0});
-  GB_CHECK_INPUT(q.tiles.size() <= kMaxTiles, "request needs %zu tiles, more than %zu",
-      q.tiles.size(), kMaxTiles);
   q.rowind.assign(rowind, rowind + nnz);
   for (uint32_t k = 0; k < nnz; ++k)
     GB_CHECK_INPUT(q.rowind[k] < n, "column index %u out of range for %u columns", q.rowind[k], n);
   q.val64.assign(rowval, rowval + nnz);
   q.b.assign(b, b + n);
+  // row tiles (from the request alone, so a solve is cut the same way
+  // whatever else is resident)
+  uint32_t T = 0;
+  GB_TRY(tile_rows_for(s, q, maxrow, &T));
+  const size_t ntiles = (static_cast<size_t>(n) + T - 1) / T;
+  GB_CHECK_INPUT(ntiles <= kMaxTiles, "request needs %zu tiles, more than %zu", ntiles, kMaxTiles);
+  for (uint32_t r = 0; r < n; r += T) q.tiles.push_back(SrvTile{0, r, std::min(T, n - r), 0});
   q.bytes = footprint(s.mixed, n, nnz);
   GB_CHECK_INPUT(q.bytes <= s.cfg.pool_bytes, "request needs %zu bytes of device memory, "
       "the pool holds %zu", q.bytes, s.cfg.pool_bytes);
@@ -871,6 +885,194 @@ int admit(gb_server & s, Request & q, uint32_t k) {
   return GOOSEBERRY_SUCCESS;
 }
 
+// ---- the tile autotuner ------------------------------------------------------------
+//
+// Key: server mode, the request's longest row (rows of up to 5, 7, 15, 63 or
+// 255 entries) and log2 of its row count.  A new key is tuned on the spot:
+// the request is copied into a batch of R replicas (about 8M rows, at most
+// 64), each with its own Krylov vectors (the matrix is shared), and for each
+// candidate size the batch runs an INIT pair, one untimed CG pair and then
+// kTuneIters CG iterations of both kernels, timed with CUDA events; the
+// fastest size is cached for the process.
+
+struct TileKey {
+  bool mixed;
+  uint32_t row_class, log2n;
+  bool operator<(const TileKey & o) const {
+    return std::tie(mixed, row_class, log2n) < std::tie(o.mixed, o.row_class, o.log2n);
+  }
+};
+std::mutex g_tile_mu;
+std::map<TileKey, uint32_t> g_tile_cache;
+constexpr int kTuneIters = 6;
+
+TileKey tile_key(bool mixed, uint32_t n, uint32_t maxrow) {
+  const uint32_t rc = maxrow <= 5 ? 5 : maxrow <= 7 ? 7 : maxrow <= 15 ? 15 : maxrow <= 63 ? 63
+                                                                                      : 255;
+  uint32_t lg = 0;
+  while ((2u << lg) <= n && lg < 31) ++lg;
+  return TileKey{mixed, rc, lg};
+}
+
+uint32_t tuned_tile_rows(bool mixed, uint32_t n, uint32_t maxrow) {
+  std::lock_guard<std::mutex> lock(g_tile_mu);
+  auto it = g_tile_cache.find(tile_key(mixed, n, maxrow));
+  return it == g_tile_cache.end() ? 0u : it->second;
+}
+
+// Times the candidate tile sizes on replicas of request q (see above).
+int tune_tile_rows(gb_server & s, const Request & q, uint32_t * best) {
+  const uint32_t n = q.n, nnz = q.nnz;
+  std::vector<uint32_t> cands;
+  for (uint32_t t = 1024; t <= 16384; t <<= 1) {
+    cands.push_back(t);
+    if (t >= n) break;
+  }
+  *best = cands.front();
+  if (cands.size() == 1) return GOOSEBERRY_SUCCESS;
+  const uint32_t R = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(64,
+      8000000ull / n)));
+  const size_t t = s.mixed ? 4 : 8;
+  const size_t mat = align256(4ull * (n + 1)) + align256(4ull * nnz) + align256(8ull * nnz) +
+                     align256(8ull * n) + (s.mixed ? align256(4ull * nnz) : 0);
+  const size_t per = align256(8ull * n) * (s.mixed ? 2 : 1) + 5 * align256(t * n);
+  const size_t max_tiles = static_cast<size_t>(R) * ((n + 1023) / 1024);
+  const size_t meta = align256(R * sizeof(SrvSlot)) + align256(max_tiles * sizeof(SrvTile)) +
+                      align256(2 * max_tiles * sizeof(double2)) + 256;
+  char * mem = nullptr;
+  GB_TRY(dev_alloc(&mem, mat + R * per + meta));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = GOOSEBERRY_SUCCESS;
+  auto fail = [&](cudaError_t e) {
+    set_error("tile autotuning failed: %s", cudaGetErrorString(e));
+    rc = GOOSEBERRY_ERROR_UNKNOWN;
+  };
+  size_t at = 0;
+  uint32_t * rp = carve<uint32_t>(mem, at, n + 1);
+  uint32_t * ri = carve<uint32_t>(mem, at, nnz);
+  double * v64 = carve<double>(mem, at, nnz);
+  double * bb = carve<double>(mem, at, n);
+  float * v32 = s.mixed ? carve<float>(mem, at, nnz) : nullptr;
+  std::vector<SrvSlot> hs(R);
+  for (uint32_t k = 0; k < R; ++k) {
+    SrvSlot & S = hs[k];
+    std::memset(&S, 0, sizeof(S));
+    S.rowptr = rp;
+    S.rowind = ri;
+    S.val64 = v64;
+    S.val32 = v32;
+    S.b = bb;
+    S.x0 = carve<double>(mem, at, n);
+    S.x1 = s.mixed ? carve<double>(mem, at, n) : nullptr;
+    for (void ** v : {&S.y, &S.r, &S.p0, &S.p1, &S.ap}) {
+      *v = mem + at;
+      at += align256(t * n);
+    }
+    S.n = n;
+  }
+  SrvSlot * d_slots = carve<SrvSlot>(mem, at, R);
+  SrvTile * d_tiles = carve<SrvTile>(mem, at, max_tiles);
+  double2 * d_part = carve<double2>(mem, at, 2 * max_tiles);
+  uint32_t * d_nt = carve<uint32_t>(mem, at, 1);
+  cudaStream_t st = s.stream;
+  cudaError_t e = cudaMemcpyAsync(rp, q.rowptr.data(), 4ull * (n + 1), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && nnz)
+    e = cudaMemcpyAsync(ri, q.rowind.data(), 4ull * nnz, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && nnz)
+    e = cudaMemcpyAsync(v64, q.val64.data(), 8ull * nnz, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(bb, q.b.data(), 8ull * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  if (e != cudaSuccess) fail(e);
+  if (rc == GOOSEBERRY_SUCCESS && s.mixed && nnz) rc = launch_round_f32(v64, v32, nnz, st);
+  SrvDev d;
+  d.slots = d_slots;
+  d.tiles = d_tiles;
+  d.ntiles = d_nt;
+  d.pa = d_part;
+  d.pb = d_part + max_tiles;
+  std::vector<SrvTile> tiles;
+  float best_ms = 1e30f;
+  for (uint32_t T : cands) {
+    if (rc != GOOSEBERRY_SUCCESS) break;
+    tiles.clear();
+    for (uint32_t k = 0; k < R; ++k) {
+      SrvSlot & S = hs[k];
+      S.tile0 = static_cast<uint32_t>(tiles.size());
+      for (uint32_t r = 0; r < n; r += T) tiles.push_back(SrvTile{k, r, std::min(T, n - r), 0});
+      S.ntiles = static_cast<uint32_t>(tiles.size()) - S.tile0;
+      S.tol_rel = 0.0;  // never converges within the trial
+      S.niter = ~0ull;
+      S.live = 1;
+      S.done = 0;
+      S.a_work = kWorkInit;
+      S.b_work = kWorkIdle;
+      S.status = GB_CG_MAXITER;
+      S.ticket_a = S.ticket_b = 0;
+    }
+    const uint32_t nt = static_cast<uint32_t>(tiles.size());
+    e = cudaMemcpyAsync(d_slots, hs.data(), R * sizeof(SrvSlot), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d_tiles, tiles.data(), nt * sizeof(SrvTile), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d_nt, &nt, sizeof(uint32_t), cudaMemcpyHostToDevice, st);
+    for (int k = 0; k < 2 + kTuneIters && e == cudaSuccess; ++k) {
+      if (k == 2) e = cudaEventRecord(e0, st);
+      if (e != cudaSuccess) break;
+      if (s.mixed) {
+        e = launch_k(srv_a_kernel<float, true>, s.grid_a, kSrvThreads, 0, st, false, d);
+        if (e == cudaSuccess)
+          e = launch_k(srv_b_kernel<float, true>, s.grid_b, kSrvThreads, 0, st, false, d);
+      } else {
+        e = launch_k(srv_a_kernel<double, false>, s.grid_a, kSrvThreads, 0, st, false, d);
+        if (e == cudaSuccess)
+          e = launch_k(srv_b_kernel<double, false>, s.grid_b, kSrvThreads, 0, st, false, d);
+      }
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e != cudaSuccess) {
+      fail(e);
+      break;
+    }
+    if (ms < best_ms) {
+      best_ms = ms;
+      *best = T;
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaStreamSynchronize(st);  // the trial's memory is released below
+  dev_free(mem);
+  if (rc == GOOSEBERRY_SUCCESS) s.stats.tunings += 1;
+  return rc;
+}
+
+// Tile rows for request q: the configured size, else the cached or freshly
+// tuned size of its key (kTileRows when tuning cannot run).
+int tile_rows_for(gb_server & s, const Request & q, uint32_t maxrow, uint32_t * out) {
+  if (s.cfg.tile_rows) {
+    *out = s.cfg.tile_rows;
+    return GOOSEBERRY_SUCCESS;
+  }
+  const TileKey key = tile_key(s.mixed, q.n, maxrow);
+  {
+    std::lock_guard<std::mutex> lock(g_tile_mu);
+    auto it = g_tile_cache.find(key);
+    if (it != g_tile_cache.end()) {
+      *out = it->second;
+      return GOOSEBERRY_SUCCESS;
+    }
+  }
+  uint32_t T = kTileRows;
+  GB_TRY(tune_tile_rows(s, q, &T));
+  std::lock_guard<std::mutex> lock(g_tile_mu);
+  *out = g_tile_cache.emplace(key, T).first->second;  // a racing tuner's first entry wins
+  return GOOSEBERRY_SUCCESS;
+}
+
 int cancel(gb_server & s, uint64_t id) {
   for (auto it = s.queue.begin(); it != s.queue.end(); ++it) {
     if (it->id != id) continue;
@@ -893,8 +1095,15 @@ int cancel(gb_server & s, uint64_t id) {
 }
 
 int step(gb_server & s, size_t * active, size_t * queued) {
+  const auto t_in = std::chrono::steady_clock::now();
+  double waited = 0.0;
   if (s.inflight) {
     GB_CUDA_TRY(cudaEventSynchronize(s.step_done));
+    waited = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_in)
+                 .count();
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, s.step_start, s.step_done) == cudaSuccess) s.stats.gpu_ms += ms;
+    s.stats.wait_ms += waited;
     s.inflight = false;
   }
   // 1. retire finished (or cancelled) solves: copy x out, free memory and
@@ -971,14 +1180,18 @@ int step(gb_server & s, size_t * active, size_t * queued) {
   for (uint32_t k = 0; k < s.cfg.max_slots; ++k) nact += s.slots[k].used ? 1 : 0;
   // 4. run the step and bring the slot table back
   if (nact) {
+    GB_CUDA_TRY(cudaEventRecord(s.step_start, s.stream));
     GB_CUDA_TRY(cudaGraphLaunch(s.graph, s.stream));
     GB_CUDA_TRY(cudaMemcpyAsync(s.h_slots, s.d_slots, s.cfg.max_slots * sizeof(SrvSlot),
         cudaMemcpyDeviceToHost, s.stream));
     GB_CUDA_TRY(cudaEventRecord(s.step_done, s.stream));
     s.inflight = true;
+    s.stats.steps += 1;
   }
   if (active) *active = nact;
   if (queued) *queued = s.queue.size();
+  s.stats.host_ms += std::chrono::duration<double, std::milli>(
+                         std::chrono::steady_clock::now() - t_in).count() - waited;
   return GOOSEBERRY_SUCCESS;
 }
 
@@ -1009,7 +1222,24 @@ int gb_server_submit(gb_server_t * s, uint64_t id, dim_t n, const ind_t * rowptr
     const dim_t * rowind, const double * rowval, const double * b, double * x_out,
     double tol_rel, size_t niter) {
   GB_CHECK_INPUT(s != nullptr, "server is NULL");
-  return gb::submit(*s, id, n, rowptr, rowind, rowval, b, x_out, tol_rel, niter);
+  const auto t0 = std::chrono::steady_clock::now();
+  const int rc = gb::submit(*s, id, n, rowptr, rowind, rowval, b, x_out, tol_rel, niter);
+  s->stats.submit_ms +=
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return rc;
+}
+
+int gb_server_stats(const gb_server_t * s, gb_server_stats_t * out) {
+  GB_CHECK_INPUT(s && out, "NULL argument");
+  *out = s->stats;
+  return GOOSEBERRY_SUCCESS;
+}
+
+int gb_server_tuned_tile_rows(int mode, uint32_t n, uint32_t max_row_nnz, uint32_t * tile_rows) {
+  GB_CHECK_INPUT(tile_rows != nullptr, "NULL argument");
+  GB_CHECK_INPUT(mode == GB_CG_MIXED || mode == GB_CG_F64, "mode must be GB_CG_MIXED or GB_CG_F64");
+  *tile_rows = gb::tuned_tile_rows(mode == GB_CG_MIXED, n, max_row_nnz);
+  return GOOSEBERRY_SUCCESS;
 }
 
 int gb_server_step(gb_server_t * s, size_t * active, size_t * queued) {

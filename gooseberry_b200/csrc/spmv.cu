@@ -383,6 +383,44 @@ spmv_tiles_kernel(const PlanView plan, const uint32_t * __restrict__ rowptr,
       plan, rowptr, rowind, val, gather, out);
 }
 
+// The row schedule in one pass, for a matrix whose rows all fit one thread's
+// register stage and whose rows all fit one wave of threads: one row per
+// thread, every entry of the row loaded at once, every gather in flight
+// together, the products summed in the reference's order with unfused
+// multiply and add (bit-identical to the pipelined row loop and to
+// blas_spmult, src/blas.c:82-91).  The whole SpMV is then three dependent
+// memory round trips (rowptr, entries, gathers) in a single wave, where the
+// pipelined loop, sized for long grid-stride runs, holds fewer threads.
+constexpr int kRow1Block = 128;
+constexpr int kRow1Stage = 12;
+template <typename V, typename Acc, class Out>
+__global__ void __launch_bounds__(kRow1Block) spmv_row1_kernel(uint32_t nrows, uint32_t ncols,
+    const uint32_t * __restrict__ rowptr, const uint32_t * __restrict__ rowind,
+    const V * __restrict__ val, const Acc * __restrict__ x, Out out) {
+  const uint32_t i = blockIdx.x * kRow1Block + threadIdx.x;
+  if (i >= nrows) return;
+  const uint32_t b = __ldg(rowptr + i), e = __ldg(rowptr + i + 1);
+  uint32_t c[kRow1Stage];
+  V v[kRow1Stage];
+#pragma unroll
+  for (int j = 0; j < kRow1Stage; ++j) {
+    if (b + j < e) {
+      c[j] = ld_l1(rowind + b + j, NoHint{});
+      v[j] = ld_l1(val + b + j, NoHint{});
+    }
+  }
+  Acc xv[kRow1Stage];
+  const uint32_t cmax = ncols - 1;
+#pragma unroll
+  for (int j = 0; j < kRow1Stage; ++j)
+    if (b + j < e) xv[j] = __ldg(x + min(c[j], cmax));
+  Acc sum = Acc(0);
+#pragma unroll
+  for (int j = 0; j < kRow1Stage; ++j)
+    if (b + j < e) sum = add_rn(sum, mul_rn(static_cast<Acc>(v[j]), xv[j]));
+  out.row(i, sum);
+}
+
 __global__ void max_index_kernel(const uint32_t * __restrict__ ind, uint32_t n,
     unsigned int * out) {
   uint32_t m = 0;
@@ -502,9 +540,35 @@ int launch_seg(const gb_csr & a, const V * val, const Gather & g, const Out & o,
   }
 }
 
+// The one-pass row kernel when the rows fit its stage and one wave holds
+// every row; *done = false leaves the launch to the pipelined row loop.
+template <typename V, typename Acc, class Gather, class Out>
+int launch_row1(const gb_csr & a, const V * val, const Gather & g, const Out & o,
+    cudaStream_t stream, bool * done) {
+  *done = false;
+  if constexpr (IsPlainGather<Gather>::value) {
+    if (a.nrows == 0 || a.plan.max_row > static_cast<uint32_t>(kRow1Stage)) return GOOSEBERRY_SUCCESS;
+    auto kern = spmv_row1_kernel<V, Acc, Out>;
+    int occ = 0;
+    GB_TRY(occupancy(reinterpret_cast<const void *>(kern), 0, &occ, kRow1Block));
+    const uint64_t wave = static_cast<uint64_t>(a.sm_count) * occ * kRow1Block;
+    if (a.nrows > wave) return GOOSEBERRY_SUCCESS;
+    kern<<<(a.nrows + kRow1Block - 1) / kRow1Block, kRow1Block, 0, stream>>>(a.nrows, a.ncols,
+        a.rowptr, a.rowind, val, g.x, o);
+    GB_CUDA_TRY(cudaGetLastError());
+    *done = true;
+  }
+  return GOOSEBERRY_SUCCESS;
+}
+
 template <typename V, typename Acc, class Gather, class Out>
 int launch_sched(const gb_csr & a, int sched, const V * val, const Gather & g,
     const Out & o, cudaStream_t stream) {
+  if (sched == GB_SCHED_ROW) {
+    bool done = false;
+    GB_TRY((launch_row1<V, Acc>(a, val, g, o, stream, &done)));
+    if (done) return GOOSEBERRY_SUCCESS;
+  }
   switch (sched) {
     case GB_SCHED_SEG: return launch_seg<V, Acc>(a, val, g, o, stream);
     case GB_SCHED_THREAD: return launch_tiles<V, Acc, SCHED_THREAD>(a, val, g, o, stream);

@@ -379,6 +379,9 @@ typedef struct gb_server_config {
   uint32_t max_slots;       /* resident solves at most                       */
   int mode;                 /* GB_CG_MIXED or GB_CG_F64                      */
   uint32_t iters_per_step;  /* CG iterations per gb_server_step (>= 1)       */
+  uint32_t tile_rows;       /* rows per work tile (a power of two in
+                               [256, 65536]), or 0: chosen per request by the
+                               tile autotuner (gb_server_tuned_tile_rows)    */
 } gb_server_config_t;
 
 typedef struct gb_server_result {
@@ -423,6 +426,37 @@ GOOSEBERRY_API int gb_server_cancel(gb_server_t * s, uint64_t id);
 
 /* Seconds since the server was created (the clock of the result stamps). */
 GOOSEBERRY_API double gb_server_clock(const gb_server_t * s);
+
+/* Where a server's time went. */
+typedef struct gb_server_stats {
+  size_t steps;             /* graph replays launched                        */
+  double gpu_ms;            /* their device time (CUDA events)               */
+  double wait_ms;           /* host time in gb_server_step waiting for the
+                               previous replay to finish                     */
+  double host_ms;           /* the rest of gb_server_step: retiring, admitting,
+                               the tile list and slot table upload           */
+  double submit_ms;         /* host time in gb_server_submit (copies, checks,
+                               tile autotuning)                              */
+  size_t tunings;           /* tile autotuner runs this server started       */
+} gb_server_stats_t;
+GOOSEBERRY_API int gb_server_stats(const gb_server_t * s, gb_server_stats_t * out);
+
+/*
+ * The tile autotuner.  The batched kernels walk a list of row tiles; a
+ * request's rows are cut into tiles when it is submitted, from the request
+ * alone, so its arithmetic (and result bits) do not depend on what else is
+ * resident.  With tile_rows = 0 the size comes from a process-wide cache
+ * keyed on the request's row-length class -- its longest row (rows of up to
+ * 5, 7, 15, 63 or 255 entries), log2 of its row count and the server mode.
+ * A key met for the first time is tuned on the spot: the request is
+ * replicated into a batch that fills the GPU (in memory outside the pool),
+ * and a few CG iterations of that batch are timed for each candidate size
+ * (1024 to 16384 rows, no larger than the request); the fastest is cached.
+ * gb_server_tuned_tile_rows reports the cached choice for a key (0: not
+ * tuned yet).  No reference counterpart.
+ */
+GOOSEBERRY_API int gb_server_tuned_tile_rows(int mode, uint32_t n, uint32_t max_row_nnz,
+    uint32_t * tile_rows);
 
 #ifdef __cplusplus
 }

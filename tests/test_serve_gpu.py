@@ -142,3 +142,56 @@ def test_cancel_queued_and_resident_requests():
     assert r9.status == "converged" and np.array_equal(r9.x, res[1].x)
     srv.close()
     alone.close()
+
+
+def test_tile_autotuner_tunes_once_per_class_and_caches():
+    """With tile_rows = 0 a request of a row-length class met for the first
+    time is tuned (its tile size timed on a replicated batch) and the choice
+    cached for the process: later requests of the class, in this server or a
+    new one, reuse it without tuning; results still converge."""
+    # a 3-D 7-point operator of 110,592 rows: a class (longest row 7, 2^16 to
+    # 2^17 rows) that no other test submits
+    A = W.diffusion_3d(48, seed=71)
+    b = W.rhs(A.nrows, 71)
+    max_row = int(np.diff(A.rowptr.astype(np.int64)).max())
+    assert gb.server_tuned_tile_rows(gb.CG_MIXED, A.nrows, max_row) == 0
+    srv = gb.Server(pool_bytes=1 << 30, max_slots=2, mode=gb.CG_MIXED, iters_per_step=8)
+    srv.submit(0, A, b, tol=1e-10, niter=20000)
+    t = gb.server_tuned_tile_rows(gb.CG_MIXED, A.nrows, max_row)
+    assert t in (1024, 2048, 4096, 8192, 16384), t
+    assert srv.stats()["tunings"] == 1
+    srv.submit(1, A, b, tol=1e-10, niter=20000)
+    assert srv.stats()["tunings"] == 1
+    res = {r.id: r for r in srv.drain()}
+    for r in res.values():
+        assert r.status == "converged" and _rel(A, r.x, b) <= 1.05e-10
+    assert np.array_equal(res[0].x, res[1].x)
+    st = srv.stats()
+    assert st["steps"] > 0 and st["gpu_ms"] > 0 and st["submit_ms"] > 0
+    other = gb.Server(pool_bytes=1 << 30, max_slots=1, mode=gb.CG_MIXED, iters_per_step=8)
+    other.submit(2, A, b, tol=1e-10, niter=20000)
+    assert other.stats()["tunings"] == 0
+    r2 = other.drain()[0]
+    assert np.array_equal(r2.x, res[0].x)  # same tiles, same bits
+    srv.close()
+    other.close()
+
+
+@pytest.mark.parametrize("tile_rows", [256, 1024, 16384])
+def test_fixed_tile_rows(tile_rows):
+    """A configured tile size is used as given (no tuning) and the solves
+    converge; a tile size that is not a power of two in [256, 65536] is
+    refused."""
+    reqs = _requests([40, 90, 130], 500)
+    srv = gb.Server(pool_bytes=1 << 30, max_slots=3, mode=gb.CG_MIXED, iters_per_step=8,
+                    tile_rows=tile_rows)
+    for rid, A, b in reqs:
+        srv.submit(rid, A, b, tol=1e-10, niter=20000)
+    res = {r.id: r for r in srv.drain()}
+    assert srv.stats()["tunings"] == 0
+    for rid, A, b in reqs:
+        assert res[rid].status == "converged" and _rel(A, res[rid].x, b) <= 1.05e-10
+    srv.close()
+    for bad in (100, 3000, 1 << 17):
+        with pytest.raises(gb.GooseberryError):
+            gb.Server(pool_bytes=1 << 28, max_slots=1, mode=gb.CG_MIXED, tile_rows=bad)
