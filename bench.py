@@ -1074,7 +1074,10 @@ def host_cores() -> int:
 def pin_openmp() -> None:
     """OpenMP placement for the reference's CPU code: one thread per physical
     core, kept close.  Must run before the reference library is loaded (libgomp
-    reads these at start-up)."""
+    reads these at start-up).  Only the reference arm sets it: with
+    OMP_PROC_BIND set, libgomp binds the process's main thread to the first
+    core when it starts, and every host thread the library later starts from
+    that thread (tile planner, text loaders) inherits that one core."""
     os.environ.setdefault("OMP_PROC_BIND", "close")
     os.environ.setdefault("OMP_PLACES", "cores")
 
@@ -1150,13 +1153,13 @@ def main():
     ap.add_argument("--requests", type=int, default=300,
                     help="requests of the serving stream (extras / --workload serving)")
     args = ap.parse_args()
-    pin_openmp()
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
 
     if args.impl == "reference":
         if int(os.environ.get("RANK", "0")) != 0:
             return 0
+        pin_openmp()
         out = run_reference_cg(args)
         print(json.dumps(out), flush=True)
         return 0

@@ -63,7 +63,8 @@ struct SegView {
 // ---- 128-bit streaming loads --------------------------------------------------
 
 // (An evict-first L2 policy on these loads, to keep x resident against the
-// matrix stream, made the 8M-row power-law SpMV slower: 0.65 -> 0.81 ms.)
+// matrix stream, made the 8M-row power-law SpMV slower: 0.65 -> 0.81 ms; so
+// did letting them allocate in L1: 0.65 -> 0.73 ms.)
 __device__ __forceinline__ void ld_stream4(const uint32_t * p, uint32_t * o) {
   asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0, %1, %2, %3}, [%4];"
                : "=r"(o[0]), "=r"(o[1]), "=r"(o[2]), "=r"(o[3])
