@@ -73,56 +73,79 @@ struct CgStatus {
 
 // Where A finds the r.r partials: B of iteration j writes buf[j & 1]
 // (stride entries apart), the init kernel writes buf[1]; count per buffer.
+// `par` = (k + 1) & 1 for the A of iteration k, fixed when the launch is
+// enqueued (a graph chunk holds an even number of iterations and every solve
+// starts at iteration 0), so that A reads the partials, r.r of the iteration
+// before and the solver state in one round of loads.
 struct RrPartials {
   const double * buf;
   unsigned count;
   unsigned stride;
+  unsigned par;
 };
-
-// The stop flag, read once per CTA so that all of its threads agree.
-__device__ __forceinline__ bool cta_done(const CgState * st) {
-  __shared__ int s_done;
-  if (threadIdx.x == 0) s_done = *reinterpret_cast<const volatile int *>(&st->done);
-  __syncthreads();
-  return s_done != 0;
-}
 
 // Start of A for iteration k = st->iter: rr_k from the last B, beta =
 // rr_k / rr_{k-1} (0 at k = 0; rr_{k-1} as the previous A recorded it), the
 // history entry and the stop test, which the reference makes after each
 // update (src/cgd.c:115-119).  CTA 0 records the outcome.  Returns false when
-// the solve stops here.
+// the solve stops here or has stopped already.  B's partials (every thread)
+// and the state (thread 0) are loaded in one round; should `rp.par` not match
+// the iteration, the partials of the right buffer are summed again.
 __device__ __forceinline__ bool cg_a_begin(CgState * st, RrPartials rp, double * beta) {
   __shared__ double red[32];
   __shared__ double s_rr[2];
-  const unsigned long long k = *reinterpret_cast<const volatile unsigned long long *>(&st->iter);
-  const double rr = ordered_sum(rp.buf + ((k + 1) & 1) * rp.stride, rp.count, red);
+  __shared__ unsigned long long s_k;
+  __shared__ int s_stop, s_mis;
+  int done = 0;
+  unsigned long long k = 0, niter = 0, hist_len = 0, hist = 0;
+  double rr_prev = 0.0, tol = 0.0;
+  double rr = ordered_sum_with(rp.buf + rp.par * rp.stride, rp.count, red, [&] {
+    if (threadIdx.x == 0) {
+      done = __ldcg(&st->done);
+      k = __ldcg(&st->iter);
+      rr_prev = __ldcg(&st->rrk[rp.par]);
+      tol = __ldcg(&st->tol);
+      niter = __ldcg(&st->niter);
+      hist = __ldcg(reinterpret_cast<const unsigned long long *>(&st->hist));
+      hist_len = __ldcg(&st->hist_len);
+    }
+  });
+  if (threadIdx.x == 0) s_mis = ((k + 1) & 1) != rp.par;
+  __syncthreads();
+  if (s_mis) {  // parity not as enqueued: sum the other buffer
+    const unsigned q = rp.par ^ 1u;
+    rr = ordered_sum(rp.buf + q * rp.stride, rp.count, red);
+    if (threadIdx.x == 0) rr_prev = __ldcg(&st->rrk[q]);
+  }
   if (threadIdx.x == 0) {
+    int stop = done ? GB_CG_CONVERGED : -1;
+    if (!done) {
+      if (k > 0) {
+        const double rnorm = sqrt(rr);
+        if (!(rnorm == rnorm) || isinf(rnorm)) stop = GB_CG_NONFINITE;
+        else if (rnorm <= tol) stop = GB_CG_CONVERGED;
+        else if (niter && k >= niter) stop = GB_CG_MAXITER;
+        if (blockIdx.x == 0 && hist && k <= hist_len)
+          reinterpret_cast<double *>(hist)[k - 1] = rnorm;
+      }
+      if (blockIdx.x == 0) {
+        st->rr = rr;
+        st->rrk[k & 1] = rr;
+        st->kb = k;
+        if (stop >= 0) {
+          st->status = stop;
+          st->done = 1;
+        }
+      }
+    }
     s_rr[0] = rr;
-    s_rr[1] = k > 0 ? __ldcg(&st->rrk[(k + 1) & 1]) : 0.0;
+    s_rr[1] = rr_prev;
+    s_k = k;
+    s_stop = stop;
   }
   __syncthreads();
-  const double rrk = s_rr[0];
-  int stop = -1;
-  if (k > 0) {
-    const double rnorm = sqrt(rrk);
-    if (!(rnorm == rnorm) || isinf(rnorm)) stop = GB_CG_NONFINITE;
-    else if (rnorm <= st->tol) stop = GB_CG_CONVERGED;
-    else if (st->niter && k >= st->niter) stop = GB_CG_MAXITER;
-    if (blockIdx.x == 0 && threadIdx.x == 0 && st->hist && k <= st->hist_len)
-      st->hist[k - 1] = rnorm;
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    st->rr = rrk;
-    st->rrk[k & 1] = rrk;
-    st->kb = k;
-    if (stop >= 0) {
-      st->status = stop;
-      st->done = 1;
-    }
-  }
-  *beta = k > 0 ? rrk / s_rr[1] : 0.0;
-  return stop < 0;
+  *beta = s_k > 0 ? s_rr[0] / s_rr[1] : 0.0;
+  return s_stop < 0;
 }
 
 // ---- A: SpMV with fused direction update and p.Ap -----------------------------
@@ -185,7 +208,6 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED>::value) cg_a_kern
     double * __restrict__ ap, double * __restrict__ longdot,
     double * __restrict__ partial, CgState * st, RrPartials rp) {
   pdl_wait_and_release();
-  if (cta_done(st)) return;
   double beta;
   if (!cg_a_begin(st, rp, &beta)) return;
   GatherP g{r, pold, beta};
@@ -213,7 +235,6 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED_ROW>::value) cg_a_
     vc.table = s_table;
   }
   pdl_wait_and_release();
-  if (cta_done(st)) return;
   double beta;
   if (!cg_a_begin(st, rp, &beta)) return;
   GatherP g{r, pold, beta};
@@ -234,17 +255,33 @@ __global__ void __launch_bounds__(kVecBlock, kSpmvMinBlocks) cg_b_kernel(size_t 
     const double * __restrict__ longdot, unsigned nlong, double * __restrict__ partial_b,
     unsigned stride, CgState * st) {
   pdl_wait_and_release();
-  if (cta_done(st)) return;
   __shared__ double red[32];
-  __shared__ double s_pap;
-  const unsigned long long k = st->kb;
-  const double rr_cur = st->rr;
-  double tot = ordered_sum(partial_a, na, red);
+  __shared__ double s_pap, s_rr;
+  __shared__ unsigned long long s_k;
+  __shared__ int s_done;
+  // A's partials (every thread) and the state (thread 0) in one round of loads
+  int done = 0;
+  unsigned long long kb = 0;
+  double rr_st = 0.0;
+  double tot = ordered_sum_with(partial_a, na, red, [&] {
+    if (threadIdx.x == 0) {
+      done = __ldcg(&st->done);
+      kb = __ldcg(&st->kb);
+      rr_st = __ldcg(&st->rr);
+    }
+  });
   if (threadIdx.x == 0) {
-    for (unsigned q = 0; q < nlong; ++q) tot += __ldcg(longdot + q);
+    if (!done)
+      for (unsigned q = 0; q < nlong; ++q) tot += __ldcg(longdot + q);
     s_pap = tot;
+    s_rr = rr_st;
+    s_k = kb;
+    s_done = done;
   }
   __syncthreads();
+  if (s_done) return;
+  const unsigned long long k = s_k;
+  const double rr_cur = s_rr;
   const double pap = s_pap;
   if (!(pap > 0.0)) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -874,16 +911,19 @@ void destroy_cg(gb_cg * s) {
   delete s;
 }
 
-RrPartials rr_partials(const gb_cg * s) {
-  return RrPartials{s->partial_b, s->grid_b, s->pstride};
+// The partials the A of iteration k reads (B of iteration k - 1 wrote them).
+RrPartials rr_partials(const gb_cg * s, size_t k) {
+  return RrPartials{s->partial_b, s->grid_b, s->pstride, static_cast<unsigned>((k + 1) & 1)};
 }
 
-int launch_a(gb_cg * s, const double * pold, double * pnew, cudaStream_t cs, bool pdl) {
+// The A of iteration k (only its parity matters).
+int launch_a(gb_cg * s, size_t k, const double * pold, double * pnew, cudaStream_t cs,
+    bool pdl) {
   return s->use_codec
              ? launch_cg_a_codec(*s->a, s->codec, s->l2_hint, s->r, pold, pnew, s->ap,
-                   s->longdot, s->partial_a, s->st, rr_partials(s), s->grid_a, cs, pdl)
+                   s->longdot, s->partial_a, s->st, rr_partials(s, k), s->grid_a, cs, pdl)
              : launch_cg_a(*s->a, s->sched, s->l2_hint, s->r, pold, pnew, s->ap, s->longdot,
-                   s->partial_a, s->st, rr_partials(s), s->grid_a, cs, pdl);
+                   s->partial_a, s->st, rr_partials(s, k), s->grid_a, cs, pdl);
 }
 
 int launch_b(gb_cg * s, const double * pnew, cudaStream_t cs, bool pdl) {
@@ -903,7 +943,7 @@ int enqueue_chunk(gb_cg * s, int slot, cudaStream_t cs) {
   for (int k = 0; k < s->chunk && rc == GOOSEBERRY_SUCCESS; ++k) {
     const double * pold = s->p[k & 1];
     double * pnew = s->p[(k + 1) & 1];
-    rc = launch_a(s, pold, pnew, cs, k > 0);
+    rc = launch_a(s, static_cast<size_t>(k), pold, pnew, cs, k > 0);
     if (rc != GOOSEBERRY_SUCCESS) break;
     rc = launch_b(s, pnew, cs, true);
   }
@@ -1259,7 +1299,7 @@ int profile_cg(gb_cg * s, const double * b, size_t iterations, double * ms, size
     const double * pold = s->p[k & 1];
     double * pnew = s->p[(k + 1) & 1];
     cudaEventRecord(ev[3 * k], stream);
-    rc = launch_a(s, pold, pnew, stream, false);
+    rc = launch_a(s, k, pold, pnew, stream, false);
     cudaEventRecord(ev[3 * k + 1], stream);
     if (rc == GOOSEBERRY_SUCCESS) rc = launch_b(s, pnew, stream, false);
     cudaEventRecord(ev[3 * k + 2], stream);

@@ -70,6 +70,32 @@ __device__ __forceinline__ double ordered_sum(const double * partial, unsigned n
   return block_sum(acc, red);
 }
 
+// ordered_sum with `side()` called by every thread right after its first
+// batch of partial loads is issued: loads made there are in flight together
+// with the partials (one round trip instead of two).  Same sum, same order.
+template <class F>
+__device__ __forceinline__ double ordered_sum_with(const double * partial, unsigned n,
+    double * red, F && side) {
+  constexpr int U = 8;
+  double acc = 0.0;
+  bool called = false;
+  for (unsigned base = 0; base < n; base += U * blockDim.x) {
+    double v[U];
+#pragma unroll
+    for (int j = 0; j < U; ++j) {
+      const unsigned i = base + j * blockDim.x + threadIdx.x;
+      v[j] = i < n ? __ldcg(partial + i) : 0.0;
+    }
+    if (!called) {
+      side();
+      called = true;
+    }
+#pragma unroll
+    for (int j = 0; j < U; ++j) acc += v[j];
+  }
+  if (!called) side();
+  return block_sum(acc, red);
+}
 
 }  // namespace
 }  // namespace gb
