@@ -256,11 +256,15 @@ def add_scalar(v: np.ndarray, s: float) -> np.ndarray:
     return v
 
 
-def cgd(rowptr, rowind, rowval, b, error: float, niter: int, history: bool = False):
+def cgd(rowptr, rowind, rowval, b, error: float, niter: int, history: bool = False,
+        out=None):
     """Conjugate gradient with the reference's contract (``src/cgd.c:40-129``):
     x0 = 0, stop when ||r||_2 <= error (absolute) or after niter iterations.
 
-    Returns ``(x, iterations, rnorm)`` (plus the ||r|| history if asked)."""
+    ``out``: optional contiguous host array (n entries of the value type) that
+    receives x -- e.g. pinned memory, which the final device-to-host copy
+    reaches without staging.  Returns ``(x, iterations, rnorm)`` (plus the
+    ||r|| history if asked)."""
     rowval = np.ascontiguousarray(rowval)
     real = _real(rowval.dtype)
     dt = rowval.dtype
@@ -268,7 +272,13 @@ def cgd(rowptr, rowind, rowval, b, error: float, niter: int, history: bool = Fal
     rowind = np.ascontiguousarray(rowind, dtype=np.uint32)
     b = np.ascontiguousarray(b, dtype=dt)
     n = len(b)
-    x = np.zeros(n, dtype=dt)
+    if out is None:
+        x = np.zeros(n, dtype=dt)
+    else:
+        if out.dtype != dt or out.shape != (n,) or not out.flags["C_CONTIGUOUS"] \
+                or not out.flags["WRITEABLE"]:
+            raise ValueError(f"out must be a writable contiguous {dt} array of {n} entries")
+        x = out
     it = C.c_size_t(0)
     rn = C.c_double(0)
     hist = np.zeros(max(int(niter), 1), dtype=np.float64) if history else None

@@ -906,8 +906,8 @@ void destroy_cg(gb_cg * s) {
   dev_free(s->st);
   dev_free(s->cta_tiles);
   dev_free(s->sync);
-  if (s->host_status) cudaFreeHost(s->host_status);
-  if (s->cancel_h) cudaFreeHost(s->cancel_h);
+  pinned_slot_free(s->host_status);
+  pinned_slot_free(s->cancel_h);
   delete s;
 }
 
@@ -1062,10 +1062,8 @@ int create_cg(const gb_csr * a, int mode, gb_cg * s) {
   const bool plain_entries = (mode & GB_CG_PLAIN_ENTRIES) != 0;
   mode &= ~(GB_CG_PERSISTENT | GB_CG_PLAIN_ENTRIES);
   GB_CHECK_INPUT(mode == GB_CG_F64 || mode == GB_CG_MIXED, "unknown CG mode %d", mode);
-  GB_CUDA_TRY(cudaHostAlloc(reinterpret_cast<void **>(&s->cancel_h), sizeof(int),
-      cudaHostAllocMapped));
-  *s->cancel_h = 0;
-  GB_CUDA_TRY(cudaHostGetDevicePointer(reinterpret_cast<void **>(&s->cancel_d), s->cancel_h, 0));
+  GB_TRY(pinned_slot_alloc(sizeof(int), reinterpret_cast<void **>(&s->cancel_h),
+      reinterpret_cast<void **>(&s->cancel_d)));
   if (mode == GB_CG_MIXED) {
     s->a = a;
     s->mode = mode;
@@ -1125,7 +1123,8 @@ int create_cg(const gb_csr * a, int mode, gb_cg * s) {
       std::max<size_t>(a->plan.longrows.size(), 1) * sizeof(double)));
   GB_TRY(dev_alloc(&s->st, sizeof(CgState)));
   GB_CUDA_TRY(cudaMemset(s->st, 0, sizeof(CgState)));
-  GB_CUDA_TRY(cudaMallocHost(&s->host_status, 2 * sizeof(CgStatus)));
+  GB_TRY(pinned_slot_alloc(2 * sizeof(CgStatus), reinterpret_cast<void **>(&s->host_status),
+      nullptr));
   if (want_persistent) GB_TRY(setup_persistent(a, s));
   if (!s->persistent) {
     GB_CUDA_TRY(cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking));

@@ -821,7 +821,7 @@ void mixed_destroy(MixedCg * m) {
   dev_free(m->st);
   if (m->col16) dev_free(m->col16);
   free_row_patterns(m->pat);
-  if (m->host_status) cudaFreeHost(m->host_status);
+  pinned_slot_free(m->host_status);
   delete m;
 }
 
@@ -886,7 +886,8 @@ int mixed_create(const gb_csr * a, bool plain_entries, MixedCg ** out) {
       std::max<size_t>(a->plan.longrows.size(), 1) * sizeof(double)));
   GB_TRY(dev_alloc(&m->st, sizeof(MixState)));
   GB_CUDA_TRY(cudaMemset(m->st, 0, sizeof(MixState)));
-  GB_CUDA_TRY(cudaMallocHost(&m->host_status, 2 * sizeof(MixStatus)));
+  GB_TRY(pinned_slot_alloc(2 * sizeof(MixStatus), reinterpret_cast<void **>(&m->host_status),
+      nullptr));
   GB_CUDA_TRY(cudaStreamCreateWithFlags(&m->cap_stream, cudaStreamNonBlocking));
   GB_TRY(capture(m, 0));
   GB_TRY(capture(m, 1));

@@ -200,6 +200,11 @@ void scratch_free(void * p, cudaStream_t s);
 // still run (the destroy paths synchronise the device first).
 int dev_alloc(void ** p, size_t bytes);
 void dev_free(void * p);
+// A zeroed pinned host slot of at most 128 bytes that kernels can read and
+// write through *dev (cancel flags, status mirrors); free only once no work
+// that uses it can still run.
+int pinned_slot_alloc(size_t bytes, void ** host, void ** dev);
+void pinned_slot_free(void * host);
 template <typename T>
 int dev_alloc(T ** p, size_t bytes) {
   return dev_alloc(reinterpret_cast<void **>(p), bytes);

@@ -213,7 +213,7 @@ struct PrBuffers {
     dev_free(partial);
     dev_free(scal);
     dev_free(sinks);
-    if (h_err) cudaFreeHost(h_err);
+    pinned_slot_free(h_err);
     if (a) gb_csr_destroy(a);
     if (st) cudaStreamDestroy(st);
   }
@@ -250,7 +250,7 @@ int pagerank_f64(dim_t n, const ind_t * rowptr, const dim_t * rowind, const doub
   GB_TRY(dev_alloc(&B.partial, std::max(g, gs) * sizeof(double)));
   GB_TRY(dev_alloc(&B.scal, 2 * sizeof(double)));
   GB_CUDA_TRY(cudaMemsetAsync(B.scal, 0, 2 * sizeof(double), B.st));
-  GB_CUDA_TRY(cudaMallocHost(&B.h_err, sizeof(double)));
+  GB_TRY(pinned_slot_alloc(sizeof(double), reinterpret_cast<void **>(&B.h_err), nullptr));
   if (!sinks.empty()) {
     GB_TRY(dev_alloc(&B.sinks, sinks.size() * sizeof(uint32_t)));
     GB_CUDA_TRY(cudaMemcpyAsync(B.sinks, sinks.data(), sinks.size() * sizeof(uint32_t),

@@ -3,6 +3,7 @@
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
+#include <cstring>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -105,6 +106,54 @@ void dev_free(void * p) {
   DevicePool d;
   if (pool_of_current_device(&d) != GOOSEBERRY_SUCCESS) return;
   cudaFreeAsync(p, d.alloc_stream);
+}
+
+namespace {
+// Small pinned, device-mapped host slots, carved from blocks that are kept for
+// the life of the process: a mapped host allocation costs milliseconds (and
+// its free a device-wide synchronisation), far more than the solve-setup work
+// it serves.
+constexpr size_t kSlotBytes = 128;
+constexpr size_t kSlotBlockBytes = 64 * 1024;
+std::mutex g_slot_mu;
+std::vector<void *> g_slot_free;
+}  // namespace
+
+int pinned_slot_alloc(size_t bytes, void ** host, void ** dev) {
+  *host = nullptr;
+  if (dev) *dev = nullptr;
+  GB_CHECK_INPUT(bytes <= kSlotBytes, "pinned slot of %zu bytes (at most %zu)", bytes,
+      kSlotBytes);
+  void * h = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_slot_mu);
+    if (g_slot_free.empty()) {
+      void * block = nullptr;
+      GB_CUDA_TRY(cudaHostAlloc(&block, kSlotBlockBytes,
+          cudaHostAllocMapped | cudaHostAllocPortable));
+      for (size_t o = kSlotBlockBytes; o >= kSlotBytes; o -= kSlotBytes)
+        g_slot_free.push_back(static_cast<char *>(block) + o - kSlotBytes);
+    }
+    h = g_slot_free.back();
+    g_slot_free.pop_back();
+  }
+  std::memset(h, 0, kSlotBytes);
+  if (dev) {
+    const cudaError_t e = cudaHostGetDevicePointer(dev, h, 0);
+    if (e != cudaSuccess) {
+      pinned_slot_free(h);
+      set_error("cudaHostGetDevicePointer failed: %s", cudaGetErrorString(e));
+      return GOOSEBERRY_ERROR_UNKNOWN;
+    }
+  }
+  *host = h;
+  return GOOSEBERRY_SUCCESS;
+}
+
+void pinned_slot_free(void * host) {
+  if (!host) return;
+  std::lock_guard<std::mutex> lock(g_slot_mu);
+  g_slot_free.push_back(host);
 }
 
 }  // namespace gb

@@ -319,6 +319,22 @@ void free_plan(Plan & plan) {
   plan.d_seg_count = nullptr;
 }
 
+namespace {
+// The segmented part of a plan, on the device (plan.seg built on the host).
+int upload_seg(Plan & plan, cudaStream_t stream) {
+  if (plan.seg.empty()) return GOOSEBERRY_SUCCESS;
+  const size_t W = plan.seg.size() - 1;
+  GB_TRY(dev_alloc(&plan.d_seg, plan.seg.size() * sizeof(SegRange)));
+  GB_TRY(dev_alloc(&plan.d_seg_rec, 2 * W * sizeof(double)));
+  GB_TRY(dev_alloc(&plan.d_seg_count, W * sizeof(unsigned int)));
+  GB_CUDA_TRY(cudaMemcpyAsync(plan.d_seg, plan.seg.data(), plan.seg.size() * sizeof(SegRange),
+      cudaMemcpyHostToDevice, stream));
+  GB_CUDA_TRY(cudaMemsetAsync(plan.d_seg_rec, 0, 2 * W * sizeof(double), stream));
+  GB_CUDA_TRY(cudaMemsetAsync(plan.d_seg_count, 0, W * sizeof(unsigned int), stream));
+  return GOOSEBERRY_SUCCESS;
+}
+}  // namespace
+
 int upload_plan(Plan & plan, cudaStream_t stream) {
   free_plan(plan);
   const size_t nt = std::max<size_t>(plan.tiles.size(), 1);
@@ -334,16 +350,7 @@ int upload_plan(Plan & plan, cudaStream_t stream) {
     GB_CUDA_TRY(cudaMemcpyAsync(plan.d_longrows, plan.longrows.data(),
         plan.longrows.size() * sizeof(LongRowDesc), cudaMemcpyHostToDevice, stream));
   GB_CUDA_TRY(cudaMemsetAsync(plan.d_long_count, 0, nl * sizeof(unsigned int), stream));
-  if (!plan.seg.empty()) {
-    const size_t W = plan.seg.size() - 1;
-    GB_TRY(dev_alloc(&plan.d_seg, plan.seg.size() * sizeof(SegRange)));
-    GB_TRY(dev_alloc(&plan.d_seg_rec, 2 * W * sizeof(double)));
-    GB_TRY(dev_alloc(&plan.d_seg_count, W * sizeof(unsigned int)));
-    GB_CUDA_TRY(cudaMemcpyAsync(plan.d_seg, plan.seg.data(), plan.seg.size() * sizeof(SegRange),
-        cudaMemcpyHostToDevice, stream));
-    GB_CUDA_TRY(cudaMemsetAsync(plan.d_seg_rec, 0, 2 * W * sizeof(double), stream));
-    GB_CUDA_TRY(cudaMemsetAsync(plan.d_seg_count, 0, W * sizeof(unsigned int), stream));
-  }
+  GB_TRY(upload_seg(plan, stream));
   GB_CUDA_TRY(cudaStreamSynchronize(stream));  // host vectors may change later
   return GOOSEBERRY_SUCCESS;
 }
@@ -666,11 +673,43 @@ int rebuild_plan(gb_csr & a, uint32_t tile_items, cudaStream_t stream) {
   GB_CUDA_TRY(cudaStreamSynchronize(stream));
   Plan p;
   GB_TRY(build_plan(a.nrows, hrp.data(), a.nnz, tile_items, p));
-  build_seg_plan(a.nrows, hrp.data(), a.nnz, seg_max_warps(a.sm_count), p);
   GB_TRY(upload_plan(p, stream));
+  // the segmented plan does not depend on the tile size: keep it
+  p.seg = std::move(a.plan.seg);
+  std::swap(p.d_seg, a.plan.d_seg);
+  std::swap(p.d_seg_rec, a.plan.d_seg_rec);
+  std::swap(p.d_seg_count, a.plan.d_seg_count);
   free_plan(a.plan);
   a.plan = std::move(p);
   return GOOSEBERRY_SUCCESS;
+}
+
+// The segmented plan is built the first time the SEG schedule is chosen (by
+// gb_csr_set_schedule or the autotuner): it costs a host pass over rowptr
+// that most matrices -- every CG operator on the row schedule -- never need.
+int ensure_seg_plan(gb_csr & a, cudaStream_t stream) {
+  if (a.plan.d_seg || a.nrows == 0) return GOOSEBERRY_SUCCESS;
+  std::vector<uint32_t> hrp(static_cast<size_t>(a.nrows) + 1);
+  GB_CUDA_TRY(cudaMemcpyAsync(hrp.data(), a.rowptr, hrp.size() * sizeof(uint32_t),
+      cudaMemcpyDeviceToHost, stream));
+  GB_CUDA_TRY(cudaStreamSynchronize(stream));
+  build_seg_plan(a.nrows, hrp.data(), a.nnz, seg_max_warps(a.sm_count), a.plan);
+  int rc = upload_seg(a.plan, stream);
+  if (rc == GOOSEBERRY_SUCCESS && cudaStreamSynchronize(stream) != cudaSuccess) {
+    set_error("segmented plan upload: %s", cudaGetErrorString(cudaGetLastError()));
+    rc = GOOSEBERRY_ERROR_UNKNOWN;
+  }
+  if (rc != GOOSEBERRY_SUCCESS) {  // leave no half-built plan behind
+    cudaDeviceSynchronize();
+    if (a.plan.d_seg) dev_free(a.plan.d_seg);
+    if (a.plan.d_seg_rec) dev_free(a.plan.d_seg_rec);
+    if (a.plan.d_seg_count) dev_free(a.plan.d_seg_count);
+    a.plan.d_seg = nullptr;
+    a.plan.d_seg_rec = nullptr;
+    a.plan.d_seg_count = nullptr;
+    a.plan.seg.clear();
+  }
+  return rc;
 }
 
 int autotune(gb_csr & a, unsigned width, cudaStream_t stream) {
@@ -680,6 +719,7 @@ int autotune(gb_csr & a, unsigned width, cudaStream_t stream) {
     auto it = g_tune_cache.find(key);
     if (it != g_tune_cache.end()) {
       GB_TRY(rebuild_plan(a, it->second.tile_items, stream));
+      if (it->second.sched == GB_SCHED_SEG) GB_TRY(ensure_seg_plan(a, stream));
       (width == GB_CSR_VALUES_F32 ? a.sched32 : a.sched64) = it->second.sched;
       return GOOSEBERRY_SUCCESS;
     }
@@ -720,6 +760,7 @@ int autotune(gb_csr & a, unsigned width, cudaStream_t stream) {
   int rc = GOOSEBERRY_SUCCESS;
   for (const Cand & cd : cands) {
     rc = rebuild_plan(a, cd.tile, stream);
+    if (rc == GOOSEBERRY_SUCCESS && cd.sched == GB_SCHED_SEG) rc = ensure_seg_plan(a, stream);
     if (rc != GOOSEBERRY_SUCCESS) break;
     {
       const int s = cd.sched;
@@ -785,6 +826,9 @@ int alloc_copy(void ** dst, const T * src, size_t n, bool device_src, cudaStream
 
 void release(gb_csr * a) {
   if (!a) return;
+  // uploads may still be in flight on the creating stream (a creation that
+  // failed part-way), and dev_free releases on the pool's own stream
+  if (a->own_rowptr || a->own_rowind || a->own_val64 || a->own_val32) cudaDeviceSynchronize();
   gb::free_plan(a->plan);
   if (a->own_rowptr) dev_free(a->own_rowptr);
   if (a->own_rowind) dev_free(a->own_rowind);
@@ -823,9 +867,9 @@ int create_impl(dim_t nrows, dim_t ncols, ind_t nnz, const ind_t * rowptr,
     GB_CUDA_TRY(cudaStreamSynchronize(stream));
     rp_host = hrp.data();
   }
-  GB_TRY(gb::build_plan(nrows, rp_host, nnz, gb::kDefaultTileItems, a->plan));
-  gb::build_seg_plan(nrows, rp_host, nnz, gb::seg_max_warps(a->sm_count), a->plan);
-
+  // Host arrays: the uploads are queued first, so that (from pinned memory)
+  // the copies run while the host builds the tile plan.  A failure after this
+  // point frees the arrays through release(), which synchronises first.
   if (dev) {
     a->rowptr = rowptr;
     a->rowind = rowind;
@@ -845,6 +889,7 @@ int create_impl(dim_t nrows, dim_t ncols, ind_t nnz, const ind_t * rowptr,
       a->val32 = static_cast<const float *>(a->own_val32);
     }
   }
+  GB_TRY(gb::build_plan(nrows, rp_host, nnz, gb::kDefaultTileItems, a->plan));
   if (want32 && !a->val32) {
     // round from the double values (already on the device, or upload them)
     const double * src = a->val64;
@@ -979,6 +1024,7 @@ int gb_csr_set_schedule(gb_csr_t * a, unsigned value_width, int schedule,
                      (tile_items ? tile_items : a->plan.tile_items) <= wm_max,
       "per-warp merge tiles need tile_items <= %u", wm_max);
   if (tile_items) GB_TRY(gb::rebuild_plan(*a, tile_items, nullptr));
+  if (schedule == GB_SCHED_SEG) GB_TRY(gb::ensure_seg_plan(*a, nullptr));
   const int s = schedule == GB_SCHED_AUTO ? gb::default_schedule(a->plan) : schedule;
   (value_width == GB_CSR_VALUES_F32 ? a->sched32 : a->sched64) = s;
   return GOOSEBERRY_SUCCESS;
