@@ -225,3 +225,13 @@ def test_planner_many_segments_match_greedy_rule():
     mt, mlong = _plan_model(rp, 2048)
     assert nlong == mlong and np.array_equal(tiles.astype(np.int64), mt)
     assert info.max_row == L.max()
+
+
+def test_cgd_out_is_checked_before_any_call():
+    """A wrong `out` array is refused on the host, before the library runs."""
+    L = W.laplacian_2d(8)
+    b = W.rhs(L.nrows, 1)
+    for bad in (np.zeros(L.nrows, dtype=np.float32), np.zeros(L.nrows + 1),
+                np.zeros((L.nrows, 2))[:, 0]):
+        with pytest.raises(ValueError):
+            gb.cgd(L.rowptr, L.rowind, L.rowval, b, 1e-8, 100, out=bad)

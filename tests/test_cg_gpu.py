@@ -45,6 +45,19 @@ def test_dropin_cgd_matches_reference_iterations(cg_golden):
         assert np.linalg.norm(x - xr) <= 1e-4 * np.linalg.norm(xr) + 1e-12, name
 
 
+def test_dropin_cgd_into_pinned_out(torch, cg_golden):
+    """cgd(out=) writes x into the caller's (here pinned) array: the same bits as
+    the default path, and the same array object comes back."""
+    c = cg_golden["laplace64"]
+    err, niter = float(c["error"]), int(c["niter"])
+    x0, it0, rn0 = gb.cgd(c["rowptr"], c["rowind"], c["rowval"], c["b"], err, niter)
+    out = torch.empty(len(c["b"]), dtype=torch.float64, pin_memory=True).numpy()
+    out[:] = np.nan
+    x1, it1, rn1 = gb.cgd(c["rowptr"], c["rowind"], c["rowval"], c["b"], err, niter, out=out)
+    assert x1 is out and it1 == it0 and rn1 == rn0
+    assert np.array_equal(x1, x0)
+
+
 def test_device_solver_relative_tolerance(torch, cg_golden):
     c = cg_golden["laplace64"]
     A = gb.CsrMatrix.from_host(rowptr=c["rowptr"], rowind=c["rowind"], rowval=c["rowval"])
