@@ -319,6 +319,12 @@ __device__ __forceinline__ void mix_refresh_rows(size_t s, size_t e,
 // the FP64 residual of its rows instead (mix_refresh_rows).  Six CTAs per SM
 // (40 registers, no spills): the update streams six vectors, and at four CTAs
 // (54 registers) it ran 21.2 us instead of 18.6 on the 160^3 operator.
+// Units of four elements per thread per pass: at one unit the update loads
+// 16 bytes per vector (21.0 -> 18.6 us on the 160^3 operator against the
+// former four scalar elements); two units spill at this register budget (21.5 us).
+#ifndef GB_B32_UNITS
+#define GB_B32_UNITS 1
+#endif
 __global__ void __launch_bounds__(kVecBlock, 6) cg_b32_kernel(size_t n,
     float * __restrict__ y, float * __restrict__ r, float * __restrict__ p,
     const float * __restrict__ pold,
@@ -358,33 +364,61 @@ __global__ void __launch_bounds__(kVecBlock, 6) cg_b32_kernel(size_t n,
   }
   const float alpha = static_cast<float>(rr_hat / pap);
   const bool fresh = st->sv[par].y_reset != 0;
-  const size_t q = n / gridDim.x, rem = n % gridDim.x;
+  // contiguous chunk per CTA in units of four elements (16-byte loads); all
+  // loads of a pass are issued before any arithmetic
+  const size_t units = (n + 3) / 4;
+  const size_t q = units / gridDim.x, rem = units % gridDim.x;
   const size_t b = blockIdx.x;
-  const size_t s = b * q + min(b, rem);
-  const size_t e = s + q + (b < rem ? 1 : 0);
+  const size_t us = b * q + min(b, rem);
+  const size_t ue = us + q + (b < rem ? 1 : 0);
+  const size_t full = n / 4;  // complete units
+  const size_t ve = min(ue, full);
+  const float4 * p4 = reinterpret_cast<const float4 *>(p);
+  const float4 * a4 = reinterpret_cast<const float4 *>(ap);
+  float4 * y4 = reinterpret_cast<float4 *>(y);
+  float4 * r4 = reinterpret_cast<float4 *>(r);
   double acc = 0.0;
-  constexpr int U = 4;
-  for (size_t base = s; base < e; base += U * kVecBlock) {
-    float pv[U], av[U], yv[U], rv[U];
+  constexpr int U = GB_B32_UNITS;
+  for (size_t base = us; base < ve; base += U * kVecBlock) {
+    float4 pv[U], av[U], yv[U], rv[U];
 #pragma unroll
     for (int j = 0; j < U; ++j) {
-      const size_t i = base + threadIdx.x + j * kVecBlock;
-      if (i < e) {
-        pv[j] = p[i];
-        av[j] = ap[i];
-        yv[j] = fresh ? 0.0f : y[i];
-        rv[j] = r[i];
+      const size_t u = base + threadIdx.x + j * kVecBlock;
+      if (u < ve) {
+        pv[j] = p4[u];
+        av[j] = a4[u];
+        yv[j] = fresh ? make_float4(0.f, 0.f, 0.f, 0.f) : y4[u];
+        rv[j] = r4[u];
       }
     }
 #pragma unroll
     for (int j = 0; j < U; ++j) {
-      const size_t i = base + threadIdx.x + j * kVecBlock;
-      if (i < e) {
-        y[i] = fmaf(alpha, pv[j], yv[j]);
-        const float rn = fmaf(-alpha, av[j], rv[j]);
-        r[i] = rn;
-        acc += static_cast<double>(rn) * static_cast<double>(rn);
+      const size_t u = base + threadIdx.x + j * kVecBlock;
+      if (u < ve) {
+        float4 yn, rn;
+        yn.x = fmaf(alpha, pv[j].x, yv[j].x);
+        yn.y = fmaf(alpha, pv[j].y, yv[j].y);
+        yn.z = fmaf(alpha, pv[j].z, yv[j].z);
+        yn.w = fmaf(alpha, pv[j].w, yv[j].w);
+        rn.x = fmaf(-alpha, av[j].x, rv[j].x);
+        rn.y = fmaf(-alpha, av[j].y, rv[j].y);
+        rn.z = fmaf(-alpha, av[j].z, rv[j].z);
+        rn.w = fmaf(-alpha, av[j].w, rv[j].w);
+        y4[u] = yn;
+        r4[u] = rn;
+        acc += static_cast<double>(rn.x) * static_cast<double>(rn.x);
+        acc += static_cast<double>(rn.y) * static_cast<double>(rn.y);
+        acc += static_cast<double>(rn.z) * static_cast<double>(rn.z);
+        acc += static_cast<double>(rn.w) * static_cast<double>(rn.w);
       }
+    }
+  }
+  if (ue > full && threadIdx.x == 0) {  // n % 4 elements past the last complete unit
+    for (size_t i = 4 * full; i < n; ++i) {
+      y[i] = fmaf(alpha, p[i], fresh ? 0.0f : y[i]);
+      const float rn = fmaf(-alpha, ap[i], r[i]);
+      r[i] = rn;
+      acc += static_cast<double>(rn) * static_cast<double>(rn);
     }
   }
   const double bs = block_sum(acc, red);
