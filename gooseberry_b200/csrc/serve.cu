@@ -79,10 +79,6 @@ constexpr int kSrvMaxRegs = GB_SRV_MAX_REGS;  // 3 CTAs of 288 threads per SM at
 // of 6 at this register budget.
 constexpr int kSrvRowStage = GB_SRV_ROW_STAGE;
 constexpr uint32_t kTileRows = GB_SRV_TILE_ROWS;
-#ifndef GB_SRV_B_ROWS
-#define GB_SRV_B_ROWS 4
-#endif
-constexpr int kBRows = GB_SRV_B_ROWS;  // rows per thread per pass of the update kernel
 constexpr uint32_t kMaxRowNnz = 255;      // longer rows belong to the single-solve CG
 constexpr double kSrvDelta = 0.1;         // reliable update trigger (see cg_mixed.cu)
 constexpr size_t kMaxTiles = 1u << 20;
@@ -387,6 +383,17 @@ struct WorkA {
 // ---- B: solution / residual update, r.r, stop or update decision;  or the
 //      reliable FP64 residual update (mixed) ----------------------------------------------
 
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+  using type = float4;
+};
+template <>
+struct Vec16<double> {
+  using type = double2;
+};
+
 template <typename T, bool MIXED>
 struct WorkB {
   uint64_t pol_m, pol_x;
@@ -416,37 +423,49 @@ struct WorkB {
     const T * ap = static_cast<const T *>(S.ap);
     T * r = static_cast<T *>(S.r);
     T * y = static_cast<T *>(S.y);
-    // passes of kBRows rows per thread: every load of a pass is in flight at once
-    for (uint32_t base = tid; base < cnt; base += kBRows * kSrvCompute) {
-      T pv[kBRows], av[kBRows], rv[kBRows];
-      double xv[kBRows];
-#pragma unroll
-      for (int j = 0; j < kBRows; ++j) {
-        const uint32_t q = base + j * kSrvCompute;
-        if (q < cnt) {
-          const uint32_t i = r0 + q;
-          pv[j] = pnew[i];
-          av[j] = ap[i];
-          rv[j] = r[i];
-          if (MIXED) xv[j] = fresh ? 0.0 : static_cast<double>(y[i]);
-          else xv[j] = S.x0[i];
-        }
+    // one row's update; s0 += r.r
+    auto one = [&](uint32_t i, T pv, T av, T rv, double xv) {
+      if (MIXED) {
+        y[i] = fma(alpha, pv, static_cast<T>(xv));
+      } else {
+        S.x0[i] = fma(static_cast<double>(alpha), static_cast<double>(pv), xv);
       }
+      const T rn = fma(-alpha, av, rv);
+      r[i] = rn;
+      s0 += static_cast<double>(rn) * static_cast<double>(rn);
+    };
+    // 16-byte units (tiles start at multiples of the tile size, and the pool
+    // places every vector on a 256-byte boundary); the rows past the last
+    // complete unit, or a tile that is not aligned, take one row per thread
+    constexpr uint32_t VN = 16 / sizeof(T);
+    using V = typename Vec16<T>::type;
+    const uint32_t nfull = (r0 % VN == 0) ? cnt / VN : 0u;
+    for (uint32_t u = tid; u < nfull; u += kSrvCompute) {
+      const uint32_t i = r0 + u * VN;
+      const V pv = *reinterpret_cast<const V *>(pnew + i);
+      const V av = *reinterpret_cast<const V *>(ap + i);
+      const V rv = *reinterpret_cast<const V *>(r + i);
+      V yv{};
+      double2 xv[VN / 2 > 0 ? VN / 2 : 1];
+      if (MIXED) {
+        if (!fresh) yv = *reinterpret_cast<const V *>(y + i);
+      } else {
 #pragma unroll
-      for (int j = 0; j < kBRows; ++j) {
-        const uint32_t q = base + j * kSrvCompute;
-        if (q < cnt) {
-          const uint32_t i = r0 + q;
-          if (MIXED) {
-            y[i] = fma(alpha, pv[j], static_cast<T>(xv[j]));
-          } else {
-            S.x0[i] = fma(static_cast<double>(alpha), static_cast<double>(pv[j]), xv[j]);
-          }
-          const T rn = fma(-alpha, av[j], rv[j]);
-          r[i] = rn;
-          s0 += static_cast<double>(rn) * static_cast<double>(rn);
-        }
+        for (uint32_t h = 0; h < VN / 2; ++h) xv[h] = reinterpret_cast<const double2 *>(S.x0 + i)[h];
       }
+      const T * pp = reinterpret_cast<const T *>(&pv);
+      const T * aa = reinterpret_cast<const T *>(&av);
+      const T * rr = reinterpret_cast<const T *>(&rv);
+      const T * yy = reinterpret_cast<const T *>(&yv);
+      const double * xx = reinterpret_cast<const double *>(xv);
+#pragma unroll
+      for (uint32_t e = 0; e < VN; ++e)
+        one(i + e, pp[e], aa[e], rr[e], MIXED ? static_cast<double>(yy[e]) : xx[e]);
+    }
+    for (uint32_t q = VN * nfull + tid; q < cnt; q += kSrvCompute) {
+      const uint32_t i = r0 + q;
+      one(i, pnew[i], ap[i], r[i],
+          MIXED ? (fresh ? 0.0 : static_cast<double>(y[i])) : S.x0[i]);
     }
   }
 
