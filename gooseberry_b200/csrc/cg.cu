@@ -399,9 +399,7 @@ int launch_cg_a_t(const gb_csr & a, const double * r, const double * pold, doubl
     cudaStream_t s, bool pdl) {
   const size_t smem = spmv_smem(SCHED, a.plan.tile_items);
   auto kern = cg_a_kernel<SCHED, HINT>;
-  if (smem > 48 * 1024)
-    GB_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void *>(kern),
-        cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  GB_TRY(raise_smem_limit(reinterpret_cast<const void *>(kern), smem));
   GB_CUDA_TRY(launch_k(kern, grid, kSpmvBlock, smem, s, pdl, plan_view(a), a.rowptr,
       a.rowind, a.val64, r, pold, pnew, ap, longdot, partial, st, rp));
   return GOOSEBERRY_SUCCESS;
@@ -508,9 +506,7 @@ int launch_cg_a_codec(const gb_csr & a, const RowCodec & c, bool hint, const dou
 template <int SCHED>
 int occupancy_cg_a(size_t smem, int * out) {
   auto kern = cg_a_kernel<SCHED, false>;
-  if (smem > 48 * 1024)
-    GB_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void *>(kern),
-        cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  GB_TRY(raise_smem_limit(reinterpret_cast<const void *>(kern), smem));
   GB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, kern, kSpmvBlock, smem));
   return GOOSEBERRY_SUCCESS;
 }
@@ -821,9 +817,7 @@ template <int SCHED>
 int persistent_setup_t(size_t smem, int * occ, const void ** fn) {
   auto kern = cg_persistent_kernel<SCHED>;
   *fn = reinterpret_cast<const void *>(kern);
-  if (smem > 48 * 1024)
-    GB_CUDA_TRY(cudaFuncSetAttribute(*fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-        static_cast<int>(smem)));
+  GB_TRY(raise_smem_limit(*fn, smem));
   GB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, kSpmvBlock, smem));
   return GOOSEBERRY_SUCCESS;
 }

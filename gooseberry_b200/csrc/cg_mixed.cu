@@ -602,9 +602,7 @@ size_t smem_of(int sched, uint32_t tile_items, size_t value_bytes) {
 
 template <typename K>
 int prep_kernel(K kern, size_t smem, int * occ) {
-  if (smem > 48 * 1024)
-    GB_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void *>(kern),
-        cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  GB_TRY(raise_smem_limit(reinterpret_cast<const void *>(kern), smem));
   if (occ)
     GB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, kSpmvBlock, smem));
   return GOOSEBERRY_SUCCESS;

@@ -205,6 +205,11 @@ void dev_free(void * p);
 // that uses it can still run.
 int pinned_slot_alloc(size_t bytes, void ** host, void ** dev);
 void pinned_slot_free(void * host);
+// Raise a kernel's dynamic shared-memory limit on the current device to at
+// least `bytes` (above the 48 KiB default).  Never lowers it: a kernel that is
+// launched, or captured in graphs, at several sizes keeps the largest limit
+// any of them needed.
+int raise_smem_limit(const void * func, size_t bytes);
 template <typename T>
 int dev_alloc(T ** p, size_t bytes) {
   return dev_alloc(reinterpret_cast<void **>(p), bytes);

@@ -4,6 +4,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -106,6 +107,25 @@ void dev_free(void * p) {
   DevicePool d;
   if (pool_of_current_device(&d) != GOOSEBERRY_SUCCESS) return;
   cudaFreeAsync(p, d.alloc_stream);
+}
+
+namespace {
+std::mutex g_smem_mu;
+std::map<std::pair<const void *, int>, size_t> g_smem_limit;
+}  // namespace
+
+int raise_smem_limit(const void * func, size_t bytes) {
+  if (bytes <= 48 * 1024) return GOOSEBERRY_SUCCESS;
+  int dev = 0;
+  GB_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_smem_mu);
+  size_t & lim = g_smem_limit[std::make_pair(func, dev)];
+  if (bytes > lim) {
+    GB_CUDA_TRY(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        static_cast<int>(bytes)));
+    lim = bytes;
+  }
+  return GOOSEBERRY_SUCCESS;
 }
 
 namespace {

@@ -447,26 +447,28 @@ __global__ void round_f32_kernel(const double * __restrict__ in, float * __restr
 
 // ---- launch helpers ---------------------------------------------------------
 
-// Resident CTAs per SM of a kernel at a dynamic shared-memory size (cached).
+// Resident CTAs per SM of a kernel at a dynamic shared-memory size (cached),
+// after raising the kernel's dynamic shared-memory limit to cover it (the
+// limit only grows: lowering it for a small tile made a later launch at a
+// larger, already cached, tile size fail with an invalid argument).
 int occupancy(const void * func, size_t smem, int * out, int block = kSpmvBlock) {
   static std::mutex mu;
-  static std::map<std::pair<const void *, size_t>, int> cache;
+  static std::map<std::tuple<const void *, size_t, int>, int> cache;
   std::lock_guard<std::mutex> lock(mu);
-  auto key = std::make_pair(func, smem);
+  int dev = 0;
+  GB_CUDA_TRY(cudaGetDevice(&dev));
+  auto key = std::make_tuple(func, smem, dev);
   auto it = cache.find(key);
   if (it != cache.end()) {
     *out = it->second;
     return GOOSEBERRY_SUCCESS;
   }
-  int dev = 0, max_smem = 0;
-  GB_CUDA_TRY(cudaGetDevice(&dev));
+  int max_smem = 0;
   GB_CUDA_TRY(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   GB_CHECK_INPUT(smem <= static_cast<size_t>(max_smem),
       "this schedule needs %zu bytes of shared memory per CTA at this tile size; the "
       "device allows %d (choose smaller tile_items)", smem, max_smem);
-  if (smem > 48 * 1024)
-    GB_CUDA_TRY(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize,
-        static_cast<int>(smem)));
+  GB_TRY(raise_smem_limit(func, smem));
   int n = 0;
   GB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, func, block, smem));
   if (n < 1) {

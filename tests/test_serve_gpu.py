@@ -55,14 +55,38 @@ def test_mix_converges_and_matches_alone(mode):
         alone.close()
 
 
+def _reference_iterations(A, b, e, niter):
+    """The reference cgd's iteration counts on this system over OpenMP thread
+    counts (its blas_dot reduces in thread order, src/blas.c:413-430, so the
+    count moves with the thread count); the oracle restatement's sequential
+    count when the reference build is missing."""
+    import oracle
+    if not oracle.ref_available("f64"):
+        return [oracle.cgd(A.rowptr, A.rowind, A.rowval, b, e, niter)[1]]
+    its = []
+    try:
+        for th in (1, 2, 4, 8):
+            oracle.ref_set_threads(th)
+            its.append(oracle.ref_cgd(A.rowptr, A.rowind, A.rowval, b, e, niter)[1])
+    finally:
+        oracle.ref_set_threads(1)
+    return its
+
+
 def test_fp64_server_matches_single_solver():
+    """The FP64 server and the single-solve CG both stop within 2 iterations
+    of the reference's own range of counts (363-367 over 1-8 threads on this
+    system: the ±2 rule of the spec, applied to a reference whose count itself
+    depends on its thread count), and their solutions agree."""
     rid, A, b = _requests([48], 300)[0]
     srv = gb.Server(pool_bytes=1 << 28, max_slots=2, mode=gb.CG_F64, iters_per_step=5)
     srv.submit(rid, A, b, tol=1e-8, niter=5000)
     r = srv.drain()[0]
     e = 1e-8 * np.linalg.norm(b)
     x, it, rn = gb.cgd(A.rowptr, A.rowind, A.rowval, b, e, 5000)
-    assert abs(r.iterations - it) <= 2
+    ref = _reference_iterations(A, b, e, 5000)
+    for got in (r.iterations, it):
+        assert min(ref) - 2 <= got <= max(ref) + 2, (got, ref)
     assert np.linalg.norm(r.x - x) <= 1e-6 * np.linalg.norm(x)
 
 

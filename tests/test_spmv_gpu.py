@@ -224,6 +224,29 @@ def test_segmented_schedule_edge_cases(torch, case):
                            x.astype(np.float32)) <= TOL32
 
 
+def test_segmented_plan_survives_tile_rebuilds(torch):
+    """SEG's plan is built when SEG is first chosen and kept when another
+    schedule rebuilds the tile plan at a new tile size: switching back to SEG
+    gives the same bits, and the tile schedule in between is right too."""
+    A = W.powerlaw_rows(60_000, 900_000, seed=12, cap=40_000)
+    x = W.dense_x(A.ncols, 12)
+    y_ref = oracle.spmv(A.rowptr, A.rowind, A.rowval, x, threads=8)
+    M = gb.CsrMatrix.from_host(A)
+    xd = _dev(torch, x)
+    M.set_schedule(gb.SCHED_SEG)
+    y1 = M.spmv(xd).cpu().numpy()
+    assert cond_scaled_err(y1, y_ref, A.rowptr, A.rowind, A.rowval, x) <= TOL64
+    for tile in (512, 4096):
+        M.set_schedule(gb.SCHED_MERGE, tile_items=tile)
+        y2 = M.spmv(xd).cpu().numpy()
+        assert cond_scaled_err(y2, y_ref, A.rowptr, A.rowind, A.rowval, x) <= TOL64
+        M.set_schedule(gb.SCHED_SEG)
+        assert np.array_equal(M.spmv(xd).cpu().numpy(), y1)
+    M.autotune()  # the tuner's SEG candidate reuses the kept plan
+    y3 = M.spmv(xd).cpu().numpy()
+    assert cond_scaled_err(y3, y_ref, A.rowptr, A.rowind, A.rowval, x) <= TOL64
+
+
 def test_segmented_schedule_needs_aligned_arrays(torch):
     """Borrowed device arrays that do not start on a 16-byte boundary cannot
     take the SEG schedule's 16-byte loads: choosing it is refused."""
