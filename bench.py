@@ -716,6 +716,24 @@ def _serve_live(srv, reqs, arr, rtol, limit_s=3600.0):
     return got, [r.t_done - c0 - arr[r.id] for r in got]
 
 
+def _serve_saturated(srv, reqs, rtol, depth, limit_s=3600.0):
+    """Every request is there at t = 0; the loop keeps `depth` of them queued
+    ahead of the device and submits the rest between steps, so the host's copy
+    of a request overlaps the device work of the ones before it."""
+    n = len(reqs)
+    i, got, queued = 0, [], 0
+    t_start = time.perf_counter()
+    while len(got) < n and time.perf_counter() - t_start < limit_s:
+        while i < n and queued < depth:
+            k, A, b = reqs[i]
+            srv.submit(k, A, b, tol=rtol)
+            i += 1
+            queued += 1
+        _, queued = srv.step()
+        got += srv.poll()
+    return got
+
+
 def serving_extra(nreq=300, seed=5, rtol=1e-10, pool=16 << 30, slots=256, ips=16,
                   load=0.8, live=True, dropin=True, arm_names=None):
     """Serving stream of 2D 5-point variable-coefficient SPD systems (side
@@ -728,8 +746,9 @@ def serving_extra(nreq=300, seed=5, rtol=1e-10, pool=16 << 30, slots=256, ips=16
       fp64_batched       the same server in plain FP64 CG;
       fp64_one_at_a_time the same server in FP64 with one slot: plain FP64 CG
                          served one solve at a time (the benchmark's baseline).
-    Each arm: the saturated rate (every request queued at t = 0, after an
-    untimed pass that grows the server to its working size), then a live run
+    Each arm: the saturated rate (every request present at t = 0 and kept
+    queued two slot-counts deep ahead of the device, after an untimed pass that
+    grows the server to its working size), then a live run
     under Poisson arrivals at `load` x the one-at-a-time arm's saturated rate,
     the same arrival times for every arm, with p50/p99 latency from arrival
     to result.  For context (streams of up to 1000 requests), the drop-in
@@ -762,9 +781,7 @@ def serving_extra(nreq=300, seed=5, rtol=1e-10, pool=16 << 30, slots=256, ips=16
             srv.submit(k, A, b, tol=rtol)
         srv.drain(timeout_s=3600)
         t0 = time.perf_counter()
-        for k, A, b in reqs:
-            srv.submit(k, A, b, tol=rtol)
-        res = srv.drain(timeout_s=3600)
+        res = _serve_saturated(srv, reqs, rtol, depth=2 * ns)
         makespan = time.perf_counter() - t0
         worst = 0.0
         for r in res:
