@@ -46,6 +46,8 @@
 #include <cstring>
 #include <deque>
 #include <map>
+#include <memory>
+#include <new>
 #include <mutex>
 #include <tuple>
 #include <vector>
@@ -610,8 +612,14 @@ class Pool {
 struct Request {
   uint64_t id = 0;
   uint32_t n = 0, nnz = 0;
-  std::vector<uint32_t> rowptr, rowind;
-  std::vector<double> val64, b;
+  // the request's copy of rowptr, rowind, the values and b: in the server's
+  // pinned staging arena when it has room (stage_len > 0), else in `own`
+  uint32_t * rowptr = nullptr;
+  uint32_t * rowind = nullptr;
+  double * val64 = nullptr;
+  double * b = nullptr;
+  size_t stage_off = 0, stage_len = 0;
+  std::unique_ptr<unsigned char[]> own;
   double * x_out = nullptr;
   double tol_rel = 0.0;
   size_t niter = 0;
@@ -633,6 +641,12 @@ struct SlotHost {
 
 size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
+// Host bytes of a queued request's arrays (rowptr, rowind, values, b).
+size_t request_host_bytes(uint32_t n, uint32_t nnz) {
+  return align256(4ull * (n + 1)) + align256(4ull * nnz) + align256(8ull * nnz) +
+         align256(8ull * n);
+}
+
 }  // namespace
 }  // namespace gb
 
@@ -651,6 +665,13 @@ struct gb_server {
   uint32_t * h_ntiles = nullptr;    // pinned
   gb::SrvTile * h_tiles = nullptr;  // pinned staging of the tile list
   double2 * d_part = nullptr;       // 2 * kMaxTiles (A and B partial sums)
+  // Pinned staging of queued requests: submit copies a request here (memory
+  // already faulted in), and admission uploads it with an asynchronous copy
+  // instead of a staged one while the device waits.  Regions go back once the
+  // copies that read them are done (the next step's wait).
+  unsigned char * stage = nullptr;
+  gb::Pool stage_alloc;
+  std::vector<std::pair<size_t, size_t>> stage_done;
   std::vector<gb::SlotHost> slots;
   std::deque<gb::Request> queue;
   std::vector<gb_server_result_t> results;
@@ -723,6 +744,7 @@ void destroy_server(gb_server * s) {
   if (s->h_slots) cudaFreeHost(s->h_slots);
   if (s->h_tiles) cudaFreeHost(s->h_tiles);
   if (s->h_ntiles) cudaFreeHost(s->h_ntiles);
+  if (s->stage) cudaFreeHost(s->stage);
   delete s;
 }
 
@@ -760,6 +782,19 @@ int create_server(const gb_server_config_t & cfg, gb_server * s) {
   GB_CUDA_TRY(cudaMalloc(&s->d_ntiles, sizeof(uint32_t)));
   GB_CUDA_TRY(cudaMemset(s->d_ntiles, 0, sizeof(uint32_t)));
   GB_CUDA_TRY(cudaMallocHost(&s->h_ntiles, sizeof(uint32_t)));
+  // the staging arena: an eighth of the device pool, between 64 MiB and
+  // 2 GiB; without it (pinning refused) requests are copied to pageable memory
+  {
+    const size_t want = std::min<size_t>(std::max<size_t>(cfg.pool_bytes / 8, 64ull << 20),
+        2ull << 30);
+    void * st = nullptr;
+    if (cudaHostAlloc(&st, want, cudaHostAllocPortable) == cudaSuccess) {
+      s->stage = static_cast<unsigned char *>(st);
+      s->stage_alloc.reset(want);
+    } else {
+      cudaGetLastError();
+    }
+  }
   *s->h_ntiles = 0;
   GB_CUDA_TRY(cudaMalloc(&s->d_part, 2 * kMaxTiles * sizeof(double2)));
   s->slots.resize(cfg.max_slots);
@@ -794,31 +829,61 @@ int submit(gb_server & s, uint64_t id, dim_t n, const ind_t * rowptr, const dim_
   q.tol_rel = tol_rel;
   q.niter = niter ? niter : std::max<size_t>(1000, 100 * static_cast<size_t>(n));
   q.t_submit = now_s(s);
-  q.rowptr.assign(rowptr, rowptr + n + 1);
-  GB_CHECK_INPUT(q.rowptr[0] == 0, "rowptr[0] must be 0");
-  uint32_t maxrow = 0;
-  for (uint32_t r = 0; r < n; ++r) {
-    GB_CHECK_INPUT(q.rowptr[r + 1] >= q.rowptr[r], "rowptr decreases at row %u", r);
-    const uint32_t l = q.rowptr[r + 1] - q.rowptr[r];
-    GB_CHECK_INPUT(l <= kMaxRowNnz, "row %u has %u nonzeros; the solve server takes at most %u",
-        r, l, kMaxRowNnz);
-    maxrow = std::max(maxrow, l);
+  const size_t hb = request_host_bytes(n, nnz);
+  unsigned char * base = nullptr;
+  size_t off = 0;
+  if (s.stage && s.stage_alloc.alloc(hb, &off)) {
+    base = s.stage + off;
+    q.stage_off = off;
+    q.stage_len = hb;
+  } else {
+    q.own.reset(new (std::nothrow) unsigned char[hb]);
+    GB_CHECK_INPUT(q.own != nullptr, "no host memory for a request of %zu bytes", hb);
+    base = q.own.get();
   }
-  q.rowind.assign(rowind, rowind + nnz);
-  for (uint32_t k = 0; k < nnz; ++k)
-    GB_CHECK_INPUT(q.rowind[k] < n, "column index %u out of range for %u columns", q.rowind[k], n);
-  q.val64.assign(rowval, rowval + nnz);
-  q.b.assign(b, b + n);
-  // row tiles (from the request alone, so a solve is cut the same way
-  // whatever else is resident)
-  uint32_t T = 0;
-  GB_TRY(tile_rows_for(s, q, maxrow, &T));
-  const size_t ntiles = (static_cast<size_t>(n) + T - 1) / T;
-  GB_CHECK_INPUT(ntiles <= kMaxTiles, "request needs %zu tiles, more than %zu", ntiles, kMaxTiles);
-  for (uint32_t r = 0; r < n; r += T) q.tiles.push_back(SrvTile{0, r, std::min(T, n - r), 0});
-  q.bytes = footprint(s.mixed, n, nnz);
-  GB_CHECK_INPUT(q.bytes <= s.cfg.pool_bytes, "request needs %zu bytes of device memory, "
-      "the pool holds %zu", q.bytes, s.cfg.pool_bytes);
+  size_t at = 0;
+  q.rowptr = reinterpret_cast<uint32_t *>(base + at);
+  at += align256(4ull * (n + 1));
+  q.rowind = reinterpret_cast<uint32_t *>(base + at);
+  at += align256(4ull * nnz);
+  q.val64 = reinterpret_cast<double *>(base + at);
+  at += align256(8ull * nnz);
+  q.b = reinterpret_cast<double *>(base + at);
+  // checks run on the copy; a refused request hands its staging region back
+  uint32_t maxrow = 0;
+  const int rc = [&]() -> int {
+    std::memcpy(q.rowptr, rowptr, 4ull * (n + 1));
+    GB_CHECK_INPUT(q.rowptr[0] == 0, "rowptr[0] must be 0");
+    for (uint32_t r = 0; r < n; ++r) {
+      GB_CHECK_INPUT(q.rowptr[r + 1] >= q.rowptr[r], "rowptr decreases at row %u", r);
+      const uint32_t l = q.rowptr[r + 1] - q.rowptr[r];
+      GB_CHECK_INPUT(l <= kMaxRowNnz,
+          "row %u has %u nonzeros; the solve server takes at most %u", r, l, kMaxRowNnz);
+      maxrow = std::max(maxrow, l);
+    }
+    if (nnz) std::memcpy(q.rowind, rowind, 4ull * nnz);
+    for (uint32_t k = 0; k < nnz; ++k)
+      GB_CHECK_INPUT(q.rowind[k] < n, "column index %u out of range for %u columns",
+          q.rowind[k], n);
+    if (nnz) std::memcpy(q.val64, rowval, 8ull * nnz);
+    std::memcpy(q.b, b, 8ull * n);
+    q.bytes = footprint(s.mixed, n, nnz);
+    GB_CHECK_INPUT(q.bytes <= s.cfg.pool_bytes, "request needs %zu bytes of device memory, "
+        "the pool holds %zu", q.bytes, s.cfg.pool_bytes);
+    // row tiles (from the request alone, so a solve is cut the same way
+    // whatever else is resident)
+    uint32_t T = 0;
+    GB_TRY(tile_rows_for(s, q, maxrow, &T));
+    const size_t ntiles = (static_cast<size_t>(n) + T - 1) / T;
+    GB_CHECK_INPUT(ntiles <= kMaxTiles, "request needs %zu tiles, more than %zu", ntiles,
+        kMaxTiles);
+    for (uint32_t r = 0; r < n; r += T) q.tiles.push_back(SrvTile{0, r, std::min(T, n - r), 0});
+    return GOOSEBERRY_SUCCESS;
+  }();
+  if (rc != GOOSEBERRY_SUCCESS) {
+    if (q.stage_len) s.stage_alloc.release(q.stage_off, q.stage_len);
+    return rc;
+  }
   s.queue.push_back(std::move(q));
   return GOOSEBERRY_SUCCESS;
 }
@@ -870,15 +935,19 @@ int admit(gb_server & s, Request & q, uint32_t k) {
     v32 = carve<float>(base, at, q.nnz);
     x1 = carve<double>(base, at, q.n);
   }
-  GB_CUDA_TRY(cudaMemcpyAsync(rp, q.rowptr.data(), 4ull * (q.n + 1), cudaMemcpyHostToDevice,
+  // (from the staging arena these copies are asynchronous; the region goes
+  // back to the arena after the step's wait, when they are done)
+  if (q.stage_len) {
+    s.stage_done.emplace_back(q.stage_off, q.stage_len);
+    q.stage_len = 0;
+  }
+  GB_CUDA_TRY(cudaMemcpyAsync(rp, q.rowptr, 4ull * (q.n + 1), cudaMemcpyHostToDevice,
       s.stream));
   if (q.nnz) {
-    GB_CUDA_TRY(cudaMemcpyAsync(ri, q.rowind.data(), 4ull * q.nnz, cudaMemcpyHostToDevice,
-        s.stream));
-    GB_CUDA_TRY(cudaMemcpyAsync(v64, q.val64.data(), 8ull * q.nnz, cudaMemcpyHostToDevice,
-        s.stream));
+    GB_CUDA_TRY(cudaMemcpyAsync(ri, q.rowind, 4ull * q.nnz, cudaMemcpyHostToDevice, s.stream));
+    GB_CUDA_TRY(cudaMemcpyAsync(v64, q.val64, 8ull * q.nnz, cudaMemcpyHostToDevice, s.stream));
   }
-  GB_CUDA_TRY(cudaMemcpyAsync(bb, q.b.data(), 8ull * q.n, cudaMemcpyHostToDevice, s.stream));
+  GB_CUDA_TRY(cudaMemcpyAsync(bb, q.b, 8ull * q.n, cudaMemcpyHostToDevice, s.stream));
   if (s.mixed && q.nnz) GB_TRY(launch_round_f32(v64, v32, q.nnz, s.stream));
   S.rowptr = rp;
   S.rowind = ri;
@@ -994,12 +1063,12 @@ int tune_tile_rows(gb_server & s, const Request & q, uint32_t * best) {
   double2 * d_part = carve<double2>(mem, at, 2 * max_tiles);
   uint32_t * d_nt = carve<uint32_t>(mem, at, 1);
   cudaStream_t st = s.stream;
-  cudaError_t e = cudaMemcpyAsync(rp, q.rowptr.data(), 4ull * (n + 1), cudaMemcpyHostToDevice, st);
+  cudaError_t e = cudaMemcpyAsync(rp, q.rowptr, 4ull * (n + 1), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess && nnz)
-    e = cudaMemcpyAsync(ri, q.rowind.data(), 4ull * nnz, cudaMemcpyHostToDevice, st);
+    e = cudaMemcpyAsync(ri, q.rowind, 4ull * nnz, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess && nnz)
-    e = cudaMemcpyAsync(v64, q.val64.data(), 8ull * nnz, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(bb, q.b.data(), 8ull * n, cudaMemcpyHostToDevice, st);
+    e = cudaMemcpyAsync(v64, q.val64, 8ull * nnz, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(bb, q.b, 8ull * n, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaEventCreate(&e0);
   if (e == cudaSuccess) e = cudaEventCreate(&e1);
   if (e != cudaSuccess) fail(e);
@@ -1101,6 +1170,7 @@ int cancel(gb_server & s, uint64_t id) {
     res.t_submit = it->t_submit;
     res.t_admit = res.t_done = now_s(s);
     s.results.push_back(res);
+    if (it->stage_len) s.stage_alloc.release(it->stage_off, it->stage_len);
     s.queue.erase(it);
     return GOOSEBERRY_SUCCESS;
   }
@@ -1116,6 +1186,7 @@ int cancel(gb_server & s, uint64_t id) {
 int step(gb_server & s, size_t * active, size_t * queued) {
   const auto t_in = std::chrono::steady_clock::now();
   double waited = 0.0;
+  const bool drained = s.inflight;  // the wait below covers all earlier work on s.stream
   if (s.inflight) {
     GB_CUDA_TRY(cudaEventSynchronize(s.step_done));
     waited = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_in)
@@ -1124,6 +1195,11 @@ int step(gb_server & s, size_t * active, size_t * queued) {
     if (cudaEventElapsedTime(&ms, s.step_start, s.step_done) == cudaSuccess) s.stats.gpu_ms += ms;
     s.stats.wait_ms += waited;
     s.inflight = false;
+  }
+  if (!s.stage_done.empty()) {  // the admissions' copies ran before the replay waited on
+    if (!drained) GB_CUDA_TRY(cudaStreamSynchronize(s.stream));
+    for (const auto & r : s.stage_done) s.stage_alloc.release(r.first, r.second);
+    s.stage_done.clear();
   }
   // 1. retire finished (or cancelled) solves: copy x out, free memory and
   //    the slot
