@@ -219,3 +219,28 @@ def test_fixed_tile_rows(tile_rows):
     for bad in (100, 3000, 1 << 17):
         with pytest.raises(gb.GooseberryError):
             gb.Server(pool_bytes=1 << 28, max_slots=1, mode=gb.CG_MIXED, tile_rows=bad)
+
+
+def test_staging_arena_overflow_takes_pageable_copies():
+    """Queued requests beyond the server's pinned staging arena (64 MiB for a
+    256 MiB pool) are kept in pageable memory: every request still converges,
+    with the same bits as in a server whose arena holds them all."""
+    reqs = _requests([256] * 18, 900)  # ~4.7 MB of host arrays each: 85 MB queued
+    small = gb.Server(pool_bytes=256 << 20, max_slots=8, mode=gb.CG_MIXED, iters_per_step=8)
+    for rid, A, b in reqs:
+        small.submit(rid, A, b, tol=1e-9, niter=20000)
+    got = {r.id: r for r in small.drain()}
+    small.close()
+    big = gb.Server(pool_bytes=2 << 30, max_slots=8, mode=gb.CG_MIXED, iters_per_step=8)
+    for rid, A, b in reqs[:3] + reqs[-3:]:
+        big.submit(rid, A, b, tol=1e-9, niter=20000)
+    ref = {r.id: r for r in big.drain()}
+    big.close()
+    assert len(got) == len(reqs)
+    for rid, A, b in reqs:
+        assert got[rid].status == "converged", (rid, got[rid])
+        assert _rel(A, got[rid].x, b) <= 1.05e-9
+    for rid in ref:
+        assert got[rid].iterations == ref[rid].iterations
+        assert np.array_equal(got[rid].x, ref[rid].x), rid
+
