@@ -1071,6 +1071,13 @@ def run_extras(args):
     ex["spmv_powerlaw_8m"] = spmv_extra("spmv_powerlaw", A, W.dense_x(A.ncols, 3), peak, flush)
     ex["rcm_reorder"] = rcm_extra(A, flush)
     del A
+    # banded operators larger than L2, where x is gathered locally: the SpMV
+    # kernels' streaming rate without the random-gather floor of the power-law
+    # matrix (the 5-point Laplacian of a 4096^2 grid, 1.34 GB per SpMV)
+    A = W.laplacian_2d(4096)
+    ex["spmv_laplace_4096"] = spmv_extra("spmv_laplace_4096", A, W.dense_x(A.ncols, 4), peak,
+                                         flush)
+    del A
     ex["mixed_cg_3d_160"] = mixed_extra(peak=peak)
     ex["serving_stream"] = serving_extra(nreq=args.requests)
     ex["spmm_laplace1024_k8"] = spmm_extra(flush=flush, peak=peak)

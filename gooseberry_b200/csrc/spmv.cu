@@ -382,7 +382,7 @@ struct OutStore {
 
 template <typename V, typename Acc, int SCHED, class Gather, class Out, bool DIRECT>
 __global__ void __launch_bounds__(DIRECT ? kDirectBlock : kSpmvBlock,
-    DIRECT ? kDirectMinBlocks : MinBlocks<SCHED>::value)
+    DIRECT ? kDirectMinBlocks : TileMinBlocks<SCHED, Gather>::value)
 spmv_tiles_kernel(const PlanView plan, const uint32_t * __restrict__ rowptr,
     const uint32_t * __restrict__ rowind, const V * __restrict__ val, const Gather gather,
     Out out) {

@@ -886,6 +886,24 @@ struct IsPlainGather<GatherPlain<X>> {
   static constexpr bool value = true;
 };
 
+// Plain y = A x on the row schedule: a 7-entry stage at three CTAs per SM
+// (the 4096^2 Laplacian, 1.34 GB: 0.67 -> 0.94 of the copy peak against a
+// 6-entry stage at two; the 160^3 operator 0.64 -> 0.76).  The CG kernels,
+// whose epilogue and gathers carry more state, keep MinBlocks<SCHED_ROW>.
+#ifndef GB_PLAIN_ROW_STAGE
+#define GB_PLAIN_ROW_STAGE 7
+#endif
+#ifndef GB_PLAIN_ROW_MIN_BLOCKS
+#define GB_PLAIN_ROW_MIN_BLOCKS 3
+#endif
+constexpr int kPlainRowStage = GB_PLAIN_ROW_STAGE;
+template <int SCHED, class Gather>
+struct TileMinBlocks {
+  static constexpr int value = (SCHED == SCHED_ROW && IsPlainGather<Gather>::value)
+                                   ? GB_PLAIN_ROW_MIN_BLOCKS
+                                   : MinBlocks<SCHED>::value;
+};
+
 // Shared memory of the direct loop: rowptr slice (tile_items + 1) and products.
 template <typename Acc>
 struct DirectSmem {
@@ -1300,8 +1318,9 @@ __device__ __forceinline__ void spmv_tiles_body(const PlanView plan,
   const auto pm = L2Pol<HINT>::stream();
   const auto px = L2Pol<HINT>::keep();
   if constexpr (SCHED == SCHED_ROW) {
-    spmv_row_loop<V, Acc>(blockIdx.x * BLOCK + threadIdx.x, plan.nrows, gridDim.x * BLOCK,
-        plan.ncols, rowptr, rowind, val, gather, out, pm, px);
+    constexpr int STAGE = IsPlainGather<Gather>::value ? kPlainRowStage : kRowStage;
+    spmv_row_loop<V, Acc, STAGE>(blockIdx.x * BLOCK + threadIdx.x, plan.nrows,
+        gridDim.x * BLOCK, plan.ncols, rowptr, rowind, val, gather, out, pm, px);
   } else if constexpr (SCHED == SCHED_WTILE) {
     constexpr int W = BLOCK / 32;
     spmv_warp_loop<V, Acc>(plan, blockIdx.x * W + (threadIdx.x >> 5), plan.ntiles,
