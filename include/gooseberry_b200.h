@@ -371,6 +371,11 @@ GOOSEBERRY_API int gb_cg_row_bytes(const gb_cg_t * s, size_t * bytes);
  * the freed slots and device memory.  Admission is by device-memory
  * footprint, bounded by pool_bytes.  No reference counterpart (the reference
  * runs one cgd call at a time, src/gooseberry_bin.c:2078-2091).
+ *
+ * Host memory: a server pins a staging arena of pool_bytes / 8, at least
+ * 64 MiB and at most 2 GiB, for the life of the server.  Submitted requests
+ * are copied there, so admission uploads them asynchronously; requests that
+ * find the arena full are copied to ordinary memory instead.
  */
 typedef struct gb_server gb_server_t;
 
