@@ -935,12 +935,7 @@ int admit(gb_server & s, Request & q, uint32_t k) {
     v32 = carve<float>(base, at, q.nnz);
     x1 = carve<double>(base, at, q.n);
   }
-  // (from the staging arena these copies are asynchronous; the region goes
-  // back to the arena after the step's wait, when they are done)
-  if (q.stage_len) {
-    s.stage_done.emplace_back(q.stage_off, q.stage_len);
-    q.stage_len = 0;
-  }
+  // (from the staging arena these copies are asynchronous)
   GB_CUDA_TRY(cudaMemcpyAsync(rp, q.rowptr, 4ull * (q.n + 1), cudaMemcpyHostToDevice,
       s.stream));
   if (q.nnz) {
@@ -949,6 +944,12 @@ int admit(gb_server & s, Request & q, uint32_t k) {
   }
   GB_CUDA_TRY(cudaMemcpyAsync(bb, q.b, 8ull * q.n, cudaMemcpyHostToDevice, s.stream));
   if (s.mixed && q.nnz) GB_TRY(launch_round_f32(v64, v32, q.nnz, s.stream));
+  // the staging region goes back to the arena after the step's wait, when the
+  // copies above are done; until every copy is queued the request keeps it
+  if (q.stage_len) {
+    s.stage_done.emplace_back(q.stage_off, q.stage_len);
+    q.stage_len = 0;
+  }
   S.rowptr = rp;
   S.rowind = ri;
   S.val64 = v64;
