@@ -690,6 +690,22 @@ def mixed_extra(side=160, rtol=1e-10, reps=2, peak=None):
                     "l2_resident": False}
         else:
             d["rel_diff_to_fp64_solution"] = float(np.linalg.norm(xh - x64) / np.linalg.norm(x64))
+            if peak:
+                # A32: FP32 values, r and p gathered (4 B each per row), p_new and
+                # Ap written; stored bytes per the solver's layout (rows of 8
+                # padded values and a pattern byte on stencils)
+                eb, rb = S.entry_bytes(), S.row_bytes()
+                a_ms = prof[0]
+                bytes_csr = 4 * (n + 1) + 8 * nnz + 16 * n
+                bytes_stored = rb * (n + 1) + eb * nnz + 16 * n
+                d["roofline"] = {
+                    "bound": "hbm", "kernel": "A32 (FP32 SpMV + p update + p.Ap in FP64)",
+                    "launch_ms": a_ms, "bytes_per_launch": bytes_csr,
+                    "achieved": bytes_csr / (a_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                    "frac": bytes_csr / (a_ms * 1e-3) / 1e9 / peak,
+                    "bytes_per_launch_stored": bytes_stored,
+                    "frac_stored": bytes_stored / (a_ms * 1e-3) / 1e9 / peak,
+                    "l2_resident": False}
         out[name] = d
         S.close()
     out["speedup_mixed_over_f64"] = out["f64"]["ms"] / out["mixed"]["ms"]

@@ -182,8 +182,11 @@ __global__ void codec_pattern_table_kernel(const uint32_t * __restrict__ rowptr,
   if (h >= kSetSlots || keys[h] == kEmpty) return;
   const uint32_t row = rep[h], b = rowptr[row], e = rowptr[row + 1];
   const uint32_t c = slot_code[h];
-  for (int j = 0; j < kPatMax; ++j)
+  // pattern rows hold at most kPatMax - 1 entries: the last slot holds the
+  // pattern's length (rows that use it need no rowptr for their length)
+  for (int j = 0; j + 1 < kPatMax; ++j)
     off[c * kPatMax + j] = b + j < e ? static_cast<int32_t>(rowind[b + j] - row) : 0;
+  off[c * kPatMax + kPatMax - 1] = static_cast<int32_t>(e - b);
 }
 
 // code8[i] = pattern of row i; then every column is checked against it
@@ -200,6 +203,7 @@ __global__ void codec_pattern_encode_kernel(const uint32_t * __restrict__ rowptr
       if (__ldg(keys + h) == h0) break;
     const uint32_t c = __ldg(slot_code + h);
     code8[i] = static_cast<uint8_t>(c);
+    if (e - b != static_cast<uint32_t>(__ldg(off + c * kPatMax + kPatMax - 1))) atomicExch(bad, 1u);
     for (uint32_t k = b; k < e; ++k)
       if (__ldg(rowind + k) != i + static_cast<uint32_t>(__ldg(off + c * kPatMax + (k - b))))
         atomicExch(bad, 1u);
