@@ -245,7 +245,8 @@ def run_cg_laplace(args, dist: Dist):
     # value per nonzero, r & p gathered once, p & Ap written); the kernel
     # itself streams a lossless compressed copy of the entries when the matrix
     # allows (16-bit column distances, 8-bit codes into the table of distinct
-    # values: entry_bytes = 3 instead of 12), reported beside it
+    # values: entry_bytes = 3 instead of 12; on pattern matrices with value
+    # codes nothing per entry and 9 bytes per row), reported beside it
     entry_bytes = S.entry_bytes()
     bytes_a = 4 * (n + 1) + 12 * nnz + 32 * n
     bytes_a_stored = S.row_bytes() * (n + 1) + entry_bytes * nnz + 32 * n
@@ -321,16 +322,20 @@ def run_cg_laplace(args, dist: Dist):
             "schedule": gb.SCHED_NAMES[A.info().schedule],
             "tile_items": A.info().tile_items,
             "matrix_bytes_per_entry": entry_bytes,
+            "matrix_bytes_per_row": S.row_bytes(),
             "l2": "flushed between steps (256 MB write, outside the timed events)",
             "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "single GPU",
         },
         "roofline": {
             "bound": "hbm",
-            "kernel": ("cg_a_codec_kernel (row schedule over the compressed entries; SpMV + "
+            "kernel": ("cg_a_ell8_kernel (row patterns, value codes in rows of 8; SpMV + "
+                       "p update + p.Ap)" if entry_bytes == 0 else
+                       "cg_a_codec_kernel (row schedule over the compressed entries; SpMV + "
                        "p update + p.Ap)" if entry_bytes < 12 else
                        "cg_a_kernel (SpMV + p update + p.Ap)"),
             "achieved": ach_a, "peak": peak, "unit": "GB/s", "frac": ach_a / peak,
-            "traffic": ncu_traffic("cg_a_codec_laplace1024" if entry_bytes < 12
+            "traffic": ncu_traffic("cg_a_ell8_laplace1024" if entry_bytes == 0
+                                   else "cg_a_codec_laplace1024" if entry_bytes < 12
                                    else "cg_a_row_laplace1024"),
             "bytes_per_launch": bytes_a, "launch_ms": ms_a, "peak_source": peak_src,
             "bytes_per_launch_stored": bytes_a_stored,

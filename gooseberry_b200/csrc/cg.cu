@@ -245,6 +245,86 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED_ROW>::value) cg_a_
   o.finish();
 }
 
+#ifndef GB_CG_ELL
+#define GB_CG_ELL 1
+#endif
+// The A kernel on a pattern matrix whose values take 8-bit codes (stencils
+// with few distinct coefficients): row i's codes in rows of 8 bytes (ell8[8 i
+// ...], zero-padded), its column offsets and length from its pattern byte and
+// the shared-memory pattern table.  A row costs its pattern byte and one
+// 8-byte load, neither of which waits on rowptr.  The products, sums, epilogue
+// and per-CTA partials are cg_a_codec_kernel's (same grid, same row order), so
+// the iterates are identical.
+__global__ void ell8_codes_kernel(uint32_t n, const uint32_t * __restrict__ rowptr,
+    const uint8_t * __restrict__ code8, uint2 * __restrict__ ell8) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t b = __ldg(rowptr + i), e = __ldg(rowptr + i + 1);
+    uint32_t w[2] = {0u, 0u};
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      if (b + j < e) w[j >> 2] |= static_cast<uint32_t>(__ldg(code8 + b + j)) << (8 * (j & 3));
+    ell8[i] = make_uint2(w[0], w[1]);
+  }
+}
+
+template <bool HINT, int STAGE>
+__global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED_ROW>::value) cg_a_ell8_kernel(
+    uint32_t nrows, const uint8_t * __restrict__ pcode, const int32_t * __restrict__ pat_off,
+    uint32_t npat, const uint2 * __restrict__ ell8, const double * __restrict__ table,
+    uint32_t ntable, const double * __restrict__ r, const double * __restrict__ pold,
+    double * __restrict__ pnew, double * __restrict__ ap, double * __restrict__ partial,
+    CgState * st, RrPartials rp) {
+  __shared__ double s_table[256];
+  __shared__ __align__(16) int32_t s_pat[256 * kPatMax];
+  for (uint32_t i = threadIdx.x; i < ntable; i += kSpmvBlock) s_table[i] = table[i];
+  for (uint32_t i = threadIdx.x; i < npat * kPatMax; i += kSpmvBlock) s_pat[i] = pat_off[i];
+  __syncthreads();
+  pdl_wait_and_release();
+  double beta;
+  if (!cg_a_begin(st, rp, &beta)) return;
+  const auto pm = L2Pol<HINT>::stream();
+  const auto px = L2Pol<HINT>::keep();
+  GatherP g{r, pold, beta};
+  OutCgA o{ap, pnew, r, pold, nullptr, partial, st, beta, 0u, 0.0};
+  const uint32_t step = gridDim.x * kSpmvBlock;
+  uint32_t i = blockIdx.x * kSpmvBlock + threadIdx.x;
+  if (i < nrows) {
+    // stage: the next row's pattern, codes and own-row operands, one row ahead
+    uint32_t c_cur = ld_l1_u8(pcode + i, pm);
+    uint2 w_cur = ell8[i];
+    OutCgA::Pre q_cur = o.pre(i);
+    for (; i < nrows; i += step) {
+      const uint32_t i1 = i + step;
+      uint32_t c_nx = 0;
+      uint2 w_nx = make_uint2(0u, 0u);
+      OutCgA::Pre q_nx{};
+      if (i1 < nrows) {
+        c_nx = ld_l1_u8(pcode + i1, pm);
+        w_nx = ell8[i1];
+        q_nx = o.pre(i1);
+      }
+      const int32_t * po = s_pat + c_cur * kPatMax;
+      const int len = po[kPatMax - 1];
+      double xv[STAGE];
+#pragma unroll
+      for (int j = 0; j < STAGE; ++j)
+        if (j < len) xv[j] = g(i + static_cast<uint32_t>(po[j]), px);
+      double sum = 0.0;
+#pragma unroll
+      for (int j = 0; j < STAGE; ++j)
+        if (j < len) {
+          const uint32_t cj = ((j < 4 ? w_cur.x : w_cur.y) >> (8 * (j & 3))) & 0xffu;
+          sum = add_rn(sum, mul_rn(s_table[cj], xv[j]));
+        }
+      o.row_pre(i, sum, q_cur);
+      c_cur = c_nx;
+      w_cur = w_nx;
+      q_cur = q_nx;
+    }
+  }
+  o.finish();
+}
+
 // ---- B: x / r update and r.r ----------------------------------------------------
 
 // Every CTA first sums A's p.Ap partials (then the long-row terms) in order
@@ -875,6 +955,8 @@ struct gb_cg {
   bool l2_hint = false;  // A kernel with L2-policy loads (working set fits in L2)
   bool use_codec = false;  // row schedule over compressed entries
   gb::RowCodec codec;
+  gb::RowPatterns pat;     // pattern matrices with coded values: rows of 8 codes
+  uint2 * ell8 = nullptr;  // [n] 8 value codes per row (cg_a_ell8_kernel)
   gb::MixedCg * mixed = nullptr;  // GB_CG_MIXED solver (owns its workspace)
 };
 
@@ -886,6 +968,8 @@ void destroy_cg(gb_cg * s) {
   cudaDeviceSynchronize();  // its memory goes back to the pool below
   mixed_destroy(s->mixed);
   free_row_codec(s->codec);
+  free_row_patterns(s->pat);
+  dev_free(s->ell8);
   for (auto & g : s->graph)
     if (g) cudaGraphExecDestroy(g);
   if (s->cap_stream) cudaStreamDestroy(s->cap_stream);
@@ -913,6 +997,18 @@ RrPartials rr_partials(const gb_cg * s, size_t k) {
 // The A of iteration k (only its parity matters).
 int launch_a(gb_cg * s, size_t k, const double * pold, double * pnew, cudaStream_t cs,
     bool pdl) {
+  if (s->ell8) {  // same grid as the codec kernel: the same partials
+    auto kern = s->codec.stage == 5
+                    ? (s->l2_hint ? cg_a_ell8_kernel<true, 5> : cg_a_ell8_kernel<false, 5>)
+                    : (s->l2_hint ? cg_a_ell8_kernel<true, 7> : cg_a_ell8_kernel<false, 7>);
+    GB_CUDA_TRY(launch_k(kern, s->grid_a, kSpmvBlock, 0, cs, pdl,
+        static_cast<uint32_t>(s->n), static_cast<const uint8_t *>(s->pat.code8),
+        static_cast<const int32_t *>(s->pat.off), s->pat.npat,
+        static_cast<const uint2 *>(s->ell8), static_cast<const double *>(s->codec.table),
+        s->codec.ntable, static_cast<const double *>(s->r), pold, pnew, s->ap, s->partial_a,
+        s->st, rr_partials(s, k)));
+    return GOOSEBERRY_SUCCESS;
+  }
   return s->use_codec
              ? launch_cg_a_codec(*s->a, s->codec, s->l2_hint, s->r, pold, pnew, s->ap,
                    s->longdot, s->partial_a, s->st, rr_partials(s, k), s->grid_a, cs, pdl)
@@ -1083,10 +1179,25 @@ int create_cg(const gb_csr * a, int mode, gb_cg * s) {
     GB_TRY(build_row_codec(*a, &s->codec, nullptr));
     s->use_codec = s->codec.col16 || s->codec.code8 || s->codec.val32;
     entry_bytes = s->codec.entry_bytes();
+    // coded values on a pattern matrix: the codes in rows of 8, no rowptr
+    if (GB_CG_ELL && s->codec.code8 && (s->codec.stage == 5 || s->codec.stage == 7)) {
+      GB_TRY(build_row_patterns(*a, &s->pat, nullptr));
+      if (s->pat.code8) {
+        GB_TRY(dev_alloc(&s->ell8, std::max<size_t>(s->n, 1) * sizeof(uint2)));
+        const unsigned g = static_cast<unsigned>(std::max<size_t>(1, std::min<size_t>(
+            (s->n + 255) / 256, static_cast<size_t>(a->sm_count) * 8)));
+        ell8_codes_kernel<<<g, 256>>>(static_cast<uint32_t>(s->n), a->rowptr, s->codec.code8,
+            s->ell8);
+        GB_CUDA_TRY(cudaGetLastError());
+        GB_CUDA_TRY(cudaDeviceSynchronize());
+        entry_bytes = 0;
+      }
+    }
   }
   // evict-first/evict-last hints keep an L2-sized working set (matrix, rowptr,
   // r, both p, Ap, x) resident across iterations; beyond L2 the plain loads win
-  GB_TRY(l2_fits(4ull * (s->n + 1) + entry_bytes * a->nnz + 40ull * s->n, &s->l2_hint));
+  GB_TRY(l2_fits((s->ell8 ? 9ull : 4ull) * (s->n + 1) + entry_bytes * a->nnz + 40ull * s->n,
+      &s->l2_hint));
   const size_t smem = spmv_smem(s->sched, a->plan.tile_items);
   int occ = 0;
   if (s->use_codec)
@@ -1369,13 +1480,14 @@ int gb_cg_set_barrier_fault(gb_cg_t * s, int drop_cta, unsigned limit_ms) {
 
 int gb_cg_entry_bytes(const gb_cg_t * s, size_t * bytes) {
   GB_CHECK_INPUT(s != nullptr && bytes != nullptr, "NULL argument");
-  *bytes = s->mixed ? mixed_entry_bytes(s->mixed) : (s->use_codec ? s->codec.entry_bytes() : 12);
+  *bytes = s->mixed ? mixed_entry_bytes(s->mixed)
+                     : (s->ell8 ? 0 : (s->use_codec ? s->codec.entry_bytes() : 12));
   return GOOSEBERRY_SUCCESS;
 }
 
 int gb_cg_row_bytes(const gb_cg_t * s, size_t * bytes) {
   GB_CHECK_INPUT(s != nullptr && bytes != nullptr, "NULL argument");
-  *bytes = s->mixed ? mixed_row_bytes(s->mixed) : 4;
+  *bytes = s->mixed ? mixed_row_bytes(s->mixed) : (s->ell8 ? 9 : 4);
   return GOOSEBERRY_SUCCESS;
 }
 

@@ -96,7 +96,7 @@ def many_patterns(n, seed):
 
 CASES = {
     # name: (matrix builder, expected bytes per entry, per row)
-    "laplace64": (lambda: W.laplacian_2d(64), 3, 4),           # 16-bit columns, value codes
+    "laplace64": (lambda: W.laplacian_2d(64), 0, 9),           # patterns, rows of 8 value codes
     "diffusion2d": (lambda: W.diffusion_2d(48, seed=5), 10, 4),  # 16-bit columns, doubles
     "diffusion2d_f32": (lambda: float_exact(W.diffusion_2d(48, seed=6)), 6, 4),
     "graph": (lambda: graph_laplacian(40000, 4, 7), 5, 4),      # 32-bit columns, codes
