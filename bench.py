@@ -51,6 +51,20 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
 
 
+def cg_a_kernel_name(entry_bytes, row_bytes):
+    """The FP64 CG's A kernel for the solver's matrix layout (stored bytes per
+    entry and per row)."""
+    if entry_bytes == 0:
+        return ("cg_a_ell8_kernel (row patterns, value codes in rows of 8; SpMV + "
+                "p update + p.Ap)" if row_bytes == 9 else
+                "cg_a_ellv_kernel (row patterns, values in rows of 6 or 8; SpMV + "
+                "p update + p.Ap)")
+    if entry_bytes < 12:
+        return ("cg_a_codec_kernel (row schedule over the compressed entries; SpMV + "
+                "p update + p.Ap)")
+    return "cg_a_kernel (SpMV + p update + p.Ap)"
+
+
 def ncu_traffic(kernel_key: str):
     """Per-launch DRAM bytes of a kernel from a committed ncu summary
     (profiles/*.txt lines `traffic_bytes_per_launch <key> <bytes> <scale>`)."""
@@ -248,6 +262,7 @@ def run_cg_laplace(args, dist: Dist):
     # values: entry_bytes = 3 instead of 12; on pattern matrices with value
     # codes nothing per entry and 9 bytes per row), reported beside it
     entry_bytes = S.entry_bytes()
+    ell8 = entry_bytes == 0 and S.row_bytes() == 9  # pattern byte + 8 value codes
     bytes_a = 4 * (n + 1) + 12 * nnz + 32 * n
     bytes_a_stored = S.row_bytes() * (n + 1) + entry_bytes * nnz + 32 * n
     bytes_b = 48 * n                             # x, p, r, Ap read; x, r written
@@ -328,13 +343,10 @@ def run_cg_laplace(args, dist: Dist):
         },
         "roofline": {
             "bound": "hbm",
-            "kernel": ("cg_a_ell8_kernel (row patterns, value codes in rows of 8; SpMV + "
-                       "p update + p.Ap)" if entry_bytes == 0 else
-                       "cg_a_codec_kernel (row schedule over the compressed entries; SpMV + "
-                       "p update + p.Ap)" if entry_bytes < 12 else
-                       "cg_a_kernel (SpMV + p update + p.Ap)"),
+            "kernel": cg_a_kernel_name(entry_bytes, S.row_bytes()),
             "achieved": ach_a, "peak": peak, "unit": "GB/s", "frac": ach_a / peak,
-            "traffic": ncu_traffic("cg_a_ell8_laplace1024" if entry_bytes == 0
+            "traffic": ncu_traffic("cg_a_ell8_laplace1024" if ell8
+                                   else "cg_a_ellv_laplace1024" if entry_bytes == 0
                                    else "cg_a_codec_laplace1024" if entry_bytes < 12
                                    else "cg_a_row_laplace1024"),
             "bytes_per_launch": bytes_a, "launch_ms": ms_a, "peak_source": peak_src,
@@ -686,7 +698,7 @@ def mixed_extra(side=160, rtol=1e-10, reps=2, peak=None):
                 bytes_csr = 4 * (n + 1) + 12 * nnz + 32 * n
                 bytes_stored = rb * (n + 1) + eb * nnz + 32 * n
                 d["roofline"] = {
-                    "bound": "hbm", "kernel": "cg_a_codec_kernel (FP64 SpMV + p update + p.Ap)",
+                    "bound": "hbm", "kernel": cg_a_kernel_name(eb, rb),
                     "launch_ms": a_ms, "bytes_per_launch": bytes_csr,
                     "achieved": bytes_csr / (a_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                     "frac": bytes_csr / (a_ms * 1e-3) / 1e9 / peak,

@@ -248,13 +248,19 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED_ROW>::value) cg_a_
 #ifndef GB_CG_ELL
 #define GB_CG_ELL 1
 #endif
-// The A kernel on a pattern matrix whose values take 8-bit codes (stencils
-// with few distinct coefficients): row i's codes in rows of 8 bytes (ell8[8 i
-// ...], zero-padded), its column offsets and length from its pattern byte and
-// the shared-memory pattern table.  A row costs its pattern byte and one
-// 8-byte load, neither of which waits on rowptr.  The products, sums, epilogue
-// and per-CTA partials are cg_a_codec_kernel's (same grid, same row order), so
-// the iterates are identical.
+// The A kernels on a pattern matrix (every row at most 7 entries, at most 256
+// distinct column-offset patterns): a row's column offsets and length come
+// from its pattern byte and the shared-memory pattern table, its values from
+// a row of 8 slots (zero-padded) that neither waits on rowptr nor on the
+// pattern.  Three value rows:
+//   EllCodes     8-bit codes into the shared table of distinct values (8 B per
+//                row: one 8-byte load),
+//   EllVals<T>   the values themselves, T = double (rows of 6 when no row has
+//                more than 5 entries, else 8: three or four 16-byte loads) or
+//                T = float when every double is exactly a float (rows of 8:
+//                two 16-byte loads).
+// The products, sums, epilogue and per-CTA partials are cg_a_codec_kernel's
+// (same grid, same row order), so the iterates are identical.
 __global__ void ell8_codes_kernel(uint32_t n, const uint32_t * __restrict__ rowptr,
     const uint8_t * __restrict__ code8, uint2 * __restrict__ ell8) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -264,6 +270,102 @@ __global__ void ell8_codes_kernel(uint32_t n, const uint32_t * __restrict__ rowp
     for (int j = 0; j < 8; ++j)
       if (b + j < e) w[j >> 2] |= static_cast<uint32_t>(__ldg(code8 + b + j)) << (8 * (j & 3));
     ell8[i] = make_uint2(w[0], w[1]);
+  }
+}
+
+// out[W i + j] = val[rowptr[i] + j] for j < the row's length, else 0.
+template <typename T, int W>
+__global__ void ell_vals_kernel(uint32_t n, const uint32_t * __restrict__ rowptr,
+    const T * __restrict__ val, T * __restrict__ out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t b = __ldg(rowptr + i), e = __ldg(rowptr + i + 1);
+#pragma unroll
+    for (int j = 0; j < W; ++j)
+      out[static_cast<size_t>(W) * i + j] = b + j < e ? __ldg(val + b + j) : T(0);
+  }
+}
+
+struct EllCodes {
+  const uint2 * rows;
+  const double * table;  // shared memory
+  using Row = uint2;
+  __device__ __forceinline__ Row load(uint32_t i) const { return rows[i]; }
+  __device__ __forceinline__ static Row zero() { return make_uint2(0u, 0u); }
+  __device__ __forceinline__ double value(const Row & w, int j) const {
+    return table[((j < 4 ? w.x : w.y) >> (8 * (j & 3))) & 0xffu];
+  }
+};
+
+// Row width in elements for a register stage of STAGE entries.
+template <typename T, int STAGE>
+struct EllWidth {
+  static constexpr int value = (sizeof(T) == 8 && STAGE <= 6) ? 6 : 8;
+};
+
+template <typename T, int STAGE>
+struct EllVals {
+  static constexpr int kW = EllWidth<T, STAGE>::value;
+  static constexpr int kPer = 16 / static_cast<int>(sizeof(T));  // elements per load
+  static constexpr int kVec = (STAGE + kPer - 1) / kPer;          // loads per row
+  using V = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
+  const T * rows;
+  struct Row {
+    V v[kVec];
+  };
+  __device__ __forceinline__ Row load(uint32_t i) const {
+    const V * p = reinterpret_cast<const V *>(rows + static_cast<size_t>(kW) * i);
+    Row w;
+#pragma unroll
+    for (int k = 0; k < kVec; ++k) w.v[k] = p[k];
+    return w;
+  }
+  __device__ __forceinline__ static Row zero() { return Row{}; }
+  __device__ __forceinline__ static double elem(const double2 & v, int k) {
+    return k == 0 ? v.x : v.y;
+  }
+  __device__ __forceinline__ static double elem(const float4 & v, int k) {
+    return static_cast<double>(k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w);
+  }
+  __device__ __forceinline__ double value(const Row & w, int j) const {
+    return elem(w.v[j / kPer], j % kPer);
+  }
+};
+
+// The row loop shared by the ELL A kernels: the next row's pattern byte,
+// value row and own-row operands are loaded one row ahead.
+template <int STAGE, class EV, class PM, class PX>
+__device__ __forceinline__ void cg_a_ell_rows(uint32_t nrows, const uint8_t * __restrict__ pcode,
+    const int32_t * s_pat, const EV & ev, const GatherP & g, OutCgA & o, PM pm, PX px) {
+  const uint32_t step = gridDim.x * kSpmvBlock;
+  uint32_t i = blockIdx.x * kSpmvBlock + threadIdx.x;
+  if (i >= nrows) return;
+  uint32_t c_cur = ld_l1_u8(pcode + i, pm);
+  typename EV::Row w_cur = ev.load(i);
+  OutCgA::Pre q_cur = o.pre(i);
+  for (; i < nrows; i += step) {
+    const uint32_t i1 = i + step;
+    uint32_t c_nx = 0;
+    typename EV::Row w_nx = EV::zero();
+    OutCgA::Pre q_nx{};
+    if (i1 < nrows) {
+      c_nx = ld_l1_u8(pcode + i1, pm);
+      w_nx = ev.load(i1);
+      q_nx = o.pre(i1);
+    }
+    const int32_t * po = s_pat + c_cur * kPatMax;
+    const int len = po[kPatMax - 1];
+    double xv[STAGE];
+#pragma unroll
+    for (int j = 0; j < STAGE; ++j)
+      if (j < len) xv[j] = g(i + static_cast<uint32_t>(po[j]), px);
+    double sum = 0.0;
+#pragma unroll
+    for (int j = 0; j < STAGE; ++j)
+      if (j < len) sum = add_rn(sum, mul_rn(ev.value(w_cur, j), xv[j]));
+    o.row_pre(i, sum, q_cur);
+    c_cur = c_nx;
+    w_cur = w_nx;
+    q_cur = q_nx;
   }
 }
 
@@ -282,46 +384,29 @@ __global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED_ROW>::value) cg_a_
   pdl_wait_and_release();
   double beta;
   if (!cg_a_begin(st, rp, &beta)) return;
-  const auto pm = L2Pol<HINT>::stream();
-  const auto px = L2Pol<HINT>::keep();
   GatherP g{r, pold, beta};
   OutCgA o{ap, pnew, r, pold, nullptr, partial, st, beta, 0u, 0.0};
-  const uint32_t step = gridDim.x * kSpmvBlock;
-  uint32_t i = blockIdx.x * kSpmvBlock + threadIdx.x;
-  if (i < nrows) {
-    // stage: the next row's pattern, codes and own-row operands, one row ahead
-    uint32_t c_cur = ld_l1_u8(pcode + i, pm);
-    uint2 w_cur = ell8[i];
-    OutCgA::Pre q_cur = o.pre(i);
-    for (; i < nrows; i += step) {
-      const uint32_t i1 = i + step;
-      uint32_t c_nx = 0;
-      uint2 w_nx = make_uint2(0u, 0u);
-      OutCgA::Pre q_nx{};
-      if (i1 < nrows) {
-        c_nx = ld_l1_u8(pcode + i1, pm);
-        w_nx = ell8[i1];
-        q_nx = o.pre(i1);
-      }
-      const int32_t * po = s_pat + c_cur * kPatMax;
-      const int len = po[kPatMax - 1];
-      double xv[STAGE];
-#pragma unroll
-      for (int j = 0; j < STAGE; ++j)
-        if (j < len) xv[j] = g(i + static_cast<uint32_t>(po[j]), px);
-      double sum = 0.0;
-#pragma unroll
-      for (int j = 0; j < STAGE; ++j)
-        if (j < len) {
-          const uint32_t cj = ((j < 4 ? w_cur.x : w_cur.y) >> (8 * (j & 3))) & 0xffu;
-          sum = add_rn(sum, mul_rn(s_table[cj], xv[j]));
-        }
-      o.row_pre(i, sum, q_cur);
-      c_cur = c_nx;
-      w_cur = w_nx;
-      q_cur = q_nx;
-    }
-  }
+  cg_a_ell_rows<STAGE>(nrows, pcode, s_pat, EllCodes{ell8, s_table}, g, o,
+      L2Pol<HINT>::stream(), L2Pol<HINT>::keep());
+  o.finish();
+}
+
+template <bool HINT, int STAGE, typename T>
+__global__ void __launch_bounds__(kSpmvBlock, MinBlocks<SCHED_ROW>::value) cg_a_ellv_kernel(
+    uint32_t nrows, const uint8_t * __restrict__ pcode, const int32_t * __restrict__ pat_off,
+    uint32_t npat, const T * __restrict__ vals, const double * __restrict__ r,
+    const double * __restrict__ pold, double * __restrict__ pnew, double * __restrict__ ap,
+    double * __restrict__ partial, CgState * st, RrPartials rp) {
+  __shared__ __align__(16) int32_t s_pat[256 * kPatMax];
+  for (uint32_t i = threadIdx.x; i < npat * kPatMax; i += kSpmvBlock) s_pat[i] = pat_off[i];
+  __syncthreads();
+  pdl_wait_and_release();
+  double beta;
+  if (!cg_a_begin(st, rp, &beta)) return;
+  GatherP g{r, pold, beta};
+  OutCgA o{ap, pnew, r, pold, nullptr, partial, st, beta, 0u, 0.0};
+  cg_a_ell_rows<STAGE>(nrows, pcode, s_pat, EllVals<T, STAGE>{vals}, g, o,
+      L2Pol<HINT>::stream(), L2Pol<HINT>::keep());
   o.finish();
 }
 
@@ -957,6 +1042,8 @@ struct gb_cg {
   gb::RowCodec codec;
   gb::RowPatterns pat;     // pattern matrices with coded values: rows of 8 codes
   uint2 * ell8 = nullptr;  // [n] 8 value codes per row (cg_a_ell8_kernel)
+  void * ellv = nullptr;   // [n * width] values per row (cg_a_ellv_kernel)
+  bool ellv_f32 = false;   // ellv holds floats (every value exactly a float)
   gb::MixedCg * mixed = nullptr;  // GB_CG_MIXED solver (owns its workspace)
 };
 
@@ -970,6 +1057,7 @@ void destroy_cg(gb_cg * s) {
   free_row_codec(s->codec);
   free_row_patterns(s->pat);
   dev_free(s->ell8);
+  dev_free(s->ellv);
   for (auto & g : s->graph)
     if (g) cudaGraphExecDestroy(g);
   if (s->cap_stream) cudaStreamDestroy(s->cap_stream);
@@ -987,6 +1075,15 @@ void destroy_cg(gb_cg * s) {
   pinned_slot_free(s->host_status);
   pinned_slot_free(s->cancel_h);
   delete s;
+}
+
+// Stored matrix bytes per row outside the entries: rowptr, or a pattern byte
+// and a row of values or codes.
+size_t cg_row_bytes(const gb_cg * s) {
+  if (s->ell8) return 1 + 8;
+  if (s->ellv)
+    return 1 + (s->ellv_f32 ? 8 * sizeof(float) : (s->codec.stage == 5 ? 6 : 8) * sizeof(double));
+  return 4;
 }
 
 // The partials the A of iteration k reads (B of iteration k - 1 wrote them).
@@ -1007,6 +1104,29 @@ int launch_a(gb_cg * s, size_t k, const double * pold, double * pnew, cudaStream
         static_cast<const uint2 *>(s->ell8), static_cast<const double *>(s->codec.table),
         s->codec.ntable, static_cast<const double *>(s->r), pold, pnew, s->ap, s->partial_a,
         s->st, rr_partials(s, k)));
+    return GOOSEBERRY_SUCCESS;
+  }
+  if (s->ellv) {  // same grid as the codec kernel: the same partials
+    const auto common = [&](auto kern, const auto * vals) {
+      return launch_k(kern, s->grid_a, kSpmvBlock, 0, cs, pdl, static_cast<uint32_t>(s->n),
+          static_cast<const uint8_t *>(s->pat.code8), static_cast<const int32_t *>(s->pat.off),
+          s->pat.npat, vals, static_cast<const double *>(s->r), pold, pnew, s->ap,
+          s->partial_a, s->st, rr_partials(s, k));
+    };
+    const bool s5 = s->codec.stage == 5, h = s->l2_hint;
+    if (s->ellv_f32) {
+      const float * v = static_cast<const float *>(s->ellv);
+      GB_CUDA_TRY(s5 ? (h ? common(cg_a_ellv_kernel<true, 5, float>, v)
+                          : common(cg_a_ellv_kernel<false, 5, float>, v))
+                     : (h ? common(cg_a_ellv_kernel<true, 7, float>, v)
+                          : common(cg_a_ellv_kernel<false, 7, float>, v)));
+    } else {
+      const double * v = static_cast<const double *>(s->ellv);
+      GB_CUDA_TRY(s5 ? (h ? common(cg_a_ellv_kernel<true, 5, double>, v)
+                          : common(cg_a_ellv_kernel<false, 5, double>, v))
+                     : (h ? common(cg_a_ellv_kernel<true, 7, double>, v)
+                          : common(cg_a_ellv_kernel<false, 7, double>, v)));
+    }
     return GOOSEBERRY_SUCCESS;
   }
   return s->use_codec
@@ -1179,15 +1299,31 @@ int create_cg(const gb_csr * a, int mode, gb_cg * s) {
     GB_TRY(build_row_codec(*a, &s->codec, nullptr));
     s->use_codec = s->codec.col16 || s->codec.code8 || s->codec.val32;
     entry_bytes = s->codec.entry_bytes();
-    // coded values on a pattern matrix: the codes in rows of 8, no rowptr
-    if (GB_CG_ELL && s->codec.code8 && (s->codec.stage == 5 || s->codec.stage == 7)) {
+    // a pattern matrix: its values (or their codes) in rows of 8, no rowptr
+    if (GB_CG_ELL && a->nnz > 0 && (s->codec.stage == 5 || s->codec.stage == 7)) {
       GB_TRY(build_row_patterns(*a, &s->pat, nullptr));
       if (s->pat.code8) {
-        GB_TRY(dev_alloc(&s->ell8, std::max<size_t>(s->n, 1) * sizeof(uint2)));
+        const size_t rows = std::max<size_t>(s->n, 1);
         const unsigned g = static_cast<unsigned>(std::max<size_t>(1, std::min<size_t>(
             (s->n + 255) / 256, static_cast<size_t>(a->sm_count) * 8)));
-        ell8_codes_kernel<<<g, 256>>>(static_cast<uint32_t>(s->n), a->rowptr, s->codec.code8,
-            s->ell8);
+        const uint32_t nr = static_cast<uint32_t>(s->n);
+        if (s->codec.code8) {
+          GB_TRY(dev_alloc(&s->ell8, rows * sizeof(uint2)));
+          ell8_codes_kernel<<<g, 256>>>(nr, a->rowptr, s->codec.code8, s->ell8);
+        } else if (s->codec.val32) {
+          GB_TRY(dev_alloc(&s->ellv, rows * 8 * sizeof(float)));
+          ell_vals_kernel<float, 8><<<g, 256>>>(nr, a->rowptr, s->codec.val32,
+              static_cast<float *>(s->ellv));
+          s->ellv_f32 = true;
+        } else if (s->codec.stage == 5) {
+          GB_TRY(dev_alloc(&s->ellv, rows * 6 * sizeof(double)));
+          ell_vals_kernel<double, 6><<<g, 256>>>(nr, a->rowptr, a->val64,
+              static_cast<double *>(s->ellv));
+        } else {
+          GB_TRY(dev_alloc(&s->ellv, rows * 8 * sizeof(double)));
+          ell_vals_kernel<double, 8><<<g, 256>>>(nr, a->rowptr, a->val64,
+              static_cast<double *>(s->ellv));
+        }
         GB_CUDA_TRY(cudaGetLastError());
         GB_CUDA_TRY(cudaDeviceSynchronize());
         entry_bytes = 0;
@@ -1196,7 +1332,7 @@ int create_cg(const gb_csr * a, int mode, gb_cg * s) {
   }
   // evict-first/evict-last hints keep an L2-sized working set (matrix, rowptr,
   // r, both p, Ap, x) resident across iterations; beyond L2 the plain loads win
-  GB_TRY(l2_fits((s->ell8 ? 9ull : 4ull) * (s->n + 1) + entry_bytes * a->nnz + 40ull * s->n,
+  GB_TRY(l2_fits(cg_row_bytes(s) * (s->n + 1) + entry_bytes * a->nnz + 40ull * s->n,
       &s->l2_hint));
   const size_t smem = spmv_smem(s->sched, a->plan.tile_items);
   int occ = 0;
@@ -1481,13 +1617,13 @@ int gb_cg_set_barrier_fault(gb_cg_t * s, int drop_cta, unsigned limit_ms) {
 int gb_cg_entry_bytes(const gb_cg_t * s, size_t * bytes) {
   GB_CHECK_INPUT(s != nullptr && bytes != nullptr, "NULL argument");
   *bytes = s->mixed ? mixed_entry_bytes(s->mixed)
-                     : (s->ell8 ? 0 : (s->use_codec ? s->codec.entry_bytes() : 12));
+                     : ((s->ell8 || s->ellv) ? 0 : (s->use_codec ? s->codec.entry_bytes() : 12));
   return GOOSEBERRY_SUCCESS;
 }
 
 int gb_cg_row_bytes(const gb_cg_t * s, size_t * bytes) {
   GB_CHECK_INPUT(s != nullptr && bytes != nullptr, "NULL argument");
-  *bytes = s->mixed ? mixed_row_bytes(s->mixed) : (s->ell8 ? 9 : 4);
+  *bytes = s->mixed ? mixed_row_bytes(s->mixed) : gb::cg_row_bytes(s);
   return GOOSEBERRY_SUCCESS;
 }
 

@@ -1,7 +1,8 @@
 """The FP64 CG's compressed matrix entries (16-bit column distances, 8-bit
-value codes, exact float values; GB_CG_PLAIN_ENTRIES turns them off) change
-only the bytes streamed: every solve is bit-identical to the solve over the
-plain CSR arrays, on matrices that take each encoding."""
+value codes, exact float values, and on pattern matrices a pattern byte with
+the row's values or codes in a row of 6 or 8; GB_CG_PLAIN_ENTRIES turns them
+off) change only the bytes streamed: every solve is bit-identical to the solve
+over the plain CSR arrays, on matrices that take each encoding."""
 from __future__ import annotations
 
 import numpy as np
@@ -96,9 +97,17 @@ def many_patterns(n, seed):
 
 CASES = {
     # name: (matrix builder, expected bytes per entry, per row)
-    "laplace64": (lambda: W.laplacian_2d(64), 0, 9),           # patterns, rows of 8 value codes
-    "diffusion2d": (lambda: W.diffusion_2d(48, seed=5), 10, 4),  # 16-bit columns, doubles
-    "diffusion2d_f32": (lambda: float_exact(W.diffusion_2d(48, seed=6)), 6, 4),
+    # row patterns: a pattern byte and a row of value codes (8), doubles (6 when
+    # no row has more than 5 entries, else 8) or floats (8) per row
+    "laplace64": (lambda: W.laplacian_2d(64), 0, 9),
+    "diffusion2d": (lambda: W.diffusion_2d(48, seed=5), 0, 49),
+    "diffusion2d_f32": (lambda: float_exact(W.diffusion_2d(48, seed=6)), 0, 33),
+    "diffusion3d": (lambda: W.diffusion_3d(24, seed=11), 0, 65),
+    "diffusion3d_f32": (lambda: float_exact(W.diffusion_3d(24, seed=13)), 0, 33),
+    "band": (lambda: banded(5000, [-200, -3, -1, 0, 1, 3, 200], 8), 0, 65),
+    # too many patterns: 16-bit columns and doubles (or exact floats) per entry
+    "many_patterns": (lambda: many_patterns(20000, 10), 10, 4),
+    "many_patterns_f32": (lambda: float_exact(many_patterns(20000, 14)), 6, 4),
     "graph": (lambda: graph_laplacian(40000, 4, 7), 5, 4),      # 32-bit columns, codes
     "graph_weighted": (lambda: graph_laplacian(40000, 4, 8, weights=True), 12, 4),
 }
