@@ -348,15 +348,18 @@ GOOSEBERRY_API int gb_cg_profile(gb_cg_t * s, const double * b, size_t iteration
 
 /* Bytes per matrix entry the solver's SpMV streams: 12 for the plain arrays
  * (4-byte column, 8-byte value); 2 + the value bytes with 16-bit column
- * distances; for MIXED the float value alone when the columns are a pattern
- * byte per row (rows of at most 7 entries forming at most 256 distinct lists
- * of column offsets from the diagonal: stencils); F64 values as 8-bit codes
- * (1), exact floats (4) or doubles (8) (see GB_CG_PLAIN_ENTRIES).  No
- * reference counterpart. */
+ * distances, F64 values as 8-bit codes (1), exact floats (4) or doubles (8)
+ * (see GB_CG_PLAIN_ENTRIES); 0 on a pattern matrix (rows of at most 7 entries
+ * forming at most 256 distinct lists of column offsets from the diagonal:
+ * stencils), whose values the solver keeps in rows of fixed width (see
+ * gb_cg_row_bytes).  No reference counterpart. */
 GOOSEBERRY_API int gb_cg_entry_bytes(const gb_cg_t * s, size_t * bytes);
 
-/* Bytes per row the solver's SpMV streams besides the entries: 4 (rowptr), 5
- * with a column-pattern byte.  No reference counterpart. */
+/* Bytes per row the solver's SpMV streams besides the entries: 4 (rowptr);
+ * on a pattern matrix a pattern byte and the row's zero-padded values or
+ * codes instead: 9 (8 codes), 33 (8 floats; MIXED, or exact floats), 49 or
+ * 65 (6 or 8 doubles); 5 (rowptr and a pattern byte) for MIXED in builds
+ * without its rows of values.  No reference counterpart. */
 GOOSEBERRY_API int gb_cg_row_bytes(const gb_cg_t * s, size_t * bytes);
 
 /* ---- batched solve server (continuous batching) ---------------------------- */
