@@ -33,6 +33,16 @@
 // first check happens after the first update, iteration k (0-based) is
 // counted before its check, and the bound is on the absolute ||r||_2
 // (src/cgd.c:87,115-119).
+//
+// A reads the matrix in the leanest layout it allows, all summing each row's
+// products in CSR order (so the iterates never depend on the layout):
+//   cg_a_kernel        the CSR arrays, on the matrix's SpMV schedule
+//   cg_a_codec_kernel  row schedule, compressed entries (16-bit column
+//                      distances; 8-bit value codes or exact floats)
+//   cg_a_ell8_kernel   pattern matrices with 8-bit value codes: a pattern byte
+//                      and a row of 8 codes per row, no rowptr
+//   cg_a_ellv_kernel   other pattern matrices: a pattern byte and a row of 6
+//                      or 8 values (doubles, or floats when exact) per row
 #include <algorithm>
 #include <cmath>
 #include <type_traits>
