@@ -235,3 +235,14 @@ def test_cgd_out_is_checked_before_any_call():
                 np.zeros((L.nrows, 2))[:, 0]):
         with pytest.raises(ValueError):
             gb.cgd(L.rowptr, L.rowind, L.rowval, b, 1e-8, 100, out=bad)
+
+
+def test_cgd_rejects_an_empty_system_on_the_host():
+    """CG on a 0 x 0 system is refused as an input error before any device
+    work, both value widths (the reference's first step would form
+    alpha = 0 / 0, src/cgd.c:89)."""
+    for dt in (np.float64, np.float32):
+        with pytest.raises(gb.GooseberryError) as e:
+            gb.cgd(np.zeros(1, np.uint32), np.zeros(0, np.uint32), np.zeros(0, dt),
+                   np.zeros(0, dt), 1e-8, 10)
+        assert e.value.code == 3 and "non-empty" in str(e.value)
