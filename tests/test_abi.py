@@ -240,7 +240,7 @@ def test_cgd_out_is_checked_before_any_call():
 def test_cgd_rejects_an_empty_system_on_the_host():
     """CG on a 0 x 0 system is refused as an input error before any device
     work, both value widths (the reference's first step would form
-    alpha = 0 / 0, src/cgd.c:89)."""
+    alpha = 0 / 0, src/cgd.c:90)."""
     for dt in (np.float64, np.float32):
         with pytest.raises(gb.GooseberryError) as e:
             gb.cgd(np.zeros(1, np.uint32), np.zeros(0, np.uint32), np.zeros(0, dt),
